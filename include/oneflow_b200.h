@@ -1,0 +1,171 @@
+/*
+ * oneflow_b200.h -- C ABI of the B200 implementation of OneFLOW's
+ * unstructured finite-volume residual + LU-SGS update path.
+ *
+ * The reference dispatches one iteration of a steady solve as string tasks
+ * (codes/solver/src/TimeIntegral.cpp:113-130, names mapped to classes in
+ * system/ns/function/funcMap.txt) operating on fields owned by UnsGrid.  Each
+ * task below replaces one of those tasks for one solver (tid 0 = NS_SOLVER,
+ * tid 1 = TURB_SOLVER); the context owns the device copies of every field.
+ *
+ * All functions return 0 on success and a negative OFG_E* code on failure;
+ * ofg_last_error() gives the message.  Nothing aborts the process (the
+ * reference's Stop() at codes/project/src/Stop.cpp:27-40 is replaced by
+ * status codes).  Host pointers are borrowed for the duration of the call.
+ * Arrays use the reference's numbering and its structure-of-arrays layout:
+ * a per-equation field is [nEqu][nCells + nBFaces] (ghost cell of boundary
+ * face f at index nCells + f), matching MRField in
+ * codes/array/include/Marray.h:29-60.
+ */
+#ifndef ONEFLOW_B200_H
+#define ONEFLOW_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define OFG_OK            0
+#define OFG_E_ARG        -1   /* bad argument / size                         */
+#define OFG_E_CUDA       -2   /* CUDA runtime error                          */
+#define OFG_E_NAN        -3   /* NaN in a residual (reference: Stop("NotANumber"),
+                                 codes/residual/src/ResidualTask.cpp:95-100)   */
+#define OFG_E_STATE      -4   /* call out of order (no mesh, no state, ...)  */
+#define OFG_E_TIMEOUT    -5   /* a bounded device wait gave up               */
+#define OFG_E_NOMEM      -6   /* device allocation failed                    */
+
+/* solver ids (reference SolverState::tid, codes/solver/src/SolverState.cpp) */
+#define OFG_NS_SOLVER     0
+#define OFG_TURB_SOLVER   1
+
+/* boundary codes (reference BC::*, codes/geometry/src/Boundary.cpp:35-54) */
+#define OFG_BC_EXTRAPOLATION 1
+#define OFG_BC_SOLID_SURFACE 2
+#define OFG_BC_SYMMETRY      3
+#define OFG_BC_FARFIELD      4
+#define OFG_BC_INFLOW        5
+#define OFG_BC_OUTFLOW       6
+
+/* arithmetic of the face terms */
+#define OFG_PREC_FP64     0   /* every step in FP64 (the all-FP64 oracle path) */
+#define OFG_PREC_MIXED    1   /* FP32 fluxes/gradients/limiters/SA source; FP64
+                                 residual accumulation, update and norms        */
+
+/*
+ * Solver parameters: the script keys the reference reads with
+ * GetDataValue<T>("key") on this path (codes/ns/src/NsCom.cpp:45-94,
+ * codes/global/src/Ctrl.cpp:40-113, codes/turb/src/TurbCom.cpp:110-350).
+ * ofg_default_params() fills the reference's test-case defaults.
+ */
+typedef struct ofg_params {
+    int    dimension;        /* 2 or 3                                         */
+    int    ischeme;          /* 1 Roe, 12 SLAU2                                */
+    int    ilim;             /* -1 first order, 0 none, 1 Barth, 2 Venkat      */
+    int    igrad;            /* 0 GG cell-weighted (reference), 1 GG face
+                                average, 2 weighted least squares (new)        */
+    int    ieigenfix;
+    int    timestepModel;    /* 0 local, 1 global, 2 local->min                */
+    int    ncfl;
+    int    visSRModel;       /* 1,2,3                                          */
+    int    visTimeStepModel;
+    int    vismodel;         /* 0 Euler, 1 laminar, 3 SA                       */
+    int    ivischeme;        /* 0 std (face average + correction)              */
+    int    isowallbc;        /* 0 adiabatic, 1 isothermal                      */
+    int    iprod_sa;         /* SA production form                             */
+    int    ft2_flag;
+    int    turb_ilim;        /* only -1 (first order SA convection) supported  */
+    int    precision;        /* OFG_PREC_*                                     */
+    int    venkat_kh3;       /* 0: eps = vencat_coef*max(qmax-qmin,1) (reference);
+                                1: eps^2 = (K h)^3 with K = vencat_coef (new)  */
+    int    reserved_i[7];
+    double vencat_coef;
+    double centropy1, centropy2;
+    double cflst, cfled;
+    double max_time_ratio;
+    double global_dt;
+    double mach_ref, aoa_degree, sideslip_degree, reynolds;
+    double gama_ref, prl, prt, tref_dim, twall_dim;
+    double inflow_viscosity;  /* SA nu~ of the freestream                      */
+    double rprod;
+    double turb_cfl_ratio;
+    double reserved_d[8];
+} ofg_params;
+
+typedef struct ofg_ctx ofg_ctx;
+
+void        ofg_default_params(ofg_params *p);
+int         ofg_create(const ofg_params *p, ofg_ctx **out);
+void        ofg_destroy(ofg_ctx *ctx);
+const char *ofg_last_error(const ofg_ctx *ctx);
+int         ofg_version(void);
+
+/*
+ * Mesh upload: the content of one .ofl zone (codes/geometry/src/UnsGrid.cpp:90-201).
+ * lCells may be negative for a boundary face, in which case the face is
+ * reversed (UnsGrid::ReadGridFaceTopology, :157-175).  Boundary faces are
+ * [0, nBFaces).  Metrics (UnsGrid::CalcMetrics, :469-900) are computed here.
+ * wall_dist (may be NULL for non-SA runs) is per interior cell.
+ */
+int ofg_upload_mesh(ofg_ctx *ctx, int nNodes, const double *xN, const double *yN, const double *zN,
+                    int nFaces, const int *faceNodeCount, const int *faceNodes,
+                    const int *lCells, const int *rCells, int nCells, int nBFaces,
+                    const int *bcType, const double *wall_dist);
+
+/* INIT_FLOWFIELD with startStrategy 0: freestream + CALC_BOUNDARY
+   (codes/uns/src/UNsRestart.cpp:48-60, codes/ns/src/NsSolverImp.cpp:61-73). */
+int ofg_init_flowfield(ofg_ctx *ctx);
+
+/* state transfer, reference layout [nEqu][nCells+nBFaces] (primitive q for
+   NS: rho,u,v,w,p; nu~ for SA).  Upload runs CALC_BOUNDARY for that solver. */
+int ofg_upload_state(ofg_ctx *ctx, int tid, const double *q);
+int ofg_download_state(ofg_ctx *ctx, int tid, double *q);
+
+/* One task each (system/ns/function/funcMap.txt, codes/turb/src/TurbSolverImp.cpp:33-42). */
+int ofg_zero_dq(ofg_ctx *ctx, int tid);             /* ZERO_DQ_FIELD          */
+int ofg_calc_time_step(ofg_ctx *ctx, int tid);      /* CALC_TIME_STEP         */
+int ofg_load_residuals(ofg_ctx *ctx, int tid);      /* LOAD_RESIDUALS         */
+int ofg_update_residuals(ofg_ctx *ctx, int tid);    /* UPDATE_RESIDUALS       */
+int ofg_init_lusgs(ofg_ctx *ctx, int tid);          /* INIT_LUSGS (no-op)     */
+int ofg_lusgs_lower(ofg_ctx *ctx, int tid);         /* LUSGS_LOWER_SWEEP      */
+int ofg_lusgs_upper(ofg_ctx *ctx, int tid);         /* LUSGS_UPPER_SWEEP      */
+int ofg_update_flowfield(ofg_ctx *ctx, int tid);    /* UPDATE_FLOWFIELD_LUSGS */
+int ofg_calc_boundary(ofg_ctx *ctx, int tid);       /* CALC_BOUNDARY          */
+
+/* The whole TimeIntegral::Lusgs sequence for every solver, nsteps outer
+   iterations (MG::Run with StrongIter, codes/multigrid/src/Multigrid.cpp:111-169,
+   :349-360), with the RMS residual of every iteration appended to the history. */
+int ofg_step(ofg_ctx *ctx, int nsteps);
+
+/* RMS residual per equation of the last UPDATE_RESIDUALS
+   (ResidualTask::CalcRes + ResAver::CalcAver,
+   codes/residual/src/ResidualTask.cpp:75-126, codes/residual/src/Residual.cpp:52-72). */
+int ofg_residual_norms(ofg_ctx *ctx, int tid, double *rms);
+
+/* Named device field -> host, reference layout:
+   "res","dq","timestep","invsr","vissr","impsr","limiter","dqdx","dqdy","dqdz",
+   "tempr","visl","vist","vol","xcc","ycc","zcc","area","xfn","yfn","zfn".
+   n_out = capacity in doubles; the size needed is returned in *n_needed. */
+int ofg_download_field(ofg_ctx *ctx, int tid, const char *name, double *out, int64_t n_out,
+                       int64_t *n_needed);
+
+/* Iteration::outerSteps for the task-level API (the CFL ramp of the next
+   CALC_TIME_STEP reads it); ofg_step advances it itself. */
+int ofg_set_outer_step(ofg_ctx *ctx, int64_t outer_steps);
+
+/* Outer-iteration counter (Iteration::outerSteps) and a counter of every
+   CUDA kernel launch this context issued (for reporting). */
+int ofg_get_counters(ofg_ctx *ctx, int64_t *outer_steps, int64_t *kernel_launches);
+
+/* Cell renumbering for the GPU sweeps: a greedy colouring of the cell graph
+   followed by a locality order inside each colour.  Writes perm[newId] = oldId
+   for interior cells and returns the number of colours (>= 1).  Pure host
+   function; apply it to the mesh arrays before ofg_upload_mesh. */
+int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells,
+                     int *perm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,722 @@
+// C ABI (include/oneflow_b200.h): context lifecycle, mesh preprocessing
+// (metrics, CSR cell->face lists, LU-SGS level schedules), state transfer,
+// one entry point per reference task, and the graph-captured outer iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ofg_ctx.h"
+
+using namespace ofg;
+
+namespace {
+
+const double SMALL = 1.0e-40;
+const double PI = 3.141592653589793;
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return c->fail(e_ == cudaErrorMemoryAllocation ? OFG_E_NOMEM : OFG_E_CUDA,     \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));            \
+    } while (0)
+
+int launch(ofg_ctx *c, int task) {
+    int rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, task, c->stream) : launch_task_f64(c, task, c->stream);
+    if (rc) return rc;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return c->fail(OFG_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return OFG_OK;
+}
+
+int sync(ofg_ctx *c) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->fail(OFG_E_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+    return OFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Metrics: UnsGrid::CalcMetrics (codes/geometry/src/UnsGrid.cpp:469-900) with
+// FaceMesh::CalcFaceNormal2D/3D and CalcFaceCenter2D/3D
+// (codes/geometry/src/FaceMesh.cpp:112-286).
+// ---------------------------------------------------------------------------
+void compute_metrics(ofg_ctx *c, int dim, const std::vector<double> &xN, const std::vector<double> &yN,
+                     const std::vector<double> &zN, const std::vector<int> &fOff, const std::vector<int> &fNod) {
+    int nF = c->nFaces, nC = c->nCells, nB = c->nBFaces, nT = c->nT;
+    c->xfn.assign(nF, 0); c->yfn.assign(nF, 0); c->zfn.assign(nF, 0); c->area.assign(nF, 0);
+    c->xfc.assign(nF, 0); c->yfc.assign(nF, 0); c->zfc.assign(nF, 0);
+    c->xcc.assign(nT, 0); c->ycc.assign(nT, 0); c->zcc.assign(nT, 0); c->vol.assign(nT, 0);
+    auto &xfn = c->xfn, &yfn = c->yfn, &zfn = c->zfn, &area = c->area, &xfc = c->xfc, &yfc = c->yfc, &zfc = c->zfc;
+    auto &xcc = c->xcc, &ycc = c->ycc, &zcc = c->zcc, &vol = c->vol;
+    const auto &lc = c->lc, &rc = c->rc;
+    if (dim == 2) {
+        for (int f = 0; f < nF; ++f) {
+            int p1 = fNod[fOff[f]], p2 = fNod[fOff[f] + 1];
+            xfn[f] = yN[p2] - yN[p1];
+            yfn[f] = xN[p1] - xN[p2];
+            zfn[f] = 0.0;
+            area[f] = std::sqrt(xfn[f] * xfn[f] + yfn[f] * yfn[f] + zfn[f] * zfn[f]);
+        }
+        for (int f = 0; f < nF; ++f) {
+            double oa = 1.0 / (area[f] + SMALL);
+            xfn[f] *= oa; yfn[f] *= oa; zfn[f] *= oa;
+        }
+        for (int f = 0; f < nF; ++f) {
+            int p1 = fNod[fOff[f]], p2 = fNod[fOff[f] + 1];
+            xfc[f] = 0.5 * (xN[p1] + xN[p2]);
+            yfc[f] = 0.5 * (yN[p1] + yN[p2]);
+            zfc[f] = 0.5 * (zN[p1] + zN[p2]);
+        }
+        for (int f = 0; f < nF; ++f) {
+            int l = lc[f], r = rc[f];
+            double dot = (xfc[f] * xfn[f] + yfc[f] * yfn[f] + zfc[f] * zfn[f]) * area[f];
+            xcc[l] += xfc[f] * dot; ycc[l] += yfc[f] * dot; zcc[l] += zfc[f] * dot; vol[l] += dot;
+            if (f >= nB) { xcc[r] -= xfc[f] * dot; ycc[r] -= yfc[f] * dot; zcc[r] -= zfc[f] * dot; vol[r] -= dot; }
+        }
+        for (int i = 0; i < nC; ++i) {
+            double tmp = 1.0 / (1.5 * vol[i] + SMALL);
+            xcc[i] *= tmp; ycc[i] *= tmp; zcc[i] *= tmp;
+            vol[i] *= 0.5;
+            if (vol[i] <= 0.0) vol[i] = -vol[i];
+        }
+    } else {
+        for (int f = 0; f < nF; ++f) {
+            int n = fOff[f + 1] - fOff[f];
+            const int *fi = &fNod[fOff[f]];
+            for (int i = 0; i < n; ++i) {
+                int p1 = fi[i], p2 = fi[(i + 1) % n];
+                double dx1 = xN[p1], dy1 = yN[p1], dz1 = zN[p1], dx2 = xN[p2], dy2 = yN[p2], dz2 = zN[p2];
+                xfn[f] += 0.5 * (dy1 * dz2 - dy2 * dz1);
+                yfn[f] += 0.5 * (dz1 * dx2 - dz2 * dx1);
+                zfn[f] += 0.5 * (dx1 * dy2 - dx2 * dy1);
+            }
+            area[f] = std::sqrt(xfn[f] * xfn[f] + yfn[f] * yfn[f] + zfn[f] * zfn[f]);
+        }
+        for (int f = 0; f < nF; ++f) {
+            double oa = 1.0 / (area[f] + SMALL);
+            xfn[f] *= oa; yfn[f] *= oa; zfn[f] *= oa;
+        }
+        const double third = 1.0 / 3.0;
+        for (int f = 0; f < nF; ++f) {
+            int n = fOff[f + 1] - fOff[f];
+            const int *fi = &fNod[fOff[f]];
+            double x0 = 0, y0 = 0, z0 = 0;
+            for (int i = 0; i < n; ++i) { x0 += xN[fi[i]]; y0 += yN[fi[i]]; z0 += zN[fi[i]]; }
+            double factor = 1.0 / n;
+            x0 *= factor; y0 *= factor; z0 *= factor;
+            double sx = 0, sy = 0, sz = 0, sarea = 0;
+            for (int i = 0; i < n; ++i) {
+                int p1 = fi[i], p2 = fi[(i + 1) % n];
+                double dx1 = xN[p1] - x0, dy1 = yN[p1] - y0, dz1 = zN[p1] - z0;
+                double dx2 = xN[p2] - x0, dy2 = yN[p2] - y0, dz2 = zN[p2] - z0;
+                double x00 = third * (xN[p1] + xN[p2] + x0);
+                double y00 = third * (yN[p1] + yN[p2] + y0);
+                double z00 = third * (zN[p1] + zN[p2] + z0);
+                double anx = dy1 * dz2 - dy2 * dz1, any = dz1 * dx2 - dz2 * dx1, anz = dx1 * dy2 - dx2 * dy1;
+                double fa = 0.5 * std::sqrt(anx * anx + any * any + anz * anz);
+                if (anx * xfn[f] + any * yfn[f] + anz * zfn[f] < 0.0) fa = -fa;
+                sarea += fa;
+                sx += fa * x00; sy += fa * y00; sz += fa * z00;
+            }
+            double os = 1.0 / (sarea + SMALL);
+            xfc[f] = sx * os; yfc[f] = sy * os; zfc[f] = sz * os;
+        }
+        for (int f = 0; f < nF; ++f) {
+            int l = lc[f], r = rc[f];
+            int n = fOff[f + 1] - fOff[f];
+            const int *fi = &fNod[fOff[f]];
+            for (int i = 0; i < n; ++i) {
+                int p2 = fi[i], p3 = fi[(i + 1) % n];
+                double x21 = xN[p2] - xfc[f], y21 = yN[p2] - yfc[f], z21 = zN[p2] - zfc[f];
+                double x31 = xN[p3] - xfc[f], y31 = yN[p3] - yfc[f], z31 = zN[p3] - zfc[f];
+                double nx = y21 * z31 - y31 * z21, ny = z21 * x31 - z31 * x21, nz = x21 * y31 - x31 * y21;
+                double trix = xfc[f] + xN[p2] + xN[p3];
+                double triy = yfc[f] + yN[p2] + yN[p3];
+                double triz = zfc[f] + zN[p2] + zN[p3];
+                double tmp = nx * trix + ny * triy + nz * triz;
+                trix *= tmp; triy *= tmp; triz *= tmp;
+                xcc[l] += trix; ycc[l] += triy; zcc[l] += triz; vol[l] += tmp;
+                xcc[r] -= trix; ycc[r] -= triy; zcc[r] -= triz; vol[r] -= tmp;
+            }
+        }
+        for (int i = 0; i < nC; ++i) {
+            double tmp = 1.0 / (4.0 * vol[i] + SMALL);
+            xcc[i] *= tmp; ycc[i] *= tmp; zcc[i] *= tmp;
+            vol[i] /= 18.0;
+            if (vol[i] <= 0.0) vol[i] = -vol[i];
+        }
+    }
+    for (int f = 0; f < nB; ++f) {
+        int l = lc[f], r = f + nC;
+        if (area[f] > SMALL) {
+            double tmp = 2.0 * ((xcc[l] - xfc[f]) * xfn[f] + (ycc[l] - yfc[f]) * yfn[f] + (zcc[l] - zfc[f]) * zfn[f]);
+            xcc[r] = xcc[l] - xfn[f] * tmp; ycc[r] = ycc[l] - yfn[f] * tmp; zcc[r] = zcc[l] - zfn[f] * tmp;
+        } else {
+            xcc[r] = -xcc[l] + 2.0 * xfc[f]; ycc[r] = -ycc[l] + 2.0 * yfc[f]; zcc[r] = -zcc[l] + 2.0 * zfc[f];
+        }
+        vol[r] = vol[l];
+    }
+}
+
+// Level schedule of a sequential sweep: a cell's level is one more than the
+// deepest level among the neighbours it reads (lower: smaller id; upper:
+// larger id).  Cells inside a level keep ascending / descending id order.
+void build_levels(ofg_ctx *c, bool lower, std::vector<int> &order, std::vector<int> &off) {
+    int N = c->nCells;
+    std::vector<int> lev(N, 0);
+    int maxl = 0;
+    auto visit = [&](int i) {
+        int L = 0;
+        for (int k = c->c2f_off[i]; k < c->c2f_off[i + 1]; ++k) {
+            int f = c->c2f[k];
+            if (f < c->nBFaces) continue;
+            int nb = c->lc[f] == i ? c->rc[f] : c->lc[f];
+            if (lower ? nb < i : nb > i) L = std::max(L, lev[nb] + 1);
+        }
+        lev[i] = L;
+        maxl = std::max(maxl, L);
+    };
+    if (lower) for (int i = 0; i < N; ++i) visit(i);
+    else for (int i = N - 1; i >= 0; --i) visit(i);
+    off.assign(maxl + 2, 0);
+    for (int i = 0; i < N; ++i) off[lev[i] + 1]++;
+    for (int l = 0; l <= maxl; ++l) off[l + 1] += off[l];
+    order.assign(N, 0);
+    std::vector<int> pos(off.begin(), off.end() - 1);
+    if (lower) for (int i = 0; i < N; ++i) order[pos[lev[i]]++] = i;
+    else for (int i = N - 1; i >= 0; --i) order[pos[lev[i]]++] = i;
+}
+
+template <typename T>
+int upload(ofg_ctx *c, T **d, const T *h, size_t n) {
+    if (*d) { cudaFree(*d); *d = nullptr; }
+    if (n == 0) n = 1;
+    CK(cudaMalloc((void **)d, n * sizeof(T)));
+    if (h) CK(cudaMemcpy(*d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    return OFG_OK;
+}
+
+void derive_params(ofg_ctx *c) {
+    const ofg_params &p = c->p;
+    DevParams &d = c->dp;
+    d.ischeme = p.ischeme; d.ilim = p.ilim; d.vismodel = p.vismodel; d.visSRModel = p.visSRModel;
+    d.visTimeStepModel = p.visTimeStepModel; d.ieigenfix = p.ieigenfix; d.timestepModel = p.timestepModel;
+    d.isowallbc = p.isowallbc; d.dim = p.dimension; d.precision = p.precision; d.venkat_kh3 = p.venkat_kh3;
+    d.igrad = p.igrad;
+    d.gama = p.gama_ref; d.centropy1 = p.centropy1; d.centropy2 = p.centropy2; d.vencat_coef = p.vencat_coef;
+    d.reynolds = p.reynolds; d.oreynolds = 1.0 / p.reynolds; d.oprl = 1.0 / p.prl; d.oprt = 1.0 / p.prt;
+    d.const_cp = 1.0 / ((p.gama_ref - 1.0) * (p.mach_ref * p.mach_ref));
+    d.statecoef = 1.0 / (p.gama_ref * (p.mach_ref * p.mach_ref));   // Chemical::CalcStateCoefNs
+    double aoa = p.aoa_degree * PI / 180.0, aos = p.sideslip_degree * PI / 180.0;
+    d.inflow[IR] = 1.0;
+    d.inflow[IU] = 1.0 * std::cos(aoa) * std::cos(aos);
+    d.inflow[IV] = 1.0 * std::sin(aoa) * std::cos(aos);
+    d.inflow[IW] = 1.0 * std::sin(aos);
+    d.inflow[IP] = d.statecoef * 1.0 * 1.0 / 1.0;
+    d.twall = p.twall_dim / p.tref_dim;
+    d.sutherland_ts = 110.4 / p.tref_dim;
+    d.max_time_ratio = p.max_time_ratio;
+    d.global_dt = p.global_dt;
+    d.nut_inf = p.inflow_viscosity;
+}
+
+double host_sutherland(const DevParams &P, double t) {
+    double t3 = t * t * t;
+    return std::sqrt(t3) * (1 + P.sutherland_ts) / (t + P.sutherland_ts);
+}
+
+int check_tid(ofg_ctx *c, int tid) {
+    if (!c) return OFG_E_ARG;
+    if (tid != OFG_NS_SOLVER) return c->fail(OFG_E_ARG, "only the NS solver (tid 0) is available in this build");
+    if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
+    if (!c->haveState) return c->fail(OFG_E_STATE, "no flow field: call ofg_init_flowfield or ofg_upload_state");
+    return OFG_OK;
+}
+
+void destroy_graphs(ofg_ctx *c) {
+    for (int i = 0; i < 2; ++i)
+        if (c->graph[i]) { cudaGraphExecDestroy(c->graph[i]); c->graph[i] = nullptr; }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ofg_version(void) { return 1; }
+
+void ofg_default_params(ofg_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->dimension = 2; p->ischeme = 1; p->ilim = 0; p->igrad = 0; p->ieigenfix = 1; p->timestepModel = 0;
+    p->ncfl = 100; p->visSRModel = 2; p->visTimeStepModel = 1; p->vismodel = 1; p->ivischeme = 0;
+    p->isowallbc = 0; p->iprod_sa = 2; p->ft2_flag = 0; p->turb_ilim = -1; p->precision = OFG_PREC_FP64;
+    p->vencat_coef = 1.0e-4; p->centropy1 = 1.0e-4; p->centropy2 = 1.0e-4; p->cflst = 0.1; p->cfled = 10.0;
+    p->max_time_ratio = 1.0e10; p->global_dt = 1.0e-3; p->mach_ref = 0.2; p->reynolds = 1.0e6;
+    p->gama_ref = 1.4; p->prl = 0.72; p->prt = 0.9; p->tref_dim = 300.0; p->twall_dim = 300.0;
+    p->inflow_viscosity = 0.01; p->rprod = 1.0; p->turb_cfl_ratio = 1.0;
+}
+
+int ofg_create(const ofg_params *p, ofg_ctx **out) {
+    if (!p || !out) return OFG_E_ARG;
+    *out = nullptr;
+    if (p->dimension != 2 && p->dimension != 3) return OFG_E_ARG;
+    if (p->ischeme != 1 && p->ischeme != 12) return OFG_E_ARG;
+    if (p->ilim < -1 || p->ilim > 2) return OFG_E_ARG;
+    if (p->igrad < 0 || p->igrad > 2) return OFG_E_ARG;
+    if (p->precision != OFG_PREC_FP64 && p->precision != OFG_PREC_MIXED) return OFG_E_ARG;
+    if (p->vismodel != 0 && p->vismodel != 1) return OFG_E_ARG;   // SA: separate solver, tid 1
+    if (p->ivischeme != 0) return OFG_E_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return OFG_E_CUDA;
+    ofg_ctx *c = new ofg_ctx();
+    c->p = *p;
+    derive_params(c);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return OFG_E_CUDA; }
+    *out = c;
+    return OFG_OK;
+}
+
+void ofg_destroy(ofg_ctx *c) {
+    if (!c) return;
+    cudaStreamSynchronize(c->stream);
+    destroy_graphs(c);
+    void *ptrs[] = {c->d_lc, c->d_rc, c->d_bct, c->d_c2f_off, c->d_c2f, c->d_lowOrder, c->d_upOrder, c->d_wdist,
+                    c->d_q[0], c->d_q[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_bcq,
+                    c->d_partial, c->d_scal, c->d_hist, c->d_grad, c->d_lim, c->d_mm, c->d_fix};
+    for (void *v : ptrs) if (v) cudaFree(v);
+    for (int i = 0; i < 11; ++i) { if (c->d_g64[i]) cudaFree(c->d_g64[i]); if (c->d_g32[i]) cudaFree(c->d_g32[i]); }
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *ofg_last_error(const ofg_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, const double *zN, int nFaces,
+                    const int *faceNodeCount, const int *faceNodes, const int *lCells, const int *rCells, int nCells,
+                    int nBFaces, const int *bcType, const double *wall_dist) {
+    if (!c) return OFG_E_ARG;
+    if (nNodes <= 0 || nFaces <= 0 || nCells <= 0 || nBFaces < 0 || nBFaces > nFaces)
+        return c->fail(OFG_E_ARG, "bad mesh sizes");
+    if (!xN || !yN || !zN || !faceNodeCount || !faceNodes || !lCells || !rCells || (nBFaces && !bcType))
+        return c->fail(OFG_E_ARG, "null mesh array");
+    destroy_graphs(c);
+    c->nCells = nCells; c->nBFaces = nBFaces; c->nFaces = nFaces; c->nT = nCells + nBFaces;
+    std::vector<double> X(xN, xN + nNodes), Y(yN, yN + nNodes), Z(zN, zN + nNodes);
+    std::vector<int> fOff(nFaces + 1, 0);
+    for (int f = 0; f < nFaces; ++f) {
+        int n = faceNodeCount[f];
+        if (n < 2 || (c->p.dimension == 3 && n < 3)) return c->fail(OFG_E_ARG, "face with too few nodes");
+        fOff[f + 1] = fOff[f] + n;
+    }
+    std::vector<int> fNod(faceNodes, faceNodes + fOff[nFaces]);
+    for (int v : fNod) if (v < 0 || v >= nNodes) return c->fail(OFG_E_ARG, "face node index out of range");
+    c->lc.assign(lCells, lCells + nFaces);
+    c->rc.assign(rCells, rCells + nFaces);
+    // UnsGrid::ReadGridFaceTopology: a negative left cell means the face is reversed
+    for (int f = 0; f < nFaces; ++f)
+        if (c->lc[f] < 0) {
+            std::reverse(fNod.begin() + fOff[f], fNod.begin() + fOff[f + 1]);
+            std::swap(c->lc[f], c->rc[f]);
+        }
+    for (int f = 0; f < nBFaces; ++f) c->rc[f] = f + nCells;   // UnsGrid::NormalizeBc
+    for (int f = 0; f < nFaces; ++f) {
+        if (c->lc[f] < 0 || c->lc[f] >= nCells) return c->fail(OFG_E_ARG, "left cell out of range");
+        if (f >= nBFaces && (c->rc[f] < 0 || c->rc[f] >= nCells || c->rc[f] == c->lc[f]))
+            return c->fail(OFG_E_ARG, "interior face with a bad right cell");
+    }
+    c->bct.assign(bcType, bcType + nBFaces);
+    for (int t : c->bct)
+        if (t < 1 || t > 7) return c->fail(OFG_E_ARG, "unsupported boundary type (interface/overset are multi-zone)");
+    compute_metrics(c, c->p.dimension, X, Y, Z, fOff, fNod);
+    for (int i = 0; i < nCells; ++i)
+        if (!(c->vol[i] > 0.0)) return c->fail(OFG_E_ARG, "degenerate cell volume");
+    // CSR cell->face in ascending face id (CellTopo::CalcC2f)
+    c->c2f_off.assign(nCells + 1, 0);
+    for (int f = 0; f < nFaces; ++f) {
+        c->c2f_off[c->lc[f] + 1]++;
+        if (f >= nBFaces) c->c2f_off[c->rc[f] + 1]++;
+    }
+    for (int i = 0; i < nCells; ++i) c->c2f_off[i + 1] += c->c2f_off[i];
+    c->c2f.assign(c->c2f_off[nCells], 0);
+    std::vector<int> pos(c->c2f_off.begin(), c->c2f_off.end() - 1);
+    for (int f = 0; f < nFaces; ++f) {
+        c->c2f[pos[c->lc[f]]++] = f;
+        if (f >= nBFaces) c->c2f[pos[c->rc[f]]++] = f;
+    }
+    build_levels(c, true, c->lowOrder, c->lowOff);
+    build_levels(c, false, c->upOrder, c->upOff);
+    c->wdist.assign(nCells, 0.0);
+    if (wall_dist) std::copy(wall_dist, wall_dist + nCells, c->wdist.begin());
+
+    // ---- device copies ----
+    int rc;
+    if ((rc = upload(c, &c->d_lc, c->lc.data(), nFaces))) return rc;
+    if ((rc = upload(c, &c->d_rc, c->rc.data(), nFaces))) return rc;
+    if ((rc = upload(c, &c->d_bct, c->bct.data(), nBFaces))) return rc;
+    if ((rc = upload(c, &c->d_c2f_off, c->c2f_off.data(), nCells + 1))) return rc;
+    if ((rc = upload(c, &c->d_c2f, c->c2f.data(), c->c2f.size()))) return rc;
+    if ((rc = upload(c, &c->d_lowOrder, c->lowOrder.data(), nCells))) return rc;
+    if ((rc = upload(c, &c->d_upOrder, c->upOrder.data(), nCells))) return rc;
+    if ((rc = upload(c, &c->d_wdist, c->wdist.data(), nCells))) return rc;
+    const std::vector<double> *geo[11] = {&c->xfn, &c->yfn, &c->zfn, &c->area, &c->xfc, &c->yfc, &c->zfc,
+                                          &c->xcc, &c->ycc, &c->zcc, &c->vol};
+    for (int i = 0; i < 11; ++i) {
+        if (c->p.precision == OFG_PREC_MIXED) {
+            std::vector<float> f(geo[i]->begin(), geo[i]->end());
+            if ((rc = upload(c, &c->d_g32[i], f.data(), f.size()))) return rc;
+        } else {
+            if ((rc = upload(c, &c->d_g64[i], geo[i]->data(), geo[i]->size()))) return rc;
+        }
+    }
+    size_t nT = c->nT, N = nCells;
+    if ((rc = upload<double>(c, &c->d_q[0], nullptr, nT * REC))) return rc;
+    if ((rc = upload<double>(c, &c->d_q[1], nullptr, nT * REC))) return rc;
+    if ((rc = upload<double>(c, &c->d_res, nullptr, N * NEQ))) return rc;
+    if ((rc = upload<double>(c, &c->d_dq, nullptr, nT * NEQ))) return rc;
+    if ((rc = upload<double>(c, &c->d_dt, nullptr, N))) return rc;
+    if ((rc = upload<double>(c, &c->d_invsr, nullptr, N))) return rc;
+    if ((rc = upload<double>(c, &c->d_vissr, nullptr, N))) return rc;
+    if ((rc = upload<double>(c, &c->d_bcq, nullptr, (size_t)std::max(nBFaces, 1) * NEQ))) return rc;
+    c->nPartialMax = std::max<size_t>((N + 255) / 256 * 10, 2 * 148 * NEQ) + 16;
+    if ((rc = upload<double>(c, &c->d_partial, nullptr, c->nPartialMax))) return rc;
+    if ((rc = upload<double>(c, &c->d_scal, nullptr, 32))) return rc;
+    c->histCap = 1 << 16;
+    if ((rc = upload<double>(c, &c->d_hist, nullptr, (size_t)c->histCap * NEQ))) return rc;
+    if ((rc = upload<int>(c, &c->d_fix, nullptr, 1 + c->fixcap))) return rc;
+    size_t rs = c->p.precision == OFG_PREC_MIXED ? sizeof(float) : sizeof(double);
+    if (c->d_grad) cudaFree(c->d_grad);
+    if (c->d_lim) cudaFree(c->d_lim);
+    if (c->d_mm) cudaFree(c->d_mm);
+    CK(cudaMalloc(&c->d_grad, N * 18 * rs));
+    CK(cudaMalloc(&c->d_lim, N * NEQ * rs));
+    CK(cudaMalloc(&c->d_mm, N * 10 * rs));
+    CK(cudaMemset(c->d_grad, 0, N * 18 * rs));
+    CK(cudaMemset(c->d_dq, 0, nT * NEQ * sizeof(double)));
+    CK(cudaMemset(c->d_bcq, 0, (size_t)std::max(nBFaces, 1) * NEQ * sizeof(double)));
+    CK(cudaMemset(c->d_scal, 0, 32 * sizeof(double)));
+    CK(cudaMemset(c->d_fix, 0, (1 + c->fixcap) * sizeof(int)));
+    if (c->p.ilim == 0) {
+        // Limiter::CalcNoLimiter: phi = 1 on every cell, every step
+        if (rs == sizeof(float)) { std::vector<float> one(N * NEQ, 1.0f); CK(cudaMemcpy(c->d_lim, one.data(), N * NEQ * rs, cudaMemcpyHostToDevice)); }
+        else { std::vector<double> one(N * NEQ, 1.0); CK(cudaMemcpy(c->d_lim, one.data(), N * NEQ * rs, cudaMemcpyHostToDevice)); }
+    }
+    c->haveMesh = true;
+    c->haveState = false;
+    c->outerSteps = 0;
+    c->hist.clear();
+    return OFG_OK;
+}
+
+int ofg_init_flowfield(ofg_ctx *c) {
+    if (!c) return OFG_E_ARG;
+    if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
+    destroy_graphs(c);
+    // UNsRestart::InitRestart: q = inflow everywhere (ghosts included)
+    std::vector<double> rec((size_t)c->nT * REC, 0.0);
+    const DevParams &P = c->dp;
+    double t = P.inflow[IP] / (P.statecoef * P.inflow[IR] * 1.0);
+    double ml = std::max(0.0, host_sutherland(P, t));
+    for (int i = 0; i < c->nT; ++i) {
+        double *o = &rec[(size_t)i * REC];
+        for (int e = 0; e < NEQ; ++e) o[e] = P.inflow[e];
+        o[ITT] = t; o[IML] = ml; o[IMT] = 0.0;
+    }
+    c->cur = 0;
+    CK(cudaMemcpy(c->d_q[0], rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_q[1], rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->d_scal, 0, 32 * sizeof(double)));
+    c->outerSteps = 0;
+    c->hist.clear();
+    c->haveState = true;
+    c->pendingNext = false;
+    int rc = launch(c, T_BOUNDARY_CUR);   // NsInitFinal -> NsCalcBoundary
+    if (rc) return rc;
+    return sync(c);
+}
+
+int ofg_upload_state(ofg_ctx *c, int tid, const double *q) {
+    if (!c || !q) return OFG_E_ARG;
+    if (tid != OFG_NS_SOLVER) return c->fail(OFG_E_ARG, "only the NS solver (tid 0) is available in this build");
+    if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
+    destroy_graphs(c);
+    std::vector<double> rec((size_t)c->nT * REC, 0.0);
+    for (int i = 0; i < c->nT; ++i)
+        for (int e = 0; e < NEQ; ++e) rec[(size_t)i * REC + e] = q[(size_t)e * c->nT + i];
+    c->cur = 0;
+    CK(cudaMemcpy(c->d_q[0], rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_q[1], rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->haveState = true;
+    c->pendingNext = false;
+    int rc = launch(c, T_BOUNDARY_CUR);
+    if (rc) return rc;
+    return sync(c);
+}
+
+int ofg_download_state(ofg_ctx *c, int tid, double *q) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if (!q) return c->fail(OFG_E_ARG, "null output");
+    if ((rc = sync(c))) return rc;
+    std::vector<double> rec((size_t)c->nT * REC);
+    CK(cudaMemcpy(rec.data(), c->d_q[c->cur], rec.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < c->nT; ++i)
+        for (int e = 0; e < NEQ; ++e) q[(size_t)e * c->nT + i] = rec[(size_t)i * REC + e];
+    return OFG_OK;
+}
+
+int ofg_zero_dq(ofg_ctx *c, int tid) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(c->d_dq, 0, (size_t)c->nT * NEQ * sizeof(double), c->stream));
+    return OFG_OK;
+}
+
+int ofg_calc_time_step(ofg_ctx *c, int tid) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if ((rc = launch(c, T_CFL))) return rc;
+    return launch(c, T_TIMESTEP);
+}
+
+int ofg_load_residuals(ofg_ctx *c, int tid) {
+    // res = -rhs with rhs = 0 on a single grid: folded into UPDATE_RESIDUALS,
+    // which starts every cell's accumulation from -0.0
+    return check_tid(c, tid);
+}
+
+int ofg_update_residuals(ofg_ctx *c, int tid) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    return launch(c, T_RESIDUAL);
+}
+
+int ofg_init_lusgs(ofg_ctx *c, int tid) { return check_tid(c, tid); }
+
+int ofg_lusgs_lower(ofg_ctx *c, int tid) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    return launch(c, T_LOWER);
+}
+
+int ofg_lusgs_upper(ofg_ctx *c, int tid) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    return launch(c, T_UPPER);
+}
+
+int ofg_update_flowfield(ofg_ctx *c, int tid) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if ((rc = launch(c, T_UPDATE))) return rc;
+    c->pendingNext = true;
+    return OFG_OK;
+}
+
+int ofg_calc_boundary(ofg_ctx *c, int tid) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if (c->pendingNext) {
+        if ((rc = launch(c, T_BOUNDARY_NEXT))) return rc;
+        c->cur ^= 1;
+        c->pendingNext = false;
+        return OFG_OK;
+    }
+    return launch(c, T_BOUNDARY_CUR);
+}
+
+int ofg_step(ofg_ctx *c, int nsteps) {
+    int rc = check_tid(c, OFG_NS_SOLVER);
+    if (rc) return rc;
+    if (nsteps < 0) return c->fail(OFG_E_ARG, "negative step count");
+    if (c->pendingNext) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
+    if (c->outerSteps + nsteps > c->histCap) return c->fail(OFG_E_ARG, "residual history capacity exceeded");
+    // the device step counter and history index follow the host counters
+    double sc[2] = {double(c->outerSteps), double(c->outerSteps)};
+    CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if ((rc = sync(c))) return rc;
+    if (!c->graph[0]) {
+        // capture one outer iteration per state-buffer parity:
+        // MG::Run -> TimeIntegral::Lusgs (ZERO_DQ_FIELD is not needed: no kernel
+        // reads a dq value it did not write in the same iteration)
+        int saveCur = c->cur;
+        for (int g = 0; g < 2; ++g) {
+            c->cur = g;
+            long long before = c->launches;
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            int tasks[] = {T_ADVANCE, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
+            for (int t : tasks) {
+                rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
+                if (rc) { cudaStreamEndCapture(c->stream, &graph); return rc; }
+            }
+            CK(cudaStreamEndCapture(c->stream, &graph));
+            CK(cudaGraphInstantiate(&c->graph[g], graph, 0));
+            cudaGraphDestroy(graph);
+            c->graphKernels[g] = c->launches - before;
+            c->launches = before;
+        }
+        c->cur = saveCur;
+    }
+    for (int it = 0; it < nsteps; ++it) {
+        CK(cudaGraphLaunch(c->graph[c->cur], c->stream));
+        c->launches += c->graphKernels[c->cur];
+        c->cur ^= 1;
+        c->outerSteps++;
+    }
+    if ((rc = sync(c))) return rc;
+    // pull the new history rows
+    size_t have = c->hist.size() / NEQ;
+    size_t want = (size_t)c->outerSteps;
+    if (want > have) {
+        std::vector<double> tmp((want - have) * NEQ);
+        CK(cudaMemcpy(tmp.data(), c->d_hist + have * NEQ, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        c->hist.insert(c->hist.end(), tmp.begin(), tmp.end());
+        for (double v : tmp)
+            if (std::isnan(v)) return c->fail(OFG_E_NAN, "NotANumber in the residual");
+    }
+    return OFG_OK;
+}
+
+int ofg_residual_norms(ofg_ctx *c, int tid, double *rms) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if (!rms) return c->fail(OFG_E_ARG, "null output");
+    // norms of the current residual field (recomputed, so per-task callers get them too)
+    if ((rc = launch(c, T_NORM))) return rc;
+    if ((rc = sync(c))) return rc;
+    CK(cudaMemcpy(rms, c->d_scal + S_NORM, NEQ * sizeof(double), cudaMemcpyDeviceToHost));
+    return OFG_OK;
+}
+
+int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64_t n_out, int64_t *n_needed) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if (!name) return c->fail(OFG_E_ARG, "null name");
+    if ((rc = sync(c))) return rc;
+    std::string s(name);
+    int64_t nT = c->nT, N = c->nCells, nF = c->nFaces;
+    std::vector<double> buf;
+    auto rec_field = [&](int comp) {
+        std::vector<double> rec((size_t)nT * REC);
+        cudaMemcpy(rec.data(), c->d_q[c->cur], rec.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        buf.resize(nT);
+        for (int64_t i = 0; i < nT; ++i) buf[i] = rec[(size_t)i * REC + comp];
+    };
+    auto aos_field = [&](const double *d, int ne, int64_t nrow, int64_t ntot) {
+        std::vector<double> tmp((size_t)nrow * ne);
+        cudaMemcpy(tmp.data(), d, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        buf.assign((size_t)ne * ntot, 0.0);
+        for (int e = 0; e < ne; ++e)
+            for (int64_t i = 0; i < nrow; ++i) buf[(size_t)e * ntot + i] = tmp[(size_t)i * ne + e];
+    };
+    auto rs_field = [&](const void *d, int ne, int stride, int off) {   // R-typed [N][stride]
+        buf.assign((size_t)ne * nT, 0.0);
+        if (c->p.precision == OFG_PREC_MIXED) {
+            std::vector<float> tmp((size_t)N * stride);
+            cudaMemcpy(tmp.data(), d, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost);
+            for (int e = 0; e < ne; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * stride + e * (stride == 18 ? 3 : 1) + off];
+        } else {
+            std::vector<double> tmp((size_t)N * stride);
+            cudaMemcpy(tmp.data(), d, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost);
+            for (int e = 0; e < ne; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * stride + e * (stride == 18 ? 3 : 1) + off];
+        }
+    };
+    auto host_vec = [&](const std::vector<double> &v) { buf = v; };
+    if (s == "res") aos_field(c->d_res, NEQ, N, nT);
+    else if (s == "dq") aos_field(c->d_dq, NEQ, nT, nT);
+    else if (s == "timestep") aos_field(c->d_dt, 1, N, nT);
+    else if (s == "invsr") aos_field(c->d_invsr, 1, N, nT);
+    else if (s == "vissr") aos_field(c->d_vissr, 1, N, nT);
+    else if (s == "impsr") {
+        std::vector<double> dt(N), iv(N), vs(N);
+        cudaMemcpy(dt.data(), c->d_dt, N * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(iv.data(), c->d_invsr, N * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(vs.data(), c->d_vissr, N * 8, cudaMemcpyDeviceToHost);
+        buf.assign(nT, 0.0);
+        for (int64_t i = 0; i < N; ++i) { double v = (1.0 / dt[i]) * c->vol[i]; v += iv[i]; v += vs[i]; buf[i] = v; }
+    }
+    else if (s == "tempr") rec_field(ITT);
+    else if (s == "visl") rec_field(IML);
+    else if (s == "vist") rec_field(IMT);
+    else if (s == "limiter") rs_field(c->d_lim, NEQ, NEQ, 0);
+    else if (s == "dqdx") rs_field(c->d_grad, NEQ, 18, 0);
+    else if (s == "dqdy") rs_field(c->d_grad, NEQ, 18, 1);
+    else if (s == "dqdz") rs_field(c->d_grad, NEQ, 18, 2);
+    else if (s == "vol") host_vec(c->vol);
+    else if (s == "xcc") host_vec(c->xcc);
+    else if (s == "ycc") host_vec(c->ycc);
+    else if (s == "zcc") host_vec(c->zcc);
+    else if (s == "area") host_vec(c->area);
+    else if (s == "xfn") host_vec(c->xfn);
+    else if (s == "yfn") host_vec(c->yfn);
+    else if (s == "zfn") host_vec(c->zfn);
+    else if (s == "reshist") host_vec(c->hist);
+    else return c->fail(OFG_E_ARG, "unknown field " + s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return c->fail(OFG_E_CUDA, cudaGetErrorString(e));
+    if (n_needed) *n_needed = (int64_t)buf.size();
+    if (out) {
+        if (n_out < (int64_t)buf.size()) return c->fail(OFG_E_ARG, "output buffer too small");
+        std::copy(buf.begin(), buf.end(), out);
+    }
+    (void)nF;
+    return OFG_OK;
+}
+
+int ofg_set_outer_step(ofg_ctx *c, int64_t outer_steps) {
+    if (!c || outer_steps < 0) return OFG_E_ARG;
+    c->outerSteps = outer_steps;
+    return OFG_OK;
+}
+
+int ofg_get_counters(ofg_ctx *c, int64_t *outer_steps, int64_t *kernel_launches) {
+    if (!c) return OFG_E_ARG;
+    if (outer_steps) *outer_steps = c->outerSteps;
+    if (kernel_launches) *kernel_launches = c->launches;
+    return OFG_OK;
+}
+
+int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm) {
+    if (nCells <= 0 || nFaces < nBFaces || !lCells || !rCells || !perm) return OFG_E_ARG;
+    // adjacency (interior faces), CSR
+    std::vector<int> deg(nCells + 1, 0);
+    for (int f = nBFaces; f < nFaces; ++f) {
+        int l = lCells[f], r = rCells[f];
+        if (l < 0 || r < 0 || l >= nCells || r >= nCells) return OFG_E_ARG;
+        deg[l + 1]++; deg[r + 1]++;
+    }
+    for (int i = 0; i < nCells; ++i) deg[i + 1] += deg[i];
+    std::vector<int> adj(deg[nCells]);
+    std::vector<int> pos(deg.begin(), deg.end() - 1);
+    for (int f = nBFaces; f < nFaces; ++f) {
+        int l = lCells[f], r = rCells[f];
+        adj[pos[l]++] = r; adj[pos[r]++] = l;
+    }
+    // greedy colouring in natural order
+    std::vector<int> col(nCells, -1);
+    int ncol = 0;
+    std::vector<int> mark(64, -1);
+    for (int i = 0; i < nCells; ++i) {
+        for (int k = deg[i]; k < deg[i + 1]; ++k) {
+            int cc = col[adj[k]];
+            if (cc >= 0) { if (cc >= (int)mark.size()) mark.resize(cc + 1, -1); mark[cc] = i; }
+        }
+        int cc = 0;
+        while (cc < (int)mark.size() && mark[cc] == i) ++cc;
+        col[i] = cc;
+        ncol = std::max(ncol, cc + 1);
+    }
+    // stable order by colour: cells of one colour keep their relative order
+    std::vector<int> cnt(ncol + 1, 0);
+    for (int i = 0; i < nCells; ++i) cnt[col[i] + 1]++;
+    for (int k = 0; k < ncol; ++k) cnt[k + 1] += cnt[k];
+    for (int i = 0; i < nCells; ++i) perm[cnt[col[i]]++] = i;
+    return ncol;
+}
+
+}  // extern "C"

@@ -1,0 +1,63 @@
+// Host-side context of one solve: mesh, parameters, device buffers and the
+// captured CUDA graphs of one outer iteration.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/oneflow_b200.h"
+#include "ofg_device.cuh"
+
+struct ofg_ctx {
+    ofg_params p{};
+    ofg::DevParams dp{};
+    std::string err;
+
+    // ---- mesh (host copies, reference numbering) ----
+    int nCells = 0, nBFaces = 0, nFaces = 0, nT = 0;
+    std::vector<int> lc, rc, bct, c2f_off, c2f;
+    std::vector<double> xfn, yfn, zfn, area, xfc, yfc, zfc, xcc, ycc, zcc, vol, wdist;
+    std::vector<int> lowOrder, lowOff, upOrder, upOff;   // LU-SGS level schedules
+    bool haveMesh = false, haveState = false;
+
+    // ---- device ----
+    cudaStream_t stream = nullptr;
+    int *d_lc = nullptr, *d_rc = nullptr, *d_bct = nullptr, *d_c2f_off = nullptr, *d_c2f = nullptr;
+    int *d_lowOrder = nullptr, *d_upOrder = nullptr;
+    double *d_g64[11] = {};    // xfn yfn zfn area xfc yfc zfc | xcc ycc zcc vol
+    float *d_g32[11] = {};
+    double *d_wdist = nullptr;
+    double *d_q[2] = {nullptr, nullptr};
+    int cur = 0;
+    bool pendingNext = false;   // UPDATE_FLOWFIELD wrote d_q[cur^1], CALC_BOUNDARY not yet run
+    double *d_res = nullptr, *d_dq = nullptr, *d_dt = nullptr, *d_invsr = nullptr, *d_vissr = nullptr;
+    double *d_bcq = nullptr, *d_partial = nullptr, *d_scal = nullptr, *d_hist = nullptr;
+    void *d_grad = nullptr, *d_lim = nullptr, *d_mm = nullptr;
+    int *d_fix = nullptr;
+    int fixcap = 4096;
+    int histCap = 0;
+    size_t nPartialMax = 0;
+
+    // ---- iteration state ----
+    long long outerSteps = 0;
+    long long launches = 0;
+    std::vector<double> hist;          // host copy of residual history
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    long long graphKernels[2] = {0, 0};
+
+    int fail(int code, const std::string &msg) {
+        err = msg;
+        return code;
+    }
+};
+
+namespace ofg {
+// tasks executed by the precision-specific launchers
+enum Task {
+    T_CFL = 0, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_BOUNDARY_CUR,
+    T_NORM, T_ADVANCE
+};
+int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);
+int launch_task_f32(ofg_ctx *c, int task, cudaStream_t s);
+}  // namespace ofg

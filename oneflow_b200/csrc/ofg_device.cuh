@@ -1,0 +1,186 @@
+// Device-side data model and the per-face physics of the residual + LU-SGS
+// path, for sm_100a.  Every function restates one reference routine (cited)
+// with the same operation order as the reference's serial code, so that the
+// FP64 build (compiled without FMA contraction) rounds like the reference.
+// The arithmetic type R is double (FP64 path) or float (mixed path: face
+// terms in FP32, accumulation in FP64 by the callers).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ofg {
+
+constexpr double SMALLD = 1.0e-40;   // codes/basic/include/HXTypeBasic.h:34
+constexpr int NEQ = 5;
+constexpr int REC = 8;               // state record: rho u v w p T mul mut
+enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4, ITT = 5, IML = 6, IMT = 7 };
+
+// slots of the small device scalar array (cfl, min dt, limiter eps, norms,
+// outer-step counter, residual-history length)
+enum { S_CFL = 0, S_MINDT = 1, S_EPS = 2 /* 5 slots */, S_NORM = 8 /* 5 slots */, S_STEP = 14, S_HISTN = 15,
+       S_NSCAL = 16 };
+
+enum BcCode { BC_EXTRAP = 1, BC_SOLID = 2, BC_SYM = 3, BC_FAR = 4, BC_INFLOW = 5, BC_OUTFLOW = 6 };
+
+template <typename R> __device__ __forceinline__ R small_v();
+template <> __device__ __forceinline__ double small_v<double>() { return 1.0e-40; }
+// 1e-40 is subnormal in FP32; the guard only has to keep a zero denominator
+// away, so the FP32 path uses the smallest normal value instead.
+template <> __device__ __forceinline__ float small_v<float>() { return 1.17549435e-38f; }
+
+template <typename R> __device__ __forceinline__ R Rsqrt(R x);
+template <> __device__ __forceinline__ double Rsqrt<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float Rsqrt<float>(float x) { return sqrtf(x); }
+template <typename R> __device__ __forceinline__ R Rabs(R x) { return x < R(0) ? -x : x; }
+template <typename R> __device__ __forceinline__ R Rmax(R a, R b) { return a > b ? a : b; }
+template <typename R> __device__ __forceinline__ R Rmin(R a, R b) { return a < b ? a : b; }
+template <typename R> __device__ __forceinline__ R SQR3(R a, R b, R c) { return a * a + b * b + c * c; }
+
+// Constant parameters of one solve (reference script keys + derived state,
+// codes/chemical/src/Chemical.cpp:280-340, codes/ns/src/NsCom.cpp:45-94).
+struct DevParams {
+    int ischeme, ilim, vismodel, visSRModel, visTimeStepModel, ieigenfix, timestepModel, isowallbc;
+    int dim, precision, venkat_kh3, igrad;
+    double gama, centropy1, centropy2, vencat_coef, reynolds, oreynolds, oprl, oprt, const_cp, statecoef;
+    double inflow[NEQ];
+    double twall, sutherland_ts, max_time_ratio, global_dt;
+    // SA
+    double nut_inf;
+};
+
+// Mesh in device memory: faces SoA, cells SoA, CSR cell->face lists in
+// ascending face id (the reference's c2f order, codes/geometry/src/CellTopo.cpp:95-119).
+template <typename R>
+struct DevGeom {
+    const R *xfn, *yfn, *zfn, *area, *xfc, *yfc, *zfc;   // [nFaces]
+    const R *xcc, *ycc, *zcc, *vol;                       // [nT]
+};
+
+struct DevMesh {
+    int nCells, nBFaces, nFaces, nT;
+    const int *lc, *rc;          // [nFaces]
+    const int *c2f_off;          // [nCells+1]
+    const int *c2f;              // [E] face ids, ascending per cell
+    const int *bcType;           // [nBFaces]
+    const double *walldist;      // [nCells]
+};
+
+// Primitive -> conservative, NsInvFlux.cpp:1355-1375 (CalcInternalEnergy :1400-1412)
+template <typename R>
+__device__ __forceinline__ void primToQ(const R *pr, R gama, R *qq) {
+    R v2 = SQR3(pr[IU], pr[IV], pr[IW]);
+    R em = (pr[IP] / pr[IR]) / (gama - R(1)) + R(0.5) * v2;
+    qq[0] = pr[IR]; qq[1] = pr[IR] * pr[IU]; qq[2] = pr[IR] * pr[IV]; qq[3] = pr[IR] * pr[IW]; qq[4] = pr[IR] * em;
+}
+
+// NsInvFlux::Roe + ModifyAbsoluteEigenvalue, codes/ns/src/NsInvFlux.cpp:167-308
+template <typename R>
+__device__ __forceinline__ void roeFlux(const R *p1, const R *p2, R xn, R yn, R zn, R gam, int ieigenfix, R ce1, R ce2,
+                                        R *flux) {
+    const R half = R(0.5), one = R(1), two = R(2), vfn = R(0);
+    R rl = p1[IR], ul = p1[IU], vl = p1[IV], wl = p1[IW], pl = p1[IP];
+    R rr = p2[IR], ur = p2[IU], vr = p2[IV], wr = p2[IW], pr = p2[IP];
+    R v2l = SQR3(ul, vl, wl), v2r = SQR3(ur, vr, wr);
+    R hl = (gam / (gam - one)) * (pl / rl) + half * v2l;
+    R hr = (gam / (gam - one)) * (pr / rr) + half * v2r;
+    R vnl = xn * ul + yn * vl + zn * wl - vfn;
+    R vnr = xn * ur + yn * vr + zn * wr - vfn;
+    R rvnl = rl * vnl, rvnr = rr * vnr;
+    R ratio = Rsqrt(rr / rl);
+    R coef = one / (one + ratio);
+    R um = (ul + ur * ratio) * coef;
+    R vm = (vl + vr * ratio) * coef;
+    R wm = (wl + wr * ratio) * coef;
+    R hm = (hl + hr * ratio) * coef;
+    R gama = (gam + gam * ratio) * coef;
+    R v2 = SQR3(um, vm, wm);
+    R vnflow = xn * um + yn * vm + zn * wm;
+    R vnrel = vnflow - vfn;
+    R gamm1 = gama - one;
+    R c2 = gamm1 * (hm - half * v2);
+    R cm = Rsqrt(Rabs(c2));
+    R aeig1 = Rabs(vnrel), aeig2 = Rabs(vnrel + cm), aeig3 = Rabs(vnrel - cm);
+    flux[0] = rvnl + rvnr;
+    flux[1] = (rvnl * ul + xn * pl) + (rvnr * ur + xn * pr);
+    flux[2] = (rvnl * vl + yn * pl) + (rvnr * vr + yn * pr);
+    flux[3] = (rvnl * wl + zn * pl) + (rvnr * wr + zn * pr);
+    flux[4] = (rvnl * hl + vfn * pl) + (rvnr * hr + vfn * pr);
+    R q1[NEQ], q2[NEQ], dqv[NEQ];
+    primToQ(p1, gam, q1);
+    primToQ(p2, gam, q2);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) dqv[e] = q2[e] - q1[e];
+    R meig1 = aeig1, meig2 = aeig2, meig3 = aeig3;
+    if (ieigenfix == 1) {
+        R mx = Rmax(aeig2, aeig3);
+        R m1 = mx * ce1, m2 = mx * ce2;
+        meig1 = Rmax(m1, aeig1); meig2 = Rmax(m2, aeig2); meig3 = Rmax(m2, aeig3);
+    }
+    R xi1 = (two * meig1 - meig2 - meig3) / (two * c2);
+    R xi2 = (meig2 - meig3) / (two * cm);
+    R dc = vnflow * dqv[0] - xn * dqv[1] - yn * dqv[2] - zn * dqv[3];
+    R c2dc = c2 * dc;
+    R ae = gama - one, af = half * ae * v2;
+    R dh = -ae * (um * dqv[1] + vm * dqv[2] + wm * dqv[3] - dqv[4]);
+    dh += af * dqv[0];
+    R term1 = dh * xi1 + dc * xi2;
+    R term2 = c2dc * xi1 + dh * xi2;
+    flux[0] -= (meig1 * dqv[0] - term1);
+    flux[1] -= (meig1 * dqv[1] - um * term1 + xn * term2);
+    flux[2] -= (meig1 * dqv[2] - vm * term1 + yn * term2);
+    flux[3] -= (meig1 * dqv[3] - wm * term1 + zn * term2);
+    flux[4] -= (meig1 * dqv[4] - hm * term1 + vnflow * term2);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) flux[e] *= half;
+}
+
+template <typename R>
+__device__ __forceinline__ R fmSplit2(R mach, R ipn) { return ipn * R(0.25) * (mach + ipn) * (mach + ipn); }
+// FPSplit5, codes/ns/src/NsInvFlux.cpp:56-65 (alpha = 0 on this path)
+template <typename R>
+__device__ __forceinline__ R fpSplit5(R mach, R alpha, R ipn) {
+    R macha = Rabs(mach);
+    if (macha >= R(1)) return R(0.5) * (R(1) + ipn * mach / (macha + small_v<R>()));
+    return fmSplit2(mach, ipn) * ((R(2) * ipn - mach) - ipn * R(16) * alpha * mach * fmSplit2(mach, -ipn));
+}
+
+// NsInvFlux::Slau2, codes/ns/src/NsInvFlux.cpp:1246-1314
+template <typename R>
+__device__ __forceinline__ void slau2Flux(const R *p1, const R *p2, R xn, R yn, R zn, R gam, R *flux) {
+    const R half = R(0.5), one = R(1), vfn = R(0);
+    R rl = p1[IR], ul = p1[IU], vl = p1[IV], wl = p1[IW], pl = p1[IP];
+    R rr = p2[IR], ur = p2[IU], vr = p2[IV], wr = p2[IW], pr = p2[IP];
+    R v2l = SQR3(ul, vl, wl), v2r = SQR3(ur, vr, wr);
+    R hl = (gam / (gam - one)) * (pl / rl) + half * v2l;
+    R hr = (gam / (gam - one)) * (pr / rr) + half * v2r;
+    R vnl = xn * ul + yn * vl + zn * wl - vfn;
+    R vnr = xn * ur + yn * vr + zn * wr - vfn;
+    R orl = one / (rl + small_v<R>()), orr = one / (rr + small_v<R>());
+    R c2l = gam * pl * orl, c2r = gam * pr * orr;
+    R cl = Rsqrt(c2l), cr = Rsqrt(c2r);
+    R cm = half * (cl + cr);
+    R t = rr / rl;
+    R vna = (Rabs(vnl) + t * Rabs(vnr)) / (one + t);
+    R ml = vnl / cm, mr = vnr / cm;
+    R g = -Rmax(Rmin(ml, R(0)), R(-1)) * Rmin(Rmax(mr, R(0)), R(1));
+    R vnp = (one - g) * vna + g * Rabs(vnl);
+    R vnn = (one - g) * vna + g * Rabs(vnr);
+    R va = Rsqrt(half * (v2l + v2r));
+    R m12 = Rmin(one, va / cm);
+    R ka = (one - m12) * (one - m12);
+    R ms = half * (rl * (vnl + vnp) + rr * (vnr - vnn) - ka * (pr - pl) / cm);
+    R fp5ml = fpSplit5(ml, R(0), one);
+    R fp5mr = fpSplit5(mr, R(0), -one);
+    R ps = R(0);
+    ps += half * (pl + pr);
+    ps += half * (fp5ml - fp5mr) * (pl - pr);
+    ps += va * (fp5ml + fp5mr - one) * Rsqrt(rl * rr) * cm;
+    R mp = half * (ms + Rabs(ms)), mn = half * (ms - Rabs(ms));
+    flux[0] = (mp + mn);
+    flux[1] = (mp * ul + mn * ur) + xn * ps;
+    flux[2] = (mp * vl + mn * vr) + yn * ps;
+    flux[3] = (mp * wl + mn * wr) + zn * ps;
+    flux[4] = (mp * hl + mn * hr) + vfn * ps;
+}
+
+}  // namespace ofg

@@ -1,0 +1,165 @@
+// Launch sequences of the tasks, templated on the face arithmetic type.
+// Included by one translation unit per precision (ofg_k64.cu is compiled
+// without FMA contraction so that the FP64 path rounds like the reference).
+#pragma once
+#include "ofg_ctx.h"
+#include "ofg_kernels.cuh"
+
+namespace ofg {
+
+
+// CFL ramp (TimeStep::CalcCfl, codes/ns/src/TimeStep.cpp:43-59).  step < 0:
+// advance the device-side outer-step counter first (graph path).
+static __global__ void k_cfl(double *scal, double step, double cflst, double cfled, int ncfl) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double it = step;
+    if (step < 0) { scal[S_STEP] += 1.0; it = scal[S_STEP]; } else { scal[S_STEP] = step; }
+    double cfl = cfled;
+    if (it < ncfl) {
+        double delta = (cfled - cflst) / ncfl;
+        cfl = cflst + delta * it;
+    }
+    scal[S_CFL] = cfl;
+}
+
+// NsCalcGamaT(F_INNER) + CalcLaminarViscosity(F_INNER) on a state buffer
+static __global__ void k_interior_tvisl(DevParams P, int nCells, double *q) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nCells) return;
+    double *o = q + (size_t)c * REC;
+    double t = o[IP] / (P.statecoef * o[IR] * 1.0);
+    o[ITT] = t;
+    o[IML] = fmax(0.0, sutherland(P, t));
+}
+
+static __global__ void k_norm_hist(double *scal, double *hist, int cap) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int n = int(scal[S_HISTN]);
+    if (n < cap)
+        for (int e = 0; e < NEQ; ++e) hist[(size_t)n * NEQ + e] = scal[S_NORM + e];
+    scal[S_HISTN] = double(n + 1);
+}
+
+template <typename R> DevGeom<R> make_geom(ofg_ctx *c);
+template <> inline DevGeom<double> make_geom<double>(ofg_ctx *c) {
+    double **g = c->d_g64;
+    return DevGeom<double>{g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], g[9], g[10]};
+}
+template <> inline DevGeom<float> make_geom<float>(ofg_ctx *c) {
+    float **g = c->d_g32;
+    return DevGeom<float>{g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], g[9], g[10]};
+}
+
+template <typename R>
+KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
+    KArgs<R> A;
+    A.P = c->dp;
+    A.M.nCells = c->nCells; A.M.nBFaces = c->nBFaces; A.M.nFaces = c->nFaces; A.M.nT = c->nT;
+    A.M.lc = c->d_lc; A.M.rc = c->d_rc; A.M.c2f_off = c->d_c2f_off; A.M.c2f = c->d_c2f; A.M.bcType = c->d_bct;
+    A.M.walldist = c->d_wdist;
+    A.G = make_geom<R>(c);
+    A.q = c->d_q[c->cur];
+    A.qn = onCurrent ? c->d_q[c->cur] : c->d_q[c->cur ^ 1];
+    A.res = c->d_res; A.dq = c->d_dq; A.dt = c->d_dt; A.invsr = c->d_invsr; A.vissr = c->d_vissr;
+    A.bcq = c->d_bcq; A.grad = (R *)c->d_grad; A.lim = (R *)c->d_lim; A.partial = c->d_partial;
+    A.scal = c->d_scal; A.fixlist = c->d_fix; A.fixcap = c->fixcap;
+    return A;
+}
+
+inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
+
+#define OFG_LAUNCH(kern, grid, block, stream, ...)                         \
+    do {                                                                   \
+        kern<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);               \
+        ++c->launches;                                                     \
+    } while (0)
+
+template <typename R>
+int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
+    const int N = c->nCells;
+    switch (task) {
+    case T_CFL: {
+        OFG_LAUNCH(k_cfl, 1, 32, s, c->d_scal, double(c->outerSteps), c->p.cflst, c->p.cfled, c->p.ncfl);
+        break;
+    }
+    case T_ADVANCE: {
+        OFG_LAUNCH(k_cfl, 1, 32, s, c->d_scal, -1.0, c->p.cflst, c->p.cfled, c->p.ncfl);
+        break;
+    }
+    case T_TIMESTEP: {
+        KArgs<R> A = make_args<R>(c, false);
+        int nb = nblk(N, 256);
+        OFG_LAUNCH(k_timestep<R>, nb, 256, s, A);
+        OFG_LAUNCH(k_timestep_min<R>, 1, 256, s, A, nb);
+        OFG_LAUNCH(k_timestep_clip<R>, nb, 256, s, A);
+        break;
+    }
+    case T_RESIDUAL: {
+        KArgs<R> A = make_args<R>(c, false);
+        bool needGrad = c->p.ilim != -1 || c->p.vismodel > 0;
+        if (needGrad) {
+            int nvar = c->p.vismodel > 0 ? 6 : 5;
+            OFG_LAUNCH(k_gradient<R>, nblk(N, 128), 128, s, A, nvar);
+        }
+        if (c->p.ilim == 1 || c->p.ilim == 2) {
+            int nb = nblk(N, 256);
+            OFG_LAUNCH(k_limiter_minmax<R>, nb, 256, s, A, (R *)c->d_mm);
+            if (c->p.ilim == 2 && !c->p.venkat_kh3) OFG_LAUNCH(k_limiter_eps<R>, 1, 256, s, A, nb);
+            OFG_LAUNCH(k_limiter<R>, nblk(N, 128), 128, s, A, (const R *)c->d_mm);
+        } else if (c->p.ilim == 0) {
+            // no limiter: phi = 1 everywhere (Limiter::CalcNoLimiter)
+            // handled by a fill done once at mesh upload
+        }
+        OFG_LAUNCH(k_residual<R>, nblk(N, 128), 128, s, A);
+        break;
+    }
+    case T_LOWER: {
+        KArgs<R> A = make_args<R>(c, false);
+        int nl = int(c->lowOff.size()) - 1;
+        for (int l = 0; l < nl; ++l) {
+            int st = c->lowOff[l], cnt = c->lowOff[l + 1] - st;
+            OFG_LAUNCH(k_lusgs_lower<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_lowOrder, st, cnt);
+        }
+        break;
+    }
+    case T_UPPER: {
+        KArgs<R> A = make_args<R>(c, false);
+        int nl = int(c->upOff.size()) - 1;
+        for (int l = 0; l < nl; ++l) {
+            int st = c->upOff[l], cnt = c->upOff[l + 1] - st;
+            OFG_LAUNCH(k_lusgs_upper<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_upOrder, st, cnt);
+        }
+        break;
+    }
+    case T_UPDATE: {
+        KArgs<R> A = make_args<R>(c, false);
+        OFG_LAUNCH(k_update<R>, nblk(N, 256), 256, s, A);
+        OFG_LAUNCH(k_solution_fix<R>, 1, 32, s, A);
+        break;
+    }
+    case T_BOUNDARY_NEXT: {
+        KArgs<R> A = make_args<R>(c, false);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A);
+        break;
+    }
+    case T_BOUNDARY_CUR: {
+        KArgs<R> A = make_args<R>(c, true);
+        OFG_LAUNCH(k_interior_tvisl, nblk(N, 256), 256, s, c->dp, N, c->d_q[c->cur]);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A);
+        break;
+    }
+    case T_NORM: {
+        KArgs<R> A = make_args<R>(c, false);
+        int nb = 2 * 148;
+        OFG_LAUNCH(k_norm_partial<R>, nb, 256, s, A);
+        OFG_LAUNCH(k_norm_final<R>, 1, 256, s, A, nb, (double *)nullptr);
+        OFG_LAUNCH(k_norm_hist, 1, 32, s, c->d_scal, c->d_hist, c->histCap);
+        break;
+    }
+    default:
+        return c->fail(OFG_E_ARG, "unknown task");
+    }
+    return OFG_OK;
+}
+
+}  // namespace ofg

@@ -1,0 +1,236 @@
+"""Seeded synthetic meshes for the benchmark configurations.
+
+No dataset is involved: every mesh is generated from a formula and a seed
+(numpy PCG64), so the GPU solver and the reference CPU solver read the same
+grid.  Face numbering follows the reference's convention (boundary faces
+first, normal pointing from lCells to rCells).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .meshio import Mesh
+
+SOLID, SYM, FAR, OUT = 2, 3, 4, 6
+
+
+def _faces_from_cells_2d(cells, bc_of_edge):
+    """Edges of a list of CCW polygons (tuples of node ids).  The first cell
+    that lists an edge owns it (lc) and keeps its direction, so the normal
+    (y2-y1, x1-x2) points from lc to rc.  Boundary edges come first, in the
+    order their owning cells list them; interior edges follow in order of
+    first appearance.  bc_of_edge(a, b) -> BC code of a boundary edge."""
+    seen = {}
+    order = []
+    for ci, cell in enumerate(cells):
+        n = len(cell)
+        for k in range(n):
+            a, b = int(cell[k]), int(cell[(k + 1) % n])
+            key = (a, b) if a < b else (b, a)
+            if key in seen:
+                seen[key][2] = ci
+            else:
+                seen[key] = [a, b, -1, ci]
+                order.append(key)
+    bnd = [seen[k] for k in order if seen[k][2] < 0]
+    inn = [seen[k] for k in order if seen[k][2] >= 0]
+    faces = bnd + inn
+    nodes = np.array([[f[0], f[1]] for f in faces], np.int64)
+    lc = np.array([f[3] for f in faces], np.int64)
+    rc = np.array([f[2] for f in faces], np.int64)
+    bct = np.array([bc_of_edge(f[0], f[1]) for f in bnd], np.int32)
+    return nodes, lc, rc, len(bnd), bct
+
+
+def bump_channel(ni: int = 256, nj: int = 128, thickness: float = 0.10, jitter: float = 0.2,
+                 seed: int = 20261203) -> Mesh:
+    """2-D channel [0,3]x[0,1] with a circular-arc bump of the given
+    thickness on the lower wall over x in [1,2]; ni x nj quads, each split in
+    two triangles with an alternating diagonal (2*ni*nj cells); interior nodes
+    jittered by U(-jitter*h, jitter*h).  Walls are SOLID_SURFACE, inlet and
+    outlet FARFIELD."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(0.0, 3.0, ni + 1)
+    # circular arc through (1,0), (1.5,t), (2,0)
+    t = thickness
+    radius = (0.25 + t * t) / (2.0 * t)
+    yb = np.where((xs > 1.0) & (xs < 2.0), np.sqrt(np.maximum(radius ** 2 - (xs - 1.5) ** 2, 0.0)) - (radius - t), 0.0)
+    eta = np.linspace(0.0, 1.0, nj + 1)
+    X = np.repeat(xs[:, None], nj + 1, axis=1)
+    Y = yb[:, None] + (1.0 - yb[:, None]) * eta[None, :]
+    hx = 3.0 / ni
+    hy = (1.0 - yb[:, None]) / nj
+    jx = rng.uniform(-jitter, jitter, X.shape) * hx
+    jy = rng.uniform(-jitter, jitter, X.shape) * hy
+    interior = np.zeros(X.shape, bool)
+    interior[1:-1, 1:-1] = True
+    X = X + np.where(interior, jx, 0.0)
+    Y = Y + np.where(interior, jy, 0.0)
+    nid = lambda i, j: i * (nj + 1) + j
+    tris = []
+    for i in range(ni):
+        for j in range(nj):
+            a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            if (i + j) % 2 == 0:
+                tris.append((a, b, c)); tris.append((a, c, d))
+            else:
+                tris.append((a, b, d)); tris.append((b, c, d))
+    x = X.ravel(); y = Y.ravel()
+
+    def bc(a, b):
+        ia, ja = divmod(a, nj + 1)
+        ib, jb = divmod(b, nj + 1)
+        if ia == ib and ia in (0, ni):
+            return FAR
+        return SOLID
+
+    nodes, lc, rc, nb, bct = _faces_from_cells_2d(tris, bc)
+    nf = nodes.shape[0]
+    return Mesh(2, x, y, np.zeros_like(x), np.full(nf, 2, np.int32), nodes.ravel().astype(np.int32),
+                lc.astype(np.int32), rc.astype(np.int32), len(tris), nb, bct,
+                meta=dict(kind="bump_channel", ni=ni, nj=nj, seed=seed, jitter=jitter))
+
+
+def plate_2d(ni: int = 48, nj: int = 32, ratio: float = 1.15, y1: float = 2.0e-4, x_lead: float = 0.5,
+             length: float = 1.0, jitter: float = 0.1, seed: int = 20261205) -> Mesh:
+    """2-D flat plate of quadrilaterals: wall (SOLID_SURFACE) on y = 0 for
+    x in [0, length], symmetry plane upstream, FARFIELD inlet and top,
+    OUTFLOW at the exit.  Wall-normal spacing grows geometrically from y1;
+    interior nodes jittered in x by U(-jitter*h, jitter*h) (seeded)."""
+    rng = np.random.default_rng(seed)
+    n_up = max(ni // 6, 2)
+    xu = -x_lead * (1.0 - np.linspace(0.0, 1.0, n_up + 1)) ** 1.5
+    xp = length * np.linspace(0.0, 1.0, ni - n_up + 1) ** 1.3
+    xs = np.concatenate([xu[:-1], xp])
+    ys = np.concatenate([[0.0], y1 * np.cumsum(ratio ** np.arange(nj))])
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    hx = np.gradient(xs)[:, None] * np.ones_like(X)
+    interior = np.zeros(X.shape, bool)
+    interior[1:-1, 1:-1] = True
+    X = X + np.where(interior, rng.uniform(-jitter, jitter, X.shape) * hx, 0.0)
+    nid = lambda i, j: i * (nj + 1) + j
+    quads = [(nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)) for i in range(ni) for j in range(nj)]
+    x, y = X.ravel(), Y.ravel()
+
+    def bc(a, b):
+        ia, ja = divmod(a, nj + 1)
+        ib, jb = divmod(b, nj + 1)
+        if ja == 0 and jb == 0:
+            return SOLID if min(xs[ia], xs[ib]) >= -1e-12 else SYM
+        if ia == ib == ni:
+            return OUT
+        return FAR
+
+    nodes, lc, rc, nb, bct = _faces_from_cells_2d(quads, bc)
+    nf = nodes.shape[0]
+    return Mesh(2, x, y, np.zeros_like(x), np.full(nf, 2, np.int32), nodes.ravel().astype(np.int32),
+                lc.astype(np.int32), rc.astype(np.int32), len(quads), nb, bct,
+                meta=dict(kind="plate_2d", ni=ni, nj=nj, seed=seed))
+
+
+# ------------------------------------------------------------------------
+# 3-D flat plate: hexahedral lattice split into 6 tetrahedra per hex
+# ------------------------------------------------------------------------
+# Kuhn split of the unit cube along the diagonal v0 -> v6; vertex ids
+# 0:(0,0,0) 1:(1,0,0) 2:(1,1,0) 3:(0,1,0) 4:(0,0,1) 5:(1,0,1) 6:(1,1,1) 7:(0,1,1).
+# Every tet is a monotone path 0 -> ... -> 6, so shared quad faces of
+# neighbouring hexes get the same diagonal and the tets conform.
+_KUHN = np.array([[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6], [0, 7, 4, 6], [0, 4, 5, 6], [0, 5, 1, 6]], np.int64)
+_CORNER = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], np.int64)
+
+
+def flat_plate_tets(nx: int = 200, ny: int = 100, nz: int = 50, ratio: float = 1.15, reynolds: float = 5.0e6,
+                    yplus: float = 1.0, x_lead: float = 0.5, length: float = 1.0, span: float = 0.5,
+                    jitter: float = 0.1, seed: int = 20261204) -> Mesh:
+    """Flat plate on y = 0, x in [0, length], preceded by a symmetry plane over
+    [-x_lead, 0).  Wall-normal spacing grows geometrically (ratio) from a
+    first cell at the requested y+ (turbulent skin-friction estimate
+    cf = 0.0592 Re^-0.2 at x = length).  Each of nx*ny*nz hexes is split into 6
+    tets (6*nx*ny*nz cells).  Interior nodes are jittered in x and z by
+    U(-jitter*h, jitter*h) (seeded).  BCs: wall SOLID_SURFACE, upstream floor
+    and both span planes SYMMETRY, inlet/top/outlet FARFIELD."""
+    rng = np.random.default_rng(seed)
+    cf = 0.0592 * reynolds ** -0.2
+    utau = np.sqrt(0.5 * cf)
+    y1 = yplus / (utau * reynolds)
+    ys = np.concatenate([[0.0], y1 * np.cumsum(ratio ** np.arange(ny))])
+    # x: cluster at the leading edge, uniform-ish on the plate
+    n_up = max(nx // 8, 2)
+    xu = -x_lead * (1.0 - np.linspace(0.0, 1.0, n_up + 1)) ** 1.5
+    xp = length * np.linspace(0.0, 1.0, nx - n_up + 1) ** 1.2
+    xs = np.concatenate([xu[:-1], xp])
+    zs = np.linspace(0.0, span, nz + 1)
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    hx = np.gradient(xs)[:, None, None] * np.ones_like(X)
+    hz = (span / nz) * np.ones_like(X)
+    interior = np.zeros(X.shape, bool)
+    interior[1:-1, 1:-1, 1:-1] = True
+    X = X + np.where(interior, rng.uniform(-jitter, jitter, X.shape) * hx, 0.0)
+    Z = Z + np.where(interior, rng.uniform(-jitter, jitter, X.shape) * hz, 0.0)
+    NX, NY, NZ = nx + 1, ny + 1, nz + 1
+    x, y, z = X.ravel(), Y.ravel(), Z.ravel()
+    nid = lambda i, j, k: (i * NY + j) * NZ + k
+
+    # hex cells in natural (k fastest, then j, then i) order, 6 tets each
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    corner = np.stack([nid(ii + c[0], jj + c[1], kk + c[2]) for c in _CORNER], axis=1)  # [nhex, 8]
+    tets = corner[:, _KUHN].reshape(-1, 4)                                           # [6*nhex, 4]
+    nc = tets.shape[0]
+    # tet faces (opposite each vertex), oriented outward
+    lf = np.array([[1, 2, 3], [0, 3, 2], [0, 1, 3], [0, 2, 1]], np.int64)
+    tri = tets[:, lf].reshape(-1, 3)
+    owner = np.repeat(np.arange(nc), 4)
+    # orient outward: normal . (face centroid - cell centroid) > 0
+    P = np.stack([x, y, z], 1)
+    cc = P[tets].mean(1)
+    a, b, c = P[tri[:, 0]], P[tri[:, 1]], P[tri[:, 2]]
+    nrm = np.cross(b - a, c - a)
+    out = np.einsum("ij,ij->i", nrm, (a + b + c) / 3.0 - cc[owner]) > 0
+    tri[~out] = tri[~out][:, [0, 2, 1]]
+    del a, b, c, nrm, out, cc
+    s = np.sort(tri, axis=1)
+    key = (s[:, 0] * (len(x)) + s[:, 1]) * len(x) + s[:, 2]
+    del s
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    del key
+    new = np.ones(ks.shape[0], bool)
+    new[1:] = ks[1:] != ks[:-1]
+    grp = np.cumsum(new) - 1
+    nf = int(grp[-1]) + 1
+    first = order[new]
+    cnt = np.bincount(grp, minlength=nf)
+    # for interior faces the second entry of the group is the other cell
+    pos2 = np.flatnonzero(new) + 1
+    has2 = cnt == 2
+    lc = owner[first]
+    rc = np.full(nf, -1, np.int64)
+    rc[has2] = owner[order[pos2[has2]]]
+    nodes = tri[first]
+    # the face keeps the lower cell as lc (its outward orientation)
+    swap = has2 & (rc < lc)
+    lc2 = np.where(swap, rc, lc)
+    rc2 = np.where(swap, lc, rc)
+    second_nodes = tri[order[np.minimum(pos2, len(order) - 1)]]
+    nodes = np.where(swap[:, None], second_nodes, nodes)
+    lc, rc = lc2, rc2
+    del order, ks, grp, new, second_nodes
+    isb = rc < 0
+    # boundary classification from the face centroid position
+    fcx = x[nodes].mean(1); fcy = y[nodes].mean(1); fcz = z[nodes].mean(1)
+    tol = 1e-12
+    bct_all = np.full(nf, FAR, np.int32)
+    floor = fcy < y1 * 1e-6
+    bct_all[floor & (fcx >= -tol)] = SOLID
+    bct_all[floor & (fcx < -tol)] = SYM
+    sidez = (np.abs(fcz) < tol) | (np.abs(fcz - span) < tol)
+    bct_all[sidez & ~floor] = SYM
+    # order: boundary faces first (by owning cell), interior faces by (lc, rc)
+    forder = np.lexsort((rc, lc, ~isb))
+    lc, rc, nodes, bct_all = lc[forder], rc[forder], nodes[forder], bct_all[forder]
+    nb = int(isb.sum())
+    mesh = Mesh(3, x, y, z, np.full(nf, 3, np.int32), nodes.ravel().astype(np.int32), lc.astype(np.int32),
+                rc.astype(np.int32), nc, nb, bct_all[:nb].copy(),
+                meta=dict(kind="flat_plate_tets", nx=nx, ny=ny, nz=nz, ratio=ratio, y1=y1, seed=seed))
+    return mesh

@@ -1,0 +1,167 @@
+"""Python face of the C ABI: one ``Solver`` per context, with one method per
+reference task (the names of system/ns/function/funcMap.txt) and the fused
+outer iteration.  The CUDA library is required: there is no CPU path."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import params as P
+from .meshio import Mesh
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libofg.so")
+
+NS_SOLVER, TURB_SOLVER = 0, 1
+_dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+class OfgError(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def load_library() -> C.CDLL:
+    """Load oneflow_b200/libofg.so (built by ``__graft_entry__.build()`` or
+    ``make -C oneflow_b200/csrc``).  Raises if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise OfgError(f"CUDA library not built: {LIB_PATH} (run make -C oneflow_b200/csrc)")
+    L = C.CDLL(LIB_PATH)
+    L.ofg_default_params.argtypes = [C.POINTER(P.OfgParams)]
+    L.ofg_create.argtypes = [C.POINTER(P.OfgParams), C.POINTER(C.c_void_p)]
+    L.ofg_destroy.argtypes = [C.c_void_p]
+    L.ofg_last_error.argtypes = [C.c_void_p]
+    L.ofg_last_error.restype = C.c_char_p
+    L.ofg_upload_mesh.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip, C.c_int, C.c_int,
+                                  _ip, C.c_void_p]
+    for name in ("ofg_init_flowfield",):
+        getattr(L, name).argtypes = [C.c_void_p]
+    L.ofg_upload_state.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ofg_download_state.argtypes = [C.c_void_p, C.c_int, _dp]
+    for name in ("ofg_zero_dq", "ofg_calc_time_step", "ofg_load_residuals", "ofg_update_residuals", "ofg_init_lusgs",
+                 "ofg_lusgs_lower", "ofg_lusgs_upper", "ofg_update_flowfield", "ofg_calc_boundary"):
+        getattr(L, name).argtypes = [C.c_void_p, C.c_int]
+    L.ofg_step.argtypes = [C.c_void_p, C.c_int]
+    L.ofg_residual_norms.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ofg_download_field.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+    L.ofg_get_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.ofg_set_outer_step.argtypes = [C.c_void_p, C.c_int64]
+    L.ofg_colour_order.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip]
+    L.ofg_version.restype = C.c_int
+    _LIB = L
+    return L
+
+
+# reference task name -> C entry point (funcMap.txt / TimeIntegral::Lusgs)
+TASKS = {
+    "ZERO_DQ_FIELD": "ofg_zero_dq",
+    "CALC_TIME_STEP": "ofg_calc_time_step",
+    "LOAD_RESIDUALS": "ofg_load_residuals",
+    "UPDATE_RESIDUALS": "ofg_update_residuals",
+    "INIT_LUSGS": "ofg_init_lusgs",
+    "LUSGS_LOWER_SWEEP": "ofg_lusgs_lower",
+    "LUSGS_UPPER_SWEEP": "ofg_lusgs_upper",
+    "UPDATE_FLOWFIELD_LUSGS": "ofg_update_flowfield",
+    "CALC_BOUNDARY": "ofg_calc_boundary",
+}
+LUSGS_SEQUENCE = ["ZERO_DQ_FIELD", "CALC_TIME_STEP", "LOAD_RESIDUALS", "UPDATE_RESIDUALS", "INIT_LUSGS",
+                  "LUSGS_LOWER_SWEEP", "LUSGS_UPPER_SWEEP", "UPDATE_FLOWFIELD_LUSGS", "CALC_BOUNDARY"]
+
+
+class Solver:
+    """One steady solve on one GPU."""
+
+    def __init__(self, mesh: Mesh, params: P.OfgParams):
+        self.L = load_library()
+        self.mesh = mesh
+        self.params = params
+        h = C.c_void_p()
+        rc = self.L.ofg_create(C.byref(params), C.byref(h))
+        if rc != 0:
+            raise OfgError(f"ofg_create failed ({rc})")
+        self.h = h
+        self.nT = mesh.n_cells + mesh.n_bfaces
+        a = mesh.as_arrays()
+        self._keep = a
+        wd = None if a["wd"] is None else a["wd"].ctypes.data_as(C.c_void_p)
+        self._check(self.L.ofg_upload_mesh(self.h, mesh.n_nodes, a["x"], a["y"], a["z"], mesh.n_faces, a["fnc"],
+                                           a["fn"], a["lc"], a["rc"], mesh.n_cells, mesh.n_bfaces, a["bct"], wd))
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.L.ofg_last_error(self.h)
+            raise OfgError(f"error {rc}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ofg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- lifecycle ----
+    def init_flowfield(self):
+        self._check(self.L.ofg_init_flowfield(self.h))
+
+    def upload_state(self, q: np.ndarray, tid: int = NS_SOLVER):
+        self._check(self.L.ofg_upload_state(self.h, tid, np.ascontiguousarray(q, np.float64).ravel()))
+
+    def state(self, tid: int = NS_SOLVER) -> np.ndarray:
+        out = np.empty(5 * self.nT, np.float64)
+        self._check(self.L.ofg_download_state(self.h, tid, out))
+        return out.reshape(5, self.nT)
+
+    # ---- tasks ----
+    def task(self, name: str, tid: int = NS_SOLVER):
+        self._check(getattr(self.L, TASKS[name])(self.h, tid))
+
+    def set_outer_step(self, n: int):
+        """Iteration::outerSteps as seen by the next CALC_TIME_STEP (task API)."""
+        self._check(self.L.ofg_set_outer_step(self.h, n))
+
+    def step(self, n: int = 1):
+        self._check(self.L.ofg_step(self.h, n))
+
+    def residual_norms(self, tid: int = NS_SOLVER) -> np.ndarray:
+        out = np.empty(5, np.float64)
+        self._check(self.L.ofg_residual_norms(self.h, tid, out))
+        return out
+
+    def field(self, name: str, tid: int = NS_SOLVER) -> np.ndarray:
+        need = C.c_int64()
+        self._check(self.L.ofg_download_field(self.h, tid, name.encode(), None, 0, C.byref(need)))
+        out = np.empty(need.value, np.float64)
+        self._check(self.L.ofg_download_field(self.h, tid, name.encode(), out.ctypes.data_as(C.c_void_p),
+                                              need.value, C.byref(need)))
+        return out
+
+    def res_history(self) -> np.ndarray:
+        return self.field("reshist").reshape(-1, 5)
+
+    def counters(self):
+        a, b = C.c_int64(), C.c_int64()
+        self._check(self.L.ofg_get_counters(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+
+def colour_order(mesh: Mesh):
+    """(perm, ncolours): the colour-major cell order of ofg_colour_order."""
+    L = load_library()
+    perm = np.empty(mesh.n_cells, np.int32)
+    a = mesh.as_arrays()
+    n = L.ofg_colour_order(mesh.n_cells, mesh.n_faces, mesh.n_bfaces, a["lc"], a["rc"], perm)
+    if n < 0:
+        raise OfgError(f"ofg_colour_order failed ({n})")
+    return perm, n

@@ -1,0 +1,1114 @@
+// CPU restatement of OneFLOW's unstructured residual + LU-SGS iteration.
+//
+// TEST INFRASTRUCTURE ONLY: this file is the oracle that the CUDA path is
+// checked against (tests/, __graft_entry__.smoke(), bench.py's CPU
+// baseline).  Nothing in the product imports, links or calls it.
+//
+// It restates, in plain sequential FP64 C++, the algorithms of the reference
+// (eric2003/OneFLOW) in the same summation order as the reference's serial
+// loops; each function cites the reference file:line it follows.  The
+// oracle is pinned against the reference itself: oracle/refbuild builds the
+// reference CPU solver into oracle/_ref and the tests compare the two on
+// the reference's own regression cases and on the seeded meshes.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+const double SMALL = 1.0e-40;   // codes/basic/include/HXTypeBasic.h:34
+const double LARGE = 1.0e40;    // codes/basic/include/HXTypeBasic.h:33
+const double half = 0.5, two3rd = 2.0 / 3.0, third = 1.0 / 3.0, fourth = 0.25;
+const double PI = 3.141592653589793;
+
+inline double SQR3(double a, double b, double c) { return a * a + b * b + c * c; }
+inline double DIST3(double a, double b, double c) { return std::sqrt(SQR3(a, b, c)); }
+inline double MAXd(double a, double b) { return a > b ? a : b; }
+inline double MINd(double a, double b) { return a < b ? a : b; }
+
+enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4 };
+const int NEQ = 5;
+
+}  // namespace
+
+struct Oracle {
+    ofg_params p;
+    // ---------------- mesh ----------------
+    int nNodes = 0, nFaces = 0, nCells = 0, nBFaces = 0, nT = 0;
+    std::vector<double> xN, yN, zN;
+    std::vector<std::vector<int>> f2n;
+    std::vector<int> lc, rc, bcType;
+    std::vector<double> xfn, yfn, zfn, area, xfc, yfc, zfc;
+    std::vector<double> xcc, ycc, zcc, vol;
+    std::vector<std::vector<int>> c2f;
+    std::vector<double> walldist;
+    // ---------------- fields (reference layout [eq][nT]) ----------------
+    std::vector<double> q[NEQ], dq[NEQ], res[NEQ];
+    std::vector<double> dqdx[NEQ], dqdy[NEQ], dqdz[NEQ], limiter[NEQ];
+    std::vector<double> bc_q[NEQ];
+    std::vector<double> tempr, dtdx, dtdy, dtdz, visl, vist;
+    std::vector<double> timestep, invsr, vissr, impsr;
+    // turbulence (SA), reference layout
+    std::vector<double> nut, dnut, resT, dtT, impsrT, invsrT, vissrT, dnutdx, dnutdy, dnutdz;
+    // ---------------- reference state ----------------
+    double statecoef = 0, pref = 0, inflow[NEQ] = {0}, oreynolds = 0, const_cp = 0, oprl = 0, oprt = 0;
+    double sutherland_ts = 0;
+    double cfl = 0;
+    long outerSteps = 0;
+    std::vector<double> resHist;      // per outer step: 5 NS RMS (+1 SA RMS if present)
+    std::string err;
+
+    // ======================= mesh & metrics =======================
+    // codes/geometry/src/UnsGrid.cpp:131-176 (face reversal), :123-129 (ghost ids)
+    int setMesh(int nn, const double *x, const double *y, const double *z, int nf, const int *fnc,
+                const int *fn, const int *l, const int *r, int nc, int nb, const int *bct, const double *wd) {
+        nNodes = nn; nFaces = nf; nCells = nc; nBFaces = nb; nT = nc + nb;
+        xN.assign(x, x + nn); yN.assign(y, y + nn); zN.assign(z, z + nn);
+        f2n.assign(nf, {});
+        size_t pos = 0;
+        for (int f = 0; f < nf; ++f) { f2n[f].assign(fn + pos, fn + pos + fnc[f]); pos += fnc[f]; }
+        lc.assign(l, l + nf); rc.assign(r, r + nf);
+        for (int f = 0; f < nf; ++f)
+            if (lc[f] < 0) { std::reverse(f2n[f].begin(), f2n[f].end()); std::swap(lc[f], rc[f]); }
+        for (int f = 0; f < nb; ++f) rc[f] = f + nc;  // UnsGrid::NormalizeBc
+        bcType.assign(bct, bct + nb);
+        walldist.assign(nT, 0.0);
+        if (wd) for (int c = 0; c < nc; ++c) walldist[c] = wd[c];
+        calcMetrics();
+        // CellTopo::CalcC2f, codes/geometry/src/CellTopo.cpp:95-119
+        c2f.assign(nT, {});
+        for (int f = 0; f < nb; ++f) c2f[lc[f]].push_back(f);
+        for (int f = nb; f < nf; ++f) { c2f[lc[f]].push_back(f); c2f[rc[f]].push_back(f); }
+        alloc();
+        return 0;
+    }
+
+    void calcMetrics() {
+        xfn.assign(nFaces, 0); yfn.assign(nFaces, 0); zfn.assign(nFaces, 0); area.assign(nFaces, 0);
+        xfc.assign(nFaces, 0); yfc.assign(nFaces, 0); zfc.assign(nFaces, 0);
+        xcc.assign(nT, 0); ycc.assign(nT, 0); zcc.assign(nT, 0); vol.assign(nT, 0);
+        if (p.dimension == 2) {
+            // FaceMesh::CalcFaceNormal2D / CalcFaceCenter2D, codes/geometry/src/FaceMesh.cpp:112-160
+            for (int f = 0; f < nFaces; ++f) {
+                int p1 = f2n[f][0], p2 = f2n[f][1];
+                xfn[f] = yN[p2] - yN[p1];
+                yfn[f] = xN[p1] - xN[p2];
+                zfn[f] = 0.0;
+                area[f] = DIST3(xfn[f], yfn[f], zfn[f]);
+            }
+            for (int f = 0; f < nFaces; ++f) {
+                double oa = 1.0 / (area[f] + SMALL);
+                xfn[f] *= oa; yfn[f] *= oa; zfn[f] *= oa;
+            }
+            for (int f = 0; f < nFaces; ++f) {
+                int p1 = f2n[f][0], p2 = f2n[f][1];
+                xfc[f] = half * (xN[p1] + xN[p2]);
+                yfc[f] = half * (yN[p1] + yN[p2]);
+                zfc[f] = half * (zN[p1] + zN[p2]);
+            }
+            // UnsGrid::CalcCellCenterVol2D, codes/geometry/src/UnsGrid.cpp:630-741
+            for (int f = 0; f < nBFaces; ++f) {
+                int l = lc[f];
+                double dot = (xfc[f] * xfn[f] + yfc[f] * yfn[f] + zfc[f] * zfn[f]) * area[f];
+                xcc[l] += xfc[f] * dot; ycc[l] += yfc[f] * dot; zcc[l] += zfc[f] * dot; vol[l] += dot;
+            }
+            for (int f = nBFaces; f < nFaces; ++f) {
+                int l = lc[f], r = rc[f];
+                double dot = (xfc[f] * xfn[f] + yfc[f] * yfn[f] + zfc[f] * zfn[f]) * area[f];
+                xcc[l] += xfc[f] * dot; ycc[l] += yfc[f] * dot; zcc[l] += zfc[f] * dot; vol[l] += dot;
+                xcc[r] -= xfc[f] * dot; ycc[r] -= yfc[f] * dot; zcc[r] -= zfc[f] * dot; vol[r] -= dot;
+            }
+            for (int c = 0; c < nCells; ++c) {
+                double tmp = 1.0 / (1.5 * vol[c] + SMALL);
+                xcc[c] *= tmp; ycc[c] *= tmp; zcc[c] *= tmp;
+                vol[c] *= half;
+                if (vol[c] <= 0.0) vol[c] = -vol[c];
+            }
+        } else {
+            // FaceMesh::CalcFaceNormal3D, codes/geometry/src/FaceMesh.cpp:162-208
+            for (int f = 0; f < nFaces; ++f) {
+                const std::vector<int> &fi = f2n[f];
+                size_t n = fi.size();
+                for (size_t i = 0; i < n; ++i) {
+                    int p1 = fi[i], p2 = fi[(i + 1) % n];
+                    double dx1 = xN[p1], dy1 = yN[p1], dz1 = zN[p1];
+                    double dx2 = xN[p2], dy2 = yN[p2], dz2 = zN[p2];
+                    xfn[f] += half * (dy1 * dz2 - dy2 * dz1);
+                    yfn[f] += half * (dz1 * dx2 - dz2 * dx1);
+                    zfn[f] += half * (dx1 * dy2 - dx2 * dy1);
+                }
+                area[f] = DIST3(xfn[f], yfn[f], zfn[f]);
+            }
+            for (int f = 0; f < nFaces; ++f) {
+                double oa = 1.0 / (area[f] + SMALL);
+                xfn[f] *= oa; yfn[f] *= oa; zfn[f] *= oa;
+            }
+            // FaceMesh::CalcFaceCenter3D, codes/geometry/src/FaceMesh.cpp:210-286
+            for (int f = 0; f < nFaces; ++f) {
+                const std::vector<int> &fi = f2n[f];
+                size_t n = fi.size();
+                double x0 = 0, y0 = 0, z0 = 0;
+                for (size_t i = 0; i < n; ++i) { x0 += xN[fi[i]]; y0 += yN[fi[i]]; z0 += zN[fi[i]]; }
+                double factor = 1.0 / n;
+                x0 *= factor; y0 *= factor; z0 *= factor;
+                double sx = 0, sy = 0, sz = 0, sarea = 0;
+                for (size_t i = 0; i < n; ++i) {
+                    int p1 = fi[i], p2 = fi[(i + 1) % n];
+                    double dx1 = xN[p1] - x0, dy1 = yN[p1] - y0, dz1 = zN[p1] - z0;
+                    double dx2 = xN[p2] - x0, dy2 = yN[p2] - y0, dz2 = zN[p2] - z0;
+                    double x00 = third * (xN[p1] + xN[p2] + x0);
+                    double y00 = third * (yN[p1] + yN[p2] + y0);
+                    double z00 = third * (zN[p1] + zN[p2] + z0);
+                    double anx = dy1 * dz2 - dy2 * dz1;
+                    double any = dz1 * dx2 - dz2 * dx1;
+                    double anz = dx1 * dy2 - dx2 * dy1;
+                    double fa = half * DIST3(anx, any, anz);
+                    double nrm = anx * xfn[f] + any * yfn[f] + anz * zfn[f];
+                    if (nrm < 0.0) fa = -fa;
+                    sarea += fa;
+                    sx += fa * x00; sy += fa * y00; sz += fa * z00;
+                }
+                double os = 1.0 / (sarea + SMALL);
+                xfc[f] = sx * os; yfc[f] = sy * os; zfc[f] = sz * os;
+            }
+            // UnsGrid::CalcCellCenterVol3D, codes/geometry/src/UnsGrid.cpp:743-886
+            for (int f = 0; f < nFaces; ++f) {
+                int l = lc[f], r = rc[f];
+                const std::vector<int> &fi = f2n[f];
+                size_t n = fi.size();
+                for (size_t i = 0; i < n; ++i) {
+                    int p2 = fi[i], p3 = fi[(i + 1) % n];
+                    double x21 = xN[p2] - xfc[f], y21 = yN[p2] - yfc[f], z21 = zN[p2] - zfc[f];
+                    double x31 = xN[p3] - xfc[f], y31 = yN[p3] - yfc[f], z31 = zN[p3] - zfc[f];
+                    double nx = y21 * z31 - y31 * z21;
+                    double ny = z21 * x31 - z31 * x21;
+                    double nz = x21 * y31 - x31 * y21;
+                    double trix = xfc[f] + xN[p2] + xN[p3];
+                    double triy = yfc[f] + yN[p2] + yN[p3];
+                    double triz = zfc[f] + zN[p2] + zN[p3];
+                    double tmp = nx * trix + ny * triy + nz * triz;
+                    trix *= tmp; triy *= tmp; triz *= tmp;
+                    xcc[l] += trix; ycc[l] += triy; zcc[l] += triz; vol[l] += tmp;
+                    xcc[r] -= trix; ycc[r] -= triy; zcc[r] -= triz; vol[r] -= tmp;
+                }
+            }
+            for (int c = 0; c < nCells; ++c) {
+                double tmp = 1.0 / (4.0 * vol[c] + SMALL);
+                xcc[c] *= tmp; ycc[c] *= tmp; zcc[c] *= tmp;
+                vol[c] /= 18.0;
+                if (vol[c] <= 0.0) vol[c] = -vol[c];
+            }
+        }
+        // ghost cells (mirror of the interior centre through the face)
+        for (int f = 0; f < nBFaces; ++f) {
+            int l = lc[f], r = f + nCells;
+            if (area[f] > SMALL) {
+                double tmp = 2.0 * ((xcc[l] - xfc[f]) * xfn[f] + (ycc[l] - yfc[f]) * yfn[f] +
+                                    (zcc[l] - zfc[f]) * zfn[f]);
+                xcc[r] = xcc[l] - xfn[f] * tmp;
+                ycc[r] = ycc[l] - yfn[f] * tmp;
+                zcc[r] = zcc[l] - zfn[f] * tmp;
+            } else {
+                xcc[r] = -xcc[l] + 2.0 * xfc[f];
+                ycc[r] = -ycc[l] + 2.0 * yfc[f];
+                zcc[r] = -zcc[l] + 2.0 * zfc[f];
+            }
+            vol[r] = vol[l];
+        }
+    }
+
+    void alloc() {
+        for (int e = 0; e < NEQ; ++e) {
+            q[e].assign(nT, 0); dq[e].assign(nT, 0); res[e].assign(nT, 0);
+            dqdx[e].assign(nT, 0); dqdy[e].assign(nT, 0); dqdz[e].assign(nT, 0);
+            limiter[e].assign(nT, 1.0); bc_q[e].assign(nBFaces, 0);
+        }
+        tempr.assign(nT, 0); dtdx.assign(nT, 0); dtdy.assign(nT, 0); dtdz.assign(nT, 0);
+        visl.assign(nT, 0); vist.assign(nT, 0);
+        timestep.assign(nT, 0); invsr.assign(nT, 0); vissr.assign(nT, 0); impsr.assign(nT, 0);
+        nut.assign(nT, 0); dnut.assign(nT, 0); resT.assign(nT, 0); dtT.assign(nT, 0);
+        impsrT.assign(nT, 0); invsrT.assign(nT, 0); vissrT.assign(nT, 0);
+        dnutdx.assign(nT, 0); dnutdy.assign(nT, 0); dnutdz.assign(nT, 0);
+    }
+
+    // ======================= reference state =======================
+    // codes/chemical/src/Chemical.cpp:280-325, codes/ns/src/NsCom.cpp:45-94
+    void initReference() {
+        statecoef = 1.0 / (p.gama_ref * p.mach_ref * p.mach_ref);
+        pref = statecoef * 1.0 * 1.0 / 1.0;
+        double aoa = p.aoa_degree * PI / 180.0, aos = p.sideslip_degree * PI / 180.0;
+        inflow[IR] = 1.0;
+        inflow[IU] = 1.0 * std::cos(aoa) * std::cos(aos);
+        inflow[IV] = 1.0 * std::sin(aoa) * std::cos(aos);
+        inflow[IW] = 1.0 * std::sin(aos);
+        inflow[IP] = pref;
+        oreynolds = 1.0 / p.reynolds;
+        oprl = 1.0 / p.prl;
+        oprt = 1.0 / p.prt;
+        const_cp = 1.0 / ((p.gama_ref - 1.0) * (p.mach_ref * p.mach_ref));
+        sutherland_ts = 110.4 / p.tref_dim;  // codes/model/src/Sutherland.cpp:47-53
+    }
+
+    // codes/model/src/Sutherland.cpp:62-66
+    double sutherland(double t) const {
+        double t3 = t * t * t;
+        return std::sqrt(t3) * (1 + sutherland_ts) / (t + sutherland_ts);
+    }
+
+    // ======================= CALC_BOUNDARY =======================
+    // NsCalcGamaT (codes/ns/src/NsRhs.cpp:71-95) on [ist, ied)
+    void calcT(int ist, int ied) {
+        for (int c = ist; c < ied; ++c) tempr[c] = q[IP][c] / (statecoef * q[IR][c] * 1.0);
+    }
+    // CalcLaminarViscosity, codes/uns/src/UNsVisFlux.cpp:442-459
+    void calcVisl(int ist, int ied) {
+        for (int c = ist; c < ied; ++c) visl[c] = MAXd(0.0, sutherland(tempr[c]));
+    }
+
+    // NsBcSolver face BCs, codes/ns/src/NsBcSolver.cpp:51-440 via
+    // UNsBcSolver::CalcBc, codes/uns/src/UNsBcSolver.cpp:55-166
+    void calcBc() {
+        double gama = p.gama_ref;
+        for (int f = 0; f < nBFaces; ++f) {
+            int bt = bcType[f];
+            int l = lc[f], r = rc[f];
+            double s[NEQ], t[NEQ], pr[NEQ];
+            bool havePrim = false;
+            for (int e = 0; e < NEQ; ++e) s[e] = q[e][l];
+            double xn = xfn[f], yn = yfn[f], zn = zfn[f], vfn = 0.0;
+            if (bt == OFG_BC_SYMMETRY || (bt == OFG_BC_SOLID_SURFACE && p.vismodel == 0)) {
+                // SymmetryBc, :396-430
+                double vn = xn * s[IU] + yn * s[IV] + zn * s[IW] - vfn;
+                for (int e = 0; e < NEQ; ++e) t[e] = s[e];
+                t[IU] = s[IU] - 2.0 * xn * vn;
+                t[IV] = s[IV] - 2.0 * yn * vn;
+                t[IW] = s[IW] - 2.0 * zn * vn;
+                for (int e = 0; e < NEQ; ++e) pr[e] = half * (s[e] + t[e]);
+                havePrim = true;
+            } else if (bt == OFG_BC_SOLID_SURFACE && p.isowallbc == 0) {
+                // AdiabaticVisWallBc + VelocityBc (vfx = 0), :357-394
+                for (int e = 0; e < NEQ; ++e) t[e] = s[e];
+                t[IU] = -t[IU] + 2.0 * 0.0;
+                t[IV] = -t[IV] + 2.0 * 0.0;
+                t[IW] = -t[IW] + 2.0 * 0.0;
+                pr[IR] = s[IR]; pr[IU] = 0.0; pr[IV] = 0.0; pr[IW] = 0.0; pr[IP] = s[IP];
+                havePrim = true;
+            } else if (bt == OFG_BC_SOLID_SURFACE) {
+                // IsothermalVisWallBc, :278-340
+                for (int e = 0; e < NEQ; ++e) t[e] = s[e];
+                t[IU] = -t[IU]; t[IV] = -t[IV]; t[IW] = -t[IW];
+                double twall = p.twall_dim / p.tref_dim;
+                double tlim = 0.1 * twall;
+                double rm = s[IR], pm = s[IP], temperature = tempr[l];
+                double rw_face = pm / (statecoef * twall * 1.0);
+                pr[IR] = rw_face; pr[IU] = 0; pr[IV] = 0; pr[IW] = 0; pr[IP] = pm;
+                double pg1 = pm, tg1 = 2.0 * twall - temperature;
+                if (tg1 < tlim) tg1 = tlim;
+                double rw = pg1 / (statecoef * twall * 1.0);
+                double rg1 = 2.0 * rw - rm;
+                rg1 = MAXd(0.5 * rw, rg1);
+                t[IR] = rg1; t[IP] = pg1;
+                (void)tg1;
+                havePrim = true;
+            } else if (bt == OFG_BC_FARFIELD) {
+                // FarFieldBc, :171-276
+                for (int e = 0; e < NEQ; ++e) t[e] = s[e];
+                double rin = s[IR], uin = s[IU], vin = s[IV], win = s[IW], pin = s[IP];
+                double rref = inflow[IR], uref = inflow[IU], vref = inflow[IV], wref = inflow[IW], pref_ = inflow[IP];
+                double vnref = xn * uref + yn * vref + zn * wref - vfn;
+                double vnin = xn * uin + yn * vin + zn * win - vfn;
+                double cref = std::sqrt(std::fabs(p.gama_ref * pref_ / rref));
+                double cin = std::sqrt(std::fabs(gama * pin / rin));
+                double gamm1 = gama - 1.0;
+                double velin = DIST3(uin, vin, win);
+                if (velin > cin) {
+                    if (vnin >= 0.0) {
+                        for (int e = 0; e < NEQ; ++e) t[e] = s[e];
+                    } else {
+                        for (int e = 0; e < NEQ; ++e) t[e] = inflow[e];
+                    }
+                } else {
+                    double riemp = vnin + 2.0 * cin / gamm1;
+                    double riemm = vnref - 2.0 * cref / gamm1;
+                    double vnb = half * (riemp + riemm);
+                    double cb = fourth * (riemp - riemm) * gamm1;
+                    double vtx, vty, vtz, entr;
+                    if (vnb >= 0.0) {
+                        entr = pin / std::pow(rin, gama);
+                        vtx = uin - xn * vnin; vty = vin - yn * vnin; vtz = win - zn * vnin;
+                    } else {
+                        entr = pref_ / std::pow(rref, gama);
+                        vtx = uref - xn * vnref; vty = vref - yn * vnref; vtz = wref - zn * vnref;
+                    }
+                    double rb = std::pow((cb * cb / (entr * gama)), 1.0 / gamm1);
+                    double ub = vtx + xn * vnb, vb = vty + yn * vnb, wb = vtz + zn * vnb;
+                    double pb = cb * cb * rb / gama;
+                    t[IR] = rb; t[IU] = ub; t[IV] = vb; t[IW] = wb; t[IP] = pb;
+                }
+            } else if (bt == OFG_BC_INFLOW) {
+                for (int e = 0; e < NEQ; ++e) t[e] = inflow[e];
+            } else {  // OUTFLOW, EXTRAPOLATION, POLE: copy interior
+                for (int e = 0; e < NEQ; ++e) t[e] = s[e];
+            }
+            for (int e = 0; e < NEQ; ++e) q[e][r] = t[e];
+            if (havePrim) for (int e = 0; e < NEQ; ++e) bc_q[e][f] = pr[e];
+        }
+    }
+
+    // NsCalcBoundary, codes/ns/src/NsSolverImp.cpp:90-97
+    void calcBoundary() {
+        calcT(0, nCells);
+        calcVisl(0, nCells);
+        calcBc();
+        calcT(nCells, nT);
+        calcVisl(nCells, nT);
+    }
+
+    void initFlowfield() {
+        initReference();
+        outerSteps = 0;
+        for (int e = 0; e < NEQ; ++e) std::fill(q[e].begin(), q[e].end(), inflow[e]);
+        calcBoundary();
+    }
+
+    // ======================= CALC_TIME_STEP =======================
+    // TimeStep::CalcCfl, codes/ns/src/TimeStep.cpp:43-59
+    void calcCfl(long iter) {
+        cfl = p.cfled;
+        if (iter < p.ncfl) {
+            double delta = (p.cfled - p.cflst) / p.ncfl;
+            cfl = p.cflst + delta * iter;
+        }
+    }
+    // TimeStep::CalcFaceInvSpec, codes/ns/src/TimeStep.cpp:61-88
+    double faceInvSpec(int f) const {
+        int l = lc[f], r = rc[f];
+        double g1 = p.gama_ref, g2 = p.gama_ref;
+        double rl = q[IR][l], ul = q[IU][l], vl = q[IV][l], wl = q[IW][l], pl = q[IP][l];
+        double rr = q[IR][r], ur = q[IU][r], vr = q[IV][r], wr = q[IW][r], pr = q[IP][r];
+        double vnl = xfn[f] * ul + yfn[f] * vl + zfn[f] * wl - 0.0;
+        double vnr = xfn[f] * ur + yfn[f] * vr + zfn[f] * wr - 0.0;
+        double gama = half * (g1 + g2);
+        double pm = half * (pl + pr), rm = half * (rl + rr);
+        double cm = std::sqrt(gama * pm / rm);
+        double vn = half * (vnl + vnr);
+        return half * area[f] * (std::fabs(vn) + cm);
+    }
+    // TimeStep::CalcFaceVisSpec, codes/ns/src/TimeStep.cpp:90-122
+    double faceVisSpec(int f) const {
+        int l = lc[f], r = rc[f];
+        double vl_ = half * (visl[l] + visl[r]), vt_ = half * (vist[l] + vist[r]);
+        double gama = half * (p.gama_ref + p.gama_ref);
+        if (p.visSRModel == 1) {
+            double density = half * (q[IR][l] + q[IR][r]);
+            double c1 = 4.0 / 3.0 * (vl_ + vt_);
+            double c2 = gama * (vl_ * oprl + vt_ * oprt);
+            double c3 = 2.0 * MAXd(c1, c2) / (p.reynolds * density);
+            return area[f] * area[f] * c3;
+        } else if (p.visSRModel == 2) {
+            double dist = std::fabs(xfn[f] * (xcc[r] - xcc[l]) + yfn[f] * (ycc[r] - ycc[l]) + zfn[f] * (zcc[r] - zcc[l]));
+            double viscosity = vl_ + vt_;
+            double density = half * (q[IR][l] + q[IR][r]);
+            double c1 = 2.0 * viscosity / (density * dist * p.reynolds + SMALL);
+            return half * c1 * area[f];
+        } else if (p.visSRModel == 3) {
+            double density = half * (q[IR][l] + q[IR][r]);
+            return area[f] * area[f] / (p.reynolds * density + SMALL);
+        }
+        return 0.0;
+    }
+    // UTimeStep::CalcTimeStep, codes/uns/src/UTimeStep.cpp:190-416
+    void calcTimeStep() {
+        calcCfl(outerSteps);
+        std::fill(invsr.begin(), invsr.begin() + nCells, 0.0);
+        for (int f = 0; f < nFaces; ++f) {
+            double s = faceInvSpec(f);
+            invsr[lc[f]] += s; invsr[rc[f]] += s;
+        }
+        std::fill(vissr.begin(), vissr.begin() + nCells, 0.0);
+        if (p.vismodel > 0) {
+            for (int f = 0; f < nFaces; ++f) {
+                double s = faceVisSpec(f);
+                vissr[lc[f]] += s; vissr[rc[f]] += s;
+            }
+        }
+        if (p.timestepModel == 1) {
+            for (int c = 0; c < nCells; ++c) timestep[c] = p.global_dt;
+            return;
+        }
+        for (int c = 0; c < nCells; ++c) timestep[c] = cfl * vol[c] / invsr[c];
+        if (p.vismodel > 0 && p.visTimeStepModel > 0) {
+            for (int c = 0; c < nCells; ++c) {
+                double vts = cfl * vol[c] / vissr[c];
+                timestep[c] *= vts / (timestep[c] + vts);
+            }
+        }
+        double minTs = LARGE;
+        for (int c = 0; c < nCells; ++c) minTs = MINd(timestep[c], minTs);
+        if (p.max_time_ratio > 0) {
+            double mx = p.max_time_ratio * minTs;
+            for (int c = 0; c < nCells; ++c) timestep[c] = MINd(timestep[c], mx);
+        }
+        if (p.timestepModel == 2) {
+            for (int c = 0; c < nCells; ++c) timestep[c] = minTs;
+        }
+    }
+
+    // ======================= gradients =======================
+    // CalcGradGGCellWeight, codes/usolver/src/UGrad.cpp:88-149
+    void gradGG(const std::vector<double> &v, std::vector<double> &gx, std::vector<double> &gy, std::vector<double> &gz) {
+        std::fill(gx.begin(), gx.end(), 0.0); std::fill(gy.begin(), gy.end(), 0.0); std::fill(gz.begin(), gz.end(), 0.0);
+        for (int f = 0; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            double value;
+            if (p.igrad == 1) {
+                value = half * (v[l] + v[r]);   // CalcGrad, UGrad.cpp:40-86
+            } else {
+                double dxl = xfc[f] - xcc[l], dyl = yfc[f] - ycc[l], dzl = zfc[f] - zcc[l];
+                double dxr = xfc[f] - xcc[r], dyr = yfc[f] - ycc[r], dzr = zfc[f] - zcc[r];
+                double delt1 = DIST3(dxl, dyl, dzl), delt2 = DIST3(dxr, dyr, dzr);
+                double delta = 1.0 / (delt1 + delt2 + SMALL);
+                double cl = delt2 * delta, cr = delt1 * delta;
+                value = cl * v[l] + cr * v[r];
+            }
+            double fnxa = xfn[f] * area[f], fnya = yfn[f] * area[f], fnza = zfn[f] * area[f];
+            gx[l] += fnxa * value; gy[l] += fnya * value; gz[l] += fnza * value;
+            if (f < nBFaces) continue;
+            gx[r] -= fnxa * value; gy[r] -= fnya * value; gz[r] -= fnza * value;
+        }
+        for (int c = 0; c < nCells; ++c) {
+            double ov = 1.0 / vol[c];
+            gx[c] *= ov; gy[c] *= ov; gz[c] *= ov;
+        }
+        for (int f = 0; f < nBFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            gx[r] = gx[l]; gy[r] = gy[l]; gz[r] = gz[l];
+        }
+    }
+
+    // Weighted least squares (new: no reference implementation).  Weights
+    // 1/|d|^2 over the face neighbours (ghosts included), solved per cell with
+    // the 3x3 normal equations (2x2 in 2D).
+    void gradLSQ(const std::vector<double> &v, std::vector<double> &gx, std::vector<double> &gy, std::vector<double> &gz) {
+        for (int c = 0; c < nCells; ++c) {
+            double a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, b1 = 0, b2 = 0, b3 = 0;
+            for (int f : c2f[c]) {
+                int nb = lc[f] == c ? rc[f] : lc[f];
+                double dx = xcc[nb] - xcc[c], dy = ycc[nb] - ycc[c], dz = zcc[nb] - zcc[c];
+                double w = 1.0 / (dx * dx + dy * dy + dz * dz);
+                double dv = v[nb] - v[c];
+                a11 += w * dx * dx; a12 += w * dx * dy; a13 += w * dx * dz;
+                a22 += w * dy * dy; a23 += w * dy * dz; a33 += w * dz * dz;
+                b1 += w * dx * dv; b2 += w * dy * dv; b3 += w * dz * dv;
+            }
+            if (p.dimension == 2) {
+                double det = a11 * a22 - a12 * a12;
+                double id = 1.0 / det;
+                gx[c] = (a22 * b1 - a12 * b2) * id;
+                gy[c] = (a11 * b2 - a12 * b1) * id;
+                gz[c] = 0.0;
+            } else {
+                double c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
+                double c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
+                double det = a11 * c11 + a12 * c12 + a13 * c13;
+                double id = 1.0 / det;
+                gx[c] = (c11 * b1 + c12 * b2 + c13 * b3) * id;
+                gy[c] = (c12 * b1 + c22 * b2 + c23 * b3) * id;
+                gz[c] = (c13 * b1 + c23 * b2 + c33 * b3) * id;
+            }
+        }
+        for (int f = 0; f < nBFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            gx[r] = gx[l]; gy[r] = gy[l]; gz[r] = gz[l];
+        }
+    }
+
+    void grad(const std::vector<double> &v, std::vector<double> &gx, std::vector<double> &gy, std::vector<double> &gz) {
+        if (p.igrad == 2) gradLSQ(v, gx, gy, gz); else gradGG(v, gx, gy, gz);
+    }
+
+    // ======================= limiter =======================
+    // codes/usolver/src/ULimiter.cpp:35-97 (functions), :377-644 (drivers)
+    static double barthFunction(double dqv, double minv, double maxv, double dot) {
+        if (dot < 0.0) return 0.0;
+        else if (dqv > maxv) return maxv / dqv;
+        else if (dqv < minv) return minv / dqv;
+        return 1.0;
+    }
+    static double vencat(double x, double y, double eps) {
+        double x2 = x * x, xy = x * y, y2 = y * y, cc = 2.0;
+        return ((x2 + eps + cc * xy) / (x2 + cc * y2 + xy + eps));
+    }
+    static double vencatFunction(double dqv, double minv, double maxv, double eps) {
+        if (dqv > SMALL) return vencat(maxv, dqv, eps);
+        else if (dqv < -SMALL) return vencat(minv, dqv, eps);
+        return 1.0;
+    }
+    void calcLimiter(int e) {
+        std::vector<double> &lim = limiter[e];
+        const std::vector<double> &v = q[e];
+        std::fill(lim.begin(), lim.end(), 1.0);
+        if (p.ilim == -1) {
+            for (int f = 0; f < nFaces; ++f) { lim[lc[f]] = 0.0; lim[rc[f]] = 0.0; }
+            return;
+        }
+        if (p.ilim == 0) return;  // the no-limiter loop writes 1.0 everywhere
+        std::vector<double> minv(nT, 0.0), maxv(nT, 0.0);
+        for (int c = 0; c < nCells; ++c) { minv[c] = v[c]; maxv[c] = v[c]; }
+        for (int f = nBFaces; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            minv[l] = MINd(minv[l], v[r]); maxv[l] = MAXd(maxv[l], v[r]);
+            minv[r] = MINd(minv[r], v[l]); maxv[r] = MAXd(maxv[r], v[l]);
+        }
+        for (int c = 0; c < nCells; ++c) { minv[c] -= v[c]; maxv[c] -= v[c]; }
+        double qmin = LARGE, qmax = -LARGE;
+        for (int c = 0; c < nCells; ++c) { qmin = MINd(qmin, minv[c]); qmax = MAXd(qmax, maxv[c]); }
+        double eps = p.vencat_coef * MAXd(qmax - qmin, 1.0);
+        double epsg = eps * eps + SMALL;
+        for (int f = 0; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            double dx1 = xfc[f] - xcc[l], dy1 = yfc[f] - ycc[l], dz1 = zfc[f] - zcc[l];
+            double dq1 = dqdx[e][l] * dx1 + dqdy[e][l] * dy1 + dqdz[e][l] * dz1;
+            double dx2 = xfc[f] - xcc[r], dy2 = yfc[f] - ycc[r], dz2 = zfc[f] - zcc[r];
+            double dq2 = dqdx[e][r] * dx2 + dqdy[e][r] * dy2 + dqdz[e][r] * dz2;
+            double l1, l2;
+            if (p.ilim == 1) {
+                double ds1 = DIST3(dx1, dy1, dz1);
+                double dot1 = (xfn[f] * dx1 + yfn[f] * dy1 + zfn[f] * dz1) / (ds1 + SMALL);
+                l1 = barthFunction(dq1, minv[l], maxv[l], dot1);
+                double ds2 = DIST3(dx2, dy2, dz2);
+                double dot2 = -(xfn[f] * dx2 + yfn[f] * dy2 + zfn[f] * dz2) / (ds2 + SMALL);
+                l2 = barthFunction(dq2, minv[r], maxv[r], dot2);
+            } else {
+                double e1 = epsg, e2 = epsg;
+                if (p.venkat_kh3) {
+                    // eps^2 = (K h)^3, h = cell size (new option; no reference form)
+                    double h1 = p.dimension == 2 ? std::sqrt(vol[l]) : std::cbrt(vol[l]);
+                    double h2 = p.dimension == 2 ? std::sqrt(vol[r]) : std::cbrt(vol[r]);
+                    double k1 = p.vencat_coef * h1, k2 = p.vencat_coef * h2;
+                    e1 = k1 * k1 * k1 + SMALL; e2 = k2 * k2 * k2 + SMALL;
+                }
+                l1 = vencatFunction(dq1, minv[l], maxv[l], e1);
+                l2 = vencatFunction(dq2, minv[r], maxv[r], e2);
+            }
+            lim[l] = MINd(lim[l], l1);
+            lim[r] = MINd(lim[r], l2);
+        }
+    }
+
+    // ======================= inviscid flux =======================
+    // NsInvFlux::Roe, codes/ns/src/NsInvFlux.cpp:186-308
+    void roe(const double *p1, const double *p2, double xn, double yn, double zn, double *flux) const {
+        const double vfn = 0.0, g1 = p.gama_ref, g2 = p.gama_ref;
+        double rl = p1[IR], ul = p1[IU], vl = p1[IV], wl = p1[IW], pl = p1[IP];
+        double rr = p2[IR], ur = p2[IU], vr = p2[IV], wr = p2[IW], pr = p2[IP];
+        double v2l = SQR3(ul, vl, wl), v2r = SQR3(ur, vr, wr);
+        double hl = (g1 / (g1 - 1.0)) * (pl / rl) + half * v2l;
+        double hr = (g2 / (g2 - 1.0)) * (pr / rr) + half * v2r;
+        double vnl = xn * ul + yn * vl + zn * wl - vfn;
+        double vnr = xn * ur + yn * vr + zn * wr - vfn;
+        double rvnl = rl * vnl, rvnr = rr * vnr;
+        double ratio = std::sqrt(rr / rl);
+        double coef = 1.0 / (1.0 + ratio);
+        double rm = std::sqrt(rl * rr);
+        double um = (ul + ur * ratio) * coef;
+        double vm = (vl + vr * ratio) * coef;
+        double wm = (wl + wr * ratio) * coef;
+        double hm = (hl + hr * ratio) * coef;
+        double pm = (pl + pr * ratio) * coef;
+        double gama = (g1 + g2 * ratio) * coef;
+        double v2 = SQR3(um, vm, wm);
+        double vnflow = xn * um + yn * vm + zn * wm;
+        double vnrel = vnflow - vfn;
+        double gamm1 = gama - 1.0;
+        double c2 = gamm1 * (hm - half * v2);
+        double cm = std::sqrt(std::fabs(c2));
+        double aeig1 = std::fabs(vnrel), aeig2 = std::fabs(vnrel + cm), aeig3 = std::fabs(vnrel - cm);
+        double f1[NEQ], f2[NEQ];
+        f1[0] = rvnl; f1[1] = rvnl * ul + xn * pl; f1[2] = rvnl * vl + yn * pl; f1[3] = rvnl * wl + zn * pl; f1[4] = rvnl * hl + vfn * pl;
+        f2[0] = rvnr; f2[1] = rvnr * ur + xn * pr; f2[2] = rvnr * vr + yn * pr; f2[3] = rvnr * wr + zn * pr; f2[4] = rvnr * hr + vfn * pr;
+        for (int e = 0; e < NEQ; ++e) flux[e] = f1[e] + f2[e];
+        double q1[NEQ], q2[NEQ], dqv[NEQ];
+        primToQ(p1, g1, q1); primToQ(p2, g2, q2);
+        for (int e = 0; e < NEQ; ++e) dqv[e] = q2[e] - q1[e];
+        double meig1 = aeig1, meig2 = aeig2, meig3 = aeig3;
+        if (p.ieigenfix == 1) {  // ModifyAbsoluteEigenvalue, :167-184
+            double mx = MAXd(aeig2, aeig3);
+            double m1 = mx * p.centropy1, m2 = mx * p.centropy2;
+            meig1 = MAXd(m1, aeig1); meig2 = MAXd(m2, aeig2); meig3 = MAXd(m2, aeig3);
+        }
+        double xi1 = (2.0 * meig1 - meig2 - meig3) / (2.0 * c2);
+        double xi2 = (meig2 - meig3) / (2.0 * cm);
+        double dc = vnflow * dqv[0] - xn * dqv[1] - yn * dqv[2] - zn * dqv[3];
+        double c2dc = c2 * dc;
+        // CalcTotalEnthalpyChange, :1334-1353
+        double ae = gama - 1.0, af = half * ae * v2;
+        double dh = -ae * (um * dqv[1] + vm * dqv[2] + wm * dqv[3] - dqv[4]);
+        dh += af * dqv[0];
+        double term1 = dh * xi1 + dc * xi2;
+        double term2 = c2dc * xi1 + dh * xi2;
+        flux[0] -= (meig1 * dqv[0] - term1);
+        flux[1] -= (meig1 * dqv[1] - um * term1 + xn * term2);
+        flux[2] -= (meig1 * dqv[2] - vm * term1 + yn * term2);
+        flux[3] -= (meig1 * dqv[3] - wm * term1 + zn * term2);
+        flux[4] -= (meig1 * dqv[4] - hm * term1 + vnflow * term2);
+        for (int e = 0; e < NEQ; ++e) flux[e] *= half;
+        (void)rm; (void)pm;
+    }
+    static void primToQ(const double *pr, double gama, double *qq) {
+        double v2 = SQR3(pr[IU], pr[IV], pr[IW]);
+        double em = (pr[IP] / pr[IR]) / (gama - 1.0) + half * v2;
+        qq[0] = pr[IR]; qq[1] = pr[IR] * pr[IU]; qq[2] = pr[IR] * pr[IV]; qq[3] = pr[IR] * pr[IW]; qq[4] = pr[IR] * em;
+    }
+    static double fmSplit2(double mach, double ipn) { return ipn * fourth * (mach + ipn) * (mach + ipn); }
+    static double fpSplit5(double mach, double alpha, double ipn) {
+        double macha = std::fabs(mach);
+        if (macha >= 1.0) return half * (1.0 + ipn * mach / (macha + SMALL));
+        return fmSplit2(mach, ipn) * ((2.0 * ipn - mach) - ipn * 16.0 * alpha * mach * fmSplit2(mach, -ipn));
+    }
+    // NsInvFlux::Slau2, codes/ns/src/NsInvFlux.cpp:1246-1314
+    void slau2(const double *p1, const double *p2, double xn, double yn, double zn, double *flux) const {
+        const double vfn = 0.0, g1 = p.gama_ref, g2 = p.gama_ref;
+        double rl = p1[IR], ul = p1[IU], vl = p1[IV], wl = p1[IW], pl = p1[IP];
+        double rr = p2[IR], ur = p2[IU], vr = p2[IV], wr = p2[IW], pr = p2[IP];
+        double v2l = SQR3(ul, vl, wl), v2r = SQR3(ur, vr, wr);
+        double hl = (g1 / (g1 - 1.0)) * (pl / rl) + half * v2l;
+        double hr = (g2 / (g2 - 1.0)) * (pr / rr) + half * v2r;
+        double vnl = xn * ul + yn * vl + zn * wl - vfn;
+        double vnr = xn * ur + yn * vr + zn * wr - vfn;
+        double orl = 1.0 / (rl + SMALL), orr = 1.0 / (rr + SMALL);
+        double c2l = g1 * pl * orl, c2r = g2 * pr * orr;
+        double cl = std::sqrt(c2l), cr = std::sqrt(c2r);
+        double cm = half * (cl + cr);
+        double t = rr / rl;
+        double vna = (std::fabs(vnl) + t * std::fabs(vnr)) / (1 + t);
+        double ml = vnl / cm, mr = vnr / cm;
+        double g = -MAXd(MINd(ml, 0.0), -1.0) * MINd(MAXd(mr, 0.0), 1.0);
+        double vnp = (1 - g) * vna + g * std::fabs(vnl);
+        double vnn = (1 - g) * vna + g * std::fabs(vnr);
+        double va = std::sqrt(half * (v2l + v2r));
+        double m12 = MINd(1.0, va / cm);
+        double ka = (1 - m12) * (1 - m12);
+        double ms = half * (rl * (vnl + vnp) + rr * (vnr - vnn) - ka * (pr - pl) / cm);
+        double fp5ml = fpSplit5(ml, 0.0, 1.0);
+        double fp5mr = fpSplit5(mr, 0.0, -1.0);
+        double ps = 0;
+        ps += half * (pl + pr);
+        ps += half * (fp5ml - fp5mr) * (pl - pr);
+        ps += va * (fp5ml + fp5mr - 1) * std::sqrt(rl * rr) * cm;
+        double mp = half * (ms + std::fabs(ms)), mn = half * (ms - std::fabs(ms));
+        flux[0] = (mp + mn);
+        flux[1] = (mp * ul + mn * ur) + xn * ps;
+        flux[2] = (mp * vl + mn * vr) + yn * ps;
+        flux[3] = (mp * wl + mn * wr) + zn * ps;
+        flux[4] = (mp * hl + mn * hr) + vfn * ps;
+    }
+
+    // UNsInvFlux::CalcFlux, codes/uns/src/UNsInvFlux.cpp:123-215
+    void invFlux() {
+        bool second = p.ilim != -1;
+        if (second) {
+            for (int e = 0; e < NEQ; ++e) grad(q[e], dqdx[e], dqdy[e], dqdz[e]);
+            for (int e = 0; e < NEQ; ++e) calcLimiter(e);
+        } else {
+            // first order: gradients are still computed by the reference, but the
+            // zero limiter multiplies them away exactly; keep them for downloads
+            for (int e = 0; e < NEQ; ++e) grad(q[e], dqdx[e], dqdy[e], dqdz[e]);
+            for (int e = 0; e < NEQ; ++e) calcLimiter(e);
+        }
+        std::vector<double> qf1(NEQ * (size_t)nFaces), qf2(NEQ * (size_t)nFaces);
+        // GetQlQr + CalcFaceValue, codes/usolver/src/ULimiter.cpp:131-256
+        for (int f = 0; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            double t1[NEQ], t2[NEQ];
+            double dx = xfc[f] - xcc[l], dy = yfc[f] - ycc[l], dz = zfc[f] - zcc[l];
+            for (int e = 0; e < NEQ; ++e) {
+                double phi = MINd(limiter[e][l], limiter[e][r]);
+                t1[e] = q[e][l] + phi * (dqdx[e][l] * dx + dqdy[e][l] * dy + dqdz[e][l] * dz);
+            }
+            bool ok1 = !(t1[IR] <= 0.0 || t1[IP] <= 0.0);
+            dx = xfc[f] - xcc[r]; dy = yfc[f] - ycc[r]; dz = zfc[f] - zcc[r];
+            for (int e = 0; e < NEQ; ++e) {
+                double phi = MINd(limiter[e][r], limiter[e][l]);
+                t2[e] = q[e][r] + phi * (dqdx[e][r] * dx + dqdy[e][r] * dy + dqdz[e][r] * dz);
+            }
+            bool ok2 = !(t2[IR] <= 0.0 || t2[IP] <= 0.0);
+            for (int e = 0; e < NEQ; ++e) {
+                qf1[e * (size_t)nFaces + f] = ok1 ? t1[e] : q[e][l];
+                qf2[e * (size_t)nFaces + f] = ok2 ? t2[e] : q[e][r];
+            }
+        }
+        // NsLimField::BcQlQrFix, codes/uns/src/UNsLimiter.cpp:67-101
+        for (int f = 0; f < nBFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            for (int e = 0; e < NEQ; ++e) {
+                double tmp = half * (q[e][l] + q[e][r]);
+                qf1[e * (size_t)nFaces + f] = tmp; qf2[e * (size_t)nFaces + f] = tmp;
+            }
+            if (bcType[f] == OFG_BC_SOLID_SURFACE)
+                for (int e = 0; e < NEQ; ++e) { qf1[e * (size_t)nFaces + f] = bc_q[e][f]; qf2[e * (size_t)nFaces + f] = bc_q[e][f]; }
+        }
+        // CalcInvFlux + AddInvFlux (AddF2CField, codes/usolver/src/UCom.cpp:144-171)
+        for (int f = 0; f < nFaces; ++f) {
+            double p1[NEQ], p2[NEQ], fl[NEQ];
+            for (int e = 0; e < NEQ; ++e) { p1[e] = qf1[e * (size_t)nFaces + f]; p2[e] = qf2[e * (size_t)nFaces + f]; }
+            if (p.ischeme == 12) slau2(p1, p2, xfn[f], yfn[f], zfn[f], fl);
+            else roe(p1, p2, xfn[f], yfn[f], zfn[f], fl);
+            for (int e = 0; e < NEQ; ++e) {
+                double v = area[f] * fl[e];
+                res[e][lc[f]] -= v;
+                if (f >= nBFaces) res[e][rc[f]] += v;
+            }
+        }
+    }
+
+    // ======================= viscous flux (STD) =======================
+    // UNsVisFlux::CalcFlux (codes/uns/src/UNsVisFlux.cpp:90-440) with the
+    // VIS_STD face gradient (codes/usolver/src/VisGrad.cpp:150-175,356-366)
+    void visFlux() {
+        if (p.vismodel == 0) return;
+        gradGG(tempr, dtdx, dtdy, dtdz);
+        for (int f = 0; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            double vl1 = visl[l], vl2 = visl[r], vt1 = vist[l], vt2 = vist[r];
+            double vlm = half * (vl1 + vl2), vtm = half * (vt1 + vt2);
+            double vis = vlm + vtm;
+            double dx = xcc[r] - xcc[l], dy = ycc[r] - ycc[l], dz = zcc[r] - zcc[l];
+            double ods = 1.0 / DIST3(dx, dy, dz);
+            dx *= ods; dy *= ods; dz *= ods;
+            double gx[6], gy[6], gz[6], qm[6];
+            for (int e = 0; e < 6; ++e) {
+                double q1 = e < NEQ ? q[e][l] : tempr[l];
+                double q2 = e < NEQ ? q[e][r] : tempr[r];
+                double ax1 = e < NEQ ? dqdx[e][l] : dtdx[l], ay1 = e < NEQ ? dqdy[e][l] : dtdy[l], az1 = e < NEQ ? dqdz[e][l] : dtdz[l];
+                double ax2 = e < NEQ ? dqdx[e][r] : dtdx[r], ay2 = e < NEQ ? dqdy[e][r] : dtdy[r], az2 = e < NEQ ? dqdz[e][r] : dtdz[r];
+                qm[e] = half * (q1 + q2);
+                gx[e] = half * (ax1 + ax2); gy[e] = half * (ay1 + ay2); gz[e] = half * (az1 + az2);
+                // CorrectGrad, VisGrad.cpp:356-366
+                double fOld = gx[e] * dx + gy[e] * dy + gz[e] * dz;
+                double fnew = (q2 - q1) * ods;
+                double df = fnew - fOld;
+                gx[e] += df * dx; gy[e] += df * dy; gz[e] += df * dz;
+            }
+            double xn = xfn[f], yn = yfn[f], zn = zfn[f];
+            double dtdn = xn * gx[5] + yn * gy[5] + zn * gz[5];
+            double kcp = (vlm * oprl + vtm * oprt) * const_cp;
+            double qNormal = 0.0;
+            qNormal += xn * 0.0 + yn * 0.0 + zn * 0.0;
+            qNormal += kcp * dtdn;
+            double dudx = gx[IU], dudy = gy[IU], dudz = gz[IU];
+            double dvdx = gx[IV], dvdy = gy[IV], dvdz = gz[IV];
+            double dwdx = gx[IW], dwdy = gy[IW], dwdz = gz[IW];
+            double divv2p3 = two3rd * (dudx + dvdy + dwdz);
+            double txx = vis * (2.0 * dudx - divv2p3);
+            double tyy = vis * (2.0 * dvdy - divv2p3);
+            double tzz = vis * (2.0 * dwdz - divv2p3);
+            double txy = vis * (dudy + dvdx);
+            double txz = vis * (dudz + dwdx);
+            double tyz = vis * (dvdz + dwdy);
+            double fv[NEQ];
+            fv[0] = 0.0;
+            fv[1] = xn * txx + yn * txy + zn * txz;
+            fv[2] = xn * txy + yn * tyy + zn * tyz;
+            fv[3] = xn * txz + yn * tyz + zn * tzz;
+            fv[4] = qm[IU] * fv[1] + qm[IV] * fv[2] + qm[IW] * fv[3] + qNormal;
+            double coeff = -oreynolds * area[f];
+            for (int e = 0; e < NEQ; ++e) {
+                double v = coeff * fv[e];
+                res[e][l] -= v;
+                if (f >= nBFaces) res[e][r] += v;
+            }
+        }
+    }
+
+    void loadResiduals() {  // LoadResiduals: res = -rhs, rhs = 0
+        for (int e = 0; e < NEQ; ++e) std::fill(res[e].begin(), res[e].end(), -0.0);
+    }
+    void updateResiduals() { invFlux(); visFlux(); }
+
+    // ======================= LU-SGS =======================
+    // UNsSpectrum::CalcImplicitSpectrum, codes/uns/src/UNsSpectrum.cpp:52-94
+    void calcImplicitSpectrum() {
+        for (int c = 0; c < nCells; ++c) impsr[c] = (1.0 / timestep[c]) * vol[c];
+        for (int c = 0; c < nCells; ++c) impsr[c] += invsr[c];
+        for (int c = 0; c < nCells; ++c) impsr[c] += vissr[c];
+    }
+
+    // per-face increment: UNsLusgs::Solve (codes/uns/src/UNsLusgs.cpp:193-208),
+    // PrepareDataFacePrim (:251-293), NsLusgs::GetStandardFluxIncrement
+    // (codes/ns/src/NsLusgs.cpp:121-202), UNsLusgs::CalcViscousTerm (:295-330).
+    // ci = the cell being solved, f its face; adds into rhs0.
+    void faceIncrement(int ci, int f, double *rhs0) const {
+        int l = lc[f], r = rc[f];
+        double xn = xfn[f], yn = yfn[f], zn = zfn[f], vfn = 0.0, fa = area[f];
+        if (r == ci) { std::swap(l, r); xn = -xn; yn = -yn; zn = -zn; vfn = -vfn; }
+        double gl = p.gama_ref, gr = p.gama_ref;
+        double rl = q[IR][l], ul = q[IU][l], vl = q[IV][l], wl = q[IW][l], pl = q[IP][l];
+        double rr = q[IR][r], ur = q[IU][r], vr = q[IV][r], wr = q[IW][r], pr = q[IP][r];
+        double hl = gl / (gl - 1.0) * pl / rl + half * SQR3(ul, vl, wl);
+        double hr = gr / (gr - 1.0) * pr / rr + half * SQR3(ur, vr, wr);
+        double tmp0 = std::sqrt(rr / rl);
+        double tmp1 = 1.0 / (1.0 + tmp0);
+        double rm = std::sqrt(rr * rl);
+        double um = (ul + ur * tmp0) * tmp1;
+        double vm = (vl + vr * tmp0) * tmp1;
+        double wm = (wl + wr * tmp0) * tmp1;
+        double hm = (hl + hr * tmp0) * tmp1;
+        double pm = rm * (hm - half * SQR3(um, vm, wm)) * (gl - 1.0) / gl;
+        double gama = gr;
+        // CalcFaceEigenValue (primF)
+        double c2f_ = std::fabs(gama * pm / rm);
+        double cmf = std::sqrt(c2f_);
+        double vnf = xn * um + yn * vm + zn * wm;
+        double maxEig = std::fabs(vnf - vfn) + cmf;
+        // neighbour state
+        double dqj[NEQ];
+        for (int e = 0; e < NEQ; ++e) dqj[e] = dq[e][r];
+        double rj = q[IR][r], uj = q[IU][r], vj = q[IV][r], wj = q[IW][r], pj = q[IP][r];
+        double c2 = std::fabs(gama * pj / rj);
+        double cm = std::sqrt(c2);
+        double vn_fluid = xn * uj + yn * vj + zn * wj;
+        double vn_rel = vn_fluid - vfn;
+        double lmd1 = vn_rel, lmd2 = vn_rel + cm, lmd3 = vn_rel - cm;
+        lmd1 = half * (lmd1 + (-1) * maxEig);
+        lmd2 = half * (lmd2 + (-1) * maxEig);
+        lmd3 = half * (lmd3 + (-1) * maxEig);
+        double x1 = (lmd1 + lmd1 - lmd2 - lmd3) / (c2 + c2);
+        double x2 = (lmd2 - lmd3) / (cm + cm);
+        double dc = vn_fluid * dqj[0] - xn * dqj[1] - yn * dqj[2] - zn * dqj[3];
+        double c2dc = c2 * dc;
+        // CalcDH, codes/ns/src/NsLusgs.cpp:348-366
+        double v2 = SQR3(uj, vj, wj);
+        double ae = gama - 1.0, af = half * ae * v2;
+        double dh = -ae * (uj * dqj[1] + vj * dqj[2] + wj * dqj[3] - dqj[4]);
+        double enthalpy = (gama / (gama - 1.0)) * (pj / rj);
+        dh += af * dqj[0];
+        double htot = enthalpy + half * v2;
+        double term1 = dh * x1 + dc * x2;
+        double term2 = c2dc * x1 + dh * x2;
+        double dfj[NEQ];
+        dfj[0] = lmd1 * dqj[0] - term1;
+        dfj[1] = lmd1 * dqj[1] - uj * term1 + xn * term2;
+        dfj[2] = lmd1 * dqj[2] - vj * term1 + yn * term2;
+        dfj[3] = lmd1 * dqj[3] - wj * term1 + zn * term2;
+        dfj[4] = lmd1 * dqj[4] - htot * term1 + vn_fluid * term2;
+        for (int e = 0; e < NEQ; ++e) dfj[e] *= fa;
+        if (p.vismodel > 0) {
+            double visrad;
+            double vl_ = visl[r], vt_ = vist[r];
+            if (p.visSRModel == 1) {
+                double density = half * (q[IR][l] + q[IR][r]);
+                double c1 = 4.0 / 3.0 * (vl_ + vt_);
+                double cc2 = p.gama_ref * (vl_ * oprl + vt_ * oprt);
+                double c3 = 2.0 * MAXd(c1, cc2) / (p.reynolds * density);
+                visrad = fa * fa * c3 / vol[r];
+            } else {
+                double dist = std::fabs(xn * (xcc[r] - xcc[l]) + yn * (ycc[r] - ycc[l]) + zn * (zcc[r] - zcc[l]));
+                double viscosity = vl_ + vt_;
+                double density = half * (q[IR][l] + q[IR][r]);
+                double c1 = 2.0 * viscosity / (density * dist * p.reynolds + SMALL);
+                visrad = half * c1 * fa;
+            }
+            for (int e = 0; e < NEQ; ++e) rhs0[e] -= visrad * dqj[e];
+        }
+        for (int e = 0; e < NEQ; ++e) rhs0[e] += dfj[e];
+    }
+
+    // UNsLusgs::LowerSweep, codes/uns/src/UNsLusgs.cpp:75-108; NsLusgs::CalcLowerChange (:230-277)
+    void lusgsLower() {
+        calcImplicitSpectrum();
+        for (int c = 0; c < nCells; ++c) {
+            double rhs0[NEQ] = {0, 0, 0, 0, 0};
+            for (int f : c2f[c]) {
+                if (lc[f] > c || rc[f] > c) continue;
+                faceIncrement(c, f, rhs0);
+            }
+            for (int e = 0; e < NEQ; ++e) dq[e][c] = (res[e][c] - rhs0[e]) / impsr[c];
+        }
+    }
+    // UNsLusgs::UpperSweep, codes/uns/src/UNsLusgs.cpp:110-138; NsLusgs::CalcUpperChange (:279-326)
+    void lusgsUpper() {
+        calcImplicitSpectrum();
+        for (int c = nCells - 1; c >= 0; --c) {
+            double rhs0[NEQ] = {0, 0, 0, 0, 0};
+            for (int f : c2f[c]) {
+                if (lc[f] < c || rc[f] < c) continue;
+                faceIncrement(c, f, rhs0);
+            }
+            for (int e = 0; e < NEQ; ++e) dq[e][c] += (-rhs0[e]) / impsr[c];
+        }
+    }
+
+    // ======================= update =======================
+    // UNsUpdate::UpdateFlowField (codes/uns/src/UNsUpdate.cpp:46-146),
+    // NsUpdate::CalcFlowField / WeekSolutionFix (codes/ns/src/NsUpdate.cpp:40-67,192-217)
+    long nFixes = 0;
+    void updateFlowfield() {
+        double gama = p.gama_ref;
+        for (int c = 0; c < nCells; ++c) {
+            double prim0[NEQ], q0[NEQ], qq[NEQ], pr[NEQ], d[NEQ];
+            for (int e = 0; e < NEQ; ++e) { prim0[e] = q[e][c]; d[e] = dq[e][c]; }
+            primToQ(prim0, gama, q0);
+            for (int e = 0; e < NEQ; ++e) qq[e] = q0[e] + d[e];
+            // QToPrim, codes/ns/src/NsInvFlux.cpp:1377-1399
+            double density = std::fabs(qq[0]);
+            double rd = 1.0 / density;
+            double um = qq[1] * rd, vm = qq[2] * rd, wm = qq[3] * rd, rem = qq[4];
+            double v2 = SQR3(um, vm, wm);
+            double reint = rem - half * density * v2;
+            pr[0] = density; pr[1] = um; pr[2] = vm; pr[3] = wm; pr[4] = (gama - 1.0) * reint;
+            if (pr[IR] <= 0.0 || pr[IP] <= 0.0) {
+                ++nFixes;
+                bool ok = false;
+                const double coefs[3] = {0.5, 0.1, 0.01};
+                for (int k = 0; k < 3 && !ok; ++k) {
+                    for (int e = 0; e < NEQ; ++e) pr[e] += coefs[k] * d[e];
+                    if (!(pr[IR] < 0.0 || pr[IP] < 0.0)) ok = true;
+                }
+                if (!ok) {  // SolutionFix: neighbour average (in-place, natural order)
+                    double sumV = 0.0;
+                    for (int e = 0; e < NEQ; ++e) pr[e] = 0.0;
+                    for (int f : c2f[c]) {
+                        int nb = lc[f] == c ? rc[f] : lc[f];
+                        sumV += 1.0;
+                        for (int e = 0; e < NEQ; ++e) {
+                            double v = q[e][nb];
+                            if (e == IR || e == IP) v = std::fabs(v);
+                            pr[e] += v * 1.0;
+                        }
+                    }
+                    double rv = 1.0 / sumV;
+                    for (int e = 0; e < NEQ; ++e) pr[e] *= rv;
+                }
+            }
+            for (int e = 0; e < NEQ; ++e) q[e][c] = pr[e];
+        }
+    }
+
+    // ======================= residual norm =======================
+    void residualRms(double *rms, bool *nan) const {
+        *nan = false;
+        for (int e = 0; e < NEQ; ++e) {
+            double s = 0.0;
+            for (int c = 0; c < nCells; ++c) {
+                double r = res[e][c];
+                if (std::isnan(r)) *nan = true;
+                s += r * r;
+            }
+            rms[e] = std::sqrt(s / nCells);
+        }
+    }
+
+    // ======================= one outer iteration =======================
+    // TimeIntegral::Lusgs (codes/solver/src/TimeIntegral.cpp:113-130)
+    void nsRelax() {
+        for (int e = 0; e < NEQ; ++e) std::fill(dq[e].begin(), dq[e].end(), 0.0);
+        calcTimeStep();
+        loadResiduals();
+        updateResiduals();
+        lusgsLower();
+        lusgsUpper();
+        updateFlowfield();
+        calcBoundary();
+    }
+
+    int step(int n) {
+        for (int it = 0; it < n; ++it) {
+            ++outerSteps;
+            nsRelax();
+            double rms[NEQ]; bool nan;
+            residualRms(rms, &nan);
+            for (int e = 0; e < NEQ; ++e) resHist.push_back(rms[e]);
+            if (nan) { err = "NotANumber in residual"; return OFG_E_NAN; }
+        }
+        return 0;
+    }
+};
+
+// ============================ C interface ============================
+extern "C" {
+
+void *oro_create(const ofg_params *p) {
+    Oracle *o = new Oracle();
+    o->p = *p;
+    return o;
+}
+void oro_destroy(void *h) { delete (Oracle *)h; }
+
+int oro_set_mesh(void *h, int nn, const double *x, const double *y, const double *z, int nf, const int *fnc,
+                 const int *fn, const int *l, const int *r, int nc, int nb, const int *bct, const double *wd) {
+    return ((Oracle *)h)->setMesh(nn, x, y, z, nf, fnc, fn, l, r, nc, nb, bct, wd);
+}
+int oro_init_flowfield(void *h) { ((Oracle *)h)->initFlowfield(); return 0; }
+int oro_step(void *h, int n) { return ((Oracle *)h)->step(n); }
+
+// individual tasks (for per-kernel parity tests)
+int oro_task(void *h, const char *name) {
+    Oracle *o = (Oracle *)h;
+    std::string s(name);
+    if (s == "ZERO_DQ_FIELD") { for (int e = 0; e < NEQ; ++e) std::fill(o->dq[e].begin(), o->dq[e].end(), 0.0); }
+    else if (s == "CALC_TIME_STEP") o->calcTimeStep();
+    else if (s == "LOAD_RESIDUALS") o->loadResiduals();
+    else if (s == "UPDATE_RESIDUALS") o->updateResiduals();
+    else if (s == "LUSGS_LOWER_SWEEP") o->lusgsLower();
+    else if (s == "LUSGS_UPPER_SWEEP") o->lusgsUpper();
+    else if (s == "UPDATE_FLOWFIELD_LUSGS") o->updateFlowfield();
+    else if (s == "CALC_BOUNDARY") o->calcBoundary();
+    else if (s == "INIT_LUSGS") {}   // CLusgsInit: no-op (codes/implicit/src/ImplicitTaskReg.cpp:69-72)
+    else if (s == "NEXT_STEP") ++o->outerSteps;
+    else return OFG_E_ARG;
+    return 0;
+}
+
+// field access, reference layout
+int64_t oro_field(void *h, const char *name, double *out) {
+    Oracle *o = (Oracle *)h;
+    std::string s(name);
+    auto put = [&](const std::vector<double> *v, int ne, int64_t n) -> int64_t {
+        if (out) for (int e = 0; e < ne; ++e) std::copy(v[e].begin(), v[e].begin() + n, out + e * n);
+        return ne * n;
+    };
+    int64_t nT = o->nT, nF = o->nFaces;
+    if (s == "q") return put(o->q, NEQ, nT);
+    if (s == "dq") return put(o->dq, NEQ, nT);
+    if (s == "res") return put(o->res, NEQ, nT);
+    if (s == "dqdx") return put(o->dqdx, NEQ, nT);
+    if (s == "dqdy") return put(o->dqdy, NEQ, nT);
+    if (s == "dqdz") return put(o->dqdz, NEQ, nT);
+    if (s == "limiter") return put(o->limiter, NEQ, nT);
+    if (s == "timestep") return put(&o->timestep, 1, nT);
+    if (s == "invsr") return put(&o->invsr, 1, nT);
+    if (s == "vissr") return put(&o->vissr, 1, nT);
+    if (s == "impsr") return put(&o->impsr, 1, nT);
+    if (s == "tempr") return put(&o->tempr, 1, nT);
+    if (s == "visl") return put(&o->visl, 1, nT);
+    if (s == "vist") return put(&o->vist, 1, nT);
+    if (s == "vol") return put(&o->vol, 1, nT);
+    if (s == "xcc") return put(&o->xcc, 1, nT);
+    if (s == "ycc") return put(&o->ycc, 1, nT);
+    if (s == "zcc") return put(&o->zcc, 1, nT);
+    if (s == "area") return put(&o->area, 1, nF);
+    if (s == "xfn") return put(&o->xfn, 1, nF);
+    if (s == "yfn") return put(&o->yfn, 1, nF);
+    if (s == "zfn") return put(&o->zfn, 1, nF);
+    if (s == "xfc") return put(&o->xfc, 1, nF);
+    if (s == "yfc") return put(&o->yfc, 1, nF);
+    if (s == "zfc") return put(&o->zfc, 1, nF);
+    if (s == "reshist") { if (out) std::copy(o->resHist.begin(), o->resHist.end(), out); return (int64_t)o->resHist.size(); }
+    return -1;
+}
+int oro_set_q(void *h, const double *qin) {
+    Oracle *o = (Oracle *)h;
+    for (int e = 0; e < NEQ; ++e) std::copy(qin + e * (int64_t)o->nT, qin + (e + 1) * (int64_t)o->nT, o->q[e].begin());
+    o->initReference();
+    o->calcBoundary();
+    return 0;
+}
+long oro_outer_steps(void *h) { return ((Oracle *)h)->outerSteps; }
+
+}  // extern "C"

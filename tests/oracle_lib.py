@@ -1,0 +1,123 @@
+"""ctypes access to the CPU oracle (oracle/liboforacle.so) and a runner for
+the reference-built oracle (oracle/_ref/oneflow_ref).  Test infrastructure."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import shutil
+import subprocess
+import tempfile
+
+import numpy as np
+
+from oneflow_b200 import params as P
+from oneflow_b200.meshio import Mesh, read_ref_dump, read_res_dat, write_case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboforacle.so")
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "oneflow_ref")
+
+_dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+def _load():
+    if not os.path.exists(ORACLE_SO):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboforacle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    lib = C.CDLL(ORACLE_SO)
+    lib.oro_create.restype = C.c_void_p
+    lib.oro_create.argtypes = [C.POINTER(P.OfgParams)]
+    lib.oro_destroy.argtypes = [C.c_void_p]
+    lib.oro_set_mesh.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_int, _ip, _ip, _ip, _ip, C.c_int, C.c_int,
+                                 _ip, C.c_void_p]
+    lib.oro_init_flowfield.argtypes = [C.c_void_p]
+    lib.oro_step.argtypes = [C.c_void_p, C.c_int]
+    lib.oro_task.argtypes = [C.c_void_p, C.c_char_p]
+    lib.oro_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+    lib.oro_field.restype = C.c_int64
+    lib.oro_set_q.argtypes = [C.c_void_p, _dp]
+    lib.oro_outer_steps.argtypes = [C.c_void_p]
+    lib.oro_outer_steps.restype = C.c_long
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = _load()
+    return _LIB
+
+
+class Oracle:
+    """One CPU solve: mirrors the reference's task sequence in FP64."""
+
+    def __init__(self, mesh: Mesh, params: P.OfgParams):
+        self.L = lib()
+        self.mesh = mesh
+        self.params = params
+        self.h = self.L.oro_create(C.byref(params))
+        a = mesh.as_arrays()
+        wd = None if a["wd"] is None else a["wd"].ctypes.data_as(C.c_void_p)
+        self._wd = a["wd"]
+        rc = self.L.oro_set_mesh(self.h, mesh.n_nodes, a["x"], a["y"], a["z"], mesh.n_faces, a["fnc"], a["fn"],
+                                 a["lc"], a["rc"], mesh.n_cells, mesh.n_bfaces, a["bct"], wd)
+        assert rc == 0
+        self.nT = mesh.n_cells + mesh.n_bfaces
+
+    def __del__(self):
+        try:
+            self.L.oro_destroy(self.h)
+        except Exception:
+            pass
+
+    def init(self):
+        self.L.oro_init_flowfield(self.h)
+
+    def step(self, n=1):
+        return self.L.oro_step(self.h, n)
+
+    def task(self, name):
+        rc = self.L.oro_task(self.h, name.encode())
+        assert rc == 0, name
+
+    def field(self, name):
+        n = self.L.oro_field(self.h, name.encode(), None)
+        assert n >= 0, name
+        out = np.empty(n, np.float64)
+        self.L.oro_field(self.h, name.encode(), out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def q(self):
+        return self.field("q").reshape(5, self.nT)
+
+    def res_history(self):
+        return self.field("reshist").reshape(-1, 5)
+
+    def set_q(self, q):
+        self.L.oro_set_q(self.h, np.ascontiguousarray(q, np.float64).ravel())
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_EXE)
+
+
+def run_ref(mesh: Mesh, params: P.OfgParams, steps: int, workdir: str = None, keep: bool = False):
+    """Run the reference CPU solver on ``mesh`` for ``steps`` iterations.
+    Returns (dump dict, res.dat rows)."""
+    tmp = workdir or tempfile.mkdtemp(prefix="ofgref_")
+    case = os.path.join(tmp, "case")
+    write_case(case, mesh, P.to_dict(params), steps)
+    dump = os.path.join(tmp, "dump.bin")
+    env = dict(os.environ, OFG_REF_DUMP=dump)
+    r = subprocess.run([REF_EXE, "0", "case"], cwd=tmp, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                       timeout=3600)
+    if r.returncode != 0:
+        raise RuntimeError(r.stdout.decode(errors="replace")[-3000:])
+    out = read_ref_dump(dump), read_res_dat(os.path.join(case, "results", "res.dat"))
+    if not keep and workdir is None:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
