@@ -1,0 +1,380 @@
+"""Benchmark of the unstructured residual + LU-SGS iteration on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl ofg|reference]
+
+One JSON line on rank 0.  A step is one outer iteration of the steady solve
+(TimeIntegral::Lusgs for every solver) over the whole mesh.  ``value`` is
+cell-iterations/s with the state resident in HBM (CUDA events on the
+library's stream, max over ranks); ``e2e`` is the same metric through the
+C ABI with the state copied host->device and back every step.  Multi-GPU runs
+are independent replicas (one solve per GPU, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from oneflow_b200 import meshgen, params as P  # noqa: E402
+from oneflow_b200.meshio import Mesh, write_case  # noqa: E402
+
+L2_BYTES = 126 * 2 ** 20
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def make_workload(name: str):
+    if name == "bump2d":
+        mesh = meshgen.bump_channel(256, 128)
+        prm = P.euler_bump()
+        desc = dict(workload="2-D Euler bump channel, 256x128 quads split into 65,536 jittered triangles, "
+                             "Mach 0.5, first-order Roe, LU-SGS, CFL 5, FP64")
+    elif name == "bump2d_small":
+        mesh = meshgen.bump_channel(64, 32)
+        prm = P.euler_bump()
+        desc = dict(workload="2-D Euler bump channel 64x32 (4,096 triangles), first-order Roe, LU-SGS, FP64")
+    else:
+        raise SystemExit(f"unknown config {name}")
+    return mesh, prm, desc
+
+
+def mesh_stats(mesh: Mesh):
+    N, B, F = mesh.n_cells, mesh.n_bfaces, mesh.n_faces
+    return dict(N=N, B=B, F=F, E=2 * F - B)
+
+
+def alg_bytes(st, prm) -> dict:
+    """Algorithmic bytes of each phase of one iteration: every array the phase
+    reads or writes counted once, at its stored precision, neighbour gathers
+    counted once (perfect reuse).  Matches the data layout of the CUDA path:
+    state record (rho,u,v,w,p[,T,mul,mut]) FP64, residual/dq FP64, geometry and
+    gradients/limiters at the face precision (8 B FP64 path, 4 B mixed)."""
+    N, B, F, E = st["N"], st["B"], st["F"], st["E"]
+    NT = N + B
+    g = 8 if prm.precision == 0 else 4
+    vis = prm.vismodel > 0
+    second = prm.ilim != -1
+    nq = 8 if vis else 5                      # state record fields a face kernel reads
+    csr = (N + 1) * 4 + E * 4
+    lcrc = F * 8
+    fgeo = F * 4 * g                          # normal (3) + area
+    fcen = F * 3 * g
+    ccen = NT * 3 * g
+    vol = N * g
+    out = {}
+    out["time_step"] = NT * nq * 8 + csr + lcrc + fgeo + vol + (ccen if vis else 0) + N * 24
+    grad = 0
+    if second or vis:
+        nv = 6 if vis else 5
+        grad = (NT * nq * 8 + csr + lcrc + fgeo + fcen + ccen + vol) + N * nv * 3 * g
+    lim = 0
+    if prm.ilim in (1, 2):
+        lim = (NT * 5 * 8 + csr + lcrc + N * 10 * g) + (N * 15 * g + N * 10 * g + csr + fcen + ccen + N * 5 * g)
+    res = NT * nq * 8 + csr + lcrc + fgeo + B * 40 + N * 40
+    if second:
+        res += N * 15 * g + N * 5 * g + fcen + ccen
+    if vis:
+        res += N * 18 * g + ccen
+    out["residual"] = grad + lim + res
+    sweep = NT * nq * 8 + N * 40 + N * 40 + N * 24 + vol + csr + lcrc + fgeo + N * 4 + (ccen if vis else 0)
+    out["lusgs_lower"] = sweep + N * 40          # res read
+    out["lusgs_upper"] = sweep + N * 40          # own dq read before write
+    out["update"] = N * 64 + N * 40 + N * 64
+    out["boundary"] = B * (64 + 64 + 40 + 4 * g)
+    out["norm"] = N * 40
+    out["cfl"] = 0
+    return out
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([v.strip() for v in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the reference built from its sources, or the oracle port)
+# ---------------------------------------------------------------------------
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "oneflow_ref")
+
+
+def _ref_run(mesh, prm, steps, workdir):
+    case = os.path.join(workdir, "case")
+    write_case(case, mesh, P.to_dict(prm), steps)
+    t0 = time.perf_counter()
+    r = subprocess.run([REF_EXE, "0", "case"], cwd=workdir, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    t1 = time.perf_counter()
+    if r.returncode != 0:
+        raise RuntimeError(f"reference run failed ({r.returncode})")
+    return t1 - t0
+
+
+def reference_throughput(mesh, prm, n1, n2, nproc):
+    """Cell-iterations/s of the reference CPU solver: nproc concurrent
+    single-rank processes, per-iteration time from the difference of an
+    n1- and an n2-iteration run (setup cancels)."""
+    times = {}
+    for n in (n1, n2):
+        dirs = [tempfile.mkdtemp(prefix="ofgref_") for _ in range(nproc)]
+        for d in dirs:
+            write_case(os.path.join(d, "case"), mesh, P.to_dict(prm), n)
+        t0 = time.perf_counter()
+        procs = [subprocess.Popen([REF_EXE, "0", "case"], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                 for d in dirs]
+        rcs = [p.wait() for p in procs]
+        times[n] = time.perf_counter() - t0
+        if any(rcs):
+            raise RuntimeError(f"reference run failed: {rcs}")
+    per_iter = (times[n2] - times[n1]) / (n2 - n1)
+    return mesh.n_cells * nproc / per_iter, per_iter
+
+
+def oracle_port_throughput(mesh, prm, n1, n2):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import Oracle
+    o = Oracle(mesh, prm)
+    o.init()
+    t0 = time.perf_counter(); o.step(n1); t1 = time.perf_counter(); o.step(n2 - n1); t2 = time.perf_counter()
+    return mesh.n_cells / ((t2 - t1) / (n2 - n1)), (t2 - t1) / (n2 - n1)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", default="bump2d")
+    ap.add_argument("--impl", default="ofg", choices=["ofg", "reference"])
+    ap.add_argument("--ordering", default="natural", choices=["natural", "colour"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    mesh, prm, desc = make_workload(args.config)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        nproc = os.cpu_count() or 1
+        if not os.path.exists(REF_EXE):
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver not built (oracle/_ref)"}))
+            return
+        if args.ordering == "colour":
+            from oneflow_b200 import colour_order
+            perm, _ = colour_order(mesh)
+            mesh = mesh.renumber_cells(perm)
+        thr, per_iter = reference_throughput(mesh, prm, args.warmup, args.warmup + args.steps, nproc)
+        line = {"metric": "cell-iters/s", "value": thr, "unit": "cell-iter/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded mesh generator)",
+                "config": dict(desc, cells=mesh.n_cells, ordering=args.ordering),
+                "cpu_baseline": {"value": thr, "unit": "cell-iter/s", "cores": nproc, "kind": "reference",
+                                 "sample": f"{nproc} concurrent single-rank reference solves of the full mesh; "
+                                           f"per-iteration time = (t({args.warmup + args.steps}) - t({args.warmup}))"
+                                           f" / {args.steps}"},
+                "e2e": {"value": thr, "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    from oneflow_b200 import Solver, colour_order
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    if args.ordering == "colour":
+        perm, ncol = colour_order(mesh)
+        mesh = mesh.renumber_cells(perm)
+    st = mesh_stats(mesh)
+    stream = torch.cuda.current_stream()
+    s = Solver(mesh, prm)
+    s.set_stream(stream.cuda_stream)
+    s.init_flowfield()
+    for _ in range(args.warmup):
+        s.step(1)
+    torch.cuda.synchronize()
+    abytes = alg_bytes(st, prm)
+    working = sum(abytes.values())
+    flush = working < 2 * L2_BYTES
+    scratch = torch.empty(int(2 * L2_BYTES // 4), dtype=torch.float32, device="cuda") if flush else None
+    _, l0 = s.counters()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = []
+    with ClockSampler(dev) as clk:
+        if flush:
+            total_ms = 0.0
+            for _ in range(args.steps):
+                scratch.fill_(1.0)          # write > L2 between timed steps
+                a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+                a.record(stream); s.step(1); b.record(stream)
+                ev.append((a, b))
+            torch.cuda.synchronize()
+            total_ms = sum(a.elapsed_time(b) for a, b in ev)
+        else:
+            a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+            a.record(stream); s.step(args.steps); b.record(stream)
+            torch.cuda.synchronize()
+            total_ms = a.elapsed_time(b)
+    _, l1 = s.counters()
+    torch.cuda.synchronize()
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = st["N"] * args.steps * world / (total_ms * 1e-3)
+
+    # per-group device times (task-by-task launch with events) for the roofline
+    prof = []
+    for _ in range(3):
+        if flush:
+            scratch.fill_(1.0)
+        prof.append(s.profile_step())
+    grp_ms = {k: statistics.median(p[0][k] for p in prof) for k in prof[0][0]}
+    grp_n = prof[0][1]
+    top = max((k for k in grp_ms if k != "cfl"), key=lambda k: grp_ms[k])
+    hbm = _peak_hbm()
+    per_launch_ms = grp_ms[top] / max(grp_n[top], 1)
+    achieved = abytes[top] / (grp_ms[top] * 1e-3) / 1e9   # GB/s over the group's launches
+    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm["value"], "unit": "GB/s",
+                "frac": achieved / hbm["value"], "traffic": None, "peak_source": hbm["source"],
+                "alg_bytes_per_step": abytes[top], "launches_per_step": grp_n[top],
+                "avg_launch_ms": per_launch_ms,
+                "whole_step_achieved_gbs": working / (total_ms / args.steps * 1e-3) / 1e9,
+                "whole_step_frac": working / (total_ms / args.steps * 1e-3) / 1e9 / hbm["value"],
+                "group_ms": grp_ms, "group_alg_bytes": abytes}
+
+    # end to end through the C ABI with host buffers
+    e2e_steps = max(3, min(args.steps, 10))
+    q = s.state()
+    h2d = q.nbytes
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.upload_state(q)
+        s.step(1)
+        q = s.state()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_val = st["N"] * e2e_steps * world / e2e_s
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = st["N"] * e2e_steps * world / float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = _cpu_baseline(mesh, prm, args.config)
+
+    clocks = clk.summary()
+    if rank == 0:
+        line = {"metric": "cell-iters/s", "value": value, "unit": "cell-iter/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prm.precision == 0 else "f32/f64",
+                "data": "synthetic (seeded mesh generator)",
+                "config": dict(desc, cells=st["N"], faces=st["F"], ordering=args.ordering,
+                               l2="flushed between timed steps" if flush else "working set larger than L2",
+                               parallelism=f"replicas x{world}"),
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+                "gpu_launches": int(l1 - l0), "clocks": clocks}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        s.close()
+        dist.destroy_process_group()
+
+
+def _peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return {"value": float(json.load(fh)["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        return {"value": 6650.0, "source": "fallback"}
+
+
+def _cpu_baseline(mesh, prm, config):
+    if os.path.exists(REF_EXE):
+        n1, n2 = (5, 25) if mesh.n_cells < 200000 else (1, 3)
+        try:
+            thr, per_iter = reference_throughput(mesh, prm, n1, n2, 1)
+            return {"value": thr, "unit": "cell-iter/s", "cores": 1, "kind": "reference",
+                    "sample": f"reference CPU solver (built from its sources), 1 process, full mesh, "
+                              f"(t({n2}) - t({n1})) / {n2 - n1} iterations"}
+        except Exception as e:  # fall back to the port
+            note = f"reference run failed: {e}"
+    else:
+        note = "reference build absent"
+    thr, per_iter = oracle_port_throughput(mesh, prm, 2, 6)
+    return {"value": thr, "unit": "cell-iter/s", "cores": 1, "kind": "port",
+            "sample": f"CPU restatement, 1 thread, full mesh, 4 iterations ({note})"}
+
+
+if __name__ == "__main__":
+    main()

@@ -150,6 +150,18 @@ int ofg_residual_norms(ofg_ctx *ctx, int tid, double *rms);
 int ofg_download_field(ofg_ctx *ctx, int tid, const char *name, double *out, int64_t n_out,
                        int64_t *n_needed);
 
+/* Run every later launch of this context on the caller's CUDA stream
+   (a cudaStream_t passed as void*; NULL restores the context's own stream).
+   Captured graphs are rebuilt on the next ofg_step. */
+int ofg_set_stream(ofg_ctx *ctx, void *stream);
+
+/* One outer iteration launched task by task (no graph) with CUDA events
+   between the groups; ms[8] receives the device time of: CFL advance,
+   CALC_TIME_STEP, UPDATE_RESIDUALS, LUSGS_LOWER_SWEEP, LUSGS_UPPER_SWEEP,
+   UPDATE_FLOWFIELD, CALC_BOUNDARY, residual norm; launches[8] the number of
+   kernel launches of each group. */
+int ofg_profile_step(ofg_ctx *ctx, double *ms, int *launches);
+
 /* Iteration::outerSteps for the task-level API (the CFL ramp of the next
    CALC_TIME_STEP reads it); ofg_step advances it itself. */
 int ofg_set_outer_step(ofg_ctx *ctx, int64_t outer_steps);

@@ -290,7 +290,7 @@ void ofg_destroy(ofg_ctx *c) {
                     c->d_partial, c->d_scal, c->d_hist, c->d_grad, c->d_lim, c->d_mm, c->d_fix};
     for (void *v : ptrs) if (v) cudaFree(v);
     for (int i = 0; i < 11; ++i) { if (c->d_g64[i]) cudaFree(c->d_g64[i]); if (c->d_g32[i]) cudaFree(c->d_g32[i]); }
-    cudaStreamDestroy(c->stream);
+    cudaStreamDestroy(c->ownStream ? c->ownStream : c->stream);
     delete c;
 }
 
@@ -665,6 +665,48 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
         std::copy(buf.begin(), buf.end(), out);
     }
     (void)nF;
+    return OFG_OK;
+}
+
+int ofg_set_stream(ofg_ctx *c, void *stream) {
+    if (!c) return OFG_E_ARG;
+    int rc = sync(c);
+    if (rc) return rc;
+    destroy_graphs(c);
+    if (!c->ownStream) c->ownStream = c->stream;
+    c->stream = stream ? (cudaStream_t)stream : c->ownStream;
+    return OFG_OK;
+}
+
+int ofg_profile_step(ofg_ctx *c, double *ms, int *launches) {
+    int rc = check_tid(c, OFG_NS_SOLVER);
+    if (rc) return rc;
+    if (!ms) return c->fail(OFG_E_ARG, "null output");
+    if (c->pendingNext) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
+    double sc[2] = {double(c->outerSteps), double(c->outerSteps)};
+    CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const int tasks[8] = {T_ADVANCE, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
+    cudaEvent_t ev[9];
+    for (int i = 0; i < 9; ++i) CK(cudaEventCreate(&ev[i]));
+    CK(cudaEventRecord(ev[0], c->stream));
+    for (int i = 0; i < 8; ++i) {
+        long long before = c->launches;
+        if ((rc = launch(c, tasks[i]))) return rc;
+        if (launches) launches[i] = int(c->launches - before);
+        CK(cudaEventRecord(ev[i + 1], c->stream));
+    }
+    CK(cudaEventSynchronize(ev[8]));
+    for (int i = 0; i < 8; ++i) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+        ms[i] = t;
+    }
+    for (int i = 0; i < 9; ++i) cudaEventDestroy(ev[i]);
+    c->cur ^= 1;
+    c->outerSteps++;
+    std::vector<double> row(NEQ);
+    CK(cudaMemcpy(row.data(), c->d_scal + S_NORM, NEQ * sizeof(double), cudaMemcpyDeviceToHost));
+    c->hist.insert(c->hist.end(), row.begin(), row.end());
     return OFG_OK;
 }
 

@@ -22,7 +22,8 @@ struct ofg_ctx {
     bool haveMesh = false, haveState = false;
 
     // ---- device ----
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // stream every launch goes to
+    cudaStream_t ownStream = nullptr;   // the context's own stream (set when a caller's stream is in use)
     int *d_lc = nullptr, *d_rc = nullptr, *d_bct = nullptr, *d_c2f_off = nullptr, *d_c2f = nullptr;
     int *d_lowOrder = nullptr, *d_upOrder = nullptr;
     double *d_g64[11] = {};    // xfn yfn zfn area xfc yfc zfc | xcc ycc zcc vol

@@ -54,6 +54,8 @@ def load_library() -> C.CDLL:
     L.ofg_download_field.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
     L.ofg_get_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.ofg_set_outer_step.argtypes = [C.c_void_p, C.c_int64]
+    L.ofg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.ofg_profile_step.argtypes = [C.c_void_p, _dp, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")]
     L.ofg_colour_order.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip]
     L.ofg_version.restype = C.c_int
     _LIB = L
@@ -133,6 +135,19 @@ class Solver:
 
     def step(self, n: int = 1):
         self._check(self.L.ofg_step(self.h, n))
+
+    def set_stream(self, stream_ptr: int):
+        """Launch on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._check(self.L.ofg_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    PROFILE_GROUPS = ("cfl", "time_step", "residual", "lusgs_lower", "lusgs_upper", "update", "boundary", "norm")
+
+    def profile_step(self):
+        """One iteration task by task with CUDA events: ({group: ms}, {group: launches})."""
+        ms = np.zeros(8, np.float64)
+        nl = np.zeros(8, np.int32)
+        self._check(self.L.ofg_profile_step(self.h, ms, nl))
+        return dict(zip(self.PROFILE_GROUPS, ms.tolist())), dict(zip(self.PROFILE_GROUPS, nl.tolist()))
 
     def residual_norms(self, tid: int = NS_SOLVER) -> np.ndarray:
         out = np.empty(5, np.float64)
