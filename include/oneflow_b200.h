@@ -90,7 +90,9 @@ typedef struct ofg_params {
     double inflow_viscosity;  /* SA nu~ of the freestream                      */
     double rprod;
     double turb_cfl_ratio;
-    double reserved_d[8];
+    double ref_sa;            /* SA nu~ of the freestream (TurbCom::InitInflow)  */
+    double max_vis_ratio;     /* cap of mu_t / mu_l                              */
+    double reserved_d[6];
 } ofg_params;
 
 typedef struct ofg_ctx ofg_ctx;
@@ -169,6 +171,12 @@ int ofg_set_outer_step(ofg_ctx *ctx, int64_t outer_steps);
 /* Outer-iteration counter (Iteration::outerSteps) and a counter of every
    CUDA kernel launch this context issued (for reporting). */
 int ofg_get_counters(ofg_ctx *ctx, int64_t *outer_steps, int64_t *kernel_launches);
+
+/* Cell centres [nCells][3] of a mesh with the reference's metrics (host
+   only, no device needed): used to build wall distances and probes. */
+int ofg_cell_centres(int dimension, int nNodes, const double *xN, const double *yN, const double *zN, int nFaces,
+                     const int *faceNodeCount, const int *faceNodes, const int *lCells, const int *rCells,
+                     int nCells, int nBFaces, double *out);
 
 /* Cell renumbering for the GPU sweeps: a greedy colouring of the cell graph
    followed by a locality order inside each colour.  Writes perm[newId] = oldId

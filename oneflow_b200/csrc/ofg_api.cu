@@ -223,7 +223,19 @@ void derive_params(ofg_ctx *c) {
     d.sutherland_ts = 110.4 / p.tref_dim;
     d.max_time_ratio = p.max_time_ratio;
     d.global_dt = p.global_dt;
-    d.nut_inf = p.inflow_viscosity;
+    d.nut_inf = p.ref_sa;   // TurbCom::InitInflow: inflow[ISA] = ref_sa for the SA model
+    d.max_vis_ratio = p.max_vis_ratio;
+    d.turb_cfl_ratio = p.turb_cfl_ratio;
+    d.rprod = p.rprod;
+    d.iprod_sa = p.iprod_sa;
+    d.ft2_flag = p.ft2_flag;
+    {
+        double karm = 0.41, karm2 = karm * karm, okarm2 = 1.0 / karm2, cb1 = 0.1355, cb2 = 0.622, cv1 = 7.1;
+        double sigma = 2.0 / 3.0, osigma = 1.0 / sigma, cw1 = cb1 * okarm2 + (1.0 + cb2) / sigma;
+        d.sa_cb1 = cb1; d.sa_cv13 = cv1 * cv1 * cv1; d.sa_cw2 = 0.3; d.sa_cw36 = std::pow(2.0, 6);
+        d.sa_ct3 = 1.2; d.sa_ct4 = 0.5; d.sa_osigma = osigma; d.sa_cw1 = cw1; d.sa_sac2 = 0.7; d.sa_sac3 = 0.9;
+        d.sa_cb2s = osigma * cb2; d.sa_cw1k = cw1 * karm2; d.sa_okarm2 = okarm2;
+    }
 }
 
 double host_sutherland(const DevParams &P, double t) {
@@ -231,9 +243,12 @@ double host_sutherland(const DevParams &P, double t) {
     return std::sqrt(t3) * (1 + P.sutherland_ts) / (t + P.sutherland_ts);
 }
 
+bool has_turb(const ofg_ctx *c) { return c->p.vismodel >= 3; }
+
 int check_tid(ofg_ctx *c, int tid) {
     if (!c) return OFG_E_ARG;
-    if (tid != OFG_NS_SOLVER) return c->fail(OFG_E_ARG, "only the NS solver (tid 0) is available in this build");
+    if (tid != OFG_NS_SOLVER && !(tid == OFG_TURB_SOLVER && has_turb(c)))
+        return c->fail(OFG_E_ARG, "no such solver in this context (tid 1 needs vismodel 3)");
     if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
     if (!c->haveState) return c->fail(OFG_E_STATE, "no flow field: call ofg_init_flowfield or ofg_upload_state");
     return OFG_OK;
@@ -269,7 +284,8 @@ int ofg_create(const ofg_params *p, ofg_ctx **out) {
     if (p->ilim < -1 || p->ilim > 2) return OFG_E_ARG;
     if (p->igrad < 0 || p->igrad > 2) return OFG_E_ARG;
     if (p->precision != OFG_PREC_FP64 && p->precision != OFG_PREC_MIXED) return OFG_E_ARG;
-    if (p->vismodel != 0 && p->vismodel != 1) return OFG_E_ARG;   // SA: separate solver, tid 1
+    if (p->vismodel != 0 && p->vismodel != 1 && p->vismodel != 3) return OFG_E_ARG;   // Euler, laminar, SA
+    if (p->vismodel == 3 && p->turb_ilim != -1) return OFG_E_ARG;   // first-order SA convection only
     if (p->ivischeme != 0) return OFG_E_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return OFG_E_CUDA;
@@ -287,7 +303,8 @@ void ofg_destroy(ofg_ctx *c) {
     destroy_graphs(c);
     void *ptrs[] = {c->d_lc, c->d_rc, c->d_bct, c->d_c2f_off, c->d_c2f, c->d_lowOrder, c->d_upOrder, c->d_wdist,
                     c->d_q[0], c->d_q[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_bcq,
-                    c->d_partial, c->d_scal, c->d_hist, c->d_grad, c->d_lim, c->d_mm, c->d_fix};
+                    c->d_partial, c->d_scal, c->d_hist, c->d_grad, c->d_lim, c->d_mm, c->d_fix,
+                    c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
     for (void *v : ptrs) if (v) cudaFree(v);
     for (int i = 0; i < 11; ++i) { if (c->d_g64[i]) cudaFree(c->d_g64[i]); if (c->d_g32[i]) cudaFree(c->d_g32[i]); }
     cudaStreamDestroy(c->ownStream ? c->ownStream : c->stream);
@@ -405,10 +422,26 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         if (rs == sizeof(float)) { std::vector<float> one(N * NEQ, 1.0f); CK(cudaMemcpy(c->d_lim, one.data(), N * NEQ * rs, cudaMemcpyHostToDevice)); }
         else { std::vector<double> one(N * NEQ, 1.0); CK(cudaMemcpy(c->d_lim, one.data(), N * NEQ * rs, cudaMemcpyHostToDevice)); }
     }
+    if (has_turb(c)) {
+        if (!wall_dist) return c->fail(OFG_E_ARG, "the SA model needs the wall distance");
+        for (int i = 0; i < nCells; ++i)
+            if (!(wall_dist[i] > 0.0)) return c->fail(OFG_E_ARG, "wall distance must be positive");
+        if ((rc = upload<double>(c, &c->d_nut, nullptr, nT))) return rc;
+        if ((rc = upload<double>(c, &c->d_dnut, nullptr, nT))) return rc;
+        if ((rc = upload<double>(c, &c->d_resT, nullptr, N))) return rc;
+        if ((rc = upload<double>(c, &c->d_impsrT, nullptr, N))) return rc;
+        if ((rc = upload<double>(c, &c->d_matL, nullptr, nFaces))) return rc;
+        if ((rc = upload<double>(c, &c->d_matR, nullptr, nFaces))) return rc;
+        if ((rc = upload<double>(c, &c->d_thist, nullptr, c->histCap))) return rc;
+        if (c->d_gnut) cudaFree(c->d_gnut);
+        CK(cudaMalloc(&c->d_gnut, N * 3 * rs));
+        CK(cudaMemset(c->d_dnut, 0, nT * sizeof(double)));
+    }
     c->haveMesh = true;
     c->haveState = false;
     c->outerSteps = 0;
     c->hist.clear();
+    c->thist.clear();
     return OFG_OK;
 }
 
@@ -432,18 +465,34 @@ int ofg_init_flowfield(ofg_ctx *c) {
     CK(cudaMemset(c->d_scal, 0, 32 * sizeof(double)));
     c->outerSteps = 0;
     c->hist.clear();
+    c->thist.clear();
     c->haveState = true;
     c->pendingNext = false;
     int rc = launch(c, T_BOUNDARY_CUR);   // NsInitFinal -> NsCalcBoundary
     if (rc) return rc;
+    if (has_turb(c)) {
+        // UTurbRestart::InitRestart (nu~ = ref_sa everywhere) + TurbInitFinal
+        std::vector<double> nut(c->nT, P.nut_inf);
+        CK(cudaMemcpyAsync(c->d_nut, nut.data(), nut.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if ((rc = launch(c, T_TURB_BOUNDARY_CUR))) return rc;
+    }
     return sync(c);
 }
 
 int ofg_upload_state(ofg_ctx *c, int tid, const double *q) {
     if (!c || !q) return OFG_E_ARG;
-    if (tid != OFG_NS_SOLVER) return c->fail(OFG_E_ARG, "only the NS solver (tid 0) is available in this build");
+    if (tid != OFG_NS_SOLVER && !(tid == OFG_TURB_SOLVER && has_turb(c)))
+        return c->fail(OFG_E_ARG, "no such solver in this context");
     if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
+    if (c->pendingNext) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
     destroy_graphs(c);
+    if (tid == OFG_TURB_SOLVER) {
+        if (!c->haveState) return c->fail(OFG_E_STATE, "upload the NS state first");
+        CK(cudaMemcpy(c->d_nut, q, (size_t)c->nT * sizeof(double), cudaMemcpyHostToDevice));
+        int rc = launch(c, T_TURB_BOUNDARY_CUR);
+        if (rc) return rc;
+        return sync(c);
+    }
     std::vector<double> rec((size_t)c->nT * REC, 0.0);
     for (int i = 0; i < c->nT; ++i)
         for (int e = 0; e < NEQ; ++e) rec[(size_t)i * REC + e] = q[(size_t)e * c->nT + i];
@@ -462,6 +511,10 @@ int ofg_download_state(ofg_ctx *c, int tid, double *q) {
     if (rc) return rc;
     if (!q) return c->fail(OFG_E_ARG, "null output");
     if ((rc = sync(c))) return rc;
+    if (tid == OFG_TURB_SOLVER) {
+        CK(cudaMemcpy(q, c->d_nut, (size_t)c->nT * sizeof(double), cudaMemcpyDeviceToHost));
+        return OFG_OK;
+    }
     std::vector<double> rec((size_t)c->nT * REC);
     CK(cudaMemcpy(rec.data(), c->d_q[c->cur], rec.size() * sizeof(double), cudaMemcpyDeviceToHost));
     for (int i = 0; i < c->nT; ++i)
@@ -472,13 +525,17 @@ int ofg_download_state(ofg_ctx *c, int tid, double *q) {
 int ofg_zero_dq(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
-    CK(cudaMemsetAsync(c->d_dq, 0, (size_t)c->nT * NEQ * sizeof(double), c->stream));
+    if (tid == OFG_TURB_SOLVER)
+        CK(cudaMemsetAsync(c->d_dnut, 0, (size_t)c->nT * sizeof(double), c->stream));
+    else
+        CK(cudaMemsetAsync(c->d_dq, 0, (size_t)c->nT * NEQ * sizeof(double), c->stream));
     return OFG_OK;
 }
 
 int ofg_calc_time_step(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
+    if (tid == OFG_TURB_SOLVER) return OFG_OK;   // no CALC_TIME_STEP in system/turb/function/funcMap.txt
     if ((rc = launch(c, T_CFL))) return rc;
     return launch(c, T_TIMESTEP);
 }
@@ -492,7 +549,8 @@ int ofg_load_residuals(ofg_ctx *c, int tid) {
 int ofg_update_residuals(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
-    return launch(c, T_RESIDUAL);
+    if (tid == OFG_TURB_SOLVER && c->pendingNext) return c->fail(OFG_E_STATE, "NS update without CALC_BOUNDARY");
+    return launch(c, tid == OFG_TURB_SOLVER ? T_TURB_RHS : T_RESIDUAL);
 }
 
 int ofg_init_lusgs(ofg_ctx *c, int tid) { return check_tid(c, tid); }
@@ -500,18 +558,23 @@ int ofg_init_lusgs(ofg_ctx *c, int tid) { return check_tid(c, tid); }
 int ofg_lusgs_lower(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
-    return launch(c, T_LOWER);
+    return launch(c, tid == OFG_TURB_SOLVER ? T_TURB_LOWER : T_LOWER);
 }
 
 int ofg_lusgs_upper(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
-    return launch(c, T_UPPER);
+    return launch(c, tid == OFG_TURB_SOLVER ? T_TURB_UPPER : T_UPPER);
 }
 
 int ofg_update_flowfield(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
+    if (tid == OFG_TURB_SOLVER) {
+        if ((rc = launch(c, T_TURB_UPDATE))) return rc;   // nu~ update + interior eddy viscosity
+        c->pendingTurb = true;
+        return OFG_OK;
+    }
     if ((rc = launch(c, T_UPDATE))) return rc;
     c->pendingNext = true;
     return OFG_OK;
@@ -520,6 +583,12 @@ int ofg_update_flowfield(ofg_ctx *c, int tid) {
 int ofg_calc_boundary(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
+    if (tid == OFG_TURB_SOLVER) {
+        // TurbCalcBoundary: CalcTurbulentViscosity + TurbCalcBc
+        rc = launch(c, c->pendingTurb ? T_TURB_BOUNDARY : T_TURB_BOUNDARY_CUR);
+        c->pendingTurb = false;
+        return rc;
+    }
     if (c->pendingNext) {
         if ((rc = launch(c, T_BOUNDARY_NEXT))) return rc;
         c->cur ^= 1;
@@ -529,31 +598,61 @@ int ofg_calc_boundary(ofg_ctx *c, int tid) {
     return launch(c, T_BOUNDARY_CUR);
 }
 
+// tasks of one outer iteration (MG::StrongIter: NS relaxation, then SA), with
+// the state-buffer flip between the two solvers
+static const int kNsTasks[] = {T_ADVANCE, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
+static const int kTurbTasks[] = {T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_NORM};
+
+static int sync_history(ofg_ctx *c) {
+    size_t have = c->hist.size() / NEQ;
+    size_t want = (size_t)c->outerSteps;
+    if (want > have) {
+        std::vector<double> tmp((want - have) * NEQ);
+        CK(cudaMemcpy(tmp.data(), c->d_hist + have * NEQ, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        c->hist.insert(c->hist.end(), tmp.begin(), tmp.end());
+        for (double v : tmp)
+            if (std::isnan(v)) return c->fail(OFG_E_NAN, "NotANumber in the NS residual");
+        if (has_turb(c)) {
+            std::vector<double> tt(want - have);
+            CK(cudaMemcpy(tt.data(), c->d_thist + have, tt.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            c->thist.insert(c->thist.end(), tt.begin(), tt.end());
+            for (double v : tt)
+                if (std::isnan(v)) return c->fail(OFG_E_NAN, "NotANumber in the SA residual");
+        }
+    }
+    return OFG_OK;
+}
+
 int ofg_step(ofg_ctx *c, int nsteps) {
     int rc = check_tid(c, OFG_NS_SOLVER);
     if (rc) return rc;
     if (nsteps < 0) return c->fail(OFG_E_ARG, "negative step count");
-    if (c->pendingNext) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
+    if (c->pendingNext || c->pendingTurb) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
     if (c->outerSteps + nsteps > c->histCap) return c->fail(OFG_E_ARG, "residual history capacity exceeded");
-    // the device step counter and history index follow the host counters
-    double sc[2] = {double(c->outerSteps), double(c->outerSteps)};
+    // the device step counter and history indices follow the host counters
+    double sc[4] = {double(c->outerSteps), double(c->outerSteps), 0.0, double(c->outerSteps)};
     CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_scal + S_THISTN, sc + 3, sizeof(double), cudaMemcpyHostToDevice, c->stream));
     if ((rc = sync(c))) return rc;
     if (!c->graph[0]) {
-        // capture one outer iteration per state-buffer parity:
-        // MG::Run -> TimeIntegral::Lusgs (ZERO_DQ_FIELD is not needed: no kernel
-        // reads a dq value it did not write in the same iteration)
+        // one outer iteration per state-buffer parity (ZERO_DQ_FIELD is not
+        // needed: no kernel reads an increment it did not write this iteration)
         int saveCur = c->cur;
         for (int g = 0; g < 2; ++g) {
-            c->cur = g;
             long long before = c->launches;
             cudaGraph_t graph;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            int tasks[] = {T_ADVANCE, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
-            for (int t : tasks) {
+            c->cur = g;
+            for (int t : kNsTasks) {
                 rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
-                if (rc) { cudaStreamEndCapture(c->stream, &graph); return rc; }
+                if (rc) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
             }
+            c->cur = g ^ 1;
+            if (has_turb(c))
+                for (int t : kTurbTasks) {
+                    rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
+                    if (rc) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
+                }
             CK(cudaStreamEndCapture(c->stream, &graph));
             CK(cudaGraphInstantiate(&c->graph[g], graph, 0));
             cudaGraphDestroy(graph);
@@ -569,17 +668,7 @@ int ofg_step(ofg_ctx *c, int nsteps) {
         c->outerSteps++;
     }
     if ((rc = sync(c))) return rc;
-    // pull the new history rows
-    size_t have = c->hist.size() / NEQ;
-    size_t want = (size_t)c->outerSteps;
-    if (want > have) {
-        std::vector<double> tmp((want - have) * NEQ);
-        CK(cudaMemcpy(tmp.data(), c->d_hist + have * NEQ, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        c->hist.insert(c->hist.end(), tmp.begin(), tmp.end());
-        for (double v : tmp)
-            if (std::isnan(v)) return c->fail(OFG_E_NAN, "NotANumber in the residual");
-    }
-    return OFG_OK;
+    return sync_history(c);
 }
 
 int ofg_residual_norms(ofg_ctx *c, int tid, double *rms) {
@@ -655,7 +744,12 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
     else if (s == "xfn") host_vec(c->xfn);
     else if (s == "yfn") host_vec(c->yfn);
     else if (s == "zfn") host_vec(c->zfn);
-    else if (s == "reshist") host_vec(c->hist);
+    else if (s == "reshist") host_vec(tid == OFG_TURB_SOLVER ? c->thist : c->hist);
+    else if (s == "turbreshist") host_vec(c->thist);
+    else if (has_turb(c) && (s == "turbq" || s == "turbdq")) aos_field(s == "turbq" ? c->d_nut : c->d_dnut, 1, nT, nT);
+    else if (has_turb(c) && s == "turbres") aos_field(c->d_resT, 1, N, nT);
+    else if (has_turb(c) && s == "turbimpsr") aos_field(c->d_impsrT, 1, N, nT);
+    else if (s == "walldist") { buf.assign(nT, 0.0); std::copy(c->wdist.begin(), c->wdist.end(), buf.begin()); }
     else return c->fail(OFG_E_ARG, "unknown field " + s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return c->fail(OFG_E_CUDA, cudaGetErrorString(e));
@@ -682,32 +776,32 @@ int ofg_profile_step(ofg_ctx *c, double *ms, int *launches) {
     int rc = check_tid(c, OFG_NS_SOLVER);
     if (rc) return rc;
     if (!ms) return c->fail(OFG_E_ARG, "null output");
-    if (c->pendingNext) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
+    if (c->pendingNext || c->pendingTurb) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
     double sc[2] = {double(c->outerSteps), double(c->outerSteps)};
     CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    const int tasks[8] = {T_ADVANCE, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
-    cudaEvent_t ev[9];
-    for (int i = 0; i < 9; ++i) CK(cudaEventCreate(&ev[i]));
+    CK(cudaMemcpyAsync(c->d_scal + S_THISTN, sc, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    // groups: the 8 NS groups, then SA rhs, lower, upper, update, boundary, norm
+    const int nns = 8, nt = has_turb(c) ? 6 : 0, n = nns + nt;
+    cudaEvent_t ev[15];
+    for (int i = 0; i <= n; ++i) CK(cudaEventCreate(&ev[i]));
     CK(cudaEventRecord(ev[0], c->stream));
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < n; ++i) {
         long long before = c->launches;
-        if ((rc = launch(c, tasks[i]))) return rc;
+        if (i == nns) c->cur ^= 1;   // the SA solver reads the relaxed NS state
+        if ((rc = launch(c, i < nns ? kNsTasks[i] : kTurbTasks[i - nns]))) return rc;
         if (launches) launches[i] = int(c->launches - before);
         CK(cudaEventRecord(ev[i + 1], c->stream));
     }
-    CK(cudaEventSynchronize(ev[8]));
-    for (int i = 0; i < 8; ++i) {
+    if (nt == 0) c->cur ^= 1;
+    CK(cudaEventSynchronize(ev[n]));
+    for (int i = 0; i < n; ++i) {
         float t = 0.f;
         CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
         ms[i] = t;
     }
-    for (int i = 0; i < 9; ++i) cudaEventDestroy(ev[i]);
-    c->cur ^= 1;
+    for (int i = 0; i <= n; ++i) cudaEventDestroy(ev[i]);
     c->outerSteps++;
-    std::vector<double> row(NEQ);
-    CK(cudaMemcpy(row.data(), c->d_scal + S_NORM, NEQ * sizeof(double), cudaMemcpyDeviceToHost));
-    c->hist.insert(c->hist.end(), row.begin(), row.end());
-    return OFG_OK;
+    return sync_history(c);
 }
 
 int ofg_set_outer_step(ofg_ctx *c, int64_t outer_steps) {
@@ -720,6 +814,33 @@ int ofg_get_counters(ofg_ctx *c, int64_t *outer_steps, int64_t *kernel_launches)
     if (!c) return OFG_E_ARG;
     if (outer_steps) *outer_steps = c->outerSteps;
     if (kernel_launches) *kernel_launches = c->launches;
+    return OFG_OK;
+}
+
+int ofg_cell_centres(int dim, int nNodes, const double *xN, const double *yN, const double *zN, int nFaces,
+                     const int *faceNodeCount, const int *faceNodes, const int *lCells, const int *rCells, int nCells,
+                     int nBFaces, double *out) {
+    if (nNodes <= 0 || nFaces <= 0 || nCells <= 0 || nBFaces < 0 || !out) return OFG_E_ARG;
+    ofg_ctx tmp;
+    tmp.nCells = nCells; tmp.nBFaces = nBFaces; tmp.nFaces = nFaces; tmp.nT = nCells + nBFaces;
+    std::vector<int> fOff(nFaces + 1, 0);
+    for (int f = 0; f < nFaces; ++f) fOff[f + 1] = fOff[f] + faceNodeCount[f];
+    std::vector<int> fNod(faceNodes, faceNodes + fOff[nFaces]);
+    tmp.lc.assign(lCells, lCells + nFaces);
+    tmp.rc.assign(rCells, rCells + nFaces);
+    for (int f = 0; f < nFaces; ++f)
+        if (tmp.lc[f] < 0) {
+            std::reverse(fNod.begin() + fOff[f], fNod.begin() + fOff[f + 1]);
+            std::swap(tmp.lc[f], tmp.rc[f]);
+        }
+    for (int f = 0; f < nBFaces; ++f) tmp.rc[f] = f + nCells;
+    for (int f = 0; f < nFaces; ++f)
+        if (tmp.lc[f] < 0 || tmp.lc[f] >= nCells || tmp.rc[f] < 0 || tmp.rc[f] >= tmp.nT) return OFG_E_ARG;
+    std::vector<double> X(xN, xN + nNodes), Y(yN, yN + nNodes), Z(zN, zN + nNodes);
+    compute_metrics(&tmp, dim, X, Y, Z, fOff, fNod);
+    for (int i = 0; i < nCells; ++i) {
+        out[3 * (size_t)i] = tmp.xcc[i]; out[3 * (size_t)i + 1] = tmp.ycc[i]; out[3 * (size_t)i + 2] = tmp.zcc[i];
+    }
     return OFG_OK;
 }
 

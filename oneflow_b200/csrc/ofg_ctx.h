@@ -32,10 +32,16 @@ struct ofg_ctx {
     double *d_q[2] = {nullptr, nullptr};
     int cur = 0;
     bool pendingNext = false;   // UPDATE_FLOWFIELD wrote d_q[cur^1], CALC_BOUNDARY not yet run
+    bool pendingTurb = false;   // SA UPDATE_FLOWFIELD ran, its CALC_BOUNDARY not yet
     double *d_res = nullptr, *d_dq = nullptr, *d_dt = nullptr, *d_invsr = nullptr, *d_vissr = nullptr;
     double *d_bcq = nullptr, *d_partial = nullptr, *d_scal = nullptr, *d_hist = nullptr;
     void *d_grad = nullptr, *d_lim = nullptr, *d_mm = nullptr;
     int *d_fix = nullptr;
+    // SA solver
+    double *d_nut = nullptr, *d_dnut = nullptr, *d_resT = nullptr, *d_impsrT = nullptr, *d_matL = nullptr,
+           *d_matR = nullptr, *d_thist = nullptr;
+    void *d_gnut = nullptr;
+    std::vector<double> thist;         // host copy of the SA residual history
     int fixcap = 4096;
     int histCap = 0;
     size_t nPartialMax = 0;
@@ -57,7 +63,8 @@ namespace ofg {
 // tasks executed by the precision-specific launchers
 enum Task {
     T_CFL = 0, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_BOUNDARY_CUR,
-    T_NORM, T_ADVANCE
+    T_NORM, T_ADVANCE,
+    T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_BOUNDARY_CUR, T_TURB_NORM
 };
 int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);
 int launch_task_f32(ofg_ctx *c, int task, cudaStream_t s);

@@ -18,7 +18,7 @@ enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4, ITT = 5, IML = 6, IMT = 7 };
 // slots of the small device scalar array (cfl, min dt, limiter eps, norms,
 // outer-step counter, residual-history length)
 enum { S_CFL = 0, S_MINDT = 1, S_EPS = 2 /* 5 slots */, S_NORM = 8 /* 5 slots */, S_STEP = 14, S_HISTN = 15,
-       S_NSCAL = 16 };
+       S_TNORM = 16, S_THISTN = 17, S_NSCAL = 18 };
 
 enum BcCode { BC_EXTRAP = 1, BC_SOLID = 2, BC_SYM = 3, BC_FAR = 4, BC_INFLOW = 5, BC_OUTFLOW = 6 };
 
@@ -44,8 +44,11 @@ struct DevParams {
     double gama, centropy1, centropy2, vencat_coef, reynolds, oreynolds, oprl, oprt, const_cp, statecoef;
     double inflow[NEQ];
     double twall, sutherland_ts, max_time_ratio, global_dt;
-    // SA
-    double nut_inf;
+    // SA (TurbCom::InitConst, codes/turb/src/TurbCom.cpp:110-350)
+    double nut_inf, max_vis_ratio, turb_cfl_ratio, rprod;
+    int iprod_sa, ft2_flag;
+    double sa_cb1, sa_cv13, sa_cw2, sa_cw36, sa_ct3, sa_ct4, sa_osigma, sa_cw1, sa_sac2, sa_sac3, sa_cb2s, sa_cw1k,
+        sa_okarm2;
 };
 
 // Mesh in device memory: faces SoA, cells SoA, CSR cell->face lists in

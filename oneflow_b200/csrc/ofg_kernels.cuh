@@ -26,6 +26,13 @@ struct KArgs {
     double *scal;         // small device scalars (cfl, eps, min dt, norms)
     int *fixlist;         // [1 + cap]: count, cell ids
     int fixcap;
+    // Spalart-Allmaras solver
+    double *nut;          // [nT] nu~ (ghosts at nCells + f)
+    double *dnut;         // [nT]
+    double *resT;         // [nCells]
+    double *impsrT;       // [nCells]
+    double *matL, *matR;  // [nFaces] sweep coefficients
+    R *gnut;              // [nCells][3]
 };
 
 

@@ -4,6 +4,7 @@
 #pragma once
 #include "ofg_ctx.h"
 #include "ofg_kernels.cuh"
+#include "ofg_turb.cuh"
 
 namespace ofg {
 
@@ -63,6 +64,8 @@ KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
     A.res = c->d_res; A.dq = c->d_dq; A.dt = c->d_dt; A.invsr = c->d_invsr; A.vissr = c->d_vissr;
     A.bcq = c->d_bcq; A.grad = (R *)c->d_grad; A.lim = (R *)c->d_lim; A.partial = c->d_partial;
     A.scal = c->d_scal; A.fixlist = c->d_fix; A.fixcap = c->fixcap;
+    A.nut = c->d_nut; A.dnut = c->d_dnut; A.resT = c->d_resT; A.impsrT = c->d_impsrT;
+    A.matL = c->d_matL; A.matR = c->d_matR; A.gnut = (R *)c->d_gnut;
     return A;
 }
 
@@ -154,6 +157,54 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         OFG_LAUNCH(k_norm_partial<R>, nb, 256, s, A);
         OFG_LAUNCH(k_norm_final<R>, 1, 256, s, A, nb, (double *)nullptr);
         OFG_LAUNCH(k_norm_hist, 1, 32, s, c->d_scal, c->d_hist, c->histCap);
+        break;
+    }
+    case T_TURB_RHS: {
+        KArgs<R> A = make_args<R>(c, true);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, 0);
+        OFG_LAUNCH(k_turb_grad<R>, nblk(N, 128), 128, s, A);
+        OFG_LAUNCH(k_turb_rhs<R>, nblk(N, 128), 128, s, A);
+        break;
+    }
+    case T_TURB_LOWER: {
+        KArgs<R> A = make_args<R>(c, true);
+        int nl = int(c->lowOff.size()) - 1;
+        for (int l = 0; l < nl; ++l) {
+            int st = c->lowOff[l], cnt = c->lowOff[l + 1] - st;
+            OFG_LAUNCH(k_turb_lower<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_lowOrder, st, cnt);
+        }
+        break;
+    }
+    case T_TURB_UPPER: {
+        KArgs<R> A = make_args<R>(c, true);
+        int nl = int(c->upOff.size()) - 1;
+        for (int l = 0; l < nl; ++l) {
+            int st = c->upOff[l], cnt = c->upOff[l + 1] - st;
+            OFG_LAUNCH(k_turb_upper<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_upOrder, st, cnt);
+        }
+        break;
+    }
+    case T_TURB_UPDATE: {
+        KArgs<R> A = make_args<R>(c, true);
+        OFG_LAUNCH(k_turb_update<R>, nblk(N, 256), 256, s, A, 1);
+        break;
+    }
+    case T_TURB_BOUNDARY: {
+        KArgs<R> A = make_args<R>(c, true);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, 1);
+        break;
+    }
+    case T_TURB_BOUNDARY_CUR: {
+        KArgs<R> A = make_args<R>(c, true);
+        OFG_LAUNCH(k_turb_vist<R>, nblk(N, 256), 256, s, A);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, 1);
+        break;
+    }
+    case T_TURB_NORM: {
+        KArgs<R> A = make_args<R>(c, true);
+        int nb = 2 * 148;
+        OFG_LAUNCH(k_turb_norm_partial<R>, nb, 256, s, A);
+        OFG_LAUNCH(k_turb_norm_final<R>, 1, 256, s, A, nb, c->d_thist, c->histCap);
         break;
     }
     default:

@@ -1,0 +1,402 @@
+// Spalart-Allmaras solver kernels (TURB_SOLVER tasks).  Same gather
+// structure as the NS kernels: one thread per cell over its faces in
+// ascending face id, so every per-cell accumulation follows the reference's
+// face-loop order.  They read the NS state of the current buffer (already
+// relaxed in this outer iteration, as in the reference's StrongIter order).
+#pragma once
+#include "ofg_kernels.cuh"
+
+namespace ofg {
+
+// CalcTurbulentViscosity: UTurbSrcFlux::CalcVist1Equ + TurbSrcFlux::CalcCellVist1Equ
+// (codes/uturb/src/UTurbSrcFlux.cpp:220-241, codes/turb/src/TurbSrcFlux.cpp:279-290)
+__device__ __forceinline__ double sa_vist(const DevParams &P, double rho, double nuet, double vl) {
+    double olam = rho / (vl + SMALLD);
+    double xsi = nuet * olam;
+    double xsi3 = xsi * xsi * xsi;
+    double fv1 = xsi3 / (xsi3 + P.sa_cv13);
+    double v = fv1 * rho * nuet;
+    return fmin(vl * P.max_vis_ratio, v);
+}
+
+// TurbBcSolver face rules (codes/turb/src/TurbBcSolver.cpp:51-262); the
+// far-field normal is scaled by GCom::faceOuterNormal, which the reference
+// never assigns (zero-initialised global), so only the sound speeds decide.
+template <typename R>
+__global__ void __launch_bounds__(256) k_turb_bc(KArgs<R> A, int withVist) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= A.M.nBFaces) return;
+    int bt = A.M.bcType[f], l = A.M.lc[f];
+    int g = A.M.nCells + f;
+    double s = A.nut[l], t = s;
+    if (bt == BC_SOLID) t = -s;
+    else if (bt == BC_INFLOW) t = A.P.nut_inf;
+    else if (bt == BC_FAR) {
+        const double *ql = A.q + (size_t)l * REC;
+        double xn = double(A.G.xfn[f]) * 0, yn = double(A.G.yfn[f]) * 0, zn = double(A.G.zfn[f]) * 0;
+        const double *inf = A.P.inflow;
+        double vnref = xn * inf[IU] + yn * inf[IV] + zn * inf[IW] - 0.0;
+        double vnin = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - 0.0;
+        double cref = sqrt(fabs(A.P.gama * inf[IP] / inf[IR]));
+        double cin = sqrt(fabs(A.P.gama * ql[IP] / ql[IR]));
+        double velin = sqrt(SQR3(ql[IU], ql[IV], ql[IW]));
+        if (velin > cin) {
+            t = vnin >= 0.0 ? s : A.P.nut_inf;
+        } else {
+            double gamm1 = A.P.gama - 1.0;
+            double riemp = vnin + 2.0 * cin / gamm1;
+            double riemm = vnref - 2.0 * cref / gamm1;
+            double vnb = 0.5 * (riemp + riemm);
+            t = vnb >= 0.0 ? s : A.P.nut_inf;
+        }
+    }
+    A.nut[g] = t;
+    if (withVist) {   // UTurbSrcFlux::SetGhostCellVist
+        double *qg = const_cast<double *>(A.q) + (size_t)g * REC;
+        qg[IMT] = A.q[(size_t)l * REC + IMT];
+    }
+}
+
+// gradient of nu~ (uturb_grad: Green-Gauss cell-weighted, or the option of the
+// NS gradients); ghosts carry the interior gradient
+template <typename R>
+__global__ void __launch_bounds__(128) k_turb_grad(KArgs<R> A) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.M.nCells) return;
+    R gx = 0, gy = 0, gz = 0;
+    int b = A.M.c2f_off[c], e = A.M.c2f_off[c + 1];
+    if (A.P.igrad == 2) {
+        R a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, b1 = 0, b2 = 0, b3 = 0;
+        R vc = R(A.nut[c]);
+        for (int k = b; k < e; ++k) {
+            int f = A.M.c2f[k];
+            int nb = other_cell(A.M.lc[f], A.M.rc[f], c);
+            R dx = A.G.xcc[nb] - A.G.xcc[c], dy = A.G.ycc[nb] - A.G.ycc[c], dz = A.G.zcc[nb] - A.G.zcc[c];
+            R w = R(1) / (dx * dx + dy * dy + dz * dz);
+            R dv = R(A.nut[nb]) - vc;
+            a11 += w * dx * dx; a12 += w * dx * dy; a13 += w * dx * dz;
+            a22 += w * dy * dy; a23 += w * dy * dz; a33 += w * dz * dz;
+            b1 += w * dx * dv; b2 += w * dy * dv; b3 += w * dz * dv;
+        }
+        if (A.P.dim == 2) {
+            R id = R(1) / (a11 * a22 - a12 * a12);
+            gx = (a22 * b1 - a12 * b2) * id; gy = (a11 * b2 - a12 * b1) * id; gz = R(0);
+        } else {
+            R c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
+            R c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
+            R id = R(1) / (a11 * c11 + a12 * c12 + a13 * c13);
+            gx = (c11 * b1 + c12 * b2 + c13 * b3) * id;
+            gy = (c12 * b1 + c22 * b2 + c23 * b3) * id;
+            gz = (c13 * b1 + c23 * b2 + c33 * b3) * id;
+        }
+    } else {
+        for (int k = b; k < e; ++k) {
+            int f = A.M.c2f[k];
+            int l = A.M.lc[f], r = A.M.rc[f];
+            R cl, cr;
+            if (A.P.igrad == 1) { cl = R(0.5); cr = R(0.5); }
+            else {
+                R dxl = A.G.xfc[f] - A.G.xcc[l], dyl = A.G.yfc[f] - A.G.ycc[l], dzl = A.G.zfc[f] - A.G.zcc[l];
+                R dxr = A.G.xfc[f] - A.G.xcc[r], dyr = A.G.yfc[f] - A.G.ycc[r], dzr = A.G.zfc[f] - A.G.zcc[r];
+                R delt1 = Rsqrt(SQR3(dxl, dyl, dzl)), delt2 = Rsqrt(SQR3(dxr, dyr, dzr));
+                R delta = R(1) / (delt1 + delt2 + small_v<R>());
+                cl = delt2 * delta; cr = delt1 * delta;
+            }
+            R value = (A.P.igrad == 1) ? R(0.5) * (R(A.nut[l]) + R(A.nut[r])) : cl * R(A.nut[l]) + cr * R(A.nut[r]);
+            R ar = A.G.area[f];
+            R fx = A.G.xfn[f] * ar, fy = A.G.yfn[f] * ar, fz = A.G.zfn[f] * ar;
+            if (l == c) { gx += fx * value; gy += fy * value; gz += fz * value; }
+            else        { gx -= fx * value; gy -= fy * value; gz -= fz * value; }
+        }
+        R ovol = R(1) / A.G.vol[c];
+        gx *= ovol; gy *= ovol; gz *= ovol;
+    }
+    R *o = A.gnut + (size_t)c * 3;
+    o[0] = gx; o[1] = gy; o[2] = gz;
+}
+
+template <typename R>
+__device__ __forceinline__ R calc_angle(R dx, R dy, R dz, R dist) {
+    // VisGradGeom::CalcAngle, codes/usolver/src/VisGrad.cpp:62-68
+    R result = dist / (Rsqrt(SQR3(dx, dy, dz)) + small_v<R>());
+    if (result > R(1)) result = R(1);
+    if (result < R(-1)) result = R(-1);
+    return R(asin(double(result)) * 180.0 / 3.141592653589793);
+}
+
+// UPDATE_RESIDUALS for SA: TurbCalcRHS (codes/turb/src/TurbRhs.cpp:57-70):
+// spectrum (UTurbSpectrum::CalcSpectrum1Equ + TurbSpectrum::CalcFaceSpectrum1Equ,
+// codes/uturb/src/UTurbSpectrum.cpp:132-240, codes/turb/src/TurbSpectrum.cpp:75-134),
+// source (TurbCom::CalcSrcSa, codes/turb/src/TurbCom.cpp:771-881), first-order
+// convection (TurbInvFlux::RoeFlux, codes/turb/src/TurbInvFlux.cpp:78-98) and
+// diffusion with the VIS_TEST face gradient (UTurbVisFlux, codes/uturb/src/UTurbVisFlux.cpp:64-407).
+template <typename R>
+__global__ void __launch_bounds__(128) k_turb_rhs(KArgs<R> A) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.M.nCells) return;
+    const DevParams &P = A.P;
+    const double half = 0.5;
+    int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
+    const double *qc = A.q + (size_t)c * REC;
+    double vol = double(A.G.vol[c]);
+    // ---- spectral radius and sweep coefficients ----
+    double imp = 0.0;
+    imp += (1.0 / (A.dt[c] * P.turb_cfl_ratio)) * vol;
+    for (int k = b; k < en; ++k) {
+        int f = A.M.c2f[k];
+        int l = A.M.lc[f], r = A.M.rc[f];
+        const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
+        double xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f], ar = A.G.area[f];
+        double vnl = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - 0.0;
+        double vnr = xn * qr[IU] + yn * qr[IV] + zn * qr[IW] - 0.0;
+        double absVn = fabs(half * (vnl + vnr));
+        double r1 = 0.0, m1 = 0.0, m2 = 0.0;
+        r1 += ar * half * absVn;
+        m1 += ar * half * (-vnl - absVn);
+        m2 += ar * half * (vnr - absVn);
+        double orl = 1.0 / (ql[IR] + SMALLD), orr = 1.0 / (qr[IR] + SMALLD);
+        double nuet1 = ql[IML] * orl + A.nut[l], nuet2 = qr[IML] * orr + A.nut[r];
+        double nueff = fabs(half * (nuet1 + nuet2));
+        double ovol = 1.0 / (half * (double(A.G.vol[l]) + double(A.G.vol[r])));
+        double d = P.oreynolds * ovol * (P.sa_osigma * nueff * (ar * ar));
+        r1 += d;
+        m1 += -d;
+        m2 += -d;
+        imp += r1;
+        if (l == c) { A.matL[f] = m1; A.matR[f] = m2; }
+    }
+    // ---- source ----
+    const R *gq = A.grad + (size_t)c * 18;
+    double dudx = gq[IU * 3], dudy = gq[IU * 3 + 1], dudz = gq[IU * 3 + 2];
+    double dvdx = gq[IV * 3], dvdy = gq[IV * 3 + 1], dvdz = gq[IV * 3 + 2];
+    double dwdx = gq[IW * 3], dwdy = gq[IW * 3 + 1], dwdz = gq[IW * 3 + 2];
+    double rho = qc[IR], nuet = A.nut[c], vl = qc[IML];
+    double olam = rho / (vl + SMALLD);
+    double ls = A.M.walldist[c];
+    double od2 = 1.0 / (ls * ls);
+    double work1 = dudx + dvdy + dwdz;
+    double work2 = SQR3(dudx, dudy, dudz);
+    double work3 = SQR3(dudy + dvdx, dvdz + dwdy, dwdx + dudz);
+    double work4 = sqrt(SQR3(dwdy - dvdz, dudz - dwdx, dvdx - dudy));
+    if (P.iprod_sa == 1) {
+        double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
+        work4 = sqrt(fabs(stp));
+    } else if (P.iprod_sa == 4) {
+        double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
+        double str = work4;
+        work4 = str - 2.0 * fmax(0.0, str - sqrt(fabs(stp)));
+    } else if (P.iprod_sa == 5) {
+        double stp = fabs(2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1);
+        double str = work4;
+        work4 = str * (1.0 - fmax(0.0, (str * str - stp) / (str * str + stp + SMALLD)));
+    }
+    double str = work4;
+    double xsi = nuet * olam + SMALLD;
+    double xsi3 = xsi * xsi * xsi;
+    double fv1 = xsi3 / (xsi3 + P.sa_cv13);
+    double fv2 = 1.0 - xsi / (1.0 + xsi * fv1);
+    double rs = nuet * P.sa_okarm2 * od2 * P.oreynolds;
+    double nuetRs = nuet * rs;
+    double sBar = rs * fv2;
+    double omega = str;
+    double stdv;
+    if (sBar >= -P.sa_sac2 * omega) stdv = omega + sBar;
+    else {
+        double term1 = (P.sa_sac2 * P.sa_sac2 * omega + P.sa_sac3 * sBar);
+        double term2 = (P.sa_sac3 - 2 * P.sa_sac2) * omega - sBar;
+        stdv = omega + omega * term1 / term2;
+    }
+    double ostd = 1.0 / (stdv + SMALLD);
+    double rr = fmin(rs * ostd, 10.0);
+    double r5 = pow(rr, 5.0);
+    double g = rr + P.sa_cw2 * (r5 * rr - rr);
+    double g6 = pow(g, 6.0);
+    double fw = g * pow((1.0 + P.sa_cw36) / (g6 + P.sa_cw36), 1.0 / 6.0);
+    double xsi2 = xsi * xsi;
+    double ft2 = P.ft2_flag ? P.sa_ct3 * exp(-P.sa_ct4 * xsi2) * 1.0 : 0.0;
+    const R *gn = A.gnut + (size_t)c * 3;
+    double grd2 = SQR3(double(gn[0]), double(gn[1]), double(gn[2]));
+    double prod = P.sa_cb1 * (1.0 - ft2) * stdv * nuet;
+    double diff = P.sa_cb2s * grd2 * P.oreynolds;
+    double dest = (P.sa_cw1k * fw - P.sa_cb1 * ft2) * nuetRs;
+    diff = fmin(P.rprod * prod, diff);
+    double srcTerm = prod - dest;
+    srcTerm += diff;
+    double q1x = fv1 / (xsi + SMALLD), q1y = 1.0 + xsi * fv1;
+    double dfv2dk = (3.0 * P.sa_cv13 * (q1x * q1x) - 1.0) / (q1y * q1y);
+    double dsdnu = P.oreynolds * P.sa_okarm2 * od2 * (fv2 + xsi * dfv2dk);
+    double dfwdg = fw / (g + SMALLD) * (1.0 - g6 / (g6 + P.sa_cw36));
+    double dgdr = 1.0 + P.sa_cw2 * (6.0 * r5 - 1.0);
+    double drdnu = P.oreynolds * P.sa_okarm2 * od2 * ostd * (1.0 - nuet * ostd * dsdnu);
+    double dfwdnu = dfwdg * dgdr * drdnu;
+    double prod0 = P.sa_cb1 * (1.0 - ft2) * stdv;
+    double dest0 = (P.sa_cw1 * fw - P.sa_cb1 * ft2 * P.sa_okarm2) * nuet * od2 * P.oreynolds;
+    double prodp = P.sa_cb1 * ((1.0 - ft2) * dsdnu);
+    double destp = (P.sa_cw1 * (fw + dfwdnu * nuet) - P.sa_cb1 * ft2 * P.sa_okarm2) * od2 * P.oreynolds;
+    double prde0 = prod0 - dest0, prdep = prodp - destp;
+    double part1 = -half * (prde0 - fabs(prde0));
+    double part2 = -half * (prdep - fabs(prdep)) * nuet;
+    imp += (part1 + part2) * vol;
+    double acc = -0.0;
+    acc += srcTerm * vol;
+    // ---- first-order convection with the NS face states ----
+    for (int k = b; k < en; ++k) {
+        int f = A.M.c2f[k];
+        int l = A.M.lc[f], r = A.M.rc[f];
+        const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
+        double t1 = A.nut[l], t2 = A.nut[r];
+        double u1 = ql[IU], v1 = ql[IV], w1 = ql[IW], u2 = qr[IU], v2 = qr[IV], w2 = qr[IW];
+        if (f < A.M.nBFaces) {
+            double tm = half * (A.nut[l] + A.nut[r]);
+            t1 = t2 = tm;
+            if (A.M.bcType[f] == BC_SOLID) {
+                const double *bq = A.bcq + (size_t)f * NEQ;
+                u1 = u2 = bq[IU]; v1 = v2 = bq[IV]; w1 = w2 = bq[IW];
+            } else {
+                u1 = u2 = half * (ql[IU] + qr[IU]);
+                v1 = v2 = half * (ql[IV] + qr[IV]);
+                w1 = w2 = half * (ql[IW] + qr[IW]);
+            }
+        }
+        double xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f];
+        double vnl = xn * u1 + yn * v1 + zn * w1 - 0.0;
+        double vnr = xn * u2 + yn * v2 + zn * w2 - 0.0;
+        double coef_l = half * (vnl + fabs(vnl)) * 1.0;
+        double coef_r = half * (vnr - fabs(vnr)) * 1.0;
+        double v = double(A.G.area[f]) * (coef_l * t1 + coef_r * t2);
+        if (l == c) acc -= v; else acc += v;
+    }
+    // ---- diffusion ----
+    for (int k = b; k < en; ++k) {
+        int f = A.M.c2f[k];
+        int l = A.M.lc[f], r = A.M.rc[f];
+        R xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f];
+        R q1 = R(A.nut[l]), q2 = R(A.nut[r]);
+        R q11 = q1, q22 = q2, qf = R(0.5) * (q1 + q2);
+        R dxl = A.G.xcc[l] - A.G.xfc[f], dyl = A.G.ycc[l] - A.G.yfc[f], dzl = A.G.zcc[l] - A.G.zfc[f];
+        R dxr = A.G.xcc[r] - A.G.xfc[f], dyr = A.G.ycc[r] - A.G.yfc[f], dzr = A.G.zcc[r] - A.G.zfc[f];
+        R d1 = xn * dxl + yn * dyl + zn * dzl;
+        R d2 = xn * dxr + yn * dyr + zn * dzr;
+        R angle1 = calc_angle(dxl, dyl, dzl, -d1);
+        R angle2 = calc_angle(dxr, dyr, dzr, d2);
+        R dqdn = R(0);
+        if (angle1 > R(20) && angle2 > R(20)) {
+            const R *g1 = A.gnut + (size_t)l * 3;
+            const R *g2 = A.gnut + (size_t)grad_cell(A.M, r) * 3;
+            q11 += g1[0] * (xn * d1 - dxl) + g1[1] * (yn * d1 - dyl) + g1[2] * (zn * d1 - dzl);
+            q22 += g2[0] * (xn * d2 - dxr) + g2[1] * (yn * d2 - dyr) + g2[2] * (zn * d2 - dzr);
+            qf = R(0.5) * (q1 + q2);
+        }
+        if (angle1 > R(0) && angle2 > R(0) && Rabs(d1) > small_v<R>() && Rabs(d2) > small_v<R>()) {
+            R dtmp = d1 * d1 + d2 * d2;
+            R c1 = d1 * d1 / dtmp, c2 = R(1) - c1;
+            if (f < A.M.nBFaces) { c1 = R(1); c2 = R(0); }
+            dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
+        }
+        const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
+        double orl = 1.0 / (ql[IR] + SMALLD), orr = 1.0 / (qr[IR] + SMALLD);
+        double visl_nv = half * (ql[IML] * orl + qr[IML] * orr);
+        double vist_nv = half * (A.nut[l] + A.nut[r]);
+        double comVis = (visl_nv + vist_nv) * P.sa_osigma;
+        double flux = -P.oreynolds * comVis * double(dqdn) * double(A.G.area[f]);
+        if (l == c) acc -= flux; else acc += flux;
+    }
+    A.impsrT[c] = imp;
+    A.resT[c] = acc;
+}
+
+// LU-SGS sweeps of the SA equation (codes/uturb/src/UTurbLusgs.cpp:90-300,
+// codes/turb/src/TurbLusgs.cpp:123-260): dfj = matrix * dq_j
+template <typename R>
+__global__ void __launch_bounds__(128) k_turb_lower(KArgs<R> A, const int *order, int start, int count) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    int c = order[start + t];
+    double rhs0 = 0.0;
+    for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
+        int f = A.M.c2f[k];
+        int l = A.M.lc[f], r = A.M.rc[f];
+        if (l > c || r > c) continue;
+        bool swap = (r == c);
+        rhs0 += (swap ? A.matL[f] : A.matR[f]) * A.dnut[swap ? l : r];
+    }
+    A.dnut[c] = (A.resT[c] - rhs0) / A.impsrT[c];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order, int start, int count) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    int c = order[start + t];
+    double rhs0 = 0.0;
+    for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
+        int f = A.M.c2f[k];
+        if (f < A.M.nBFaces) continue;   // ghost increments are zero
+        int l = A.M.lc[f], r = A.M.rc[f];
+        if (l < c || r < c) continue;
+        bool swap = (r == c);
+        rhs0 += (swap ? A.matL[f] : A.matR[f]) * A.dnut[swap ? l : r];
+    }
+    A.dnut[c] += (-rhs0) / A.impsrT[c];
+}
+
+// UPDATE_FLOWFIELD (TurbUpdate::CalcFlowField1Equ, crelax = 1) fused with the
+// interior half of CALC_BOUNDARY (the eddy viscosity of the new nu~)
+template <typename R>
+__global__ void __launch_bounds__(256) k_turb_update(KArgs<R> A, int withVist) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.M.nCells) return;
+    double qOld = A.nut[c], qNew = qOld + A.dnut[c];
+    double v = (1.0 - 1.0) * qOld + 1.0 * qNew;
+    A.nut[c] = v;
+    if (withVist) {
+        double *qc = const_cast<double *>(A.q) + (size_t)c * REC;
+        qc[IMT] = sa_vist(A.P, qc[IR], v, qc[IML]);
+    }
+}
+
+// interior eddy viscosity only (CALC_BOUNDARY without an update)
+template <typename R>
+__global__ void __launch_bounds__(256) k_turb_vist(KArgs<R> A) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.M.nCells) return;
+    double *qc = const_cast<double *>(A.q) + (size_t)c * REC;
+    qc[IMT] = sa_vist(A.P, qc[IR], A.nut[c], qc[IML]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_turb_norm_partial(KArgs<R> A) {
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.M.nCells; c += gridDim.x * blockDim.x)
+        acc += A.resT[c] * A.resT[c];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) A.partial[blockIdx.x] = s[0];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_turb_norm_final(KArgs<R> A, int nPartial, double *hist, int cap) {
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nPartial; i += blockDim.x) acc += A.partial[i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double rms = sqrt(s[0] / A.M.nCells);
+        A.scal[S_TNORM] = rms;
+        int n = int(A.scal[S_THISTN]);
+        if (n < cap) hist[n] = rms;
+        A.scal[S_THISTN] = double(n + 1);
+    }
+}
+
+}  // namespace ofg

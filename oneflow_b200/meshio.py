@@ -198,8 +198,8 @@ def write_case(case_dir: str, mesh: Mesh, params: dict, max_steps: int) -> None:
             ("int", "turbulentResidualSmoothOrNot", 0), ("int", "turbulentSourceModel", 0),
             ("int", "ft2_flag", p["ft2_flag"]), ("int", "turb_ilim", -1), ("int", "tns_ilim", -1),
             ("Real", "turbulentRelaxationCoefficient", 1.0), ("Real", "coefficientOfMinimumTurbulentQuantity", 1.0e-5),
-            ("Real", "ref_sa", 0.1), ("Real", "ref_sst", 0.001), ("int", "iturb_visflux", 2),
-            ("int", "iprod_sa", p["iprod_sa"]), ("int", "iprod_sst", 1), ("Real", "max_vis_ratio", 1.0e6),
+            ("Real", "ref_sa", p["ref_sa"]), ("Real", "ref_sst", 0.001), ("int", "iturb_visflux", 2),
+            ("int", "iprod_sa", p["iprod_sa"]), ("int", "iprod_sst", 1), ("Real", "max_vis_ratio", p["max_vis_ratio"]),
             ("Real", "rprod", p["rprod"]), ("int", "monitorMaximumTurbulentViscosityCoefficient", 0),
             ("int", "numberOfAbnormalTurbulentCellsLimit", 1), ("Real", "turb_cfl_ratio", p["turb_cfl_ratio"]),
             ("string", "turbresFile", '"results/turbres.dat"'), ("string", "turbflowFile", '"restart/turbflow.dat"'),

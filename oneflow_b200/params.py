@@ -12,12 +12,12 @@ _INT = ["dimension", "ischeme", "ilim", "igrad", "ieigenfix", "timestepModel", "
         "precision", "venkat_kh3"]
 _DBL = ["vencat_coef", "centropy1", "centropy2", "cflst", "cfled", "max_time_ratio", "global_dt", "mach_ref",
         "aoa_degree", "sideslip_degree", "reynolds", "gama_ref", "prl", "prt", "tref_dim", "twall_dim",
-        "inflow_viscosity", "rprod", "turb_cfl_ratio"]
+        "inflow_viscosity", "rprod", "turb_cfl_ratio", "ref_sa", "max_vis_ratio"]
 
 
 class OfgParams(C.Structure):
     _fields_ = ([(n, C.c_int) for n in _INT] + [("reserved_i", C.c_int * 7)] +
-                [(n, C.c_double) for n in _DBL] + [("reserved_d", C.c_double * 8)])
+                [(n, C.c_double) for n in _DBL] + [("reserved_d", C.c_double * 6)])
 
 
 def defaults(**kw) -> OfgParams:
@@ -61,6 +61,8 @@ def defaults(**kw) -> OfgParams:
     p.inflow_viscosity = 0.01
     p.rprod = 1.0
     p.turb_cfl_ratio = 1.0
+    p.ref_sa = 0.1
+    p.max_vis_ratio = 1.0e6
     for k, v in kw.items():
         if not hasattr(p, k):
             raise KeyError(k)

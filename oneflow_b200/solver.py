@@ -121,9 +121,11 @@ class Solver:
         self._check(self.L.ofg_upload_state(self.h, tid, np.ascontiguousarray(q, np.float64).ravel()))
 
     def state(self, tid: int = NS_SOLVER) -> np.ndarray:
-        out = np.empty(5 * self.nT, np.float64)
+        """[5][nCells+nBFaces] primitive NS state, or [nCells+nBFaces] nu~ for tid 1."""
+        ne = 5 if tid == NS_SOLVER else 1
+        out = np.empty(ne * self.nT, np.float64)
         self._check(self.L.ofg_download_state(self.h, tid, out))
-        return out.reshape(5, self.nT)
+        return out.reshape(5, self.nT) if ne == 5 else out
 
     # ---- tasks ----
     def task(self, name: str, tid: int = NS_SOLVER):

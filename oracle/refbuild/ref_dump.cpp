@@ -9,6 +9,7 @@
 #include "Zone.h"
 #include "ZoneState.h"
 #include "UnsGrid.h"
+#include "CellMesh.h"
 #include "DataBase.h"
 #include "HXArray.h"
 #include <cstdio>
@@ -40,6 +41,11 @@ void OfgRefDump()
     if (!fp) return;
     int nCells = grid->nCells;
     int nTCell = nCells + grid->nBFaces;
+    // the wall distance (CellMesh::dist, one value per interior cell)
+    RealField &dist = grid->cellMesh->dist;
+    MRField distField(1, nTCell);
+    for (int i = 0; i < nCells && i < (int)dist.size(); ++i) distField[0][i] = dist[i];
+    if (turb) fields.push_back({"walldist", &distField});
     int nf = (int)fields.size();
     std::fwrite(&nCells, 4, 1, fp);
     std::fwrite(&nTCell, 4, 1, fp);

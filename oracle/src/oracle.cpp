@@ -60,7 +60,8 @@ struct Oracle {
     double sutherland_ts = 0;
     double cfl = 0;
     long outerSteps = 0;
-    std::vector<double> resHist;      // per outer step: 5 NS RMS (+1 SA RMS if present)
+    std::vector<double> resHist;      // per outer step: 5 NS RMS
+    std::vector<double> turbHist;     // per outer step: SA RMS
     std::string err;
 
     // ======================= mesh & metrics =======================
@@ -374,6 +375,10 @@ struct Oracle {
         outerSteps = 0;
         for (int e = 0; e < NEQ; ++e) std::fill(q[e].begin(), q[e].end(), inflow[e]);
         calcBoundary();
+        if (turb()) {   // UTurbRestart::InitRestart + TurbInitFinal
+            std::fill(nut.begin(), nut.end(), p.ref_sa);
+            turbBoundary();
+        }
     }
 
     // ======================= CALC_TIME_STEP =======================
@@ -1004,6 +1009,315 @@ struct Oracle {
         }
     }
 
+    // ======================= Spalart-Allmaras solver =======================
+    // constants: TurbCom::InitConst (codes/turb/src/TurbCom.cpp:110-350)
+    struct SaConst {
+        double karm = 0.41, karm2, okarm2, cb1 = 0.1355, cb2 = 0.622, cv1 = 7.1, cv13, cw2 = 0.3, cw3 = 2.0, cw36;
+        double ct3 = 1.2, ct4 = 0.5, sigma = 2.0 / 3.0, osigma, cw1, sac2 = 0.7, sac3 = 0.9, cb2s, cw1k;
+        SaConst() {
+            karm2 = karm * karm; okarm2 = 1.0 / karm2; cv13 = cv1 * cv1 * cv1; cw36 = std::pow(cw3, 6);
+            osigma = 1.0 / sigma; cw1 = cb1 * okarm2 + (1.0 + cb2) / sigma; cb2s = osigma * cb2; cw1k = cw1 * karm2;
+        }
+    } sa;
+    std::vector<double> matL, matR;
+    bool turb() const { return p.vismodel >= 3; }
+
+    // CalcTurbulentViscosity -> UTurbSrcFlux::CalcVist (codes/uturb/src/UTurbSrcFlux.cpp:101-243),
+    // TurbSrcFlux::CalcCellVist1Equ (codes/turb/src/TurbSrcFlux.cpp:279-290)
+    void calcVist() {
+        for (int c = 0; c < nCells; ++c) {
+            double rho = q[IR][c], nuet = nut[c], vl = visl[c];
+            double olam = rho / (vl + SMALL);
+            double xsi = nuet * olam;
+            double xsi3 = xsi * xsi * xsi;
+            double fv1 = xsi3 / (xsi3 + sa.cv13);
+            double v = fv1 * rho * nuet;
+            vist[c] = MINd(vl * p.max_vis_ratio, v);
+        }
+        for (int f = 0; f < nBFaces; ++f) vist[rc[f]] = vist[lc[f]];
+    }
+    // TurbBcSolver (codes/turb/src/TurbBcSolver.cpp:51-262) via UTurbBcSolver::CalcBc
+    void turbBc() {
+        for (int f = 0; f < nBFaces; ++f) {
+            int bt = bcType[f], l = lc[f], r = rc[f];
+            double s = nut[l], t = s;
+            if (bt == OFG_BC_SOLID_SURFACE) t = -s;
+            else if (bt == OFG_BC_INFLOW) t = p.ref_sa;
+            else if (bt == OFG_BC_FARFIELD) {
+                // the normal is scaled by gcom.faceOuterNormal, a member of a
+                // global object that is never assigned (zero-initialised), so
+                // the turbulent far-field decision sees a zero normal velocity
+                // (codes/turb/src/TurbBcSolver.cpp:154-156, codes/global/include/Com.h:38)
+                double xn = xfn[f] * 0, yn = yfn[f] * 0, zn = zfn[f] * 0;
+                double rin = q[IR][l], uin = q[IU][l], vin = q[IV][l], win = q[IW][l], pin = q[IP][l];
+                double vnref = xn * inflow[IU] + yn * inflow[IV] + zn * inflow[IW] - 0.0;
+                double vnin = xn * uin + yn * vin + zn * win - 0.0;
+                double cref = std::sqrt(std::fabs(p.gama_ref * inflow[IP] / inflow[IR]));
+                double cin = std::sqrt(std::fabs(p.gama_ref * pin / rin));
+                double velin = DIST3(uin, vin, win);
+                if (velin > cin) {
+                    t = vnin >= 0.0 ? s : p.ref_sa;
+                } else {
+                    double gamm1 = p.gama_ref - 1.0;
+                    double riemp = vnin + 2.0 * cin / gamm1;
+                    double riemm = vnref - 2.0 * cref / gamm1;
+                    double vnb = half * (riemp + riemm);
+                    t = vnb >= 0.0 ? s : p.ref_sa;
+                }
+            }
+            nut[r] = t;
+        }
+    }
+    void turbBoundary() { calcVist(); turbBc(); }
+
+    // UTurbSpectrum::CalcSpectrum1Equ + TurbSpectrum::CalcFaceSpectrum1Equ
+    // (codes/uturb/src/UTurbSpectrum.cpp:132-240, codes/turb/src/TurbSpectrum.cpp:75-134)
+    void turbSpectrum() {
+        std::fill(impsrT.begin(), impsrT.end(), 0.0);
+        matL.assign(nFaces, 0.0); matR.assign(nFaces, 0.0);
+        for (int c = 0; c < nCells; ++c) {
+            double ts = timestep[c] * p.turb_cfl_ratio;
+            impsrT[c] += (1.0 / ts) * vol[c];
+        }
+        for (int f = 0; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            double r1 = 0, r2 = 0, m1 = 0, m2 = 0;
+            double vnl = xfn[f] * q[IU][l] + yfn[f] * q[IV][l] + zfn[f] * q[IW][l] - 0.0;
+            double vnr = xfn[f] * q[IU][r] + yfn[f] * q[IV][r] + zfn[f] * q[IW][r] - 0.0;
+            double vnRel = half * (vnl + vnr);
+            double absVn = std::fabs(vnRel);
+            r1 += area[f] * half * absVn;
+            r2 += area[f] * half * absVn;
+            m1 += area[f] * half * (-vnl - absVn);
+            m2 += area[f] * half * (vnr - absVn);
+            double orl = 1.0 / (q[IR][l] + SMALL), orr = 1.0 / (q[IR][r] + SMALL);
+            double nuet1 = visl[l] * orl + nut[l], nuet2 = visl[r] * orr + nut[r];
+            double nueff = std::fabs(half * (nuet1 + nuet2));
+            double cv = half * (vol[l] + vol[r]);
+            double ovol = 1.0 / cv;
+            double areaS2 = area[f] * area[f];
+            r1 += oreynolds * ovol * (sa.osigma * nueff * areaS2);
+            r2 += oreynolds * ovol * (sa.osigma * nueff * areaS2);
+            m1 += -oreynolds * ovol * (sa.osigma * nueff * areaS2);
+            m2 += -oreynolds * ovol * (sa.osigma * nueff * areaS2);
+            impsrT[l] += r1; impsrT[r] += r2;
+            matL[f] += m1; matR[f] += m2;
+        }
+    }
+
+    // TurbCom::CalcSrcSa (codes/turb/src/TurbCom.cpp:771-881) per cell, added as
+    // UTurbSrcFlux::Update1Equ does (codes/uturb/src/UTurbSrcFlux.cpp:315-319)
+    void turbSource() {
+        gradGG(nut, dnutdx, dnutdy, dnutdz);   // uturb_grad (GG cell-weighted)
+        for (int c = 0; c < nCells; ++c) {
+            double dudx = dqdx[IU][c], dudy = dqdy[IU][c], dudz = dqdz[IU][c];
+            double dvdx = dqdx[IV][c], dvdy = dqdy[IV][c], dvdz = dqdz[IV][c];
+            double dwdx = dqdx[IW][c], dwdy = dqdy[IW][c], dwdz = dqdz[IW][c];
+            double rho = q[IR][c], nuet = nut[c], vl = visl[c];
+            double olam = rho / (vl + SMALL);
+            double ls = walldist[c];
+            double d2 = ls * ls, od2 = 1.0 / d2;
+            // CalcWorkVar / CalcSaProd, TurbCom.cpp:429-466
+            double work1 = dudx + dvdy + dwdz;
+            double work2 = SQR3(dudx, dudy, dudz);
+            double work3 = SQR3(dudy + dvdx, dvdz + dwdy, dwdx + dudz);
+            double work4 = DIST3(dwdy - dvdz, dudz - dwdx, dvdx - dudy);
+            if (p.iprod_sa == 1) {
+                double stp = 2.0 * work2 + work3 - two3rd * work1 * work1;
+                work4 = std::sqrt(std::fabs(stp));
+            } else if (p.iprod_sa == 4) {
+                double stp = 2.0 * work2 + work3 - two3rd * work1 * work1;
+                double str = work4;
+                work4 = str - 2.0 * MAXd(0.0, str - std::sqrt(std::fabs(stp)));
+            } else if (p.iprod_sa == 5) {
+                double stp = 2.0 * work2 + work3 - two3rd * work1 * work1;
+                double str = work4;
+                stp = std::fabs(stp);
+                work4 = str * (1.0 - MAXd(0.0, (str * str - stp) / (str * str + stp + SMALL)));
+            }
+            double str = work4;
+            double xsi = nuet * olam + SMALL;
+            double xsi3 = xsi * xsi * xsi;
+            double fv1 = xsi3 / (xsi3 + sa.cv13);
+            double fv2 = 1.0 - xsi / (1.0 + xsi * fv1);
+            double rs = nuet * sa.okarm2 * od2 * oreynolds;
+            double nuetRs = nuet * rs;
+            double sBar = rs * fv2;
+            double omega = str;
+            double std_;
+            if (sBar >= -sa.sac2 * omega) {
+                std_ = omega + sBar;
+            } else {
+                double term1 = (sa.sac2 * sa.sac2 * omega + sa.sac3 * sBar);
+                double term2 = (sa.sac3 - 2 * sa.sac2) * omega - sBar;
+                std_ = omega + omega * term1 / term2;
+            }
+            double ostd = 1.0 / (std_ + SMALL);
+            double r = rs * ostd;
+            r = MINd(r, 10.0);
+            double r5 = std::pow(r, 5);
+            double g = r + sa.cw2 * (r5 * r - r);
+            double g6 = std::pow(g, 6);
+            double or6 = 1.0 / 6.0;
+            double fw = g * std::pow((1.0 + sa.cw36) / (g6 + sa.cw36), or6);
+            double xsi2 = xsi * xsi;
+            double ft2 = 0.0;
+            if (p.ft2_flag) ft2 = sa.ct3 * std::exp(-sa.ct4 * xsi2) * 1.0;
+            double grd2 = SQR3(dnutdx[c], dnutdy[c], dnutdz[c]);
+            double prod = sa.cb1 * (1.0 - ft2) * std_ * nuet;
+            double diff = sa.cb2s * grd2 * oreynolds;
+            double dest = (sa.cw1k * fw - sa.cb1 * ft2) * nuetRs;
+            diff = MINd(p.rprod * prod, diff);
+            double srcTerm = prod - dest;
+            srcTerm += diff;
+            double dfv2dk = (3.0 * sa.cv13 * std::pow(fv1 / (xsi + SMALL), 2) - 1.0) / std::pow(1.0 + xsi * fv1, 2);
+            double dsdnu = oreynolds * sa.okarm2 * od2 * (fv2 + xsi * dfv2dk);
+            double dfwdg = fw / (g + SMALL) * (1.0 - g6 / (g6 + sa.cw36));
+            double dgdr = 1.0 + sa.cw2 * (6.0 * r5 - 1.0);
+            double drdnu = oreynolds * sa.okarm2 * od2 * ostd * (1.0 - nuet * ostd * dsdnu);
+            double dfwdnu = dfwdg * dgdr * drdnu;
+            double prod0 = sa.cb1 * (1.0 - ft2) * std_;
+            double dest0 = (sa.cw1 * fw - sa.cb1 * ft2 * sa.okarm2) * nuet * od2 * oreynolds;
+            double prodp = sa.cb1 * ((1.0 - ft2) * dsdnu);
+            double destp = (sa.cw1 * (fw + dfwdnu * nuet) - sa.cb1 * ft2 * sa.okarm2) * od2 * oreynolds;
+            double prde0 = prod0 - dest0, prdep = prodp - destp;
+            double part1 = -half * (prde0 - std::fabs(prde0));
+            double part2 = -half * (prdep - std::fabs(prdep)) * nuet;
+            double spec = part1 + part2;
+            impsrT[c] += spec * vol[c];
+            resT[c] += srcTerm * vol[c];
+        }
+    }
+
+    // UTurbInvFlux (codes/uturb/src/UTurbInvFlux.cpp:55-202) with the first
+    // order turbulent and NS face states (turb_ilim = tns_ilim = -1) and
+    // TurbInvFlux::RoeFlux (codes/turb/src/TurbInvFlux.cpp:78-98), rho_coef = 1
+    void turbInvFlux() {
+        for (int f = 0; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            double t1 = nut[l], t2 = nut[r];
+            double u1 = q[IU][l], v1 = q[IV][l], w1 = q[IW][l], u2 = q[IU][r], v2 = q[IV][r], w2 = q[IW][r];
+            if (f < nBFaces) {
+                double tm = half * (nut[l] + nut[r]);
+                t1 = t2 = tm;
+                if (bcType[f] == OFG_BC_SOLID_SURFACE) {
+                    u1 = u2 = bc_q[IU][f]; v1 = v2 = bc_q[IV][f]; w1 = w2 = bc_q[IW][f];
+                } else {
+                    u1 = u2 = half * (q[IU][l] + q[IU][r]);
+                    v1 = v2 = half * (q[IV][l] + q[IV][r]);
+                    w1 = w2 = half * (q[IW][l] + q[IW][r]);
+                }
+            }
+            double vnl = xfn[f] * u1 + yfn[f] * v1 + zfn[f] * w1 - 0.0;
+            double vnr = xfn[f] * u2 + yfn[f] * v2 + zfn[f] * w2 - 0.0;
+            double vnl_p = half * (vnl + std::fabs(vnl));
+            double vnr_n = half * (vnr - std::fabs(vnr));
+            double coef_l = vnl_p * (1.0 * 1.0 + (1.0 - 1.0) * 0.0);
+            double coef_r = vnr_n * (1.0 * 1.0 + (1.0 - 1.0) * 0.0);
+            double flux = coef_l * t1 + coef_r * t2;
+            double v = area[f] * flux;
+            resT[l] -= v;
+            if (f >= nBFaces) resT[r] += v;
+        }
+    }
+
+    static double calcAngle(double dx, double dy, double dz, double dist) {
+        double result = dist / (DIST3(dx, dy, dz) + SMALL);
+        if (result > 1.0) result = 1.0;
+        if (result < -1.0) result = -1.0;
+        return std::asin(result) * 180.0 / PI;
+    }
+    // UTurbVisFlux::CalcVisFlux1Equ with the VIS_TEST face gradient
+    // (codes/uturb/src/UTurbVisFlux.cpp:64-407, codes/usolver/src/VisGrad.cpp:60-120,248-290)
+    void turbVisFlux() {
+        for (int f = 0; f < nFaces; ++f) {
+            int l = lc[f], r = rc[f];
+            double xn = xfn[f], yn = yfn[f], zn = zfn[f];
+            double q1 = nut[l], q2 = nut[r];
+            double q11 = q1, q22 = q2;
+            double qf = half * (q1 + q2);
+            double dxl = xcc[l] - xfc[f], dyl = ycc[l] - yfc[f], dzl = zcc[l] - zfc[f];
+            double dxr = xcc[r] - xfc[f], dyr = ycc[r] - yfc[f], dzr = zcc[r] - zfc[f];
+            double d1 = xn * dxl + yn * dyl + zn * dzl;
+            double d2 = xn * dxr + yn * dyr + zn * dzr;
+            double dxnl = xn * d1 - dxl, dynl = yn * d1 - dyl, dznl = zn * d1 - dzl;
+            double dxnr = xn * d2 - dxr, dynr = yn * d2 - dyr, dznr = zn * d2 - dzr;
+            double angle1 = calcAngle(dxl, dyl, dzl, -d1);
+            double angle2 = calcAngle(dxr, dyr, dzr, d2);
+            double dqdn = 0.0;
+            if (angle1 > 20.0 && angle2 > 20.0) {
+                q11 += dnutdx[l] * dxnl + dnutdy[l] * dynl + dnutdz[l] * dznl;
+                q22 += dnutdx[r] * dxnr + dnutdy[r] * dynr + dnutdz[r] * dznr;
+                qf = half * (q1 + q2);
+            }
+            if (angle1 > 0.0 && angle2 > 0.0 && std::fabs(d1) > SMALL && std::fabs(d2) > SMALL) {
+                double dtmp = d1 * d1 + d2 * d2;
+                double c1 = d1 * d1 / dtmp, c2 = 1.0 - c1;
+                if (f < nBFaces) { c1 = 1.0; c2 = 0.0; }
+                double dqdn1 = (q11 - qf) / d1;
+                double dqdn2 = (q22 - qf) / d2;
+                dqdn = c1 * dqdn1 + c2 * dqdn2;
+            }
+            double orl = 1.0 / (q[IR][l] + SMALL), orr = 1.0 / (q[IR][r] + SMALL);
+            double visl_nv = half * (visl[l] * orl + visl[r] * orr);
+            double vist_nv = half * (q1 + q2);
+            double comVis = (visl_nv + vist_nv) * sa.osigma;
+            double flux = -oreynolds * comVis * dqdn * area[f];
+            resT[l] -= flux;
+            if (f >= nBFaces) resT[r] += flux;
+        }
+    }
+
+    // UTurbLusgs sweeps (codes/uturb/src/UTurbLusgs.cpp:90-300) with
+    // TurbLusgs::GetStandardFluxIncrement (codes/turb/src/TurbLusgs.cpp:123-129)
+    void turbLower() {
+        for (int c = 0; c < nCells; ++c) {
+            double rhs0 = 0.0;
+            for (int f : c2f[c]) {
+                if (lc[f] > c || rc[f] > c) continue;
+                bool swap = rc[f] == c;
+                int nb = swap ? lc[f] : rc[f];
+                double m = swap ? matL[f] : matR[f];
+                rhs0 += m * dnut[nb];
+            }
+            dnut[c] = (resT[c] - rhs0) / impsrT[c];
+        }
+    }
+    void turbUpper() {
+        for (int c = nCells - 1; c >= 0; --c) {
+            double rhs0 = 0.0;
+            for (int f : c2f[c]) {
+                if (lc[f] < c || rc[f] < c) continue;
+                bool swap = rc[f] == c;
+                int nb = swap ? lc[f] : rc[f];
+                double m = swap ? matL[f] : matR[f];
+                rhs0 += m * dnut[nb];
+            }
+            dnut[c] += (-rhs0) / impsrT[c];
+        }
+    }
+    // UTurbUpdate::UpdateFlowField1EquStd / TurbUpdate::CalcFlowField1Equ (crelax = 1)
+    void turbUpdate() {
+        for (int c = 0; c < nCells; ++c) {
+            double qOld = nut[c], qNew = qOld + dnut[c];
+            nut[c] = (1.0 - 1.0) * qOld + 1.0 * qNew;
+        }
+    }
+    void turbRelax() {
+        std::fill(dnut.begin(), dnut.end(), 0.0);
+        std::fill(resT.begin(), resT.end(), -0.0);
+        // TurbCalcRHS, codes/turb/src/TurbRhs.cpp:57-70
+        turbBc();
+        turbSpectrum();
+        turbSource();
+        turbInvFlux();
+        turbVisFlux();
+        turbLower();
+        turbUpper();
+        turbUpdate();
+        turbBoundary();
+    }
+
     // ======================= one outer iteration =======================
     // TimeIntegral::Lusgs (codes/solver/src/TimeIntegral.cpp:113-130)
     void nsRelax() {
@@ -1020,10 +1334,16 @@ struct Oracle {
     int step(int n) {
         for (int it = 0; it < n; ++it) {
             ++outerSteps;
-            nsRelax();
+            nsRelax();   // MG::StrongIter: NS relaxation, then the turbulence solver
+            if (turb()) turbRelax();
             double rms[NEQ]; bool nan;
             residualRms(rms, &nan);
             for (int e = 0; e < NEQ; ++e) resHist.push_back(rms[e]);
+            if (turb()) {
+                double s = 0.0;
+                for (int c = 0; c < nCells; ++c) { s += resT[c] * resT[c]; if (std::isnan(resT[c])) nan = true; }
+                turbHist.push_back(std::sqrt(s / nCells));
+            }
             if (nan) { err = "NotANumber in residual"; return OFG_E_NAN; }
         }
         return 0;
@@ -1060,6 +1380,16 @@ int oro_task(void *h, const char *name) {
     else if (s == "UPDATE_FLOWFIELD_LUSGS") o->updateFlowfield();
     else if (s == "CALC_BOUNDARY") o->calcBoundary();
     else if (s == "INIT_LUSGS") {}   // CLusgsInit: no-op (codes/implicit/src/ImplicitTaskReg.cpp:69-72)
+    // the turbulence solver's tasks (tid TURB_SOLVER)
+    else if (s == "TURB:ZERO_DQ_FIELD") std::fill(o->dnut.begin(), o->dnut.end(), 0.0);
+    else if (s == "TURB:CALC_TIME_STEP" || s == "TURB:LOAD_RESIDUALS" || s == "TURB:INIT_LUSGS") {
+        if (s == "TURB:LOAD_RESIDUALS") std::fill(o->resT.begin(), o->resT.end(), -0.0);
+    }
+    else if (s == "TURB:UPDATE_RESIDUALS") { o->turbBc(); o->turbSpectrum(); o->turbSource(); o->turbInvFlux(); o->turbVisFlux(); }
+    else if (s == "TURB:LUSGS_LOWER_SWEEP") o->turbLower();
+    else if (s == "TURB:LUSGS_UPPER_SWEEP") o->turbUpper();
+    else if (s == "TURB:UPDATE_FLOWFIELD_LUSGS") o->turbUpdate();
+    else if (s == "TURB:CALC_BOUNDARY") o->turbBoundary();
     else if (s == "NEXT_STEP") ++o->outerSteps;
     else return OFG_E_ARG;
     return 0;
@@ -1100,6 +1430,12 @@ int64_t oro_field(void *h, const char *name, double *out) {
     if (s == "yfc") return put(&o->yfc, 1, nF);
     if (s == "zfc") return put(&o->zfc, 1, nF);
     if (s == "reshist") { if (out) std::copy(o->resHist.begin(), o->resHist.end(), out); return (int64_t)o->resHist.size(); }
+    if (s == "turbreshist") { if (out) std::copy(o->turbHist.begin(), o->turbHist.end(), out); return (int64_t)o->turbHist.size(); }
+    if (s == "turbq") return put(&o->nut, 1, nT);
+    if (s == "turbres") return put(&o->resT, 1, nT);
+    if (s == "turbdq") return put(&o->dnut, 1, nT);
+    if (s == "turbimpsr") return put(&o->impsrT, 1, nT);
+    if (s == "walldist") return put(&o->walldist, 1, nT);
     return -1;
 }
 int oro_set_q(void *h, const double *qin) {
