@@ -36,6 +36,19 @@ L2_BYTES = 126 * 2 ** 20
 # workloads
 # ---------------------------------------------------------------------------
 def make_workload(name: str):
+    from oneflow_b200.walldist import plate_wall_distance
+    if name in ("plate3d", "plate3d_small", "plate3d_sample"):
+        dims = {"plate3d": (200, 100, 50), "plate3d_small": (40, 20, 10), "plate3d_sample": (200, 100, 5)}[name]
+        mesh = meshgen.flat_plate_tets(*dims)
+        mesh.wall_dist = plate_wall_distance(mesh)
+        prm = P.rans_plate()
+        nx, ny, nz = dims
+        desc = dict(workload=f"3-D RANS-SA flat plate: {nx}x{ny}x{nz} hexes split into 6 tets "
+                             f"({6 * nx * ny * nz:,} cells), wall-normal ratio 1.15, first cell y+~1 at Re 5e6, "
+                             "Mach 0.2, Roe 2nd order, least-squares gradients, Venkatakrishnan eps^2=(K h)^3 K=5, "
+                             "SA, LU-SGS; FP32 face terms, FP64 accumulation/update/norms",
+                    lattice=list(dims))
+        return mesh, prm, desc
     if name == "bump2d":
         mesh = meshgen.bump_channel(256, 128)
         prm = P.euler_bump()
@@ -48,6 +61,31 @@ def make_workload(name: str):
     else:
         raise SystemExit(f"unknown config {name}")
     return mesh, prm, desc
+
+
+_SAMPLE = {"plate3d": "plate3d_sample"}
+
+
+def make_workload_desc(name: str):
+    """Description of a workload without building its mesh."""
+    if name == "plate3d":
+        return None, None, dict(workload="3-D RANS-SA flat plate: 200x100x50 hexes split into 6 tets (6,000,000 cells), "
+                                          "Roe 2nd order, least-squares gradients, Venkatakrishnan K=5, SA, LU-SGS",
+                                lattice=[200, 100, 50])
+    return make_workload(name)
+
+
+def _ref_procs(mesh) -> int:
+    """Concurrent reference processes: all host cores, bounded by memory
+    (about 1 kB of reference state per cell) and by 64."""
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        n = min(n, max(1, int(avail * 0.5 // (mesh.n_cells * 1200 + 1))))
+    except Exception:
+        pass
+    return max(1, min(n, 64))
 
 
 def mesh_stats(mesh: Mesh):
@@ -195,9 +233,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--config", default="bump2d")
+    ap.add_argument("--config", default="plate3d")
     ap.add_argument("--impl", default="ofg", choices=["ofg", "reference"])
-    ap.add_argument("--ordering", default="natural", choices=["natural", "colour"])
+    ap.add_argument("--ordering", default="colour", choices=["natural", "colour"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -215,32 +253,39 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    mesh, prm, desc = make_workload(args.config)
-
     if args.impl == "reference":
         if rank != 0:
             return
-        nproc = os.cpu_count() or 1
         if not os.path.exists(REF_EXE):
             print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver not built (oracle/_ref)"}))
             return
+        # the reference runs on a bounded sample of the workload: the same
+        # configuration on a mesh small enough that nproc concurrent
+        # single-rank solves fit the host and the run ends in minutes
+        sample = _SAMPLE.get(args.config, args.config)
+        mesh, prm, desc = make_workload(sample)
+        _, _, full_desc = make_workload_desc(args.config)
+        prm.precision = 0
+        nproc = _ref_procs(mesh)
         if args.ordering == "colour":
             from oneflow_b200 import colour_order
             perm, _ = colour_order(mesh)
             mesh = mesh.renumber_cells(perm)
-        thr, per_iter = reference_throughput(mesh, prm, args.warmup, args.warmup + args.steps, nproc)
+        steps = min(args.steps, 5) if mesh.n_cells > 200000 else args.steps
+        thr, per_iter = reference_throughput(mesh, prm, 2, 2 + steps, nproc)
         line = {"metric": "cell-iters/s", "value": thr, "unit": "cell-iter/s", "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (seeded mesh generator)",
-                "config": dict(desc, cells=mesh.n_cells, ordering=args.ordering),
+                "config": dict(full_desc, ordering=args.ordering, sample=desc["workload"], sample_cells=mesh.n_cells),
                 "cpu_baseline": {"value": thr, "unit": "cell-iter/s", "cores": nproc, "kind": "reference",
-                                 "sample": f"{nproc} concurrent single-rank reference solves of the full mesh; "
-                                           f"per-iteration time = (t({args.warmup + args.steps}) - t({args.warmup}))"
-                                           f" / {args.steps}"},
+                                 "sample": f"{nproc} concurrent single-rank reference solves of a {mesh.n_cells:,}-cell "
+                                           f"sample of the workload; per-iteration time = (t({2 + steps}) - t(2)) / {steps}"},
                 "e2e": {"value": thr, "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
+
+    mesh, prm, desc = make_workload(args.config)
 
     import torch
     from oneflow_b200 import Solver, colour_order
@@ -339,6 +384,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prm.precision == 0 else "f32/f64",
                 "data": "synthetic (seeded mesh generator)",
                 "config": dict(desc, cells=st["N"], faces=st["F"], ordering=args.ordering,
+                               sweep_levels=list(s.sweep_levels()),
                                l2="flushed between timed steps" if flush else "working set larger than L2",
                                parallelism=f"replicas x{world}"),
                 "roofline": roofline, "cpu_baseline": cpu,
@@ -360,12 +406,16 @@ def _peak_hbm():
 
 
 def _cpu_baseline(mesh, prm, config):
+    if config in _SAMPLE:
+        mesh, prm, _ = make_workload(_SAMPLE[config])
+    prm.precision = 0
     if os.path.exists(REF_EXE):
-        n1, n2 = (5, 25) if mesh.n_cells < 200000 else (1, 3)
+        n1, n2 = (5, 25) if mesh.n_cells < 200000 else (2, 4)
         try:
             thr, per_iter = reference_throughput(mesh, prm, n1, n2, 1)
             return {"value": thr, "unit": "cell-iter/s", "cores": 1, "kind": "reference",
-                    "sample": f"reference CPU solver (built from its sources), 1 process, full mesh, "
+                    "sample": f"reference CPU solver (built from its sources), 1 process, {mesh.n_cells:,}-cell "
+                              f"{'sample' if config in _SAMPLE else 'full mesh'}, "
                               f"(t({n2}) - t({n1})) / {n2 - n1} iterations"}
         except Exception as e:  # fall back to the port
             note = f"reference run failed: {e}"

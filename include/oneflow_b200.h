@@ -158,11 +158,17 @@ int ofg_download_field(ofg_ctx *ctx, int tid, const char *name, double *out, int
 int ofg_set_stream(ofg_ctx *ctx, void *stream);
 
 /* One outer iteration launched task by task (no graph) with CUDA events
-   between the groups; ms[8] receives the device time of: CFL advance,
+   between the groups; ms[] receives the device time of: CFL advance,
    CALC_TIME_STEP, UPDATE_RESIDUALS, LUSGS_LOWER_SWEEP, LUSGS_UPPER_SWEEP,
-   UPDATE_FLOWFIELD, CALC_BOUNDARY, residual norm; launches[8] the number of
-   kernel launches of each group. */
+   UPDATE_FLOWFIELD, CALC_BOUNDARY, residual norm, and with the SA model six
+   more (its UPDATE_RESIDUALS, lower, upper, update, boundary, norm);
+   launches[] the number of kernel launches of each group.  Both arrays
+   must hold 16 entries. */
 int ofg_profile_step(ofg_ctx *ctx, double *ms, int *launches);
+
+/* Number of dependency levels of the lower and upper LU-SGS sweeps in the
+   uploaded cell numbering (each level is one parallel launch). */
+int ofg_sweep_levels(ofg_ctx *ctx, int *lower_levels, int *upper_levels);
 
 /* Iteration::outerSteps for the task-level API (the CFL ramp of the next
    CALC_TIME_STEP reads it); ofg_step advances it itself. */

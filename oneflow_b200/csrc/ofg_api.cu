@@ -804,6 +804,14 @@ int ofg_profile_step(ofg_ctx *c, double *ms, int *launches) {
     return sync_history(c);
 }
 
+int ofg_sweep_levels(ofg_ctx *c, int *lower_levels, int *upper_levels) {
+    if (!c) return OFG_E_ARG;
+    if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
+    if (lower_levels) *lower_levels = int(c->lowOff.size()) - 1;
+    if (upper_levels) *upper_levels = int(c->upOff.size()) - 1;
+    return OFG_OK;
+}
+
 int ofg_set_outer_step(ofg_ctx *c, int64_t outer_steps) {
     if (!c || outer_steps < 0) return OFG_E_ARG;
     c->outerSteps = outer_steps;

@@ -55,6 +55,7 @@ def load_library() -> C.CDLL:
     L.ofg_get_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.ofg_set_outer_step.argtypes = [C.c_void_p, C.c_int64]
     L.ofg_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.ofg_sweep_levels.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.ofg_profile_step.argtypes = [C.c_void_p, _dp, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")]
     L.ofg_colour_order.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip]
     L.ofg_version.restype = C.c_int
@@ -142,14 +143,17 @@ class Solver:
         """Launch on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self.L.ofg_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
-    PROFILE_GROUPS = ("cfl", "time_step", "residual", "lusgs_lower", "lusgs_upper", "update", "boundary", "norm")
+    PROFILE_GROUPS = ("cfl", "time_step", "residual", "lusgs_lower", "lusgs_upper", "update", "boundary", "norm",
+                      "sa_residual", "sa_lower", "sa_upper", "sa_update", "sa_boundary", "sa_norm")
 
     def profile_step(self):
         """One iteration task by task with CUDA events: ({group: ms}, {group: launches})."""
-        ms = np.zeros(8, np.float64)
-        nl = np.zeros(8, np.int32)
+        ms = np.zeros(16, np.float64)
+        nl = np.zeros(16, np.int32)
         self._check(self.L.ofg_profile_step(self.h, ms, nl))
-        return dict(zip(self.PROFILE_GROUPS, ms.tolist())), dict(zip(self.PROFILE_GROUPS, nl.tolist()))
+        n = 14 if self.params.vismodel >= 3 else 8
+        names = self.PROFILE_GROUPS[:n]
+        return dict(zip(names, ms[:n].tolist())), dict(zip(names, nl[:n].tolist()))
 
     def residual_norms(self, tid: int = NS_SOLVER) -> np.ndarray:
         out = np.empty(5, np.float64)
@@ -166,6 +170,12 @@ class Solver:
 
     def res_history(self) -> np.ndarray:
         return self.field("reshist").reshape(-1, 5)
+
+    def sweep_levels(self):
+        """(lower, upper) number of LU-SGS dependency levels of this numbering."""
+        a, b = C.c_int(), C.c_int()
+        self._check(self.L.ofg_sweep_levels(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def counters(self):
         a, b = C.c_int64(), C.c_int64()

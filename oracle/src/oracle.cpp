@@ -777,7 +777,7 @@ struct Oracle {
     // VIS_STD face gradient (codes/usolver/src/VisGrad.cpp:150-175,356-366)
     void visFlux() {
         if (p.vismodel == 0) return;
-        gradGG(tempr, dtdx, dtdy, dtdz);
+        grad(tempr, dtdx, dtdy, dtdz);   // UTGrad: the reference's GG cell-weighted for igrad 0
         for (int f = 0; f < nFaces; ++f) {
             int l = lc[f], r = rc[f];
             double vl1 = visl[l], vl2 = visl[r], vt1 = vist[l], vt2 = vist[r];
@@ -1108,7 +1108,7 @@ struct Oracle {
     // TurbCom::CalcSrcSa (codes/turb/src/TurbCom.cpp:771-881) per cell, added as
     // UTurbSrcFlux::Update1Equ does (codes/uturb/src/UTurbSrcFlux.cpp:315-319)
     void turbSource() {
-        gradGG(nut, dnutdx, dnutdy, dnutdz);   // uturb_grad (GG cell-weighted)
+        grad(nut, dnutdx, dnutdy, dnutdz);   // uturb_grad (GG cell-weighted for igrad 0)
         for (int c = 0; c < nCells; ++c) {
             double dudx = dqdx[IU][c], dudy = dqdy[IU][c], dudz = dqdz[IU][c];
             double dvdx = dqdx[IV][c], dvdy = dqdy[IV][c], dvdz = dqdz[IV][c];
