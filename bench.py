@@ -328,12 +328,7 @@ def main():
             total_ms = a.elapsed_time(b)
     _, l1 = s.counters()
     torch.cuda.synchronize()
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
-    value = st["N"] * args.steps * world / (total_ms * 1e-3)
+    total_ms, value = replica_aggregate(total_ms, st["N"], args.steps, world, dist)
 
     # per-group device times (task-by-task launch with events) for the roofline
     prof = []
@@ -395,6 +390,20 @@ def main():
         dist.barrier()
         s.close()
         dist.destroy_process_group()
+
+
+def replica_aggregate(total_ms, cells, steps, world, dist):
+    """Independent replicas (one solve per GPU, no data-path collective): the
+    job time is the slowest rank's device time, and the whole-job throughput
+    counts every rank's cell-iterations.  Returns (max ms, cell-iter/s)."""
+    if dist is not None and world > 1:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() and dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(total_ms)], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    return total_ms, cells * steps * world / (total_ms * 1e-3)
 
 
 def _peak_hbm():

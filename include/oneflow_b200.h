@@ -79,7 +79,13 @@ typedef struct ofg_params {
     int    precision;        /* OFG_PREC_*                                     */
     int    venkat_kh3;       /* 0: eps = vencat_coef*max(qmax-qmin,1) (reference);
                                 1: eps^2 = (K h)^3 with K = vencat_coef (new)  */
-    int    reserved_i[7];
+    int    sweep_order;      /* LU-SGS sweep order: 0 the cell numbering (reference);
+                                1 colour-major: a greedy colouring of the cell
+                                graph in natural order, colours ascending, cell
+                                ids ascending inside a colour.  Identical to the
+                                reference run on the mesh renumbered that way
+                                (ofg_colour_order), with storage left in place. */
+    int    reserved_i[6];
     double vencat_coef;
     double centropy1, centropy2;
     double cflst, cfled;
@@ -98,6 +104,7 @@ typedef struct ofg_params {
 typedef struct ofg_ctx ofg_ctx;
 
 void        ofg_default_params(ofg_params *p);
+int         ofg_params_size(void);   /* sizeof(ofg_params), for binding checks */
 int         ofg_create(const ofg_params *p, ofg_ctx **out);
 void        ofg_destroy(ofg_ctx *ctx);
 const char *ofg_last_error(const ofg_ctx *ctx);

@@ -167,8 +167,64 @@ void compute_metrics(ofg_ctx *c, int dim, const std::vector<double> &xN, const s
 // Level schedule of a sequential sweep: a cell's level is one more than the
 // deepest level among the neighbours it reads (lower: smaller id; upper:
 // larger id).  Cells inside a level keep ascending / descending id order.
+// Greedy colouring of the cell graph (interior faces) in natural order and
+// the colour-major order: colours ascending, ids ascending inside a colour.
+// Returns the number of colours, fills perm[position] = cell.
+int colour_major_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm) {
+    std::vector<int> deg(nCells + 1, 0);
+    for (int f = nBFaces; f < nFaces; ++f) {
+        int l = lCells[f], r = rCells[f];
+        if (l < 0 || r < 0 || l >= nCells || r >= nCells) return OFG_E_ARG;
+        deg[l + 1]++; deg[r + 1]++;
+    }
+    for (int i = 0; i < nCells; ++i) deg[i + 1] += deg[i];
+    std::vector<int> adj(deg[nCells]);
+    std::vector<int> pos(deg.begin(), deg.end() - 1);
+    for (int f = nBFaces; f < nFaces; ++f) {
+        int l = lCells[f], r = rCells[f];
+        adj[pos[l]++] = r; adj[pos[r]++] = l;
+    }
+    std::vector<int> col(nCells, -1);
+    int ncol = 0;
+    std::vector<int> mark(64, -1);
+    for (int i = 0; i < nCells; ++i) {
+        for (int k = deg[i]; k < deg[i + 1]; ++k) {
+            int cc = col[adj[k]];
+            if (cc >= 0) { if (cc >= (int)mark.size()) mark.resize(cc + 1, -1); mark[cc] = i; }
+        }
+        int cc = 0;
+        while (cc < (int)mark.size() && mark[cc] == i) ++cc;
+        col[i] = cc;
+        ncol = std::max(ncol, cc + 1);
+    }
+    std::vector<int> cnt(ncol + 1, 0);
+    for (int i = 0; i < nCells; ++i) cnt[col[i] + 1]++;
+    for (int k = 0; k < ncol; ++k) cnt[k + 1] += cnt[k];
+    for (int i = 0; i < nCells; ++i) perm[cnt[col[i]]++] = i;
+    return ncol;
+}
+
+// Sweep key: the position of every cell in the LU-SGS order (ghosts after
+// every interior cell, as their ids nCells + f are in the reference).
+void build_sweep_key(ofg_ctx *c) {
+    int N = c->nCells;
+    c->keyOrder.resize(N);
+    if (c->p.sweep_order == 1) {
+        colour_major_order(N, c->nFaces, c->nBFaces, c->lc.data(), c->rc.data(), c->keyOrder.data());
+    } else {
+        for (int i = 0; i < N; ++i) c->keyOrder[i] = i;
+    }
+    c->key.assign(c->nT, 0);
+    for (int k = 0; k < N; ++k) c->key[c->keyOrder[k]] = k;
+    for (int f = 0; f < c->nBFaces; ++f) c->key[N + f] = N + f;
+}
+
+// Level schedule of a sequential sweep: a cell's level is one more than the
+// deepest level among the neighbours it reads (lower: smaller key; upper:
+// larger key).  Inside a level, cells keep the sweep order.
 void build_levels(ofg_ctx *c, bool lower, std::vector<int> &order, std::vector<int> &off) {
     int N = c->nCells;
+    const std::vector<int> &key = c->key;
     std::vector<int> lev(N, 0);
     int maxl = 0;
     auto visit = [&](int i) {
@@ -177,20 +233,20 @@ void build_levels(ofg_ctx *c, bool lower, std::vector<int> &order, std::vector<i
             int f = c->c2f[k];
             if (f < c->nBFaces) continue;
             int nb = c->lc[f] == i ? c->rc[f] : c->lc[f];
-            if (lower ? nb < i : nb > i) L = std::max(L, lev[nb] + 1);
+            if (lower ? key[nb] < key[i] : key[nb] > key[i]) L = std::max(L, lev[nb] + 1);
         }
         lev[i] = L;
         maxl = std::max(maxl, L);
     };
-    if (lower) for (int i = 0; i < N; ++i) visit(i);
-    else for (int i = N - 1; i >= 0; --i) visit(i);
+    if (lower) for (int k = 0; k < N; ++k) visit(c->keyOrder[k]);
+    else for (int k = N - 1; k >= 0; --k) visit(c->keyOrder[k]);
     off.assign(maxl + 2, 0);
     for (int i = 0; i < N; ++i) off[lev[i] + 1]++;
     for (int l = 0; l <= maxl; ++l) off[l + 1] += off[l];
     order.assign(N, 0);
     std::vector<int> pos(off.begin(), off.end() - 1);
-    if (lower) for (int i = 0; i < N; ++i) order[pos[lev[i]]++] = i;
-    else for (int i = N - 1; i >= 0; --i) order[pos[lev[i]]++] = i;
+    if (lower) for (int k = 0; k < N; ++k) { int i = c->keyOrder[k]; order[pos[lev[i]]++] = i; }
+    else for (int k = N - 1; k >= 0; --k) { int i = c->keyOrder[k]; order[pos[lev[i]]++] = i; }
 }
 
 template <typename T>
@@ -265,6 +321,8 @@ extern "C" {
 
 int ofg_version(void) { return 1; }
 
+int ofg_params_size(void) { return int(sizeof(ofg_params)); }
+
 void ofg_default_params(ofg_params *p) {
     std::memset(p, 0, sizeof(*p));
     p->dimension = 2; p->ischeme = 1; p->ilim = 0; p->igrad = 0; p->ieigenfix = 1; p->timestepModel = 0;
@@ -273,7 +331,7 @@ void ofg_default_params(ofg_params *p) {
     p->vencat_coef = 1.0e-4; p->centropy1 = 1.0e-4; p->centropy2 = 1.0e-4; p->cflst = 0.1; p->cfled = 10.0;
     p->max_time_ratio = 1.0e10; p->global_dt = 1.0e-3; p->mach_ref = 0.2; p->reynolds = 1.0e6;
     p->gama_ref = 1.4; p->prl = 0.72; p->prt = 0.9; p->tref_dim = 300.0; p->twall_dim = 300.0;
-    p->inflow_viscosity = 0.01; p->rprod = 1.0; p->turb_cfl_ratio = 1.0;
+    p->inflow_viscosity = 0.01; p->rprod = 1.0; p->turb_cfl_ratio = 1.0; p->ref_sa = 0.1; p->max_vis_ratio = 1.0e6;
 }
 
 int ofg_create(const ofg_params *p, ofg_ctx **out) {
@@ -284,6 +342,7 @@ int ofg_create(const ofg_params *p, ofg_ctx **out) {
     if (p->ilim < -1 || p->ilim > 2) return OFG_E_ARG;
     if (p->igrad < 0 || p->igrad > 2) return OFG_E_ARG;
     if (p->precision != OFG_PREC_FP64 && p->precision != OFG_PREC_MIXED) return OFG_E_ARG;
+    if (p->sweep_order != 0 && p->sweep_order != 1) return OFG_E_ARG;
     if (p->vismodel != 0 && p->vismodel != 1 && p->vismodel != 3) return OFG_E_ARG;   // Euler, laminar, SA
     if (p->vismodel == 3 && p->turb_ilim != -1) return OFG_E_ARG;   // first-order SA convection only
     if (p->ivischeme != 0) return OFG_E_ARG;
@@ -301,7 +360,7 @@ void ofg_destroy(ofg_ctx *c) {
     if (!c) return;
     cudaStreamSynchronize(c->stream);
     destroy_graphs(c);
-    void *ptrs[] = {c->d_lc, c->d_rc, c->d_bct, c->d_c2f_off, c->d_c2f, c->d_lowOrder, c->d_upOrder, c->d_wdist,
+    void *ptrs[] = {c->d_lc, c->d_rc, c->d_bct, c->d_c2f_off, c->d_c2f, c->d_lowOrder, c->d_upOrder, c->d_key, c->d_wdist,
                     c->d_q[0], c->d_q[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_bcq,
                     c->d_partial, c->d_scal, c->d_hist, c->d_grad, c->d_lim, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
@@ -365,6 +424,7 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         c->c2f[pos[c->lc[f]]++] = f;
         if (f >= nBFaces) c->c2f[pos[c->rc[f]]++] = f;
     }
+    build_sweep_key(c);
     build_levels(c, true, c->lowOrder, c->lowOff);
     build_levels(c, false, c->upOrder, c->upOff);
     c->wdist.assign(nCells, 0.0);
@@ -379,6 +439,7 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     if ((rc = upload(c, &c->d_c2f, c->c2f.data(), c->c2f.size()))) return rc;
     if ((rc = upload(c, &c->d_lowOrder, c->lowOrder.data(), nCells))) return rc;
     if ((rc = upload(c, &c->d_upOrder, c->upOrder.data(), nCells))) return rc;
+    if ((rc = upload(c, &c->d_key, c->key.data(), c->nT))) return rc;
     if ((rc = upload(c, &c->d_wdist, c->wdist.data(), nCells))) return rc;
     const std::vector<double> *geo[11] = {&c->xfn, &c->yfn, &c->zfn, &c->area, &c->xfc, &c->yfc, &c->zfc,
                                           &c->xcc, &c->ycc, &c->zcc, &c->vol};
@@ -854,40 +915,7 @@ int ofg_cell_centres(int dim, int nNodes, const double *xN, const double *yN, co
 
 int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm) {
     if (nCells <= 0 || nFaces < nBFaces || !lCells || !rCells || !perm) return OFG_E_ARG;
-    // adjacency (interior faces), CSR
-    std::vector<int> deg(nCells + 1, 0);
-    for (int f = nBFaces; f < nFaces; ++f) {
-        int l = lCells[f], r = rCells[f];
-        if (l < 0 || r < 0 || l >= nCells || r >= nCells) return OFG_E_ARG;
-        deg[l + 1]++; deg[r + 1]++;
-    }
-    for (int i = 0; i < nCells; ++i) deg[i + 1] += deg[i];
-    std::vector<int> adj(deg[nCells]);
-    std::vector<int> pos(deg.begin(), deg.end() - 1);
-    for (int f = nBFaces; f < nFaces; ++f) {
-        int l = lCells[f], r = rCells[f];
-        adj[pos[l]++] = r; adj[pos[r]++] = l;
-    }
-    // greedy colouring in natural order
-    std::vector<int> col(nCells, -1);
-    int ncol = 0;
-    std::vector<int> mark(64, -1);
-    for (int i = 0; i < nCells; ++i) {
-        for (int k = deg[i]; k < deg[i + 1]; ++k) {
-            int cc = col[adj[k]];
-            if (cc >= 0) { if (cc >= (int)mark.size()) mark.resize(cc + 1, -1); mark[cc] = i; }
-        }
-        int cc = 0;
-        while (cc < (int)mark.size() && mark[cc] == i) ++cc;
-        col[i] = cc;
-        ncol = std::max(ncol, cc + 1);
-    }
-    // stable order by colour: cells of one colour keep their relative order
-    std::vector<int> cnt(ncol + 1, 0);
-    for (int i = 0; i < nCells; ++i) cnt[col[i] + 1]++;
-    for (int k = 0; k < ncol; ++k) cnt[k + 1] += cnt[k];
-    for (int i = 0; i < nCells; ++i) perm[cnt[col[i]]++] = i;
-    return ncol;
+    return colour_major_order(nCells, nFaces, nBFaces, lCells, rCells, perm);
 }
 
 }  // extern "C"

@@ -19,13 +19,14 @@ struct ofg_ctx {
     std::vector<int> lc, rc, bct, c2f_off, c2f;
     std::vector<double> xfn, yfn, zfn, area, xfc, yfc, zfc, xcc, ycc, zcc, vol, wdist;
     std::vector<int> lowOrder, lowOff, upOrder, upOff;   // LU-SGS level schedules
+    std::vector<int> key, keyOrder;                      // sweep position of each cell, and its inverse
     bool haveMesh = false, haveState = false;
 
     // ---- device ----
     cudaStream_t stream = nullptr;      // stream every launch goes to
     cudaStream_t ownStream = nullptr;   // the context's own stream (set when a caller's stream is in use)
     int *d_lc = nullptr, *d_rc = nullptr, *d_bct = nullptr, *d_c2f_off = nullptr, *d_c2f = nullptr;
-    int *d_lowOrder = nullptr, *d_upOrder = nullptr;
+    int *d_lowOrder = nullptr, *d_upOrder = nullptr, *d_key = nullptr;
     double *d_g64[11] = {};    // xfn yfn zfn area xfc yfc zfc | xcc ycc zcc vol
     float *d_g32[11] = {};
     double *d_wdist = nullptr;

@@ -66,6 +66,7 @@ struct DevMesh {
     const int *c2f;              // [E] face ids, ascending per cell
     const int *bcType;           // [nBFaces]
     const double *walldist;      // [nCells]
+    const int *key;              // [nT] position of each cell in the sweep order (ghosts last)
 };
 
 // Primitive -> conservative, NsInvFlux.cpp:1355-1375 (CalcInternalEnergy :1400-1412)

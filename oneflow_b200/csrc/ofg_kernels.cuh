@@ -626,9 +626,10 @@ __global__ void __launch_bounds__(128) k_lusgs_lower(KArgs<R> A, const int *orde
     int c = order[start + t];
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
     int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
+    int kc = A.M.key[c];
     for (int k = b; k < en; ++k) {
         int f = A.M.c2f[k];
-        if (A.M.lc[f] > c || A.M.rc[f] > c) continue;
+        if (A.M.key[A.M.lc[f]] > kc || A.M.key[A.M.rc[f]] > kc) continue;   // UNsLusgs::CanNotLowerSolve
         face_increment(A, c, f, rhs0);
     }
     double rad = implicit_radius(A, c);
@@ -645,10 +646,11 @@ __global__ void __launch_bounds__(128) k_lusgs_upper(KArgs<R> A, const int *orde
     int c = order[start + t];
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
     int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
+    int kc = A.M.key[c];
     for (int k = b; k < en; ++k) {
         int f = A.M.c2f[k];
         if (f < A.M.nBFaces) continue;   // ghost dq is zero: no contribution
-        if (A.M.lc[f] < c || A.M.rc[f] < c) continue;
+        if (A.M.key[A.M.lc[f]] < kc || A.M.key[A.M.rc[f]] < kc) continue;   // UNsLusgs::CanNotUpperSolve
         face_increment(A, c, f, rhs0);
     }
     double rad = implicit_radius(A, c);
@@ -728,7 +730,7 @@ __global__ void k_solution_fix(KArgs<R> A) {
     int *ids = A.fixlist + 1;
     for (int i = 1; i < n; ++i) {   // insertion sort (the list is short)
         int v = ids[i], j = i - 1;
-        while (j >= 0 && ids[j] > v) { ids[j + 1] = ids[j]; --j; }
+        while (j >= 0 && A.M.key[ids[j]] > A.M.key[v]) { ids[j + 1] = ids[j]; --j; }
         ids[j + 1] = v;
     }
     for (int i = 0; i < n; ++i) {
@@ -737,7 +739,8 @@ __global__ void k_solution_fix(KArgs<R> A) {
         for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
             int f = A.M.c2f[k];
             int nb = other_cell(A.M.lc[f], A.M.rc[f], c);
-            const double *src = (nb < c) ? A.qn + (size_t)nb * REC : A.q + (size_t)nb * REC;
+            bool done = nb < A.M.nCells && A.M.key[nb] < A.M.key[c];   // already updated in sweep order
+            const double *src = done ? A.qn + (size_t)nb * REC : A.q + (size_t)nb * REC;
             sumV += 1.0;
             for (int e = 0; e < NEQ; ++e) {
                 double v = src[e];

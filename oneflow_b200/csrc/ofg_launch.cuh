@@ -58,6 +58,7 @@ KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
     A.M.nCells = c->nCells; A.M.nBFaces = c->nBFaces; A.M.nFaces = c->nFaces; A.M.nT = c->nT;
     A.M.lc = c->d_lc; A.M.rc = c->d_rc; A.M.c2f_off = c->d_c2f_off; A.M.c2f = c->d_c2f; A.M.bcType = c->d_bct;
     A.M.walldist = c->d_wdist;
+    A.M.key = c->d_key;
     A.G = make_geom<R>(c);
     A.q = c->d_q[c->cur];
     A.qn = onCurrent ? c->d_q[c->cur] : c->d_q[c->cur ^ 1];

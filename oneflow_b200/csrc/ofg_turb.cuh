@@ -313,10 +313,11 @@ __global__ void __launch_bounds__(128) k_turb_lower(KArgs<R> A, const int *order
     if (t >= count) return;
     int c = order[start + t];
     double rhs0 = 0.0;
+    int kc = A.M.key[c];
     for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
         int f = A.M.c2f[k];
         int l = A.M.lc[f], r = A.M.rc[f];
-        if (l > c || r > c) continue;
+        if (A.M.key[l] > kc || A.M.key[r] > kc) continue;
         bool swap = (r == c);
         rhs0 += (swap ? A.matL[f] : A.matR[f]) * A.dnut[swap ? l : r];
     }
@@ -329,11 +330,12 @@ __global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order
     if (t >= count) return;
     int c = order[start + t];
     double rhs0 = 0.0;
+    int kc = A.M.key[c];
     for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
         int f = A.M.c2f[k];
         if (f < A.M.nBFaces) continue;   // ghost increments are zero
         int l = A.M.lc[f], r = A.M.rc[f];
-        if (l < c || r < c) continue;
+        if (A.M.key[l] < kc || A.M.key[r] < kc) continue;
         bool swap = (r == c);
         rhs0 += (swap ? A.matL[f] : A.matR[f]) * A.dnut[swap ? l : r];
     }

@@ -9,14 +9,14 @@ import ctypes as C
 
 _INT = ["dimension", "ischeme", "ilim", "igrad", "ieigenfix", "timestepModel", "ncfl", "visSRModel",
         "visTimeStepModel", "vismodel", "ivischeme", "isowallbc", "iprod_sa", "ft2_flag", "turb_ilim",
-        "precision", "venkat_kh3"]
+        "precision", "venkat_kh3", "sweep_order"]
 _DBL = ["vencat_coef", "centropy1", "centropy2", "cflst", "cfled", "max_time_ratio", "global_dt", "mach_ref",
         "aoa_degree", "sideslip_degree", "reynolds", "gama_ref", "prl", "prt", "tref_dim", "twall_dim",
         "inflow_viscosity", "rprod", "turb_cfl_ratio", "ref_sa", "max_vis_ratio"]
 
 
 class OfgParams(C.Structure):
-    _fields_ = ([(n, C.c_int) for n in _INT] + [("reserved_i", C.c_int * 7)] +
+    _fields_ = ([(n, C.c_int) for n in _INT] + [("reserved_i", C.c_int * 6)] +
                 [(n, C.c_double) for n in _DBL] + [("reserved_d", C.c_double * 6)])
 
 

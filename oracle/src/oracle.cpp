@@ -85,8 +85,43 @@ struct Oracle {
         c2f.assign(nT, {});
         for (int f = 0; f < nb; ++f) c2f[lc[f]].push_back(f);
         for (int f = nb; f < nf; ++f) { c2f[lc[f]].push_back(f); c2f[rc[f]].push_back(f); }
+        buildKey();
         alloc();
         return 0;
+    }
+
+    // Sweep order.  sweep_order 0: the cell numbering (the reference).
+    // sweep_order 1: colour-major (greedy colouring in natural order, colours
+    // ascending, ids ascending inside a colour) -- the order in which the
+    // reference would sweep the mesh renumbered that way.  Ghosts come last.
+    std::vector<int> key, keyOrder;
+    void buildKey() {
+        keyOrder.resize(nCells);
+        if (p.sweep_order == 1) {
+            std::vector<int> col(nCells, -1);
+            int ncol = 0;
+            for (int i = 0; i < nCells; ++i) {
+                std::vector<char> used(ncol + 1, 0);
+                for (int f : c2f[i]) {
+                    if (f < nBFaces) continue;
+                    int nb = lc[f] == i ? rc[f] : lc[f];
+                    if (col[nb] >= 0) used[col[nb]] = 1;
+                }
+                int cc = 0;
+                while (cc < (int)used.size() && used[cc]) ++cc;
+                col[i] = cc;
+                ncol = std::max(ncol, cc + 1);
+            }
+            int k = 0;
+            for (int cc = 0; cc < ncol; ++cc)
+                for (int i = 0; i < nCells; ++i)
+                    if (col[i] == cc) keyOrder[k++] = i;
+        } else {
+            for (int i = 0; i < nCells; ++i) keyOrder[i] = i;
+        }
+        key.assign(nT, 0);
+        for (int k = 0; k < nCells; ++k) key[keyOrder[k]] = k;
+        for (int f = 0; f < nBFaces; ++f) key[nCells + f] = nCells + f;
     }
 
     void calcMetrics() {
@@ -927,10 +962,11 @@ struct Oracle {
     // UNsLusgs::LowerSweep, codes/uns/src/UNsLusgs.cpp:75-108; NsLusgs::CalcLowerChange (:230-277)
     void lusgsLower() {
         calcImplicitSpectrum();
-        for (int c = 0; c < nCells; ++c) {
+        for (int k = 0; k < nCells; ++k) {
+            int c = keyOrder[k];
             double rhs0[NEQ] = {0, 0, 0, 0, 0};
             for (int f : c2f[c]) {
-                if (lc[f] > c || rc[f] > c) continue;
+                if (key[lc[f]] > key[c] || key[rc[f]] > key[c]) continue;
                 faceIncrement(c, f, rhs0);
             }
             for (int e = 0; e < NEQ; ++e) dq[e][c] = (res[e][c] - rhs0[e]) / impsr[c];
@@ -939,10 +975,11 @@ struct Oracle {
     // UNsLusgs::UpperSweep, codes/uns/src/UNsLusgs.cpp:110-138; NsLusgs::CalcUpperChange (:279-326)
     void lusgsUpper() {
         calcImplicitSpectrum();
-        for (int c = nCells - 1; c >= 0; --c) {
+        for (int k = nCells - 1; k >= 0; --k) {
+            int c = keyOrder[k];
             double rhs0[NEQ] = {0, 0, 0, 0, 0};
             for (int f : c2f[c]) {
-                if (lc[f] < c || rc[f] < c) continue;
+                if (key[lc[f]] < key[c] || key[rc[f]] < key[c]) continue;
                 faceIncrement(c, f, rhs0);
             }
             for (int e = 0; e < NEQ; ++e) dq[e][c] += (-rhs0[e]) / impsr[c];
@@ -955,7 +992,8 @@ struct Oracle {
     long nFixes = 0;
     void updateFlowfield() {
         double gama = p.gama_ref;
-        for (int c = 0; c < nCells; ++c) {
+        for (int kk = 0; kk < nCells; ++kk) {
+            int c = keyOrder[kk];   // in place, in sweep order (SolutionFix reads updated neighbours)
             double prim0[NEQ], q0[NEQ], qq[NEQ], pr[NEQ], d[NEQ];
             for (int e = 0; e < NEQ; ++e) { prim0[e] = q[e][c]; d[e] = dq[e][c]; }
             primToQ(prim0, gama, q0);
@@ -1271,10 +1309,11 @@ struct Oracle {
     // UTurbLusgs sweeps (codes/uturb/src/UTurbLusgs.cpp:90-300) with
     // TurbLusgs::GetStandardFluxIncrement (codes/turb/src/TurbLusgs.cpp:123-129)
     void turbLower() {
-        for (int c = 0; c < nCells; ++c) {
+        for (int k = 0; k < nCells; ++k) {
+            int c = keyOrder[k];
             double rhs0 = 0.0;
             for (int f : c2f[c]) {
-                if (lc[f] > c || rc[f] > c) continue;
+                if (key[lc[f]] > key[c] || key[rc[f]] > key[c]) continue;
                 bool swap = rc[f] == c;
                 int nb = swap ? lc[f] : rc[f];
                 double m = swap ? matL[f] : matR[f];
@@ -1284,10 +1323,11 @@ struct Oracle {
         }
     }
     void turbUpper() {
-        for (int c = nCells - 1; c >= 0; --c) {
+        for (int k = nCells - 1; k >= 0; --k) {
+            int c = keyOrder[k];
             double rhs0 = 0.0;
             for (int f : c2f[c]) {
-                if (lc[f] < c || rc[f] < c) continue;
+                if (key[lc[f]] < key[c] || key[rc[f]] < key[c]) continue;
                 bool swap = rc[f] == c;
                 int nb = swap ? lc[f] : rc[f];
                 double m = swap ? matL[f] : matR[f];

@@ -1,0 +1,35 @@
+"""Seeded cases of the golden fixtures (tests/golden/*.npz): the mesh and the
+parameters of each, regenerated from their seeds."""
+from oneflow_b200 import colour_order, meshgen, params as P
+from oneflow_b200.walldist import plate_wall_distance, wall_distance
+
+CASES = {
+    "bump_euler_roe1": dict(steps=50),
+    "bump_euler_roe_venkat": dict(steps=30),
+    "bump_euler_roe_barth": dict(steps=30),
+    "plate2d_laminar_slau2": dict(steps=30),
+    "plate2d_sa_roe": dict(steps=30),
+    "plate3d_sa_roe": dict(steps=10),
+    "plate3d_sa_roe_colour_renumbered": dict(steps=10),
+}
+
+
+def build(name):
+    steps = CASES[name]["steps"]
+    if name.startswith("bump"):
+        mesh = meshgen.bump_channel(32, 16)
+        kw = {"bump_euler_roe1": {}, "bump_euler_roe_venkat": dict(ilim=2, vencat_coef=0.05),
+              "bump_euler_roe_barth": dict(ilim=1)}[name]
+        return mesh, P.euler_bump(**kw), steps
+    if name == "plate2d_laminar_slau2":
+        return meshgen.plate_2d(24, 16), P.defaults(ischeme=12, ilim=0, mach_ref=0.2, reynolds=1e5, vismodel=1), steps
+    if name == "plate2d_sa_roe":
+        mesh = meshgen.plate_2d(32, 24, y1=1e-5, ratio=1.25)
+        mesh.wall_dist = wall_distance(mesh)
+        return mesh, P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=5e6, vismodel=3), steps
+    mesh = meshgen.flat_plate_tets(8, 6, 4, ratio=1.3)
+    mesh.wall_dist = plate_wall_distance(mesh)
+    if name == "plate3d_sa_roe_colour_renumbered":
+        perm, _ = colour_order(mesh)
+        mesh = mesh.renumber_cells(perm)
+    return mesh, P.defaults(dimension=3, ischeme=1, ilim=0, vismodel=3, mach_ref=0.2, reynolds=5e6), steps

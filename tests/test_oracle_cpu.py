@@ -1,0 +1,102 @@
+"""CPU tests (no GPU): the oracle pinned against the reference.
+
+1. The reference's own regression cases (test/*/autotest/res.dat,
+   turbres.dat) under the reference's comparator (every number within 1e-8
+   absolute, test/test.py:38-53) -- needs the reference sources, skipped when
+   they are absent.
+2. The committed golden fixtures (tests/golden/*.npz, made by running the
+   reference build on seeded meshes with tests/golden/make_golden.py).
+3. The colour-major sweep order equals the reference run on the renumbered mesh.
+"""
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oneflow_b200 import colour_order, meshgen, params as P
+from oneflow_b200.meshio import read_ofl, read_res_dat
+from oneflow_b200.walldist import plate_wall_distance, wall_distance
+from golden_cases import CASES, build
+from oracle_lib import Oracle
+
+REF = "/root/reference/test"
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _script_keys(case_dir):
+    kv = {}
+    for f in os.listdir(os.path.join(case_dir, "script")):
+        for line in open(os.path.join(case_dir, "script", f), encoding="latin-1"):
+            m = re.match(r"\s*(int|Real|string)\s+(\w+)\s*=\s*([^;\s]+)", line.split("//")[0])
+            if m:
+                kv[m.group(2)] = m.group(3)
+    return kv
+
+
+@pytest.mark.parametrize("case", ["plateuns2dslau2", "turbplateuns2droe_sa", "rae2822_roe_sa"])
+def test_oracle_reproduces_reference_regression_goldens(case):
+    d = os.path.join(REF, case)
+    if not os.path.isdir(d):
+        pytest.skip("reference sources not mounted")
+    kv = _script_keys(d)
+    mesh = read_ofl(os.path.join(d, kv["gridFileName"].strip('"')), dim=int(kv["dimension"]))
+    prm = P.defaults(**{k: (int(v) if k in P._INT else float(v)) for k, v in kv.items() if k in P._INT + P._DBL})
+    if prm.vismodel >= 3:
+        mesh.wall_dist = wall_distance(mesh)
+    o = Oracle(mesh, prm)
+    o.init()
+    assert o.step(int(kv["maxSteps"])) == 0
+    gold = read_res_dat(os.path.join(d, "autotest", "res.dat"))
+    # the reference's comparator: each printed number within 1e-8
+    assert np.abs(o.res_history() - gold[:, 2:7]).max() < 1e-8
+    if prm.vismodel >= 3:
+        tgold = read_res_dat(os.path.join(d, "autotest", "turbres.dat"))
+        assert np.abs(o.field("turbreshist") - tgold[:, 2]).max() < 1e-8
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_oracle_matches_reference_fixture(name):
+    mesh, prm, steps = build(name)
+    g = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    assert json.loads(str(g["params"])) == pytest.approx(P.to_dict(prm))
+    o = Oracle(mesh, prm)
+    o.init()
+    o.step(steps)
+    q, qg = o.q(), g["q"]
+    N = mesh.n_cells
+    assert np.abs(q[:, :N] - qg[:, :N]).max() / np.abs(qg[:, :N]).max() < 1e-12
+    # residual history as the reference printed it (6 significant digits):
+    # within half a unit of the last printed digit
+    h, hg = o.res_history(), g["reshist"]
+    assert np.all(np.abs(h - hg) <= 5.01e-6 * np.abs(hg) + 1e-12)
+    if "turbq" in g:
+        a, b = o.field("turbq")[:N], g["turbq"][:N]
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5
+
+
+def test_colour_sweep_order_equals_renumbered_mesh():
+    mesh = meshgen.flat_plate_tets(8, 6, 4, ratio=1.3)
+    mesh.wall_dist = plate_wall_distance(mesh)
+    base = dict(dimension=3, ischeme=1, ilim=0, vismodel=3, mach_ref=0.2, reynolds=5e6)
+    perm, ncol = colour_order(mesh)
+    assert ncol >= 2 and sorted(perm.tolist()) == list(range(mesh.n_cells))
+    a = Oracle(mesh, P.defaults(**base, sweep_order=1)); a.init(); a.step(8)
+    b = Oracle(mesh.renumber_cells(perm), P.defaults(**base)); b.init(); b.step(8)
+    N = mesh.n_cells
+    # bitwise: the same arithmetic in the same order
+    assert np.array_equal(a.q()[:, :N][:, perm], b.q()[:, :N])
+    assert np.array_equal(a.field("turbq")[:N][perm], b.field("turbq")[:N])
+    # and the renumbered-mesh fixture (made by the reference) is the same solve
+    g = np.load(os.path.join(HERE, "golden", "plate3d_sa_roe_colour_renumbered.npz"))
+    c = Oracle(mesh, P.defaults(**base, sweep_order=1)); c.init(); c.step(10)
+    assert np.abs(c.q()[:, :N][:, perm] - g["q"][:, :N]).max() / np.abs(g["q"]).max() < 1e-12
+
+
+def test_oracle_first_order_bump_is_bitwise_reference():
+    # the FP64 restatement rounds exactly like the reference on this case
+    mesh, prm, steps = build("bump_euler_roe1")
+    g = np.load(os.path.join(HERE, "golden", "bump_euler_roe1.npz"))
+    o = Oracle(mesh, prm); o.init(); o.step(steps)
+    assert np.array_equal(o.q(), g["q"])
