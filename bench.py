@@ -94,45 +94,56 @@ def mesh_stats(mesh: Mesh):
 
 
 def alg_bytes(st, prm) -> dict:
-    """Algorithmic bytes of each phase of one iteration: every array the phase
-    reads or writes counted once, at its stored precision, neighbour gathers
-    counted once (perfect reuse).  Matches the data layout of the CUDA path:
-    state record (rho,u,v,w,p[,T,mul,mut]) FP64, residual/dq FP64, geometry and
-    gradients/limiters at the face precision (8 B FP64 path, 4 B mixed)."""
+    """Algorithmic bytes of each profile group of one outer iteration: every
+    array a kernel of the group reads or writes counted once per kernel, at its
+    stored size, neighbour gathers counted once (perfect reuse).  Data layout of
+    the CUDA path (g = 8 B FP64 path, 4 B mixed):
+      state record (rho u v w p T mu_l mu_t): FP64 master 64 B, face kernels read
+        the copy at the face precision (8g B; the master itself on the FP64 path)
+      face record 8g B (normal, area, centre), cell record 4g B (centre, volume)
+      gradient+limiter record 24g B, neighbour list entry 8 B (face|side, cell)
+      residual, dq 40 B; dt, inviscid and viscous radii 8 B each."""
     N, B, F, E = st["N"], st["B"], st["F"], st["E"]
     NT = N + B
+    FI = F - B
     g = 8 if prm.precision == 0 else 4
+    mixed = prm.precision != 0
     vis = prm.vismodel > 0
-    second = prm.ilim != -1
-    nq = 8 if vis else 5                      # state record fields a face kernel reads
-    csr = (N + 1) * 4 + E * 4
-    lcrc = F * 8
-    fgeo = F * 4 * g                          # normal (3) + area
-    fcen = F * 3 * g
-    ccen = NT * 3 * g
-    vol = N * g
-    out = {}
-    out["time_step"] = NT * nq * 8 + csr + lcrc + fgeo + vol + (ccen if vis else 0) + N * 24
-    grad = 0
-    if second or vis:
-        nv = 6 if vis else 5
-        grad = (NT * nq * 8 + csr + lcrc + fgeo + fcen + ccen + vol) + N * nv * 3 * g
-    lim = 0
-    if prm.ilim in (1, 2):
-        lim = (NT * 5 * 8 + csr + lcrc + N * 10 * g) + (N * 15 * g + N * 10 * g + csr + fcen + ccen + N * 5 * g)
-    res = NT * nq * 8 + csr + lcrc + fgeo + B * 40 + N * 40
-    if second:
-        res += N * 15 * g + N * 5 * g + fcen + ccen
-    if vis:
-        res += N * 18 * g + ccen
-    out["residual"] = grad + lim + res
-    sweep = NT * nq * 8 + N * 40 + N * 40 + N * 24 + vol + csr + lcrc + fgeo + N * 4 + (ccen if vis else 0)
-    out["lusgs_lower"] = sweep + N * 40          # res read
-    out["lusgs_upper"] = sweep + N * 40          # own dq read before write
-    out["update"] = N * 64 + N * 40 + N * 64
-    out["boundary"] = B * (64 + 64 + 40 + 4 * g)
+    sa = prm.vismodel >= 3
+    need_grad = prm.ilim != -1 or vis
+    lsq = prm.igrad == 2
+    qs = NT * 8 * g                            # state records read by face kernels
+    cg = NT * 4 * g
+    fg = F * 8 * g
+    nbl = E * 8 + (N + 1) * 4
+    half_lists = FI * 8 + (N + 1) * 4          # lower (or upper) lists: each interior face once
+    gl = N * 24 * g
+    out = {"cfl": 0}
+    res = 0
+    if need_grad:
+        res += qs + cg + nbl + (0 if lsq else fg) + gl           # k_gradlim
+        if prm.ilim == 2 and not prm.venkat_kh3:
+            res += N * 10 * g + (gl + N * 10 * g + cg + nbl + fg + N * 5 * g)   # min/max, global eps pass
+    res += qs + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24   # k_residual
+    res += N * 16                                                # time-step clip
+    out["residual"] = res
+    sweep = qs + cg + F * 4 * g + half_lists + N * 40 + N * 40 + N * 24 + N * 4   # + dq of neighbours, own dq
+    out["lusgs_lower"] = sweep + N * 40                          # + res
+    out["lusgs_upper"] = sweep + N * 40                          # + own dq read before the write
+    out["update"] = N * 64 + N * 40 + N * 64 + (N * 8 * g if mixed else 0)
+    out["boundary"] = B * (4 + 4 + 8 * g + 64 + 8 + 64 + 40) + (B * 8 * g if mixed else 0)
     out["norm"] = N * 40
-    out["cfl"] = 0
+    if sa:
+        grad_nut = NT * 8 + nbl + cg + (0 if lsq else fg) + N * 4 * g
+        rhs = qs + cg + fg + nbl + NT * 8 + N * 4 * g + N * 12 * g + N * 16 + N * 8 + N * 8 + B * 44 \
+            + F * 16 + N * 16
+        out["sa_residual"] = B * 24 + grad_nut + rhs
+        sa_sweep = half_lists + FI * 16 + N * 8 + N * 8 + N * 8 + N * 8 + N * 4
+        out["sa_lower"] = sa_sweep
+        out["sa_upper"] = sa_sweep
+        out["sa_update"] = N * 8 * 3 + N * 24 + N * 8 + (N * g if mixed else 0)
+        out["sa_boundary"] = B * (4 + 4 + 8 * g + 24 + 8 + 16)
+        out["sa_norm"] = N * 8
     return out
 
 
@@ -291,9 +302,10 @@ def main():
     from oneflow_b200 import Solver, colour_order
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
-    if args.ordering == "colour":
-        perm, ncol = colour_order(mesh)
-        mesh = mesh.renumber_cells(perm)
+    # colour ordering: the LU-SGS sweeps run in colour-major order (identical to
+    # the reference solving the mesh renumbered by ofg_colour_order) while the
+    # cells stay stored in the generator's spatial order
+    prm.sweep_order = 1 if args.ordering == "colour" else 0
     st = mesh_stats(mesh)
     stream = torch.cuda.current_stream()
     s = Solver(mesh, prm)

@@ -166,7 +166,8 @@ int ofg_set_stream(ofg_ctx *ctx, void *stream);
 
 /* One outer iteration launched task by task (no graph) with CUDA events
    between the groups; ms[] receives the device time of: CFL advance,
-   CALC_TIME_STEP, UPDATE_RESIDUALS, LUSGS_LOWER_SWEEP, LUSGS_UPPER_SWEEP,
+   CALC_TIME_STEP + UPDATE_RESIDUALS (one fused gather: gradients, limiter,
+   fluxes, time step), LUSGS_LOWER_SWEEP, LUSGS_UPPER_SWEEP,
    UPDATE_FLOWFIELD, CALC_BOUNDARY, residual norm, and with the SA model six
    more (its UPDATE_RESIDUALS, lower, upper, update, boundary, norm);
    launches[] the number of kernel launches of each group.  Both arrays

@@ -249,12 +249,70 @@ void build_levels(ofg_ctx *c, bool lower, std::vector<int> &order, std::vector<i
     else for (int k = N - 1; k >= 0; --k) { int i = c->keyOrder[k]; order[pos[lev[i]]++] = i; }
 }
 
+// Per-cell neighbour lists in ascending face id (the c2f order), one int2 per
+// face: {face | side << 31, neighbour}, side = 1 where the cell is the face's
+// right cell.  Full lists for the residual and gradient gathers; for the
+// sweeps, the interior faces to cells earlier (lower) and later (upper) in
+// the sweep order.
+struct NbLists {
+    std::vector<int> nbOff, nbl, loOff, lol, upOff, upl;
+};
+
+void build_lists(const ofg_ctx *c, NbLists &L) {
+    int N = c->nCells;
+    L.nbOff.assign(N + 1, 0); L.loOff.assign(N + 1, 0); L.upOff.assign(N + 1, 0);
+    L.nbl.clear(); L.lol.clear(); L.upl.clear();
+    L.nbl.reserve(2 * c->c2f.size());
+    for (int i = 0; i < N; ++i) {
+        int ki = c->key[i];
+        for (int k = c->c2f_off[i]; k < c->c2f_off[i + 1]; ++k) {
+            int f = c->c2f[k];
+            bool right = c->rc[f] == i && f >= c->nBFaces;
+            int nb = right ? c->lc[f] : c->rc[f];
+            int tag = int(unsigned(f) | (right ? 0x80000000u : 0u));
+            L.nbl.push_back(tag); L.nbl.push_back(nb);
+            if (f < c->nBFaces) continue;
+            if (c->key[nb] < ki) { L.lol.push_back(tag); L.lol.push_back(nb); }
+            else { L.upl.push_back(tag); L.upl.push_back(nb); }
+        }
+        L.nbOff[i + 1] = int(L.nbl.size() / 2);
+        L.loOff[i + 1] = int(L.lol.size() / 2);
+        L.upOff[i + 1] = int(L.upl.size() / 2);
+    }
+}
+
+// face records [F][8] (nx ny nz area xfc yfc zfc 0) and cell records [nT][4]
+// (xcc ycc zcc vol) at the face precision
+template <typename R>
+void pack_geometry(const ofg_ctx *c, std::vector<R> &fg, std::vector<R> &cg) {
+    fg.assign((size_t)c->nFaces * 8, R(0));
+    for (int f = 0; f < c->nFaces; ++f) {
+        R *o = &fg[(size_t)f * 8];
+        o[0] = R(c->xfn[f]); o[1] = R(c->yfn[f]); o[2] = R(c->zfn[f]); o[3] = R(c->area[f]);
+        o[4] = R(c->xfc[f]); o[5] = R(c->yfc[f]); o[6] = R(c->zfc[f]);
+    }
+    cg.assign((size_t)c->nT * 4, R(0));
+    for (int i = 0; i < c->nT; ++i) {
+        R *o = &cg[(size_t)i * 4];
+        o[0] = R(c->xcc[i]); o[1] = R(c->ycc[i]); o[2] = R(c->zcc[i]); o[3] = R(c->vol[i]);
+    }
+}
+
 template <typename T>
 int upload(ofg_ctx *c, T **d, const T *h, size_t n) {
     if (*d) { cudaFree(*d); *d = nullptr; }
     if (n == 0) n = 1;
     CK(cudaMalloc((void **)d, n * sizeof(T)));
     if (h) CK(cudaMemcpy(*d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    return OFG_OK;
+}
+
+int upload_bytes(ofg_ctx *c, void **d, const void *h, size_t bytes) {
+    if (*d) { cudaFree(*d); *d = nullptr; }
+    if (bytes == 0) bytes = 16;
+    CK(cudaMalloc(d, bytes));
+    if (h) CK(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
+    else CK(cudaMemset(*d, 0, bytes));
     return OFG_OK;
 }
 
@@ -360,12 +418,12 @@ void ofg_destroy(ofg_ctx *c) {
     if (!c) return;
     cudaStreamSynchronize(c->stream);
     destroy_graphs(c);
-    void *ptrs[] = {c->d_lc, c->d_rc, c->d_bct, c->d_c2f_off, c->d_c2f, c->d_lowOrder, c->d_upOrder, c->d_key, c->d_wdist,
-                    c->d_q[0], c->d_q[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_bcq,
-                    c->d_partial, c->d_scal, c->d_hist, c->d_grad, c->d_lim, c->d_mm, c->d_fix,
+    void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
+                    c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist,
+                    c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr,
+                    c->d_bcq, c->d_partial, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
     for (void *v : ptrs) if (v) cudaFree(v);
-    for (int i = 0; i < 11; ++i) { if (c->d_g64[i]) cudaFree(c->d_g64[i]); if (c->d_g32[i]) cudaFree(c->d_g32[i]); }
     cudaStreamDestroy(c->ownStream ? c->ownStream : c->stream);
     delete c;
 }
@@ -432,57 +490,62 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
 
     // ---- device copies ----
     int rc;
-    if ((rc = upload(c, &c->d_lc, c->lc.data(), nFaces))) return rc;
-    if ((rc = upload(c, &c->d_rc, c->rc.data(), nFaces))) return rc;
+    const bool mixed = c->p.precision == OFG_PREC_MIXED;
+    {
+        NbLists L;
+        build_lists(c, L);
+        std::vector<int> lcb(c->lc.begin(), c->lc.begin() + nBFaces);
+        if ((rc = upload(c, &c->d_lcb, lcb.data(), nBFaces))) return rc;
+        if ((rc = upload(c, &c->d_nb_off, L.nbOff.data(), L.nbOff.size()))) return rc;
+        if ((rc = upload(c, &c->d_nbl, L.nbl.data(), L.nbl.size()))) return rc;
+        if ((rc = upload(c, &c->d_lo_off, L.loOff.data(), L.loOff.size()))) return rc;
+        if ((rc = upload(c, &c->d_lol, L.lol.data(), L.lol.size()))) return rc;
+        if ((rc = upload(c, &c->d_up_off, L.upOff.data(), L.upOff.size()))) return rc;
+        if ((rc = upload(c, &c->d_upl, L.upl.data(), L.upl.size()))) return rc;
+    }
     if ((rc = upload(c, &c->d_bct, c->bct.data(), nBFaces))) return rc;
-    if ((rc = upload(c, &c->d_c2f_off, c->c2f_off.data(), nCells + 1))) return rc;
-    if ((rc = upload(c, &c->d_c2f, c->c2f.data(), c->c2f.size()))) return rc;
     if ((rc = upload(c, &c->d_lowOrder, c->lowOrder.data(), nCells))) return rc;
     if ((rc = upload(c, &c->d_upOrder, c->upOrder.data(), nCells))) return rc;
     if ((rc = upload(c, &c->d_key, c->key.data(), c->nT))) return rc;
     if ((rc = upload(c, &c->d_wdist, c->wdist.data(), nCells))) return rc;
-    const std::vector<double> *geo[11] = {&c->xfn, &c->yfn, &c->zfn, &c->area, &c->xfc, &c->yfc, &c->zfc,
-                                          &c->xcc, &c->ycc, &c->zcc, &c->vol};
-    for (int i = 0; i < 11; ++i) {
-        if (c->p.precision == OFG_PREC_MIXED) {
-            std::vector<float> f(geo[i]->begin(), geo[i]->end());
-            if ((rc = upload(c, &c->d_g32[i], f.data(), f.size()))) return rc;
-        } else {
-            if ((rc = upload(c, &c->d_g64[i], geo[i]->data(), geo[i]->size()))) return rc;
-        }
+    if (mixed) {
+        std::vector<float> fg, cg;
+        pack_geometry(c, fg, cg);
+        if ((rc = upload_bytes(c, &c->d_fgeo, fg.data(), fg.size() * sizeof(float)))) return rc;
+        if ((rc = upload_bytes(c, &c->d_cgeo, cg.data(), cg.size() * sizeof(float)))) return rc;
+    } else {
+        std::vector<double> fg, cg;
+        pack_geometry(c, fg, cg);
+        if ((rc = upload_bytes(c, &c->d_fgeo, fg.data(), fg.size() * sizeof(double)))) return rc;
+        if ((rc = upload_bytes(c, &c->d_cgeo, cg.data(), cg.size() * sizeof(double)))) return rc;
     }
     size_t nT = c->nT, N = nCells;
     if ((rc = upload<double>(c, &c->d_q[0], nullptr, nT * REC))) return rc;
     if ((rc = upload<double>(c, &c->d_q[1], nullptr, nT * REC))) return rc;
+    for (int i = 0; i < 2; ++i) {
+        if (c->d_qs[i]) { cudaFree(c->d_qs[i]); c->d_qs[i] = nullptr; }
+        if (mixed) CK(cudaMalloc(&c->d_qs[i], nT * REC * sizeof(float)));
+    }
     if ((rc = upload<double>(c, &c->d_res, nullptr, N * NEQ))) return rc;
     if ((rc = upload<double>(c, &c->d_dq, nullptr, nT * NEQ))) return rc;
     if ((rc = upload<double>(c, &c->d_dt, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_invsr, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_vissr, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_bcq, nullptr, (size_t)std::max(nBFaces, 1) * NEQ))) return rc;
-    c->nPartialMax = std::max<size_t>((N + 255) / 256 * 10, 2 * 148 * NEQ) + 16;
+    c->nPartialMax = std::max<size_t>((N + 127) / 128 * 10, 2 * 148 * NEQ) + 16;
     if ((rc = upload<double>(c, &c->d_partial, nullptr, c->nPartialMax))) return rc;
     if ((rc = upload<double>(c, &c->d_scal, nullptr, 32))) return rc;
     c->histCap = 1 << 16;
     if ((rc = upload<double>(c, &c->d_hist, nullptr, (size_t)c->histCap * NEQ))) return rc;
     if ((rc = upload<int>(c, &c->d_fix, nullptr, 1 + c->fixcap))) return rc;
-    size_t rs = c->p.precision == OFG_PREC_MIXED ? sizeof(float) : sizeof(double);
-    if (c->d_grad) cudaFree(c->d_grad);
-    if (c->d_lim) cudaFree(c->d_lim);
-    if (c->d_mm) cudaFree(c->d_mm);
-    CK(cudaMalloc(&c->d_grad, N * 18 * rs));
-    CK(cudaMalloc(&c->d_lim, N * NEQ * rs));
-    CK(cudaMalloc(&c->d_mm, N * 10 * rs));
-    CK(cudaMemset(c->d_grad, 0, N * 18 * rs));
+    size_t rs = mixed ? sizeof(float) : sizeof(double);
+    if ((rc = upload_bytes(c, &c->d_gl, nullptr, N * GLR * rs))) return rc;
+    bool venkatGlobal = c->p.ilim == 2 && !c->p.venkat_kh3;
+    if ((rc = upload_bytes(c, &c->d_mm, nullptr, venkatGlobal ? N * MMR * rs : 0))) return rc;
     CK(cudaMemset(c->d_dq, 0, nT * NEQ * sizeof(double)));
     CK(cudaMemset(c->d_bcq, 0, (size_t)std::max(nBFaces, 1) * NEQ * sizeof(double)));
     CK(cudaMemset(c->d_scal, 0, 32 * sizeof(double)));
     CK(cudaMemset(c->d_fix, 0, (1 + c->fixcap) * sizeof(int)));
-    if (c->p.ilim == 0) {
-        // Limiter::CalcNoLimiter: phi = 1 on every cell, every step
-        if (rs == sizeof(float)) { std::vector<float> one(N * NEQ, 1.0f); CK(cudaMemcpy(c->d_lim, one.data(), N * NEQ * rs, cudaMemcpyHostToDevice)); }
-        else { std::vector<double> one(N * NEQ, 1.0); CK(cudaMemcpy(c->d_lim, one.data(), N * NEQ * rs, cudaMemcpyHostToDevice)); }
-    }
     if (has_turb(c)) {
         if (!wall_dist) return c->fail(OFG_E_ARG, "the SA model needs the wall distance");
         for (int i = 0; i < nCells; ++i)
@@ -494,8 +557,7 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         if ((rc = upload<double>(c, &c->d_matL, nullptr, nFaces))) return rc;
         if ((rc = upload<double>(c, &c->d_matR, nullptr, nFaces))) return rc;
         if ((rc = upload<double>(c, &c->d_thist, nullptr, c->histCap))) return rc;
-        if (c->d_gnut) cudaFree(c->d_gnut);
-        CK(cudaMalloc(&c->d_gnut, N * 3 * rs));
+        if ((rc = upload_bytes(c, &c->d_gnut, nullptr, N * 4 * rs))) return rc;
         CK(cudaMemset(c->d_dnut, 0, nT * sizeof(double)));
     }
     c->haveMesh = true;
@@ -661,7 +723,8 @@ int ofg_calc_boundary(ofg_ctx *c, int tid) {
 
 // tasks of one outer iteration (MG::StrongIter: NS relaxation, then SA), with
 // the state-buffer flip between the two solvers
-static const int kNsTasks[] = {T_ADVANCE, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
+// (CALC_TIME_STEP, LOAD_RESIDUALS and UPDATE_RESIDUALS share one gather: T_TS_RES)
+static const int kNsTasks[] = {T_ADVANCE, T_TS_RES, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
 static const int kTurbTasks[] = {T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_NORM};
 
 static int sync_history(ofg_ctx *c) {
@@ -764,16 +827,17 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
         for (int e = 0; e < ne; ++e)
             for (int64_t i = 0; i < nrow; ++i) buf[(size_t)e * ntot + i] = tmp[(size_t)i * ne + e];
     };
-    auto rs_field = [&](const void *d, int ne, int stride, int off) {   // R-typed [N][stride]
-        buf.assign((size_t)ne * nT, 0.0);
+    // gradient+limiter records (R-typed [N][GLR]): component e at off + e * step
+    auto gl_field = [&](int off, int step) {
+        buf.assign((size_t)NEQ * nT, 0.0);
         if (c->p.precision == OFG_PREC_MIXED) {
-            std::vector<float> tmp((size_t)N * stride);
-            cudaMemcpy(tmp.data(), d, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost);
-            for (int e = 0; e < ne; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * stride + e * (stride == 18 ? 3 : 1) + off];
+            std::vector<float> tmp((size_t)N * GLR);
+            cudaMemcpy(tmp.data(), c->d_gl, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost);
+            for (int e = 0; e < NEQ; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * GLR + off + e * step];
         } else {
-            std::vector<double> tmp((size_t)N * stride);
-            cudaMemcpy(tmp.data(), d, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost);
-            for (int e = 0; e < ne; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * stride + e * (stride == 18 ? 3 : 1) + off];
+            std::vector<double> tmp((size_t)N * GLR);
+            cudaMemcpy(tmp.data(), c->d_gl, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost);
+            for (int e = 0; e < NEQ; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * GLR + off + e * step];
         }
     };
     auto host_vec = [&](const std::vector<double> &v) { buf = v; };
@@ -793,10 +857,10 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
     else if (s == "tempr") rec_field(ITT);
     else if (s == "visl") rec_field(IML);
     else if (s == "vist") rec_field(IMT);
-    else if (s == "limiter") rs_field(c->d_lim, NEQ, NEQ, 0);
-    else if (s == "dqdx") rs_field(c->d_grad, NEQ, 18, 0);
-    else if (s == "dqdy") rs_field(c->d_grad, NEQ, 18, 1);
-    else if (s == "dqdz") rs_field(c->d_grad, NEQ, 18, 2);
+    else if (s == "limiter") gl_field(18, 1);
+    else if (s == "dqdx") gl_field(0, 3);
+    else if (s == "dqdy") gl_field(1, 3);
+    else if (s == "dqdz") gl_field(2, 3);
     else if (s == "vol") host_vec(c->vol);
     else if (s == "xcc") host_vec(c->xcc);
     else if (s == "ycc") host_vec(c->ycc);
@@ -841,8 +905,9 @@ int ofg_profile_step(ofg_ctx *c, double *ms, int *launches) {
     double sc[2] = {double(c->outerSteps), double(c->outerSteps)};
     CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_scal + S_THISTN, sc, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    // groups: the 8 NS groups, then SA rhs, lower, upper, update, boundary, norm
-    const int nns = 8, nt = has_turb(c) ? 6 : 0, n = nns + nt;
+    // groups: the 7 NS groups (cfl, time step + residual, lower, upper, update,
+    // boundary, norm), then SA rhs, lower, upper, update, boundary, norm
+    const int nns = 7, nt = has_turb(c) ? 6 : 0, n = nns + nt;
     cudaEvent_t ev[15];
     for (int i = 0; i <= n; ++i) CK(cudaEventCreate(&ev[i]));
     CK(cudaEventRecord(ev[0], c->stream));

@@ -25,18 +25,20 @@ struct ofg_ctx {
     // ---- device ----
     cudaStream_t stream = nullptr;      // stream every launch goes to
     cudaStream_t ownStream = nullptr;   // the context's own stream (set when a caller's stream is in use)
-    int *d_lc = nullptr, *d_rc = nullptr, *d_bct = nullptr, *d_c2f_off = nullptr, *d_c2f = nullptr;
+    int *d_lcb = nullptr, *d_bct = nullptr;                 // left cell and BC code of each boundary face
+    int *d_nb_off = nullptr, *d_nbl = nullptr;              // per-cell neighbour lists (int2 pairs)
+    int *d_lo_off = nullptr, *d_lol = nullptr, *d_up_off = nullptr, *d_upl = nullptr;
     int *d_lowOrder = nullptr, *d_upOrder = nullptr, *d_key = nullptr;
-    double *d_g64[11] = {};    // xfn yfn zfn area xfc yfc zfc | xcc ycc zcc vol
-    float *d_g32[11] = {};
+    void *d_fgeo = nullptr, *d_cgeo = nullptr;              // face / cell records at the face precision
     double *d_wdist = nullptr;
     double *d_q[2] = {nullptr, nullptr};
+    float *d_qs[2] = {nullptr, nullptr};                    // FP32 copies of the state records (mixed path)
     int cur = 0;
     bool pendingNext = false;   // UPDATE_FLOWFIELD wrote d_q[cur^1], CALC_BOUNDARY not yet run
     bool pendingTurb = false;   // SA UPDATE_FLOWFIELD ran, its CALC_BOUNDARY not yet
     double *d_res = nullptr, *d_dq = nullptr, *d_dt = nullptr, *d_invsr = nullptr, *d_vissr = nullptr;
     double *d_bcq = nullptr, *d_partial = nullptr, *d_scal = nullptr, *d_hist = nullptr;
-    void *d_grad = nullptr, *d_lim = nullptr, *d_mm = nullptr;
+    void *d_gl = nullptr, *d_mm = nullptr;                  // gradient+limiter records, min/max differences
     int *d_fix = nullptr;
     // SA solver
     double *d_nut = nullptr, *d_dnut = nullptr, *d_resT = nullptr, *d_impsrT = nullptr, *d_matL = nullptr,
@@ -64,7 +66,7 @@ namespace ofg {
 // tasks executed by the precision-specific launchers
 enum Task {
     T_CFL = 0, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_BOUNDARY_CUR,
-    T_NORM, T_ADVANCE,
+    T_NORM, T_ADVANCE, T_TS_RES,
     T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_BOUNDARY_CUR, T_TURB_NORM
 };
 int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);

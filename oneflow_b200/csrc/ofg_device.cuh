@@ -14,6 +14,10 @@ constexpr double SMALLD = 1.0e-40;   // codes/basic/include/HXTypeBasic.h:34
 constexpr int NEQ = 5;
 constexpr int REC = 8;               // state record: rho u v w p T mul mut
 enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4, ITT = 5, IML = 6, IMT = 7 };
+constexpr int GLR = 24;   // gradient+limiter record: [var*3+dir] for 6 vars (q, T), limiter at 18..22
+constexpr int FGR = 8;    // face record: nx ny nz area xfc yfc zfc -
+constexpr int CGR = 4;    // cell record: xcc ycc zcc vol
+constexpr int MMR = 10;   // neighbour min/max differences per cell (Venkatakrishnan with the zone-wide eps)
 
 // slots of the small device scalar array (cfl, min dt, limiter eps, norms,
 // outer-step counter, residual-history length)
@@ -49,24 +53,6 @@ struct DevParams {
     int iprod_sa, ft2_flag;
     double sa_cb1, sa_cv13, sa_cw2, sa_cw36, sa_ct3, sa_ct4, sa_osigma, sa_cw1, sa_sac2, sa_sac3, sa_cb2s, sa_cw1k,
         sa_okarm2;
-};
-
-// Mesh in device memory: faces SoA, cells SoA, CSR cell->face lists in
-// ascending face id (the reference's c2f order, codes/geometry/src/CellTopo.cpp:95-119).
-template <typename R>
-struct DevGeom {
-    const R *xfn, *yfn, *zfn, *area, *xfc, *yfc, *zfc;   // [nFaces]
-    const R *xcc, *ycc, *zcc, *vol;                       // [nT]
-};
-
-struct DevMesh {
-    int nCells, nBFaces, nFaces, nT;
-    const int *lc, *rc;          // [nFaces]
-    const int *c2f_off;          // [nCells+1]
-    const int *c2f;              // [E] face ids, ascending per cell
-    const int *bcType;           // [nBFaces]
-    const double *walldist;      // [nCells]
-    const int *key;              // [nT] position of each cell in the sweep order (ghosts last)
 };
 
 // Primitive -> conservative, NsInvFlux.cpp:1355-1375 (CalcInternalEnergy :1400-1412)

@@ -1,8 +1,14 @@
-// Kernels of the NS residual + LU-SGS iteration (templated on the face
-// arithmetic type R).  Every kernel is a cell-centred gather over the CSR
-// cell->face list in ascending face id, which is the order in which the
-// reference's serial face loops scatter into a cell, so the FP64
-// accumulations round exactly as the reference's do and no atomics are used.
+// Kernels of the NS residual + LU-SGS iteration, templated on the face
+// arithmetic type R (double: the all-FP64 path; float: FP32 face terms with
+// FP64 accumulation, update and norms).
+//
+// Every kernel is a cell-centred gather over a precomputed per-cell
+// neighbour list in ascending face id -- the order in which the reference's
+// serial face loops scatter into a cell -- so the FP64 accumulations round
+// like the reference's and no atomics are used.  Data is packed for 128-bit
+// loads: the state record (rho,u,v,w,p,T,mu_l,mu_t), the gradient+limiter
+// record, the face record (normal, area, centre) and the cell record
+// (centre, volume).
 #pragma once
 #include "ofg_device.cuh"
 
@@ -12,118 +18,99 @@ namespace ofg {
 template <typename R>
 struct KArgs {
     DevParams P;
-    DevMesh M;
-    DevGeom<R> G;
-    const double *q;      // current state records [nT][REC]
-    double *qn;           // next state records    [nT][REC]
-    double *res;          // [nCells][NEQ]
-    double *dq;           // [nT][NEQ]
-    double *dt, *invsr, *vissr;   // [nCells]
-    double *bcq;          // [nBFaces][NEQ]
-    R *grad;              // [nCells][18]: (var*3 + dir), var 0-4 = q, 5 = T
-    R *lim;               // [nCells][NEQ]
-    double *partial;      // per-block partials
-    double *scal;         // small device scalars (cfl, eps, min dt, norms)
-    int *fixlist;         // [1 + cap]: count, cell ids
-    int fixcap;
-    // Spalart-Allmaras solver
-    double *nut;          // [nT] nu~ (ghosts at nCells + f)
-    double *dnut;         // [nT]
-    double *resT;         // [nCells]
-    double *impsrT;       // [nCells]
-    double *matL, *matR;  // [nFaces] sweep coefficients
-    R *gnut;              // [nCells][3]
+    int nCells, nBFaces, nFaces, nT;
+    const int *nb_off; const int2 *nbl;    // all faces of a cell {face | side<<31, neighbour}
+    const int *lo_off; const int2 *lol;    // faces to earlier cells of the sweep order
+    const int *up_off; const int2 *upl;    // faces to later cells of the sweep order (interior only)
+    const int *bcType;                     // [nBFaces]
+    const int *key;                        // [nT] sweep position
+    const double *walldist;                // [nCells]
+    const R *fgeo;                         // [nFaces][FGR]
+    const R *cgeo;                         // [nT][CGR]
+    const double *q;  double *qn;          // master state records [nT][REC], current / next
+    const R *qs;      R *qsn;              // state records read by face kernels (== master in FP64)
+    double *res, *dq, *dt, *invsr, *vissr, *bcq;
+    R *gl;                                 // [nCells][GLR]
+    R *mm;                                 // [nCells][MMR]
+    double *partial, *scal;
+    int *fixlist; int fixcap;
+    // Spalart-Allmaras
+    double *nut, *dnut, *resT, *impsrT, *matL, *matR;
+    R *gnut;                               // [nCells][4]
 };
 
+// ---------------------------------------------------------------------------
+// vector loads
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ld4(const float *p, float *o) {
+    float4 a = __ldg(reinterpret_cast<const float4 *>(p));
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+}
+__device__ __forceinline__ void ld4(const double *p, double *o) {
+    double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+template <typename T> __device__ __forceinline__ void ld8(const T *p, T *o) { ld4(p, o); ld4(p + 4, o + 4); }
+// plain (coherent) loads for data written earlier in the same kernel launch sequence but
+// possibly by this kernel's other blocks (LU-SGS increments)
+__device__ __forceinline__ void ldc5(const double *p, double *o) {
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) o[e] = p[e];
+}
 
-__device__ __forceinline__ int other_cell(int l, int r, int c) { return l == c ? r : l; }
+__device__ __forceinline__ void st4(float *p, const float *v) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double *p, const double *v) {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+
+__device__ __forceinline__ int nb_face(int2 e) { return e.x & 0x7fffffff; }
+__device__ __forceinline__ bool nb_right(int2 e) { return e.x < 0; }   // the cell is the face's right cell
 
 // ---------------------------------------------------------------------------
-// CALC_TIME_STEP: UTimeStep::CalcTimeStep, codes/uns/src/UTimeStep.cpp:190-416,
-// face radii TimeStep::CalcFaceInvSpec/CalcFaceVisSpec, codes/ns/src/TimeStep.cpp:61-122
+// CALC_TIME_STEP face radii: TimeStep::CalcFaceInvSpec / CalcFaceVisSpec
+// (codes/ns/src/TimeStep.cpp:61-122), as seen from the face's own left/right
 // ---------------------------------------------------------------------------
 template <typename R>
-__device__ __forceinline__ double face_inv_spec(const KArgs<R> &A, int f) {
-    int l = A.M.lc[f], r = A.M.rc[f];
-    const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-    R xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f], ar = A.G.area[f];
-    R gama = R(A.P.gama);
-    R rl = R(ql[IR]), ul = R(ql[IU]), vl = R(ql[IV]), wl = R(ql[IW]), pl = R(ql[IP]);
-    R rr = R(qr[IR]), ur = R(qr[IU]), vr = R(qr[IV]), wr = R(qr[IW]), pr = R(qr[IP]);
-    R vnl = xn * ul + yn * vl + zn * wl - R(0);
-    R vnr = xn * ur + yn * vr + zn * wr - R(0);
+__device__ __forceinline__ double face_inv_spec(const DevParams &P, const R *ql, const R *qr, const R *fg) {
+    R xn = fg[0], yn = fg[1], zn = fg[2], ar = fg[3];
+    R gama = R(P.gama);
+    R vnl = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - R(0);
+    R vnr = xn * qr[IU] + yn * qr[IV] + zn * qr[IW] - R(0);
     R g = R(0.5) * (gama + gama);
-    R pm = R(0.5) * (pl + pr), rm = R(0.5) * (rl + rr);
+    R pm = R(0.5) * (ql[IP] + qr[IP]), rm = R(0.5) * (ql[IR] + qr[IR]);
     R cm = Rsqrt(g * pm / rm);
     R vn = R(0.5) * (vnl + vnr);
     return double(R(0.5) * ar * (Rabs(vn) + cm));
 }
 
 template <typename R>
-__device__ __forceinline__ double face_vis_spec(const KArgs<R> &A, int f) {
-    int l = A.M.lc[f], r = A.M.rc[f];
-    const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-    R ar = A.G.area[f];
-    R vl = R(0.5) * (R(ql[IML]) + R(qr[IML]));
-    R vt = R(0.5) * (R(ql[IMT]) + R(qr[IMT]));
-    R density = R(0.5) * (R(ql[IR]) + R(qr[IR]));
-    if (A.P.visSRModel == 1) {
+__device__ __forceinline__ double face_vis_spec(const DevParams &P, const R *ql, const R *qr, const R *fg,
+                                                const R *cgl, const R *cgr) {
+    R ar = fg[3];
+    R vl = R(0.5) * (ql[IML] + qr[IML]);
+    R vt = R(0.5) * (ql[IMT] + qr[IMT]);
+    R density = R(0.5) * (ql[IR] + qr[IR]);
+    if (P.visSRModel == 1) {
         R c1 = R(4.0) / R(3.0) * (vl + vt);
-        R c2 = R(A.P.gama) * (vl * R(A.P.oprl) + vt * R(A.P.oprt));
-        R c3 = R(2.0) * Rmax(c1, c2) / (R(A.P.reynolds) * density);
+        R c2 = R(P.gama) * (vl * R(P.oprl) + vt * R(P.oprt));
+        R c3 = R(2.0) * Rmax(c1, c2) / (R(P.reynolds) * density);
         return double(ar * ar * c3);
-    } else if (A.P.visSRModel == 2) {
-        R dist = Rabs(A.G.xfn[f] * (A.G.xcc[r] - A.G.xcc[l]) + A.G.yfn[f] * (A.G.ycc[r] - A.G.ycc[l]) +
-                      A.G.zfn[f] * (A.G.zcc[r] - A.G.zcc[l]));
+    } else if (P.visSRModel == 2) {
+        R dist = Rabs(fg[0] * (cgr[0] - cgl[0]) + fg[1] * (cgr[1] - cgl[1]) + fg[2] * (cgr[2] - cgl[2]));
         R viscosity = vl + vt;
-        R c1 = R(2.0) * viscosity / (density * dist * R(A.P.reynolds) + small_v<R>());
+        R c1 = R(2.0) * viscosity / (density * dist * R(P.reynolds) + small_v<R>());
         return double(R(0.5) * c1 * ar);
-    } else if (A.P.visSRModel == 3) {
-        return double(ar * ar / (R(A.P.reynolds) * density + small_v<R>()));
+    } else if (P.visSRModel == 3) {
+        return double(ar * ar / (R(P.reynolds) * density + small_v<R>()));
     }
     return 0.0;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256) k_timestep(KArgs<R> A) {
-    __shared__ double smin[256];
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double mydt = 1.0e40;
-    if (c < A.M.nCells) {
-        double cfl = A.scal[S_CFL];
-        int b = A.M.c2f_off[c], e = A.M.c2f_off[c + 1];
-        double inv = 0.0;
-        for (int k = b; k < e; ++k) inv += face_inv_spec(A, A.M.c2f[k]);
-        double vis = 0.0;
-        if (A.P.vismodel > 0)
-            for (int k = b; k < e; ++k) vis += face_vis_spec(A, A.M.c2f[k]);
-        double vol = double(A.G.vol[c]);
-        double ts;
-        if (A.P.timestepModel == 1) {
-            ts = A.P.global_dt;
-        } else {
-            ts = cfl * vol / inv;
-            if (A.P.vismodel > 0 && A.P.visTimeStepModel > 0) {
-                double vts = cfl * vol / vis;
-                ts *= vts / (ts + vts);
-            }
-        }
-        A.invsr[c] = inv;
-        A.vissr[c] = vis;
-        A.dt[c] = ts;
-        mydt = ts;
-    }
-    smin[threadIdx.x] = mydt;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) A.partial[blockIdx.x] = smin[0];
-}
-
-// UTimeStep::CalcMinTimeStep: zone-wide minimum of the local steps (single
-// block over the per-block partials; min is exact in any order)
+// UTimeStep::CalcMinTimeStep: zone-wide minimum (single block over per-block
+// partials; min is exact in any order)
 template <typename R>
 __global__ void __launch_bounds__(256) k_timestep_min(KArgs<R> A, int nPartial) {
     __shared__ double smin[256];
@@ -143,152 +130,221 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_timestep_clip(KArgs<R> A) {
     if (A.P.timestepModel == 1) return;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
+    if (c >= A.nCells) return;
     double mn = A.scal[S_MINDT];
     if (A.P.timestepModel == 2) { A.dt[c] = mn; return; }
     if (A.P.max_time_ratio > 0) A.dt[c] = fmin(A.dt[c], A.P.max_time_ratio * mn);
 }
 
 // ---------------------------------------------------------------------------
-// Gradients: CalcGradGGCellWeight (codes/usolver/src/UGrad.cpp:88-149) or the
-// face-average Green-Gauss (:40-86); weighted least squares is new.
-// var 0-4: q (rho,u,v,w,p), var 5: temperature (UTGrad, codes/uns/src/UNsGrad.cpp:81-101)
+// Gradients + limiter in one gather.  Gradients: CalcGradGGCellWeight
+// (codes/usolver/src/UGrad.cpp:88-149), the face-average Green-Gauss
+// (:40-86) or weighted least squares (new).  var 0-4: q, var 5: temperature
+// (UTGrad, codes/uns/src/UNsGrad.cpp:81-101).  Limiter: Limiter::CalcMinMaxDiff
+// + CalcBarthLimiter / CalcVencatLimiter (codes/usolver/src/ULimiter.cpp:377-644).
+// limMode: 0 gradients only (limiter preset), 1 local limiter (Barth, or
+// Venkatakrishnan with eps^2 = (K h)^3), 2 min/max and block extremes for the
+// zone-wide Venkatakrishnan eps (limiter in k_limiter_global).
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(128) k_gradient(KArgs<R> A, int nvar) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
-    R gx[6], gy[6], gz[6];
+__device__ __forceinline__ R barth_fn(R dqv, R minv, R maxv, R dot) {
+    if (dot < R(0)) return R(0);
+    else if (dqv > maxv) return maxv / dqv;
+    else if (dqv < minv) return minv / dqv;
+    return R(1);
+}
+template <typename R>
+__device__ __forceinline__ R venkat(R x, R y, R eps) {
+    R x2 = x * x, xy = x * y, y2 = y * y, cc = R(2);
+    return ((x2 + eps + cc * xy) / (x2 + cc * y2 + xy + eps));
+}
+template <typename R>
+__device__ __forceinline__ R venkat_fn(R dqv, R minv, R maxv, R eps) {
+    if (dqv > small_v<R>()) return venkat(maxv, dqv, eps);
+    else if (dqv < -small_v<R>()) return venkat(minv, dqv, eps);
+    return R(1);
+}
+
+// limiter value of cell c over its faces (gradient g, neighbour min/max mn/mx)
+template <typename R>
+__device__ __forceinline__ void cell_limiter(const KArgs<R> &A, int c, const R *cgc, const R *g, const R *mn,
+                                             const R *mx, const R *eps, R *lim) {
 #pragma unroll
-    for (int v = 0; v < 6; ++v) gx[v] = gy[v] = gz[v] = R(0);
-    int b = A.M.c2f_off[c], e = A.M.c2f_off[c + 1];
-    if (A.P.igrad == 2) {
-        // weighted least squares over face neighbours (ghosts included), w = 1/|d|^2
-        R a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, bb[6][3];
-#pragma unroll
-        for (int v = 0; v < 6; ++v) bb[v][0] = bb[v][1] = bb[v][2] = R(0);
-        const double *qc = A.q + (size_t)c * REC;
-        for (int k = b; k < e; ++k) {
-            int f = A.M.c2f[k];
-            int nb = other_cell(A.M.lc[f], A.M.rc[f], c);
-            R dx = A.G.xcc[nb] - A.G.xcc[c], dy = A.G.ycc[nb] - A.G.ycc[c], dz = A.G.zcc[nb] - A.G.zcc[c];
-            R w = R(1) / (dx * dx + dy * dy + dz * dz);
-            a11 += w * dx * dx; a12 += w * dx * dy; a13 += w * dx * dz;
-            a22 += w * dy * dy; a23 += w * dy * dz; a33 += w * dz * dz;
-            const double *qn = A.q + (size_t)nb * REC;
-            for (int v = 0; v < nvar; ++v) {
-                int iv = v < 5 ? v : ITT;
-                R dv = R(qn[iv]) - R(qc[iv]);
-                bb[v][0] += w * dx * dv; bb[v][1] += w * dy * dv; bb[v][2] += w * dz * dv;
-            }
+    for (int e = 0; e < NEQ; ++e) lim[e] = R(1);
+    for (int k = A.nb_off[c]; k < A.nb_off[c + 1]; ++k) {
+        int2 en = __ldg(&A.nbl[k]);
+        int f = nb_face(en);
+        R fg[FGR];
+        ld8(A.fgeo + (size_t)f * FGR, fg);
+        R dx = fg[4] - cgc[0], dy = fg[5] - cgc[1], dz = fg[6] - cgc[2];
+        R dot = R(0);
+        if (A.P.ilim == 1) {
+            R ds = Rsqrt(SQR3(dx, dy, dz));
+            R nd = fg[0] * dx + fg[1] * dy + fg[2] * dz;
+            dot = nb_right(en) ? -nd / (ds + small_v<R>()) : nd / (ds + small_v<R>());
         }
-        if (A.P.dim == 2) {
-            R id = R(1) / (a11 * a22 - a12 * a12);
-            for (int v = 0; v < nvar; ++v) {
-                gx[v] = (a22 * bb[v][0] - a12 * bb[v][1]) * id;
-                gy[v] = (a11 * bb[v][1] - a12 * bb[v][0]) * id;
-                gz[v] = R(0);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) {
+            R dqf = g[e * 3 + 0] * dx + g[e * 3 + 1] * dy + g[e * 3 + 2] * dz;
+            R v = (A.P.ilim == 1) ? barth_fn(dqf, mn[e], mx[e], dot) : venkat_fn(dqf, mn[e], mx[e], eps[e]);
+            lim[e] = Rmin(lim[e], v);
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_gradlim(KArgs<R> A, int nvar, int limMode) {
+    __shared__ double sred[2 * NEQ][128];
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = c < A.nCells;
+    R mn[NEQ], mx[NEQ];
+    if (active) {
+        R qc[REC], cgc[CGR];
+        ld8(A.qs + (size_t)c * REC, qc);
+        ld4(A.cgeo + (size_t)c * CGR, cgc);
+        R gx[6], gy[6], gz[6];
+#pragma unroll
+        for (int v = 0; v < 6; ++v) gx[v] = gy[v] = gz[v] = R(0);
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) mn[e] = mx[e] = qc[e];
+        int b = A.nb_off[c], en = A.nb_off[c + 1];
+        if (A.P.igrad == 2) {
+            // weighted least squares over face neighbours (ghosts included), w = 1/|d|^2
+            R a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, bb[6][3];
+#pragma unroll
+            for (int v = 0; v < 6; ++v) bb[v][0] = bb[v][1] = bb[v][2] = R(0);
+            for (int k = b; k < en; ++k) {
+                int2 e2 = __ldg(&A.nbl[k]);
+                int nb = e2.y;
+                R qn[REC], cgn[CGR];
+                ld8(A.qs + (size_t)nb * REC, qn);
+                ld4(A.cgeo + (size_t)nb * CGR, cgn);
+                R dx = cgn[0] - cgc[0], dy = cgn[1] - cgc[1], dz = cgn[2] - cgc[2];
+                R w = R(1) / (dx * dx + dy * dy + dz * dz);
+                a11 += w * dx * dx; a12 += w * dx * dy; a13 += w * dx * dz;
+                a22 += w * dy * dy; a23 += w * dy * dz; a33 += w * dz * dz;
+#pragma unroll
+                for (int v = 0; v < 6; ++v) {
+                    if (v >= nvar) break;
+                    int iv = v < 5 ? v : ITT;
+                    R dv = qn[iv] - qc[iv];
+                    bb[v][0] += w * dx * dv; bb[v][1] += w * dy * dv; bb[v][2] += w * dz * dv;
+                }
+                if (nb < A.nCells) {
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) { mn[e] = Rmin(mn[e], qn[e]); mx[e] = Rmax(mx[e], qn[e]); }
+                }
+            }
+            if (A.P.dim == 2) {
+                R id = R(1) / (a11 * a22 - a12 * a12);
+#pragma unroll
+                for (int v = 0; v < 6; ++v) {
+                    gx[v] = (a22 * bb[v][0] - a12 * bb[v][1]) * id;
+                    gy[v] = (a11 * bb[v][1] - a12 * bb[v][0]) * id;
+                    gz[v] = R(0);
+                }
+            } else {
+                R c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
+                R c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
+                R id = R(1) / (a11 * c11 + a12 * c12 + a13 * c13);
+#pragma unroll
+                for (int v = 0; v < 6; ++v) {
+                    gx[v] = (c11 * bb[v][0] + c12 * bb[v][1] + c13 * bb[v][2]) * id;
+                    gy[v] = (c12 * bb[v][0] + c22 * bb[v][1] + c23 * bb[v][2]) * id;
+                    gz[v] = (c13 * bb[v][0] + c23 * bb[v][1] + c33 * bb[v][2]) * id;
+                }
             }
         } else {
-            R c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
-            R c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
-            R id = R(1) / (a11 * c11 + a12 * c12 + a13 * c13);
-            for (int v = 0; v < nvar; ++v) {
-                gx[v] = (c11 * bb[v][0] + c12 * bb[v][1] + c13 * bb[v][2]) * id;
-                gy[v] = (c12 * bb[v][0] + c22 * bb[v][1] + c23 * bb[v][2]) * id;
-                gz[v] = (c13 * bb[v][0] + c23 * bb[v][1] + c33 * bb[v][2]) * id;
+            for (int k = b; k < en; ++k) {
+                int2 e2 = __ldg(&A.nbl[k]);
+                int f = nb_face(e2), nb = e2.y;
+                bool right = nb_right(e2);
+                R qn[REC], cgn[CGR], fg[FGR];
+                ld8(A.qs + (size_t)nb * REC, qn);
+                ld4(A.cgeo + (size_t)nb * CGR, cgn);
+                ld8(A.fgeo + (size_t)f * FGR, fg);
+                const R *ql = right ? qn : qc, *qr = right ? qc : qn;
+                const R *cl_ = right ? cgn : cgc, *cr_ = right ? cgc : cgn;
+                R cl, cr;
+                if (A.P.igrad == 1) {
+                    cl = R(0.5); cr = R(0.5);
+                } else {
+                    R dxl = fg[4] - cl_[0], dyl = fg[5] - cl_[1], dzl = fg[6] - cl_[2];
+                    R dxr = fg[4] - cr_[0], dyr = fg[5] - cr_[1], dzr = fg[6] - cr_[2];
+                    R delt1 = Rsqrt(SQR3(dxl, dyl, dzl)), delt2 = Rsqrt(SQR3(dxr, dyr, dzr));
+                    R delta = R(1) / (delt1 + delt2 + small_v<R>());
+                    cl = delt2 * delta; cr = delt1 * delta;
+                }
+                R ar = fg[3];
+                R fnxa = fg[0] * ar, fnya = fg[1] * ar, fnza = fg[2] * ar;
+#pragma unroll
+                for (int v = 0; v < 6; ++v) {
+                    if (v >= nvar) break;
+                    int iv = v < 5 ? v : ITT;
+                    R value = (A.P.igrad == 1) ? R(0.5) * (ql[iv] + qr[iv]) : cl * ql[iv] + cr * qr[iv];
+                    if (!right) { gx[v] += fnxa * value; gy[v] += fnya * value; gz[v] += fnza * value; }
+                    else        { gx[v] -= fnxa * value; gy[v] -= fnya * value; gz[v] -= fnza * value; }
+                }
+                if (nb < A.nCells) {
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) { mn[e] = Rmin(mn[e], qn[e]); mx[e] = Rmax(mx[e], qn[e]); }
+                }
             }
+            R ovol = R(1) / cgc[3];
+#pragma unroll
+            for (int v = 0; v < 6; ++v) { gx[v] *= ovol; gy[v] *= ovol; gz[v] *= ovol; }
         }
-    } else {
-        for (int k = b; k < e; ++k) {
-            int f = A.M.c2f[k];
-            int l = A.M.lc[f], r = A.M.rc[f];
-            R cl, cr;
-            if (A.P.igrad == 1) {
-                cl = R(0.5); cr = R(0.5);
-            } else {
-                R dxl = A.G.xfc[f] - A.G.xcc[l], dyl = A.G.yfc[f] - A.G.ycc[l], dzl = A.G.zfc[f] - A.G.zcc[l];
-                R dxr = A.G.xfc[f] - A.G.xcc[r], dyr = A.G.yfc[f] - A.G.ycc[r], dzr = A.G.zfc[f] - A.G.zcc[r];
-                R delt1 = Rsqrt(SQR3(dxl, dyl, dzl)), delt2 = Rsqrt(SQR3(dxr, dyr, dzr));
-                R delta = R(1) / (delt1 + delt2 + small_v<R>());
-                cl = delt2 * delta; cr = delt1 * delta;
-            }
-            R ar = A.G.area[f];
-            R fnxa = A.G.xfn[f] * ar, fnya = A.G.yfn[f] * ar, fnza = A.G.zfn[f] * ar;
-            const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-            bool left = (l == c);
-            for (int v = 0; v < nvar; ++v) {
-                int iv = v < 5 ? v : ITT;
-                R value = (A.P.igrad == 1) ? R(0.5) * (R(ql[iv]) + R(qr[iv])) : cl * R(ql[iv]) + cr * R(qr[iv]);
-                if (left) { gx[v] += fnxa * value; gy[v] += fnya * value; gz[v] += fnza * value; }
-                else      { gx[v] -= fnxa * value; gy[v] -= fnya * value; gz[v] -= fnza * value; }
-            }
+        R rec[GLR];
+#pragma unroll
+        for (int v = 0; v < 6; ++v) { rec[v * 3] = gx[v]; rec[v * 3 + 1] = gy[v]; rec[v * 3 + 2] = gz[v]; }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) { mn[e] -= qc[e]; mx[e] -= qc[e]; }
+        R lim[NEQ];
+        if (limMode == 1) {
+            R eps[NEQ];
+            R h = A.P.dim == 2 ? Rsqrt(cgc[3]) : R(cbrt(double(cgc[3])));
+            R kk = R(A.P.vencat_coef) * h;
+            R epsc = kk * kk * kk + small_v<R>();
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) eps[e] = epsc;
+            cell_limiter(A, c, cgc, rec, mn, mx, eps, lim);
+        } else {
+            R pre = (A.P.ilim == 0) ? R(1) : R(0);   // CalcNoLimiter / CalcZeroLimiter
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) lim[e] = pre;
         }
-        R ovol = R(1) / A.G.vol[c];
-        for (int v = 0; v < nvar; ++v) { gx[v] *= ovol; gy[v] *= ovol; gz[v] *= ovol; }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) rec[18 + e] = lim[e];
+        rec[23] = R(0);
+        R *o = A.gl + (size_t)c * GLR;
+#pragma unroll
+        for (int i = 0; i < GLR; i += 4) st4(o + i, rec + i);
+        if (limMode == 2) {
+            R *m = A.mm + (size_t)c * MMR;
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) { m[e] = mn[e]; m[5 + e] = mx[e]; }
+        }
     }
-    R *g = A.grad + (size_t)c * 18;
-    for (int v = 0; v < nvar; ++v) { g[v * 3 + 0] = gx[v]; g[v * 3 + 1] = gy[v]; g[v * 3 + 2] = gz[v]; }
-}
-
-// gradient of a (possibly ghost) cell: ghosts carry their interior cell's
-// gradient (UGrad.cpp:140-148)
-__device__ __forceinline__ int grad_cell(const DevMesh &M, int c) {
-    return c < M.nCells ? c : M.lc[c - M.nCells];
-}
-
-// ---------------------------------------------------------------------------
-// Limiter: Limiter::CalcMinMaxDiff + CalcBarthLimiter/CalcVencatLimiter,
-// codes/usolver/src/ULimiter.cpp:377-644.  Pass 1: neighbour min/max
-// differences per cell and the zone-wide extremes (block partials).
-// ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256) k_limiter_minmax(KArgs<R> A, R *mm /* [nCells][10] */) {
-    __shared__ double smn[NEQ][256], smx[NEQ][256];
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double lmin[NEQ], lmax[NEQ];
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e) { lmin[e] = 1.0e40; lmax[e] = -1.0e40; }
-    if (c < A.M.nCells) {
-        const double *qc = A.q + (size_t)c * REC;
-        R mn[NEQ], mx[NEQ];
-#pragma unroll
-        for (int e = 0; e < NEQ; ++e) mn[e] = mx[e] = R(qc[e]);
-        int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
-        for (int k = b; k < en; ++k) {
-            int f = A.M.c2f[k];
-            if (f < A.M.nBFaces) continue;   // only interface boundaries count
-            int nb = other_cell(A.M.lc[f], A.M.rc[f], c);
-            const double *qn = A.q + (size_t)nb * REC;
-#pragma unroll
-            for (int e = 0; e < NEQ; ++e) { mn[e] = Rmin(mn[e], R(qn[e])); mx[e] = Rmax(mx[e], R(qn[e])); }
-        }
-        R *o = mm + (size_t)c * 10;
+    if (limMode == 2) {   // block extremes for the zone-wide eps (ULimiter.cpp:571-593)
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) {
-            mn[e] -= R(qc[e]); mx[e] -= R(qc[e]);
-            o[e] = mn[e]; o[5 + e] = mx[e];
-            lmin[e] = double(mn[e]); lmax[e] = double(mx[e]);
-        }
-    }
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e) { smn[e][threadIdx.x] = lmin[e]; smx[e][threadIdx.x] = lmax[e]; }
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-#pragma unroll
-            for (int e = 0; e < NEQ; ++e) {
-                smn[e][threadIdx.x] = fmin(smn[e][threadIdx.x], smn[e][threadIdx.x + s]);
-                smx[e][threadIdx.x] = fmax(smx[e][threadIdx.x], smx[e][threadIdx.x + s]);
-            }
+            sred[e][threadIdx.x] = active ? double(mn[e]) : 1.0e40;
+            sred[NEQ + e][threadIdx.x] = active ? double(mx[e]) : -1.0e40;
         }
         __syncthreads();
-    }
-    if (threadIdx.x == 0) {
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) {
 #pragma unroll
-        for (int e = 0; e < NEQ; ++e) {
-            A.partial[(size_t)blockIdx.x * 10 + e] = smn[e][0];
-            A.partial[(size_t)blockIdx.x * 10 + 5 + e] = smx[e][0];
+                for (int e = 0; e < NEQ; ++e) {
+                    sred[e][threadIdx.x] = fmin(sred[e][threadIdx.x], sred[e][threadIdx.x + s]);
+                    sred[NEQ + e][threadIdx.x] = fmax(sred[NEQ + e][threadIdx.x], sred[NEQ + e][threadIdx.x + s]);
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int e = 0; e < 2 * NEQ; ++e) A.partial[(size_t)blockIdx.x * 10 + e] = sred[e][0];
         }
     }
 }
@@ -327,106 +383,62 @@ __global__ void __launch_bounds__(256) k_limiter_eps(KArgs<R> A, int nPartial) {
 }
 
 template <typename R>
-__device__ __forceinline__ R barth_fn(R dqv, R minv, R maxv, R dot) {
-    if (dot < R(0)) return R(0);
-    else if (dqv > maxv) return maxv / dqv;
-    else if (dqv < minv) return minv / dqv;
-    return R(1);
-}
-template <typename R>
-__device__ __forceinline__ R venkat(R x, R y, R eps) {
-    R x2 = x * x, xy = x * y, y2 = y * y, cc = R(2);
-    return ((x2 + eps + cc * xy) / (x2 + cc * y2 + xy + eps));
-}
-template <typename R>
-__device__ __forceinline__ R venkat_fn(R dqv, R minv, R maxv, R eps) {
-    if (dqv > small_v<R>()) return venkat(maxv, dqv, eps);
-    else if (dqv < -small_v<R>()) return venkat(minv, dqv, eps);
-    return R(1);
-}
-
-// pass 2: per cell, min over its faces of the face limiter value on its side
-template <typename R>
-__global__ void __launch_bounds__(128) k_limiter(KArgs<R> A, const R *mm) {
+__global__ void __launch_bounds__(128) k_limiter_global(KArgs<R> A) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
-    R lim[NEQ];
+    if (c >= A.nCells) return;
+    R cgc[CGR], rec[GLR];
+    ld4(A.cgeo + (size_t)c * CGR, cgc);
+    R *o = A.gl + (size_t)c * GLR;
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) lim[e] = R(1);
-    const R *g = A.grad + (size_t)c * 18;
-    const R *m = mm + (size_t)c * 10;
-    R eps[NEQ];
-    R epsc = R(0);
-    if (A.P.venkat_kh3) {
-        R h = A.P.dim == 2 ? Rsqrt(A.G.vol[c]) : R(cbrt(double(A.G.vol[c])));
-        R k = R(A.P.vencat_coef) * h;
-        epsc = k * k * k + small_v<R>();
-    }
+    for (int i = 0; i < GLR; i += 4) ld4(o + i, rec + i);
+    const R *m = A.mm + (size_t)c * MMR;
+    R mn[NEQ], mx[NEQ], eps[NEQ], lim[NEQ];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) eps[e] = A.P.venkat_kh3 ? epsc : R(A.scal[S_EPS + e]);
-    int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
-    for (int k = b; k < en; ++k) {
-        int f = A.M.c2f[k];
-        R dx = A.G.xfc[f] - A.G.xcc[c], dy = A.G.yfc[f] - A.G.ycc[c], dz = A.G.zfc[f] - A.G.zcc[c];
-        R dot = R(0);
-        if (A.P.ilim == 1) {
-            R ds = Rsqrt(SQR3(dx, dy, dz));
-            R nd = A.G.xfn[f] * dx + A.G.yfn[f] * dy + A.G.zfn[f] * dz;
-            dot = (A.M.lc[f] == c) ? nd / (ds + small_v<R>()) : -nd / (ds + small_v<R>());
-        }
+    for (int e = 0; e < NEQ; ++e) { mn[e] = m[e]; mx[e] = m[5 + e]; eps[e] = R(A.scal[S_EPS + e]); }
+    cell_limiter(A, c, cgc, rec, mn, mx, eps, lim);
 #pragma unroll
-        for (int e = 0; e < NEQ; ++e) {
-            R dqf = g[e * 3 + 0] * dx + g[e * 3 + 1] * dy + g[e * 3 + 2] * dz;
-            R v = (A.P.ilim == 1) ? barth_fn(dqf, m[e], m[5 + e], dot) : venkat_fn(dqf, m[e], m[5 + e], eps[e]);
-            lim[e] = Rmin(lim[e], v);
-        }
-    }
-    R *o = A.lim + (size_t)c * NEQ;
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e) o[e] = lim[e];
+    for (int e = 0; e < NEQ; ++e) o[18 + e] = lim[e];
 }
 
 // ---------------------------------------------------------------------------
 // UPDATE_RESIDUALS: UNsInvFlux::CalcFlux (codes/uns/src/UNsInvFlux.cpp:123-215)
-// + UNsVisFlux::CalcFlux (codes/uns/src/UNsVisFlux.cpp:90-440), accumulated
-// per cell in ascending face order (AddF2CField, codes/usolver/src/UCom.cpp:144-171).
+// + UNsVisFlux::CalcFlux (codes/uns/src/UNsVisFlux.cpp:90-440), per cell in
+// ascending face order (AddF2CField, codes/usolver/src/UCom.cpp:144-171),
+// fused with the spectral radii and local time step of CALC_TIME_STEP.
 // ---------------------------------------------------------------------------
+// face states qL/qR of face f (left l, right r): NsLimField::BcQlQrFix
+// (codes/uns/src/UNsLimiter.cpp:67-101) on boundary faces, LimField::CalcFaceValue
+// (codes/usolver/src/ULimiter.cpp:188-256) + NsCheckFunction inside
 template <typename R>
-__device__ __forceinline__ void face_states(const KArgs<R> &A, int f, R *t1, R *t2) {
-    int l = A.M.lc[f], r = A.M.rc[f];
-    const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-    if (f < A.M.nBFaces) {
-        // NsLimField::BcQlQrFix, codes/uns/src/UNsLimiter.cpp:67-101
-        if (A.M.bcType[f] == BC_SOLID) {
+__device__ __forceinline__ void face_states(const KArgs<R> &A, int f, const R *ql, const R *qr, const R *fg,
+                                            const R *cgl, const R *cgr, const R *gll, const R *glr, R *t1, R *t2) {
+    if (f < A.nBFaces) {
+        if (A.bcType[f] == BC_SOLID) {
             const double *b = A.bcq + (size_t)f * NEQ;
 #pragma unroll
             for (int e = 0; e < NEQ; ++e) t1[e] = t2[e] = R(b[e]);
         } else {
 #pragma unroll
-            for (int e = 0; e < NEQ; ++e) t1[e] = t2[e] = R(0.5) * (R(ql[e]) + R(qr[e]));
+            for (int e = 0; e < NEQ; ++e) t1[e] = t2[e] = R(0.5) * (ql[e] + qr[e]);
         }
         return;
     }
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) { t1[e] = R(ql[e]); t2[e] = R(qr[e]); }
+    for (int e = 0; e < NEQ; ++e) { t1[e] = ql[e]; t2[e] = qr[e]; }
     if (A.P.ilim == -1) return;   // first order: the zero limiter keeps the cell values
-    // LimField::CalcFaceValue, codes/usolver/src/ULimiter.cpp:188-256
     R u1[NEQ], u2[NEQ];
-    const R *gl = A.grad + (size_t)l * 18, *gr = A.grad + (size_t)r * 18;
-    const R *ll = A.lim + (size_t)l * NEQ, *lr = A.lim + (size_t)r * NEQ;
-    R dx = A.G.xfc[f] - A.G.xcc[l], dy = A.G.yfc[f] - A.G.ycc[l], dz = A.G.zfc[f] - A.G.zcc[l];
+    R dx = fg[4] - cgl[0], dy = fg[5] - cgl[1], dz = fg[6] - cgl[2];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) {
-        R phi = Rmin(ll[e], lr[e]);
-        u1[e] = t1[e] + phi * (gl[e * 3] * dx + gl[e * 3 + 1] * dy + gl[e * 3 + 2] * dz);
+        R phi = Rmin(gll[18 + e], glr[18 + e]);
+        u1[e] = t1[e] + phi * (gll[e * 3] * dx + gll[e * 3 + 1] * dy + gll[e * 3 + 2] * dz);
     }
-    dx = A.G.xfc[f] - A.G.xcc[r]; dy = A.G.yfc[f] - A.G.ycc[r]; dz = A.G.zfc[f] - A.G.zcc[r];
+    dx = fg[4] - cgr[0]; dy = fg[5] - cgr[1]; dz = fg[6] - cgr[2];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) {
-        R phi = Rmin(lr[e], ll[e]);
-        u2[e] = t2[e] + phi * (gr[e * 3] * dx + gr[e * 3 + 1] * dy + gr[e * 3 + 2] * dz);
+        R phi = Rmin(glr[18 + e], gll[18 + e]);
+        u2[e] = t2[e] + phi * (glr[e * 3] * dx + glr[e * 3 + 1] * dy + glr[e * 3 + 2] * dz);
     }
-    // NsCheckFunction, codes/ns/src/NsCom.cpp:133-137
     if (!(u1[IR] <= R(0) || u1[IP] <= R(0)))
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) t1[e] = u1[e];
@@ -435,37 +447,35 @@ __device__ __forceinline__ void face_states(const KArgs<R> &A, int f, R *t1, R *
         for (int e = 0; e < NEQ; ++e) t2[e] = u2[e];
 }
 
-// viscous face flux (VIS_STD face gradient), returns fv[NEQ] before the
-// -S/Re factor; UNsVisFlux::PrepareFaceValue/StdMethod/CalcStress/CalcNsVisFlux
+// viscous face flux with the VIS_STD face gradient, before the -S/Re factor
+// (UNsVisFlux::PrepareFaceValue/StdMethod/CalcStress/CalcNsVisFlux,
+// codes/usolver/src/VisGrad.cpp:150-175,356-366)
 template <typename R>
-__device__ __forceinline__ void face_vis_flux(const KArgs<R> &A, int f, R *fv) {
-    int l = A.M.lc[f], r = A.M.rc[f];
-    const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-    const R *gl = A.grad + (size_t)l * 18, *gr = A.grad + (size_t)grad_cell(A.M, r) * 18;
+__device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, const R *qr, const R *fg, const R *cgl,
+                                              const R *cgr, const R *gl, const R *gr, R *fv) {
     R half = R(0.5);
-    R vlm = half * (R(ql[IML]) + R(qr[IML])), vtm = half * (R(ql[IMT]) + R(qr[IMT]));
+    R vlm = half * (ql[IML] + qr[IML]), vtm = half * (ql[IMT] + qr[IMT]);
     R vis = vlm + vtm;
-    R dx = A.G.xcc[r] - A.G.xcc[l], dy = A.G.ycc[r] - A.G.ycc[l], dz = A.G.zcc[r] - A.G.zcc[l];
+    R dx = cgr[0] - cgl[0], dy = cgr[1] - cgl[1], dz = cgr[2] - cgl[2];
     R ods = R(1) / Rsqrt(SQR3(dx, dy, dz));
     dx *= ods; dy *= ods; dz *= ods;
     R gx[6], gy[6], gz[6], qm[6];
 #pragma unroll
     for (int v = 0; v < 6; ++v) {
         int iv = v < 5 ? v : ITT;
-        R q1 = R(ql[iv]), q2 = R(qr[iv]);
+        R q1 = ql[iv], q2 = qr[iv];
         qm[v] = half * (q1 + q2);
         gx[v] = half * (gl[v * 3] + gr[v * 3]);
         gy[v] = half * (gl[v * 3 + 1] + gr[v * 3 + 1]);
         gz[v] = half * (gl[v * 3 + 2] + gr[v * 3 + 2]);
-        // CorrectGrad, codes/usolver/src/VisGrad.cpp:356-366
         R fOld = gx[v] * dx + gy[v] * dy + gz[v] * dz;
         R fnew = (q2 - q1) * ods;
         R df = fnew - fOld;
         gx[v] += df * dx; gy[v] += df * dy; gz[v] += df * dz;
     }
-    R xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f];
+    R xn = fg[0], yn = fg[1], zn = fg[2];
     R dtdn = xn * gx[5] + yn * gy[5] + zn * gz[5];
-    R kcp = (vlm * R(A.P.oprl) + vtm * R(A.P.oprt)) * R(A.P.const_cp);
+    R kcp = (vlm * R(P.oprl) + vtm * R(P.oprt)) * R(P.const_cp);
     R qNormal = R(0);
     qNormal += xn * R(0) + yn * R(0) + zn * R(0);
     qNormal += kcp * dtdn;
@@ -483,47 +493,144 @@ __device__ __forceinline__ void face_vis_flux(const KArgs<R> &A, int f, R *fv) {
     fv[4] = qm[IU] * fv[1] + qm[IV] * fv[2] + qm[IW] * fv[3] + qNormal;
 }
 
-template <typename R>
+// One gather pass per cell: face radii + time step, inviscid residual and
+// viscous residual.  The FP64 path adds the viscous face terms after all the
+// inviscid ones, as the reference's two scatter passes do; the FP32 path keeps
+// them in a second FP64 accumulator and adds it at the end (one pass over the
+// faces instead of two).
+// MODE 0: residual and time step (one outer iteration), 1: time step only
+// (the CALC_TIME_STEP task), 2: residual only (the UPDATE_RESIDUALS task).
+template <typename R, int MODE>
 __global__ void __launch_bounds__(128) k_residual(KArgs<R> A) {
+    __shared__ double smin[128];
+    constexpr bool exactOrder = sizeof(R) == 8;
+    constexpr bool doRes = MODE != 1, doDt = MODE != 2;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
-    double acc[NEQ];
+    double mydt = 1.0e40;
+    if (c < A.nCells) {
+        const DevParams &P = A.P;
+        R qc[REC], cgc[CGR], glc[GLR];
+        ld8(A.qs + (size_t)c * REC, qc);
+        ld4(A.cgeo + (size_t)c * CGR, cgc);
+        bool needGl = doRes && (P.ilim != -1 || P.vismodel > 0);
+        if (needGl) {
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) acc[e] = -0.0;   // LoadResiduals: res = -rhs, rhs = 0
-    int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
-    R gam = R(A.P.gama), ce1 = R(A.P.centropy1), ce2 = R(A.P.centropy2);
-    for (int k = b; k < en; ++k) {
-        int f = A.M.c2f[k];
-        R t1[NEQ], t2[NEQ], fl[NEQ];
-        face_states(A, f, t1, t2);
-        R xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f], ar = A.G.area[f];
-        if (A.P.ischeme == 12) slau2Flux(t1, t2, xn, yn, zn, gam, fl);
-        else roeFlux(t1, t2, xn, yn, zn, gam, A.P.ieigenfix, ce1, ce2, fl);
-        bool left = A.M.lc[f] == c;
-#pragma unroll
-        for (int e = 0; e < NEQ; ++e) {
-            double v = double(ar * fl[e]);
-            if (left) acc[e] -= v; else acc[e] += v;
+            for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)c * GLR + i, glc + i);
         }
-    }
-    if (A.P.vismodel > 0) {
-        R orey = R(A.P.oreynolds);
+        R gam = R(P.gama), ce1 = R(P.centropy1), ce2 = R(P.centropy2), orey = R(P.oreynolds);
+        double inv = 0.0, vis = 0.0;
+        double acc[NEQ], accv[NEQ];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) { acc[e] = -0.0; accv[e] = 0.0; }   // LoadResiduals: res = -rhs, rhs = 0
+        int b = A.nb_off[c], en = A.nb_off[c + 1];
         for (int k = b; k < en; ++k) {
-            int f = A.M.c2f[k];
-            R fv[NEQ];
-            face_vis_flux(A, f, fv);
-            R coeff = -orey * A.G.area[f];
-            bool left = A.M.lc[f] == c;
+            int2 e2 = __ldg(&A.nbl[k]);
+            int f = nb_face(e2), nb = e2.y;
+            bool right = nb_right(e2);
+            R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
+            ld8(A.qs + (size_t)nb * REC, qn);
+            ld8(A.fgeo + (size_t)f * FGR, fg);
+            ld4(A.cgeo + (size_t)nb * CGR, cgn);
+            bool ghost = nb >= A.nCells;
+            if (needGl && !ghost) {
+#pragma unroll
+                for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)nb * GLR + i, gln + i);
+            }
+            const R *ql = right ? qn : qc, *qr = right ? qc : qn;
+            const R *cgl = right ? cgn : cgc, *cgr = right ? cgc : cgn;
+            // ghost cells carry their interior cell's gradient (UGrad.cpp:140-148)
+            const R *gll = right ? gln : glc, *glr = (right || ghost) ? glc : gln;
+            if (doDt) {
+                inv += face_inv_spec(P, ql, qr, fg);
+                if (P.vismodel > 0) vis += face_vis_spec(P, ql, qr, fg, cgl, cgr);
+            }
+            if (!doRes) continue;
+            R t1[NEQ], t2[NEQ], fl[NEQ];
+            face_states(A, f, ql, qr, fg, cgl, cgr, gll, glr, t1, t2);
+            if (P.ischeme == 12) slau2Flux(t1, t2, fg[0], fg[1], fg[2], gam, fl);
+            else roeFlux(t1, t2, fg[0], fg[1], fg[2], gam, P.ieigenfix, ce1, ce2, fl);
+            R ar = fg[3];
 #pragma unroll
             for (int e = 0; e < NEQ; ++e) {
-                double v = double(coeff * fv[e]);
-                if (left) acc[e] -= v; else acc[e] += v;
+                double v = double(ar * fl[e]);
+                if (!right) acc[e] -= v; else acc[e] += v;
+            }
+            if (!exactOrder && P.vismodel > 0) {
+                R fv[NEQ];
+                face_vis_flux(P, ql, qr, fg, cgl, cgr, gll, glr, fv);
+                R coeff = -orey * ar;
+#pragma unroll
+                for (int e = 0; e < NEQ; ++e) {
+                    double v = double(coeff * fv[e]);
+                    if (!right) accv[e] -= v; else accv[e] += v;
+                }
             }
         }
-    }
-    double *o = A.res + (size_t)c * NEQ;
+        if (doRes && P.vismodel > 0) {
+            if (exactOrder) {
+                for (int k = b; k < en; ++k) {
+                    int2 e2 = __ldg(&A.nbl[k]);
+                    int f = nb_face(e2), nb = e2.y;
+                    bool right = nb_right(e2);
+                    R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
+                    ld8(A.qs + (size_t)nb * REC, qn);
+                    ld8(A.fgeo + (size_t)f * FGR, fg);
+                    ld4(A.cgeo + (size_t)nb * CGR, cgn);
+                    bool ghost = nb >= A.nCells;
+                    if (!ghost) {
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) o[e] = acc[e];
+                        for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)nb * GLR + i, gln + i);
+                    }
+                    const R *ql = right ? qn : qc, *qr = right ? qc : qn;
+                    const R *cgl = right ? cgn : cgc, *cgr = right ? cgc : cgn;
+                    const R *gll = right ? gln : glc, *glr = (right || ghost) ? glc : gln;
+                    R fv[NEQ];
+                    face_vis_flux(P, ql, qr, fg, cgl, cgr, gll, glr, fv);
+                    R coeff = -orey * fg[3];
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) {
+                        double v = double(coeff * fv[e]);
+                        if (!right) acc[e] -= v; else acc[e] += v;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < NEQ; ++e) acc[e] += accv[e];
+            }
+        }
+        if (doRes) {
+            double *o = A.res + (size_t)c * NEQ;
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) o[e] = acc[e];
+        }
+        if (doDt) {
+            // local time step (UTimeStep::CalcInvTimeStep / CalcVisTimeStep)
+            double cfl = A.scal[S_CFL];
+            double vol = double(cgc[3]);
+            double ts;
+            if (P.timestepModel == 1) {
+                ts = P.global_dt;
+            } else {
+                ts = cfl * vol / inv;
+                if (P.vismodel > 0 && P.visTimeStepModel > 0) {
+                    double vts = cfl * vol / vis;
+                    ts *= vts / (ts + vts);
+                }
+            }
+            A.invsr[c] = inv;
+            A.vissr[c] = vis;
+            A.dt[c] = ts;
+            mydt = ts;
+        }
+    }
+    if (!doDt) return;
+    smin[threadIdx.x] = mydt;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) A.partial[blockIdx.x] = smin[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -531,17 +638,16 @@ __global__ void __launch_bounds__(128) k_residual(KArgs<R> A) {
 // face increment NsLusgs::GetStandardFluxIncrement (codes/ns/src/NsLusgs.cpp:121-202)
 // with the Roe-averaged face radius (UNsLusgs::PrepareDataFacePrim :251-293)
 // and the viscous radius (UNsLusgs::CalcViscousTerm :295-330).  Level-scheduled:
-// every cell of a level only reads dq of cells in earlier levels.
+// every cell of a level only reads increments of cells in earlier levels.
 // ---------------------------------------------------------------------------
+// qa: the cell being solved (left after GCom::SetGeometry's swap), qb: neighbour
 template <typename R>
-__device__ __forceinline__ void face_increment(const KArgs<R> &A, int ci, int f, double *rhs0) {
-    int l = A.M.lc[f], r = A.M.rc[f];
-    R xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f], fa = A.G.area[f], vfn = R(0);
-    if (r == ci) { r = l; l = ci; xn = -xn; yn = -yn; zn = -zn; vfn = -vfn; }
-    const double *qa = A.q + (size_t)l * REC, *qb = A.q + (size_t)r * REC;
-    R half = R(0.5), one = R(1), gl = R(A.P.gama), gr = gl;
-    R rl = R(qa[IR]), ul = R(qa[IU]), vl = R(qa[IV]), wl = R(qa[IW]), pl = R(qa[IP]);
-    R rr = R(qb[IR]), ur = R(qb[IU]), vr = R(qb[IV]), wr = R(qb[IW]), pr = R(qb[IP]);
+__device__ __forceinline__ void face_increment(const DevParams &P, const R *qa, const R *qb, const double *dqj, R xn,
+                                               R yn, R zn, R fa, const R *cga, const R *cgb, double *rhs0) {
+    R vfn = R(0);
+    R half = R(0.5), one = R(1), gl = R(P.gama), gr = gl;
+    R rl = qa[IR], ul = qa[IU], vl = qa[IV], wl = qa[IW], pl = qa[IP];
+    R rr = qb[IR], ur = qb[IU], vr = qb[IV], wr = qb[IW], pr = qb[IP];
     R hl = gl / (gl - one) * pl / rl + half * SQR3(ul, vl, wl);
     R hr = gr / (gr - one) * pr / rr + half * SQR3(ur, vr, wr);
     R tmp0 = Rsqrt(rr / rl);
@@ -557,7 +663,6 @@ __device__ __forceinline__ void face_increment(const KArgs<R> &A, int ci, int f,
     R cmf = Rsqrt(c2f_);
     R vnf = xn * um + yn * vm + zn * wm;
     R maxEig = Rabs(vnf - vfn) + cmf;
-    const double *dqj = A.dq + (size_t)r * NEQ;
     R d0 = R(dqj[0]), d1 = R(dqj[1]), d2 = R(dqj[2]), d3 = R(dqj[3]), d4 = R(dqj[4]);
     R rj = rr, uj = ur, vj = vr, wj = wr, pj = pr;
     R c2 = Rabs(gama * pj / rj);
@@ -588,19 +693,19 @@ __device__ __forceinline__ void face_increment(const KArgs<R> &A, int ci, int f,
     df[4] = lmd1 * d4 - htot * term1 + vn_fluid * term2;
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) df[e] *= fa;
-    if (A.P.vismodel > 0) {
-        R vl_ = R(qb[IML]), vt_ = R(qb[IMT]);
+    if (P.vismodel > 0) {
+        R vl_ = qb[IML], vt_ = qb[IMT];
         R visrad;
         R density = half * (rl + rr);
-        if (A.P.visSRModel == 1) {
+        if (P.visSRModel == 1) {
             R c1 = R(4.0) / R(3.0) * (vl_ + vt_);
-            R cc2 = R(A.P.gama) * (vl_ * R(A.P.oprl) + vt_ * R(A.P.oprt));
-            R c3 = R(2) * Rmax(c1, cc2) / (R(A.P.reynolds) * density);
-            visrad = fa * fa * c3 / A.G.vol[r];
+            R cc2 = R(P.gama) * (vl_ * R(P.oprl) + vt_ * R(P.oprt));
+            R c3 = R(2) * Rmax(c1, cc2) / (R(P.reynolds) * density);
+            visrad = fa * fa * c3 / cgb[3];
         } else {
-            R dist = Rabs(xn * (A.G.xcc[r] - A.G.xcc[l]) + yn * (A.G.ycc[r] - A.G.ycc[l]) + zn * (A.G.zcc[r] - A.G.zcc[l]));
+            R dist = Rabs(xn * (cgb[0] - cga[0]) + yn * (cgb[1] - cga[1]) + zn * (cgb[2] - cga[2]));
             R viscosity = vl_ + vt_;
-            R c1 = R(2) * viscosity / (density * dist * R(A.P.reynolds) + small_v<R>());
+            R c1 = R(2) * viscosity / (density * dist * R(P.reynolds) + small_v<R>());
             visrad = half * c1 * fa;
         }
         rhs0[0] -= double(visrad * d0); rhs0[1] -= double(visrad * d1); rhs0[2] -= double(visrad * d2);
@@ -611,9 +716,29 @@ __device__ __forceinline__ void face_increment(const KArgs<R> &A, int ci, int f,
 }
 
 template <typename R>
+__device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *off, const int2 *list, double *rhs0) {
+    R qc[REC], cgc[CGR];
+    ld8(A.qs + (size_t)c * REC, qc);
+    ld4(A.cgeo + (size_t)c * CGR, cgc);
+    for (int k = off[c]; k < off[c + 1]; ++k) {
+        int2 e2 = __ldg(&list[k]);
+        int f = nb_face(e2), nb = e2.y;
+        R qn[REC], cgn[CGR], fg[FGR];
+        double dqj[NEQ];
+        ld8(A.qs + (size_t)nb * REC, qn);
+        ld4(A.cgeo + (size_t)nb * CGR, cgn);
+        ld4(A.fgeo + (size_t)f * FGR, fg);
+        ldc5(A.dq + (size_t)nb * NEQ, dqj);
+        R xn = fg[0], yn = fg[1], zn = fg[2];
+        if (nb_right(e2)) { xn = -xn; yn = -yn; zn = -zn; }   // GCom::SetGeometry
+        face_increment(A.P, qc, qn, dqj, xn, yn, zn, fg[3], cgc, cgn, rhs0);
+    }
+}
+
+template <typename R>
 __device__ __forceinline__ double implicit_radius(const KArgs<R> &A, int c) {
     // UNsSpectrum::CalcImplicitSpectrum (sp2 = 1 for a steady solve)
-    double s = (1.0 / A.dt[c]) * double(A.G.vol[c]);
+    double s = (1.0 / A.dt[c]) * double(A.cgeo[(size_t)c * CGR + 3]);
     s += A.invsr[c];
     s += A.vissr[c];
     return s;
@@ -625,13 +750,7 @@ __global__ void __launch_bounds__(128) k_lusgs_lower(KArgs<R> A, const int *orde
     if (t >= count) return;
     int c = order[start + t];
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
-    int kc = A.M.key[c];
-    for (int k = b; k < en; ++k) {
-        int f = A.M.c2f[k];
-        if (A.M.key[A.M.lc[f]] > kc || A.M.key[A.M.rc[f]] > kc) continue;   // UNsLusgs::CanNotLowerSolve
-        face_increment(A, c, f, rhs0);
-    }
+    sweep_rhs0(A, c, A.lo_off, A.lol, rhs0);
     double rad = implicit_radius(A, c);
     const double *rs = A.res + (size_t)c * NEQ;
     double *d = A.dq + (size_t)c * NEQ;
@@ -645,14 +764,7 @@ __global__ void __launch_bounds__(128) k_lusgs_upper(KArgs<R> A, const int *orde
     if (t >= count) return;
     int c = order[start + t];
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
-    int kc = A.M.key[c];
-    for (int k = b; k < en; ++k) {
-        int f = A.M.c2f[k];
-        if (f < A.M.nBFaces) continue;   // ghost dq is zero: no contribution
-        if (A.M.key[A.M.lc[f]] < kc || A.M.key[A.M.rc[f]] < kc) continue;   // UNsLusgs::CanNotUpperSolve
-        face_increment(A, c, f, rhs0);
-    }
+    sweep_rhs0(A, c, A.up_off, A.upl, rhs0);   // ghost increments are zero: boundary faces not listed
     double rad = implicit_radius(A, c);
     double *d = A.dq + (size_t)c * NEQ;
 #pragma unroll
@@ -663,8 +775,8 @@ __global__ void __launch_bounds__(128) k_lusgs_upper(KArgs<R> A, const int *orde
 // UPDATE_FLOWFIELD_LUSGS: NsUpdate::CalcFlowField + WeekSolutionFix
 // (codes/ns/src/NsUpdate.cpp:40-67,192-217), QToPrim (codes/ns/src/NsInvFlux.cpp:1377-1399);
 // then the interior half of CALC_BOUNDARY: NsCalcGamaT + CalcLaminarViscosity.
-// Writes the next state buffer; cells that still fail go to a list for the
-// sequential neighbour-average fix (UNsUpdate::SolutionFix).
+// Writes the next state buffer (and its FP32 copy); cells that still fail go
+// to a list for the neighbour-average fix (UNsUpdate::SolutionFix).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double sutherland(const DevParams &P, double t) {
     // codes/model/src/Sutherland.cpp:62-66
@@ -673,9 +785,39 @@ __device__ __forceinline__ double sutherland(const DevParams &P, double t) {
 }
 
 template <typename R>
+__device__ __forceinline__ void store_state(const KArgs<R> &A, int i, const double *rec) {
+    double *o = A.qn + (size_t)i * REC;
+    st4(o, rec);
+    st4(o + 4, rec + 4);
+    if (sizeof(R) == 4) {
+        R s[REC];
+#pragma unroll
+        for (int e = 0; e < REC; ++e) s[e] = R(rec[e]);
+        st4(A.qsn + (size_t)i * REC, s);
+        st4(A.qsn + (size_t)i * REC + 4, s + 4);
+    }
+}
+
+// NsCalcGamaT(F_INNER) + CalcLaminarViscosity(F_INNER) on the current buffer
+// (after a state upload or the initial field); refreshes the FP32 copy too
+template <typename R>
+__global__ void __launch_bounds__(256) k_interior_tvisl(KArgs<R> A) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.nCells) return;
+    const double *qc = A.q + (size_t)c * REC;
+    double rec[REC];
+#pragma unroll
+    for (int e = 0; e < REC; ++e) rec[e] = qc[e];
+    double t = rec[IP] / (A.P.statecoef * rec[IR] * 1.0);
+    rec[ITT] = t;
+    rec[IML] = fmax(0.0, sutherland(A.P, t));
+    store_state(A, c, rec);
+}
+
+template <typename R>
 __global__ void __launch_bounds__(256) k_update(KArgs<R> A) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
+    if (c >= A.nCells) return;
     const double *qc = A.q + (size_t)c * REC;
     const double *d = A.dq + (size_t)c * NEQ;
     double gama = A.P.gama;
@@ -706,21 +848,23 @@ __global__ void __launch_bounds__(256) k_update(KArgs<R> A) {
             if (slot < A.fixcap) A.fixlist[1 + slot] = c;
         }
     }
-    double *o = A.qn + (size_t)c * REC;
+    double rec[REC];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) o[e] = pr[e];
+    for (int e = 0; e < NEQ; ++e) rec[e] = pr[e];
+    rec[ITT] = 0.0; rec[IML] = 0.0;
     if (!needFix) {
         double t = pr[IP] / (A.P.statecoef * pr[IR] * 1.0);
-        o[ITT] = t;
-        o[IML] = fmax(0.0, sutherland(A.P, t));
+        rec[ITT] = t;
+        rec[IML] = fmax(0.0, sutherland(A.P, t));
     }
-    o[IMT] = qc[IMT];
+    rec[IMT] = qc[IMT];
+    store_state(A, c, rec);
 }
 
 // UNsUpdate::SolutionFix (codes/uns/src/UNsUpdate.cpp:94-133) for the cells
-// that failed every positivity retry.  The reference updates in place in
-// natural order, so a neighbour with a lower id contributes its new value and
-// one with a higher id its old value; one thread replays that order.
+// that failed every positivity retry.  The reference updates in place in its
+// sweep order, so a neighbour earlier in that order contributes its new value
+// and a later one its old value; one thread replays that order.
 template <typename R>
 __global__ void k_solution_fix(KArgs<R> A) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -728,18 +872,17 @@ __global__ void k_solution_fix(KArgs<R> A) {
     if (n <= 0) return;
     if (n > A.fixcap) n = A.fixcap;
     int *ids = A.fixlist + 1;
-    for (int i = 1; i < n; ++i) {   // insertion sort (the list is short)
+    for (int i = 1; i < n; ++i) {   // insertion sort by sweep position (the list is short)
         int v = ids[i], j = i - 1;
-        while (j >= 0 && A.M.key[ids[j]] > A.M.key[v]) { ids[j + 1] = ids[j]; --j; }
+        while (j >= 0 && A.key[ids[j]] > A.key[v]) { ids[j + 1] = ids[j]; --j; }
         ids[j + 1] = v;
     }
     for (int i = 0; i < n; ++i) {
         int c = ids[i];
         double pr[NEQ] = {0, 0, 0, 0, 0}, sumV = 0.0;
-        for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
-            int f = A.M.c2f[k];
-            int nb = other_cell(A.M.lc[f], A.M.rc[f], c);
-            bool done = nb < A.M.nCells && A.M.key[nb] < A.M.key[c];   // already updated in sweep order
+        for (int k = A.nb_off[c]; k < A.nb_off[c + 1]; ++k) {
+            int nb = A.nbl[k].y;
+            bool done = nb < A.nCells && A.key[nb] < A.key[c];
             const double *src = done ? A.qn + (size_t)nb * REC : A.q + (size_t)nb * REC;
             sumV += 1.0;
             for (int e = 0; e < NEQ; ++e) {
@@ -749,11 +892,13 @@ __global__ void k_solution_fix(KArgs<R> A) {
             }
         }
         double rv = 1.0 / sumV;
-        double *o = A.qn + (size_t)c * REC;
-        for (int e = 0; e < NEQ; ++e) o[e] = pr[e] * rv;
-        double t = o[IP] / (A.P.statecoef * o[IR] * 1.0);
-        o[ITT] = t;
-        o[IML] = fmax(0.0, sutherland(A.P, t));
+        double rec[REC];
+        for (int e = 0; e < NEQ; ++e) rec[e] = pr[e] * rv;
+        double t = rec[IP] / (A.P.statecoef * rec[IR] * 1.0);
+        rec[ITT] = t;
+        rec[IML] = fmax(0.0, sutherland(A.P, t));
+        rec[IMT] = A.q[(size_t)c * REC + IMT];
+        store_state(A, c, rec);
     }
     A.fixlist[0] = 0;
 }
@@ -761,19 +906,21 @@ __global__ void k_solution_fix(KArgs<R> A) {
 // ---------------------------------------------------------------------------
 // CALC_BOUNDARY, ghost half: UNsBcSolver::CalcBc (codes/uns/src/UNsBcSolver.cpp:55-166)
 // with NsBcSolver's face BCs (codes/ns/src/NsBcSolver.cpp:51-440), then
-// NsCalcGamaT + CalcLaminarViscosity on the ghost cells.  Operates on qn.
+// NsCalcGamaT + CalcLaminarViscosity on the ghost cells.  Operates on qn
+// (interior cells already final), ghost records written to qn.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(256) k_boundary(KArgs<R> A) {
+__global__ void __launch_bounds__(256) k_boundary(KArgs<R> A, const int *lcb) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= A.M.nBFaces) return;
-    int bt = A.M.bcType[f];
-    int l = A.M.lc[f];
+    if (f >= A.nBFaces) return;
+    int bt = A.bcType[f];
+    int l = lcb[f];
     const double *s = A.qn + (size_t)l * REC;
-    double *g = A.qn + (size_t)(A.M.nCells + f) * REC;
+    int g = A.nCells + f;
     double t[NEQ], pr[NEQ];
     bool havePrim = false;
-    double xn = double(A.G.xfn[f]), yn = double(A.G.yfn[f]), zn = double(A.G.zfn[f]), vfn = 0.0;
+    const R *fg = A.fgeo + (size_t)f * FGR;
+    double xn = double(fg[0]), yn = double(fg[1]), zn = double(fg[2]), vfn = 0.0;
     double gama = A.P.gama;
     if (bt == BC_SYM || (bt == BC_SOLID && A.P.vismodel == 0)) {
         double vn = xn * s[IU] + yn * s[IV] + zn * s[IW] - vfn;
@@ -853,12 +1000,14 @@ __global__ void __launch_bounds__(256) k_boundary(KArgs<R> A) {
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) t[e] = s[e];
     }
+    double rec[REC];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) g[e] = t[e];
+    for (int e = 0; e < NEQ; ++e) rec[e] = t[e];
     double tt = t[IP] / (A.P.statecoef * t[IR] * 1.0);
-    g[ITT] = tt;
-    g[IML] = fmax(0.0, sutherland(A.P, tt));
-    g[IMT] = A.q[(size_t)(A.M.nCells + f) * REC + IMT];   // ghost eddy viscosity is set by the SA solver
+    rec[ITT] = tt;
+    rec[IML] = fmax(0.0, sutherland(A.P, tt));
+    rec[IMT] = A.q[(size_t)g * REC + IMT];   // ghost eddy viscosity is set by the SA solver
+    store_state(A, g, rec);
     if (havePrim) {
         double *b = A.bcq + (size_t)f * NEQ;
 #pragma unroll
@@ -875,7 +1024,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) k_norm_partial(KArgs<R> A) {
     __shared__ double s[NEQ][256];
     double acc[NEQ] = {0, 0, 0, 0, 0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.M.nCells; c += gridDim.x * blockDim.x) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.nCells; c += gridDim.x * blockDim.x) {
         const double *r = A.res + (size_t)c * NEQ;
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) acc[e] += r[e] * r[e];
@@ -912,7 +1061,7 @@ __global__ void __launch_bounds__(256) k_norm_final(KArgs<R> A, int nPartial, do
     }
     if (threadIdx.x == 0) {
         for (int e = 0; e < NEQ; ++e) {
-            double rms = sqrt(s[e][0] / A.M.nCells);
+            double rms = sqrt(s[e][0] / A.nCells);
             A.scal[S_NORM + e] = rms;
             if (hist) hist[e] = rms;
         }

@@ -8,7 +8,6 @@
 
 namespace ofg {
 
-
 // CFL ramp (TimeStep::CalcCfl, codes/ns/src/TimeStep.cpp:43-59).  step < 0:
 // advance the device-side outer-step counter first (graph path).
 static __global__ void k_cfl(double *scal, double step, double cflst, double cfled, int ncfl) {
@@ -23,16 +22,6 @@ static __global__ void k_cfl(double *scal, double step, double cflst, double cfl
     scal[S_CFL] = cfl;
 }
 
-// NsCalcGamaT(F_INNER) + CalcLaminarViscosity(F_INNER) on a state buffer
-static __global__ void k_interior_tvisl(DevParams P, int nCells, double *q) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nCells) return;
-    double *o = q + (size_t)c * REC;
-    double t = o[IP] / (P.statecoef * o[IR] * 1.0);
-    o[ITT] = t;
-    o[IML] = fmax(0.0, sutherland(P, t));
-}
-
 static __global__ void k_norm_hist(double *scal, double *hist, int cap) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     int n = int(scal[S_HISTN]);
@@ -41,32 +30,31 @@ static __global__ void k_norm_hist(double *scal, double *hist, int cap) {
     scal[S_HISTN] = double(n + 1);
 }
 
-template <typename R> DevGeom<R> make_geom(ofg_ctx *c);
-template <> inline DevGeom<double> make_geom<double>(ofg_ctx *c) {
-    double **g = c->d_g64;
-    return DevGeom<double>{g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], g[9], g[10]};
-}
-template <> inline DevGeom<float> make_geom<float>(ofg_ctx *c) {
-    float **g = c->d_g32;
-    return DevGeom<float>{g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], g[9], g[10]};
-}
-
 template <typename R>
 KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
     KArgs<R> A;
     A.P = c->dp;
-    A.M.nCells = c->nCells; A.M.nBFaces = c->nBFaces; A.M.nFaces = c->nFaces; A.M.nT = c->nT;
-    A.M.lc = c->d_lc; A.M.rc = c->d_rc; A.M.c2f_off = c->d_c2f_off; A.M.c2f = c->d_c2f; A.M.bcType = c->d_bct;
-    A.M.walldist = c->d_wdist;
-    A.M.key = c->d_key;
-    A.G = make_geom<R>(c);
+    A.nCells = c->nCells; A.nBFaces = c->nBFaces; A.nFaces = c->nFaces; A.nT = c->nT;
+    A.nb_off = c->d_nb_off; A.nbl = reinterpret_cast<const int2 *>(c->d_nbl);
+    A.lo_off = c->d_lo_off; A.lol = reinterpret_cast<const int2 *>(c->d_lol);
+    A.up_off = c->d_up_off; A.upl = reinterpret_cast<const int2 *>(c->d_upl);
+    A.bcType = c->d_bct; A.key = c->d_key; A.walldist = c->d_wdist;
+    A.fgeo = static_cast<const R *>(c->d_fgeo); A.cgeo = static_cast<const R *>(c->d_cgeo);
+    int nx = onCurrent ? c->cur : c->cur ^ 1;
     A.q = c->d_q[c->cur];
-    A.qn = onCurrent ? c->d_q[c->cur] : c->d_q[c->cur ^ 1];
+    A.qn = c->d_q[nx];
+    if (sizeof(R) == 4) {
+        A.qs = reinterpret_cast<const R *>(c->d_qs[c->cur]);
+        A.qsn = reinterpret_cast<R *>(c->d_qs[nx]);
+    } else {
+        A.qs = reinterpret_cast<const R *>(A.q);
+        A.qsn = reinterpret_cast<R *>(A.qn);
+    }
     A.res = c->d_res; A.dq = c->d_dq; A.dt = c->d_dt; A.invsr = c->d_invsr; A.vissr = c->d_vissr;
-    A.bcq = c->d_bcq; A.grad = (R *)c->d_grad; A.lim = (R *)c->d_lim; A.partial = c->d_partial;
-    A.scal = c->d_scal; A.fixlist = c->d_fix; A.fixcap = c->fixcap;
+    A.bcq = c->d_bcq; A.gl = static_cast<R *>(c->d_gl); A.mm = static_cast<R *>(c->d_mm);
+    A.partial = c->d_partial; A.scal = c->d_scal; A.fixlist = c->d_fix; A.fixcap = c->fixcap;
     A.nut = c->d_nut; A.dnut = c->d_dnut; A.resT = c->d_resT; A.impsrT = c->d_impsrT;
-    A.matL = c->d_matL; A.matR = c->d_matR; A.gnut = (R *)c->d_gnut;
+    A.matL = c->d_matL; A.matR = c->d_matR; A.gnut = static_cast<R *>(c->d_gnut);
     return A;
 }
 
@@ -77,6 +65,23 @@ inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
         kern<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__);               \
         ++c->launches;                                                     \
     } while (0)
+
+// gradients and limiter of the current state (UPDATE_RESIDUALS' first half)
+template <typename R>
+void launch_gradlim(ofg_ctx *c, const KArgs<R> &A, cudaStream_t s) {
+    const int N = c->nCells;
+    bool needGrad = c->p.ilim != -1 || c->p.vismodel > 0;
+    if (!needGrad) return;
+    int nvar = c->p.vismodel > 0 ? 6 : 5;
+    bool venkatGlobal = c->p.ilim == 2 && !c->p.venkat_kh3;
+    int limMode = (c->p.ilim == 1 || c->p.ilim == 2) ? (venkatGlobal ? 2 : 1) : 0;
+    int nb = nblk(N, 128);
+    OFG_LAUNCH(k_gradlim<R>, nb, 128, s, A, nvar, limMode);
+    if (limMode == 2) {
+        OFG_LAUNCH(k_limiter_eps<R>, 1, 256, s, A, nb);
+        OFG_LAUNCH(k_limiter_global<R>, nb, 128, s, A);
+    }
+}
 
 template <typename R>
 int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
@@ -90,31 +95,27 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         OFG_LAUNCH(k_cfl, 1, 32, s, c->d_scal, -1.0, c->p.cflst, c->p.cfled, c->p.ncfl);
         break;
     }
-    case T_TIMESTEP: {
+    case T_TIMESTEP: {   // CALC_TIME_STEP alone
         KArgs<R> A = make_args<R>(c, false);
-        int nb = nblk(N, 256);
-        OFG_LAUNCH(k_timestep<R>, nb, 256, s, A);
+        int nb = nblk(N, 128);
+        OFG_LAUNCH((k_residual<R, 1>), nb, 128, s, A);
         OFG_LAUNCH(k_timestep_min<R>, 1, 256, s, A, nb);
-        OFG_LAUNCH(k_timestep_clip<R>, nb, 256, s, A);
+        OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }
-    case T_RESIDUAL: {
+    case T_RESIDUAL: {   // UPDATE_RESIDUALS alone
         KArgs<R> A = make_args<R>(c, false);
-        bool needGrad = c->p.ilim != -1 || c->p.vismodel > 0;
-        if (needGrad) {
-            int nvar = c->p.vismodel > 0 ? 6 : 5;
-            OFG_LAUNCH(k_gradient<R>, nblk(N, 128), 128, s, A, nvar);
-        }
-        if (c->p.ilim == 1 || c->p.ilim == 2) {
-            int nb = nblk(N, 256);
-            OFG_LAUNCH(k_limiter_minmax<R>, nb, 256, s, A, (R *)c->d_mm);
-            if (c->p.ilim == 2 && !c->p.venkat_kh3) OFG_LAUNCH(k_limiter_eps<R>, 1, 256, s, A, nb);
-            OFG_LAUNCH(k_limiter<R>, nblk(N, 128), 128, s, A, (const R *)c->d_mm);
-        } else if (c->p.ilim == 0) {
-            // no limiter: phi = 1 everywhere (Limiter::CalcNoLimiter)
-            // handled by a fill done once at mesh upload
-        }
-        OFG_LAUNCH(k_residual<R>, nblk(N, 128), 128, s, A);
+        launch_gradlim<R>(c, A, s);
+        OFG_LAUNCH((k_residual<R, 2>), nblk(N, 128), 128, s, A);
+        break;
+    }
+    case T_TS_RES: {     // CALC_TIME_STEP + LOAD_RESIDUALS + UPDATE_RESIDUALS in one gather
+        KArgs<R> A = make_args<R>(c, false);
+        launch_gradlim<R>(c, A, s);
+        int nb = nblk(N, 128);
+        OFG_LAUNCH((k_residual<R, 0>), nb, 128, s, A);
+        OFG_LAUNCH(k_timestep_min<R>, 1, 256, s, A, nb);
+        OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }
     case T_LOWER: {
@@ -143,13 +144,13 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     }
     case T_BOUNDARY_NEXT: {
         KArgs<R> A = make_args<R>(c, false);
-        if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb);
         break;
     }
     case T_BOUNDARY_CUR: {
         KArgs<R> A = make_args<R>(c, true);
-        OFG_LAUNCH(k_interior_tvisl, nblk(N, 256), 256, s, c->dp, N, c->d_q[c->cur]);
-        if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A);
+        OFG_LAUNCH(k_interior_tvisl<R>, nblk(N, 256), 256, s, A);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb);
         break;
     }
     case T_NORM: {
@@ -162,7 +163,7 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     }
     case T_TURB_RHS: {
         KArgs<R> A = make_args<R>(c, true);
-        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, 0);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb, 0);
         OFG_LAUNCH(k_turb_grad<R>, nblk(N, 128), 128, s, A);
         OFG_LAUNCH(k_turb_rhs<R>, nblk(N, 128), 128, s, A);
         break;
@@ -192,13 +193,13 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     }
     case T_TURB_BOUNDARY: {
         KArgs<R> A = make_args<R>(c, true);
-        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, 1);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb, 1);
         break;
     }
     case T_TURB_BOUNDARY_CUR: {
         KArgs<R> A = make_args<R>(c, true);
         OFG_LAUNCH(k_turb_vist<R>, nblk(N, 256), 256, s, A);
-        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, 1);
+        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb, 1);
         break;
     }
     case T_TURB_NORM: {

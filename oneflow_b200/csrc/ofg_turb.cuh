@@ -1,8 +1,8 @@
-// Spalart-Allmaras solver kernels (TURB_SOLVER tasks).  Same gather
-// structure as the NS kernels: one thread per cell over its faces in
-// ascending face id, so every per-cell accumulation follows the reference's
-// face-loop order.  They read the NS state of the current buffer (already
-// relaxed in this outer iteration, as in the reference's StrongIter order).
+// Spalart-Allmaras solver kernels (TURB_SOLVER tasks).  Same gather structure
+// as the NS kernels: one thread per cell over its neighbour list in ascending
+// face id, so every per-cell accumulation follows the reference's face-loop
+// order.  They read the NS state of the current buffer (already relaxed in
+// this outer iteration, as in the reference's StrongIter order).
 #pragma once
 #include "ofg_kernels.cuh"
 
@@ -19,21 +19,29 @@ __device__ __forceinline__ double sa_vist(const DevParams &P, double rho, double
     return fmin(vl * P.max_vis_ratio, v);
 }
 
+// write the eddy viscosity of cell i into the master record and its FP32 copy
+template <typename R>
+__device__ __forceinline__ void put_vist(const KArgs<R> &A, int i, double v) {
+    const_cast<double *>(A.q)[(size_t)i * REC + IMT] = v;
+    if (sizeof(R) == 4) const_cast<R *>(A.qs)[(size_t)i * REC + IMT] = R(v);
+}
+
 // TurbBcSolver face rules (codes/turb/src/TurbBcSolver.cpp:51-262); the
 // far-field normal is scaled by GCom::faceOuterNormal, which the reference
 // never assigns (zero-initialised global), so only the sound speeds decide.
 template <typename R>
-__global__ void __launch_bounds__(256) k_turb_bc(KArgs<R> A, int withVist) {
+__global__ void __launch_bounds__(256) k_turb_bc(KArgs<R> A, const int *lcb, int withVist) {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= A.M.nBFaces) return;
-    int bt = A.M.bcType[f], l = A.M.lc[f];
-    int g = A.M.nCells + f;
+    if (f >= A.nBFaces) return;
+    int bt = A.bcType[f], l = lcb[f];
+    int g = A.nCells + f;
     double s = A.nut[l], t = s;
     if (bt == BC_SOLID) t = -s;
     else if (bt == BC_INFLOW) t = A.P.nut_inf;
     else if (bt == BC_FAR) {
         const double *ql = A.q + (size_t)l * REC;
-        double xn = double(A.G.xfn[f]) * 0, yn = double(A.G.yfn[f]) * 0, zn = double(A.G.zfn[f]) * 0;
+        const R *fg = A.fgeo + (size_t)f * FGR;
+        double xn = double(fg[0]) * 0, yn = double(fg[1]) * 0, zn = double(fg[2]) * 0;
         const double *inf = A.P.inflow;
         double vnref = xn * inf[IU] + yn * inf[IV] + zn * inf[IW] - 0.0;
         double vnin = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - 0.0;
@@ -51,27 +59,27 @@ __global__ void __launch_bounds__(256) k_turb_bc(KArgs<R> A, int withVist) {
         }
     }
     A.nut[g] = t;
-    if (withVist) {   // UTurbSrcFlux::SetGhostCellVist
-        double *qg = const_cast<double *>(A.q) + (size_t)g * REC;
-        qg[IMT] = A.q[(size_t)l * REC + IMT];
-    }
+    if (withVist) put_vist(A, g, A.q[(size_t)l * REC + IMT]);   // UTurbSrcFlux::SetGhostCellVist
 }
 
-// gradient of nu~ (uturb_grad: Green-Gauss cell-weighted, or the option of the
-// NS gradients); ghosts carry the interior gradient
+// gradient of nu~ (uturb_grad: Green-Gauss cell-weighted for igrad 0, or the
+// option chosen for the NS gradients); ghosts carry the interior gradient
 template <typename R>
 __global__ void __launch_bounds__(128) k_turb_grad(KArgs<R> A) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
+    if (c >= A.nCells) return;
+    R cgc[CGR];
+    ld4(A.cgeo + (size_t)c * CGR, cgc);
     R gx = 0, gy = 0, gz = 0;
-    int b = A.M.c2f_off[c], e = A.M.c2f_off[c + 1];
+    int b = A.nb_off[c], e = A.nb_off[c + 1];
+    R vc = R(A.nut[c]);
     if (A.P.igrad == 2) {
         R a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, b1 = 0, b2 = 0, b3 = 0;
-        R vc = R(A.nut[c]);
         for (int k = b; k < e; ++k) {
-            int f = A.M.c2f[k];
-            int nb = other_cell(A.M.lc[f], A.M.rc[f], c);
-            R dx = A.G.xcc[nb] - A.G.xcc[c], dy = A.G.ycc[nb] - A.G.ycc[c], dz = A.G.zcc[nb] - A.G.zcc[c];
+            int nb = __ldg(&A.nbl[k]).y;
+            R cgn[CGR];
+            ld4(A.cgeo + (size_t)nb * CGR, cgn);
+            R dx = cgn[0] - cgc[0], dy = cgn[1] - cgc[1], dz = cgn[2] - cgc[2];
             R w = R(1) / (dx * dx + dy * dy + dz * dz);
             R dv = R(A.nut[nb]) - vc;
             a11 += w * dx * dx; a12 += w * dx * dy; a13 += w * dx * dz;
@@ -91,28 +99,35 @@ __global__ void __launch_bounds__(128) k_turb_grad(KArgs<R> A) {
         }
     } else {
         for (int k = b; k < e; ++k) {
-            int f = A.M.c2f[k];
-            int l = A.M.lc[f], r = A.M.rc[f];
+            int2 e2 = __ldg(&A.nbl[k]);
+            int f = nb_face(e2), nb = e2.y;
+            bool right = nb_right(e2);
+            R cgn[CGR], fg[FGR];
+            ld4(A.cgeo + (size_t)nb * CGR, cgn);
+            ld8(A.fgeo + (size_t)f * FGR, fg);
+            R vn = R(A.nut[nb]);
+            R vl = right ? vn : vc, vr = right ? vc : vn;
+            const R *cl_ = right ? cgn : cgc, *cr_ = right ? cgc : cgn;
             R cl, cr;
             if (A.P.igrad == 1) { cl = R(0.5); cr = R(0.5); }
             else {
-                R dxl = A.G.xfc[f] - A.G.xcc[l], dyl = A.G.yfc[f] - A.G.ycc[l], dzl = A.G.zfc[f] - A.G.zcc[l];
-                R dxr = A.G.xfc[f] - A.G.xcc[r], dyr = A.G.yfc[f] - A.G.ycc[r], dzr = A.G.zfc[f] - A.G.zcc[r];
+                R dxl = fg[4] - cl_[0], dyl = fg[5] - cl_[1], dzl = fg[6] - cl_[2];
+                R dxr = fg[4] - cr_[0], dyr = fg[5] - cr_[1], dzr = fg[6] - cr_[2];
                 R delt1 = Rsqrt(SQR3(dxl, dyl, dzl)), delt2 = Rsqrt(SQR3(dxr, dyr, dzr));
                 R delta = R(1) / (delt1 + delt2 + small_v<R>());
                 cl = delt2 * delta; cr = delt1 * delta;
             }
-            R value = (A.P.igrad == 1) ? R(0.5) * (R(A.nut[l]) + R(A.nut[r])) : cl * R(A.nut[l]) + cr * R(A.nut[r]);
-            R ar = A.G.area[f];
-            R fx = A.G.xfn[f] * ar, fy = A.G.yfn[f] * ar, fz = A.G.zfn[f] * ar;
-            if (l == c) { gx += fx * value; gy += fy * value; gz += fz * value; }
+            R value = (A.P.igrad == 1) ? R(0.5) * (vl + vr) : cl * vl + cr * vr;
+            R ar = fg[3];
+            R fx = fg[0] * ar, fy = fg[1] * ar, fz = fg[2] * ar;
+            if (!right) { gx += fx * value; gy += fy * value; gz += fz * value; }
             else        { gx -= fx * value; gy -= fy * value; gz -= fz * value; }
         }
-        R ovol = R(1) / A.G.vol[c];
+        R ovol = R(1) / cgc[3];
         gx *= ovol; gy *= ovol; gz *= ovol;
     }
-    R *o = A.gnut + (size_t)c * 3;
-    o[0] = gx; o[1] = gy; o[2] = gz;
+    R o[4] = {gx, gy, gz, R(0)};
+    st4(A.gnut + (size_t)c * 4, o);
 }
 
 template <typename R>
@@ -130,177 +145,205 @@ __device__ __forceinline__ R calc_angle(R dx, R dy, R dz, R dist) {
 // source (TurbCom::CalcSrcSa, codes/turb/src/TurbCom.cpp:771-881), first-order
 // convection (TurbInvFlux::RoeFlux, codes/turb/src/TurbInvFlux.cpp:78-98) and
 // diffusion with the VIS_TEST face gradient (UTurbVisFlux, codes/uturb/src/UTurbVisFlux.cpp:64-407).
+// The FP64 path keeps the reference's three face passes (spectrum, convection,
+// diffusion) in order; the FP32 path fuses them into one pass with separate
+// FP64 accumulators that are added in the reference's order at the end.
 template <typename R>
 __global__ void __launch_bounds__(128) k_turb_rhs(KArgs<R> A) {
+    constexpr bool exactOrder = sizeof(R) == 8;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
+    if (c >= A.nCells) return;
     const DevParams &P = A.P;
     const double half = 0.5;
-    int b = A.M.c2f_off[c], en = A.M.c2f_off[c + 1];
-    const double *qc = A.q + (size_t)c * REC;
-    double vol = double(A.G.vol[c]);
-    // ---- spectral radius and sweep coefficients ----
+    int b = A.nb_off[c], en = A.nb_off[c + 1];
+    R qc[REC], cgc[CGR], gnc[4];
+    ld8(A.qs + (size_t)c * REC, qc);
+    ld4(A.cgeo + (size_t)c * CGR, cgc);
+    ld4(A.gnut + (size_t)c * 4, gnc);
+    double nutc = A.nut[c];
+    double vol = double(cgc[3]);
     double imp = 0.0;
     imp += (1.0 / (A.dt[c] * P.turb_cfl_ratio)) * vol;
-    for (int k = b; k < en; ++k) {
-        int f = A.M.c2f[k];
-        int l = A.M.lc[f], r = A.M.rc[f];
-        const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-        double xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f], ar = A.G.area[f];
-        double vnl = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - 0.0;
-        double vnr = xn * qr[IU] + yn * qr[IV] + zn * qr[IW] - 0.0;
-        double absVn = fabs(half * (vnl + vnr));
-        double r1 = 0.0, m1 = 0.0, m2 = 0.0;
-        r1 += ar * half * absVn;
-        m1 += ar * half * (-vnl - absVn);
-        m2 += ar * half * (vnr - absVn);
-        double orl = 1.0 / (ql[IR] + SMALLD), orr = 1.0 / (qr[IR] + SMALLD);
-        double nuet1 = ql[IML] * orl + A.nut[l], nuet2 = qr[IML] * orr + A.nut[r];
-        double nueff = fabs(half * (nuet1 + nuet2));
-        double ovol = 1.0 / (half * (double(A.G.vol[l]) + double(A.G.vol[r])));
-        double d = P.oreynolds * ovol * (P.sa_osigma * nueff * (ar * ar));
-        r1 += d;
-        m1 += -d;
-        m2 += -d;
-        imp += r1;
-        if (l == c) { A.matL[f] = m1; A.matR[f] = m2; }
-    }
-    // ---- source ----
-    const R *gq = A.grad + (size_t)c * 18;
-    double dudx = gq[IU * 3], dudy = gq[IU * 3 + 1], dudz = gq[IU * 3 + 2];
-    double dvdx = gq[IV * 3], dvdy = gq[IV * 3 + 1], dvdz = gq[IV * 3 + 2];
-    double dwdx = gq[IW * 3], dwdy = gq[IW * 3 + 1], dwdz = gq[IW * 3 + 2];
-    double rho = qc[IR], nuet = A.nut[c], vl = qc[IML];
-    double olam = rho / (vl + SMALLD);
-    double ls = A.M.walldist[c];
-    double od2 = 1.0 / (ls * ls);
-    double work1 = dudx + dvdy + dwdz;
-    double work2 = SQR3(dudx, dudy, dudz);
-    double work3 = SQR3(dudy + dvdx, dvdz + dwdy, dwdx + dudz);
-    double work4 = sqrt(SQR3(dwdy - dvdz, dudz - dwdx, dvdx - dudy));
-    if (P.iprod_sa == 1) {
-        double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
-        work4 = sqrt(fabs(stp));
-    } else if (P.iprod_sa == 4) {
-        double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
-        double str = work4;
-        work4 = str - 2.0 * fmax(0.0, str - sqrt(fabs(stp)));
-    } else if (P.iprod_sa == 5) {
-        double stp = fabs(2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1);
-        double str = work4;
-        work4 = str * (1.0 - fmax(0.0, (str * str - stp) / (str * str + stp + SMALLD)));
-    }
-    double str = work4;
-    double xsi = nuet * olam + SMALLD;
-    double xsi3 = xsi * xsi * xsi;
-    double fv1 = xsi3 / (xsi3 + P.sa_cv13);
-    double fv2 = 1.0 - xsi / (1.0 + xsi * fv1);
-    double rs = nuet * P.sa_okarm2 * od2 * P.oreynolds;
-    double nuetRs = nuet * rs;
-    double sBar = rs * fv2;
-    double omega = str;
-    double stdv;
-    if (sBar >= -P.sa_sac2 * omega) stdv = omega + sBar;
-    else {
-        double term1 = (P.sa_sac2 * P.sa_sac2 * omega + P.sa_sac3 * sBar);
-        double term2 = (P.sa_sac3 - 2 * P.sa_sac2) * omega - sBar;
-        stdv = omega + omega * term1 / term2;
-    }
-    double ostd = 1.0 / (stdv + SMALLD);
-    double rr = fmin(rs * ostd, 10.0);
-    double r5 = pow(rr, 5.0);
-    double g = rr + P.sa_cw2 * (r5 * rr - rr);
-    double g6 = pow(g, 6.0);
-    double fw = g * pow((1.0 + P.sa_cw36) / (g6 + P.sa_cw36), 1.0 / 6.0);
-    double xsi2 = xsi * xsi;
-    double ft2 = P.ft2_flag ? P.sa_ct3 * exp(-P.sa_ct4 * xsi2) * 1.0 : 0.0;
-    const R *gn = A.gnut + (size_t)c * 3;
-    double grd2 = SQR3(double(gn[0]), double(gn[1]), double(gn[2]));
-    double prod = P.sa_cb1 * (1.0 - ft2) * stdv * nuet;
-    double diff = P.sa_cb2s * grd2 * P.oreynolds;
-    double dest = (P.sa_cw1k * fw - P.sa_cb1 * ft2) * nuetRs;
-    diff = fmin(P.rprod * prod, diff);
-    double srcTerm = prod - dest;
-    srcTerm += diff;
-    double q1x = fv1 / (xsi + SMALLD), q1y = 1.0 + xsi * fv1;
-    double dfv2dk = (3.0 * P.sa_cv13 * (q1x * q1x) - 1.0) / (q1y * q1y);
-    double dsdnu = P.oreynolds * P.sa_okarm2 * od2 * (fv2 + xsi * dfv2dk);
-    double dfwdg = fw / (g + SMALLD) * (1.0 - g6 / (g6 + P.sa_cw36));
-    double dgdr = 1.0 + P.sa_cw2 * (6.0 * r5 - 1.0);
-    double drdnu = P.oreynolds * P.sa_okarm2 * od2 * ostd * (1.0 - nuet * ostd * dsdnu);
-    double dfwdnu = dfwdg * dgdr * drdnu;
-    double prod0 = P.sa_cb1 * (1.0 - ft2) * stdv;
-    double dest0 = (P.sa_cw1 * fw - P.sa_cb1 * ft2 * P.sa_okarm2) * nuet * od2 * P.oreynolds;
-    double prodp = P.sa_cb1 * ((1.0 - ft2) * dsdnu);
-    double destp = (P.sa_cw1 * (fw + dfwdnu * nuet) - P.sa_cb1 * ft2 * P.sa_okarm2) * od2 * P.oreynolds;
-    double prde0 = prod0 - dest0, prdep = prodp - destp;
-    double part1 = -half * (prde0 - fabs(prde0));
-    double part2 = -half * (prdep - fabs(prdep)) * nuet;
-    imp += (part1 + part2) * vol;
+    double conv = 0.0, diffu = 0.0;   // FP32 path: per-pass accumulators
     double acc = -0.0;
-    acc += srcTerm * vol;
-    // ---- first-order convection with the NS face states ----
-    for (int k = b; k < en; ++k) {
-        int f = A.M.c2f[k];
-        int l = A.M.lc[f], r = A.M.rc[f];
-        const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-        double t1 = A.nut[l], t2 = A.nut[r];
-        double u1 = ql[IU], v1 = ql[IV], w1 = ql[IW], u2 = qr[IU], v2 = qr[IV], w2 = qr[IW];
-        if (f < A.M.nBFaces) {
-            double tm = half * (A.nut[l] + A.nut[r]);
-            t1 = t2 = tm;
-            if (A.M.bcType[f] == BC_SOLID) {
-                const double *bq = A.bcq + (size_t)f * NEQ;
-                u1 = u2 = bq[IU]; v1 = v2 = bq[IV]; w1 = w2 = bq[IW];
-            } else {
-                u1 = u2 = half * (ql[IU] + qr[IU]);
-                v1 = v2 = half * (ql[IV] + qr[IV]);
-                w1 = w2 = half * (ql[IW] + qr[IW]);
+    // FP64: pass 0 spectrum, then the source, pass 1 convection, pass 2
+    // diffusion (the TurbCalcRHS order)
+    for (int pass = 0; pass < (exactOrder ? 3 : 1); ++pass) {
+        for (int k = b; k < en; ++k) {
+            int2 e2 = __ldg(&A.nbl[k]);
+            int f = nb_face(e2), nb = e2.y;
+            bool right = nb_right(e2);
+            R qn[REC], cgn[CGR], fg[FGR];
+            ld8(A.qs + (size_t)nb * REC, qn);
+            ld8(A.fgeo + (size_t)f * FGR, fg);
+            ld4(A.cgeo + (size_t)nb * CGR, cgn);
+            double nutn = A.nut[nb];
+            const R *ql = right ? qn : qc, *qr = right ? qc : qn;
+            const R *cgl = right ? cgn : cgc, *cgr = right ? cgc : cgn;
+            double nl = right ? nutn : nutc, nr = right ? nutc : nutn;
+            double xn = fg[0], yn = fg[1], zn = fg[2], ar = fg[3];
+            if (!exactOrder || pass == 0) {
+                // ---- spectral radius and sweep coefficients ----
+                double vnl = xn * double(ql[IU]) + yn * double(ql[IV]) + zn * double(ql[IW]) - 0.0;
+                double vnr = xn * double(qr[IU]) + yn * double(qr[IV]) + zn * double(qr[IW]) - 0.0;
+                double absVn = fabs(half * (vnl + vnr));
+                double r1 = 0.0, m1 = 0.0, m2 = 0.0;
+                r1 += ar * half * absVn;
+                m1 += ar * half * (-vnl - absVn);
+                m2 += ar * half * (vnr - absVn);
+                double orl = 1.0 / (double(ql[IR]) + SMALLD), orr = 1.0 / (double(qr[IR]) + SMALLD);
+                double nuet1 = double(ql[IML]) * orl + nl, nuet2 = double(qr[IML]) * orr + nr;
+                double nueff = fabs(half * (nuet1 + nuet2));
+                double ovol = 1.0 / (half * (double(cgl[3]) + double(cgr[3])));
+                double d = P.oreynolds * ovol * (P.sa_osigma * nueff * (ar * ar));
+                r1 += d;
+                m1 += -d;
+                m2 += -d;
+                imp += r1;
+                if (!right) { A.matL[f] = m1; A.matR[f] = m2; }
+            }
+            if (!exactOrder || pass == 1) {
+                // ---- first-order convection with the NS face states ----
+                double t1 = nl, t2 = nr;
+                double u1 = ql[IU], v1 = ql[IV], w1 = ql[IW], u2 = qr[IU], v2 = qr[IV], w2 = qr[IW];
+                if (f < A.nBFaces) {
+                    double tm = half * (nl + nr);
+                    t1 = t2 = tm;
+                    if (A.bcType[f] == BC_SOLID) {
+                        const double *bq = A.bcq + (size_t)f * NEQ;
+                        u1 = u2 = bq[IU]; v1 = v2 = bq[IV]; w1 = w2 = bq[IW];
+                    } else {
+                        u1 = u2 = half * (double(ql[IU]) + double(qr[IU]));
+                        v1 = v2 = half * (double(ql[IV]) + double(qr[IV]));
+                        w1 = w2 = half * (double(ql[IW]) + double(qr[IW]));
+                    }
+                }
+                double vnl = xn * u1 + yn * v1 + zn * w1 - 0.0;
+                double vnr = xn * u2 + yn * v2 + zn * w2 - 0.0;
+                double coef_l = half * (vnl + fabs(vnl)) * 1.0;
+                double coef_r = half * (vnr - fabs(vnr)) * 1.0;
+                double v = ar * (coef_l * t1 + coef_r * t2);
+                if (exactOrder) { if (!right) acc -= v; else acc += v; }
+                else { if (!right) conv -= v; else conv += v; }
+            }
+            if (!exactOrder || pass == 2) {
+                // ---- diffusion (VIS_TEST face gradient) ----
+                R fxn = fg[0], fyn = fg[1], fzn = fg[2];
+                R q1 = R(nl), q2 = R(nr);
+                R q11 = q1, q22 = q2, qf = R(0.5) * (q1 + q2);
+                R dxl = cgl[0] - fg[4], dyl = cgl[1] - fg[5], dzl = cgl[2] - fg[6];
+                R dxr = cgr[0] - fg[4], dyr = cgr[1] - fg[5], dzr = cgr[2] - fg[6];
+                R d1 = fxn * dxl + fyn * dyl + fzn * dzl;
+                R d2 = fxn * dxr + fyn * dyr + fzn * dzr;
+                R angle1 = calc_angle(dxl, dyl, dzl, -d1);
+                R angle2 = calc_angle(dxr, dyr, dzr, d2);
+                R dqdn = R(0);
+                if (angle1 > R(20) && angle2 > R(20)) {
+                    R gn[4];
+                    bool ghost = nb >= A.nCells;
+                    if (!ghost) ld4(A.gnut + (size_t)nb * 4, gn);
+                    const R *g1 = right ? gn : gnc;
+                    const R *g2 = (right || ghost) ? gnc : gn;
+                    q11 += g1[0] * (fxn * d1 - dxl) + g1[1] * (fyn * d1 - dyl) + g1[2] * (fzn * d1 - dzl);
+                    q22 += g2[0] * (fxn * d2 - dxr) + g2[1] * (fyn * d2 - dyr) + g2[2] * (fzn * d2 - dzr);
+                    qf = R(0.5) * (q1 + q2);
+                }
+                if (angle1 > R(0) && angle2 > R(0) && Rabs(d1) > small_v<R>() && Rabs(d2) > small_v<R>()) {
+                    R dtmp = d1 * d1 + d2 * d2;
+                    R c1 = d1 * d1 / dtmp, c2 = R(1) - c1;
+                    if (f < A.nBFaces) { c1 = R(1); c2 = R(0); }
+                    dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
+                }
+                double orl = 1.0 / (double(ql[IR]) + SMALLD), orr = 1.0 / (double(qr[IR]) + SMALLD);
+                double visl_nv = half * (double(ql[IML]) * orl + double(qr[IML]) * orr);
+                double vist_nv = half * (nl + nr);
+                double comVis = (visl_nv + vist_nv) * P.sa_osigma;
+                double flux = -P.oreynolds * comVis * double(dqdn) * ar;
+                if (exactOrder) { if (!right) acc -= flux; else acc += flux; }
+                else { if (!right) diffu -= flux; else diffu += flux; }
             }
         }
-        double xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f];
-        double vnl = xn * u1 + yn * v1 + zn * w1 - 0.0;
-        double vnr = xn * u2 + yn * v2 + zn * w2 - 0.0;
-        double coef_l = half * (vnl + fabs(vnl)) * 1.0;
-        double coef_r = half * (vnr - fabs(vnr)) * 1.0;
-        double v = double(A.G.area[f]) * (coef_l * t1 + coef_r * t2);
-        if (l == c) acc -= v; else acc += v;
-    }
-    // ---- diffusion ----
-    for (int k = b; k < en; ++k) {
-        int f = A.M.c2f[k];
-        int l = A.M.lc[f], r = A.M.rc[f];
-        R xn = A.G.xfn[f], yn = A.G.yfn[f], zn = A.G.zfn[f];
-        R q1 = R(A.nut[l]), q2 = R(A.nut[r]);
-        R q11 = q1, q22 = q2, qf = R(0.5) * (q1 + q2);
-        R dxl = A.G.xcc[l] - A.G.xfc[f], dyl = A.G.ycc[l] - A.G.yfc[f], dzl = A.G.zcc[l] - A.G.zfc[f];
-        R dxr = A.G.xcc[r] - A.G.xfc[f], dyr = A.G.ycc[r] - A.G.yfc[f], dzr = A.G.zcc[r] - A.G.zfc[f];
-        R d1 = xn * dxl + yn * dyl + zn * dzl;
-        R d2 = xn * dxr + yn * dyr + zn * dzr;
-        R angle1 = calc_angle(dxl, dyl, dzl, -d1);
-        R angle2 = calc_angle(dxr, dyr, dzr, d2);
-        R dqdn = R(0);
-        if (angle1 > R(20) && angle2 > R(20)) {
-            const R *g1 = A.gnut + (size_t)l * 3;
-            const R *g2 = A.gnut + (size_t)grad_cell(A.M, r) * 3;
-            q11 += g1[0] * (xn * d1 - dxl) + g1[1] * (yn * d1 - dyl) + g1[2] * (zn * d1 - dzl);
-            q22 += g2[0] * (xn * d2 - dxr) + g2[1] * (yn * d2 - dyr) + g2[2] * (zn * d2 - dzr);
-            qf = R(0.5) * (q1 + q2);
+        if (pass == 0 || !exactOrder) {
+            // ---- source term (per cell, after the spectrum) ----
+            double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
+            {
+                R gq[GLR];
+#pragma unroll
+                for (int i = 0; i < 12; i += 4) ld4(A.gl + (size_t)c * GLR + i, gq + i);
+                dudx = gq[IU * 3]; dudy = gq[IU * 3 + 1]; dudz = gq[IU * 3 + 2];
+                dvdx = gq[IV * 3]; dvdy = gq[IV * 3 + 1]; dvdz = gq[IV * 3 + 2];
+                dwdx = gq[IW * 3]; dwdy = gq[IW * 3 + 1]; dwdz = gq[IW * 3 + 2];
+            }
+            double rho = A.q[(size_t)c * REC + IR], nuet = nutc, vlc = A.q[(size_t)c * REC + IML];
+            double olam = rho / (vlc + SMALLD);
+            double ls = A.walldist[c];
+            double od2 = 1.0 / (ls * ls);
+            double work1 = dudx + dvdy + dwdz;
+            double work2 = SQR3(dudx, dudy, dudz);
+            double work3 = SQR3(dudy + dvdx, dvdz + dwdy, dwdx + dudz);
+            double work4 = sqrt(SQR3(dwdy - dvdz, dudz - dwdx, dvdx - dudy));
+            if (P.iprod_sa == 1) {
+                double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
+                work4 = sqrt(fabs(stp));
+            } else if (P.iprod_sa == 4) {
+                double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
+                double str = work4;
+                work4 = str - 2.0 * fmax(0.0, str - sqrt(fabs(stp)));
+            } else if (P.iprod_sa == 5) {
+                double stp = fabs(2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1);
+                double str = work4;
+                work4 = str * (1.0 - fmax(0.0, (str * str - stp) / (str * str + stp + SMALLD)));
+            }
+            double str = work4;
+            double xsi = nuet * olam + SMALLD;
+            double xsi3 = xsi * xsi * xsi;
+            double fv1 = xsi3 / (xsi3 + P.sa_cv13);
+            double fv2 = 1.0 - xsi / (1.0 + xsi * fv1);
+            double rs = nuet * P.sa_okarm2 * od2 * P.oreynolds;
+            double nuetRs = nuet * rs;
+            double sBar = rs * fv2;
+            double omega = str;
+            double stdv;
+            if (sBar >= -P.sa_sac2 * omega) stdv = omega + sBar;
+            else {
+                double term1 = (P.sa_sac2 * P.sa_sac2 * omega + P.sa_sac3 * sBar);
+                double term2 = (P.sa_sac3 - 2 * P.sa_sac2) * omega - sBar;
+                stdv = omega + omega * term1 / term2;
+            }
+            double ostd = 1.0 / (stdv + SMALLD);
+            double rr = fmin(rs * ostd, 10.0);
+            double r5 = pow(rr, 5.0);
+            double g = rr + P.sa_cw2 * (r5 * rr - rr);
+            double g6 = pow(g, 6.0);
+            double fw = g * pow((1.0 + P.sa_cw36) / (g6 + P.sa_cw36), 1.0 / 6.0);
+            double xsi2 = xsi * xsi;
+            double ft2 = P.ft2_flag ? P.sa_ct3 * exp(-P.sa_ct4 * xsi2) * 1.0 : 0.0;
+            double grd2 = SQR3(double(gnc[0]), double(gnc[1]), double(gnc[2]));
+            double prod = P.sa_cb1 * (1.0 - ft2) * stdv * nuet;
+            double diff = P.sa_cb2s * grd2 * P.oreynolds;
+            double dest = (P.sa_cw1k * fw - P.sa_cb1 * ft2) * nuetRs;
+            diff = fmin(P.rprod * prod, diff);
+            double srcTerm = prod - dest;
+            srcTerm += diff;
+            double q1x = fv1 / (xsi + SMALLD), q1y = 1.0 + xsi * fv1;
+            double dfv2dk = (3.0 * P.sa_cv13 * (q1x * q1x) - 1.0) / (q1y * q1y);
+            double dsdnu = P.oreynolds * P.sa_okarm2 * od2 * (fv2 + xsi * dfv2dk);
+            double dfwdg = fw / (g + SMALLD) * (1.0 - g6 / (g6 + P.sa_cw36));
+            double dgdr = 1.0 + P.sa_cw2 * (6.0 * r5 - 1.0);
+            double drdnu = P.oreynolds * P.sa_okarm2 * od2 * ostd * (1.0 - nuet * ostd * dsdnu);
+            double dfwdnu = dfwdg * dgdr * drdnu;
+            double prod0 = P.sa_cb1 * (1.0 - ft2) * stdv;
+            double dest0 = (P.sa_cw1 * fw - P.sa_cb1 * ft2 * P.sa_okarm2) * nuet * od2 * P.oreynolds;
+            double prodp = P.sa_cb1 * ((1.0 - ft2) * dsdnu);
+            double destp = (P.sa_cw1 * (fw + dfwdnu * nuet) - P.sa_cb1 * ft2 * P.sa_okarm2) * od2 * P.oreynolds;
+            double prde0 = prod0 - dest0, prdep = prodp - destp;
+            double part1 = -half * (prde0 - fabs(prde0));
+            double part2 = -half * (prdep - fabs(prdep)) * nuet;
+            imp += (part1 + part2) * vol;
+            acc += srcTerm * vol;
         }
-        if (angle1 > R(0) && angle2 > R(0) && Rabs(d1) > small_v<R>() && Rabs(d2) > small_v<R>()) {
-            R dtmp = d1 * d1 + d2 * d2;
-            R c1 = d1 * d1 / dtmp, c2 = R(1) - c1;
-            if (f < A.M.nBFaces) { c1 = R(1); c2 = R(0); }
-            dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
-        }
-        const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
-        double orl = 1.0 / (ql[IR] + SMALLD), orr = 1.0 / (qr[IR] + SMALLD);
-        double visl_nv = half * (ql[IML] * orl + qr[IML] * orr);
-        double vist_nv = half * (A.nut[l] + A.nut[r]);
-        double comVis = (visl_nv + vist_nv) * P.sa_osigma;
-        double flux = -P.oreynolds * comVis * double(dqdn) * double(A.G.area[f]);
-        if (l == c) acc -= flux; else acc += flux;
     }
+    if (!exactOrder) { acc += conv; acc += diffu; }
     A.impsrT[c] = imp;
     A.resT[c] = acc;
 }
@@ -313,13 +356,10 @@ __global__ void __launch_bounds__(128) k_turb_lower(KArgs<R> A, const int *order
     if (t >= count) return;
     int c = order[start + t];
     double rhs0 = 0.0;
-    int kc = A.M.key[c];
-    for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
-        int f = A.M.c2f[k];
-        int l = A.M.lc[f], r = A.M.rc[f];
-        if (A.M.key[l] > kc || A.M.key[r] > kc) continue;
-        bool swap = (r == c);
-        rhs0 += (swap ? A.matL[f] : A.matR[f]) * A.dnut[swap ? l : r];
+    for (int k = A.lo_off[c]; k < A.lo_off[c + 1]; ++k) {
+        int2 e2 = __ldg(&A.lol[k]);
+        int f = nb_face(e2);
+        rhs0 += (nb_right(e2) ? A.matL[f] : A.matR[f]) * A.dnut[e2.y];
     }
     A.dnut[c] = (A.resT[c] - rhs0) / A.impsrT[c];
 }
@@ -330,14 +370,10 @@ __global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order
     if (t >= count) return;
     int c = order[start + t];
     double rhs0 = 0.0;
-    int kc = A.M.key[c];
-    for (int k = A.M.c2f_off[c]; k < A.M.c2f_off[c + 1]; ++k) {
-        int f = A.M.c2f[k];
-        if (f < A.M.nBFaces) continue;   // ghost increments are zero
-        int l = A.M.lc[f], r = A.M.rc[f];
-        if (A.M.key[l] < kc || A.M.key[r] < kc) continue;
-        bool swap = (r == c);
-        rhs0 += (swap ? A.matL[f] : A.matR[f]) * A.dnut[swap ? l : r];
+    for (int k = A.up_off[c]; k < A.up_off[c + 1]; ++k) {   // ghost increments are zero: not listed
+        int2 e2 = __ldg(&A.upl[k]);
+        int f = nb_face(e2);
+        rhs0 += (nb_right(e2) ? A.matL[f] : A.matR[f]) * A.dnut[e2.y];
     }
     A.dnut[c] += (-rhs0) / A.impsrT[c];
 }
@@ -347,13 +383,13 @@ __global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order
 template <typename R>
 __global__ void __launch_bounds__(256) k_turb_update(KArgs<R> A, int withVist) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
+    if (c >= A.nCells) return;
     double qOld = A.nut[c], qNew = qOld + A.dnut[c];
     double v = (1.0 - 1.0) * qOld + 1.0 * qNew;
     A.nut[c] = v;
     if (withVist) {
-        double *qc = const_cast<double *>(A.q) + (size_t)c * REC;
-        qc[IMT] = sa_vist(A.P, qc[IR], v, qc[IML]);
+        const double *qc = A.q + (size_t)c * REC;
+        put_vist(A, c, sa_vist(A.P, qc[IR], v, qc[IML]));
     }
 }
 
@@ -361,16 +397,16 @@ __global__ void __launch_bounds__(256) k_turb_update(KArgs<R> A, int withVist) {
 template <typename R>
 __global__ void __launch_bounds__(256) k_turb_vist(KArgs<R> A) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.M.nCells) return;
-    double *qc = const_cast<double *>(A.q) + (size_t)c * REC;
-    qc[IMT] = sa_vist(A.P, qc[IR], A.nut[c], qc[IML]);
+    if (c >= A.nCells) return;
+    const double *qc = A.q + (size_t)c * REC;
+    put_vist(A, c, sa_vist(A.P, qc[IR], A.nut[c], qc[IML]));
 }
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_turb_norm_partial(KArgs<R> A) {
     __shared__ double s[256];
     double acc = 0.0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.M.nCells; c += gridDim.x * blockDim.x)
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.nCells; c += gridDim.x * blockDim.x)
         acc += A.resT[c] * A.resT[c];
     s[threadIdx.x] = acc;
     __syncthreads();
@@ -393,7 +429,7 @@ __global__ void __launch_bounds__(256) k_turb_norm_final(KArgs<R> A, int nPartia
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        double rms = sqrt(s[0] / A.M.nCells);
+        double rms = sqrt(s[0] / A.nCells);
         A.scal[S_TNORM] = rms;
         int n = int(A.scal[S_THISTN]);
         if (n < cap) hist[n] = rms;

@@ -143,15 +143,16 @@ class Solver:
         """Launch on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self.L.ofg_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
-    PROFILE_GROUPS = ("cfl", "time_step", "residual", "lusgs_lower", "lusgs_upper", "update", "boundary", "norm",
+    PROFILE_GROUPS = ("cfl", "residual", "lusgs_lower", "lusgs_upper", "update", "boundary", "norm",
                       "sa_residual", "sa_lower", "sa_upper", "sa_update", "sa_boundary", "sa_norm")
 
     def profile_step(self):
-        """One iteration task by task with CUDA events: ({group: ms}, {group: launches})."""
+        """One iteration task by task with CUDA events: ({group: ms}, {group: launches}).
+        "residual" is the fused time step + gradients + limiter + flux gather."""
         ms = np.zeros(16, np.float64)
         nl = np.zeros(16, np.int32)
         self._check(self.L.ofg_profile_step(self.h, ms, nl))
-        n = 14 if self.params.vismodel >= 3 else 8
+        n = 13 if self.params.vismodel >= 3 else 7
         names = self.PROFILE_GROUPS[:n]
         return dict(zip(names, ms[:n].tolist())), dict(zip(names, nl[:n].tolist()))
 

@@ -58,3 +58,15 @@ def test_3d_mixed_tracks_fp64():
     b = Solver(m, P.defaults(**d, precision=1)); b.init_flowfield(); b.step(20)
     assert rel(b.state(), a.state()) < 1e-4
     assert rel(b.state(TURB_SOLVER), a.state(TURB_SOLVER)) < 1e-2
+
+
+@pytest.mark.parametrize("name", ["gg_nolim_roe", "lsq_venkat_kh3_roe"])
+def test_colour_sweep_order_on_gpu_matches_oracle(name):
+    m = mesh3d("natural")
+    prm = P.defaults(**CASES[name], sweep_order=1)
+    o = Oracle(m, prm); o.init(); o.step(12)
+    g = Solver(m, prm); g.init_flowfield(); g.step(12)
+    assert g.sweep_levels() == (g.sweep_levels()[0], g.sweep_levels()[0]) and g.sweep_levels()[0] <= 8
+    assert rel(g.state(), o.q()) < 1e-10
+    a, b = g.state(TURB_SOLVER), o.field("turbq")
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5
