@@ -221,7 +221,7 @@ void build_sweep_key(ofg_ctx *c) {
 
 // Level schedule of a sequential sweep: a cell's level is one more than the
 // deepest level among the neighbours it reads (lower: smaller key; upper:
-// larger key).  Inside a level, cells keep the sweep order.
+// larger key).
 void build_levels(ofg_ctx *c, bool lower, std::vector<int> &order, std::vector<int> &off) {
     int N = c->nCells;
     const std::vector<int> &key = c->key;
@@ -245,8 +245,9 @@ void build_levels(ofg_ctx *c, bool lower, std::vector<int> &order, std::vector<i
     for (int l = 0; l <= maxl; ++l) off[l + 1] += off[l];
     order.assign(N, 0);
     std::vector<int> pos(off.begin(), off.end() - 1);
-    if (lower) for (int k = 0; k < N; ++k) { int i = c->keyOrder[k]; order[pos[lev[i]]++] = i; }
-    else for (int k = N - 1; k >= 0; --k) { int i = c->keyOrder[k]; order[pos[lev[i]]++] = i; }
+    // inside a level the cells are independent; both sweeps list them in
+    // ascending sweep order
+    for (int k = 0; k < N; ++k) { int i = c->keyOrder[k]; order[pos[lev[i]]++] = i; }
 }
 
 // Per-cell neighbour lists in ascending face id (the c2f order), one int2 per
@@ -420,7 +421,7 @@ void ofg_destroy(ofg_ctx *c) {
     destroy_graphs(c);
     void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
                     c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist,
-                    c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr,
+                    c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_rad,
                     c->d_bcq, c->d_partial, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
     for (void *v : ptrs) if (v) cudaFree(v);
@@ -526,11 +527,13 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         if (c->d_qs[i]) { cudaFree(c->d_qs[i]); c->d_qs[i] = nullptr; }
         if (mixed) CK(cudaMalloc(&c->d_qs[i], nT * REC * sizeof(float)));
     }
+    size_t rs = mixed ? sizeof(float) : sizeof(double);
     if ((rc = upload<double>(c, &c->d_res, nullptr, N * NEQ))) return rc;
-    if ((rc = upload<double>(c, &c->d_dq, nullptr, nT * NEQ))) return rc;
+    if ((rc = upload_bytes(c, &c->d_dq, nullptr, N * DQR * rs))) return rc;
     if ((rc = upload<double>(c, &c->d_dt, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_invsr, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_vissr, nullptr, N))) return rc;
+    if ((rc = upload<double>(c, &c->d_rad, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_bcq, nullptr, (size_t)std::max(nBFaces, 1) * NEQ))) return rc;
     c->nPartialMax = std::max<size_t>((N + 127) / 128 * 10, 2 * 148 * NEQ) + 16;
     if ((rc = upload<double>(c, &c->d_partial, nullptr, c->nPartialMax))) return rc;
@@ -538,11 +541,9 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     c->histCap = 1 << 16;
     if ((rc = upload<double>(c, &c->d_hist, nullptr, (size_t)c->histCap * NEQ))) return rc;
     if ((rc = upload<int>(c, &c->d_fix, nullptr, 1 + c->fixcap))) return rc;
-    size_t rs = mixed ? sizeof(float) : sizeof(double);
     if ((rc = upload_bytes(c, &c->d_gl, nullptr, N * GLR * rs))) return rc;
     bool venkatGlobal = c->p.ilim == 2 && !c->p.venkat_kh3;
     if ((rc = upload_bytes(c, &c->d_mm, nullptr, venkatGlobal ? N * MMR * rs : 0))) return rc;
-    CK(cudaMemset(c->d_dq, 0, nT * NEQ * sizeof(double)));
     CK(cudaMemset(c->d_bcq, 0, (size_t)std::max(nBFaces, 1) * NEQ * sizeof(double)));
     CK(cudaMemset(c->d_scal, 0, 32 * sizeof(double)));
     CK(cudaMemset(c->d_fix, 0, (1 + c->fixcap) * sizeof(int)));
@@ -651,7 +652,9 @@ int ofg_zero_dq(ofg_ctx *c, int tid) {
     if (tid == OFG_TURB_SOLVER)
         CK(cudaMemsetAsync(c->d_dnut, 0, (size_t)c->nT * sizeof(double), c->stream));
     else
-        CK(cudaMemsetAsync(c->d_dq, 0, (size_t)c->nT * NEQ * sizeof(double), c->stream));
+        CK(cudaMemsetAsync(c->d_dq, 0,
+                           (size_t)c->nCells * DQR * (c->p.precision == OFG_PREC_MIXED ? sizeof(float) : sizeof(double)),
+                           c->stream));
     return OFG_OK;
 }
 
@@ -812,7 +815,7 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
     if (!name) return c->fail(OFG_E_ARG, "null name");
     if ((rc = sync(c))) return rc;
     std::string s(name);
-    int64_t nT = c->nT, N = c->nCells, nF = c->nFaces;
+    int64_t nT = c->nT, N = c->nCells;
     std::vector<double> buf;
     auto rec_field = [&](int comp) {
         std::vector<double> rec((size_t)nT * REC);
@@ -842,7 +845,18 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
     };
     auto host_vec = [&](const std::vector<double> &v) { buf = v; };
     if (s == "res") aos_field(c->d_res, NEQ, N, nT);
-    else if (s == "dq") aos_field(c->d_dq, NEQ, nT, nT);
+    else if (s == "dq") {   // [nCells][DQR] records at the face precision; ghosts 0
+        buf.assign((size_t)NEQ * nT, 0.0);
+        if (c->p.precision == OFG_PREC_MIXED) {
+            std::vector<float> tmp((size_t)N * DQR);
+            cudaMemcpy(tmp.data(), c->d_dq, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost);
+            for (int e = 0; e < NEQ; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * DQR + e];
+        } else {
+            std::vector<double> tmp((size_t)N * DQR);
+            cudaMemcpy(tmp.data(), c->d_dq, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost);
+            for (int e = 0; e < NEQ; ++e) for (int64_t i = 0; i < N; ++i) buf[(size_t)e * nT + i] = tmp[(size_t)i * DQR + e];
+        }
+    }
     else if (s == "timestep") aos_field(c->d_dt, 1, N, nT);
     else if (s == "invsr") aos_field(c->d_invsr, 1, N, nT);
     else if (s == "vissr") aos_field(c->d_vissr, 1, N, nT);
@@ -883,7 +897,6 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
         if (n_out < (int64_t)buf.size()) return c->fail(OFG_E_ARG, "output buffer too small");
         std::copy(buf.begin(), buf.end(), out);
     }
-    (void)nF;
     return OFG_OK;
 }
 

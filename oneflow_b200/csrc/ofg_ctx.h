@@ -36,7 +36,8 @@ struct ofg_ctx {
     int cur = 0;
     bool pendingNext = false;   // UPDATE_FLOWFIELD wrote d_q[cur^1], CALC_BOUNDARY not yet run
     bool pendingTurb = false;   // SA UPDATE_FLOWFIELD ran, its CALC_BOUNDARY not yet
-    double *d_res = nullptr, *d_dq = nullptr, *d_dt = nullptr, *d_invsr = nullptr, *d_vissr = nullptr;
+    double *d_res = nullptr, *d_dt = nullptr, *d_invsr = nullptr, *d_vissr = nullptr, *d_rad = nullptr;
+    void *d_dq = nullptr;                                   // [nCells][DQR] at the face precision
     double *d_bcq = nullptr, *d_partial = nullptr, *d_scal = nullptr, *d_hist = nullptr;
     void *d_gl = nullptr, *d_mm = nullptr;                  // gradient+limiter records, min/max differences
     int *d_fix = nullptr;

@@ -14,9 +14,31 @@ constexpr double SMALLD = 1.0e-40;   // codes/basic/include/HXTypeBasic.h:34
 constexpr int NEQ = 5;
 constexpr int REC = 8;               // state record: rho u v w p T mul mut
 enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4, ITT = 5, IML = 6, IMT = 7 };
+// Minimum resident 128-thread blocks per SM asked of the compiler for the
+// FP32 gather kernels; caps their registers at 65536 / (128 n).  Chosen by
+// timing the 6M-cell plate (no spills at these caps).  The FP64 kernels keep
+// the compiler's choice.
+#ifndef OFG_MINB_RES
+#define OFG_MINB_RES 4
+#endif
+#ifndef OFG_MINB_GL
+#define OFG_MINB_GL 8
+#endif
+#ifndef OFG_MINB_SW
+#define OFG_MINB_SW 8
+#endif
+#ifndef OFG_MINB_TR
+#define OFG_MINB_TR 8
+#endif
+template <typename R> struct MinBlocks { enum { res = 1, gl = 1, sw = 1, tr = 1 }; };
+template <> struct MinBlocks<float> {
+    enum { res = OFG_MINB_RES, gl = OFG_MINB_GL, sw = OFG_MINB_SW, tr = OFG_MINB_TR };
+};
+
 constexpr int GLR = 24;   // gradient+limiter record: [var*3+dir] for 6 vars (q, T), limiter at 18..22
 constexpr int FGR = 8;    // face record: nx ny nz area xfc yfc zfc -
 constexpr int CGR = 4;    // cell record: xcc ycc zcc vol
+constexpr int DQR = 8;    // increment record: dq[5] + 3 zero slots (64 B FP64, 32 B FP32: whole sectors)
 constexpr int MMR = 10;   // neighbour min/max differences per cell (Venkatakrishnan with the zone-wide eps)
 
 // slots of the small device scalar array (cfl, min dt, limiter eps, norms,
@@ -35,7 +57,9 @@ template <> __device__ __forceinline__ float small_v<float>() { return 1.1754943
 template <typename R> __device__ __forceinline__ R Rsqrt(R x);
 template <> __device__ __forceinline__ double Rsqrt<double>(double x) { return sqrt(x); }
 template <> __device__ __forceinline__ float Rsqrt<float>(float x) { return sqrtf(x); }
-template <typename R> __device__ __forceinline__ R Rabs(R x) { return x < R(0) ? -x : x; }
+template <typename R> __device__ __forceinline__ R Rabs(R x);   // std::abs: clears the sign of -0.0 too
+template <> __device__ __forceinline__ double Rabs<double>(double x) { return fabs(x); }
+template <> __device__ __forceinline__ float Rabs<float>(float x) { return fabsf(x); }
 template <typename R> __device__ __forceinline__ R Rmax(R a, R b) { return a > b ? a : b; }
 template <typename R> __device__ __forceinline__ R Rmin(R a, R b) { return a < b ? a : b; }
 template <typename R> __device__ __forceinline__ R SQR3(R a, R b, R c) { return a * a + b * b + c * c; }

@@ -29,7 +29,8 @@ struct KArgs {
     const R *cgeo;                         // [nT][CGR]
     const double *q;  double *qn;          // master state records [nT][REC], current / next
     const R *qs;      R *qsn;              // state records read by face kernels (== master in FP64)
-    double *res, *dq, *dt, *invsr, *vissr, *bcq;
+    double *res, *dt, *invsr, *vissr, *rad, *bcq;   // rad: LU-SGS diagonal
+    R *dq;                                 // [nCells][DQR] LU-SGS increments (whole sectors per cell)
     R *gl;                                 // [nCells][GLR]
     R *mm;                                 // [nCells][MMR]
     double *partial, *scal;
@@ -51,11 +52,17 @@ __device__ __forceinline__ void ld4(const double *p, double *o) {
     o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
 }
 template <typename T> __device__ __forceinline__ void ld8(const T *p, T *o) { ld4(p, o); ld4(p + 4, o + 4); }
-// plain (coherent) loads for data written earlier in the same kernel launch sequence but
-// possibly by this kernel's other blocks (LU-SGS increments)
-__device__ __forceinline__ void ldc5(const double *p, double *o) {
+// plain (coherent) vector loads, for a record the same launch writes afterwards
+__device__ __forceinline__ void ldp8(const float *p, float *o) {
+    float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w; o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+__device__ __forceinline__ void ldp8(const double *p, double *o) {
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) o[e] = p[e];
+    for (int i = 0; i < 4; ++i) {
+        double2 a = reinterpret_cast<const double2 *>(p)[i];
+        o[2 * i] = a.x; o[2 * i + 1] = a.y;
+    }
 }
 
 __device__ __forceinline__ void st4(float *p, const float *v) {
@@ -125,15 +132,32 @@ __global__ void __launch_bounds__(256) k_timestep_min(KArgs<R> A, int nPartial) 
     if (threadIdx.x == 0) A.scal[S_MINDT] = smin[0];
 }
 
-// UTimeStep::ModifyTimeStep / CalcLgTimeStep
+// UTimeStep::ModifyTimeStep / CalcLgTimeStep, then the diagonal of the
+// LU-SGS system for the sweeps: UNsSpectrum::CalcImplicitSpectrum
+// (sp2 = 1 for a steady solve), rad = (1/dt) vol + inviscid + viscous radius
 template <typename R>
 __global__ void __launch_bounds__(256) k_timestep_clip(KArgs<R> A) {
-    if (A.P.timestepModel == 1) return;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= A.nCells) return;
-    double mn = A.scal[S_MINDT];
-    if (A.P.timestepModel == 2) { A.dt[c] = mn; return; }
-    if (A.P.max_time_ratio > 0) A.dt[c] = fmin(A.dt[c], A.P.max_time_ratio * mn);
+    double ts = A.dt[c];
+    if (A.P.timestepModel != 1) {
+        double mn = A.scal[S_MINDT];
+        if (A.P.timestepModel == 2) { ts = mn; A.dt[c] = ts; }
+        else if (A.P.max_time_ratio > 0) { ts = fmin(ts, A.P.max_time_ratio * mn); A.dt[c] = ts; }
+    }
+    double s = (1.0 / ts) * double(A.cgeo[(size_t)c * CGR + 3]);
+    s += A.invsr[c];
+    s += A.vissr[c];
+    A.rad[c] = s;
+}
+
+// x + (-y) / d without the division when it adds nothing: y = +0.0 and d > 0
+// give -0.0, and v + (-0.0) == v bit for bit.  (Measured: without the test,
+// the first upper-sweep level, whose cells have no later neighbours and so
+// y = +0.0, executed three times the instructions of the first lower level.)
+__device__ __forceinline__ double add_neg_quot(double x, double y, double d) {
+    if (y == 0.0 && !signbit(y) && d > 0.0) return x;
+    return x + (-y) / d;
 }
 
 // ---------------------------------------------------------------------------
@@ -193,7 +217,7 @@ __device__ __forceinline__ void cell_limiter(const KArgs<R> &A, int c, const R *
 }
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_gradlim(KArgs<R> A, int nvar, int limMode) {
+__global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, int nvar, int limMode) {
     __shared__ double sred[2 * NEQ][128];
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     bool active = c < A.nCells;
@@ -495,13 +519,13 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
 
 // One gather pass per cell: face radii + time step, inviscid residual and
 // viscous residual.  The FP64 path adds the viscous face terms after all the
-// inviscid ones, as the reference's two scatter passes do; the FP32 path keeps
-// them in a second FP64 accumulator and adds it at the end (one pass over the
-// faces instead of two).
+// inviscid ones, as the reference's two scatter passes do; the FP32 path adds
+// each face's inviscid and viscous terms together (one pass over the faces
+// instead of two).
 // MODE 0: residual and time step (one outer iteration), 1: time step only
 // (the CALC_TIME_STEP task), 2: residual only (the UPDATE_RESIDUALS task).
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128) k_residual(KArgs<R> A) {
+__global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A) {
     __shared__ double smin[128];
     constexpr bool exactOrder = sizeof(R) == 8;
     constexpr bool doRes = MODE != 1, doDt = MODE != 2;
@@ -519,9 +543,9 @@ __global__ void __launch_bounds__(128) k_residual(KArgs<R> A) {
         }
         R gam = R(P.gama), ce1 = R(P.centropy1), ce2 = R(P.centropy2), orey = R(P.oreynolds);
         double inv = 0.0, vis = 0.0;
-        double acc[NEQ], accv[NEQ];
+        double acc[NEQ];
 #pragma unroll
-        for (int e = 0; e < NEQ; ++e) { acc[e] = -0.0; accv[e] = 0.0; }   // LoadResiduals: res = -rhs, rhs = 0
+        for (int e = 0; e < NEQ; ++e) acc[e] = -0.0;   // LoadResiduals: res = -rhs, rhs = 0
         int b = A.nb_off[c], en = A.nb_off[c + 1];
         for (int k = b; k < en; ++k) {
             int2 e2 = __ldg(&A.nbl[k]);
@@ -550,24 +574,27 @@ __global__ void __launch_bounds__(128) k_residual(KArgs<R> A) {
             if (P.ischeme == 12) slau2Flux(t1, t2, fg[0], fg[1], fg[2], gam, fl);
             else roeFlux(t1, t2, fg[0], fg[1], fg[2], gam, P.ieigenfix, ce1, ce2, fl);
             R ar = fg[3];
-#pragma unroll
-            for (int e = 0; e < NEQ; ++e) {
-                double v = double(ar * fl[e]);
-                if (!right) acc[e] -= v; else acc[e] += v;
-            }
             if (!exactOrder && P.vismodel > 0) {
+                // FP32 path: the face's viscous term joins its inviscid term
+                // (both exact in FP64) before the FP64 accumulation
                 R fv[NEQ];
                 face_vis_flux(P, ql, qr, fg, cgl, cgr, gll, glr, fv);
                 R coeff = -orey * ar;
 #pragma unroll
                 for (int e = 0; e < NEQ; ++e) {
-                    double v = double(coeff * fv[e]);
-                    if (!right) accv[e] -= v; else accv[e] += v;
+                    double v = double(ar * fl[e]) + double(coeff * fv[e]);
+                    if (!right) acc[e] -= v; else acc[e] += v;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < NEQ; ++e) {
+                    double v = double(ar * fl[e]);
+                    if (!right) acc[e] -= v; else acc[e] += v;
                 }
             }
         }
-        if (doRes && P.vismodel > 0) {
-            if (exactOrder) {
+        if (exactOrder && doRes && P.vismodel > 0) {
+            {
                 for (int k = b; k < en; ++k) {
                     int2 e2 = __ldg(&A.nbl[k]);
                     int f = nb_face(e2), nb = e2.y;
@@ -593,9 +620,6 @@ __global__ void __launch_bounds__(128) k_residual(KArgs<R> A) {
                         if (!right) acc[e] -= v; else acc[e] += v;
                     }
                 }
-            } else {
-#pragma unroll
-                for (int e = 0; e < NEQ; ++e) acc[e] += accv[e];
             }
         }
         if (doRes) {
@@ -642,7 +666,7 @@ __global__ void __launch_bounds__(128) k_residual(KArgs<R> A) {
 // ---------------------------------------------------------------------------
 // qa: the cell being solved (left after GCom::SetGeometry's swap), qb: neighbour
 template <typename R>
-__device__ __forceinline__ void face_increment(const DevParams &P, const R *qa, const R *qb, const double *dqj, R xn,
+__device__ __forceinline__ void face_increment(const DevParams &P, const R *qa, const R *qb, const R *dqj, R xn,
                                                R yn, R zn, R fa, const R *cga, const R *cgb, double *rhs0) {
     R vfn = R(0);
     R half = R(0.5), one = R(1), gl = R(P.gama), gr = gl;
@@ -723,12 +747,13 @@ __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *
     for (int k = off[c]; k < off[c + 1]; ++k) {
         int2 e2 = __ldg(&list[k]);
         int f = nb_face(e2), nb = e2.y;
-        R qn[REC], cgn[CGR], fg[FGR];
-        double dqj[NEQ];
+        R qn[REC], cgn[CGR], fg[FGR], dqj[DQR];
         ld8(A.qs + (size_t)nb * REC, qn);
         ld4(A.cgeo + (size_t)nb * CGR, cgn);
         ld4(A.fgeo + (size_t)f * FGR, fg);
-        ldc5(A.dq + (size_t)nb * NEQ, dqj);
+        // the neighbour's increment was written by an earlier level's launch
+        // and is not written by this one: read-only here
+        ld8(A.dq + (size_t)nb * DQR, dqj);
         R xn = fg[0], yn = fg[1], zn = fg[2];
         if (nb_right(e2)) { xn = -xn; yn = -yn; zn = -zn; }   // GCom::SetGeometry
         face_increment(A.P, qc, qn, dqj, xn, yn, zn, fg[3], cgc, cgn, rhs0);
@@ -736,39 +761,36 @@ __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *
 }
 
 template <typename R>
-__device__ __forceinline__ double implicit_radius(const KArgs<R> &A, int c) {
-    // UNsSpectrum::CalcImplicitSpectrum (sp2 = 1 for a steady solve)
-    double s = (1.0 / A.dt[c]) * double(A.cgeo[(size_t)c * CGR + 3]);
-    s += A.invsr[c];
-    s += A.vissr[c];
-    return s;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(128) k_lusgs_lower(KArgs<R> A, const int *order, int start, int count) {
+__global__ void __launch_bounds__(128, MinBlocks<R>::sw) k_lusgs_lower(KArgs<R> A, const int *order, int start, int count) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     int c = order[start + t];
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
     sweep_rhs0(A, c, A.lo_off, A.lol, rhs0);
-    double rad = implicit_radius(A, c);
+    double rad = A.rad[c];
     const double *rs = A.res + (size_t)c * NEQ;
-    double *d = A.dq + (size_t)c * NEQ;
+    R o[DQR];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) d[e] = (rs[e] - rhs0[e]) / rad;
+    for (int e = 0; e < NEQ; ++e) o[e] = R((rs[e] - rhs0[e]) / rad);
+    o[5] = o[6] = o[7] = R(0);
+    st4(A.dq + (size_t)c * DQR, o);
+    st4(A.dq + (size_t)c * DQR + 4, o + 4);
 }
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_lusgs_upper(KArgs<R> A, const int *order, int start, int count) {
+__global__ void __launch_bounds__(128, MinBlocks<R>::sw) k_lusgs_upper(KArgs<R> A, const int *order, int start, int count) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     int c = order[start + t];
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
     sweep_rhs0(A, c, A.up_off, A.upl, rhs0);   // ghost increments are zero: boundary faces not listed
-    double rad = implicit_radius(A, c);
-    double *d = A.dq + (size_t)c * NEQ;
+    double rad = A.rad[c];
+    R o[DQR];
+    ldp8(A.dq + (size_t)c * DQR, o);   // its own lower-sweep increment, rewritten below
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) d[e] += (-rhs0[e]) / rad;
+    for (int e = 0; e < NEQ; ++e) o[e] = R(add_neg_quot(double(o[e]), rhs0[e], rad));
+    st4(A.dq + (size_t)c * DQR, o);
+    st4(A.dq + (size_t)c * DQR + 4, o + 4);
 }
 
 // ---------------------------------------------------------------------------
@@ -819,11 +841,12 @@ __global__ void __launch_bounds__(256) k_update(KArgs<R> A) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= A.nCells) return;
     const double *qc = A.q + (size_t)c * REC;
-    const double *d = A.dq + (size_t)c * NEQ;
+    R d[DQR];
+    ld8(A.dq + (size_t)c * DQR, d);
     double gama = A.P.gama;
     double prim0[NEQ], q0[NEQ], qq[NEQ], pr[NEQ], dd[NEQ];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) { prim0[e] = qc[e]; dd[e] = d[e]; }
+    for (int e = 0; e < NEQ; ++e) { prim0[e] = qc[e]; dd[e] = double(d[e]); }
     primToQ(prim0, gama, q0);
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) qq[e] = q0[e] + dd[e];

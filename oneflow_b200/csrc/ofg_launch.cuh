@@ -50,7 +50,8 @@ KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
         A.qs = reinterpret_cast<const R *>(A.q);
         A.qsn = reinterpret_cast<R *>(A.qn);
     }
-    A.res = c->d_res; A.dq = c->d_dq; A.dt = c->d_dt; A.invsr = c->d_invsr; A.vissr = c->d_vissr;
+    A.res = c->d_res; A.dq = static_cast<R *>(c->d_dq); A.dt = c->d_dt; A.invsr = c->d_invsr; A.vissr = c->d_vissr;
+    A.rad = c->d_rad;
     A.bcq = c->d_bcq; A.gl = static_cast<R *>(c->d_gl); A.mm = static_cast<R *>(c->d_mm);
     A.partial = c->d_partial; A.scal = c->d_scal; A.fixlist = c->d_fix; A.fixcap = c->fixcap;
     A.nut = c->d_nut; A.dnut = c->d_dnut; A.resT = c->d_resT; A.impsrT = c->d_impsrT;

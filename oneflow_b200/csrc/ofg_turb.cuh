@@ -136,6 +136,7 @@ __device__ __forceinline__ R calc_angle(R dx, R dy, R dz, R dist) {
     R result = dist / (Rsqrt(SQR3(dx, dy, dz)) + small_v<R>());
     if (result > R(1)) result = R(1);
     if (result < R(-1)) result = R(-1);
+    if (sizeof(R) == 4) return R(asinf(float(result)) * 57.29577951f);
     return R(asin(double(result)) * 180.0 / 3.141592653589793);
 }
 
@@ -149,7 +150,7 @@ __device__ __forceinline__ R calc_angle(R dx, R dy, R dz, R dist) {
 // diffusion) in order; the FP32 path fuses them into one pass with separate
 // FP64 accumulators that are added in the reference's order at the end.
 template <typename R>
-__global__ void __launch_bounds__(128) k_turb_rhs(KArgs<R> A) {
+__global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_rhs(KArgs<R> A) {
     constexpr bool exactOrder = sizeof(R) == 8;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= A.nCells) return;
@@ -177,59 +178,62 @@ __global__ void __launch_bounds__(128) k_turb_rhs(KArgs<R> A) {
             ld8(A.qs + (size_t)nb * REC, qn);
             ld8(A.fgeo + (size_t)f * FGR, fg);
             ld4(A.cgeo + (size_t)nb * CGR, cgn);
-            double nutn = A.nut[nb];
             const R *ql = right ? qn : qc, *qr = right ? qc : qn;
             const R *cgl = right ? cgn : cgc, *cgr = right ? cgc : cgn;
-            double nl = right ? nutn : nutc, nr = right ? nutc : nutn;
-            double xn = fg[0], yn = fg[1], zn = fg[2], ar = fg[3];
+            // face terms at the face precision (FP64 path: the reference's
+            // arithmetic), accumulated in FP64
+            R nutn = R(A.nut[nb]), nutcR = R(nutc);
+            R nl = right ? nutn : nutcR, nr = right ? nutcR : nutn;
+            R xn = fg[0], yn = fg[1], zn = fg[2], ar = fg[3];
+            const R hf = R(0.5);
             if (!exactOrder || pass == 0) {
                 // ---- spectral radius and sweep coefficients ----
-                double vnl = xn * double(ql[IU]) + yn * double(ql[IV]) + zn * double(ql[IW]) - 0.0;
-                double vnr = xn * double(qr[IU]) + yn * double(qr[IV]) + zn * double(qr[IW]) - 0.0;
-                double absVn = fabs(half * (vnl + vnr));
-                double r1 = 0.0, m1 = 0.0, m2 = 0.0;
-                r1 += ar * half * absVn;
-                m1 += ar * half * (-vnl - absVn);
-                m2 += ar * half * (vnr - absVn);
-                double orl = 1.0 / (double(ql[IR]) + SMALLD), orr = 1.0 / (double(qr[IR]) + SMALLD);
-                double nuet1 = double(ql[IML]) * orl + nl, nuet2 = double(qr[IML]) * orr + nr;
-                double nueff = fabs(half * (nuet1 + nuet2));
-                double ovol = 1.0 / (half * (double(cgl[3]) + double(cgr[3])));
-                double d = P.oreynolds * ovol * (P.sa_osigma * nueff * (ar * ar));
+                R vnl = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - R(0);
+                R vnr = xn * qr[IU] + yn * qr[IV] + zn * qr[IW] - R(0);
+                R absVn = Rabs(hf * (vnl + vnr));
+                R r1 = R(0), m1 = R(0), m2 = R(0);
+                r1 += ar * hf * absVn;
+                m1 += ar * hf * (-vnl - absVn);
+                m2 += ar * hf * (vnr - absVn);
+                R orl = R(1) / (ql[IR] + small_v<R>()), orr = R(1) / (qr[IR] + small_v<R>());
+                R nuet1 = ql[IML] * orl + nl, nuet2 = qr[IML] * orr + nr;
+                R nueff = Rabs(hf * (nuet1 + nuet2));
+                R ovol = R(1) / (hf * (cgl[3] + cgr[3]));
+                R d = R(P.oreynolds) * ovol * (R(P.sa_osigma) * nueff * (ar * ar));
                 r1 += d;
                 m1 += -d;
                 m2 += -d;
-                imp += r1;
-                if (!right) { A.matL[f] = m1; A.matR[f] = m2; }
+                imp += double(r1);
+                if (!right) { A.matL[f] = double(m1); A.matR[f] = double(m2); }
             }
             if (!exactOrder || pass == 1) {
                 // ---- first-order convection with the NS face states ----
-                double t1 = nl, t2 = nr;
-                double u1 = ql[IU], v1 = ql[IV], w1 = ql[IW], u2 = qr[IU], v2 = qr[IV], w2 = qr[IW];
+                R t1 = nl, t2 = nr;
+                R u1 = ql[IU], v1 = ql[IV], w1 = ql[IW], u2 = qr[IU], v2 = qr[IV], w2 = qr[IW];
                 if (f < A.nBFaces) {
-                    double tm = half * (nl + nr);
+                    R tm = hf * (nl + nr);
                     t1 = t2 = tm;
                     if (A.bcType[f] == BC_SOLID) {
                         const double *bq = A.bcq + (size_t)f * NEQ;
-                        u1 = u2 = bq[IU]; v1 = v2 = bq[IV]; w1 = w2 = bq[IW];
+                        u1 = u2 = R(bq[IU]); v1 = v2 = R(bq[IV]); w1 = w2 = R(bq[IW]);
                     } else {
-                        u1 = u2 = half * (double(ql[IU]) + double(qr[IU]));
-                        v1 = v2 = half * (double(ql[IV]) + double(qr[IV]));
-                        w1 = w2 = half * (double(ql[IW]) + double(qr[IW]));
+                        u1 = u2 = hf * (ql[IU] + qr[IU]);
+                        v1 = v2 = hf * (ql[IV] + qr[IV]);
+                        w1 = w2 = hf * (ql[IW] + qr[IW]);
                     }
                 }
-                double vnl = xn * u1 + yn * v1 + zn * w1 - 0.0;
-                double vnr = xn * u2 + yn * v2 + zn * w2 - 0.0;
-                double coef_l = half * (vnl + fabs(vnl)) * 1.0;
-                double coef_r = half * (vnr - fabs(vnr)) * 1.0;
-                double v = ar * (coef_l * t1 + coef_r * t2);
+                R vnl = xn * u1 + yn * v1 + zn * w1 - R(0);
+                R vnr = xn * u2 + yn * v2 + zn * w2 - R(0);
+                R coef_l = hf * (vnl + Rabs(vnl)) * R(1);
+                R coef_r = hf * (vnr - Rabs(vnr)) * R(1);
+                double v = double(ar * (coef_l * t1 + coef_r * t2));
                 if (exactOrder) { if (!right) acc -= v; else acc += v; }
                 else { if (!right) conv -= v; else conv += v; }
             }
             if (!exactOrder || pass == 2) {
                 // ---- diffusion (VIS_TEST face gradient) ----
                 R fxn = fg[0], fyn = fg[1], fzn = fg[2];
-                R q1 = R(nl), q2 = R(nr);
+                R q1 = nl, q2 = nr;
                 R q11 = q1, q22 = q2, qf = R(0.5) * (q1 + q2);
                 R dxl = cgl[0] - fg[4], dyl = cgl[1] - fg[5], dzl = cgl[2] - fg[6];
                 R dxr = cgr[0] - fg[4], dyr = cgr[1] - fg[5], dzr = cgr[2] - fg[6];
@@ -254,11 +258,11 @@ __global__ void __launch_bounds__(128) k_turb_rhs(KArgs<R> A) {
                     if (f < A.nBFaces) { c1 = R(1); c2 = R(0); }
                     dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
                 }
-                double orl = 1.0 / (double(ql[IR]) + SMALLD), orr = 1.0 / (double(qr[IR]) + SMALLD);
-                double visl_nv = half * (double(ql[IML]) * orl + double(qr[IML]) * orr);
-                double vist_nv = half * (nl + nr);
-                double comVis = (visl_nv + vist_nv) * P.sa_osigma;
-                double flux = -P.oreynolds * comVis * double(dqdn) * ar;
+                R orl = R(1) / (ql[IR] + small_v<R>()), orr = R(1) / (qr[IR] + small_v<R>());
+                R visl_nv = hf * (ql[IML] * orl + qr[IML] * orr);
+                R vist_nv = hf * (nl + nr);
+                R comVis = (visl_nv + vist_nv) * R(P.sa_osigma);
+                double flux = double(-R(P.oreynolds) * comVis * dqdn * ar);
                 if (exactOrder) { if (!right) acc -= flux; else acc += flux; }
                 else { if (!right) diffu -= flux; else diffu += flux; }
             }
@@ -375,7 +379,7 @@ __global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order
         int f = nb_face(e2);
         rhs0 += (nb_right(e2) ? A.matL[f] : A.matR[f]) * A.dnut[e2.y];
     }
-    A.dnut[c] += (-rhs0) / A.impsrT[c];
+    A.dnut[c] = add_neg_quot(A.dnut[c], rhs0, A.impsrT[c]);
 }
 
 // UPDATE_FLOWFIELD (TurbUpdate::CalcFlowField1Equ, crelax = 1) fused with the
