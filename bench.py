@@ -125,14 +125,15 @@ def alg_bytes(st, prm) -> dict:
         if prm.ilim == 2 and not prm.venkat_kh3:
             res += N * 10 * g + (gl + N * 10 * g + cg + nbl + fg + N * 5 * g)   # min/max, global eps pass
     res += qs + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24   # k_residual
-    res += N * 16                                                # time-step clip
+    res += N * 24 + N * g + N * 16                               # time-step clip: dt, radii, vol -> dt, diagonal
     out["residual"] = res
-    sweep = qs + cg + F * 4 * g + half_lists + N * 40 + N * 40 + N * 24 + N * 4   # + dq of neighbours, own dq
+    dq = N * 8 * g                                               # increment records
+    sweep = qs + cg + F * 4 * g + half_lists + dq + dq + N * 8 + N * 4   # neighbour dq, own dq write, diagonal, order
     out["lusgs_lower"] = sweep + N * 40                          # + res
-    out["lusgs_upper"] = sweep + N * 40                          # + own dq read before the write
-    out["update"] = N * 64 + N * 40 + N * 64 + (N * 8 * g if mixed else 0)
+    out["lusgs_upper"] = sweep + dq                              # + own dq read before the write
+    out["update"] = N * 64 + dq + N * 64 + (N * 8 * g if mixed else 0)
     out["boundary"] = B * (4 + 4 + 8 * g + 64 + 8 + 64 + 40) + (B * 8 * g if mixed else 0)
-    out["norm"] = N * 40
+    out["norm"] = ((N + 127) // 128) * 40                        # per-block sums left by the residual kernel
     if sa:
         grad_nut = NT * 8 + nbl + cg + (0 if lsq else fg) + N * 4 * g
         rhs = qs + cg + fg + nbl + NT * 8 + N * 4 * g + N * 12 * g + N * 16 + N * 8 + N * 8 + B * 44 \
@@ -143,7 +144,7 @@ def alg_bytes(st, prm) -> dict:
         out["sa_upper"] = sa_sweep
         out["sa_update"] = N * 8 * 3 + N * 24 + N * 8 + (N * g if mixed else 0)
         out["sa_boundary"] = B * (4 + 4 + 8 * g + 24 + 8 + 16)
-        out["sa_norm"] = N * 8
+        out["sa_norm"] = ((N + 127) // 128) * 8
     return out
 
 

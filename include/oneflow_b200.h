@@ -147,9 +147,11 @@ int ofg_calc_boundary(ofg_ctx *ctx, int tid);       /* CALC_BOUNDARY          */
    :349-360), with the RMS residual of every iteration appended to the history. */
 int ofg_step(ofg_ctx *ctx, int nsteps);
 
-/* RMS residual per equation of the last UPDATE_RESIDUALS
+/* RMS residual per equation of the solver's last UPDATE_RESIDUALS
    (ResidualTask::CalcRes + ResAver::CalcAver,
-   codes/residual/src/ResidualTask.cpp:75-126, codes/residual/src/Residual.cpp:52-72). */
+   codes/residual/src/ResidualTask.cpp:75-126, codes/residual/src/Residual.cpp:52-72):
+   rms[0..4] for the NS solver, rms[0] for the SA solver.  The residual
+   history is not touched. */
 int ofg_residual_norms(ofg_ctx *ctx, int tid, double *rms);
 
 /* Named device field -> host, reference layout:

@@ -422,7 +422,7 @@ void ofg_destroy(ofg_ctx *c) {
     void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
                     c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist,
                     c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_rad,
-                    c->d_bcq, c->d_partial, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
+                    c->d_bcq, c->d_partial, c->d_npart, c->d_tpart, c->d_red, c->d_redCount, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
     for (void *v : ptrs) if (v) cudaFree(v);
     cudaStreamDestroy(c->ownStream ? c->ownStream : c->stream);
@@ -537,6 +537,14 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     if ((rc = upload<double>(c, &c->d_bcq, nullptr, (size_t)std::max(nBFaces, 1) * NEQ))) return rc;
     c->nPartialMax = std::max<size_t>((N + 127) / 128 * 10, 2 * 148 * NEQ) + 16;
     if ((rc = upload<double>(c, &c->d_partial, nullptr, c->nPartialMax))) return rc;
+    size_t nb128 = (N + 127) / 128;
+    if ((rc = upload<double>(c, &c->d_npart, nullptr, nb128 * NEQ))) return rc;
+    if ((rc = upload<double>(c, &c->d_tpart, nullptr, nb128))) return rc;
+    CK(cudaMemset(c->d_npart, 0, nb128 * NEQ * sizeof(double)));
+    CK(cudaMemset(c->d_tpart, 0, nb128 * sizeof(double)));
+    if ((rc = upload<double>(c, &c->d_red, nullptr, (size_t)kRedBlocks * NEQ))) return rc;
+    if ((rc = upload<unsigned int>(c, &c->d_redCount, nullptr, 1))) return rc;
+    CK(cudaMemset(c->d_redCount, 0, sizeof(unsigned int)));
     if ((rc = upload<double>(c, &c->d_scal, nullptr, 32))) return rc;
     c->histCap = 1 << 16;
     if ((rc = upload<double>(c, &c->d_hist, nullptr, (size_t)c->histCap * NEQ))) return rc;
@@ -802,10 +810,12 @@ int ofg_residual_norms(ofg_ctx *c, int tid, double *rms) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
     if (!rms) return c->fail(OFG_E_ARG, "null output");
-    // norms of the current residual field (recomputed, so per-task callers get them too)
-    if ((rc = launch(c, T_NORM))) return rc;
+    // from the per-block sums the residual kernels leave (per-task callers get them too)
+    bool turb = tid == OFG_TURB_SOLVER;
+    if ((rc = launch(c, turb ? T_TURB_NORM_ONLY : T_NORM_ONLY))) return rc;
     if ((rc = sync(c))) return rc;
-    CK(cudaMemcpy(rms, c->d_scal + S_NORM, NEQ * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(rms, c->d_scal + (turb ? S_TNORM : S_NORM), (turb ? 1 : NEQ) * sizeof(double),
+                  cudaMemcpyDeviceToHost));
     return OFG_OK;
 }
 

@@ -35,6 +35,8 @@ template <> struct MinBlocks<float> {
     enum { res = OFG_MINB_RES, gl = OFG_MINB_GL, sw = OFG_MINB_SW, tr = OFG_MINB_TR };
 };
 
+constexpr int kRedBlocks = 148;   // blocks of the grid reductions (one per SM)
+
 constexpr int GLR = 24;   // gradient+limiter record: [var*3+dir] for 6 vars (q, T), limiter at 18..22
 constexpr int FGR = 8;    // face record: nx ny nz area xfc yfc zfc -
 constexpr int CGR = 4;    // cell record: xcc ycc zcc vol

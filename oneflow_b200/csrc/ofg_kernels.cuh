@@ -34,6 +34,8 @@ struct KArgs {
     R *gl;                                 // [nCells][GLR]
     R *mm;                                 // [nCells][MMR]
     double *partial, *scal;
+    double *npart, *tpart;                 // per-block sums of squares of res / resT (128-cell blocks)
+    double *red; unsigned int *redCount;   // block sums and ticket of the grid reductions
     int *fixlist; int fixcap;
     // Spalart-Allmaras
     double *nut, *dnut, *resT, *impsrT, *matL, *matR;
@@ -71,6 +73,85 @@ __device__ __forceinline__ void st4(float *p, const float *v) {
 __device__ __forceinline__ void st4(double *p, const double *v) {
     reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
     reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// Block reductions for 1-D blocks of up to 1024 threads (a multiple of 32),
+// in a fixed shuffle/tree order (run-to-run deterministic).  Every thread of
+// the block must call them.
+template <int N>
+__device__ __forceinline__ void block_sum_to(const double *v, double *out) {
+    __shared__ double s[32][N];
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        double x = v[e];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (l == 0) s[w][e] = x;
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            double y = l < nw ? s[l][e] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
+            if (l == 0) out[e] = y;
+        }
+    }
+}
+
+// Deterministic sum over the grid of n records of N doubles (in[i*N+e]):
+// every block adds a contiguous chunk in a fixed order and leaves its sum in
+// red[block]; the last block to finish (ticket on *counter) adds the block
+// sums in block order into out[] (valid in that block's thread 0 only) and
+// re-arms the counter.  Returns true in the block that produced out[].
+template <int N>
+__device__ __forceinline__ bool grid_sum_last(const double *in, int n, double *red, unsigned int *counter,
+                                              double *out) {
+    int G = gridDim.x;
+    int per = (n + G - 1) / G;
+    int b0 = blockIdx.x * per, b1 = min(n, b0 + per);
+    double acc[N];
+#pragma unroll
+    for (int e = 0; e < N; ++e) acc[e] = 0.0;
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x)
+#pragma unroll
+        for (int e = 0; e < N; ++e) acc[e] += in[(size_t)i * N + e];
+    __shared__ double tot[N];
+    __shared__ bool last;
+    block_sum_to<N>(acc, tot);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) red[(size_t)blockIdx.x * N + e] = tot[e];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == unsigned(G - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+#pragma unroll
+    for (int e = 0; e < N; ++e) acc[e] = 0.0;
+    for (int i = threadIdx.x; i < G; i += blockDim.x)
+#pragma unroll
+        for (int e = 0; e < N; ++e) acc[e] += __ldcg(red + (size_t)i * N + e);
+    block_sum_to<N>(acc, out);
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+__device__ __forceinline__ double block_min(double x) {
+    __shared__ double s[32];
+    __shared__ double r;
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+    if (l == 0) s[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        double y = l < nw ? s[l] : 1.0e300;
+        for (int o = 16; o > 0; o >>= 1) y = fmin(y, __shfl_down_sync(0xffffffffu, y, o));
+        if (l == 0) r = y;
+    }
+    __syncthreads();
+    return r;
 }
 
 __device__ __forceinline__ int nb_face(int2 e) { return e.x & 0x7fffffff; }
@@ -114,22 +195,6 @@ __device__ __forceinline__ double face_vis_spec(const DevParams &P, const R *ql,
         return double(ar * ar / (R(P.reynolds) * density + small_v<R>()));
     }
     return 0.0;
-}
-
-// UTimeStep::CalcMinTimeStep: zone-wide minimum (single block over per-block
-// partials; min is exact in any order)
-template <typename R>
-__global__ void __launch_bounds__(256) k_timestep_min(KArgs<R> A, int nPartial) {
-    __shared__ double smin[256];
-    double m = 1.0e40;
-    for (int i = threadIdx.x; i < nPartial; i += blockDim.x) m = fmin(m, A.partial[i]);
-    smin[threadIdx.x] = m;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) A.scal[S_MINDT] = smin[0];
 }
 
 // UTimeStep::ModifyTimeStep / CalcLgTimeStep, then the diagonal of the
@@ -526,11 +591,11 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
 // (the CALC_TIME_STEP task), 2: residual only (the UPDATE_RESIDUALS task).
 template <typename R, int MODE>
 __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A) {
-    __shared__ double smin[128];
     constexpr bool exactOrder = sizeof(R) == 8;
     constexpr bool doRes = MODE != 1, doDt = MODE != 2;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     double mydt = 1.0e40;
+    double sq[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (c < A.nCells) {
         const DevParams &P = A.P;
         R qc[REC], cgc[CGR], glc[GLR];
@@ -625,7 +690,7 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
         if (doRes) {
             double *o = A.res + (size_t)c * NEQ;
 #pragma unroll
-            for (int e = 0; e < NEQ; ++e) o[e] = acc[e];
+            for (int e = 0; e < NEQ; ++e) { o[e] = acc[e]; sq[e] = acc[e] * acc[e]; }
         }
         if (doDt) {
             // local time step (UTimeStep::CalcInvTimeStep / CalcVisTimeStep)
@@ -647,14 +712,15 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
             mydt = ts;
         }
     }
-    if (!doDt) return;
-    smin[threadIdx.x] = mydt;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + s]);
-        __syncthreads();
+    // block epilogue: sums of squares for the residual norm (fixed order:
+    // deterministic), and the zone-wide minimum time step by an atomic minimum
+    // on the bit pattern (non-negative doubles order like their bits)
+    if (doRes) block_sum_to<NEQ>(sq, A.npart + (size_t)blockIdx.x * NEQ);
+    if (doDt) {
+        double m = block_min(mydt);
+        if (threadIdx.x == 0)
+            atomicMin(reinterpret_cast<unsigned long long *>(A.scal + S_MINDT), (unsigned long long)__double_as_longlong(m));
     }
-    if (threadIdx.x == 0) A.partial[blockIdx.x] = smin[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -1041,54 +1107,15 @@ __global__ void __launch_bounds__(256) k_boundary(KArgs<R> A, const int *lcb) {
 // ---------------------------------------------------------------------------
 // Residual norms: ResidualTask::CalcRes + ResAver::CalcAver
 // (codes/residual/src/ResidualTask.cpp:75-126, codes/residual/src/Residual.cpp:52-72).
-// Two-stage fixed-shape reduction in FP64: deterministic run to run.
+// The residual kernel leaves per-block sums of squares; they are added in a
+// fixed order (FP64, deterministic run to run) by a grid of blocks whose last
+// block to finish produces the norms.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(256) k_norm_partial(KArgs<R> A) {
-    __shared__ double s[NEQ][256];
-    double acc[NEQ] = {0, 0, 0, 0, 0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.nCells; c += gridDim.x * blockDim.x) {
-        const double *r = A.res + (size_t)c * NEQ;
-#pragma unroll
-        for (int e = 0; e < NEQ; ++e) acc[e] += r[e] * r[e];
-    }
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e) s[e][threadIdx.x] = acc[e];
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if (threadIdx.x < st)
-#pragma unroll
-            for (int e = 0; e < NEQ; ++e) s[e][threadIdx.x] += s[e][threadIdx.x + st];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-#pragma unroll
-        for (int e = 0; e < NEQ; ++e) A.partial[(size_t)blockIdx.x * NEQ + e] = s[e][0];
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256) k_norm_final(KArgs<R> A, int nPartial, double *hist) {
-    __shared__ double s[NEQ][256];
-    double acc[NEQ] = {0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < nPartial; i += blockDim.x)
-#pragma unroll
-        for (int e = 0; e < NEQ; ++e) acc[e] += A.partial[(size_t)i * NEQ + e];
-#pragma unroll
-    for (int e = 0; e < NEQ; ++e) s[e][threadIdx.x] = acc[e];
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if (threadIdx.x < st)
-#pragma unroll
-            for (int e = 0; e < NEQ; ++e) s[e][threadIdx.x] += s[e][threadIdx.x + st];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        for (int e = 0; e < NEQ; ++e) {
-            double rms = sqrt(s[e][0] / A.nCells);
-            A.scal[S_NORM + e] = rms;
-            if (hist) hist[e] = rms;
-        }
-    }
+__global__ void __launch_bounds__(256) k_norm_final(KArgs<R> A, int nPartial) {
+    __shared__ double tot[NEQ];
+    if (grid_sum_last<NEQ>(A.npart, nPartial, A.red, A.redCount, tot) && threadIdx.x == 0)
+        for (int e = 0; e < NEQ; ++e) A.scal[S_NORM + e] = sqrt(tot[e] / A.nCells);
 }
 
 }  // namespace ofg

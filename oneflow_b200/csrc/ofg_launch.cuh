@@ -9,9 +9,11 @@
 namespace ofg {
 
 // CFL ramp (TimeStep::CalcCfl, codes/ns/src/TimeStep.cpp:43-59).  step < 0:
-// advance the device-side outer-step counter first (graph path).
+// advance the device-side outer-step counter first (graph path).  Also resets
+// the zone-wide minimum time step that the residual kernel's blocks lower.
 static __global__ void k_cfl(double *scal, double step, double cflst, double cfled, int ncfl) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    scal[S_MINDT] = 1.0e40;
     double it = step;
     if (step < 0) { scal[S_STEP] += 1.0; it = scal[S_STEP]; } else { scal[S_STEP] = step; }
     double cfl = cfled;
@@ -54,6 +56,7 @@ KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
     A.rad = c->d_rad;
     A.bcq = c->d_bcq; A.gl = static_cast<R *>(c->d_gl); A.mm = static_cast<R *>(c->d_mm);
     A.partial = c->d_partial; A.scal = c->d_scal; A.fixlist = c->d_fix; A.fixcap = c->fixcap;
+    A.npart = c->d_npart; A.tpart = c->d_tpart; A.red = c->d_red; A.redCount = c->d_redCount;
     A.nut = c->d_nut; A.dnut = c->d_dnut; A.resT = c->d_resT; A.impsrT = c->d_impsrT;
     A.matL = c->d_matL; A.matR = c->d_matR; A.gnut = static_cast<R *>(c->d_gnut);
     return A;
@@ -96,11 +99,9 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         OFG_LAUNCH(k_cfl, 1, 32, s, c->d_scal, -1.0, c->p.cflst, c->p.cfled, c->p.ncfl);
         break;
     }
-    case T_TIMESTEP: {   // CALC_TIME_STEP alone
+    case T_TIMESTEP: {   // CALC_TIME_STEP alone (after T_CFL, which resets the minimum)
         KArgs<R> A = make_args<R>(c, false);
-        int nb = nblk(N, 128);
-        OFG_LAUNCH((k_residual<R, 1>), nb, 128, s, A);
-        OFG_LAUNCH(k_timestep_min<R>, 1, 256, s, A, nb);
+        OFG_LAUNCH((k_residual<R, 1>), nblk(N, 128), 128, s, A);
         OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }
@@ -113,9 +114,7 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     case T_TS_RES: {     // CALC_TIME_STEP + LOAD_RESIDUALS + UPDATE_RESIDUALS in one gather
         KArgs<R> A = make_args<R>(c, false);
         launch_gradlim<R>(c, A, s);
-        int nb = nblk(N, 128);
-        OFG_LAUNCH((k_residual<R, 0>), nb, 128, s, A);
-        OFG_LAUNCH(k_timestep_min<R>, 1, 256, s, A, nb);
+        OFG_LAUNCH((k_residual<R, 0>), nblk(N, 128), 128, s, A);
         OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }
@@ -154,12 +153,11 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb);
         break;
     }
-    case T_NORM: {
+    case T_NORM:         // norms of the last residual, appended to the history
+    case T_NORM_ONLY: {  // the same without the history entry
         KArgs<R> A = make_args<R>(c, false);
-        int nb = 2 * 148;
-        OFG_LAUNCH(k_norm_partial<R>, nb, 256, s, A);
-        OFG_LAUNCH(k_norm_final<R>, 1, 256, s, A, nb, (double *)nullptr);
-        OFG_LAUNCH(k_norm_hist, 1, 32, s, c->d_scal, c->d_hist, c->histCap);
+        OFG_LAUNCH(k_norm_final<R>, kRedBlocks, 256, s, A, nblk(N, 128));
+        if (task == T_NORM) OFG_LAUNCH(k_norm_hist, 1, 32, s, c->d_scal, c->d_hist, c->histCap);
         break;
     }
     case T_TURB_RHS: {
@@ -203,11 +201,11 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb, 1);
         break;
     }
-    case T_TURB_NORM: {
+    case T_TURB_NORM:
+    case T_TURB_NORM_ONLY: {
         KArgs<R> A = make_args<R>(c, true);
-        int nb = 2 * 148;
-        OFG_LAUNCH(k_turb_norm_partial<R>, nb, 256, s, A);
-        OFG_LAUNCH(k_turb_norm_final<R>, 1, 256, s, A, nb, c->d_thist, c->histCap);
+        OFG_LAUNCH(k_turb_norm_final<R>, kRedBlocks, 256, s, A, nblk(N, 128),
+                   task == T_TURB_NORM ? c->d_thist : (double *)nullptr, c->histCap);
         break;
     }
     default:

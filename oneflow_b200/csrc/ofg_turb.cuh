@@ -19,11 +19,23 @@ __device__ __forceinline__ double sa_vist(const DevParams &P, double rho, double
     return fmin(vl * P.max_vis_ratio, v);
 }
 
-// write the eddy viscosity of cell i into the master record and its FP32 copy
+// write the eddy viscosity of cell i into the master record and its FP32
+// copy, rewriting whole 32-byte sectors (p T mu_l mu_t of the master, the
+// whole copy) rather than single words
 template <typename R>
 __device__ __forceinline__ void put_vist(const KArgs<R> &A, int i, double v) {
-    const_cast<double *>(A.q)[(size_t)i * REC + IMT] = v;
-    if (sizeof(R) == 4) const_cast<R *>(A.qs)[(size_t)i * REC + IMT] = R(v);
+    double2 *m = reinterpret_cast<double2 *>(const_cast<double *>(A.q) + (size_t)i * REC);
+    double2 a = m[2], b = m[3];
+    b.y = v;
+    m[2] = a;
+    m[3] = b;
+    if (sizeof(R) == 4) {
+        float4 *s = reinterpret_cast<float4 *>(const_cast<R *>(A.qs) + (size_t)i * REC);
+        float4 s0 = s[0], s1 = s[1];
+        s1.w = float(v);
+        s[0] = s0;
+        s[1] = s1;
+    }
 }
 
 // TurbBcSolver face rules (codes/turb/src/TurbBcSolver.cpp:51-262); the
@@ -150,10 +162,8 @@ __device__ __forceinline__ R calc_angle(R dx, R dy, R dz, R dist) {
 // diffusion) in order; the FP32 path fuses them into one pass with separate
 // FP64 accumulators that are added in the reference's order at the end.
 template <typename R>
-__global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_rhs(KArgs<R> A) {
+__device__ __forceinline__ double turb_rhs_cell(const KArgs<R> &A, int c) {
     constexpr bool exactOrder = sizeof(R) == 8;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.nCells) return;
     const DevParams &P = A.P;
     const double half = 0.5;
     int b = A.nb_off[c], en = A.nb_off[c + 1];
@@ -350,6 +360,20 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_rhs(KArgs<R> A) 
     if (!exactOrder) { acc += conv; acc += diffu; }
     A.impsrT[c] = imp;
     A.resT[c] = acc;
+    return acc;
+}
+
+// one thread per cell; the block leaves the sum of squares of its residuals
+// for the norm
+template <typename R>
+__global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_rhs(KArgs<R> A) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double sq = 0.0;
+    if (c < A.nCells) {
+        double r = turb_rhs_cell(A, c);
+        sq = r * r;
+    }
+    block_sum_to<1>(&sq, A.tpart + blockIdx.x);
 }
 
 // LU-SGS sweeps of the SA equation (codes/uturb/src/UTurbLusgs.cpp:90-300,
@@ -407,37 +431,16 @@ __global__ void __launch_bounds__(256) k_turb_vist(KArgs<R> A) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_turb_norm_partial(KArgs<R> A) {
-    __shared__ double s[256];
-    double acc = 0.0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.nCells; c += gridDim.x * blockDim.x)
-        acc += A.resT[c] * A.resT[c];
-    s[threadIdx.x] = acc;
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) A.partial[blockIdx.x] = s[0];
-}
-
-template <typename R>
 __global__ void __launch_bounds__(256) k_turb_norm_final(KArgs<R> A, int nPartial, double *hist, int cap) {
-    __shared__ double s[256];
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < nPartial; i += blockDim.x) acc += A.partial[i];
-    s[threadIdx.x] = acc;
-    __syncthreads();
-    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-        if (threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        double rms = sqrt(s[0] / A.nCells);
+    __shared__ double tot;
+    if (grid_sum_last<1>(A.tpart, nPartial, A.red, A.redCount, &tot) && threadIdx.x == 0) {
+        double rms = sqrt(tot / A.nCells);
         A.scal[S_TNORM] = rms;
-        int n = int(A.scal[S_THISTN]);
-        if (n < cap) hist[n] = rms;
-        A.scal[S_THISTN] = double(n + 1);
+        if (hist) {   // one more entry of the SA residual history
+            int n = int(A.scal[S_THISTN]);
+            if (n < cap) hist[n] = rms;
+            A.scal[S_THISTN] = double(n + 1);
+        }
     }
 }
 

@@ -157,9 +157,10 @@ class Solver:
         return dict(zip(names, ms[:n].tolist())), dict(zip(names, nl[:n].tolist()))
 
     def residual_norms(self, tid: int = NS_SOLVER) -> np.ndarray:
-        out = np.empty(5, np.float64)
+        """RMS residual of the solver's last UPDATE_RESIDUALS: 5 values (NS) or 1 (SA)."""
+        out = np.zeros(5, np.float64)
         self._check(self.L.ofg_residual_norms(self.h, tid, out))
-        return out
+        return out if tid == NS_SOLVER else out[:1]
 
     def field(self, name: str, tid: int = NS_SOLVER) -> np.ndarray:
         need = C.c_int64()

@@ -110,3 +110,18 @@ def test_determinism_bitwise():
     b = Solver(mesh, prm); b.init_flowfield(); b.step(20)
     assert np.array_equal(a.state(), b.state())
     assert np.array_equal(a.res_history(), b.res_history())
+
+
+def test_residual_norms_match_the_residual_field_and_leave_the_history():
+    mesh = meshgen.bump_channel(32, 16)
+    prm = P.euler_bump(ilim=2, vencat_coef=0.05)
+    g = Solver(mesh, prm); g.init_flowfield(); g.step(5)
+    h0 = g.res_history().copy()
+    N = mesh.n_cells
+    for t in LUSGS_SEQUENCE[:4]:   # up to UPDATE_RESIDUALS
+        g.task(t)
+    res = g.field("res").reshape(5, -1)[:, :N]
+    want = np.sqrt((res * res).mean(axis=1))
+    got = g.residual_norms()
+    assert np.allclose(got, want, rtol=1e-12, atol=0)
+    assert np.array_equal(g.res_history(), h0)

@@ -66,3 +66,12 @@ def test_sa_mixed_precision_tracks_fp64():
     b = Solver(mesh, prm32); b.init_flowfield(); b.step(30)
     assert rel(b.state(), a.state()) < 1e-4
     assert rel(b.state(TURB_SOLVER), a.state(TURB_SOLVER)) < 1e-2
+
+
+def test_sa_residual_norm_matches_the_residual_field():
+    m, prm = sa_case()
+    g = Solver(m, prm); g.init_flowfield(); g.step(3)
+    g.task("UPDATE_RESIDUALS", TURB_SOLVER)
+    N = m.n_cells
+    r = g.field("turbres", TURB_SOLVER)[:N]
+    assert np.allclose(g.residual_norms(TURB_SOLVER), [np.sqrt((r * r).mean())], rtol=1e-12, atol=0)
