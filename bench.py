@@ -88,6 +88,22 @@ def _ref_procs(mesh) -> int:
     return max(1, min(n, 64))
 
 
+KERNEL_OF_GROUP = {"gradlim": "k_gradlim", "residual": "k_residual<float,0> (flux + time-step gather)",
+                   "clip": "k_timestep_clip", "lusgs_lower": "k_lusgs_lower", "lusgs_upper": "k_lusgs_upper",
+                   "update": "k_update", "sa_residual": "k_turb_rhs", "sa_grad": "k_turb_grad"}
+
+# DRAM bytes (read + write) per cell of one step's launches of a profile
+# group, from `ncu --section MemoryWorkloadAnalysis` of the 600,000-cell plate
+# sample (plate3d_sample: same kernels, layout and sweep levels); the kernels
+# stream their arrays once per launch, so the traffic scales with the cell
+# count.  Command and table: profiles/ncu_memory_plate3d_sample.md.
+NCU_TRAFFIC_PER_CELL = {
+    ("plate3d", "residual"): 300.3, ("plate3d", "gradlim"): 200.1, ("plate3d", "clip"): 40.0,
+    ("plate3d", "lusgs_lower"): 478.0, ("plate3d", "lusgs_upper"): 392.0, ("plate3d", "update"): 108.1,
+    ("plate3d", "sa_grad"): 63.9, ("plate3d", "sa_residual"): 399.8,
+}
+
+
 def mesh_stats(mesh: Mesh):
     N, B, F = mesh.n_cells, mesh.n_bfaces, mesh.n_faces
     return dict(N=N, B=B, F=F, E=2 * F - B)
@@ -119,14 +135,20 @@ def alg_bytes(st, prm) -> dict:
     half_lists = FI * 8 + (N + 1) * 4          # lower (or upper) lists: each interior face once
     gl = N * 24 * g
     out = {"cfl": 0}
-    res = 0
+    gradlim = 0
     if need_grad:
-        res += qs + cg + nbl + (0 if lsq else fg) + gl           # k_gradlim
+        # k_gradlim: states + centres of the cell and its neighbours, list,
+        # face records (Green-Gauss weights or the limiter's face centres)
+        gradlim += qs + cg + nbl + fg + gl
         if prm.ilim == 2 and not prm.venkat_kh3:
-            res += N * 10 * g + (gl + N * 10 * g + cg + nbl + fg + N * 5 * g)   # min/max, global eps pass
-    res += qs + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24   # k_residual
-    res += N * 24 + N * g + N * 16                               # time-step clip: dt, radii, vol -> dt, diagonal
-    out["residual"] = res
+            gradlim += N * 10 * g + (gl + N * 10 * g + cg + nbl + fg + N * 5 * g)   # min/max, global eps pass
+    out["gradlim"] = gradlim
+    # k_residual: states, centres, face records, list, gradient records of the
+    # cell and its neighbours, wall states; writes res, dt and the two radii,
+    # and the per-block norm sums
+    out["residual"] = qs + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24 \
+        + ((N + 127) // 128) * 40
+    out["clip"] = N * 24 + N * g + N * 16                        # dt, radii, vol -> dt, diagonal
     dq = N * 8 * g                                               # increment records
     sweep = qs + cg + F * 4 * g + half_lists + dq + dq + N * 8 + N * 4   # neighbour dq, own dq write, diagonal, order
     out["lusgs_lower"] = sweep + N * 40                          # + res
@@ -138,11 +160,14 @@ def alg_bytes(st, prm) -> dict:
         grad_nut = NT * 8 + nbl + cg + (0 if lsq else fg) + N * 4 * g
         rhs = qs + cg + fg + nbl + NT * 8 + N * 4 * g + N * 12 * g + N * 16 + N * 8 + N * 8 + B * 44 \
             + F * 16 + N * 16
-        out["sa_residual"] = B * 24 + grad_nut + rhs
+        out["sa_grad"] = B * 24 + grad_nut
+        out["sa_residual"] = rhs
         sa_sweep = half_lists + FI * 16 + N * 8 + N * 8 + N * 8 + N * 8 + N * 4
         out["sa_lower"] = sa_sweep
         out["sa_upper"] = sa_sweep
-        out["sa_update"] = N * 8 * 3 + N * 24 + N * 8 + (N * g if mixed else 0)
+        # nu~ and its increment read, nu~ written; rho and mu_l read; the
+        # master record's last sector and the FP32 copy rewritten whole
+        out["sa_update"] = N * 24 + N * 8 + N * 32 + N * 32 + (N * 8 * g if mixed else 0)
         out["sa_boundary"] = B * (4 + 4 + 8 * g + 24 + 8 + 16)
         out["sa_norm"] = ((N + 127) // 128) * 8
     return out
@@ -355,24 +380,31 @@ def main():
     hbm = _peak_hbm()
     per_launch_ms = grp_ms[top] / max(grp_n[top], 1)
     achieved = abytes[top] / (grp_ms[top] * 1e-3) / 1e9   # GB/s over the group's launches
-    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm["value"], "unit": "GB/s",
-                "frac": achieved / hbm["value"], "traffic": None, "peak_source": hbm["source"],
+    tpc = NCU_TRAFFIC_PER_CELL.get((args.config, top))
+    traffic = tpc * st["N"] / max(grp_n[top], 1) if tpc else None
+    roofline = {"bound": "hbm", "kernel": KERNEL_OF_GROUP.get(top, top), "group": top, "achieved": achieved,
+                "peak": hbm["value"], "unit": "GB/s", "frac": achieved / hbm["value"], "traffic": traffic,
+                "traffic_source": "ncu dram bytes per cell on the 600k-cell sample, scaled by cells" if tpc else None,
+                "peak_source": hbm["source"],
                 "alg_bytes_per_step": abytes[top], "launches_per_step": grp_n[top],
                 "avg_launch_ms": per_launch_ms,
                 "whole_step_achieved_gbs": working / (total_ms / args.steps * 1e-3) / 1e9,
                 "whole_step_frac": working / (total_ms / args.steps * 1e-3) / 1e9 / hbm["value"],
                 "group_ms": grp_ms, "group_alg_bytes": abytes}
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers: every step uploads the
+    # state q[5][nCells+nBFaces] from pinned host memory (the reference's field
+    # layout), runs one outer iteration and reads the new state back
     e2e_steps = max(3, min(args.steps, 10))
-    q = s.state()
-    h2d = q.nbytes
+    qh = torch.empty((5, s.nT), dtype=torch.float64, pin_memory=True).numpy()
+    s.state(out=qh)
+    h2d = qh.nbytes
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        s.upload_state(q)
+        s.upload_state(qh)
         s.step(1)
-        q = s.state()
+        s.state(out=qh)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_val = st["N"] * e2e_steps * world / e2e_s

@@ -167,11 +167,12 @@ int ofg_download_field(ofg_ctx *ctx, int tid, const char *name, double *out, int
 int ofg_set_stream(ofg_ctx *ctx, void *stream);
 
 /* One outer iteration launched task by task (no graph) with CUDA events
-   between the groups; ms[] receives the device time of: CFL advance,
-   CALC_TIME_STEP + UPDATE_RESIDUALS (one fused gather: gradients, limiter,
-   fluxes, time step), LUSGS_LOWER_SWEEP, LUSGS_UPPER_SWEEP,
-   UPDATE_FLOWFIELD, CALC_BOUNDARY, residual norm, and with the SA model six
-   more (its UPDATE_RESIDUALS, lower, upper, update, boundary, norm);
+   between the groups; ms[] receives the device time of: CFL advance;
+   CALC_TIME_STEP + UPDATE_RESIDUALS as its three kernels (gradients +
+   limiter, flux/time-step gather, time-step clip); LUSGS_LOWER_SWEEP,
+   LUSGS_UPPER_SWEEP, UPDATE_FLOWFIELD, CALC_BOUNDARY, residual norm; and
+   with the SA model seven more (nu~ boundary + gradient, its rhs gather,
+   lower, upper, update, boundary, norm);
    launches[] the number of kernel launches of each group.  Both arrays
    must hold 16 entries. */
 int ofg_profile_step(ofg_ctx *ctx, double *ms, int *launches);

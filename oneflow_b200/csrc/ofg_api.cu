@@ -422,7 +422,7 @@ void ofg_destroy(ofg_ctx *c) {
     void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
                     c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist,
                     c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_rad,
-                    c->d_bcq, c->d_partial, c->d_npart, c->d_tpart, c->d_red, c->d_redCount, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
+                    c->d_bcq, c->d_partial, c->d_npart, c->d_tpart, c->d_red, c->d_redCount, c->d_stage, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
     for (void *v : ptrs) if (v) cudaFree(v);
     cudaStreamDestroy(c->ownStream ? c->ownStream : c->stream);
@@ -528,6 +528,7 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         if (mixed) CK(cudaMalloc(&c->d_qs[i], nT * REC * sizeof(float)));
     }
     size_t rs = mixed ? sizeof(float) : sizeof(double);
+    if (c->d_stage) { cudaFree(c->d_stage); c->d_stage = nullptr; }   // sized by nT: re-made on first use
     if ((rc = upload<double>(c, &c->d_res, nullptr, N * NEQ))) return rc;
     if ((rc = upload_bytes(c, &c->d_dq, nullptr, N * DQR * rs))) return rc;
     if ((rc = upload<double>(c, &c->d_dt, nullptr, N))) return rc;
@@ -611,30 +612,38 @@ int ofg_init_flowfield(ofg_ctx *c) {
     return sync(c);
 }
 
+// staging buffer for state transfers: [5][nT] FP64, allocated on first use
+static int ensure_stage(ofg_ctx *c) {
+    if (c->d_stage) return OFG_OK;
+    CK(cudaMalloc(&c->d_stage, (size_t)NEQ * c->nT * sizeof(double)));
+    return OFG_OK;
+}
+
 int ofg_upload_state(ofg_ctx *c, int tid, const double *q) {
     if (!c || !q) return OFG_E_ARG;
     if (tid != OFG_NS_SOLVER && !(tid == OFG_TURB_SOLVER && has_turb(c)))
         return c->fail(OFG_E_ARG, "no such solver in this context");
     if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
     if (c->pendingNext) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
-    destroy_graphs(c);
+    int rc;
     if (tid == OFG_TURB_SOLVER) {
         if (!c->haveState) return c->fail(OFG_E_STATE, "upload the NS state first");
-        CK(cudaMemcpy(c->d_nut, q, (size_t)c->nT * sizeof(double), cudaMemcpyHostToDevice));
-        int rc = launch(c, T_TURB_BOUNDARY_CUR);
-        if (rc) return rc;
+        CK(cudaMemcpyAsync(c->d_nut, q, (size_t)c->nT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if ((rc = launch(c, T_TURB_BOUNDARY_CUR))) return rc;
         return sync(c);
     }
-    std::vector<double> rec((size_t)c->nT * REC, 0.0);
-    for (int i = 0; i < c->nT; ++i)
-        for (int e = 0; e < NEQ; ++e) rec[(size_t)i * REC + e] = q[(size_t)e * c->nT + i];
-    c->cur = 0;
-    CK(cudaMemcpy(c->d_q[0], rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->d_q[1], rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice));
+    // host [5][nT] -> staging -> the records of the current buffer (the eddy
+    // viscosity, a field of its own in the reference, is kept); then
+    // temperature, laminar viscosity and the ghost states as after a restart
+    if ((rc = ensure_stage(c))) return rc;
+    CK(cudaMemcpyAsync(c->d_stage, q, (size_t)NEQ * c->nT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (!c->haveState) {   // first state: start the records from zero (no eddy viscosity yet)
+        CK(cudaMemsetAsync(c->d_q[c->cur], 0, (size_t)c->nT * REC * sizeof(double), c->stream));
+    }
+    if ((rc = launch(c, T_PACK_STATE))) return rc;
     c->haveState = true;
     c->pendingNext = false;
-    int rc = launch(c, T_BOUNDARY_CUR);
-    if (rc) return rc;
+    if ((rc = launch(c, T_BOUNDARY_CUR))) return rc;
     return sync(c);
 }
 
@@ -642,16 +651,14 @@ int ofg_download_state(ofg_ctx *c, int tid, double *q) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
     if (!q) return c->fail(OFG_E_ARG, "null output");
-    if ((rc = sync(c))) return rc;
     if (tid == OFG_TURB_SOLVER) {
-        CK(cudaMemcpy(q, c->d_nut, (size_t)c->nT * sizeof(double), cudaMemcpyDeviceToHost));
-        return OFG_OK;
+        CK(cudaMemcpyAsync(q, c->d_nut, (size_t)c->nT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        return sync(c);
     }
-    std::vector<double> rec((size_t)c->nT * REC);
-    CK(cudaMemcpy(rec.data(), c->d_q[c->cur], rec.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < c->nT; ++i)
-        for (int e = 0; e < NEQ; ++e) q[(size_t)e * c->nT + i] = rec[(size_t)i * REC + e];
-    return OFG_OK;
+    if ((rc = ensure_stage(c))) return rc;
+    if ((rc = launch(c, T_UNPACK_STATE))) return rc;
+    CK(cudaMemcpyAsync(q, c->d_stage, (size_t)NEQ * c->nT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return sync(c);
 }
 
 int ofg_zero_dq(ofg_ctx *c, int tid) {
@@ -733,8 +740,10 @@ int ofg_calc_boundary(ofg_ctx *c, int tid) {
 }
 
 // tasks of one outer iteration (MG::StrongIter: NS relaxation, then SA), with
-// the state-buffer flip between the two solvers
-// (CALC_TIME_STEP, LOAD_RESIDUALS and UPDATE_RESIDUALS share one gather: T_TS_RES)
+// the state-buffer flip between the two solvers.  CALC_TIME_STEP,
+// LOAD_RESIDUALS and UPDATE_RESIDUALS share one gather (T_TS_RES).
+// (Measured on the 6M-cell plate: fusing UPDATE_FLOWFIELD into the upper
+// sweep's level launches was slower than the separate streaming pass.)
 static const int kNsTasks[] = {T_ADVANCE, T_TS_RES, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_NORM};
 static const int kTurbTasks[] = {T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_NORM};
 
@@ -928,16 +937,22 @@ int ofg_profile_step(ofg_ctx *c, double *ms, int *launches) {
     double sc[2] = {double(c->outerSteps), double(c->outerSteps)};
     CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_scal + S_THISTN, sc, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    // groups: the 7 NS groups (cfl, time step + residual, lower, upper, update,
-    // boundary, norm), then SA rhs, lower, upper, update, boundary, norm
-    const int nns = 7, nt = has_turb(c) ? 6 : 0, n = nns + nt;
-    cudaEvent_t ev[15];
+    // groups: the 9 NS groups (cfl; gradients+limiter, flux/time-step gather,
+    // time-step clip; lower, upper, update, boundary, norm), then the 7 SA
+    // groups (nu~ boundary+gradient, rhs gather, lower, upper, update,
+    // boundary, norm): the kernels of one ofg_step in the same order
+    static const int kNsProf[] = {T_ADVANCE, T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_LOWER, T_UPPER, T_UPDATE,
+                                  T_BOUNDARY_NEXT, T_NORM};
+    static const int kTurbProf[] = {T_P_TURB_GRAD, T_P_TURB_FLUX, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE,
+                                    T_TURB_BOUNDARY, T_TURB_NORM};
+    const int nns = 9, nt = has_turb(c) ? 7 : 0, n = nns + nt;
+    cudaEvent_t ev[17];
     for (int i = 0; i <= n; ++i) CK(cudaEventCreate(&ev[i]));
     CK(cudaEventRecord(ev[0], c->stream));
     for (int i = 0; i < n; ++i) {
         long long before = c->launches;
         if (i == nns) c->cur ^= 1;   // the SA solver reads the relaxed NS state
-        if ((rc = launch(c, i < nns ? kNsTasks[i] : kTurbTasks[i - nns]))) return rc;
+        if ((rc = launch(c, i < nns ? kNsProf[i] : kTurbProf[i - nns]))) return rc;
         if (launches) launches[i] = int(c->launches - before);
         CK(cudaEventRecord(ev[i + 1], c->stream));
     }

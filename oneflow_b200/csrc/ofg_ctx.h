@@ -38,6 +38,7 @@ struct ofg_ctx {
     bool pendingTurb = false;   // SA UPDATE_FLOWFIELD ran, its CALC_BOUNDARY not yet
     double *d_res = nullptr, *d_dt = nullptr, *d_invsr = nullptr, *d_vissr = nullptr, *d_rad = nullptr;
     void *d_dq = nullptr;                                   // [nCells][DQR] at the face precision
+    double *d_stage = nullptr;                              // [5][nT] state transfer staging (on first use)
     double *d_bcq = nullptr, *d_partial = nullptr, *d_scal = nullptr, *d_hist = nullptr;
     double *d_npart = nullptr, *d_tpart = nullptr;          // per-block sums of squares of the residuals
     double *d_red = nullptr;                                // [kRedBlocks][5] block sums of the grid reductions
@@ -70,9 +71,11 @@ namespace ofg {
 // tasks executed by the precision-specific launchers
 enum Task {
     T_CFL = 0, T_TIMESTEP, T_RESIDUAL, T_LOWER, T_UPPER, T_UPDATE, T_BOUNDARY_NEXT, T_BOUNDARY_CUR,
-    T_NORM, T_ADVANCE, T_TS_RES, T_NORM_ONLY,
+    T_NORM, T_ADVANCE, T_TS_RES, T_NORM_ONLY, T_PACK_STATE, T_UNPACK_STATE,
     T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_BOUNDARY_CUR, T_TURB_NORM,
-    T_TURB_NORM_ONLY
+    T_TURB_NORM_ONLY,
+    // parts of T_TS_RES / T_TURB_RHS, timed separately by ofg_profile_step
+    T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_P_TURB_GRAD, T_P_TURB_FLUX
 };
 int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);
 int launch_task_f32(ofg_ctx *c, int task, cudaStream_t s);

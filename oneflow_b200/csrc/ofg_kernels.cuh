@@ -886,6 +886,26 @@ __device__ __forceinline__ void store_state(const KArgs<R> &A, int i, const doub
     }
 }
 
+// state transfer between the reference's field layout q[5][nCells+nBFaces]
+// (staged in device memory) and the records of the current buffer
+template <typename R>
+__global__ void __launch_bounds__(256) k_pack_state(KArgs<R> A, const double *stage) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nT) return;
+    double *o = A.qn + (size_t)i * REC;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) o[e] = stage[(size_t)e * A.nT + i];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_unpack_state(KArgs<R> A, double *stage) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nT) return;
+    const double *o = A.q + (size_t)i * REC;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) stage[(size_t)e * A.nT + i] = o[e];
+}
+
 // NsCalcGamaT(F_INNER) + CalcLaminarViscosity(F_INNER) on the current buffer
 // (after a state upload or the initial field); refreshes the FP32 copy too
 template <typename R>
@@ -903,16 +923,12 @@ __global__ void __launch_bounds__(256) k_interior_tvisl(KArgs<R> A) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_update(KArgs<R> A) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= A.nCells) return;
+__device__ __forceinline__ void update_cell(const KArgs<R> &A, int c, const double *dd) {
     const double *qc = A.q + (size_t)c * REC;
-    R d[DQR];
-    ld8(A.dq + (size_t)c * DQR, d);
     double gama = A.P.gama;
-    double prim0[NEQ], q0[NEQ], qq[NEQ], pr[NEQ], dd[NEQ];
+    double prim0[NEQ], q0[NEQ], qq[NEQ], pr[NEQ];
 #pragma unroll
-    for (int e = 0; e < NEQ; ++e) { prim0[e] = qc[e]; dd[e] = double(d[e]); }
+    for (int e = 0; e < NEQ; ++e) prim0[e] = qc[e];
     primToQ(prim0, gama, q0);
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) qq[e] = q0[e] + dd[e];
@@ -948,6 +964,18 @@ __global__ void __launch_bounds__(256) k_update(KArgs<R> A) {
     }
     rec[IMT] = qc[IMT];
     store_state(A, c, rec);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_update(KArgs<R> A) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.nCells) return;
+    R d[DQR];
+    ld8(A.dq + (size_t)c * DQR, d);
+    double dd[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) dd[e] = double(d[e]);
+    update_cell(A, c, dd);
 }
 
 // UNsUpdate::SolutionFix (codes/uns/src/UNsUpdate.cpp:94-133) for the cells

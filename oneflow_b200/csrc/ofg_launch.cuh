@@ -111,11 +111,14 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         OFG_LAUNCH((k_residual<R, 2>), nblk(N, 128), 128, s, A);
         break;
     }
-    case T_TS_RES: {     // CALC_TIME_STEP + LOAD_RESIDUALS + UPDATE_RESIDUALS in one gather
+    case T_TS_RES:       // CALC_TIME_STEP + LOAD_RESIDUALS + UPDATE_RESIDUALS in one gather
+    case T_P_GRADLIM:    // (its three parts, launched separately by the profiler)
+    case T_P_FLUX:
+    case T_P_CLIP: {
         KArgs<R> A = make_args<R>(c, false);
-        launch_gradlim<R>(c, A, s);
-        OFG_LAUNCH((k_residual<R, 0>), nblk(N, 128), 128, s, A);
-        OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
+        if (task == T_TS_RES || task == T_P_GRADLIM) launch_gradlim<R>(c, A, s);
+        if (task == T_TS_RES || task == T_P_FLUX) OFG_LAUNCH((k_residual<R, 0>), nblk(N, 128), 128, s, A);
+        if (task == T_TS_RES || task == T_P_CLIP) OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }
     case T_LOWER: {
@@ -153,6 +156,16 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         if (c->nBFaces > 0) OFG_LAUNCH(k_boundary<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb);
         break;
     }
+    case T_PACK_STATE: {
+        KArgs<R> A = make_args<R>(c, true);
+        OFG_LAUNCH(k_pack_state<R>, nblk(c->nT, 256), 256, s, A, (const double *)c->d_stage);
+        break;
+    }
+    case T_UNPACK_STATE: {
+        KArgs<R> A = make_args<R>(c, true);
+        OFG_LAUNCH(k_unpack_state<R>, nblk(c->nT, 256), 256, s, A, c->d_stage);
+        break;
+    }
     case T_NORM:         // norms of the last residual, appended to the history
     case T_NORM_ONLY: {  // the same without the history entry
         KArgs<R> A = make_args<R>(c, false);
@@ -160,11 +173,15 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         if (task == T_NORM) OFG_LAUNCH(k_norm_hist, 1, 32, s, c->d_scal, c->d_hist, c->histCap);
         break;
     }
-    case T_TURB_RHS: {
+    case T_TURB_RHS:
+    case T_P_TURB_GRAD:  // (its parts, launched separately by the profiler)
+    case T_P_TURB_FLUX: {
         KArgs<R> A = make_args<R>(c, true);
-        if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb, 0);
-        OFG_LAUNCH(k_turb_grad<R>, nblk(N, 128), 128, s, A);
-        OFG_LAUNCH(k_turb_rhs<R>, nblk(N, 128), 128, s, A);
+        if (task != T_P_TURB_FLUX) {
+            if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb, 0);
+            OFG_LAUNCH(k_turb_grad<R>, nblk(N, 128), 128, s, A);
+        }
+        if (task != T_P_TURB_GRAD) OFG_LAUNCH(k_turb_rhs<R>, nblk(N, 128), 128, s, A);
         break;
     }
     case T_TURB_LOWER: {

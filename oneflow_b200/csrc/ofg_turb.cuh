@@ -392,6 +392,19 @@ __global__ void __launch_bounds__(128) k_turb_lower(KArgs<R> A, const int *order
     A.dnut[c] = (A.resT[c] - rhs0) / A.impsrT[c];
 }
 
+// UPDATE_FLOWFIELD (TurbUpdate::CalcFlowField1Equ, crelax = 1) fused with the
+// interior half of CALC_BOUNDARY (the eddy viscosity of the new nu~)
+template <typename R>
+__device__ __forceinline__ void turb_update_cell(const KArgs<R> &A, int c, double dn, int withVist) {
+    double qOld = A.nut[c], qNew = qOld + dn;
+    double v = (1.0 - 1.0) * qOld + 1.0 * qNew;
+    A.nut[c] = v;
+    if (withVist) {
+        const double *qc = A.q + (size_t)c * REC;
+        put_vist(A, c, sa_vist(A.P, qc[IR], v, qc[IML]));
+    }
+}
+
 template <typename R>
 __global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order, int start, int count) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -406,19 +419,11 @@ __global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order
     A.dnut[c] = add_neg_quot(A.dnut[c], rhs0, A.impsrT[c]);
 }
 
-// UPDATE_FLOWFIELD (TurbUpdate::CalcFlowField1Equ, crelax = 1) fused with the
-// interior half of CALC_BOUNDARY (the eddy viscosity of the new nu~)
 template <typename R>
 __global__ void __launch_bounds__(256) k_turb_update(KArgs<R> A, int withVist) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= A.nCells) return;
-    double qOld = A.nut[c], qNew = qOld + A.dnut[c];
-    double v = (1.0 - 1.0) * qOld + 1.0 * qNew;
-    A.nut[c] = v;
-    if (withVist) {
-        const double *qc = A.q + (size_t)c * REC;
-        put_vist(A, c, sa_vist(A.P, qc[IR], v, qc[IML]));
-    }
+    turb_update_cell(A, c, A.dnut[c], withVist);
 }
 
 // interior eddy viscosity only (CALC_BOUNDARY without an update)

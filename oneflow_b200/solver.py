@@ -121,12 +121,18 @@ class Solver:
     def upload_state(self, q: np.ndarray, tid: int = NS_SOLVER):
         self._check(self.L.ofg_upload_state(self.h, tid, np.ascontiguousarray(q, np.float64).ravel()))
 
-    def state(self, tid: int = NS_SOLVER) -> np.ndarray:
-        """[5][nCells+nBFaces] primitive NS state, or [nCells+nBFaces] nu~ for tid 1."""
+    def state(self, tid: int = NS_SOLVER, out: np.ndarray = None) -> np.ndarray:
+        """[5][nCells+nBFaces] primitive NS state, or [nCells+nBFaces] nu~ for tid 1.
+        ``out``: a C-contiguous float64 array of that size to fill (e.g. a view
+        of pinned host memory, which makes the copy a direct DMA)."""
         ne = 5 if tid == NS_SOLVER else 1
-        out = np.empty(ne * self.nT, np.float64)
-        self._check(self.L.ofg_download_state(self.h, tid, out))
-        return out.reshape(5, self.nT) if ne == 5 else out
+        if out is None:
+            out = np.empty(ne * self.nT, np.float64)
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != ne * self.nT:
+            raise ValueError("out must be a C-contiguous float64 array of the state's size")
+        flat = out.reshape(-1)
+        self._check(self.L.ofg_download_state(self.h, tid, flat))
+        return out.reshape(5, self.nT) if ne == 5 else out.reshape(-1)
 
     # ---- tasks ----
     def task(self, name: str, tid: int = NS_SOLVER):
@@ -143,16 +149,17 @@ class Solver:
         """Launch on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self.L.ofg_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
-    PROFILE_GROUPS = ("cfl", "residual", "lusgs_lower", "lusgs_upper", "update", "boundary", "norm",
-                      "sa_residual", "sa_lower", "sa_upper", "sa_update", "sa_boundary", "sa_norm")
+    PROFILE_GROUPS = ("cfl", "gradlim", "residual", "clip", "lusgs_lower", "lusgs_upper", "update", "boundary",
+                      "norm", "sa_grad", "sa_residual", "sa_lower", "sa_upper", "sa_update", "sa_boundary", "sa_norm")
 
     def profile_step(self):
         """One iteration task by task with CUDA events: ({group: ms}, {group: launches}).
-        "residual" is the fused time step + gradients + limiter + flux gather."""
+        "residual" is the flux + time-step gather kernel alone; "gradlim" the
+        gradient+limiter kernel(s) before it, "clip" the time-step clip after it."""
         ms = np.zeros(16, np.float64)
         nl = np.zeros(16, np.int32)
         self._check(self.L.ofg_profile_step(self.h, ms, nl))
-        n = 13 if self.params.vismodel >= 3 else 7
+        n = 16 if self.params.vismodel >= 3 else 9
         names = self.PROFILE_GROUPS[:n]
         return dict(zip(names, ms[:n].tolist())), dict(zip(names, nl[:n].tolist()))
 
