@@ -466,7 +466,9 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     }
     c->bct.assign(bcType, bcType + nBFaces);
     for (int t : c->bct)
-        if (t < 1 || t > 7) return c->fail(OFG_E_ARG, "unsupported boundary type (interface/overset are multi-zone)");
+        if (t < 1 || t > 6)
+            return c->fail(OFG_E_ARG, "unsupported boundary type (codes 1-6; interface, overset, periodic and pole "
+                                      "faces belong to multi-zone or structured cases)");
     compute_metrics(c, c->p.dimension, X, Y, Z, fOff, fNod);
     for (int i = 0; i < nCells; ++i)
         if (!(c->vol[i] > 0.0)) return c->fail(OFG_E_ARG, "degenerate cell volume");
