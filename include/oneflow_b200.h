@@ -35,6 +35,7 @@ extern "C" {
 #define OFG_E_STATE      -4   /* call out of order (no mesh, no state, ...)  */
 #define OFG_E_TIMEOUT    -5   /* a bounded device wait gave up               */
 #define OFG_E_NOMEM      -6   /* device allocation failed                    */
+#define OFG_E_SIZE       -7   /* request larger than a fixed scratch allows  */
 
 /* solver ids (reference SolverState::tid, codes/solver/src/SolverState.cpp) */
 #define OFG_NS_SOLVER     0
@@ -201,6 +202,37 @@ int ofg_cell_centres(int dimension, int nNodes, const double *xN, const double *
    function; apply it to the mesh arrays before ofg_upload_mesh. */
 int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells,
                      int *perm);
+
+/* ---- allocation-free entry point (no counterpart in the reference: OneFLOW
+   computes its residual norms on the host, ResidualTask::CalcRes) ---- */
+
+#define OFG_NOALLOC_MAX_EQ 8   /* equations per cell the fixed scratch holds */
+
+/* RMS per equation, sqrt(sum_i res[i][e]^2 / n_cells), of a residual array
+   res[n_cells][n_eq] (FP64, row per cell, e.g. the solver's own "res" layout)
+   that the caller keeps in device memory; writes rms_out[n_eq] in device
+   memory, stream-ordered on `stream` (a cudaStream_t, NULL = legacy default
+   stream).  Same quantity as ofg_residual_norms, without a context.
+
+   It allocates nothing: no device or host allocation, no allocating library
+   routine.  It is meant for callers that must not allocate at this point --
+   a host that has given the device memory to its own pool, or a convergence
+   monitor running between the iterations of a solve that cannot take the
+   implicit device synchronisation a cudaMalloc/cudaFree may cause.  Its
+   scratch is a fixed static device array of this library (18,952 bytes per
+   device: 296 blocks x 8 partial sums + a ticket), so:
+     - n_eq above OFG_NOALLOC_MAX_EQ returns OFG_E_SIZE (devices with an
+       ordinal of 64 or more too); n_cells may be any positive count;
+     - the ticket in the scratch must be zero when a call starts: it is zero
+       when the library is loaded and every completed call leaves it zero;
+     - calls that overlap in time on the same device race on the scratch:
+       serialise them (one stream, or an event between streams);
+     - the first call on each device (made with that device current) looks up
+       the scratch address with cudaGetSymbolAddress and loads the module;
+       make that first call before capturing any stream.
+   Returns OFG_OK, OFG_E_ARG (null pointer, n_cells < 1, n_eq < 1), OFG_E_SIZE
+   or OFG_E_CUDA. */
+int ofg_residual_rms_noalloc(const double *res, int64_t n_cells, int n_eq, double *rms_out, void *stream);
 
 #ifdef __cplusplus
 }
