@@ -282,7 +282,7 @@ void build_lists(const ofg_ctx *c, NbLists &L) {
     }
 }
 
-// face records [F][8] (nx ny nz area xfc yfc zfc 0) and cell records [nT][4]
+// face records [F][8] (nx ny nz area xfc yfc zfc dist) and cell records [nT][4]
 // (xcc ycc zcc vol) at the face precision
 template <typename R>
 void pack_geometry(const ofg_ctx *c, std::vector<R> &fg, std::vector<R> &cg) {
@@ -291,6 +291,12 @@ void pack_geometry(const ofg_ctx *c, std::vector<R> &fg, std::vector<R> &cg) {
         R *o = &fg[(size_t)f * 8];
         o[0] = R(c->xfn[f]); o[1] = R(c->yfn[f]); o[2] = R(c->zfn[f]); o[3] = R(c->area[f]);
         o[4] = R(c->xfc[f]); o[5] = R(c->yfc[f]); o[6] = R(c->zfc[f]);
+        // normal distance between the two cell centres, for the LU-SGS viscous
+        // radius (UNsLusgs::CalcViscousTerm): the same value, bit for bit, as
+        // the sweep computes from either side (both signs flip there)
+        int l = c->lc[f], r = c->rc[f];
+        o[7] = R(std::fabs(c->xfn[f] * (c->xcc[r] - c->xcc[l]) + c->yfn[f] * (c->ycc[r] - c->ycc[l]) +
+                           c->zfn[f] * (c->zcc[r] - c->zcc[l])));
     }
     cg.assign((size_t)c->nT * 4, R(0));
     for (int i = 0; i < c->nT; ++i) {

@@ -38,7 +38,7 @@ template <> struct MinBlocks<float> {
 constexpr int kRedBlocks = 148;   // blocks of the grid reductions (one per SM)
 
 constexpr int GLR = 24;   // gradient+limiter record: [var*3+dir] for 6 vars (q, T), limiter at 18..22
-constexpr int FGR = 8;    // face record: nx ny nz area xfc yfc zfc -
+constexpr int FGR = 8;    // face record: nx ny nz area xfc yfc zfc dist (|n . (x_r - x_l)|)
 constexpr int CGR = 4;    // cell record: xcc ycc zcc vol
 constexpr int DQR = 8;    // increment record: dq[5] + 3 zero slots (64 B FP64, 32 B FP32: whole sectors)
 constexpr int MMR = 10;   // neighbour min/max differences per cell (Venkatakrishnan with the zone-wide eps)

@@ -730,10 +730,12 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
 // and the viscous radius (UNsLusgs::CalcViscousTerm :295-330).  Level-scheduled:
 // every cell of a level only reads increments of cells in earlier levels.
 // ---------------------------------------------------------------------------
-// qa: the cell being solved (left after GCom::SetGeometry's swap), qb: neighbour
+// qa: the cell being solved (left after GCom::SetGeometry's swap), qb: neighbour;
+// dist = |n . (x_b - x_a)| (the face record's eighth slot, the same from both
+// sides), volb the neighbour's volume (read only for visSRModel 1)
 template <typename R>
 __device__ __forceinline__ void face_increment(const DevParams &P, const R *qa, const R *qb, const R *dqj, R xn,
-                                               R yn, R zn, R fa, const R *cga, const R *cgb, double *rhs0) {
+                                               R yn, R zn, R fa, R dist, R volb, double *rhs0) {
     R vfn = R(0);
     R half = R(0.5), one = R(1), gl = R(P.gama), gr = gl;
     R rl = qa[IR], ul = qa[IU], vl = qa[IV], wl = qa[IW], pl = qa[IP];
@@ -791,9 +793,8 @@ __device__ __forceinline__ void face_increment(const DevParams &P, const R *qa, 
             R c1 = R(4.0) / R(3.0) * (vl_ + vt_);
             R cc2 = R(P.gama) * (vl_ * R(P.oprl) + vt_ * R(P.oprt));
             R c3 = R(2) * Rmax(c1, cc2) / (R(P.reynolds) * density);
-            visrad = fa * fa * c3 / cgb[3];
+            visrad = fa * fa * c3 / volb;
         } else {
-            R dist = Rabs(xn * (cgb[0] - cga[0]) + yn * (cgb[1] - cga[1]) + zn * (cgb[2] - cga[2]));
             R viscosity = vl_ + vt_;
             R c1 = R(2) * viscosity / (density * dist * R(P.reynolds) + small_v<R>());
             visrad = half * c1 * fa;
@@ -807,22 +808,21 @@ __device__ __forceinline__ void face_increment(const DevParams &P, const R *qa, 
 
 template <typename R>
 __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *off, const int2 *list, double *rhs0) {
-    R qc[REC], cgc[CGR];
+    R qc[REC];
     ld8(A.qs + (size_t)c * REC, qc);
-    ld4(A.cgeo + (size_t)c * CGR, cgc);
     for (int k = off[c]; k < off[c + 1]; ++k) {
         int2 e2 = __ldg(&list[k]);
         int f = nb_face(e2), nb = e2.y;
-        R qn[REC], cgn[CGR], fg[FGR], dqj[DQR];
+        R qn[REC], fg[FGR], dqj[DQR];
         ld8(A.qs + (size_t)nb * REC, qn);
-        ld4(A.cgeo + (size_t)nb * CGR, cgn);
-        ld4(A.fgeo + (size_t)f * FGR, fg);
+        ld8(A.fgeo + (size_t)f * FGR, fg);
         // the neighbour's increment was written by an earlier level's launch
         // and is not written by this one: read-only here
         ld8(A.dq + (size_t)nb * DQR, dqj);
+        R volb = A.P.visSRModel == 1 ? A.cgeo[(size_t)nb * CGR + 3] : R(1);
         R xn = fg[0], yn = fg[1], zn = fg[2];
         if (nb_right(e2)) { xn = -xn; yn = -yn; zn = -zn; }   // GCom::SetGeometry
-        face_increment(A.P, qc, qn, dqj, xn, yn, zn, fg[3], cgc, cgn, rhs0);
+        face_increment(A.P, qc, qn, dqj, xn, yn, zn, fg[3], fg[7], volb, rhs0);
     }
 }
 
