@@ -162,6 +162,17 @@ int ofg_residual_norms(ofg_ctx *ctx, int tid, double *rms);
 int ofg_download_field(ofg_ctx *ctx, int tid, const char *name, double *out, int64_t n_out,
                        int64_t *n_needed);
 
+/* Aerodynamic forces of the current state on the solid-wall faces
+   (AerodynamicForceTask: CalcAeroForce, codes/force/src/AeroForceTask.cpp:186-451,
+   compressible branch; AeroForceInfo::CalcCoef, codes/force/src/Force.cpp:263-281):
+   wall pressure extrapolated with the interior cell's gradient of the last
+   UPDATE_RESIDUALS, viscous stress from its velocity gradient corrected
+   along the cell-to-ghost line.  out[13]: total force x y z, pressure part
+   x y z, viscous part x y z (sums over the wall faces, nondimensional as in
+   the reference), CL, CD, CD_pres, CD_vis with reference area aref.
+   (The reference does not accumulate moments, so none are returned.) */
+int ofg_forces(ofg_ctx *ctx, double aref, double *out);
+
 /* Run every later launch of this context on the caller's CUDA stream
    (a cudaStream_t passed as void*; NULL restores the context's own stream).
    Captured graphs are rebuilt on the next ofg_step. */

@@ -426,7 +426,7 @@ void ofg_destroy(ofg_ctx *c) {
     cudaStreamSynchronize(c->stream);
     destroy_graphs(c);
     void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
-                    c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist,
+                    c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist, c->d_wall, c->d_wallG,
                     c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_rad,
                     c->d_bcq, c->d_partial, c->d_npart, c->d_tpart, c->d_red, c->d_redCount, c->d_stage, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
@@ -517,6 +517,27 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     if ((rc = upload(c, &c->d_upOrder, c->upOrder.data(), nCells))) return rc;
     if ((rc = upload(c, &c->d_key, c->key.data(), c->nT))) return rc;
     if ((rc = upload(c, &c->d_wdist, c->wdist.data(), nCells))) return rc;
+    {
+        // solid-wall faces and their FP64 geometry for the force integration
+        // (the quantities CalcAeroForce forms per face, AeroForceTask.cpp:262-330)
+        std::vector<int> wall;
+        std::vector<double> wg;
+        for (int f = 0; f < nBFaces; ++f) {
+            if (c->bct[f] != OFG_BC_SOLID_SURFACE) continue;
+            int l = c->lc[f], r = c->rc[f];
+            wall.push_back(f); wall.push_back(l);
+            double dx = c->xcc[r] - c->xcc[l], dy = c->ycc[r] - c->ycc[l], dz = c->zcc[r] - c->zcc[l];
+            double ods = 1.0 / std::sqrt(dx * dx + dy * dy + dz * dz);
+            double g[16] = {c->xfn[f] * c->area[f], c->yfn[f] * c->area[f], c->zfn[f] * c->area[f],
+                            c->xfn[f], c->yfn[f], c->zfn[f], c->area[f],
+                            c->xfc[f] - c->xcc[l], c->yfc[f] - c->ycc[l], c->zfc[f] - c->zcc[l],
+                            dx * ods, dy * ods, dz * ods, ods, 0.0, 0.0};
+            wg.insert(wg.end(), g, g + 16);
+        }
+        c->nWall = int(wall.size() / 2);
+        if ((rc = upload(c, &c->d_wall, wall.data(), wall.size()))) return rc;
+        if ((rc = upload(c, &c->d_wallG, wg.data(), wg.size()))) return rc;
+    }
     if (mixed) {
         std::vector<float> fg, cg;
         pack_geometry(c, fg, cg);
@@ -608,6 +629,7 @@ int ofg_init_flowfield(ofg_ctx *c) {
     c->hist.clear();
     c->thist.clear();
     c->haveState = true;
+    c->lastResBuf = -1;
     c->pendingNext = false;
     int rc = launch(c, T_BOUNDARY_CUR);   // NsInitFinal -> NsCalcBoundary
     if (rc) return rc;
@@ -650,6 +672,7 @@ int ofg_upload_state(ofg_ctx *c, int tid, const double *q) {
     }
     if ((rc = launch(c, T_PACK_STATE))) return rc;
     c->haveState = true;
+    c->lastResBuf = -1;
     c->pendingNext = false;
     if ((rc = launch(c, T_BOUNDARY_CUR))) return rc;
     return sync(c);
@@ -699,6 +722,7 @@ int ofg_update_residuals(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;
     if (tid == OFG_TURB_SOLVER && c->pendingNext) return c->fail(OFG_E_STATE, "NS update without CALC_BOUNDARY");
+    if (tid == OFG_NS_SOLVER) c->lastResBuf = c->cur;
     return launch(c, tid == OFG_TURB_SOLVER ? T_TURB_RHS : T_RESIDUAL);
 }
 
@@ -816,6 +840,7 @@ int ofg_step(ofg_ctx *c, int nsteps) {
     for (int it = 0; it < nsteps; ++it) {
         CK(cudaGraphLaunch(c->graph[c->cur], c->stream));
         c->launches += c->graphKernels[c->cur];
+        c->lastResBuf = c->cur;   // this iteration's residual pass read the buffer it started from
         c->cur ^= 1;
         c->outerSteps++;
     }
@@ -833,6 +858,45 @@ int ofg_residual_norms(ofg_ctx *c, int tid, double *rms) {
     if ((rc = sync(c))) return rc;
     CK(cudaMemcpy(rms, c->d_scal + (turb ? S_TNORM : S_NORM), (turb ? 1 : NEQ) * sizeof(double),
                   cudaMemcpyDeviceToHost));
+    return OFG_OK;
+}
+
+int ofg_forces(ofg_ctx *c, double aref, double *out) {
+    int rc = check_tid(c, OFG_NS_SOLVER);
+    if (rc) return rc;
+    if (!out || !(aref > 0.0)) return c->fail(OFG_E_ARG, "null output or non-positive reference area");
+    double f[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (c->nWall > 0) {
+        if (c->p.ilim == -1 && c->p.vismodel == 0) {
+            // first-order inviscid runs keep no gradients, but the reference
+            // computes them in every residual pass and extrapolates the wall
+            // pressure with them: the gradients of the state that pass read
+            // (still in the other buffer), or none before any pass
+            if (c->lastResBuf < 0) {
+                size_t rs = c->p.precision == OFG_PREC_MIXED ? sizeof(float) : sizeof(double);
+                CK(cudaMemsetAsync(c->d_gl, 0, (size_t)c->nCells * GLR * rs, c->stream));
+            } else {
+                int save = c->cur;
+                c->cur = c->lastResBuf;
+                rc = launch(c, T_GRAD_ONLY);
+                c->cur = save;
+                if (rc) return rc;
+            }
+        }
+        if ((rc = launch(c, T_FORCES))) return rc;
+        if ((rc = sync(c))) return rc;
+        CK(cudaMemcpy(f, c->d_scal + S_FORCE, sizeof(f), cudaMemcpyDeviceToHost));
+    }
+    for (int k = 0; k < 9; ++k) out[k] = f[k];
+    // AeroForceInfo::CalcCoef, codes/force/src/Force.cpp:263-281 (AeroCom::CalcCL/CalcCD :142-153)
+    double aoa = c->p.aoa_degree * PI / 180.0, aos = c->p.sideslip_degree * PI / 180.0;
+    double sina = std::sin(aoa), cosa = std::cos(aoa), sinb = std::sin(aos), cosb = std::cos(aos);
+    double cf[3], cpres[3];
+    for (int k = 0; k < 3; ++k) { cf[k] = f[k] / aref; cpres[k] = f[3 + k] / aref; }
+    out[9] = -sina * cf[0] + cosa * cf[1];
+    out[10] = cosa * cosb * cf[0] + sina * cosb * cf[1] + sinb * cf[2];
+    out[11] = cosa * cosb * cpres[0] + sina * cosb * cpres[1] + sinb * cpres[2];
+    out[12] = out[10] - out[11];
     return OFG_OK;
 }
 
@@ -965,6 +1029,7 @@ int ofg_profile_step(ofg_ctx *c, double *ms, int *launches) {
         CK(cudaEventRecord(ev[i + 1], c->stream));
     }
     if (nt == 0) c->cur ^= 1;
+    c->lastResBuf = c->cur ^ 1;
     CK(cudaEventSynchronize(ev[n]));
     for (int i = 0; i < n; ++i) {
         float t = 0.f;

@@ -31,9 +31,13 @@ struct ofg_ctx {
     int *d_lowOrder = nullptr, *d_upOrder = nullptr, *d_key = nullptr;
     void *d_fgeo = nullptr, *d_cgeo = nullptr;              // face / cell records at the face precision
     double *d_wdist = nullptr;
+    int nWall = 0;
+    int *d_wall = nullptr;                                  // solid-wall faces {face, interior cell} (int2)
+    double *d_wallG = nullptr;                              // their FP64 geometry [nWall][16] (k_forces)
     double *d_q[2] = {nullptr, nullptr};
     float *d_qs[2] = {nullptr, nullptr};                    // FP32 copies of the state records (mixed path)
     int cur = 0;
+    int lastResBuf = -1;        // state buffer of the last residual pass (-1: none since the state was set)
     bool pendingNext = false;   // UPDATE_FLOWFIELD wrote d_q[cur^1], CALC_BOUNDARY not yet run
     bool pendingTurb = false;   // SA UPDATE_FLOWFIELD ran, its CALC_BOUNDARY not yet
     double *d_res = nullptr, *d_dt = nullptr, *d_invsr = nullptr, *d_vissr = nullptr, *d_rad = nullptr;
@@ -75,7 +79,8 @@ enum Task {
     T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_BOUNDARY_CUR, T_TURB_NORM,
     T_TURB_NORM_ONLY,
     // parts of T_TS_RES / T_TURB_RHS, timed separately by ofg_profile_step
-    T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_P_TURB_GRAD, T_P_TURB_FLUX
+    T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_P_TURB_GRAD, T_P_TURB_FLUX,
+    T_FORCES, T_GRAD_ONLY
 };
 int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);
 int launch_task_f32(ofg_ctx *c, int task, cudaStream_t s);

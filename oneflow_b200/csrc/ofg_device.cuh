@@ -46,7 +46,7 @@ constexpr int MMR = 10;   // neighbour min/max differences per cell (Venkatakris
 // slots of the small device scalar array (cfl, min dt, limiter eps, norms,
 // outer-step counter, residual-history length)
 enum { S_CFL = 0, S_MINDT = 1, S_EPS = 2 /* 5 slots */, S_NORM = 8 /* 5 slots */, S_STEP = 14, S_HISTN = 15,
-       S_TNORM = 16, S_THISTN = 17, S_NSCAL = 18 };
+       S_TNORM = 16, S_THISTN = 17, S_FORCE = 20 /* 9 slots: total, pressure, viscous force */, S_NSCAL = 29 };
 
 enum BcCode { BC_EXTRAP = 1, BC_SOLID = 2, BC_SYM = 3, BC_FAR = 4, BC_INFLOW = 5, BC_OUTFLOW = 6 };
 

@@ -1135,6 +1135,84 @@ __global__ void __launch_bounds__(256) k_boundary(KArgs<R> A, const int *lcb) {
 // ---------------------------------------------------------------------------
 // Residual norms: ResidualTask::CalcRes + ResAver::CalcAver
 // (codes/residual/src/ResidualTask.cpp:75-126, codes/residual/src/Residual.cpp:52-72).
+// Aerodynamic forces: CalcAeroForce (codes/force/src/AeroForceTask.cpp:186-451,
+// the compressible branch) over the solid-wall faces.  Wall geometry comes in
+// FP64 from the host (wg[w][16]: n*area, n, area, face centre - cell centre,
+// unit cell-to-ghost vector, 1/distance), so both paths integrate with the
+// reference's geometry; the gradients are the last residual pass's records.
+// Sums in a fixed order; out[9] = total, pressure, viscous force.
+template <typename R>
+__global__ void __launch_bounds__(256) k_forces(KArgs<R> A, const int2 *wall, const double *wg, int nWall,
+                                                double *out) {
+    double acc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+    const DevParams &P = A.P;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nWall; w += gridDim.x * blockDim.x) {
+        int f = wall[w].x, l = wall[w].y, r = A.nCells + f;
+        const double *g = wg + (size_t)w * 16;
+        const double *ql = A.q + (size_t)l * REC, *qr = A.q + (size_t)r * REC;
+        const R *gr = A.gl + (size_t)l * GLR;
+        double wp = ql[IP] + double(gr[IP * 3]) * g[7] + double(gr[IP * 3 + 1]) * g[8] + double(gr[IP * 3 + 2]) * g[9];
+        if (wp < 0.0) wp = ql[IP];
+        double cp = 2.0 * (wp - P.inflow[IP]);
+        double fp[3] = {g[0] * cp, g[1] * cp, g[2] * cp};
+        double fv[3] = {0.0, 0.0, 0.0};
+        if (P.vismodel > 0) {
+            double d[3][3];   // [u v w][x y z]
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) d[e][k] = double(gr[(IU + e) * 3 + k]);
+            double dx = g[10], dy = g[11], dz = g[12], ods = g[13];
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {   // CorrectGrad, codes/usolver/src/VisGrad.cpp:355-365
+                double fOld = d[e][0] * dx + d[e][1] * dy + d[e][2] * dz;
+                double fnew = (qr[IU + e] - ql[IU + e]) * ods;
+                double df = fnew - fOld;
+                d[e][0] += df * dx; d[e][1] += df * dy; d[e][2] += df * dz;
+            }
+            double vis = ql[IML];   // Stress::CalcForce, codes/solver/src/Stress.cpp:40-64
+            double divv2p3 = (2.0 / 3.0) * (d[0][0] + d[1][1] + d[2][2]);
+            double txx = vis * (2.0 * d[0][0] - divv2p3);
+            double tyy = vis * (2.0 * d[1][1] - divv2p3);
+            double tzz = vis * (2.0 * d[2][2] - divv2p3);
+            double txy = vis * (d[0][1] + d[1][0]);
+            double txz = vis * (d[0][2] + d[2][0]);
+            double tyz = vis * (d[1][2] + d[2][1]);
+            double coef = -2.0 * g[6] * P.oreynolds;
+            fv[0] = coef * (g[3] * txx + g[4] * txy + g[5] * txz);
+            fv[1] = coef * (g[3] * txy + g[4] * tyy + g[5] * tyz);
+            fv[2] = coef * (g[3] * txz + g[4] * tyz + g[5] * tzz);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            acc[k] += fp[k] + fv[k];
+            acc[3 + k] += fp[k];
+            acc[6 + k] += fv[k];
+        }
+    }
+    // per-thread sums -> one record per thread for the grid reduction
+    __shared__ double tot[9];
+    __shared__ bool last;
+    block_sum_to<9>(acc, tot);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) A.red[(size_t)blockIdx.x * 9 + k] = tot[k];
+        __threadfence();
+        last = atomicAdd(A.redCount, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    for (int k = 0; k < 9; ++k) {
+        double s = 0.0;
+        for (unsigned int b = 0; b < gridDim.x; ++b) s += __ldcg(A.red + (size_t)b * 9 + k);
+        out[k] = s;
+    }
+    *A.redCount = 0u;
+}
+
 // The residual kernel leaves per-block sums of squares; they are added in a
 // fixed order (FP64, deterministic run to run) by a grid of blocks whose last
 // block to finish produces the norms.

@@ -166,6 +166,20 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         OFG_LAUNCH(k_unpack_state<R>, nblk(c->nT, 256), 256, s, A, c->d_stage);
         break;
     }
+    case T_GRAD_ONLY: {   // gradients of the current buffer (no limiter), for a path that keeps none
+        KArgs<R> A = make_args<R>(c, true);
+        OFG_LAUNCH(k_gradlim<R>, nblk(N, 128), 128, s, A, 5, 0);
+        break;
+    }
+    case T_FORCES: {
+        KArgs<R> A = make_args<R>(c, true);
+        if (c->nWall == 0) break;
+        int nb = nblk(c->nWall, 256);
+        if (nb > 64) nb = 64;   // the block sums fit the reduction buffer
+        OFG_LAUNCH(k_forces<R>, nb, 256, s, A, reinterpret_cast<const int2 *>(c->d_wall), (const double *)c->d_wallG,
+                   c->nWall, c->d_scal + S_FORCE);
+        break;
+    }
     case T_NORM:         // norms of the last residual, appended to the history
     case T_NORM_ONLY: {  // the same without the history entry
         KArgs<R> A = make_args<R>(c, false);

@@ -51,6 +51,7 @@ def load_library() -> C.CDLL:
         getattr(L, name).argtypes = [C.c_void_p, C.c_int]
     L.ofg_step.argtypes = [C.c_void_p, C.c_int]
     L.ofg_residual_norms.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ofg_forces.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
     L.ofg_download_field.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
     L.ofg_get_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.ofg_set_outer_step.argtypes = [C.c_void_p, C.c_int64]
@@ -162,6 +163,15 @@ class Solver:
         n = 16 if self.params.vismodel >= 3 else 9
         names = self.PROFILE_GROUPS[:n]
         return dict(zip(names, ms[:n].tolist())), dict(zip(names, nl[:n].tolist()))
+
+    FORCE_NAMES = ("Fx", "Fy", "Fz", "Fpx", "Fpy", "Fpz", "Fvx", "Fvy", "Fvz", "CL", "CD", "CD_pres", "CD_vis")
+
+    def forces(self, aref: float = 1.0) -> np.ndarray:
+        """Aerodynamic forces of the current state on the solid walls (ofg_forces):
+        [13] = total, pressure and viscous force (x y z each), CL, CD, CD_pres, CD_vis."""
+        out = np.zeros(13, np.float64)
+        self._check(self.L.ofg_forces(self.h, C.c_double(aref), out.ctypes.data_as(C.c_void_p)))
+        return out
 
     def residual_norms(self, tid: int = NS_SOLVER) -> np.ndarray:
         """RMS residual of the solver's last UPDATE_RESIDUALS: 5 values (NS) or 1 (SA)."""

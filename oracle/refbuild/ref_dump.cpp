@@ -12,6 +12,8 @@
 #include "CellMesh.h"
 #include "DataBase.h"
 #include "HXArray.h"
+#include "Force.h"
+#include "AeroForceTask.h"
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -46,6 +48,22 @@ void OfgRefDump()
     MRField distField(1, nTCell);
     for (int i = 0; i < nCells && i < (int)dist.size(); ++i) distField[0][i] = dist[i];
     if (turb) fields.push_back({"walldist", &distField});
+    // the aerodynamic forces of the final state, by the reference's own
+    // routines (AerodynamicForceTask::Run without its 4-digit file dump):
+    // first 13 values of a one-row field "forces": total x y z, pressure
+    // x y z, viscous x y z, CL, CD, CD_pres, CD_vis
+    MRField forceField(1, nTCell);
+    aeroForceInfo.Init();
+    CalcAeroForce(0);
+    aeroForceInfo.CollectForce();
+    aeroForceInfo.CalcCoef();
+    {
+        AeroForce &t = aeroForceInfo.totalForce;
+        double v[13] = {t.total.x, t.total.y, t.total.z, t.pres.x, t.pres.y, t.pres.z, t.vis.x, t.vis.y, t.vis.z,
+                        aeroForceInfo.cl, aeroForceInfo.cd, aeroForceInfo.cd_pres, aeroForceInfo.cd_vis};
+        for (int k = 0; k < 13 && k < nTCell; ++k) forceField[0][k] = v[k];
+    }
+    fields.push_back({"forces", &forceField});
     int nf = (int)fields.size();
     std::fwrite(&nCells, 4, 1, fp);
     std::fwrite(&nTCell, 4, 1, fp);

@@ -1388,6 +1388,72 @@ struct Oracle {
         }
         return 0;
     }
+
+    // ======================= aerodynamic forces =======================
+    // CalcAeroForce (codes/force/src/AeroForceTask.cpp:186-451, the
+    // compressible branch): over the solid-wall faces, in face order, the
+    // pressure force (wall pressure extrapolated with the interior cell's
+    // gradient, cp = 2 (p_w - p_inf)) and, with a viscous model, the viscous
+    // force from the interior cell's velocity gradient corrected along the
+    // cell-to-ghost line (CorrectGrad, codes/usolver/src/VisGrad.cpp:355-365)
+    // and the stress of Stress::CalcForce (codes/solver/src/Stress.cpp:40-64)
+    // with the interior laminar viscosity.  Sums as AeroForce::AddForce
+    // (codes/force/src/Force.cpp:215-221), coefficients as
+    // AeroForceInfo::CalcCoef (:263-281).  out[13]: total force x y z,
+    // pressure part x y z, viscous part x y z, CL, CD, CD_pres, CD_vis.
+    void forces(double aref, double *out) {
+        double tot[3] = {0, 0, 0}, pr[3] = {0, 0, 0}, vs[3] = {0, 0, 0};
+        for (int f = 0; f < nBFaces; ++f) {
+            if (bcType[f] != OFG_BC_SOLID_SURFACE) continue;
+            int l = lc[f], r = rc[f];
+            double fanx = xfn[f] * area[f], fany = yfn[f] * area[f], fanz = zfn[f] * area[f];
+            double dx = xfc[f] - xcc[l], dy = yfc[f] - ycc[l], dz = zfc[f] - zcc[l];
+            double wp = q[IP][l] + dqdx[IP][l] * dx + dqdy[IP][l] * dy + dqdz[IP][l] * dz;
+            if (wp < 0.0) wp = q[IP][l];
+            double cp = 2.0 * (wp - inflow[IP]);
+            double fp[3] = {fanx * cp, fany * cp, fanz * cp};
+            double fv[3] = {0.0, 0.0, 0.0};
+            if (p.vismodel > 0) {
+                double g[3][3];   // [u v w][x y z]
+                for (int e = 0; e < 3; ++e) { g[e][0] = dqdx[IU + e][l]; g[e][1] = dqdy[IU + e][l]; g[e][2] = dqdz[IU + e][l]; }
+                dx = xcc[r] - xcc[l]; dy = ycc[r] - ycc[l]; dz = zcc[r] - zcc[l];
+                double ods = 1.0 / DIST3(dx, dy, dz);
+                dx *= ods; dy *= ods; dz *= ods;
+                for (int e = 0; e < 3; ++e) {
+                    double fOld = g[e][0] * dx + g[e][1] * dy + g[e][2] * dz;
+                    double fnew = (q[IU + e][r] - q[IU + e][l]) * ods;
+                    double df = fnew - fOld;
+                    g[e][0] += df * dx; g[e][1] += df * dy; g[e][2] += df * dz;
+                }
+                double vis = visl[l];
+                double divv2p3 = two3rd * (g[0][0] + g[1][1] + g[2][2]);
+                double txx = vis * (2.0 * g[0][0] - divv2p3);
+                double tyy = vis * (2.0 * g[1][1] - divv2p3);
+                double tzz = vis * (2.0 * g[2][2] - divv2p3);
+                double txy = vis * (g[0][1] + g[1][0]);
+                double txz = vis * (g[0][2] + g[2][0]);
+                double tyz = vis * (g[1][2] + g[2][1]);
+                double coef = -2.0 * area[f] * oreynolds;
+                fv[0] = coef * (xfn[f] * txx + yfn[f] * txy + zfn[f] * txz);
+                fv[1] = coef * (xfn[f] * txy + yfn[f] * tyy + zfn[f] * tyz);
+                fv[2] = coef * (xfn[f] * txz + yfn[f] * tyz + zfn[f] * tzz);
+            }
+            for (int k = 0; k < 3; ++k) {
+                tot[k] += fp[k] + fv[k];
+                pr[k] += fp[k];
+                vs[k] += fv[k];
+            }
+        }
+        for (int k = 0; k < 3; ++k) { out[k] = tot[k]; out[3 + k] = pr[k]; out[6 + k] = vs[k]; }
+        double aoa = p.aoa_degree * PI / 180.0, aos = p.sideslip_degree * PI / 180.0;
+        double sina = std::sin(aoa), cosa = std::cos(aoa), sinb = std::sin(aos), cosb = std::cos(aos);
+        double cf[3], cpres[3];
+        for (int k = 0; k < 3; ++k) { cf[k] = tot[k] / aref; cpres[k] = pr[k] / aref; }
+        out[9] = -sina * cf[0] + cosa * cf[1];
+        out[10] = cosa * cosb * cf[0] + sina * cosb * cf[1] + sinb * cf[2];
+        out[11] = cosa * cosb * cpres[0] + sina * cosb * cpres[1] + sinb * cpres[2];
+        out[12] = out[10] - out[11];
+    }
 };
 
 // ============================ C interface ============================
@@ -1486,5 +1552,10 @@ int oro_set_q(void *h, const double *qin) {
     return 0;
 }
 long oro_outer_steps(void *h) { return ((Oracle *)h)->outerSteps; }
+int oro_forces(void *h, double aref, double *out) {
+    if (!h || !out || !(aref > 0.0)) return OFG_E_ARG;
+    ((Oracle *)h)->forces(aref, out);
+    return 0;
+}
 
 }  // extern "C"

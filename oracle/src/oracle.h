@@ -15,6 +15,7 @@ int oro_task(void *h, const char *name);
 int64_t oro_field(void *h, const char *name, double *out);
 int oro_set_q(void *h, const double *qin);
 long oro_outer_steps(void *h);
+int oro_forces(void *h, double aref, double *out);   /* out[13], see Oracle::forces */
 #ifdef __cplusplus
 }
 #endif

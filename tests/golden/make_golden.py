@@ -5,8 +5,9 @@ seeded meshes, with the full-precision dump hook of oracle/refbuild.
     python tests/golden/make_golden.py
 
 Each fixture <case>.npz holds the case parameters, the final primitive state
-q [5][nCells+nBFaces], nu~ for SA cases, and the residual history the
-reference printed (res.dat / turbres.dat rows).  The meshes are regenerated
+q [5][nCells+nBFaces], nu~ for SA cases, the aerodynamic forces of the final
+state (total, pressure, viscous x y z, CL, CD, CD_pres, CD_vis) and the
+residual history the reference printed (res.dat / turbres.dat rows).  The meshes are regenerated
 from their seeds by the tests, so only the outputs are stored."""
 import json
 import os
@@ -31,6 +32,8 @@ def main():
         out = {"q": dump["q"], "reshist": rows[:, 2:7], "params": json.dumps(P.to_dict(prm)), "steps": steps}
         if "turbq" in dump:
             out["turbq"] = dump["turbq"][0]
+        if "forces" in dump:   # the reference's own force routine, full precision
+            out["forces"] = dump["forces"].ravel()[:13]
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print(name, mesh.n_cells, "cells", steps, "steps")
 

@@ -39,6 +39,7 @@ def _load():
     lib.oro_set_q.argtypes = [C.c_void_p, _dp]
     lib.oro_outer_steps.argtypes = [C.c_void_p]
     lib.oro_outer_steps.restype = C.c_long
+    lib.oro_forces.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
     return lib
 
 
@@ -99,6 +100,12 @@ class Oracle:
 
     def set_q(self, q):
         self.L.oro_set_q(self.h, np.ascontiguousarray(q, np.float64).ravel())
+
+    def forces(self, aref=1.0):
+        """[13]: total, pressure and viscous force (x y z each), CL, CD, CD_pres, CD_vis."""
+        out = np.zeros(13, np.float64)
+        assert self.L.oro_forces(self.h, aref, out.ctypes.data_as(C.c_void_p)) == 0
+        return out
 
 
 def ref_available() -> bool:
