@@ -3,7 +3,10 @@
 // with the same operation order as the reference's serial code, so that the
 // FP64 build (compiled without FMA contraction) rounds like the reference.
 // The arithmetic type R is double (FP64 path) or float (mixed path: face
-// terms in FP32, accumulation in FP64 by the callers).
+// terms in FP32, accumulation in FP64 by the callers; the face states, the
+// central part of the Roe flux and the gradient differences are formed in FP64
+// from the FP64 state records, so that the FP32 rounding of the large
+// low-Mach pressure and enthalpy terms sets no floor under the residual).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -19,10 +22,10 @@ enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4, ITT = 5, IML = 6, IMT = 7 };
 // timing the 6M-cell plate (no spills at these caps).  The FP64 kernels keep
 // the compiler's choice.
 #ifndef OFG_MINB_RES
-#define OFG_MINB_RES 4
+#define OFG_MINB_RES 3
 #endif
 #ifndef OFG_MINB_GL
-#define OFG_MINB_GL 8
+#define OFG_MINB_GL 6
 #endif
 #ifndef OFG_MINB_SW
 #define OFG_MINB_SW 8
@@ -148,6 +151,75 @@ __device__ __forceinline__ void roeFlux(const R *p1, const R *p2, R xn, R yn, R 
     flux[4] -= (meig1 * dqv[4] - hm * term1 + vnflow * term2);
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) flux[e] *= half;
+}
+
+// The same Roe flux for the FP32-face path, split by magnitude.  The central
+// part fc = F(qL) + F(qR) and the jump qR - qL of the conservative variables
+// are formed in FP64 from the FP64 face states p1/p2: at low Mach numbers they
+// carry the large pressure and enthalpy terms (p ~ 1/(gamma M^2)), whose FP32
+// rounding would set the floor of the converged residual.  The Roe averages,
+// eigenvalues and the dissipation d = |A| (qR - qL), a small correction near
+// convergence, are FP32, from the FP32 copies f1/f2 of the same states.  The
+// face flux is (fc - d) / 2.  og1 = 1/(gamma-1); the FP64 part has no division.
+__device__ __forceinline__ void roeFluxMixed(const double *p1, const double *p2, const float *f1, const float *f2,
+                                             float xnf, float ynf, float znf, float gam, double og1, int ieigenfix,
+                                             float ce1, float ce2, double *fc, float *d) {
+    const double xn = xnf, yn = ynf, zn = znf;
+    double rl = p1[IR], ul = p1[IU], vl = p1[IV], wl = p1[IW], pl = p1[IP];
+    double rr = p2[IR], ur = p2[IU], vr = p2[IV], wr = p2[IW], pr = p2[IP];
+    double el = pl * og1 + 0.5 * rl * SQR3(ul, vl, wl);   // total energy per volume
+    double er = pr * og1 + 0.5 * rr * SQR3(ur, vr, wr);
+    double vnl = xn * ul + yn * vl + zn * wl, vnr = xn * ur + yn * vr + zn * wr;
+    double rvnl = rl * vnl, rvnr = rr * vnr;
+    fc[0] = rvnl + rvnr;
+    fc[1] = (rvnl * ul + xn * pl) + (rvnr * ur + xn * pr);
+    fc[2] = (rvnl * vl + yn * pl) + (rvnr * vr + yn * pr);
+    fc[3] = (rvnl * wl + zn * pl) + (rvnr * wr + zn * pr);
+    fc[4] = vnl * (el + pl) + vnr * (er + pr);
+    float dqv[NEQ];
+    dqv[0] = float(rr - rl);
+    dqv[1] = float(rr * ur - rl * ul);
+    dqv[2] = float(rr * vr - rl * vl);
+    dqv[3] = float(rr * wr - rl * wl);
+    dqv[4] = float(er - el);
+    const float half = 0.5f, one = 1.0f, two = 2.0f;
+    float rlf = f1[IR], rrf = f2[IR];
+    float gg1 = gam / (gam - one);
+    float hl = gg1 * (f1[IP] / rlf) + half * SQR3(f1[IU], f1[IV], f1[IW]);
+    float hr = gg1 * (f2[IP] / rrf) + half * SQR3(f2[IU], f2[IV], f2[IW]);
+    float ratio = sqrtf(rrf / rlf);
+    float coef = one / (one + ratio);
+    float um = (f1[IU] + f2[IU] * ratio) * coef;
+    float vm = (f1[IV] + f2[IV] * ratio) * coef;
+    float wm = (f1[IW] + f2[IW] * ratio) * coef;
+    float hm = (hl + hr * ratio) * coef;
+    float gama = (gam + gam * ratio) * coef;
+    float v2 = SQR3(um, vm, wm);
+    float vnflow = xnf * um + ynf * vm + znf * wm;
+    float gamm1 = gama - one;
+    float c2 = gamm1 * (hm - half * v2);
+    float cm = sqrtf(fabsf(c2));
+    float aeig1 = fabsf(vnflow), aeig2 = fabsf(vnflow + cm), aeig3 = fabsf(vnflow - cm);
+    float meig1 = aeig1, meig2 = aeig2, meig3 = aeig3;
+    if (ieigenfix == 1) {
+        float mx = fmaxf(aeig2, aeig3);
+        float m1 = mx * ce1, m2 = mx * ce2;
+        meig1 = fmaxf(m1, aeig1); meig2 = fmaxf(m2, aeig2); meig3 = fmaxf(m2, aeig3);
+    }
+    float xi1 = (two * meig1 - meig2 - meig3) / (two * c2);
+    float xi2 = (meig2 - meig3) / (two * cm);
+    float dc = vnflow * dqv[0] - xnf * dqv[1] - ynf * dqv[2] - znf * dqv[3];
+    float c2dc = c2 * dc;
+    float ae = gama - one, af = half * ae * v2;
+    float dh = -ae * (um * dqv[1] + vm * dqv[2] + wm * dqv[3] - dqv[4]);
+    dh += af * dqv[0];
+    float term1 = dh * xi1 + dc * xi2;
+    float term2 = c2dc * xi1 + dh * xi2;
+    d[0] = meig1 * dqv[0] - term1;
+    d[1] = meig1 * dqv[1] - um * term1 + xnf * term2;
+    d[2] = meig1 * dqv[2] - vm * term1 + ynf * term2;
+    d[3] = meig1 * dqv[3] - wm * term1 + znf * term2;
+    d[4] = meig1 * dqv[4] - hm * term1 + vnflow * term2;
 }
 
 template <typename R>

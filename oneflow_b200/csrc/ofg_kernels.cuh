@@ -287,15 +287,19 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     bool active = c < A.nCells;
     R mn[NEQ], mx[NEQ];
+    // The FP32 path forms every neighbour difference in FP64 from the FP64
+    // records (a difference of two FP32-rounded pressures would carry the
+    // rounding of p itself) and sums differences, not values, over the faces.
+    constexpr bool mixed = sizeof(R) == 4;
     if (active) {
         R qc[REC], cgc[CGR];
-        ld8(A.qs + (size_t)c * REC, qc);
+        if constexpr (!mixed) ld8(A.qs + (size_t)c * REC, qc);
         ld4(A.cgeo + (size_t)c * CGR, cgc);
         R gx[6], gy[6], gz[6];
 #pragma unroll
         for (int v = 0; v < 6; ++v) gx[v] = gy[v] = gz[v] = R(0);
 #pragma unroll
-        for (int e = 0; e < NEQ; ++e) mn[e] = mx[e] = qc[e];
+        for (int e = 0; e < NEQ; ++e) mn[e] = mx[e] = mixed ? R(0) : qc[e];
         int b = A.nb_off[c], en = A.nb_off[c + 1];
         if (A.P.igrad == 2) {
             // weighted least squares over face neighbours (ghosts included), w = 1/|d|^2
@@ -305,8 +309,18 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
             for (int k = b; k < en; ++k) {
                 int2 e2 = __ldg(&A.nbl[k]);
                 int nb = e2.y;
-                R qn[REC], cgn[CGR];
-                ld8(A.qs + (size_t)nb * REC, qn);
+                R qn[REC], cgn[CGR], dn[6];
+                if constexpr (mixed) {
+                    double t[REC];
+                    ld8(A.q + (size_t)nb * REC, t);
+#pragma unroll
+                    for (int v = 0; v < 6; ++v)   // the cell's own values re-read (L1 hits), not held
+                        dn[v] = R(t[v < 5 ? v : ITT] - __ldg(A.q + (size_t)c * REC + (v < 5 ? v : ITT)));
+                } else {
+                    ld8(A.qs + (size_t)nb * REC, qn);
+#pragma unroll
+                    for (int v = 0; v < 6; ++v) dn[v] = qn[v < 5 ? v : ITT] - qc[v < 5 ? v : ITT];
+                }
                 ld4(A.cgeo + (size_t)nb * CGR, cgn);
                 R dx = cgn[0] - cgc[0], dy = cgn[1] - cgc[1], dz = cgn[2] - cgc[2];
                 R w = R(1) / (dx * dx + dy * dy + dz * dz);
@@ -315,13 +329,15 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
 #pragma unroll
                 for (int v = 0; v < 6; ++v) {
                     if (v >= nvar) break;
-                    int iv = v < 5 ? v : ITT;
-                    R dv = qn[iv] - qc[iv];
+                    R dv = dn[v];
                     bb[v][0] += w * dx * dv; bb[v][1] += w * dy * dv; bb[v][2] += w * dz * dv;
                 }
                 if (nb < A.nCells) {
 #pragma unroll
-                    for (int e = 0; e < NEQ; ++e) { mn[e] = Rmin(mn[e], qn[e]); mx[e] = Rmax(mx[e], qn[e]); }
+                    for (int e = 0; e < NEQ; ++e) {
+                        R m = mixed ? dn[e] : qn[e];
+                        mn[e] = Rmin(mn[e], m); mx[e] = Rmax(mx[e], m);
+                    }
                 }
             }
             if (A.P.dim == 2) {
@@ -348,8 +364,16 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
                 int2 e2 = __ldg(&A.nbl[k]);
                 int f = nb_face(e2), nb = e2.y;
                 bool right = nb_right(e2);
-                R qn[REC], cgn[CGR], fg[FGR];
-                ld8(A.qs + (size_t)nb * REC, qn);
+                R qn[REC], cgn[CGR], fg[FGR], dn[6];
+                if constexpr (mixed) {
+                    double t[REC];
+                    ld8(A.q + (size_t)nb * REC, t);
+#pragma unroll
+                    for (int v = 0; v < 6; ++v)   // the cell's own values re-read (L1 hits), not held
+                        dn[v] = R(t[v < 5 ? v : ITT] - __ldg(A.q + (size_t)c * REC + (v < 5 ? v : ITT)));
+                } else {
+                    ld8(A.qs + (size_t)nb * REC, qn);
+                }
                 ld4(A.cgeo + (size_t)nb * CGR, cgn);
                 ld8(A.fgeo + (size_t)f * FGR, fg);
                 const R *ql = right ? qn : qc, *qr = right ? qc : qn;
@@ -366,17 +390,25 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
                 }
                 R ar = fg[3];
                 R fnxa = fg[0] * ar, fnya = fg[1] * ar, fnza = fg[2] * ar;
+                // FP32 path: face value minus the cell value (the cell's own
+                // term sums to zero over the closed cell surface)
+                R wn = right ? cl : cr;
 #pragma unroll
                 for (int v = 0; v < 6; ++v) {
                     if (v >= nvar) break;
                     int iv = v < 5 ? v : ITT;
-                    R value = (A.P.igrad == 1) ? R(0.5) * (ql[iv] + qr[iv]) : cl * ql[iv] + cr * qr[iv];
+                    R value;
+                    if constexpr (mixed) value = wn * dn[v];
+                    else value = (A.P.igrad == 1) ? R(0.5) * (ql[iv] + qr[iv]) : cl * ql[iv] + cr * qr[iv];
                     if (!right) { gx[v] += fnxa * value; gy[v] += fnya * value; gz[v] += fnza * value; }
                     else        { gx[v] -= fnxa * value; gy[v] -= fnya * value; gz[v] -= fnza * value; }
                 }
                 if (nb < A.nCells) {
 #pragma unroll
-                    for (int e = 0; e < NEQ; ++e) { mn[e] = Rmin(mn[e], qn[e]); mx[e] = Rmax(mx[e], qn[e]); }
+                    for (int e = 0; e < NEQ; ++e) {
+                        R m = mixed ? dn[e] : qn[e];
+                        mn[e] = Rmin(mn[e], m); mx[e] = Rmax(mx[e], m);
+                    }
                 }
             }
             R ovol = R(1) / cgc[3];
@@ -386,8 +418,10 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
         R rec[GLR];
 #pragma unroll
         for (int v = 0; v < 6; ++v) { rec[v * 3] = gx[v]; rec[v * 3 + 1] = gy[v]; rec[v * 3 + 2] = gz[v]; }
+        if constexpr (!mixed) {
 #pragma unroll
-        for (int e = 0; e < NEQ; ++e) { mn[e] -= qc[e]; mx[e] -= qc[e]; }
+            for (int e = 0; e < NEQ; ++e) { mn[e] -= qc[e]; mx[e] -= qc[e]; }
+        }
         R lim[NEQ];
         if (limMode == 1) {
             R eps[NEQ];
@@ -536,12 +570,59 @@ __device__ __forceinline__ void face_states(const KArgs<R> &A, int f, const R *q
         for (int e = 0; e < NEQ; ++e) t2[e] = u2[e];
 }
 
+// The same face states for the FP32-face path, formed in FP64 (t1, t2) from
+// the FP64 cell values (qlD, qrD) plus the FP32 limited gradient corrections,
+// so that they carry no FP32 rounding of the (large) cell values; s1, s2 are
+// their FP32 counterparts from the FP32 copies (qlf, qrf) of the cell values.
+__device__ __forceinline__ void face_states_mixed(const KArgs<float> &A, int f, const double *qlD, const double *qrD,
+                                                  const float *qlf, const float *qrf, const float *fg,
+                                                  const float *cgl, const float *cgr, const float *gll,
+                                                  const float *glr, double *t1, double *t2, float *s1, float *s2) {
+    if (f < A.nBFaces) {
+        if (A.bcType[f] == BC_SOLID) {
+            const double *b = A.bcq + (size_t)f * NEQ;
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) { t1[e] = t2[e] = b[e]; s1[e] = s2[e] = float(b[e]); }
+        } else {
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) {
+                t1[e] = t2[e] = 0.5 * (qlD[e] + qrD[e]);
+                s1[e] = s2[e] = 0.5f * (qlf[e] + qrf[e]);
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) { t1[e] = qlD[e]; t2[e] = qrD[e]; s1[e] = qlf[e]; s2[e] = qrf[e]; }
+    if (A.P.ilim == -1) return;
+    float c1[NEQ], c2[NEQ];
+    float dx = fg[4] - cgl[0], dy = fg[5] - cgl[1], dz = fg[6] - cgl[2];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+        c1[e] = fminf(gll[18 + e], glr[18 + e]) * (gll[e * 3] * dx + gll[e * 3 + 1] * dy + gll[e * 3 + 2] * dz);
+    dx = fg[4] - cgr[0]; dy = fg[5] - cgr[1]; dz = fg[6] - cgr[2];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e)
+        c2[e] = fminf(glr[18 + e], gll[18 + e]) * (glr[e * 3] * dx + glr[e * 3 + 1] * dy + glr[e * 3 + 2] * dz);
+    double r1 = t1[IR] + double(c1[IR]), p1 = t1[IP] + double(c1[IP]);
+    double r2 = t2[IR] + double(c2[IR]), p2 = t2[IP] + double(c2[IP]);
+    if (!(r1 <= 0.0 || p1 <= 0.0)) {
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) { t1[e] += double(c1[e]); s1[e] += c1[e]; }
+    }
+    if (!(r2 <= 0.0 || p2 <= 0.0)) {
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) { t2[e] += double(c2[e]); s2[e] += c2[e]; }
+    }
+}
+
 // viscous face flux with the VIS_STD face gradient, before the -S/Re factor
 // (UNsVisFlux::PrepareFaceValue/StdMethod/CalcStress/CalcNsVisFlux,
 // codes/usolver/src/VisGrad.cpp:150-175,356-366)
+// dlr: qr - ql of the six gradient variables (rho, u, v, w, p, T)
 template <typename R>
-__device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, const R *qr, const R *fg, const R *cgl,
-                                              const R *cgr, const R *gl, const R *gr, R *fv) {
+__device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, const R *qr, const R *dlr, const R *fg,
+                                              const R *cgl, const R *cgr, const R *gl, const R *gr, R *fv) {
     R half = R(0.5);
     R vlm = half * (ql[IML] + qr[IML]), vtm = half * (ql[IMT] + qr[IMT]);
     R vis = vlm + vtm;
@@ -558,7 +639,7 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
         gy[v] = half * (gl[v * 3 + 1] + gr[v * 3 + 1]);
         gz[v] = half * (gl[v * 3 + 2] + gr[v * 3 + 2]);
         R fOld = gx[v] * dx + gy[v] * dy + gz[v] * dz;
-        R fnew = (q2 - q1) * ods;
+        R fnew = dlr[v] * ods;
         R df = fnew - fOld;
         gx[v] += df * dx; gy[v] += df * dy; gz[v] += df * dz;
     }
@@ -582,6 +663,18 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
     fv[4] = qm[IU] * fv[1] + qm[IV] * fv[2] + qm[IW] * fv[3] + qNormal;
 }
 
+template <typename R>
+__device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, const R *qr, const R *fg, const R *cgl,
+                                              const R *cgr, const R *gl, const R *gr, R *fv) {
+    R dlr[6];
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+        int iv = v < 5 ? v : ITT;
+        dlr[v] = qr[iv] - ql[iv];
+    }
+    face_vis_flux(P, ql, qr, dlr, fg, cgl, cgr, gl, gr, fv);
+}
+
 // One gather pass per cell: face radii + time step, inviscid residual and
 // viscous residual.  The FP64 path adds the viscous face terms after all the
 // inviscid ones, as the reference's two scatter passes do; the FP32 path adds
@@ -599,8 +692,16 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
     if (c < A.nCells) {
         const DevParams &P = A.P;
         R qc[REC], cgc[CGR], glc[GLR];
-        ld8(A.qs + (size_t)c * REC, qc);
+        if constexpr (exactOrder) {
+            ld8(A.qs + (size_t)c * REC, qc);
+        } else {
+            double t[REC];
+            ld8(A.q + (size_t)c * REC, t);
+#pragma unroll
+            for (int i = 0; i < REC; ++i) qc[i] = R(t[i]);
+        }
         ld4(A.cgeo + (size_t)c * CGR, cgc);
+        const double og1 = 1.0 / (P.gama - 1.0);
         bool needGl = doRes && (P.ilim != -1 || P.vismodel > 0);
         if (needGl) {
 #pragma unroll
@@ -617,7 +718,17 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
             int f = nb_face(e2), nb = e2.y;
             bool right = nb_right(e2);
             R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
-            ld8(A.qs + (size_t)nb * REC, qn);
+            double qnD[NEQ];
+            if constexpr (exactOrder) {
+                ld8(A.qs + (size_t)nb * REC, qn);
+            } else {
+                double t[REC];
+                ld8(A.q + (size_t)nb * REC, t);
+#pragma unroll
+                for (int i = 0; i < REC; ++i) qn[i] = R(t[i]);
+#pragma unroll
+                for (int e = 0; e < NEQ; ++e) qnD[e] = t[e];
+            }
             ld8(A.fgeo + (size_t)f * FGR, fg);
             ld4(A.cgeo + (size_t)nb * CGR, cgn);
             bool ghost = nb >= A.nCells;
@@ -634,28 +745,58 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
                 if (P.vismodel > 0) vis += face_vis_spec(P, ql, qr, fg, cgl, cgr);
             }
             if (!doRes) continue;
+            if constexpr (!exactOrder) {
+                // FP32 path: FP64 face states and central flux; the FP32
+                // dissipation and viscous term join before the FP64 accumulation
+                double qcD[NEQ];   // re-read per face (an L1 hit) rather than held in registers
+                ld4(A.q + (size_t)c * REC, qcD);
+                qcD[IP] = __ldg(A.q + (size_t)c * REC + IP);
+                const double *qlD = right ? qnD : qcD, *qrD = right ? qcD : qnD;
+                R fvs[NEQ];   // viscous term, formed first while fewer values are live
+                if (P.vismodel > 0) {
+                    R fv[NEQ];
+                    face_vis_flux(P, ql, qr, fg, cgl, cgr, gll, glr, fv);
+                    R coeff = -orey * fg[3];
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) fvs[e] = coeff * fv[e];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) fvs[e] = R(0);
+                }
+                double t1[NEQ], t2[NEQ];
+                R s1[NEQ], s2[NEQ];
+                face_states_mixed(A, f, qlD, qrD, ql, qr, fg, cgl, cgr, gll, glr, t1, t2, s1, s2);
+                if (P.ischeme == 12) {
+                    R fs[NEQ];
+                    slau2Flux(s1, s2, fg[0], fg[1], fg[2], gam, fs);
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) {
+                        double v = double(fg[3] * fs[e] + fvs[e]);
+                        if (!right) acc[e] -= v; else acc[e] += v;
+                    }
+                } else {
+                    double fc[NEQ];
+                    R d[NEQ];
+                    roeFluxMixed(t1, t2, s1, s2, fg[0], fg[1], fg[2], gam, og1, P.ieigenfix, ce1, ce2, fc, d);
+                    R har = R(0.5) * fg[3];
+                    double hard = double(har);
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) {
+                        double v = hard * fc[e] - double(har * d[e] - fvs[e]);
+                        if (!right) acc[e] -= v; else acc[e] += v;
+                    }
+                }
+                continue;
+            }
             R t1[NEQ], t2[NEQ], fl[NEQ];
             face_states(A, f, ql, qr, fg, cgl, cgr, gll, glr, t1, t2);
             if (P.ischeme == 12) slau2Flux(t1, t2, fg[0], fg[1], fg[2], gam, fl);
             else roeFlux(t1, t2, fg[0], fg[1], fg[2], gam, P.ieigenfix, ce1, ce2, fl);
             R ar = fg[3];
-            if (!exactOrder && P.vismodel > 0) {
-                // FP32 path: the face's viscous term joins its inviscid term
-                // (both exact in FP64) before the FP64 accumulation
-                R fv[NEQ];
-                face_vis_flux(P, ql, qr, fg, cgl, cgr, gll, glr, fv);
-                R coeff = -orey * ar;
 #pragma unroll
-                for (int e = 0; e < NEQ; ++e) {
-                    double v = double(ar * fl[e]) + double(coeff * fv[e]);
-                    if (!right) acc[e] -= v; else acc[e] += v;
-                }
-            } else {
-#pragma unroll
-                for (int e = 0; e < NEQ; ++e) {
-                    double v = double(ar * fl[e]);
-                    if (!right) acc[e] -= v; else acc[e] += v;
-                }
+            for (int e = 0; e < NEQ; ++e) {
+                double v = double(ar * fl[e]);
+                if (!right) acc[e] -= v; else acc[e] += v;
             }
         }
         if (exactOrder && doRes && P.vismodel > 0) {
