@@ -98,9 +98,9 @@ KERNEL_OF_GROUP = {"gradlim": "k_gradlim", "residual": "k_residual<float,0> (flu
 # stream their arrays once per launch, so the traffic scales with the cell
 # count.  Command and table: profiles/ncu_memory_plate3d_sample.md.
 NCU_TRAFFIC_PER_CELL = {
-    ("plate3d", "residual"): 300.3, ("plate3d", "gradlim"): 200.1, ("plate3d", "clip"): 40.0,
-    ("plate3d", "lusgs_lower"): 478.0, ("plate3d", "lusgs_upper"): 392.0, ("plate3d", "update"): 108.1,
-    ("plate3d", "sa_grad"): 63.9, ("plate3d", "sa_residual"): 399.8,
+    ("plate3d", "residual"): 334.7, ("plate3d", "gradlim"): 241.3, ("plate3d", "clip"): 40.0,
+    ("plate3d", "lusgs_lower"): 445.4, ("plate3d", "lusgs_upper"): 356.9, ("plate3d", "update"): 109.7,
+    ("plate3d", "sa_grad"): 63.5, ("plate3d", "sa_residual"): 398.9,
 }
 
 
@@ -114,8 +114,10 @@ def alg_bytes(st, prm) -> dict:
     array a kernel of the group reads or writes counted once per kernel, at its
     stored size, neighbour gathers counted once (perfect reuse).  Data layout of
     the CUDA path (g = 8 B FP64 path, 4 B mixed):
-      state record (rho u v w p T mu_l mu_t): FP64 master 64 B, face kernels read
-        the copy at the face precision (8g B; the master itself on the FP64 path)
+      state record (rho u v w p T mu_l mu_t): FP64 master 64 B, read by the
+        gradient and residual kernels (both paths: the mixed path forms its face
+        states and gradient differences in FP64); the sweeps and the SA kernels
+        read the copy at the face precision (8g B)
       face record 8g B (normal, area, centre), cell record 4g B (centre, volume)
       gradient+limiter record 24g B, neighbour list entry 8 B (face|side, cell)
       residual, dq 40 B; dt, inviscid and viscous radii 8 B each."""
@@ -128,7 +130,8 @@ def alg_bytes(st, prm) -> dict:
     sa = prm.vismodel >= 3
     need_grad = prm.ilim != -1 or vis
     lsq = prm.igrad == 2
-    qs = NT * 8 * g                            # state records read by face kernels
+    qs = NT * 8 * g                            # state records at the face precision
+    qm = NT * 64                               # FP64 master records
     cg = NT * 4 * g
     fg = F * 8 * g
     nbl = E * 8 + (N + 1) * 4
@@ -139,14 +142,14 @@ def alg_bytes(st, prm) -> dict:
     if need_grad:
         # k_gradlim: states + centres of the cell and its neighbours, list,
         # face records (Green-Gauss weights or the limiter's face centres)
-        gradlim += qs + cg + nbl + fg + gl
+        gradlim += qm + cg + nbl + fg + gl
         if prm.ilim == 2 and not prm.venkat_kh3:
             gradlim += N * 10 * g + (gl + N * 10 * g + cg + nbl + fg + N * 5 * g)   # min/max, global eps pass
     out["gradlim"] = gradlim
     # k_residual: states, centres, face records, list, gradient records of the
     # cell and its neighbours, wall states; writes res, dt and the two radii,
     # and the per-block norm sums
-    out["residual"] = qs + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24 \
+    out["residual"] = qm + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24 \
         + ((N + 127) // 128) * 40
     out["clip"] = N * 24 + N * g + N * 16                        # dt, radii, vol -> dt, diagonal
     dq = N * 8 * g                                               # increment records
@@ -274,6 +277,7 @@ def main():
     ap.add_argument("--impl", default="ofg", choices=["ofg", "reference"])
     ap.add_argument("--ordering", default="colour", choices=["natural", "colour"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8-drop runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -416,6 +420,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = _cpu_baseline(mesh, prm, args.config)
+    conv = None
+    if rank == 0 and world == 1 and not args.no_converge:
+        conv = time_to_drop("bump2d_small", 1e-8, stream)
 
     clocks = clk.summary()
     if rank == 0:
@@ -429,7 +436,7 @@ def main():
                                parallelism=f"replicas x{world}"),
                 "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-                "gpu_launches": int(l1 - l0), "clocks": clocks}
+                "gpu_launches": int(l1 - l0), "clocks": clocks, "time_to_1e-8": conv}
         print(json.dumps(line))
     if dist:
         dist.barrier()
@@ -449,6 +456,44 @@ def replica_aggregate(total_ms, cells, steps, world, dist):
         total_ms = float(t.item())
         dist.barrier()
     return total_ms, cells * steps * world / (total_ms * 1e-3)
+
+
+def time_to_drop(config: str, target: float, stream, chunk: int = 200, max_iters: int = 40000):
+    """Device time for the RMS density residual to fall by `target` relative
+    to the first iteration, from a cold (free-stream) start, on the FP64 and
+    the FP32-face paths: steps in chunks of `chunk` iterations (CUDA events
+    around each chunk), the crossing iteration read from the residual history;
+    the time of the last chunk is prorated to that iteration."""
+    import torch
+    from oneflow_b200 import Solver
+    mesh, prm0, desc = make_workload(config)
+    out = {"workload": desc["workload"], "cells": mesh.n_cells, "target_drop": target}
+    for key, prec in (("f64", 0), ("f32_faces", 1)):
+        prm = make_workload(config)[1]
+        prm.precision = prec
+        prm.sweep_order = 1          # colour-major sweeps, as in the throughput runs
+        s = Solver(mesh, prm)
+        s.set_stream(stream.cuda_stream)
+        s.init_flowfield()
+        total, done, hit = 0.0, 0, None
+        while done < max_iters and hit is None:
+            a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+            a.record(stream); s.step(chunk); b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b)
+            h = s.res_history()[:, 0]
+            below = np.nonzero(h[done:done + chunk] / h[0] <= target)[0]
+            if below.size:
+                hit = done + int(below[0]) + 1
+                total += ms * (below[0] + 1) / chunk
+            else:
+                total += ms
+            done += chunk
+        h = s.res_history()[:, 0]
+        out[key] = {"iterations": hit, "seconds": total * 1e-3 if hit else None,
+                    "final_drop": float(h[-1] / h[0]), "iterations_run": done}
+        s.close()
+    return out
 
 
 def _peak_hbm():

@@ -164,7 +164,7 @@ int ofg_download_field(ofg_ctx *ctx, int tid, const char *name, double *out, int
 
 /* Aerodynamic forces of the current state on the solid-wall faces
    (AerodynamicForceTask: CalcAeroForce, codes/force/src/AeroForceTask.cpp:186-451,
-   compressible branch; AeroForceInfo::CalcCoef, codes/force/src/Force.cpp:263-281):
+   compressible branch; AeroForceInfo::CalcCoef, codes/force/src/Force.cpp:254-269):
    wall pressure extrapolated with the interior cell's gradient of the last
    UPDATE_RESIDUALS, viscous stress from its velocity gradient corrected
    along the cell-to-ghost line.  out[13]: total force x y z, pressure part

@@ -888,7 +888,7 @@ int ofg_forces(ofg_ctx *c, double aref, double *out) {
         CK(cudaMemcpy(f, c->d_scal + S_FORCE, sizeof(f), cudaMemcpyDeviceToHost));
     }
     for (int k = 0; k < 9; ++k) out[k] = f[k];
-    // AeroForceInfo::CalcCoef, codes/force/src/Force.cpp:263-281 (AeroCom::CalcCL/CalcCD :142-153)
+    // AeroForceInfo::CalcCoef, codes/force/src/Force.cpp:254-269 (AeroCom::CalcCL/CalcCD :148-158)
     double aoa = c->p.aoa_degree * PI / 180.0, aos = c->p.sideslip_degree * PI / 180.0;
     double sina = std::sin(aoa), cosa = std::cos(aoa), sinb = std::sin(aos), cosb = std::cos(aos);
     double cf[3], cpres[3];

@@ -1398,8 +1398,8 @@ struct Oracle {
     // cell-to-ghost line (CorrectGrad, codes/usolver/src/VisGrad.cpp:355-365)
     // and the stress of Stress::CalcForce (codes/solver/src/Stress.cpp:40-64)
     // with the interior laminar viscosity.  Sums as AeroForce::AddForce
-    // (codes/force/src/Force.cpp:215-221), coefficients as
-    // AeroForceInfo::CalcCoef (:263-281).  out[13]: total force x y z,
+    // (codes/force/src/Force.cpp:202-208), coefficients as
+    // AeroForceInfo::CalcCoef (:254-269).  out[13]: total force x y z,
     // pressure part x y z, viscous part x y z, CL, CD, CD_pres, CD_vis.
     void forces(double aref, double *out) {
         double tot[3] = {0, 0, 0}, pr[3] = {0, 0, 0}, vs[3] = {0, 0, 0};
