@@ -36,6 +36,7 @@ extern "C" {
 #define OFG_E_TIMEOUT    -5   /* a bounded device wait gave up               */
 #define OFG_E_NOMEM      -6   /* device allocation failed                    */
 #define OFG_E_SIZE       -7   /* request larger than a fixed scratch allows  */
+#define OFG_E_IO         -8   /* file could not be opened, read or written   */
 
 /* solver ids (reference SolverState::tid, codes/solver/src/SolverState.cpp) */
 #define OFG_NS_SOLVER     0
@@ -131,6 +132,30 @@ int ofg_init_flowfield(ofg_ctx *ctx);
    NS: rho,u,v,w,p; nu~ for SA).  Upload runs CALC_BOUNDARY for that solver. */
 int ofg_upload_state(ofg_ctx *ctx, int tid, const double *q);
 int ofg_download_state(ofg_ctx *ctx, int tid, double *q);
+
+/* Restart files in the reference's layout (READ_RESTART / DUMP_RESTART:
+   Restart::Read / Restart::Dump, codes/restart/src/Restart.cpp:144-164, with
+   ReadRestartHeader / DumpRestartHeader :178-182,190-194 and ReadUnsteady /
+   DumpUnsteady :74-120, written per zone by DataBook::WriteFile,
+   codes/database/src/DataBook.cpp:283-316).  One single-zone record:
+     int64 byte count of what follows, int32 outer step, f64 current time,
+     q1[n][nT], q2[n][nT], res1[n][nT], res2[n][nT]   (f64, n = 5 for NS
+     "flowFile", 1 for SA "turbflowFile", nT = nCells + nBFaces)
+   Write: q1 = the current state; q2 = the state one outer iteration earlier
+   (Unsteady::UpdateUnsteady, codes/unsteady/src/Unsteady.cpp:44-58, shifts q1
+   into q2 after every outer step; here the NS solver's other state buffer,
+   or q1 when no iteration has completed since the state was set; always q1
+   for SA, whose update is in place);
+   res1 = res2 = 0 (a steady run never sets them).  The outer step written is
+   the context's counter.
+   Read: the state becomes q1 (as Restart::ReadUnsteady sets q = q1), CALC_BOUNDARY
+   runs as after ofg_upload_state, and for the NS solver the context's outer
+   step counter is set from the file (the CFL ramp continues from it).  The
+   file's step and time are returned through the optional pointers.  A record
+   of another size (another mesh, interface data of a multi-zone grid) is
+   rejected with OFG_E_ARG; file errors return OFG_E_IO. */
+int ofg_write_restart(ofg_ctx *ctx, int tid, const char *path, double curr_time);
+int ofg_read_restart(ofg_ctx *ctx, int tid, const char *path, int64_t *outer_step, double *curr_time);
 
 /* One task each (system/ns/function/funcMap.txt, codes/turb/src/TurbSolverImp.cpp:33-42). */
 int ofg_zero_dq(ofg_ctx *ctx, int tid);             /* ZERO_DQ_FIELD          */

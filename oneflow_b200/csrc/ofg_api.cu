@@ -692,6 +692,88 @@ int ofg_download_state(ofg_ctx *c, int tid, double *q) {
     return sync(c);
 }
 
+// ---------------------------------------------------------------------------
+// Restart files: the single-zone record Restart::Dump writes through
+// DataBook::WriteFile (codes/restart/src/Restart.cpp:155-164,190-194,99-120,
+// codes/database/src/DataBook.cpp:301-316): int64 byte count, int32 outer
+// step, f64 time, then q1, q2, res1, res2 as [n][nT] f64.
+// ---------------------------------------------------------------------------
+static int64_t restart_bytes(const ofg_ctx *c, int n) {
+    return int64_t(sizeof(int32_t) + sizeof(double)) + 4 * int64_t(n) * c->nT * int64_t(sizeof(double));
+}
+
+int ofg_write_restart(ofg_ctx *c, int tid, const char *path, double curr_time) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if (!path) return c->fail(OFG_E_ARG, "null path");
+    if (!c->haveState) return c->fail(OFG_E_STATE, "no state to write");
+    if (c->pendingNext || c->pendingTurb) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
+    if (c->outerSteps > INT32_MAX) return c->fail(OFG_E_ARG, "outer step does not fit the file's int32");
+    const int n = tid == OFG_TURB_SOLVER ? 1 : NEQ;
+    const size_t block = size_t(n) * c->nT;
+    std::vector<double> rec(4 * block, 0.0);   // q1, q2, res1 = res2 = 0
+    if ((rc = ofg_download_state(c, tid, rec.data()))) return rc;
+    // the other NS state buffer holds the state one outer iteration earlier
+    // once an iteration has completed from it
+    if (tid == OFG_NS_SOLVER && c->lastResBuf == (c->cur ^ 1)) {
+        c->cur ^= 1;
+        rc = ofg_download_state(c, tid, rec.data() + block);
+        c->cur ^= 1;
+        if (rc) return rc;
+    } else {
+        std::copy(rec.begin(), rec.begin() + block, rec.begin() + block);
+    }
+    int64_t bytes = restart_bytes(c, n);
+    int32_t step = int32_t(c->outerSteps);
+    std::FILE *f = std::fopen(path, "wb");
+    if (!f) return c->fail(OFG_E_IO, std::string("cannot create ") + path);
+    bool ok = std::fwrite(&bytes, sizeof bytes, 1, f) == 1 && std::fwrite(&step, sizeof step, 1, f) == 1 &&
+              std::fwrite(&curr_time, sizeof curr_time, 1, f) == 1 &&
+              std::fwrite(rec.data(), sizeof(double), rec.size(), f) == rec.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return c->fail(OFG_E_IO, std::string("write failed: ") + path);
+    return OFG_OK;
+}
+
+int ofg_read_restart(ofg_ctx *c, int tid, const char *path, int64_t *outer_step, double *curr_time) {
+    if (!c) return OFG_E_ARG;
+    if (tid != OFG_NS_SOLVER && !(tid == OFG_TURB_SOLVER && has_turb(c)))
+        return c->fail(OFG_E_ARG, "no such solver in this context (tid 1 needs vismodel 3)");
+    if (!path) return c->fail(OFG_E_ARG, "null path");
+    if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
+    if (tid == OFG_TURB_SOLVER && !c->haveState) return c->fail(OFG_E_STATE, "read the NS restart first");
+    int rc;
+    const int n = tid == OFG_TURB_SOLVER ? 1 : NEQ;
+    const size_t block = size_t(n) * c->nT;
+    std::FILE *f = std::fopen(path, "rb");
+    if (!f) return c->fail(OFG_E_IO, std::string("cannot open ") + path);
+    int64_t bytes = 0;
+    int32_t step = 0;
+    double t = 0.0;
+    std::vector<double> q1(block);
+    bool ok = std::fread(&bytes, sizeof bytes, 1, f) == 1;
+    if (ok && bytes != restart_bytes(c, n)) {
+        std::fclose(f);
+        return c->fail(OFG_E_ARG, "restart record of " + std::to_string(bytes) + " bytes; this mesh and solver need " +
+                                      std::to_string(restart_bytes(c, n)) + " (one zone, " + std::to_string(n) +
+                                      " equations, " + std::to_string(c->nT) + " cells with ghosts)");
+    }
+    ok = ok && std::fread(&step, sizeof step, 1, f) == 1 && std::fread(&t, sizeof t, 1, f) == 1 &&
+         std::fread(q1.data(), sizeof(double), block, f) == block;
+    // q2, res1, res2 follow; anything after them is another zone's record
+    long size = -1;
+    if (ok && std::fseek(f, 0, SEEK_END) == 0) size = std::ftell(f);
+    std::fclose(f);
+    if (!ok || size < long(sizeof bytes) + long(bytes))
+        return c->fail(OFG_E_IO, std::string("short or unreadable restart file: ") + path);
+    if (size > long(sizeof bytes) + long(bytes)) return c->fail(OFG_E_ARG, std::string("more than one zone in ") + path);
+    if ((rc = ofg_upload_state(c, tid, q1.data()))) return rc;
+    if (tid == OFG_NS_SOLVER) c->outerSteps = step;
+    if (outer_step) *outer_step = step;
+    if (curr_time) *curr_time = t;
+    return OFG_OK;
+}
+
 int ofg_zero_dq(ofg_ctx *c, int tid) {
     int rc = check_tid(c, tid);
     if (rc) return rc;

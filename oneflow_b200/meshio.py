@@ -125,12 +125,17 @@ def _region_ids(bc_type: np.ndarray) -> np.ndarray:
     return np.array([lut[int(v)] for v in bc_type], np.int32)
 
 
-def write_case(case_dir: str, mesh: Mesh, params: dict, max_steps: int) -> None:
+def write_case(case_dir: str, mesh: Mesh, params: dict, max_steps: int, start_strategy: int = 0,
+               field_save: int = 10 ** 8) -> None:
     """Write a reference project directory (script/, grid/, results/, ...)
-    that runs ``mesh`` with ``params`` for ``max_steps`` outer iterations.
+    that runs ``mesh`` with ``params`` up to outer iteration ``max_steps``.
 
     ``params`` holds the reference's script keys (see ofg_params).  The file
-    set mirrors the reference's regression cases (test/*/script)."""
+    set mirrors the reference's regression cases (test/*/script).
+    ``start_strategy`` 1 starts from restart/flow.dat (and restart/turbflow.dat
+    for SA), which the caller places there (codes/restart/src/RestartTaskReg.cpp:141-163); the
+    reference writes those files whenever the outer step is a multiple of
+    ``field_save`` (nFieldSave, codes/ns/src/NsSolverImp.cpp:154-157)."""
     for sub in ("script", "grid", "results", "restart", "visual", "log"):
         os.makedirs(os.path.join(case_dir, sub), exist_ok=True)
     write_ofl(mesh, os.path.join(case_dir, "grid", "mesh.ofl"))
@@ -154,8 +159,8 @@ def write_case(case_dir: str, mesh: Mesh, params: dict, max_steps: int) -> None:
         "dimension.txt": [("int", "dimension", mesh.dim)],
         "tolerence.txt": [("Real", "ptTol", 1.0e-10)],
         "cfd.txt": [
-            ("int", "startStrategy", 0), ("int", "iexitflag", 0), ("int", "maxSteps", max_steps),
-            ("Real", "maxTime", 0.2), ("int", "nFieldSave", 10 ** 8), ("int", "nForceSave", 1),
+            ("int", "startStrategy", start_strategy), ("int", "iexitflag", 0), ("int", "maxSteps", max_steps),
+            ("Real", "maxTime", 0.2), ("int", "nFieldSave", field_save), ("int", "nForceSave", 1),
             ("int", "nResSave", 1), ("int", "nVisualSave", 10 ** 8), ("int", "addVisualizationSteps", 0),
             ("string", "gridFileName", '"grid/mesh.ofl"'), ("string", "aeroFile", '"results/aero.dat"'),
             ("string", "resFile", '"results/res.dat"'), ("string", "wallaeroFile", '"results/wallaero.dat"'),
@@ -256,3 +261,37 @@ def read_res_dat(path: str) -> np.ndarray:
         if tok and tok[0].lstrip("-").isdigit():
             rows.append([float(t) for t in tok])
     return np.array(rows)
+
+
+def read_flow_dat(path: str, n_eq: int, n_t: int) -> dict:
+    """A restart file in the reference's layout (Restart::Dump through
+    DataBook::WriteFile, codes/restart/src/Restart.cpp:155-164,190-194,99-120,
+    codes/database/src/DataBook.cpp:301-316), one zone: int64 byte count,
+    int32 outer step, f64 time, then q1, q2, res1, res2 as [n_eq][n_t] f64.
+    Returns {"step", "time", "q1", "q2", "res1", "res2"}."""
+    buf = open(path, "rb").read()
+    nbytes = int(np.frombuffer(buf, "<i8", 1, 0)[0])
+    need = 4 + 8 + 4 * n_eq * n_t * 8
+    if nbytes != need or len(buf) != 8 + nbytes:
+        raise ValueError(f"{path}: record of {nbytes} bytes in a {len(buf)}-byte file; "
+                         f"{n_eq} equations x {n_t} cells need {need}")
+    out = {"step": int(np.frombuffer(buf, "<i4", 1, 8)[0]), "time": float(np.frombuffer(buf, "<f8", 1, 12)[0])}
+    a = np.frombuffer(buf, "<f8", 4 * n_eq * n_t, 20).reshape(4, n_eq, n_t)
+    for k, name in enumerate(("q1", "q2", "res1", "res2")):
+        out[name] = a[k].copy()
+    return out
+
+
+def write_flow_dat(path: str, q1: np.ndarray, step: int, time: float = 0.0, q2: np.ndarray = None,
+                   res1: np.ndarray = None, res2: np.ndarray = None) -> None:
+    """Write the same single-zone restart record (q2 defaults to q1, the
+    residuals to zero)."""
+    q1 = np.atleast_2d(np.asarray(q1, "<f8"))
+    z = np.zeros_like(q1)
+    parts = [q1, q1 if q2 is None else q2, z if res1 is None else res1, z if res2 is None else res2]
+    body = np.concatenate([np.asarray(p, "<f8").reshape(q1.shape).ravel() for p in parts])
+    with open(path, "wb") as fh:
+        fh.write(np.array([4 + 8 + body.nbytes], "<i8").tobytes())
+        fh.write(np.array([step], "<i4").tobytes())
+        fh.write(np.array([time], "<f8").tobytes())
+        fh.write(body.tobytes())

@@ -46,6 +46,8 @@ def load_library() -> C.CDLL:
         getattr(L, name).argtypes = [C.c_void_p]
     L.ofg_upload_state.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ofg_download_state.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ofg_write_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_double]
+    L.ofg_read_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     for name in ("ofg_zero_dq", "ofg_calc_time_step", "ofg_load_residuals", "ofg_update_residuals", "ofg_init_lusgs",
                  "ofg_lusgs_lower", "ofg_lusgs_upper", "ofg_update_flowfield", "ofg_calc_boundary"):
         getattr(L, name).argtypes = [C.c_void_p, C.c_int]
@@ -134,6 +136,19 @@ class Solver:
         flat = out.reshape(-1)
         self._check(self.L.ofg_download_state(self.h, tid, flat))
         return out.reshape(5, self.nT) if ne == 5 else out.reshape(-1)
+
+    def write_restart(self, path: str, tid: int = NS_SOLVER, curr_time: float = 0.0):
+        """DUMP_RESTART: the solver's restart record in the reference's file
+        layout (ofg_write_restart; "flowFile" for NS, "turbflowFile" for SA)."""
+        self._check(self.L.ofg_write_restart(self.h, tid, os.fsencode(path), C.c_double(curr_time)))
+
+    def read_restart(self, path: str, tid: int = NS_SOLVER):
+        """READ_RESTART from a file in the reference's layout (ofg_read_restart):
+        the state becomes the file's q1; for NS the outer step counter follows
+        the file.  Returns (outer step, time) of the file."""
+        step, t = C.c_int64(), C.c_double()
+        self._check(self.L.ofg_read_restart(self.h, tid, os.fsencode(path), C.byref(step), C.byref(t)))
+        return step.value, t.value
 
     # ---- tasks ----
     def task(self, name: str, tid: int = NS_SOLVER):

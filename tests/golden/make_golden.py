@@ -8,7 +8,16 @@ Each fixture <case>.npz holds the case parameters, the final primitive state
 q [5][nCells+nBFaces], nu~ for SA cases, the aerodynamic forces of the final
 state (total, pressure, viscous x y z, CL, CD, CD_pres, CD_vis) and the
 residual history the reference printed (res.dat / turbres.dat rows).  The meshes are regenerated
-from their seeds by the tests, so only the outputs are stored."""
+from their seeds by the tests, so only the outputs are stored.
+
+restart_<case>.npz holds the restart files the reference wrote at outer step
+RESTART_CASES[case] of the same case (restart/flow.dat, and restart/turbflow.dat
+for SA), as the arrays of their single-zone record: step, time, q1, q2 (the
+residual records are zero in a steady run).  oneflow_b200.meshio.write_flow_dat
+rebuilds the files byte for byte from them; the reference continued from those
+files reaches the same state as its uninterrupted run (<case>.npz) bitwise.
+
+    python tests/golden/make_golden.py --restart-only   # only the restart fixtures"""
 import json
 import os
 import sys
@@ -20,12 +29,38 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
-from oneflow_b200 import params as P  # noqa: E402
-from golden_cases import CASES, build  # noqa: E402
+from oneflow_b200 import meshio, params as P  # noqa: E402
+from golden_cases import CASES, RESTART_CASES, build  # noqa: E402
 from oracle_lib import run_ref  # noqa: E402
 
 
+def restart_fixtures():
+    import tempfile
+    for name, at in RESTART_CASES.items():
+        mesh, prm, steps = build(name)
+        files = {}
+        run_ref(mesh, prm, at, restart_out=files)
+        nt = mesh.n_cells + mesh.n_bfaces
+        out = {}
+        for fname, key, ne in (("flow.dat", "ns", 5), ("turbflow.dat", "turb", 1)):
+            if fname not in files:
+                continue
+            with tempfile.NamedTemporaryFile(suffix=".dat") as tmp:
+                tmp.write(files[fname]); tmp.flush()
+                rec = meshio.read_flow_dat(tmp.name, ne, nt)
+                meshio.write_flow_dat(tmp.name + ".chk", rec["q1"], rec["step"], rec["time"], q2=rec["q2"])
+                same = open(tmp.name + ".chk", "rb").read() == files[fname]
+                os.remove(tmp.name + ".chk")
+            assert same and not rec["res1"].any() and not rec["res2"].any(), fname
+            out.update({f"{key}_q1": rec["q1"], f"{key}_q2": rec["q2"], "step": rec["step"], "time": rec["time"]})
+        np.savez_compressed(os.path.join(HERE, f"restart_{name}.npz"), **out)
+        print("restart", name, "at step", at, sorted(files))
+
+
 def main():
+    restart_fixtures()
+    if "--restart-only" in sys.argv:
+        return
     for name, spec in CASES.items():
         mesh, prm, steps = build(name)
         dump, rows = run_ref(mesh, prm, steps)

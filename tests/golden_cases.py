@@ -12,6 +12,8 @@ CASES = {
     "plate3d_sa_roe": dict(steps=10),
     "plate3d_sa_roe_colour_renumbered": dict(steps=10),
 }
+# cases whose restart files (written by the reference at this outer step) are fixtures too
+RESTART_CASES = {"bump_euler_roe_venkat": 20, "plate2d_sa_roe": 20}
 
 
 def build(name):

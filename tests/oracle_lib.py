@@ -112,12 +112,20 @@ def ref_available() -> bool:
     return os.path.exists(REF_EXE)
 
 
-def run_ref(mesh: Mesh, params: P.OfgParams, steps: int, workdir: str = None, keep: bool = False):
-    """Run the reference CPU solver on ``mesh`` for ``steps`` iterations.
-    Returns (dump dict, res.dat rows)."""
+def run_ref(mesh: Mesh, params: P.OfgParams, steps: int, workdir: str = None, keep: bool = False,
+            restart_in: dict = None, restart_out: dict = None):
+    """Run the reference CPU solver on ``mesh`` up to outer iteration ``steps``.
+    Returns (dump dict, res.dat rows).  ``restart_in`` ({"flow.dat": bytes,
+    "turbflow.dat": bytes}) starts it from those restart files (startStrategy 1);
+    with ``restart_out`` (a dict) it writes restart files at its last step
+    (nFieldSave = steps), which are put there by name."""
     tmp = workdir or tempfile.mkdtemp(prefix="ofgref_")
     case = os.path.join(tmp, "case")
-    write_case(case, mesh, P.to_dict(params), steps)
+    write_case(case, mesh, P.to_dict(params), steps, start_strategy=1 if restart_in else 0,
+               field_save=steps if restart_out is not None else 10 ** 8)
+    for name, data in (restart_in or {}).items():
+        with open(os.path.join(case, "restart", name), "wb") as fh:
+            fh.write(data)
     dump = os.path.join(tmp, "dump.bin")
     env = dict(os.environ, OFG_REF_DUMP=dump)
     r = subprocess.run([REF_EXE, "0", "case"], cwd=tmp, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
@@ -125,6 +133,11 @@ def run_ref(mesh: Mesh, params: P.OfgParams, steps: int, workdir: str = None, ke
     if r.returncode != 0:
         raise RuntimeError(r.stdout.decode(errors="replace")[-3000:])
     out = read_ref_dump(dump), read_res_dat(os.path.join(case, "results", "res.dat"))
+    if restart_out is not None:
+        for name in ("flow.dat", "turbflow.dat"):
+            fn = os.path.join(case, "restart", name)
+            if os.path.exists(fn):
+                restart_out[name] = open(fn, "rb").read()
     if not keep and workdir is None:
         shutil.rmtree(tmp, ignore_errors=True)
     return out
