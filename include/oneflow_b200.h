@@ -116,13 +116,23 @@ int         ofg_version(void);
  * Mesh upload: the content of one .ofl zone (codes/geometry/src/UnsGrid.cpp:90-201).
  * lCells may be negative for a boundary face, in which case the face is
  * reversed (UnsGrid::ReadGridFaceTopology, :157-175).  Boundary faces are
- * [0, nBFaces).  Metrics (UnsGrid::CalcMetrics, :469-900) are computed here.
- * wall_dist (may be NULL for non-SA runs) is per interior cell.
+ * [0, nBFaces).  Metrics (UnsGrid::CalcMetrics, :469-900) are computed here,
+ * on the GPU.  wall_dist is per interior cell; NULL makes an SA solve compute
+ * it (ofg_calc_wall_dist) and is ignored otherwise.
  */
 int ofg_upload_mesh(ofg_ctx *ctx, int nNodes, const double *xN, const double *yN, const double *zN,
                     int nFaces, const int *faceNodeCount, const int *faceNodes,
                     const int *lCells, const int *rCells, int nCells, int nBFaces,
                     const int *bcType, const double *wall_dist);
+
+/* CALC_WALL_DIST (CalcWallDist + CalcPoint2FaceDist, codes/geometry/src/WallDist.cpp:136-330):
+   the distance from every cell centre to the nearest SOLID_SURFACE face
+   (segments in 2-D; triangles in 3-D, faces of more than three nodes fanned
+   about their node average), computed on the GPU and used by the SA source
+   from then on.  ofg_upload_mesh runs it by itself for an SA solve whose
+   wall_dist is NULL (the reference's ireadwdst = 0); the result is readable
+   as the field "walldist". */
+int ofg_calc_wall_dist(ofg_ctx *ctx);
 
 /* INIT_FLOWFIELD with startStrategy 0: freestream + CALC_BOUNDARY
    (codes/uns/src/UNsRestart.cpp:48-60, codes/ns/src/NsSolverImp.cpp:61-73). */
@@ -182,7 +192,8 @@ int ofg_residual_norms(ofg_ctx *ctx, int tid, double *rms);
 
 /* Named device field -> host, reference layout:
    "res","dq","timestep","invsr","vissr","impsr","limiter","dqdx","dqdy","dqdz",
-   "tempr","visl","vist","vol","xcc","ycc","zcc","area","xfn","yfn","zfn".
+   "tempr","visl","vist","vol","xcc","ycc","zcc","area","xfn","yfn","zfn",
+   "xfc","yfc","zfc","walldist".
    n_out = capacity in doubles; the size needed is returned in *n_needed. */
 int ofg_download_field(ofg_ctx *ctx, int tid, const char *name, double *out, int64_t n_out,
                        int64_t *n_needed);

@@ -475,9 +475,6 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         if (t < 1 || t > 6)
             return c->fail(OFG_E_ARG, "unsupported boundary type (codes 1-6; interface, overset, periodic and pole "
                                       "faces belong to multi-zone or structured cases)");
-    compute_metrics(c, c->p.dimension, X, Y, Z, fOff, fNod);
-    for (int i = 0; i < nCells; ++i)
-        if (!(c->vol[i] > 0.0)) return c->fail(OFG_E_ARG, "degenerate cell volume");
     // CSR cell->face in ascending face id (CellTopo::CalcC2f)
     c->c2f_off.assign(nCells + 1, 0);
     for (int f = 0; f < nFaces; ++f) {
@@ -494,8 +491,6 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     build_sweep_key(c);
     build_levels(c, true, c->lowOrder, c->lowOff);
     build_levels(c, false, c->upOrder, c->upOff);
-    c->wdist.assign(nCells, 0.0);
-    if (wall_dist) std::copy(wall_dist, wall_dist + nCells, c->wdist.begin());
 
     // ---- device copies ----
     int rc;
@@ -512,6 +507,16 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         if ((rc = upload(c, &c->d_up_off, L.upOff.data(), L.upOff.size()))) return rc;
         if ((rc = upload(c, &c->d_upl, L.upl.data(), L.upl.size()))) return rc;
     }
+    // metrics on the GPU (UnsGrid::CalcMetrics); for an SA solve without a
+    // caller-supplied wall distance, CALC_WALL_DIST on the GPU as well
+    c->xN = std::move(X); c->yN = std::move(Y); c->zN = std::move(Z);
+    c->fOff = std::move(fOff); c->fNod = std::move(fNod);
+    const bool needWall = has_turb(c) && !wall_dist;
+    c->wdist.assign(nCells, 0.0);
+    if (wall_dist) std::copy(wall_dist, wall_dist + nCells, c->wdist.begin());
+    if ((rc = gpu_geometry(c, c->xN, c->yN, c->zN, c->fOff, c->fNod, true, needWall))) return rc;
+    for (int i = 0; i < nCells; ++i)
+        if (!(c->vol[i] > 0.0)) return c->fail(OFG_E_ARG, "degenerate cell volume");
     if ((rc = upload(c, &c->d_bct, c->bct.data(), nBFaces))) return rc;
     if ((rc = upload(c, &c->d_lowOrder, c->lowOrder.data(), nCells))) return rc;
     if ((rc = upload(c, &c->d_upOrder, c->upOrder.data(), nCells))) return rc;
@@ -586,9 +591,8 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     CK(cudaMemset(c->d_scal, 0, 32 * sizeof(double)));
     CK(cudaMemset(c->d_fix, 0, (1 + c->fixcap) * sizeof(int)));
     if (has_turb(c)) {
-        if (!wall_dist) return c->fail(OFG_E_ARG, "the SA model needs the wall distance");
-        for (int i = 0; i < nCells; ++i)
-            if (!(wall_dist[i] > 0.0)) return c->fail(OFG_E_ARG, "wall distance must be positive");
+        for (int i = 0; i < nCells; ++i)   // supplied, or computed on the GPU above
+            if (!(c->wdist[i] > 0.0)) return c->fail(OFG_E_ARG, "wall distance must be positive");
         if ((rc = upload<double>(c, &c->d_nut, nullptr, nT))) return rc;
         if ((rc = upload<double>(c, &c->d_dnut, nullptr, nT))) return rc;
         if ((rc = upload<double>(c, &c->d_resT, nullptr, N))) return rc;
@@ -690,6 +694,15 @@ int ofg_download_state(ofg_ctx *c, int tid, double *q) {
     if ((rc = launch(c, T_UNPACK_STATE))) return rc;
     CK(cudaMemcpyAsync(q, c->d_stage, (size_t)NEQ * c->nT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return sync(c);
+}
+
+int ofg_calc_wall_dist(ofg_ctx *c) {
+    if (!c) return OFG_E_ARG;
+    if (!c->haveMesh) return c->fail(OFG_E_STATE, "no mesh uploaded");
+    int rc = gpu_geometry(c, c->xN, c->yN, c->zN, c->fOff, c->fNod, false, true);
+    if (rc) return rc;
+    CK(cudaMemcpy(c->d_wdist, c->wdist.data(), (size_t)c->nCells * sizeof(double), cudaMemcpyHostToDevice));
+    return OFG_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1056,6 +1069,9 @@ int ofg_download_field(ofg_ctx *c, int tid, const char *name, double *out, int64
     else if (s == "xfn") host_vec(c->xfn);
     else if (s == "yfn") host_vec(c->yfn);
     else if (s == "zfn") host_vec(c->zfn);
+    else if (s == "xfc") host_vec(c->xfc);
+    else if (s == "yfc") host_vec(c->yfc);
+    else if (s == "zfc") host_vec(c->zfc);
     else if (s == "reshist") host_vec(tid == OFG_TURB_SOLVER ? c->thist : c->hist);
     else if (s == "turbreshist") host_vec(c->thist);
     else if (has_turb(c) && (s == "turbq" || s == "turbdq")) aos_field(s == "turbq" ? c->d_nut : c->d_dnut, 1, nT, nT);

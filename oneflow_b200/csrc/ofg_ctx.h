@@ -18,6 +18,8 @@ struct ofg_ctx {
     int nCells = 0, nBFaces = 0, nFaces = 0, nT = 0;
     std::vector<int> lc, rc, bct, c2f_off, c2f;
     std::vector<double> xfn, yfn, zfn, area, xfc, yfc, zfc, xcc, ycc, zcc, vol, wdist;
+    std::vector<double> xN, yN, zN;                      // nodes, and the face->node lists (CSR, reversed
+    std::vector<int> fOff, fNod;                         // faces turned) the metrics were computed from
     std::vector<int> lowOrder, lowOff, upOrder, upOff;   // LU-SGS level schedules
     std::vector<int> key, keyOrder;                      // sweep position of each cell, and its inverse
     bool haveMesh = false, haveState = false;
@@ -84,4 +86,8 @@ enum Task {
 };
 int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);
 int launch_task_f32(ofg_ctx *c, int task, cudaStream_t s);
+// ofg_geom.cu: metrics (metrics = true) and/or the wall distance on the GPU
+int gpu_geometry(ofg_ctx *c, const std::vector<double> &X, const std::vector<double> &Y,
+                 const std::vector<double> &Z, const std::vector<int> &fOff, const std::vector<int> &fNod,
+                 bool metrics, bool wallDist);
 }  // namespace ofg

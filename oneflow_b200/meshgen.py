@@ -234,3 +234,73 @@ def flat_plate_tets(nx: int = 200, ny: int = 100, nz: int = 50, ratio: float = 1
                 rc.astype(np.int32), nc, nb, bct_all[:nb].copy(),
                 meta=dict(kind="flat_plate_tets", nx=nx, ny=ny, nz=nz, ratio=ratio, y1=y1, seed=seed))
     return mesh
+
+
+# the six quad faces of a hex (corner order of _CORNER), each outward-oriented
+_HEX_FACES = np.array([[0, 3, 2, 1], [4, 5, 6, 7], [0, 1, 5, 4], [3, 7, 6, 2], [0, 4, 7, 3], [1, 2, 6, 5]], np.int64)
+
+
+def bump_box_hexes(nx: int = 12, ny: int = 8, nz: int = 10, height: float = 0.15, jitter: float = 0.15,
+                   seed: int = 20261203) -> Mesh:
+    """Hexahedral box [0,1] x [0,1] x [0,1] over a Gaussian bump on its floor
+    (y_floor = height * exp(-((x-.5)^2 + (z-.5)^2) / 0.05)); the layers above
+    follow the floor, fading out towards the top.  Interior nodes jittered
+    (seeded), so the quad faces are warped.  BCs: floor SOLID_SURFACE, the
+    other five sides FARFIELD.  A mesh with non-planar quadrilateral walls,
+    for metrics and wall-distance tests."""
+    rng = np.random.default_rng(seed)
+    xs, ys, zs = np.linspace(0, 1, nx + 1), np.linspace(0, 1, ny + 1), np.linspace(0, 1, nz + 1)
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    floor = height * np.exp(-((X - 0.5) ** 2 + (Z - 0.5) ** 2) / 0.05)
+    Y = Y + floor * (1.0 - Y)
+    interior = np.zeros(X.shape, bool)
+    interior[1:-1, 1:-1, 1:-1] = True
+    h = np.array([1.0 / nx, 1.0 / ny, 1.0 / nz])
+    for A, hh in ((X, h[0]), (Y, h[1]), (Z, h[2])):
+        A += np.where(interior, rng.uniform(-jitter, jitter, A.shape) * hh, 0.0)
+    NY, NZ = ny + 1, nz + 1
+    x, y, z = X.ravel(), Y.ravel(), Z.ravel()
+    nid = lambda i, j, k: (i * NY + j) * NZ + k
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    corner = np.stack([nid(ii + c[0], jj + c[1], kk + c[2]) for c in _CORNER], axis=1)   # [nc, 8]
+    nc = corner.shape[0]
+    quad = corner[:, _HEX_FACES].reshape(-1, 4)
+    owner = np.repeat(np.arange(nc), 6)
+    # the left-handed corner order of _CORNER makes these faces inward: flip
+    P = np.stack([x, y, z], 1)
+    cc = P[corner].mean(1)
+    fc = P[quad].mean(1)
+    nrm = np.cross(P[quad[:, 2]] - P[quad[:, 0]], P[quad[:, 3]] - P[quad[:, 1]])
+    inward = np.einsum("ij,ij->i", nrm, fc - cc[owner]) < 0
+    quad[inward] = quad[inward][:, ::-1]
+    s = np.sort(quad, axis=1)
+    key = ((s[:, 0] * len(x) + s[:, 1]) * len(x) + s[:, 2]) * len(x) + s[:, 3]
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    new = np.ones(ks.shape[0], bool)
+    new[1:] = ks[1:] != ks[:-1]
+    grp = np.cumsum(new) - 1
+    nf = int(grp[-1]) + 1
+    first = order[new]
+    cnt = np.bincount(grp, minlength=nf)
+    pos2 = np.flatnonzero(new) + 1
+    has2 = cnt == 2
+    lc = owner[first]
+    rc = np.full(nf, -1, np.int64)
+    rc[has2] = owner[order[pos2[has2]]]
+    nodes = quad[first]
+    swap = has2 & (rc < lc)
+    second = quad[order[np.minimum(pos2, len(order) - 1)]]
+    nodes = np.where(swap[:, None], second, nodes)
+    lc, rc = np.where(swap, rc, lc), np.where(swap, lc, rc)
+    isb = rc < 0
+    bct_all = np.full(nf, FAR, np.int32)
+    floor_nodes = nid(*np.meshgrid(np.arange(nx + 1), [0], np.arange(nz + 1), indexing="ij")).ravel()
+    bct_all[isb & np.all(np.isin(nodes, floor_nodes), axis=1)] = SOLID
+    forder = np.lexsort((rc, lc, ~isb))
+    lc, rc, nodes, bct_all = lc[forder], rc[forder], nodes[forder], bct_all[forder]
+    nb = int(isb.sum())
+    return Mesh(3, x, y, z, np.full(nf, 4, np.int32), nodes.ravel().astype(np.int32), lc.astype(np.int32),
+                rc.astype(np.int32), nc, nb, bct_all[:nb].copy(),
+                meta=dict(kind="bump_box_hexes", nx=nx, ny=ny, nz=nz, seed=seed))

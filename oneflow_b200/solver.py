@@ -46,6 +46,7 @@ def load_library() -> C.CDLL:
         getattr(L, name).argtypes = [C.c_void_p]
     L.ofg_upload_state.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ofg_download_state.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ofg_calc_wall_dist.argtypes = [C.c_void_p]
     L.ofg_write_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_double]
     L.ofg_read_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     for name in ("ofg_zero_dq", "ofg_calc_time_step", "ofg_load_residuals", "ofg_update_residuals", "ofg_init_lusgs",
@@ -136,6 +137,11 @@ class Solver:
         flat = out.reshape(-1)
         self._check(self.L.ofg_download_state(self.h, tid, flat))
         return out.reshape(5, self.nT) if ne == 5 else out.reshape(-1)
+
+    def calc_wall_dist(self):
+        """CALC_WALL_DIST on the GPU (ofg_calc_wall_dist); the SA source uses it
+        from then on.  The distances: field("walldist")."""
+        self._check(self.L.ofg_calc_wall_dist(self.h))
 
     def write_restart(self, path: str, tid: int = NS_SOLVER, curr_time: float = 0.0):
         """DUMP_RESTART: the solver's restart record in the reference's file

@@ -17,7 +17,11 @@ residual records are zero in a steady run).  oneflow_b200.meshio.write_flow_dat
 rebuilds the files byte for byte from them; the reference continued from those
 files reaches the same state as its uninterrupted run (<case>.npz) bitwise.
 
-    python tests/golden/make_golden.py --restart-only   # only the restart fixtures"""
+walldist_<name>.npz holds the wall distance the reference computed itself
+(CALC_WALL_DIST, ireadwdst = 0) on the meshes of WALLDIST_CASES.
+
+    python tests/golden/make_golden.py --restart-only   # only the restart fixtures
+    python tests/golden/make_golden.py --walldist-only  # only the wall-distance fixtures"""
 import json
 import os
 import sys
@@ -30,7 +34,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 from oneflow_b200 import meshio, params as P  # noqa: E402
-from golden_cases import CASES, RESTART_CASES, build  # noqa: E402
+from golden_cases import CASES, RESTART_CASES, WALLDIST_CASES, build, build_walldist  # noqa: E402
 from oracle_lib import run_ref  # noqa: E402
 
 
@@ -57,10 +61,23 @@ def restart_fixtures():
         print("restart", name, "at step", at, sorted(files))
 
 
+def walldist_fixtures():
+    for name in WALLDIST_CASES:
+        mesh, prm = build_walldist(name)
+        dump, _ = run_ref(mesh, prm, 1)
+        wd = dump["walldist"][0, :mesh.n_cells]
+        np.savez_compressed(os.path.join(HERE, f"walldist_{name}.npz"), walldist=wd)
+        print("walldist", name, mesh.n_cells, "cells", float(wd.min()), float(wd.max()))
+
+
 def main():
+    if "--walldist-only" in sys.argv:
+        walldist_fixtures()
+        return
     restart_fixtures()
     if "--restart-only" in sys.argv:
         return
+    walldist_fixtures()
     for name, spec in CASES.items():
         mesh, prm, steps = build(name)
         dump, rows = run_ref(mesh, prm, steps)

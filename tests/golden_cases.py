@@ -12,6 +12,22 @@ CASES = {
     "plate3d_sa_roe": dict(steps=10),
     "plate3d_sa_roe_colour_renumbered": dict(steps=10),
 }
+# meshes whose wall distance the reference computed itself (ireadwdst = 0):
+# tests/golden/walldist_<name>.npz
+WALLDIST_CASES = ("plate2d_sa_roe", "plate3d_sa_roe", "hexbox_sa")
+
+
+def build_walldist(name):
+    """mesh (without a wall distance) and SA parameters of a wall-distance case"""
+    if name == "hexbox_sa":
+        mesh = meshgen.bump_box_hexes()
+        prm = P.defaults(dimension=3, ischeme=1, ilim=0, vismodel=3, mach_ref=0.2, reynolds=5e6)
+    else:
+        mesh, prm, _ = build(name)
+    mesh.wall_dist = None
+    return mesh, prm
+
+
 # cases whose restart files (written by the reference at this outer step) are fixtures too
 RESTART_CASES = {"bump_euler_roe_venkat": 20, "plate2d_sa_roe": 20}
 

@@ -77,6 +77,17 @@ def test_host_metrics_match_oracle(dim):
     assert np.array_equal(cc[:, 2], o.field("zcc")[:N])
 
 
+@pytest.mark.parametrize("name", ["plate2d_sa_roe", "plate3d_sa_roe", "hexbox_sa"])
+def test_host_wall_distance_matches_the_reference(name):
+    # the numpy restatement of CALC_WALL_DIST (used to write the distance files
+    # the reference reads) against the distances the reference computed itself
+    from golden_cases import build_walldist
+    from oneflow_b200.walldist import wall_distance
+    mesh, _ = build_walldist(name)
+    ref = np.load(os.path.join(ROOT, "tests", "golden", f"walldist_{name}.npz"))["walldist"]
+    assert np.abs(wall_distance(mesh) / ref - 1.0).max() < 1e-14
+
+
 def test_colour_order_is_a_proper_colouring():
     mesh = meshgen.flat_plate_tets(6, 5, 4)
     perm, ncol = colour_order(mesh)
