@@ -278,6 +278,7 @@ def main():
     ap.add_argument("--ordering", default="colour", choices=["natural", "colour"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8-drop runs")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched airfoil runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -433,6 +434,9 @@ def main():
     conv = None
     if rank == 0 and world == 1 and not args.no_converge:
         conv = time_to_drop("bump2d_small", 1e-8, stream)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_throughput()
 
     clocks = clk.summary()
     if rank == 0:
@@ -447,7 +451,8 @@ def main():
                 "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": int(l1 - l0), "clocks": clocks, "time_to_1e-8": conv,
-                "setup": {"calc_wall_dist_s": wall_s, "wall_dist_vs_closed_form": wall_err}}
+                "setup": {"calc_wall_dist_s": wall_s, "wall_dist_vs_closed_form": wall_err},
+                "batched": batched}
         print(json.dumps(line))
     if dist:
         dist.barrier()
@@ -467,6 +472,48 @@ def replica_aggregate(total_ms, cells, steps, world, dist):
         total_ms = float(t.item())
         dist.barrier()
     return total_ms, cells * steps * world / (total_ms * 1e-3)
+
+
+def batched_throughput(n_cases: int = 64, steps: int = 10, warmup: int = 3):
+    """The batched configuration: 64 seeded 2-D RANS-SA airfoil solves of
+    uneven sizes (20k-400k cells, 7.9M in all), advanced (a) one after
+    another, each by its own graph launches, and (b) together by one batch
+    graph launch per iteration.  Host wall clock around the synchronous calls
+    (both include their launch overheads), after warm-up (graphs captured)."""
+    import torch
+    from oneflow_b200 import Batch, Solver
+    cases = meshgen.airfoil_cases(n_cases)
+    ss = []
+    for mesh, fs in cases:
+        s = Solver(mesh, P.rans_airfoil(**fs))
+        s.init_flowfield()
+        ss.append(s)
+    cells = sum(m.n_cells for m, _ in cases)
+    for s in ss:
+        s.step(warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in ss:
+        s.step(steps)
+    torch.cuda.synchronize()
+    seq = time.perf_counter() - t0
+    b = Batch(ss)
+    b.step(warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.step(steps)
+    torch.cuda.synchronize()
+    bat = time.perf_counter() - t0
+    b.close()
+    for s in ss:
+        s.close()
+    return {"workload": f"{n_cases} 2-D RANS-SA NACA 4-digit airfoils, hybrid O-grids of "
+                        f"{min(m.n_cells for m, _ in cases):,}-{max(m.n_cells for m, _ in cases):,} cells, "
+                        "Mach 0.3-0.8, AoA -2..8 deg, Re 1e6-1e7 (seeded); Roe 2nd order Green-Gauss + Venkatakrishnan, "
+                        "SA, LU-SGS, FP32 faces",
+            "cells": cells, "steps": steps, "unit": "cell-iter/s",
+            "sequential": cells * steps / seq, "batched": cells * steps / bat,
+            "timing": "host wall clock around synchronous calls, after warm-up"}
 
 
 def time_to_drop(config: str, target: float, stream, chunk: int = 200, max_iters: int = 40000):

@@ -183,6 +183,20 @@ int ofg_calc_boundary(ofg_ctx *ctx, int tid);       /* CALC_BOUNDARY          */
    :349-360), with the RMS residual of every iteration appended to the history. */
 int ofg_step(ofg_ctx *ctx, int nsteps);
 
+/* Batched solves: n independent contexts (each its own mesh, parameters and
+   state) advanced together, as if ofg_step(ctx, nsteps) ran on each: one
+   CUDA-graph launch per outer iteration whose branches are the contexts'
+   own iteration graphs, so that many small solves share the GPU at once.
+   The reference runs one case per process (MG::Run); this replaces a set of
+   such runs.  Results are bitwise those of ofg_step on each context.  The
+   contexts stay usable on their own between batch steps (the batch rebuilds
+   its graph when one of them changed).  Errors name the context. */
+typedef struct ofg_batch ofg_batch;
+int         ofg_batch_create(ofg_ctx *const *ctxs, int n, ofg_batch **out);
+int         ofg_batch_step(ofg_batch *batch, int nsteps);
+void        ofg_batch_destroy(ofg_batch *batch);
+const char *ofg_batch_last_error(const ofg_batch *batch);
+
 /* RMS residual per equation of the solver's last UPDATE_RESIDUALS
    (ResidualTask::CalcRes + ResAver::CalcAver,
    codes/residual/src/ResidualTask.cpp:75-126, codes/residual/src/Residual.cpp:52-72):

@@ -376,8 +376,11 @@ int check_tid(ofg_ctx *c, int tid) {
 }
 
 void destroy_graphs(ofg_ctx *c) {
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i) {
         if (c->graph[i]) { cudaGraphExecDestroy(c->graph[i]); c->graph[i] = nullptr; }
+        if (c->graphT[i]) { cudaGraphDestroy(c->graphT[i]); c->graphT[i] = nullptr; }
+    }
+    c->graphGen++;
 }
 
 }  // namespace
@@ -894,53 +897,160 @@ static int sync_history(ofg_ctx *c) {
     return OFG_OK;
 }
 
-int ofg_step(ofg_ctx *c, int nsteps) {
+// checks before n fused outer iterations; the device step counter and history
+// indices follow the host counters (queued on the context's stream)
+static int prepare_steps(ofg_ctx *c, int nsteps) {
     int rc = check_tid(c, OFG_NS_SOLVER);
     if (rc) return rc;
     if (nsteps < 0) return c->fail(OFG_E_ARG, "negative step count");
     if (c->pendingNext || c->pendingTurb) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
     if (c->outerSteps + nsteps > c->histCap) return c->fail(OFG_E_ARG, "residual history capacity exceeded");
-    // the device step counter and history indices follow the host counters
     double sc[4] = {double(c->outerSteps), double(c->outerSteps), 0.0, double(c->outerSteps)};
     CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_scal + S_THISTN, sc + 3, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    if ((rc = sync(c))) return rc;
-    if (!c->graph[0]) {
-        // one outer iteration per state-buffer parity (ZERO_DQ_FIELD is not
-        // needed: no kernel reads an increment it did not write this iteration)
-        int saveCur = c->cur;
-        for (int g = 0; g < 2; ++g) {
-            long long before = c->launches;
-            cudaGraph_t graph;
-            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            c->cur = g;
-            for (int t : kNsTasks) {
+    return sync(c);
+}
+
+// one outer iteration per state-buffer parity, captured once (ZERO_DQ_FIELD
+// is not needed: no kernel reads an increment it did not write this iteration)
+static int ensure_graphs(ofg_ctx *c) {
+    if (c->graph[0]) return OFG_OK;
+    int rc, saveCur = c->cur;
+    for (int g = 0; g < 2; ++g) {
+        long long before = c->launches;
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->cur = g;
+        for (int t : kNsTasks) {
+            rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
+            if (rc) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
+        }
+        c->cur = g ^ 1;
+        if (has_turb(c))
+            for (int t : kTurbTasks) {
                 rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
                 if (rc) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
             }
-            c->cur = g ^ 1;
-            if (has_turb(c))
-                for (int t : kTurbTasks) {
-                    rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
-                    if (rc) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
-                }
-            CK(cudaStreamEndCapture(c->stream, &graph));
-            CK(cudaGraphInstantiate(&c->graph[g], graph, 0));
-            cudaGraphDestroy(graph);
-            c->graphKernels[g] = c->launches - before;
-            c->launches = before;
-        }
-        c->cur = saveCur;
+        CK(cudaStreamEndCapture(c->stream, &graph));
+        CK(cudaGraphInstantiate(&c->graph[g], graph, 0));
+        c->graphT[g] = graph;   // kept: a batch embeds it as a child graph
+        c->graphKernels[g] = c->launches - before;
+        c->launches = before;
     }
+    c->cur = saveCur;
+    return OFG_OK;
+}
+
+// host bookkeeping of one outer iteration launched from parity c->cur
+static void account_step(ofg_ctx *c) {
+    c->launches += c->graphKernels[c->cur];
+    c->lastResBuf = c->cur;   // this iteration's residual pass read the buffer it started from
+    c->cur ^= 1;
+    c->outerSteps++;
+}
+
+int ofg_step(ofg_ctx *c, int nsteps) {
+    int rc = prepare_steps(c, nsteps);
+    if (rc) return rc;
+    if ((rc = ensure_graphs(c))) return rc;
     for (int it = 0; it < nsteps; ++it) {
         CK(cudaGraphLaunch(c->graph[c->cur], c->stream));
-        c->launches += c->graphKernels[c->cur];
-        c->lastResBuf = c->cur;   // this iteration's residual pass read the buffer it started from
-        c->cur ^= 1;
-        c->outerSteps++;
+        account_step(c);
     }
     if ((rc = sync(c))) return rc;
     return sync_history(c);
+}
+
+// ---------------------------------------------------------------------------
+// Batched solves: independent contexts advanced by one graph launch per outer
+// iteration, whose branches are the contexts' own iteration graphs.
+// ---------------------------------------------------------------------------
+struct ofg_batch {
+    std::vector<ofg_ctx *> ctx;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};   // [k]: each context at parity built[i] ^ k
+    std::vector<int> built;                          // the contexts' parities when the execs were built
+    std::vector<unsigned> gen;                       // and their graph generations
+    std::string err;
+    int fail(int code, const std::string &m) { err = m; return code; }
+};
+
+static void batch_release(ofg_batch *b) {
+    for (auto &e : b->exec)
+        if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+}
+
+int ofg_batch_create(ofg_ctx *const *ctxs, int n, ofg_batch **out) {
+    if (!ctxs || n <= 0 || !out) return OFG_E_ARG;
+    auto *b = new ofg_batch();
+    for (int i = 0; i < n; ++i) {
+        if (!ctxs[i]) { delete b; return OFG_E_ARG; }
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i]) { delete b; return OFG_E_ARG; }   // each context once
+        b->ctx.push_back(ctxs[i]);
+    }
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { delete b; return OFG_E_CUDA; }
+    *out = b;
+    return OFG_OK;
+}
+
+void ofg_batch_destroy(ofg_batch *b) {
+    if (!b) return;
+    cudaStreamSynchronize(b->stream);
+    batch_release(b);
+    cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+const char *ofg_batch_last_error(const ofg_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int ofg_batch_step(ofg_batch *b, int nsteps) {
+    if (!b) return OFG_E_ARG;
+    const int n = int(b->ctx.size());
+    for (int i = 0; i < n; ++i) {
+        ofg_ctx *c = b->ctx[i];
+        int rc = prepare_steps(c, nsteps);
+        if (!rc) rc = ensure_graphs(c);
+        if (rc) return b->fail(rc, "context " + std::to_string(i) + ": " + c->err);
+    }
+    // the two batch graphs stay valid while every context keeps the graphs
+    // they were built from and all contexts have flipped parity together
+    bool valid = b->exec[0] && int(b->built.size()) == n;
+    int flip = valid ? (b->ctx[0]->cur ^ b->built[0]) : 0;
+    for (int i = 0; valid && i < n; ++i)
+        valid = b->gen[i] == b->ctx[i]->graphGen && (b->ctx[i]->cur ^ b->built[i]) == flip;
+    if (!valid) {
+        batch_release(b);
+        b->built.assign(n, 0); b->gen.assign(n, 0);
+        for (int i = 0; i < n; ++i) { b->built[i] = b->ctx[i]->cur; b->gen[i] = b->ctx[i]->graphGen; }
+        for (int k = 0; k < 2; ++k) {
+            cudaGraph_t g;
+            if (cudaGraphCreate(&g, 0) != cudaSuccess) return b->fail(OFG_E_CUDA, "cudaGraphCreate");
+            for (int i = 0; i < n; ++i) {
+                cudaGraphNode_t node;
+                if (cudaGraphAddChildGraphNode(&node, g, nullptr, 0, b->ctx[i]->graphT[b->built[i] ^ k]) != cudaSuccess) {
+                    cudaGraphDestroy(g);
+                    return b->fail(OFG_E_CUDA, "cudaGraphAddChildGraphNode");
+                }
+            }
+            cudaError_t e = cudaGraphInstantiate(&b->exec[k], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return b->fail(OFG_E_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+        }
+        flip = 0;
+    }
+    for (int it = 0; it < nsteps; ++it) {
+        if (cudaGraphLaunch(b->exec[flip], b->stream) != cudaSuccess) return b->fail(OFG_E_CUDA, "cudaGraphLaunch");
+        for (ofg_ctx *c : b->ctx) account_step(c);
+        flip ^= 1;
+    }
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return b->fail(OFG_E_CUDA, cudaGetErrorString(e));
+    for (int i = 0; i < n; ++i) {
+        int rc = sync_history(b->ctx[i]);
+        if (rc) return b->fail(rc, "context " + std::to_string(i) + ": " + b->ctx[i]->err);
+    }
+    return OFG_OK;
 }
 
 int ofg_residual_norms(ofg_ctx *c, int tid, double *rms) {

@@ -65,6 +65,8 @@ struct ofg_ctx {
     long long launches = 0;
     std::vector<double> hist;          // host copy of residual history
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraph_t graphT[2] = {nullptr, nullptr};   // their templates (child graphs of a batch)
+    unsigned graphGen = 0;                         // bumped whenever the graphs are dropped
     long long graphKernels[2] = {0, 0};
 
     int fail(int code, const std::string &msg) {

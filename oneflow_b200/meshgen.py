@@ -304,3 +304,158 @@ def bump_box_hexes(nx: int = 12, ny: int = 8, nz: int = 10, height: float = 0.15
     return Mesh(3, x, y, z, np.full(nf, 4, np.int32), nodes.ravel().astype(np.int32), lc.astype(np.int32),
                 rc.astype(np.int32), nc, nb, bct_all[:nb].copy(),
                 meta=dict(kind="bump_box_hexes", nx=nx, ny=ny, nz=nz, seed=seed))
+
+
+def _faces_from_polygons_2d(poly: np.ndarray, counts: np.ndarray, n_nodes: int):
+    """Vectorised edge extraction for CCW polygons given as a padded node
+    array poly[nc, kmax] with counts[nc] valid entries: returns (nodes[nf,2],
+    lc, rc) with boundary edges (rc = -1) first, each edge directed as its
+    owner (the lower-numbered cell) lists it, so (y2-y1, x1-x2) points from lc
+    to rc."""
+    nc, kmax = poly.shape
+    k = np.arange(kmax)[None, :]
+    valid = k < counts[:, None]
+    nxt = np.where(k + 1 < counts[:, None], np.roll(poly, -1, axis=1), poly[:, :1])
+    a, b = poly[valid], nxt[valid]
+    owner = np.repeat(np.arange(nc), counts)
+    key = np.minimum(a, b).astype(np.int64) * n_nodes + np.maximum(a, b)
+    order = np.lexsort((owner, key))
+    ks = key[order]
+    new = np.ones(ks.shape[0], bool)
+    new[1:] = ks[1:] != ks[:-1]
+    grp = np.cumsum(new) - 1
+    nf = int(grp[-1]) + 1
+    first = order[new]
+    cnt = np.bincount(grp, minlength=nf)
+    pos2 = np.flatnonzero(new) + 1
+    lc = owner[first]
+    rc = np.full(nf, -1, np.int64)
+    has2 = cnt == 2
+    rc[has2] = owner[order[pos2[has2]]]
+    nodes = np.stack([a[first], b[first]], 1)
+    isb = rc < 0
+    forder = np.lexsort((rc, lc, ~isb))
+    return nodes[forder], lc[forder], rc[forder], int(isb.sum())
+
+
+def naca4_surface(m: float, p: float, t: float, n_half: int) -> np.ndarray:
+    """Closed NACA 4-digit section (max camber m, its position p, thickness t,
+    chord 1; thickness polynomial with the closed-trailing-edge coefficient
+    -0.1036), cosine-spaced: 2 n_half points from the trailing edge along the
+    lower surface to the leading edge and back along the upper surface."""
+    beta = np.linspace(0.0, np.pi, n_half + 1)
+    x = 0.5 * (1.0 - np.cos(beta))
+    yt = 5.0 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+    if m > 0.0:
+        fore = x < p
+        yc = np.where(fore, m / p ** 2 * (2 * p * x - x ** 2), m / (1 - p) ** 2 * ((1 - 2 * p) + 2 * p * x - x ** 2))
+        dyc = np.where(fore, 2 * m / p ** 2 * (p - x), 2 * m / (1 - p) ** 2 * (p - x))
+    else:
+        yc = np.zeros_like(x); dyc = np.zeros_like(x)
+    th = np.arctan(dyc)
+    xu, yu = x - yt * np.sin(th), yc + yt * np.cos(th)
+    xl, yl = x + yt * np.sin(th), yc - yt * np.cos(th)
+    lower = np.stack([xl[::-1], yl[::-1]], 1)          # TE -> LE
+    upper = np.stack([xu[1:-1], yu[1:-1]], 1)          # after LE -> before TE
+    return np.concatenate([lower, upper])
+
+
+def naca_ogrid(m: float = 0.02, p: float = 0.4, t: float = 0.12, n_surface: int = 200, n_layers: int = 100,
+               n_quad_layers: int = None, y1: float = 1.0e-5, radius: float = 20.0) -> Mesh:
+    """Hybrid O-grid around a NACA 4-digit section: n_surface points on the
+    section, n_layers layers out to a circle of the given radius (chords)
+    about mid-chord, the layer spacing growing geometrically from y1 at the
+    wall.  The inner n_quad_layers layers are quadrilaterals (the boundary
+    layer), the rest split into triangles (alternating diagonals).  Layers
+    leave the wall along its normals (the bisector at the trailing edge) and
+    then run straight to the circle point at the same arc-length fraction.
+    BCs: section SOLID_SURFACE, circle FARFIELD."""
+    if n_quad_layers is None:
+        n_quad_layers = n_layers // 2
+    S = naca4_surface(m, p, t, n_surface // 2)
+    n = S.shape[0]
+    seg = np.linalg.norm(np.roll(S, -1, 0) - S, axis=1)
+    s = np.concatenate([[0.0], np.cumsum(seg)[:-1]]) / seg.sum()
+    ang = -2.0 * np.pi * s                              # same turning sense as the section loop
+    Cc = np.stack([0.5 + radius * np.cos(ang), radius * np.sin(ang)], 1)
+    # layer fractions: first step y1/radius, geometric growth to 1
+    d0 = y1 / radius
+    lo, hi = 1.0 + 1e-12, 2.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if d0 * (r ** n_layers - 1.0) / (r - 1.0) > 1.0:
+            hi = r
+        else:
+            lo = r
+    f = np.concatenate([[0.0], np.cumsum(d0 * r ** np.arange(n_layers))])
+    f /= f[-1]
+    # within `reach` of the wall the layers follow the section's normals (the
+    # bisector at the trailing edge), so the boundary-layer cells are
+    # wall-normal; beyond it straight lines run on to the circle
+    tng = np.roll(S, -1, 0) - np.roll(S, 1, 0)
+    nrm = np.stack([-tng[:, 1], tng[:, 0]], 1)          # outward for the section's clockwise loop
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    reach = 0.05
+    d = (f * radius)[:, None, None]
+    E = S + reach * nrm
+    near = S[None] + np.minimum(d, reach) * nrm[None]
+    far = E[None] + np.clip((d - reach) / (radius - reach), 0.0, 1.0) * (Cc - E)[None]
+    P = np.where(d <= reach, near, far)                                 # [K+1, n, 2]
+    x, y = P[..., 0].ravel(), P[..., 1].ravel()
+    nid = lambda k, i: k * n + (i % n)
+    kk, ii = np.meshgrid(np.arange(n_layers), np.arange(n), indexing="ij")
+    a, b, c, d = nid(kk, ii), nid(kk, ii + 1), nid(kk + 1, ii + 1), nid(kk + 1, ii)
+    quad = kk < n_quad_layers
+    qa = np.stack([a[quad], b[quad], c[quad], d[quad]], 1)
+    tk, ti = kk[~quad], ii[~quad]
+    alt = (tk + ti) % 2 == 0
+    A, B, Cn, D = a[~quad], b[~quad], c[~quad], d[~quad]
+    t1 = np.where(alt[:, None], np.stack([A, B, Cn], 1), np.stack([A, B, D], 1))
+    t2 = np.where(alt[:, None], np.stack([A, Cn, D], 1), np.stack([B, Cn, D], 1))
+    tri = np.stack([t1, t2], 1).reshape(-1, 3)
+    poly = np.full((qa.shape[0] + tri.shape[0], 4), -1, np.int64)
+    poly[:qa.shape[0]] = qa
+    poly[qa.shape[0]:, :3] = tri
+    counts = np.concatenate([np.full(qa.shape[0], 4), np.full(tri.shape[0], 3)])
+    # counter-clockwise cells (shoelace area > 0)
+    idx = np.where(poly < 0, poly[:, :1], poly)
+    px, py = x[idx], y[idx]
+    kx = np.arange(4)[None, :] < counts[:, None]
+    nx_ = np.where(np.arange(4)[None, :] + 1 < counts[:, None], np.roll(px, -1, 1), px[:, :1])
+    ny_ = np.where(np.arange(4)[None, :] + 1 < counts[:, None], np.roll(py, -1, 1), py[:, :1])
+    area2 = np.where(kx, px * ny_ - nx_ * py, 0.0).sum(1)
+    cw = area2 < 0
+    for cnt in (3, 4):
+        sel = cw & (counts == cnt)
+        poly[sel, :cnt] = poly[sel, :cnt][:, ::-1]
+    nodes, lc, rc, nb = _faces_from_polygons_2d(poly, counts, x.shape[0])
+    wall = nodes[:nb].max(1) < n
+    bct = np.where(wall, SOLID, FAR).astype(np.int32)
+    nf = nodes.shape[0]
+    return Mesh(2, x, y, np.zeros_like(x), np.full(nf, 2, np.int32), nodes.ravel().astype(np.int32),
+                lc.astype(np.int32), rc.astype(np.int32), poly.shape[0], nb, bct,
+                meta=dict(kind="naca_ogrid", m=m, p=p, t=t, n_surface=n, n_layers=n_layers))
+
+
+def airfoil_cases(n_cases: int = 64, seed: int = 20261205, min_cells: int = 20000, max_cells: int = 400000):
+    """Seeded batch of 2-D RANS-SA airfoil solves: NACA 4-digit sections
+    (camber 0-6 % at 40 % chord, thickness 8-18 %), hybrid O-grids whose cell
+    counts are log-uniform in [min_cells, max_cells], Mach U(0.3, 0.8), AoA
+    U(-2, 8) degrees, Re log-uniform in [1e6, 1e7]; first-cell height for
+    y+ ~ 1.  Returns [(mesh, dict(mach, aoa, reynolds))]; the meshes carry no
+    wall distance (an SA solve computes it on the GPU)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_cases):
+        m, t = rng.uniform(0.0, 0.06), rng.uniform(0.08, 0.18)
+        cells = float(np.exp(rng.uniform(np.log(min_cells), np.log(max_cells))))
+        mach, aoa = rng.uniform(0.3, 0.8), rng.uniform(-2.0, 8.0)
+        re = float(np.exp(rng.uniform(np.log(1e6), np.log(1e7))))
+        # quads in the inner half of the layers, two triangles per cell outside:
+        # cells = n_s * 1.5 * n_layers with n_layers = n_s / 2
+        ns = int(round(np.sqrt(cells / 0.75) / 2.0)) * 2
+        nl = max(ns // 2, 8)
+        utau = np.sqrt(0.5 * 0.0592 * re ** -0.2)
+        mesh = naca_ogrid(m, 0.4, t, ns, nl, y1=1.0 / (utau * re))
+        out.append((mesh, dict(mach=mach, aoa=aoa, reynolds=re)))
+    return out

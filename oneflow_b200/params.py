@@ -90,3 +90,15 @@ def rans_plate(**kw) -> OfgParams:
                 reynolds=5.0e6, cflst=5.0, cfled=50.0, ncfl=200, precision=1)
     base.update(kw)
     return defaults(**base)
+
+
+def rans_airfoil(mach: float, aoa: float, reynolds: float, **kw) -> OfgParams:
+    """2-D RANS-SA airfoil (the batched cases): Roe, second order with
+    Green-Gauss gradients and the Venkatakrishnan limiter, LU-SGS,
+    colour-major sweeps, mixed precision.  (Least-squares gradients on the
+    curved, high-aspect-ratio O-grid cells near the wall drove the SA
+    production unstable within twenty iterations, in the oracle as well.)"""
+    base = dict(dimension=2, ischeme=1, ilim=2, igrad=0, vencat_coef=5.0, venkat_kh3=1, vismodel=3, mach_ref=mach,
+                aoa_degree=aoa, reynolds=reynolds, cflst=1.0, cfled=20.0, ncfl=200, precision=1, sweep_order=1)
+    base.update(kw)
+    return defaults(**base)

@@ -47,6 +47,11 @@ def load_library() -> C.CDLL:
     L.ofg_upload_state.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ofg_download_state.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ofg_calc_wall_dist.argtypes = [C.c_void_p]
+    L.ofg_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
+    L.ofg_batch_step.argtypes = [C.c_void_p, C.c_int]
+    L.ofg_batch_destroy.argtypes = [C.c_void_p]
+    L.ofg_batch_last_error.argtypes = [C.c_void_p]
+    L.ofg_batch_last_error.restype = C.c_char_p
     L.ofg_write_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_double]
     L.ofg_read_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     for name in ("ofg_zero_dq", "ofg_calc_time_step", "ofg_load_residuals", "ofg_update_residuals", "ofg_init_lusgs",
@@ -232,3 +237,36 @@ def colour_order(mesh: Mesh):
     if n < 0:
         raise OfgError(f"ofg_colour_order failed ({n})")
     return perm, n
+
+
+class Batch:
+    """Independent solves advanced together (ofg_batch_*): one CUDA-graph
+    launch per outer iteration for all of them, bitwise the same as
+    ``Solver.step`` on each.  Close the batch before its solvers."""
+
+    def __init__(self, solvers):
+        self.L = load_library()
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s.h.value for s in self.solvers])
+        h = C.c_void_p()
+        rc = self.L.ofg_batch_create(arr, len(self.solvers), C.byref(h))
+        if rc != 0:
+            raise OfgError(f"ofg_batch_create failed ({rc})")
+        self.h = h
+
+    def step(self, n: int = 1):
+        rc = self.L.ofg_batch_step(self.h, n)
+        if rc != 0:
+            msg = self.L.ofg_batch_last_error(self.h)
+            raise OfgError(f"error {rc}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ofg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
