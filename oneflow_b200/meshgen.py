@@ -459,3 +459,107 @@ def airfoil_cases(n_cases: int = 64, seed: int = 20261205, min_cells: int = 2000
         mesh = naca_ogrid(m, 0.4, t, ns, nl, y1=1.0 / (utau * re))
         out.append((mesh, dict(mach=mach, aoa=aoa, reynolds=re)))
     return out
+
+
+def _faces_3d(faces_list, owners, n_nodes):
+    """Shared-face extraction for 3-D cells: faces_list is a list of node
+    arrays [m, k] (k = 3 or 4, each face listed outward from its owner) with
+    owners [m].  Returns (face node lists, counts, lc, rc) with boundary faces
+    first (ordered by owner), interior faces ordered by (lc, rc); each face
+    keeps the node order of its lower-numbered cell, so its normal points
+    from lc to rc."""
+    keys, nodes, cnts, own = [], [], [], []
+    for F, O in zip(faces_list, owners):
+        k = F.shape[1]
+        s = np.sort(F, axis=1).astype(np.int64)
+        key = np.zeros(F.shape[0], np.int64) + k
+        for c in range(k):
+            key = key * n_nodes + s[:, c]
+        if k == 3:
+            key = key * n_nodes + n_nodes - 1      # distinct from any quad key
+        keys.append(key)
+        pad = np.full((F.shape[0], 4), -1, np.int64)
+        pad[:, :k] = F
+        nodes.append(pad); cnts.append(np.full(F.shape[0], k)); own.append(O)
+    key = np.concatenate(keys); nodes = np.concatenate(nodes); cnt = np.concatenate(cnts)
+    owner = np.concatenate(own)
+    order = np.lexsort((owner, key))
+    ks = key[order]
+    new = np.ones(ks.shape[0], bool)
+    new[1:] = ks[1:] != ks[:-1]
+    grp = np.cumsum(new) - 1
+    nf = int(grp[-1]) + 1
+    first = order[new]
+    num = np.bincount(grp, minlength=nf)
+    pos2 = np.flatnonzero(new) + 1
+    lc = owner[first]
+    rc = np.full(nf, -1, np.int64)
+    has2 = num == 2
+    rc[has2] = owner[order[pos2[has2]]]
+    fn, fc = nodes[first], cnt[first]
+    isb = rc < 0
+    forder = np.lexsort((rc, lc, ~isb))
+    return fn[forder], fc[forder], lc[forder], rc[forder], int(isb.sum())
+
+
+def bump_box_mixed(nx: int = 12, ny: int = 8, nz: int = 10, height: float = 0.15, jitter: float = 0.15,
+                   prism_from: int = None, seed: int = 20261203) -> Mesh:
+    """The bump box of bump_box_hexes with the columns i >= prism_from (default
+    nx/2) split into two triangular prisms each (through the diagonal of the
+    column's x-z quad), so hexahedra and prisms share quadrilateral side faces
+    and the floor carries quadrilateral and triangular wall faces.  BCs: floor
+    SOLID_SURFACE, the other sides FARFIELD."""
+    if prism_from is None:
+        prism_from = nx // 2
+    rng = np.random.default_rng(seed)
+    xs, ys, zs = np.linspace(0, 1, nx + 1), np.linspace(0, 1, ny + 1), np.linspace(0, 1, nz + 1)
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    Y = Y + height * np.exp(-((X - 0.5) ** 2 + (Z - 0.5) ** 2) / 0.05) * (1.0 - Y)
+    interior = np.zeros(X.shape, bool)
+    interior[1:-1, 1:-1, 1:-1] = True
+    h = np.array([1.0 / nx, 1.0 / ny, 1.0 / nz])
+    for A, hh in ((X, h[0]), (Y, h[1]), (Z, h[2])):
+        A += np.where(interior, rng.uniform(-jitter, jitter, A.shape) * hh, 0.0)
+    NY, NZ = ny + 1, nz + 1
+    x, y, z = X.ravel(), Y.ravel(), Z.ravel()
+    P = np.stack([x, y, z], 1)
+    nid = lambda i, j, k: (i * NY + j) * NZ + k
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    corner = np.stack([nid(ii + c[0], jj + c[1], kk + c[2]) for c in _CORNER], axis=1)
+    hexm = ii < prism_from
+    H = corner[hexm]
+    Pc = corner[~hexm]
+    # prism A: (c0 c1 c5 | c3 c2 c6), prism B: (c0 c5 c4 | c3 c6 c7), cells of a column adjacent
+    pa = Pc[:, [0, 1, 5, 3, 2, 6]]
+    pb = Pc[:, [0, 5, 4, 3, 6, 7]]
+    prisms = np.stack([pa, pb], 1).reshape(-1, 6)
+    nh, npr = H.shape[0], prisms.shape[0]
+    nc = nh + npr
+    # faces of each cell (any orientation; made outward below)
+    hq = H[:, _HEX_FACES].reshape(-1, 4); hq_own = np.repeat(np.arange(nh), 6)
+    tri_idx = np.array([[0, 1, 2], [3, 4, 5]]); quad_idx = np.array([[0, 1, 4, 3], [1, 2, 5, 4], [2, 0, 3, 5]])
+    pt = prisms[:, tri_idx].reshape(-1, 3); pt_own = nh + np.repeat(np.arange(npr), 2)
+    pq = prisms[:, quad_idx].reshape(-1, 4); pq_own = nh + np.repeat(np.arange(npr), 3)
+    cc = np.concatenate([P[H].mean(1), P[prisms].mean(1)])
+
+    def outward(F, own):
+        fcn = P[F].mean(1)
+        if F.shape[1] == 3:
+            n = np.cross(P[F[:, 1]] - P[F[:, 0]], P[F[:, 2]] - P[F[:, 0]])
+        else:
+            n = np.cross(P[F[:, 2]] - P[F[:, 0]], P[F[:, 3]] - P[F[:, 1]])
+        inward = np.einsum("ij,ij->i", n, fcn - cc[own]) < 0
+        F = F.copy()
+        F[inward] = F[inward][:, ::-1]
+        return F
+
+    fn, fc, lc, rc, nb = _faces_3d([outward(hq, hq_own), outward(pt, pt_own), outward(pq, pq_own)],
+                                   [hq_own, pt_own, pq_own], len(x))
+    floor_nodes = nid(*np.meshgrid(np.arange(nx + 1), [0], np.arange(nz + 1), indexing="ij")).ravel()
+    fb = fn[:nb]
+    on_floor = np.all(np.isin(np.where(fb < 0, floor_nodes[0], fb), floor_nodes), axis=1)
+    bct = np.where(on_floor, SOLID, FAR).astype(np.int32)
+    flat = fn[np.arange(4)[None, :] < fc[:, None]]          # row by row: each face's nodes in order
+    return Mesh(3, x, y, z, fc.astype(np.int32), flat.astype(np.int32), lc.astype(np.int32), rc.astype(np.int32),
+                nc, nb, bct, meta=dict(kind="bump_box_mixed", nx=nx, ny=ny, nz=nz, prism_from=prism_from, seed=seed))

@@ -21,7 +21,8 @@ walldist_<name>.npz holds the wall distance the reference computed itself
 (CALC_WALL_DIST, ireadwdst = 0) on the meshes of WALLDIST_CASES.
 
     python tests/golden/make_golden.py --restart-only   # only the restart fixtures
-    python tests/golden/make_golden.py --walldist-only  # only the wall-distance fixtures"""
+    python tests/golden/make_golden.py --walldist-only  # only the wall-distance fixtures
+    python tests/golden/make_golden.py --case=<name>    # one case fixture"""
 import json
 import os
 import sys
@@ -74,11 +75,16 @@ def main():
     if "--walldist-only" in sys.argv:
         walldist_fixtures()
         return
-    restart_fixtures()
+    if not any(a.startswith("--case=") for a in sys.argv):
+        restart_fixtures()
     if "--restart-only" in sys.argv:
         return
-    walldist_fixtures()
+    if not any(a.startswith("--case=") for a in sys.argv):
+        walldist_fixtures()
+    only = [a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--case=")]
     for name, spec in CASES.items():
+        if only and name not in only:
+            continue
         mesh, prm, steps = build(name)
         dump, rows = run_ref(mesh, prm, steps)
         out = {"q": dump["q"], "reshist": rows[:, 2:7], "params": json.dumps(P.to_dict(prm)), "steps": steps}

@@ -11,6 +11,7 @@ CASES = {
     "plate2d_sa_roe": dict(steps=30),
     "plate3d_sa_roe": dict(steps=10),
     "plate3d_sa_roe_colour_renumbered": dict(steps=10),
+    "mixed3d_slau2_gg_barth_sa": dict(steps=10),
 }
 # meshes whose wall distance the reference computed itself (ireadwdst = 0):
 # tests/golden/walldist_<name>.npz
@@ -45,6 +46,13 @@ def build(name):
         mesh = meshgen.plate_2d(32, 24, y1=1e-5, ratio=1.25)
         mesh.wall_dist = wall_distance(mesh)
         return mesh, P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=5e6, vismodel=3), steps
+    if name == "mixed3d_slau2_gg_barth_sa":
+        # hexahedra and prisms over a bump: SLAU2, Green-Gauss, Barth, SA at
+        # the transonic swept-wing condition (Mach 0.84, AoA 3.06, Re 1.2e7)
+        mesh = meshgen.bump_box_mixed()
+        mesh.wall_dist = wall_distance(mesh)
+        return mesh, P.defaults(dimension=3, ischeme=12, ilim=1, igrad=0, vismodel=3, mach_ref=0.84,
+                                aoa_degree=3.06, reynolds=1.2e7), steps
     mesh = meshgen.flat_plate_tets(8, 6, 4, ratio=1.3)
     mesh.wall_dist = plate_wall_distance(mesh)
     if name == "plate3d_sa_roe_colour_renumbered":
