@@ -713,8 +713,17 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) acc[e] = -0.0;   // LoadResiduals: res = -rhs, rhs = 0
         int b = A.nb_off[c], en = A.nb_off[c + 1];
+        // the next neighbour-list entry is loaded one face ahead, so that the
+        // loads of a face's records do not wait on its list entry
+        int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);
+        double qcD[NEQ];   // FP32 path: the FP64 cell values the face states start from
+        if constexpr (!exactOrder) {
+            ld4(A.q + (size_t)c * REC, qcD);
+            qcD[IP] = __ldg(A.q + (size_t)c * REC + IP);
+        }
         for (int k = b; k < en; ++k) {
-            int2 e2 = __ldg(&A.nbl[k]);
+            int2 e2 = e2n;
+            if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
             int f = nb_face(e2), nb = e2.y;
             bool right = nb_right(e2);
             R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
@@ -748,9 +757,6 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
             if constexpr (!exactOrder) {
                 // FP32 path: FP64 face states and central flux; the FP32
                 // dissipation and viscous term join before the FP64 accumulation
-                double qcD[NEQ];   // re-read per face (an L1 hit) rather than held in registers
-                ld4(A.q + (size_t)c * REC, qcD);
-                qcD[IP] = __ldg(A.q + (size_t)c * REC + IP);
                 const double *qlD = right ? qnD : qcD, *qrD = right ? qcD : qnD;
                 R fvs[NEQ];   // viscous term, formed first while fewer values are live
                 if (P.vismodel > 0) {
@@ -801,8 +807,10 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
         }
         if (exactOrder && doRes && P.vismodel > 0) {
             {
+                int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
                 for (int k = b; k < en; ++k) {
-                    int2 e2 = __ldg(&A.nbl[k]);
+                    int2 e2 = e2n;
+                    if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
                     int f = nb_face(e2), nb = e2.y;
                     bool right = nb_right(e2);
                     R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
@@ -951,8 +959,11 @@ template <typename R>
 __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *off, const int2 *list, double *rhs0) {
     R qc[REC];
     ld8(A.qs + (size_t)c * REC, qc);
-    for (int k = off[c]; k < off[c + 1]; ++k) {
-        int2 e2 = __ldg(&list[k]);
+    const int kb = off[c], ke = off[c + 1];
+    int2 e2n = kb < ke ? __ldg(&list[kb]) : make_int2(0, 0);   // list entry one face ahead
+    for (int k = kb; k < ke; ++k) {
+        int2 e2 = e2n;
+        if (k + 1 < ke) e2n = __ldg(&list[k + 1]);
         int f = nb_face(e2), nb = e2.y;
         R qn[REC], fg[FGR], dqj[DQR];
         ld8(A.qs + (size_t)nb * REC, qn);

@@ -180,8 +180,10 @@ __device__ __forceinline__ double turb_rhs_cell(const KArgs<R> &A, int c) {
     // FP64: pass 0 spectrum, then the source, pass 1 convection, pass 2
     // diffusion (the TurbCalcRHS order)
     for (int pass = 0; pass < (exactOrder ? 3 : 1); ++pass) {
+        int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
         for (int k = b; k < en; ++k) {
-            int2 e2 = __ldg(&A.nbl[k]);
+            int2 e2 = e2n;
+            if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
             int f = nb_face(e2), nb = e2.y;
             bool right = nb_right(e2);
             R qn[REC], cgn[CGR], fg[FGR];
