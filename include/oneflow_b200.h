@@ -197,6 +197,30 @@ int         ofg_batch_step(ofg_batch *batch, int nsteps);
 void        ofg_batch_destroy(ofg_batch *batch);
 const char *ofg_batch_last_error(const ofg_batch *batch);
 
+/* Coordinate MLP for warm starts (no counterpart in the reference): n_in
+   inputs -> depth hidden layers of `width` (a multiple of 16) with GELU ->
+   n_out outputs; BF16 weights and activations on the tensor cores with FP32
+   accumulation, FP32 master weights, Adam (beta 0.9 / 0.999, eps 1e-8), mean
+   squared error.  Weights start U(-1/sqrt(fan_in), 1/sqrt(fan_in)) from
+   `seed`, biases 0.  x, y are device arrays [n][n_in], [n][n_out] (FP32).
+   Parameters as one host array: per layer W[fan_in][fan_out], then b. */
+typedef struct ofg_mlp ofg_mlp;
+int         ofg_mlp_create(int n_in, int width, int depth, int n_out, uint64_t seed, ofg_mlp **out);
+void        ofg_mlp_destroy(ofg_mlp *mlp);
+const char *ofg_mlp_last_error(const ofg_mlp *mlp);
+int64_t     ofg_mlp_num_params(const ofg_mlp *mlp);
+int         ofg_mlp_get_params(ofg_mlp *mlp, float *out);
+int         ofg_mlp_set_params(ofg_mlp *mlp, const float *in);     /* also resets the Adam moments */
+int         ofg_mlp_predict(ofg_mlp *mlp, const float *x, int64_t n, float *y);
+/* loss and gradient (host, parameter layout) of one batch, n a multiple of
+   64 up to 65,536; no update */
+int         ofg_mlp_loss_grad(ofg_mlp *mlp, const float *x, const float *y, int64_t n, float *loss, float *grad);
+/* `steps` Adam steps at rate lr on minibatches of `batch` rows (a multiple of
+   64 up to 65,536) drawn by a seeded hash; loss_out[steps] (host, may be
+   NULL) gets each minibatch's loss */
+int         ofg_mlp_train(ofg_mlp *mlp, const float *x, const float *y, int64_t n, int batch, int steps, float lr,
+                          uint64_t seed, float *loss_out);
+
 /* RMS residual per equation of the solver's last UPDATE_RESIDUALS
    (ResidualTask::CalcRes + ResAver::CalcAver,
    codes/residual/src/ResidualTask.cpp:75-126, codes/residual/src/Residual.cpp:52-72):
