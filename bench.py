@@ -279,6 +279,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8-drop runs")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched airfoil runs")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start experiment")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -437,6 +438,10 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_throughput()
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        from oneflow_b200 import warmstart
+        learned = warmstart.run_experiment()
 
     clocks = clk.summary()
     if rank == 0:
@@ -452,7 +457,7 @@ def main():
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": int(l1 - l0), "clocks": clocks, "time_to_1e-8": conv,
                 "setup": {"calc_wall_dist_s": wall_s, "wall_dist_vs_closed_form": wall_err},
-                "batched": batched}
+                "batched": batched, "learned_warm_start": learned}
         print(json.dumps(line))
     if dist:
         dist.barrier()

@@ -1,0 +1,209 @@
+"""Learned warm start of steady solves: a coordinate MLP (BF16 tensor-core
+kernels, oneflow_b200.mlp) trained on converged solutions this solver
+produced, predicting the initial flow field of a new case.  The cold-started
+solve stays the fallback and the judge: a warm-started case counts as
+converged only when its RMS density residual falls below the same absolute
+threshold as the cold start's (the cold start's first residual x 1e-8).
+
+The case family here is the 2-D Euler bump channel (circular-arc bumps of
+thickness 4-10 % in a 3 x 1 channel, jittered triangles, Mach 0.3-0.6,
+first-order Roe, LU-SGS, colour-major sweeps, FP64): every case has its own
+mesh, so the network sees the geometry through its inputs."""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import meshgen, params as P
+from .solver import Batch, Solver
+
+GAMMA = 1.4
+FEATURES = ("x", "y", "wall_distance", "mach", "thickness", "bump_height_at_x", "y_over_channel", "mach^2")
+
+
+def bump_cases(n: int, seed: int, ni: int = 64, nj: int = 32):
+    """n seeded cases: (mesh, mach, thickness)"""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        t, mach = rng.uniform(0.04, 0.10), rng.uniform(0.3, 0.6)
+        mesh = meshgen.bump_channel(ni, nj, thickness=t, seed=int(rng.integers(1 << 31)))
+        out.append((mesh, mach, t))
+    return out
+
+
+def case_params(mach: float):
+    return P.euler_bump(mach_ref=mach, sweep_order=1)
+
+
+def features(solver: Solver, mach: float, t: float) -> np.ndarray:
+    """[nCells][8] inputs of the network for one case (cell centres, the wall
+    distance computed on the GPU, the case parameters, the local bump height)"""
+    N = solver.mesh.n_cells
+    x, y = solver.field("xcc")[:N], solver.field("ycc")[:N]
+    solver.calc_wall_dist()
+    d = solver.field("walldist")[:N]
+    r = (0.25 + t * t) / (2.0 * t)
+    yb = np.where((x > 1.0) & (x < 2.0), np.sqrt(np.maximum(r * r - (x - 1.5) ** 2, 0.0)) - (r - t), 0.0)
+    eta = (y - yb) / (1.0 - yb)
+    return np.stack([x, y, d, np.full(N, mach), np.full(N, t), yb, eta, np.full(N, mach * mach)], 1)
+
+
+def targets(q: np.ndarray, mach: float, n_cells: int) -> np.ndarray:
+    """[nCells][4] outputs: rho, u, v and p scaled by the free-stream pressure 1/(gamma M^2)"""
+    return np.stack([q[0, :n_cells], q[1, :n_cells], q[2, :n_cells], q[4, :n_cells] * GAMMA * mach * mach], 1)
+
+
+def state_from_prediction(pred: np.ndarray, mach: float, n_t: int) -> np.ndarray:
+    """primitive state [5][nT] from a prediction of the interior cells (ghost
+    entries start at a valid state and are reset by CALC_BOUNDARY)"""
+    n = pred.shape[0]
+    q = np.zeros((5, n_t))
+    q[0, :n], q[1, :n], q[2, :n] = pred[:, 0], pred[:, 1], pred[:, 2]
+    q[4, :n] = pred[:, 3] / (GAMMA * mach * mach)
+    q[0] = np.maximum(q[0], 1e-3)
+    q[4] = np.maximum(q[4], 1e-3 / (GAMMA * mach * mach))
+    q[:, n:] = q[:, :1]
+    return q
+
+
+def solve_to(solvers, threshold, batch: bool, chunk: int = 200, max_iters: int = 40000):
+    """Iterate the solvers until each one's RMS density residual is below its
+    threshold.  batch: one Batch for all (every case advances until the last
+    converges); else one after another.  Returns (iterations per case, None
+    where the limit came first; wall seconds) -- host wall clock around
+    synchronous calls."""
+    iters = [None] * len(solvers)
+
+    def check(k, s):
+        h = s.res_history()[:, 0]
+        hit = np.nonzero(h <= threshold[k])[0]
+        if hit.size:
+            iters[k] = int(hit[0]) + 1
+
+    t0 = time.perf_counter()
+    if batch:
+        b = Batch(solvers)
+        done = 0
+        while done < max_iters and any(i is None for i in iters):
+            b.step(chunk)
+            done += chunk
+            for k, s in enumerate(solvers):
+                if iters[k] is None:
+                    check(k, s)
+        b.close()
+    else:
+        for k, s in enumerate(solvers):
+            done = 0
+            while done < max_iters and iters[k] is None:
+                s.step(chunk)
+                done += chunk
+                check(k, s)
+    return iters, time.perf_counter() - t0
+
+
+def build_dataset(cases, drop: float = 1e-8):
+    """Converge every case (batched, cold start) and return the network's
+    inputs and outputs over all interior cells, and the iteration counts"""
+    solvers = []
+    for mesh, mach, t in cases:
+        s = Solver(mesh, case_params(mach))
+        s.init_flowfield()
+        solvers.append(s)
+    first = []
+    for s in solvers:   # the first residual of a cold start sets each case's threshold
+        s.step(1)
+        first.append(s.res_history()[0, 0])
+    iters, _ = solve_to(solvers, [f * drop for f in first], batch=True)
+    X, Y = [], []
+    for (mesh, mach, t), s in zip(cases, solvers):
+        X.append(features(s, mach, t))
+        Y.append(targets(s.state(), mach, mesh.n_cells))
+        s.close()
+    return np.concatenate(X), np.concatenate(Y), iters
+
+
+class Normaliser:
+    def __init__(self, a: np.ndarray):
+        self.mean = a.mean(0)
+        self.std = np.maximum(a.std(0), 1e-6)
+
+    def fwd(self, a):
+        return (a - self.mean) / self.std
+
+    def inv(self, a):
+        return a * self.std + self.mean
+
+
+def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth: int = 6, train_steps: int = 3000,
+                   batch: int = 8192, lr: float = 1e-3, seed: int = 20261206, drop: float = 1e-8):
+    """Train on n_train converged cases, then solve n_test held-out cases to
+    the same absolute threshold four ways: cold one after another (the plain
+    solve), cold batched, warm one after another, warm batched.  Returns a
+    dict of iterations, wall seconds and the training summary."""
+    import torch
+    from .mlp import MLP
+    t0 = time.perf_counter()
+    X, Y, _ = build_dataset(bump_cases(n_train, seed), drop)
+    t_data = time.perf_counter() - t0
+    nx, ny = Normaliser(X), Normaliser(Y)
+    xd = torch.tensor(nx.fwd(X), dtype=torch.float32, device="cuda").contiguous()
+    yd = torch.tensor(ny.fwd(Y), dtype=torch.float32, device="cuda").contiguous()
+    net = MLP(X.shape[1], width, depth, Y.shape[1], seed=seed)
+    t0 = time.perf_counter()
+    losses = net.train(xd, yd, steps=train_steps, batch=batch, lr=lr, seed=seed)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+
+    test = bump_cases(n_test, seed + 1)
+
+    def cold():
+        ss = []
+        for mesh, mach, t in test:
+            s = Solver(mesh, case_params(mach))
+            s.init_flowfield()
+            ss.append(s)
+        return ss
+
+    # thresholds from the cold starts' first residuals
+    thr = []
+    for s in cold():
+        s.step(1)
+        thr.append(s.res_history()[0, 0] * drop)
+        s.close()
+
+    def warm():
+        t0 = time.perf_counter()
+        ss = []
+        for mesh, mach, t in test:
+            s = Solver(mesh, case_params(mach))
+            s.init_flowfield()
+            f = torch.tensor(nx.fwd(features(s, mach, t)), dtype=torch.float32, device="cuda").contiguous()
+            pred = ny.inv(net.predict(f).cpu().numpy().astype(np.float64))
+            s.upload_state(state_from_prediction(pred, mach, s.nT))
+            ss.append(s)
+        return ss, time.perf_counter() - t0
+
+    out = {"family": "2-D Euler bump channels, 64x32 quads -> 4,096 jittered triangles each, bump thickness "
+                     "4-10 %, Mach 0.3-0.6, first-order Roe, LU-SGS, CFL 5, colour-major sweeps, FP64",
+           "features": list(FEATURES), "network": f"{X.shape[1]}->{depth}x{width} GELU->{Y.shape[1]}, BF16 WMMA",
+           "train_cases": n_train, "test_cases": n_test, "train_samples": int(X.shape[0]),
+           "train_steps": train_steps, "batch": batch, "lr": lr,
+           "loss_first": float(losses[0]), "loss_last": float(np.mean(losses[-50:])),
+           "data_s": t_data, "train_s": t_train, "threshold": f"cold first residual x {drop:g}"}
+    for name, is_warm, batched in (("plain", False, False), ("cold_batched", False, True),
+                                   ("warm", True, False), ("warm_batched", True, True)):
+        if is_warm:
+            ss, t_pred = warm()
+        else:
+            ss, t_pred = cold(), 0.0
+        it, t = solve_to(ss, thr, batch=batched)
+        out[name] = {"iterations_mean": float(np.mean([i if i is not None else np.nan for i in it])),
+                     "converged": int(sum(i is not None for i in it)), "seconds": t + t_pred,
+                     "predict_s": t_pred}
+        for s in ss:
+            s.close()
+    out["speedup_warm_batched_vs_plain"] = out["plain"]["seconds"] / out["warm_batched"]["seconds"]
+    net.close()
+    return out

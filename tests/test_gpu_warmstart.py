@@ -1,0 +1,29 @@
+"""Learned warm start end to end on a small budget: converged bump solutions
+from this solver train the BF16 tensor-core MLP, whose predictions start
+held-out cases; the cold-started solve is the judge -- every warm-started
+case must reach the cold start's absolute threshold (first residual x 1e-8),
+and it must get there in fewer iterations."""
+import numpy as np
+import pytest
+
+from oneflow_b200 import warmstart
+
+pytestmark = pytest.mark.gpu
+
+
+def test_warm_start_converges_to_the_cold_threshold_in_fewer_iterations():
+    r = warmstart.run_experiment(n_train=24, n_test=4, train_steps=400)
+    assert r["loss_last"] < 0.05 * r["loss_first"]
+    for k in ("plain", "cold_batched", "warm", "warm_batched"):
+        assert r[k]["converged"] == r["test_cases"], k
+    # batching changes nothing in the iterates (bitwise), so neither the counts
+    assert r["plain"]["iterations_mean"] == r["cold_batched"]["iterations_mean"]
+    assert r["warm"]["iterations_mean"] == r["warm_batched"]["iterations_mean"]
+    # measured 5,563 against 7,559 with this budget
+    assert r["warm"]["iterations_mean"] < 0.9 * r["plain"]["iterations_mean"]
+
+
+def test_prediction_state_is_physical():
+    pred = np.array([[1.0, 0.5, 0.0, 1.0], [-0.2, 0.4, 0.1, -1.0]])
+    q = warmstart.state_from_prediction(pred, 0.5, 5)
+    assert q.shape == (5, 5) and np.all(q[0] > 0) and np.all(q[4] > 0) and np.all(q[3] == 0)
