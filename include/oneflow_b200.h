@@ -87,7 +87,11 @@ typedef struct ofg_params {
                                 ids ascending inside a colour.  Identical to the
                                 reference run on the mesh renumbered that way
                                 (ofg_colour_order), with storage left in place. */
-    int    reserved_i[6];
+    int    time_integral;    /* 2 LU-SGS (TimeIntegral::Lusgs; 0 means 2), 1 the
+                                multi-stage scheme (TimeIntegral::RungeKutta) */
+    int    rk_stage;         /* stages of the multi-stage scheme (stage i scales
+                                its update by 1/(i+1), codes/global/src/Ctrl.cpp:72-77) */
+    int    reserved_i[4];
     double vencat_coef;
     double centropy1, centropy2;
     double cflst, cfled;
@@ -166,6 +170,14 @@ int ofg_download_state(ofg_ctx *ctx, int tid, double *q);
    rejected with OFG_E_ARG; file errors return OFG_E_IO. */
 int ofg_write_restart(ofg_ctx *ctx, int tid, const char *path, double curr_time);
 int ofg_read_restart(ofg_ctx *ctx, int tid, const char *path, int64_t *outer_step, double *curr_time);
+
+/* CALC_LHS of the multi-stage scheme (ULhs::CalcLHS, codes/usolver/src/ULhs.cpp:47-65):
+   res *= (dt / vol) * lhscoef, which is also the increment the next
+   UPDATE_FLOWFIELD adds (UNsField::Init makes dq the residual field under
+   MULTI_STAGE, codes/uns/src/UNsCom.cpp:85-88).  TimeIntegral::RungeKutta
+   (codes/solver/src/TimeIntegral.cpp:81-111) calls it once per stage with
+   lhscoef = 1/(stage+1).  NS solver only. */
+int ofg_calc_lhs(ofg_ctx *ctx, int tid, double lhscoef);
 
 /* One task each (system/ns/function/funcMap.txt, codes/turb/src/TurbSolverImp.cpp:33-42). */
 int ofg_zero_dq(ofg_ctx *ctx, int tid);             /* ZERO_DQ_FIELD          */

@@ -365,6 +365,7 @@ double host_sutherland(const DevParams &P, double t) {
 }
 
 bool has_turb(const ofg_ctx *c) { return c->p.vismodel >= 3; }
+bool multi_stage(const ofg_ctx *c) { return c->p.time_integral == 1; }
 
 int check_tid(ofg_ctx *c, int tid) {
     if (!c) return OFG_E_ARG;
@@ -400,6 +401,7 @@ void ofg_default_params(ofg_params *p) {
     p->max_time_ratio = 1.0e10; p->global_dt = 1.0e-3; p->mach_ref = 0.2; p->reynolds = 1.0e6;
     p->gama_ref = 1.4; p->prl = 0.72; p->prt = 0.9; p->tref_dim = 300.0; p->twall_dim = 300.0;
     p->inflow_viscosity = 0.01; p->rprod = 1.0; p->turb_cfl_ratio = 1.0; p->ref_sa = 0.1; p->max_vis_ratio = 1.0e6;
+    p->time_integral = 2; p->rk_stage = 1;
 }
 
 int ofg_create(const ofg_params *p, ofg_ctx **out) {
@@ -414,6 +416,9 @@ int ofg_create(const ofg_params *p, ofg_ctx **out) {
     if (p->vismodel != 0 && p->vismodel != 1 && p->vismodel != 3) return OFG_E_ARG;   // Euler, laminar, SA
     if (p->vismodel == 3 && p->turb_ilim != -1) return OFG_E_ARG;   // first-order SA convection only
     if (p->ivischeme != 0) return OFG_E_ARG;
+    if (p->time_integral < 0 || p->time_integral > 2) return OFG_E_ARG;
+    // the multi-stage scheme: NS solver only, 1..16 stages
+    if (p->time_integral == 1 && (p->rk_stage < 1 || p->rk_stage > 16 || p->vismodel == 3)) return OFG_E_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return OFG_E_CUDA;
     ofg_ctx *c = new ofg_ctx();
@@ -731,7 +736,7 @@ int ofg_write_restart(ofg_ctx *c, int tid, const char *path, double curr_time) {
     if ((rc = ofg_download_state(c, tid, rec.data()))) return rc;
     // the other NS state buffer holds the state one outer iteration earlier
     // once an iteration has completed from it
-    if (tid == OFG_NS_SOLVER && c->lastResBuf == (c->cur ^ 1)) {
+    if (tid == OFG_NS_SOLVER && c->lastResBuf == (c->cur ^ 1) && !(multi_stage(c) && c->p.rk_stage > 1)) {
         c->cur ^= 1;
         rc = ofg_download_state(c, tid, rec.data() + block);
         c->cur ^= 1;
@@ -788,6 +793,15 @@ int ofg_read_restart(ofg_ctx *c, int tid, const char *path, int64_t *outer_step,
     if (outer_step) *outer_step = step;
     if (curr_time) *curr_time = t;
     return OFG_OK;
+}
+
+int ofg_calc_lhs(ofg_ctx *c, int tid, double lhscoef) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if (tid != OFG_NS_SOLVER) return c->fail(OFG_E_ARG, "CALC_LHS is built for the NS solver");
+    if (c->lastResBuf != c->cur) return c->fail(OFG_E_STATE, "CALC_LHS needs UPDATE_RESIDUALS of the current state");
+    c->lhsCoef = lhscoef;
+    return launch(c, T_CALC_LHS);
 }
 
 int ofg_zero_dq(ofg_ctx *c, int tid) {
@@ -921,9 +935,32 @@ static int ensure_graphs(ofg_ctx *c) {
         cudaGraph_t graph;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         c->cur = g;
-        for (int t : kNsTasks) {
-            rc = c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
-            if (rc) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
+        auto run = [&](int t) {
+            return c->p.precision == OFG_PREC_MIXED ? launch_task_f32(c, t, c->stream) : launch_task_f64(c, t, c->stream);
+        };
+        if (multi_stage(c)) {
+            // TimeIntegral::RungeKutta (codes/solver/src/TimeIntegral.cpp:81-111): the
+            // time step once, then per stage the residual, CALC_LHS with
+            // lhscoef = 1/(stage+1), UPDATE_FLOWFIELD and CALC_BOUNDARY, each
+            // stage reading the buffer the previous one wrote.  (LOAD_Q copies q
+            // to a field UPDATE_FLOWFIELD never reads -- GetUpdateField,
+            // codes/update/src/Update.cpp:64-86, sets its pointer arguments by
+            // value -- so it has no effect on the iterates and is not run.)
+            const int st[] = {T_ADVANCE, T_TIMESTEP};
+            for (int t : st)
+                if ((rc = run(t))) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
+            for (int k = 0; k < c->p.rk_stage; ++k) {
+                c->cur = g ^ (k & 1);
+                c->lhsCoef = 1.0 / (k + 1);
+                const int stage[] = {T_RESIDUAL, T_CALC_LHS, T_UPDATE, T_BOUNDARY_NEXT};
+                for (int t : stage)
+                    if ((rc = run(t))) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
+            }
+            if ((rc = run(T_NORM))) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
+        } else {
+            for (int t : kNsTasks) {
+                if ((rc = run(t))) { cudaStreamEndCapture(c->stream, &graph); c->cur = saveCur; return rc; }
+            }
         }
         c->cur = g ^ 1;
         if (has_turb(c))
@@ -941,11 +978,13 @@ static int ensure_graphs(ofg_ctx *c) {
     return OFG_OK;
 }
 
-// host bookkeeping of one outer iteration launched from parity c->cur
+// host bookkeeping of one outer iteration launched from parity c->cur (the
+// multi-stage scheme moves between the two state buffers once per stage)
 static void account_step(ofg_ctx *c) {
     c->launches += c->graphKernels[c->cur];
-    c->lastResBuf = c->cur;   // this iteration's residual pass read the buffer it started from
-    c->cur ^= 1;
+    int flips = multi_stage(c) ? c->p.rk_stage : 1;
+    c->lastResBuf = c->cur ^ ((flips - 1) & 1);   // the buffer the last residual pass read
+    c->cur ^= flips & 1;
     c->outerSteps++;
 }
 

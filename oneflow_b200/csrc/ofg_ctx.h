@@ -39,6 +39,7 @@ struct ofg_ctx {
     double *d_q[2] = {nullptr, nullptr};
     float *d_qs[2] = {nullptr, nullptr};                    // FP32 copies of the state records (mixed path)
     int cur = 0;
+    double lhsCoef = 1.0;       // lhscoef of the next CALC_LHS (multi-stage scheme)
     int lastResBuf = -1;        // state buffer of the last residual pass (-1: none since the state was set)
     bool pendingNext = false;   // UPDATE_FLOWFIELD wrote d_q[cur^1], CALC_BOUNDARY not yet run
     bool pendingTurb = false;   // SA UPDATE_FLOWFIELD ran, its CALC_BOUNDARY not yet
@@ -84,7 +85,7 @@ enum Task {
     T_TURB_NORM_ONLY,
     // parts of T_TS_RES / T_TURB_RHS, timed separately by ofg_profile_step
     T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_P_TURB_GRAD, T_P_TURB_FLUX,
-    T_FORCES, T_GRAD_ONLY
+    T_FORCES, T_GRAD_ONLY, T_CALC_LHS
 };
 int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);
 int launch_task_f32(ofg_ctx *c, int task, cudaStream_t s);

@@ -1012,6 +1012,39 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::sw) k_lusgs_upper(KArgs<R> 
 }
 
 // ---------------------------------------------------------------------------
+// CALC_LHS of the multi-stage scheme: ULhs::CalcLHS (codes/usolver/src/ULhs.cpp:47-65),
+// res *= (dt / vol) * lhscoef in place.  Under MULTI_STAGE the update's
+// increment field is the residual itself (UNsField::Init,
+// codes/uns/src/UNsCom.cpp:85-88), so the scaled values also go to the
+// increment records UPDATE_FLOWFIELD adds; and the residual history of the
+// iteration is the norm of this scaled residual (ResidualTask::CalcRes reads
+// the residual field after the last stage), so the per-block sums of squares
+// are written again here.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(128) k_calc_lhs(KArgs<R> A, double coef) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double sq[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (c < A.nCells) {
+        double f = (A.dt[c] / double(A.cgeo[(size_t)c * CGR + 3])) * coef;
+        double *r = A.res + (size_t)c * NEQ;
+        R d[DQR];
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) {
+            double v = r[e] * f;
+            r[e] = v;
+            sq[e] = v * v;
+            d[e] = R(v);
+        }
+#pragma unroll
+        for (int e = NEQ; e < DQR; ++e) d[e] = R(0);
+        st4(A.dq + (size_t)c * DQR, d);
+        st4(A.dq + (size_t)c * DQR + 4, d + 4);
+    }
+    block_sum_to<NEQ>(sq, A.npart + (size_t)blockIdx.x * NEQ);
+}
+
+// ---------------------------------------------------------------------------
 // UPDATE_FLOWFIELD_LUSGS: NsUpdate::CalcFlowField + WeekSolutionFix
 // (codes/ns/src/NsUpdate.cpp:40-67,192-217), QToPrim (codes/ns/src/NsInvFlux.cpp:1377-1399);
 // then the interior half of CALC_BOUNDARY: NsCalcGamaT + CalcLaminarViscosity.

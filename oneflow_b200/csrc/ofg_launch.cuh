@@ -121,6 +121,11 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         if (task == T_TS_RES || task == T_P_CLIP) OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }
+    case T_CALC_LHS: {   // CALC_LHS of the multi-stage scheme (same 128-cell blocks as the norm partials)
+        KArgs<R> A = make_args<R>(c, false);
+        OFG_LAUNCH(k_calc_lhs<R>, nblk(N, 128), 128, s, A, c->lhsCoef);
+        break;
+    }
     case T_LOWER: {
         KArgs<R> A = make_args<R>(c, false);
         int nl = int(c->lowOff.size()) - 1;

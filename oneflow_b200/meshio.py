@@ -171,7 +171,8 @@ def write_case(case_dir: str, mesh: Mesh, params: dict, max_steps: int, start_st
             ("Real", "cflst", p["cflst"]), ("Real", "cfled", p["cfled"]), ("int", "ncfl", p["ncfl"]),
             ("Real", "max_time_ratio", p["max_time_ratio"]), ("int", "visSRModel", p["visSRModel"]),
             ("int", "visTimeStepModel", p["visTimeStepModel"]), ("int", "chemModel", 0),
-            ("int", "idualtime", 0), ("int", "time_integral", 2), ("int", "rk_stage", 1),
+            ("int", "idualtime", 0), ("int", "time_integral", p.get("time_integral", 2) or 2),
+            ("int", "rk_stage", p.get("rk_stage", 1)),
             ("int", "linearTwoStepMethods", 1), ("int", "ischeme", p["ischeme"]),
             ("int", "ivischeme", p["ivischeme"]), ("int", "ieigenfix", p["ieigenfix"]),
             ("Real", "centropy1", p["centropy1"]), ("Real", "centropy2", p["centropy2"]),

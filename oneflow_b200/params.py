@@ -9,14 +9,14 @@ import ctypes as C
 
 _INT = ["dimension", "ischeme", "ilim", "igrad", "ieigenfix", "timestepModel", "ncfl", "visSRModel",
         "visTimeStepModel", "vismodel", "ivischeme", "isowallbc", "iprod_sa", "ft2_flag", "turb_ilim",
-        "precision", "venkat_kh3", "sweep_order"]
+        "precision", "venkat_kh3", "sweep_order", "time_integral", "rk_stage"]
 _DBL = ["vencat_coef", "centropy1", "centropy2", "cflst", "cfled", "max_time_ratio", "global_dt", "mach_ref",
         "aoa_degree", "sideslip_degree", "reynolds", "gama_ref", "prl", "prt", "tref_dim", "twall_dim",
         "inflow_viscosity", "rprod", "turb_cfl_ratio", "ref_sa", "max_vis_ratio"]
 
 
 class OfgParams(C.Structure):
-    _fields_ = ([(n, C.c_int) for n in _INT] + [("reserved_i", C.c_int * 6)] +
+    _fields_ = ([(n, C.c_int) for n in _INT] + [("reserved_i", C.c_int * 4)] +
                 [(n, C.c_double) for n in _DBL] + [("reserved_d", C.c_double * 6)])
 
 
@@ -42,6 +42,8 @@ def defaults(**kw) -> OfgParams:
     p.turb_ilim = -1
     p.precision = 0
     p.venkat_kh3 = 0
+    p.time_integral = 2
+    p.rk_stage = 1
     p.vencat_coef = 0.0001
     p.centropy1 = 0.0001
     p.centropy2 = 0.0001

@@ -47,6 +47,7 @@ def load_library() -> C.CDLL:
     L.ofg_upload_state.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ofg_download_state.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ofg_calc_wall_dist.argtypes = [C.c_void_p]
+    L.ofg_calc_lhs.argtypes = [C.c_void_p, C.c_int, C.c_double]
     L.ofg_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]
     L.ofg_batch_step.argtypes = [C.c_void_p, C.c_int]
     L.ofg_batch_destroy.argtypes = [C.c_void_p]
@@ -164,6 +165,10 @@ class Solver:
     # ---- tasks ----
     def task(self, name: str, tid: int = NS_SOLVER):
         self._check(getattr(self.L, TASKS[name])(self.h, tid))
+
+    def calc_lhs(self, lhscoef: float, tid: int = NS_SOLVER):
+        """CALC_LHS of the multi-stage scheme (ofg_calc_lhs): res *= dt/vol * lhscoef."""
+        self._check(self.L.ofg_calc_lhs(self.h, tid, C.c_double(lhscoef)))
 
     def set_outer_step(self, n: int):
         """Iteration::outerSteps as seen by the next CALC_TIME_STEP (task API)."""

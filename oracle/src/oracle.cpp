@@ -1371,10 +1371,40 @@ struct Oracle {
         calcBoundary();
     }
 
+    // CALC_LHS, ULhs::CalcLHS (codes/usolver/src/ULhs.cpp:47-65): res *= (dt/vol)
+    // * lhscoef; under MULTI_STAGE the update's increment field is the residual
+    // itself (UNsField::Init, codes/uns/src/UNsCom.cpp:85-88)
+    void calcLhs(double lhscoef) {
+        for (int e = 0; e < NEQ; ++e)
+            for (int c = 0; c < nCells; ++c) {
+                res[e][c] *= (timestep[c] / vol[c]) * lhscoef;
+                dq[e][c] = res[e][c];
+            }
+    }
+    // TimeIntegral::RungeKutta (codes/solver/src/TimeIntegral.cpp:81-111) on the
+    // finest grid: the time step once, then per stage the residual, CALC_LHS
+    // with lhscoef = rk_coef[stage] = 1/(stage+1) (Ctrl::Init,
+    // codes/global/src/Ctrl.cpp:72-77), UPDATE_FLOWFIELD from the current state
+    // and CALC_BOUNDARY.  LOAD_Q stores q in a field that UPDATE_FLOWFIELD does
+    // not read (GetUpdateField, codes/update/src/Update.cpp:64-86, assigns its
+    // pointer parameters by value), so it changes nothing here.
+    void nsRelaxMultiStage() {
+        calcTimeStep();
+        for (int k = 0; k < p.rk_stage; ++k) {
+            loadResiduals();
+            updateResiduals();
+            calcLhs(1.0 / (k + 1));
+            updateFlowfield();
+            calcBoundary();
+        }
+    }
+
     int step(int n) {
         for (int it = 0; it < n; ++it) {
             ++outerSteps;
-            nsRelax();   // MG::StrongIter: NS relaxation, then the turbulence solver
+            // MG::StrongIter: NS relaxation, then the turbulence solver
+            if (p.time_integral == 1) nsRelaxMultiStage();
+            else nsRelax();
             if (turb()) turbRelax();
             double rms[NEQ]; bool nan;
             residualRms(rms, &nan);

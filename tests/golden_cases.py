@@ -12,6 +12,8 @@ CASES = {
     "plate3d_sa_roe": dict(steps=10),
     "plate3d_sa_roe_colour_renumbered": dict(steps=10),
     "mixed3d_slau2_gg_barth_sa": dict(steps=10),
+    "bump_euler_rk3": dict(steps=30),
+    "plate2d_laminar_roe_rk2": dict(steps=30),
 }
 # meshes whose wall distance the reference computed itself (ireadwdst = 0):
 # tests/golden/walldist_<name>.npz
@@ -35,6 +37,12 @@ RESTART_CASES = {"bump_euler_roe_venkat": 20, "plate2d_sa_roe": 20}
 
 def build(name):
     steps = CASES[name]["steps"]
+    if name == "bump_euler_rk3":
+        # the multi-stage scheme (TimeIntegral::RungeKutta), 3 stages, CFL 0.8
+        return meshgen.bump_channel(32, 16), P.euler_bump(time_integral=1, rk_stage=3, cflst=0.8, cfled=0.8), steps
+    if name == "plate2d_laminar_roe_rk2":
+        return meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5, vismodel=1,
+                                                     time_integral=1, rk_stage=2, cflst=0.5, cfled=0.5), steps
     if name.startswith("bump"):
         mesh = meshgen.bump_channel(32, 16)
         kw = {"bump_euler_roe1": {}, "bump_euler_roe_venkat": dict(ilim=2, vencat_coef=0.05),

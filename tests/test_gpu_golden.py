@@ -69,3 +69,21 @@ def test_mixed_mesh_fp32_face_path_tracks_fp64():
     b = Solver(mesh, prm1); b.init_flowfield(); b.step(steps)
     qa, qb = a.state(), b.state()
     assert np.abs(qb - qa).max() / np.abs(qa).max() < 1e-4
+
+
+def test_multi_stage_task_by_task_equals_the_fused_iteration():
+    # TimeIntegral::RungeKutta through the task entry points, stage by stage,
+    # against ofg_step's captured iteration: bitwise
+    mesh, prm, _ = build("bump_euler_rk3")
+    a = Solver(mesh, prm); a.init_flowfield(); a.step(4)
+    b = Solver(mesh, prm); b.init_flowfield()
+    for it in range(4):
+        b.set_outer_step(it + 1)
+        b.task("CALC_TIME_STEP")
+        for k in range(prm.rk_stage):
+            b.task("LOAD_RESIDUALS")
+            b.task("UPDATE_RESIDUALS")
+            b.calc_lhs(1.0 / (k + 1))
+            b.task("UPDATE_FLOWFIELD_LUSGS")
+            b.task("CALC_BOUNDARY")
+    assert np.array_equal(a.state(), b.state())
