@@ -240,6 +240,13 @@ int         ofg_mlp_train(ofg_mlp *mlp, const float *x, const float *y, int64_t 
    history is not touched. */
 int ofg_residual_norms(ofg_ctx *ctx, int tid, double *rms);
 
+/* Largest |residual| per equation of the solver's last UPDATE_RESIDUALS and
+   the first cell (lowest index) that holds it -- the resmax record of
+   ResidualTask::CalcRes (codes/residual/src/ResidualTask.cpp:91-123; its
+   centre and volume are the fields "xcc".."vol" at that index).  resmax and
+   cell get 5 entries (NS) or 1 (SA). */
+int ofg_residual_max(ofg_ctx *ctx, int tid, double *resmax, int64_t *cell);
+
 /* Named device field -> host, reference layout:
    "res","dq","timestep","invsr","vissr","impsr","limiter","dqdx","dqdy","dqdz",
    "tempr","visl","vist","vol","xcc","ycc","zcc","area","xfn","yfn","zfn",

@@ -1092,6 +1092,65 @@ int ofg_batch_step(ofg_batch *b, int nsteps) {
     return OFG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Largest |residual| per equation and the first cell holding it
+// (ResidualTask::CalcRes, codes/residual/src/ResidualTask.cpp:91-107: a strict
+// comparison in ascending cell order keeps the first).  Per 128-cell block:
+// out[block][e] = the block's maximum, out[block][neq + e] = its lowest cell
+// index (as a double, exact), combined on the host in block order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_res_max(const double *res, int n, int neq, double *out) {
+    __shared__ double sv[128];
+    __shared__ int si[128];
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int e = 0; e < neq; ++e) {
+        sv[threadIdx.x] = c < n ? fabs(res[(size_t)c * neq + e]) : -1.0;
+        si[threadIdx.x] = c;
+        __syncthreads();
+        for (int w = 64; w > 0; w >>= 1) {
+            if (threadIdx.x < w) {
+                double a = sv[threadIdx.x], b = sv[threadIdx.x + w];
+                if (b > a || (b == a && si[threadIdx.x + w] < si[threadIdx.x])) {
+                    sv[threadIdx.x] = b;
+                    si[threadIdx.x] = si[threadIdx.x + w];
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            out[(size_t)blockIdx.x * 2 * neq + e] = sv[0];
+            out[(size_t)blockIdx.x * 2 * neq + neq + e] = double(si[0]);
+        }
+        __syncthreads();
+    }
+}
+
+int ofg_residual_max(ofg_ctx *c, int tid, double *resmax, int64_t *cell) {
+    int rc = check_tid(c, tid);
+    if (rc) return rc;
+    if (!resmax || !cell) return c->fail(OFG_E_ARG, "null output");
+    bool turb = tid == OFG_TURB_SOLVER;
+    const int neq = turb ? 1 : NEQ, n = c->nCells, nb = (n + 127) / 128;
+    if ((size_t)nb * 2 * neq > c->nPartialMax) return c->fail(OFG_E_ARG, "partials buffer too small");
+    k_res_max<<<nb, 128, 0, c->stream>>>(turb ? c->d_resT : c->d_res, n, neq, c->d_partial);
+    CK(cudaGetLastError());
+    c->launches++;
+    std::vector<double> part((size_t)nb * 2 * neq);
+    CK(cudaMemcpyAsync(part.data(), c->d_partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    for (int e = 0; e < neq; ++e) {
+        double m = -1.0;
+        int64_t at = 0;
+        for (int b = 0; b < nb; ++b) {   // ascending blocks: the first cell wins ties
+            double v = part[(size_t)b * 2 * neq + e];
+            if (v > m) { m = v; at = int64_t(part[(size_t)b * 2 * neq + neq + e]); }
+        }
+        resmax[e] = m;
+        cell[e] = at;
+    }
+    return OFG_OK;
+}
+
 int ofg_residual_norms(ofg_ctx *c, int tid, double *rms) {
     int rc = check_tid(c, tid);
     if (rc) return rc;

@@ -60,6 +60,7 @@ def load_library() -> C.CDLL:
         getattr(L, name).argtypes = [C.c_void_p, C.c_int]
     L.ofg_step.argtypes = [C.c_void_p, C.c_int]
     L.ofg_residual_norms.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ofg_residual_max.argtypes = [C.c_void_p, C.c_int, _dp, np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")]
     L.ofg_forces.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
     L.ofg_download_field.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
     L.ofg_get_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
@@ -209,6 +210,15 @@ class Solver:
         out = np.zeros(5, np.float64)
         self._check(self.L.ofg_residual_norms(self.h, tid, out))
         return out if tid == NS_SOLVER else out[:1]
+
+    def residual_max(self, tid: int = NS_SOLVER):
+        """(largest |residual| per equation, first cell holding it) of the last
+        UPDATE_RESIDUALS: 5 entries (NS) or 1 (SA)."""
+        v = np.zeros(5, np.float64)
+        i = np.zeros(5, np.int64)
+        self._check(self.L.ofg_residual_max(self.h, tid, v, i))
+        n = 5 if tid == NS_SOLVER else 1
+        return v[:n], i[:n]
 
     def field(self, name: str, tid: int = NS_SOLVER) -> np.ndarray:
         need = C.c_int64()

@@ -87,3 +87,21 @@ def test_multi_stage_task_by_task_equals_the_fused_iteration():
             b.task("UPDATE_FLOWFIELD_LUSGS")
             b.task("CALC_BOUNDARY")
     assert np.array_equal(a.state(), b.state())
+
+
+@pytest.mark.parametrize("name", ["bump_euler_roe_venkat", "plate2d_sa_roe"])
+def test_residual_max_and_its_cell(name):
+    # ResidualTask's resmax record: the largest |res| per equation and the
+    # first cell (in cell order) that holds it
+    mesh, prm, _ = build(name)
+    g = Solver(mesh, prm)
+    g.init_flowfield()
+    g.step(3)
+    N, nT = mesh.n_cells, mesh.n_cells + mesh.n_bfaces
+    r = np.abs(g.field("res").reshape(5, -1)[:, :N])
+    v, i = g.residual_max()
+    assert np.array_equal(v, r.max(1)) and np.array_equal(i, r.argmax(1))
+    if prm.vismodel >= 3:
+        t = np.abs(g.field("turbres", TURB_SOLVER)[:N])
+        v, i = g.residual_max(TURB_SOLVER)
+        assert v[0] == t.max() and i[0] == t.argmax()
