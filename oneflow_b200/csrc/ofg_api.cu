@@ -330,6 +330,7 @@ void derive_params(ofg_ctx *c) {
     d.visTimeStepModel = p.visTimeStepModel; d.ieigenfix = p.ieigenfix; d.timestepModel = p.timestepModel;
     d.isowallbc = p.isowallbc; d.dim = p.dimension; d.precision = p.precision; d.venkat_kh3 = p.venkat_kh3;
     d.igrad = p.igrad;
+    d.ivischeme = p.ivischeme;
     d.gama = p.gama_ref; d.centropy1 = p.centropy1; d.centropy2 = p.centropy2; d.vencat_coef = p.vencat_coef;
     d.reynolds = p.reynolds; d.oreynolds = 1.0 / p.reynolds; d.oprl = 1.0 / p.prl; d.oprt = 1.0 / p.prt;
     d.const_cp = 1.0 / ((p.gama_ref - 1.0) * (p.mach_ref * p.mach_ref));
@@ -415,7 +416,7 @@ int ofg_create(const ofg_params *p, ofg_ctx **out) {
     if (p->sweep_order != 0 && p->sweep_order != 1) return OFG_E_ARG;
     if (p->vismodel != 0 && p->vismodel != 1 && p->vismodel != 3) return OFG_E_ARG;   // Euler, laminar, SA
     if (p->vismodel == 3 && p->turb_ilim != -1) return OFG_E_ARG;   // first-order SA convection only
-    if (p->ivischeme != 0) return OFG_E_ARG;
+    if (p->ivischeme != 0 && p->ivischeme != 1) return OFG_E_ARG;   // VIS_STD, VIS_AVER
     if (p->time_integral < 0 || p->time_integral > 2) return OFG_E_ARG;
     // the multi-stage scheme: NS solver only, 1..16 stages
     if (p->time_integral == 1 && (p->rk_stage < 1 || p->rk_stage > 16 || p->vismodel == 3)) return OFG_E_ARG;

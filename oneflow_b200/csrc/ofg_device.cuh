@@ -73,7 +73,7 @@ template <typename R> __device__ __forceinline__ R SQR3(R a, R b, R c) { return 
 // codes/chemical/src/Chemical.cpp:280-340, codes/ns/src/NsCom.cpp:45-94).
 struct DevParams {
     int ischeme, ilim, vismodel, visSRModel, visTimeStepModel, ieigenfix, timestepModel, isowallbc;
-    int dim, precision, venkat_kh3, igrad;
+    int dim, precision, venkat_kh3, igrad, ivischeme;
     double gama, centropy1, centropy2, vencat_coef, reynolds, oreynolds, oprl, oprt, const_cp, statecoef;
     double inflow[NEQ];
     double twall, sutherland_ts, max_time_ratio, global_dt;

@@ -616,7 +616,9 @@ __device__ __forceinline__ void face_states_mixed(const KArgs<float> &A, int f, 
     }
 }
 
-// viscous face flux with the VIS_STD face gradient, before the -S/Re factor
+// viscous face flux with the VIS_STD face gradient (VIS_AVER: the average of
+// the cell gradients, UNsVisFlux::AverMethod, codes/uns/src/UNsVisFlux.cpp:357-366),
+// before the -S/Re factor
 // (UNsVisFlux::PrepareFaceValue/StdMethod/CalcStress/CalcNsVisFlux,
 // codes/usolver/src/VisGrad.cpp:150-175,356-366)
 // dlr: qr - ql of the six gradient variables (rho, u, v, w, p, T)
@@ -638,10 +640,12 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
         gx[v] = half * (gl[v * 3] + gr[v * 3]);
         gy[v] = half * (gl[v * 3 + 1] + gr[v * 3 + 1]);
         gz[v] = half * (gl[v * 3 + 2] + gr[v * 3 + 2]);
-        R fOld = gx[v] * dx + gy[v] * dy + gz[v] * dz;
-        R fnew = dlr[v] * ods;
-        R df = fnew - fOld;
-        gx[v] += df * dx; gy[v] += df * dy; gz[v] += df * dz;
+        if (P.ivischeme != 1) {   // VIS_STD's CorrectGrad; VIS_AVER keeps the average
+            R fOld = gx[v] * dx + gy[v] * dy + gz[v] * dz;
+            R fnew = dlr[v] * ods;
+            R df = fnew - fOld;
+            gx[v] += df * dx; gy[v] += df * dy; gz[v] += df * dz;
+        }
     }
     R xn = fg[0], yn = fg[1], zn = fg[2];
     R dtdn = xn * gx[5] + yn * gy[5] + zn * gz[5];

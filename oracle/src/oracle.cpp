@@ -829,11 +829,14 @@ struct Oracle {
                 double ax2 = e < NEQ ? dqdx[e][r] : dtdx[r], ay2 = e < NEQ ? dqdy[e][r] : dtdy[r], az2 = e < NEQ ? dqdz[e][r] : dtdz[r];
                 qm[e] = half * (q1 + q2);
                 gx[e] = half * (ax1 + ax2); gy[e] = half * (ay1 + ay2); gz[e] = half * (az1 + az2);
-                // CorrectGrad, VisGrad.cpp:356-366
-                double fOld = gx[e] * dx + gy[e] * dy + gz[e] * dz;
-                double fnew = (q2 - q1) * ods;
-                double df = fnew - fOld;
-                gx[e] += df * dx; gy[e] += df * dy; gz[e] += df * dz;
+                // CorrectGrad, VisGrad.cpp:356-366 (VIS_STD); VIS_AVER keeps the
+                // average (UNsVisFlux::AverMethod, codes/uns/src/UNsVisFlux.cpp:357-366)
+                if (p.ivischeme != 1) {
+                    double fOld = gx[e] * dx + gy[e] * dy + gz[e] * dz;
+                    double fnew = (q2 - q1) * ods;
+                    double df = fnew - fOld;
+                    gx[e] += df * dx; gy[e] += df * dy; gz[e] += df * dz;
+                }
             }
             double xn = xfn[f], yn = yfn[f], zn = zfn[f];
             double dtdn = xn * gx[5] + yn * gy[5] + zn * gz[5];

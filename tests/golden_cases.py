@@ -14,6 +14,7 @@ CASES = {
     "mixed3d_slau2_gg_barth_sa": dict(steps=10),
     "bump_euler_rk3": dict(steps=30),
     "plate2d_laminar_roe_rk2": dict(steps=30),
+    "plate2d_laminar_roe_visaver": dict(steps=30),
 }
 # meshes whose wall distance the reference computed itself (ireadwdst = 0):
 # tests/golden/walldist_<name>.npz
@@ -43,6 +44,10 @@ def build(name):
     if name == "plate2d_laminar_roe_rk2":
         return meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5, vismodel=1,
                                                      time_integral=1, rk_stage=2, cflst=0.5, cfled=0.5), steps
+    if name == "plate2d_laminar_roe_visaver":
+        # VIS_AVER viscous face gradient (ivischeme = 1)
+        return meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5, vismodel=1,
+                                                     ivischeme=1), steps
     if name.startswith("bump"):
         mesh = meshgen.bump_channel(32, 16)
         kw = {"bump_euler_roe1": {}, "bump_euler_roe_venkat": dict(ilim=2, vencat_coef=0.05),
