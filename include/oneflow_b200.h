@@ -73,7 +73,7 @@ typedef struct ofg_params {
     int    visSRModel;       /* 1,2,3                                          */
     int    visTimeStepModel;
     int    vismodel;         /* 0 Euler, 1 laminar, 3 SA                       */
-    int    ivischeme;        /* 0 std (face average + correction), 1 aver      */
+    int    ivischeme;        /* 0 std, 1 aver, 2 test, 3 new1, 4 new2         */
     int    isowallbc;        /* 0 adiabatic, 1 isothermal                      */
     int    iprod_sa;         /* SA production form                             */
     int    ft2_flag;

@@ -416,7 +416,7 @@ int ofg_create(const ofg_params *p, ofg_ctx **out) {
     if (p->sweep_order != 0 && p->sweep_order != 1) return OFG_E_ARG;
     if (p->vismodel != 0 && p->vismodel != 1 && p->vismodel != 3) return OFG_E_ARG;   // Euler, laminar, SA
     if (p->vismodel == 3 && p->turb_ilim != -1) return OFG_E_ARG;   // first-order SA convection only
-    if (p->ivischeme != 0 && p->ivischeme != 1) return OFG_E_ARG;   // VIS_STD, VIS_AVER
+    if (p->ivischeme < 0 || p->ivischeme > 4) return OFG_E_ARG;   // VIS_STD, AVER, TEST, NEW1, NEW2
     if (p->time_integral < 0 || p->time_integral > 2) return OFG_E_ARG;
     // the multi-stage scheme: NS solver only, 1..16 stages
     if (p->time_integral == 1 && (p->rk_stage < 1 || p->rk_stage > 16 || p->vismodel == 3)) return OFG_E_ARG;

@@ -616,15 +616,133 @@ __device__ __forceinline__ void face_states_mixed(const KArgs<float> &A, int f, 
     }
 }
 
+// Face geometry of the VIS_TEST / VIS_NEW1 / VIS_NEW2 face gradients: the
+// distance weights and normal offsets of VisGradGeom::CalcFaceWeight /
+// PrepareCellGeom (codes/usolver/src/VisGrad.cpp:44-97) and the face tangents
+// of GCom::CalcTangent (codes/global/src/Com.cpp:74-121).
+template <typename R> struct VisGeomD {
+    R fw1, fw2, d1, d2, dxnl, dynl, dznl, dxnr, dynr, dznr, angle1, angle2, t1[3], t2[3];
+};
+
+template <typename R> __device__ __forceinline__ R vis_angle(R dx, R dy, R dz, R dist) {
+    R r = dist / (Rsqrt(SQR3(dx, dy, dz)) + small_v<R>());
+    if (r > R(1)) r = R(1);
+    if (r < R(-1)) r = R(-1);
+    return asin(r) * R(180) / R(3.141592653589793);
+}
+
+template <typename R>
+__device__ __forceinline__ void vis_geom(const R *fg, const R *cgl, const R *cgr, VisGeomD<R> &G) {
+    R xn = fg[0], yn = fg[1], zn = fg[2];
+    R ax = fg[4] - cgl[0], ay = fg[5] - cgl[1], az = fg[6] - cgl[2];
+    R bx = fg[4] - cgr[0], by = fg[5] - cgr[1], bz = fg[6] - cgr[2];
+    R delt1 = Rsqrt(SQR3(ax, ay, az)), delt2 = Rsqrt(SQR3(bx, by, bz));
+    R delta = R(1) / (delt1 + delt2 + small_v<R>());
+    G.fw1 = delt2 * delta;
+    G.fw2 = delt1 * delta;
+    R dxl = cgl[0] - fg[4], dyl = cgl[1] - fg[5], dzl = cgl[2] - fg[6];
+    R dxr = cgr[0] - fg[4], dyr = cgr[1] - fg[5], dzr = cgr[2] - fg[6];
+    G.d1 = xn * dxl + yn * dyl + zn * dzl;
+    G.d2 = xn * dxr + yn * dyr + zn * dzr;
+    G.dxnl = xn * G.d1 - dxl; G.dynl = yn * G.d1 - dyl; G.dznl = zn * G.d1 - dzl;
+    G.dxnr = xn * G.d2 - dxr; G.dynr = yn * G.d2 - dyr; G.dznr = zn * G.d2 - dzr;
+    G.angle1 = vis_angle(dxl, dyl, dzl, -G.d1);
+    G.angle2 = vis_angle(dxr, dyr, dzr, G.d2);
+    R *t1 = G.t1, *t2 = G.t2;
+    if (xn != R(0)) { t1[0] = yn; t1[1] = -xn; t1[2] = R(0); }
+    else if (yn != R(0)) { t1[0] = -yn; t1[1] = xn; t1[2] = R(0); }
+    else if (zn != R(0)) { t1[0] = R(0); t1[1] = -zn; t1[2] = yn; }
+    else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) t1[k] = t2[k] = R(0);
+        return;
+    }
+    R dtmp = R(1) / Rsqrt(SQR3(t1[0], t1[1], t1[2]));
+    t1[0] *= dtmp; t1[1] *= dtmp; t1[2] *= dtmp;
+    t2[0] = yn * t1[2] - zn * t1[1];
+    t2[1] = zn * t1[0] - xn * t1[2];
+    t2[2] = xn * t1[1] - yn * t1[0];
+}
+
+// One variable's face gradient and normal derivative under VIS_TEST (2),
+// VIS_NEW1 (3) or VIS_NEW2 (4): VisGrad::CalcTestMethod / CalcNew1Method /
+// CalcNew2Method followed by ModifyFaceGrad (codes/usolver/src/VisGrad.cpp:268-353).
+// g1, g2: the left and right cell gradients; a boundary face weights the
+// left side only in VIS_TEST.
+template <typename R>
+__device__ __forceinline__ void vis_variant(int scheme, const VisGeomD<R> &G, bool bface, R xn, R yn, R zn, R q1,
+                                            R q2, const R *g1, const R *g2, R *grad, R &dqdn) {
+    const R sm = small_v<R>();
+    R q = R(0.5) * (q1 + q2), q11 = q1, q22 = q2;
+    dqdn = R(0);
+    if (scheme == 2) {
+        if (G.angle1 > R(20) && G.angle2 > R(20)) {
+            q11 += g1[0] * G.dxnl + g1[1] * G.dynl + g1[2] * G.dznl;
+            q22 += g2[0] * G.dxnr + g2[1] * G.dynr + g2[2] * G.dznr;
+        }
+        if (G.angle1 > R(0) && G.angle2 > R(0) && Rabs(G.d1) > sm && Rabs(G.d2) > sm) {
+            R dtmp = G.d1 * G.d1 + G.d2 * G.d2;
+            R c1 = G.d1 * G.d1 / dtmp, c2 = R(1) - c1;
+            if (bface) { c1 = R(1); c2 = R(0); }
+            R dqdn1 = (q11 - q) / G.d1, dqdn2 = (q22 - q) / G.d2;
+            dqdn = c1 * dqdn1 + c2 * dqdn2;
+        }
+    } else if (scheme == 3) {
+        if (G.d1 * G.d2 < R(0) && Rabs(G.d1) > sm && Rabs(G.d2) > sm) {
+            R d = R(-2) * G.d1 * G.d2 / (G.d1 * G.d1 + G.d2 * G.d2 + sm);
+            R od = d / (G.d2 - G.d1);
+            q11 += g1[0] * G.dxnl + g1[1] * G.dynl + g1[2] * G.dznl;
+            q22 += g2[0] * G.dxnr + g2[1] * G.dynr + g2[2] * G.dznr;
+            dqdn = (q22 - q11) * od;
+        }
+    } else {
+        R d = R(-2) * G.d1 * G.d2 / (G.d1 * G.d1 + G.d2 * G.d2 + sm);
+        if (d > R(0.1)) {
+            q11 += g1[0] * G.dxnl + g1[1] * G.dynl + g1[2] * G.dznl;
+            q22 += g2[0] * G.dxnr + g2[1] * G.dynr + g2[2] * G.dznr;
+            R dqdn1 = (q11 - q) / G.d1, dqdn2 = (q22 - q) / G.d2;
+            if (dqdn1 * dqdn2 > R(0)) dqdn = R(2) * dqdn1 * dqdn2 / (dqdn1 + dqdn2);
+        }
+    }
+    R gx = G.fw1 * g1[0] + G.fw2 * g2[0];
+    R gy = G.fw1 * g1[1] + G.fw2 * g2[1];
+    R gz = G.fw1 * g1[2] + G.fw2 * g2[2];
+    R dqdt1 = G.t1[0] * gx + G.t1[1] * gy + G.t1[2] * gz;
+    R dqdt2 = G.t2[0] * gx + G.t2[1] * gy + G.t2[2] * gz;
+    grad[0] = xn * dqdn + G.t1[0] * dqdt1 + G.t2[0] * dqdt2;
+    grad[1] = yn * dqdn + G.t1[1] * dqdt1 + G.t2[1] * dqdt2;
+    grad[2] = zn * dqdn + G.t1[2] * dqdt1 + G.t2[2] * dqdt2;
+}
+
+// The six face gradients of VIS_TEST / NEW1 / NEW2 and the scheme's dT/dn,
+// which the heat flux takes.  Compiled only into the k_residual instances for
+// these schemes (VV): even an untaken call costs the common path registers.
+template <typename R>
+__device__ __forceinline__ void vis_variant_grads(int scheme, const R *fg, const R *cgl, const R *cgr, const R *ql,
+                                               const R *qr, const R *gl, const R *gr, bool bface, R *gx, R *gy,
+                                               R *gz, R &dtdn) {
+    VisGeomD<R> G;
+    vis_geom(fg, cgl, cgr, G);
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+        int iv = v < 5 ? v : ITT;
+        R gr3[3], dn;
+        vis_variant(scheme, G, bface, fg[0], fg[1], fg[2], ql[iv], qr[iv], gl + v * 3, gr + v * 3, gr3, dn);
+        gx[v] = gr3[0]; gy[v] = gr3[1]; gz[v] = gr3[2];
+        if (v == 5) dtdn = dn;
+    }
+}
+
 // viscous face flux with the VIS_STD face gradient (VIS_AVER: the average of
-// the cell gradients, UNsVisFlux::AverMethod, codes/uns/src/UNsVisFlux.cpp:357-366),
-// before the -S/Re factor
+// the cell gradients, UNsVisFlux::AverMethod, codes/uns/src/UNsVisFlux.cpp:357-366;
+// VIS_TEST / NEW1 / NEW2: vis_variant above), before the -S/Re factor
 // (UNsVisFlux::PrepareFaceValue/StdMethod/CalcStress/CalcNsVisFlux,
 // codes/usolver/src/VisGrad.cpp:150-175,356-366)
 // dlr: qr - ql of the six gradient variables (rho, u, v, w, p, T)
-template <typename R>
+template <typename R, bool VV>
 __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, const R *qr, const R *dlr, const R *fg,
-                                              const R *cgl, const R *cgr, const R *gl, const R *gr, R *fv) {
+                                              const R *cgl, const R *cgr, const R *gl, const R *gr, bool bface,
+                                              R *fv) {
     R half = R(0.5);
     R vlm = half * (ql[IML] + qr[IML]), vtm = half * (ql[IMT] + qr[IMT]);
     R vis = vlm + vtm;
@@ -640,7 +758,7 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
         gx[v] = half * (gl[v * 3] + gr[v * 3]);
         gy[v] = half * (gl[v * 3 + 1] + gr[v * 3 + 1]);
         gz[v] = half * (gl[v * 3 + 2] + gr[v * 3 + 2]);
-        if (P.ivischeme != 1) {   // VIS_STD's CorrectGrad; VIS_AVER keeps the average
+        if (P.ivischeme == 0) {   // VIS_STD's CorrectGrad; VIS_AVER keeps the average
             R fOld = gx[v] * dx + gy[v] * dy + gz[v] * dz;
             R fnew = dlr[v] * ods;
             R df = fnew - fOld;
@@ -649,6 +767,8 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
     }
     R xn = fg[0], yn = fg[1], zn = fg[2];
     R dtdn = xn * gx[5] + yn * gy[5] + zn * gz[5];
+    if constexpr (VV)   // TEST / NEW1 / NEW2 replace the face gradients
+        vis_variant_grads(P.ivischeme, fg, cgl, cgr, ql, qr, gl, gr, bface, gx, gy, gz, dtdn);
     R kcp = (vlm * R(P.oprl) + vtm * R(P.oprt)) * R(P.const_cp);
     R qNormal = R(0);
     qNormal += xn * R(0) + yn * R(0) + zn * R(0);
@@ -667,16 +787,16 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
     fv[4] = qm[IU] * fv[1] + qm[IV] * fv[2] + qm[IW] * fv[3] + qNormal;
 }
 
-template <typename R>
+template <typename R, bool VV>
 __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, const R *qr, const R *fg, const R *cgl,
-                                              const R *cgr, const R *gl, const R *gr, R *fv) {
+                                              const R *cgr, const R *gl, const R *gr, bool bface, R *fv) {
     R dlr[6];
 #pragma unroll
     for (int v = 0; v < 6; ++v) {
         int iv = v < 5 ? v : ITT;
         dlr[v] = qr[iv] - ql[iv];
     }
-    face_vis_flux(P, ql, qr, dlr, fg, cgl, cgr, gl, gr, fv);
+    face_vis_flux<R, VV>(P, ql, qr, dlr, fg, cgl, cgr, gl, gr, bface, fv);
 }
 
 // One gather pass per cell: face radii + time step, inviscid residual and
@@ -686,7 +806,7 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
 // instead of two).
 // MODE 0: residual and time step (one outer iteration), 1: time step only
 // (the CALC_TIME_STEP task), 2: residual only (the UPDATE_RESIDUALS task).
-template <typename R, int MODE>
+template <typename R, int MODE, bool VV = false>
 __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A) {
     constexpr bool exactOrder = sizeof(R) == 8;
     constexpr bool doRes = MODE != 1, doDt = MODE != 2;
@@ -765,7 +885,7 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
                 R fvs[NEQ];   // viscous term, formed first while fewer values are live
                 if (P.vismodel > 0) {
                     R fv[NEQ];
-                    face_vis_flux(P, ql, qr, fg, cgl, cgr, gll, glr, fv);
+                    face_vis_flux<R, VV>(P, ql, qr, fg, cgl, cgr, gll, glr, ghost, fv);
                     R coeff = -orey * fg[3];
 #pragma unroll
                     for (int e = 0; e < NEQ; ++e) fvs[e] = coeff * fv[e];
@@ -830,7 +950,7 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
                     const R *cgl = right ? cgn : cgc, *cgr = right ? cgc : cgn;
                     const R *gll = right ? gln : glc, *glr = (right || ghost) ? glc : gln;
                     R fv[NEQ];
-                    face_vis_flux(P, ql, qr, fg, cgl, cgr, gll, glr, fv);
+                    face_vis_flux<R, VV>(P, ql, qr, fg, cgl, cgr, gll, glr, ghost, fv);
                     R coeff = -orey * fg[3];
 #pragma unroll
                     for (int e = 0; e < NEQ; ++e) {

@@ -108,7 +108,8 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     case T_RESIDUAL: {   // UPDATE_RESIDUALS alone
         KArgs<R> A = make_args<R>(c, false);
         launch_gradlim<R>(c, A, s);
-        OFG_LAUNCH((k_residual<R, 2>), nblk(N, 128), 128, s, A);
+        if (c->p.ivischeme >= 2) OFG_LAUNCH((k_residual<R, 2, true>), nblk(N, 128), 128, s, A);
+        else OFG_LAUNCH((k_residual<R, 2>), nblk(N, 128), 128, s, A);
         break;
     }
     case T_TS_RES:       // CALC_TIME_STEP + LOAD_RESIDUALS + UPDATE_RESIDUALS in one gather
@@ -117,7 +118,10 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     case T_P_CLIP: {
         KArgs<R> A = make_args<R>(c, false);
         if (task == T_TS_RES || task == T_P_GRADLIM) launch_gradlim<R>(c, A, s);
-        if (task == T_TS_RES || task == T_P_FLUX) OFG_LAUNCH((k_residual<R, 0>), nblk(N, 128), 128, s, A);
+        if (task == T_TS_RES || task == T_P_FLUX) {   // VV: the TEST / NEW1 / NEW2 viscous face gradients
+            if (c->p.ivischeme >= 2) OFG_LAUNCH((k_residual<R, 0, true>), nblk(N, 128), 128, s, A);
+            else OFG_LAUNCH((k_residual<R, 0>), nblk(N, 128), 128, s, A);
+        }
         if (task == T_TS_RES || task == T_P_CLIP) OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }

@@ -810,6 +810,92 @@ struct Oracle {
     // ======================= viscous flux (STD) =======================
     // UNsVisFlux::CalcFlux (codes/uns/src/UNsVisFlux.cpp:90-440) with the
     // VIS_STD face gradient (codes/usolver/src/VisGrad.cpp:150-175,356-366)
+    // Face gradients of the VIS_TEST / VIS_NEW1 / VIS_NEW2 schemes for one
+    // variable: VisGrad::CalcTestMethod, CalcNew1Method, CalcNew2Method and
+    // ModifyFaceGrad (codes/usolver/src/VisGrad.cpp:268-353) with the geometry of
+    // VisGradGeom::CalcFaceWeight / PrepareCellGeom (:44-97) and the face
+    // tangents of GCom::CalcTangent (codes/global/src/Com.cpp:74-121).
+    struct VisGeom {
+        double fw1, fw2, d1, d2, dxnl, dynl, dznl, dxnr, dynr, dznr, angle1, angle2, t1[3], t2[3];
+    };
+    static double visAngle(double dx, double dy, double dz, double dist) {
+        double result = dist / (DIST3(dx, dy, dz) + SMALL);
+        if (result > 1.0) result = 1.0;
+        if (result < -1.0) result = -1.0;
+        return std::asin(result) * 180.0 / 3.141592653589793;
+    }
+    VisGeom visGeom(int f, int l, int r) const {
+        VisGeom G;
+        double xn = xfn[f], yn = yfn[f], zn = zfn[f];
+        double ax = xfc[f] - xcc[l], ay = yfc[f] - ycc[l], az = zfc[f] - zcc[l];
+        double bx = xfc[f] - xcc[r], by = yfc[f] - ycc[r], bz = zfc[f] - zcc[r];
+        double delt1 = DIST3(ax, ay, az), delt2 = DIST3(bx, by, bz);
+        double delta = 1.0 / (delt1 + delt2 + SMALL);
+        G.fw1 = delt2 * delta;
+        G.fw2 = delt1 * delta;
+        double dxl = xcc[l] - xfc[f], dyl = ycc[l] - yfc[f], dzl = zcc[l] - zfc[f];
+        double dxr = xcc[r] - xfc[f], dyr = ycc[r] - yfc[f], dzr = zcc[r] - zfc[f];
+        G.d1 = xn * dxl + yn * dyl + zn * dzl;
+        G.d2 = xn * dxr + yn * dyr + zn * dzr;
+        G.dxnl = xn * G.d1 - dxl; G.dynl = yn * G.d1 - dyl; G.dznl = zn * G.d1 - dzl;
+        G.dxnr = xn * G.d2 - dxr; G.dynr = yn * G.d2 - dyr; G.dznr = zn * G.d2 - dzr;
+        G.angle1 = visAngle(dxl, dyl, dzl, -G.d1);
+        G.angle2 = visAngle(dxr, dyr, dzr, G.d2);
+        double *t1 = G.t1, *t2 = G.t2;
+        if (xn != 0.0) { t1[0] = yn; t1[1] = -xn; t1[2] = 0.0; }
+        else if (yn != 0.0) { t1[0] = -yn; t1[1] = xn; t1[2] = 0.0; }
+        else if (zn != 0.0) { t1[0] = 0.0; t1[1] = -zn; t1[2] = yn; }
+        else { for (int k = 0; k < 3; ++k) t1[k] = t2[k] = 0.0; return G; }
+        double dtmp = 1.0 / DIST3(t1[0], t1[1], t1[2]);
+        t1[0] *= dtmp; t1[1] *= dtmp; t1[2] *= dtmp;
+        t2[0] = yn * t1[2] - zn * t1[1];
+        t2[1] = zn * t1[0] - xn * t1[2];
+        t2[2] = xn * t1[1] - yn * t1[0];
+        return G;
+    }
+    void visVariant(const VisGeom &G, bool bface, double xn, double yn, double zn, double q1, double q2,
+                    const double *g1, const double *g2, double *grad, double &dqdn) const {
+        const int scheme = p.ivischeme;
+        double q = half * (q1 + q2), q11 = q1, q22 = q2;
+        dqdn = 0.0;
+        auto side = [&]() {   // AccurateSideValue
+            q11 += g1[0] * G.dxnl + g1[1] * G.dynl + g1[2] * G.dznl;
+            q22 += g2[0] * G.dxnr + g2[1] * G.dynr + g2[2] * G.dznr;
+        };
+        if (scheme == 2) {
+            if (G.angle1 > 20.0 && G.angle2 > 20.0) { side(); q = half * (q1 + q2); }
+            if (G.angle1 > 0.0 && G.angle2 > 0.0 && std::fabs(G.d1) > SMALL && std::fabs(G.d2) > SMALL) {
+                double dtmp = G.d1 * G.d1 + G.d2 * G.d2;
+                double c1 = G.d1 * G.d1 / dtmp, c2 = 1.0 - c1;
+                if (bface) { c1 = 1.0; c2 = 0.0; }
+                double dqdn1 = (q11 - q) / G.d1, dqdn2 = (q22 - q) / G.d2;
+                dqdn = c1 * dqdn1 + c2 * dqdn2;
+            }
+        } else if (scheme == 3) {
+            if (G.d1 * G.d2 < 0.0 && std::fabs(G.d1) > SMALL && std::fabs(G.d2) > SMALL) {
+                double d = -2.0 * G.d1 * G.d2 / (G.d1 * G.d1 + G.d2 * G.d2 + SMALL);
+                double od = d / (G.d2 - G.d1);
+                side();
+                dqdn = (q22 - q11) * od;
+            }
+        } else {
+            double d = -2.0 * G.d1 * G.d2 / (G.d1 * G.d1 + G.d2 * G.d2 + SMALL);
+            if (d > 0.1) {
+                side();
+                double dqdn1 = (q11 - q) / G.d1, dqdn2 = (q22 - q) / G.d2;
+                if (dqdn1 * dqdn2 > 0.0) dqdn = 2.0 * dqdn1 * dqdn2 / (dqdn1 + dqdn2);
+            }
+        }
+        double gx = G.fw1 * g1[0] + G.fw2 * g2[0];
+        double gy = G.fw1 * g1[1] + G.fw2 * g2[1];
+        double gz = G.fw1 * g1[2] + G.fw2 * g2[2];
+        double dqdt1 = G.t1[0] * gx + G.t1[1] * gy + G.t1[2] * gz;
+        double dqdt2 = G.t2[0] * gx + G.t2[1] * gy + G.t2[2] * gz;
+        grad[0] = xn * dqdn + G.t1[0] * dqdt1 + G.t2[0] * dqdt2;
+        grad[1] = yn * dqdn + G.t1[1] * dqdt1 + G.t2[1] * dqdt2;
+        grad[2] = zn * dqdn + G.t1[2] * dqdt1 + G.t2[2] * dqdt2;
+    }
+
     void visFlux() {
         if (p.vismodel == 0) return;
         grad(tempr, dtdx, dtdy, dtdz);   // UTGrad: the reference's GG cell-weighted for igrad 0
@@ -840,6 +926,19 @@ struct Oracle {
             }
             double xn = xfn[f], yn = yfn[f], zn = zfn[f];
             double dtdn = xn * gx[5] + yn * gy[5] + zn * gz[5];
+            if (p.ivischeme >= 2) {   // TEST / NEW1 / NEW2: the face gradients above are replaced
+                VisGeom G = visGeom(f, l, r);
+                for (int e = 0; e < 6; ++e) {
+                    double q1 = e < NEQ ? q[e][l] : tempr[l];
+                    double q2 = e < NEQ ? q[e][r] : tempr[r];
+                    double g1[3] = {e < NEQ ? dqdx[e][l] : dtdx[l], e < NEQ ? dqdy[e][l] : dtdy[l], e < NEQ ? dqdz[e][l] : dtdz[l]};
+                    double g2[3] = {e < NEQ ? dqdx[e][r] : dtdx[r], e < NEQ ? dqdy[e][r] : dtdy[r], e < NEQ ? dqdz[e][r] : dtdz[r]};
+                    double gr[3], dn;
+                    visVariant(G, f < nBFaces, xn, yn, zn, q1, q2, g1, g2, gr, dn);
+                    gx[e] = gr[0]; gy[e] = gr[1]; gz[e] = gr[2];
+                    if (e == 5) dtdn = dn;   // SaveFacePara: the heat flux takes the scheme's dT/dn
+                }
+            }
             double kcp = (vlm * oprl + vtm * oprt) * const_cp;
             double qNormal = 0.0;
             qNormal += xn * 0.0 + yn * 0.0 + zn * 0.0;

@@ -15,6 +15,10 @@ CASES = {
     "bump_euler_rk3": dict(steps=30),
     "plate2d_laminar_roe_rk2": dict(steps=30),
     "plate2d_laminar_roe_visaver": dict(steps=30),
+    "plate2d_laminar_roe_vistest": dict(steps=30),
+    "plate2d_laminar_roe_visnew1": dict(steps=30),
+    "plate2d_laminar_roe_visnew2": dict(steps=30),
+    "mixed3d_laminar_vistest": dict(steps=10),
 }
 # meshes whose wall distance the reference computed itself (ireadwdst = 0):
 # tests/golden/walldist_<name>.npz
@@ -44,10 +48,14 @@ def build(name):
     if name == "plate2d_laminar_roe_rk2":
         return meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5, vismodel=1,
                                                      time_integral=1, rk_stage=2, cflst=0.5, cfled=0.5), steps
-    if name == "plate2d_laminar_roe_visaver":
-        # VIS_AVER viscous face gradient (ivischeme = 1)
+    if name.startswith("plate2d_laminar_roe_vis"):
+        # the viscous face-gradient schemes: VIS_AVER, VIS_TEST, VIS_NEW1, VIS_NEW2
+        iv = {"visaver": 1, "vistest": 2, "visnew1": 3, "visnew2": 4}[name.rsplit("_", 1)[1]]
         return meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5, vismodel=1,
-                                                     ivischeme=1), steps
+                                                     ivischeme=iv), steps
+    if name == "mixed3d_laminar_vistest":
+        return meshgen.bump_box_mixed(), P.defaults(dimension=3, ischeme=1, ilim=0, vismodel=1, mach_ref=0.3,
+                                                    reynolds=1e4, ivischeme=2), steps
     if name.startswith("bump"):
         mesh = meshgen.bump_channel(32, 16)
         kw = {"bump_euler_roe1": {}, "bump_euler_roe_venkat": dict(ilim=2, vencat_coef=0.05),

@@ -62,8 +62,12 @@ def test_mixed_mesh_task_by_task_against_the_oracle():
             assert np.abs(a - b).max() <= 1e-10 * max(np.abs(b).max(), 1e-30), (it, f)
 
 
-def test_mixed_mesh_fp32_face_path_tracks_fp64():
-    mesh, prm, steps = build("mixed3d_slau2_gg_barth_sa")
+# the FP32 face path (its own viscous face-gradient code) against FP64
+@pytest.mark.parametrize("name", ["mixed3d_slau2_gg_barth_sa", "plate2d_laminar_roe_vistest",
+                                  "plate2d_laminar_roe_visnew1", "plate2d_laminar_roe_visnew2",
+                                  "mixed3d_laminar_vistest"])
+def test_fp32_face_path_tracks_fp64(name):
+    mesh, prm, steps = build(name)
     a = Solver(mesh, prm); a.init_flowfield(); a.step(steps)
     prm1 = P.defaults(**{**P.to_dict(prm), "precision": 1})
     b = Solver(mesh, prm1); b.init_flowfield(); b.step(steps)
