@@ -122,7 +122,11 @@ int         ofg_version(void);
  * reversed (UnsGrid::ReadGridFaceTopology, :157-175).  Boundary faces are
  * [0, nBFaces).  Metrics (UnsGrid::CalcMetrics, :469-900) are computed here,
  * on the GPU.  wall_dist is per interior cell; NULL makes an SA solve compute
- * it (ofg_calc_wall_dist) and is ignored otherwise.
+ * it (ofg_calc_wall_dist) and is ignored otherwise.  Malformed input (no
+ * cells or faces, indices out of range, a face of fewer than 2 (2-D) or 3
+ * (3-D) nodes, an interior face with one cell on both sides, a boundary code
+ * outside 1-6) returns OFG_E_ARG; after any refused upload the context holds
+ * no mesh (calls that run kernels return OFG_E_STATE) until one succeeds.
  */
 int ofg_upload_mesh(ofg_ctx *ctx, int nNodes, const double *xN, const double *yN, const double *zN,
                     int nFaces, const int *faceNodeCount, const int *faceNodes,

@@ -450,6 +450,10 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
                     const int *faceNodeCount, const int *faceNodes, const int *lCells, const int *rCells, int nCells,
                     int nBFaces, const int *bcType, const double *wall_dist) {
     if (!c) return OFG_E_ARG;
+    // the context's sizes change before the arrays are checked: after a
+    // refused upload no call runs kernels until an upload succeeds
+    c->haveMesh = false;
+    c->haveState = false;
     if (nNodes <= 0 || nFaces <= 0 || nCells <= 0 || nBFaces < 0 || nBFaces > nFaces)
         return c->fail(OFG_E_ARG, "bad mesh sizes");
     if (!xN || !yN || !zN || !faceNodeCount || !faceNodes || !lCells || !rCells || (nBFaces && !bcType))

@@ -63,6 +63,8 @@ def test_bad_arguments_are_rejected():
     assert L.ofg_create(C.byref(prm), C.byref(h)) == -1
     prm = P.euler_bump(sweep_order=5)
     assert L.ofg_create(C.byref(prm), C.byref(h)) == -1
+    prm = P.euler_bump(ivischeme=5)        # viscous face-gradient schemes are 0-4
+    assert L.ofg_create(C.byref(prm), C.byref(h)) == -1
 
 
 @pytest.mark.parametrize("dim", [2, 3])
