@@ -29,6 +29,10 @@ def cases():
                                                                        reynolds=1e5, vismodel=1)),
         "laminar_roe_plate_ramp": (meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.3,
                                                                          reynolds=2e5, vismodel=1)),
+        # the viscous face-gradient schemes TEST, NEW1, NEW2 (their own k_residual instances)
+        **{f"laminar_roe_plate_vis{v}": (meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.3,
+                                                                               reynolds=2e5, vismodel=1, ivischeme=iv))
+           for v, iv in (("test", 2), ("new1", 3), ("new2", 4))},
     }
 
 
