@@ -96,7 +96,7 @@ KERNEL_OF_GROUP = {"gradlim": "k_gradlim", "residual": "k_residual<float,0> (flu
 # group, from `ncu --section MemoryWorkloadAnalysis` of the 600,000-cell plate
 # sample (plate3d_sample: same kernels, layout and sweep levels); the kernels
 # stream their arrays once per launch, so the traffic scales with the cell
-# count.  Command and table: profiles/ncu_memory_plate3d_sample.md.
+# count.
 NCU_TRAFFIC_PER_CELL = {
     ("plate3d", "residual"): 334.7, ("plate3d", "gradlim"): 241.3, ("plate3d", "clip"): 40.0,
     ("plate3d", "lusgs_lower"): 445.4, ("plate3d", "lusgs_upper"): 356.9, ("plate3d", "update"): 109.7,

@@ -305,9 +305,12 @@ int ofg_cell_centres(int dimension, int nNodes, const double *xN, const double *
                      int nCells, int nBFaces, double *out);
 
 /* Cell renumbering for the GPU sweeps: a greedy colouring of the cell graph
-   followed by a locality order inside each colour.  Writes perm[newId] = oldId
-   for interior cells and returns the number of colours (>= 1).  Pure host
-   function; apply it to the mesh arrays before ofg_upload_mesh. */
+   (interior faces, cells visited in natural order), colours ascending and cell
+   ids ascending inside a colour.  Writes perm[newId] = oldId for interior
+   cells and returns the number of colours (>= 1).  Pure host function; apply
+   it to the mesh arrays before ofg_upload_mesh.  Returns OFG_E_ARG for
+   nCells < 1, nBFaces < 0, nFaces < nBFaces, a null pointer or an interior
+   face whose cells are out of range; perm is undefined after an error. */
 int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells,
                      int *perm);
 
@@ -331,13 +334,17 @@ int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, con
    device: 296 blocks x 8 partial sums + a ticket), so:
      - n_eq above OFG_NOALLOC_MAX_EQ returns OFG_E_SIZE (devices with an
        ordinal of 64 or more too); n_cells may be any positive count;
-     - the ticket in the scratch must be zero when a call starts: it is zero
-       when the library is loaded and every completed call leaves it zero;
+     - every call first clears the scratch's ticket on `stream` (a 4-byte
+       cudaMemsetAsync, which allocates nothing), then runs one kernel; the
+       partial sums are rewritten by every call before they are read;
      - calls that overlap in time on the same device race on the scratch:
        serialise them (one stream, or an event between streams);
      - the first call on each device (made with that device current) looks up
        the scratch address with cudaGetSymbolAddress and loads the module;
-       make that first call before capturing any stream.
+       make that first call before capturing any stream;
+     - the looked-up address is kept for the life of the process: after a
+       cudaDeviceReset of a device this entry point must not be called on
+       that device again (the kept address would be stale).
    Returns OFG_OK, OFG_E_ARG (null pointer, n_cells < 1, n_eq < 1), OFG_E_SIZE
    or OFG_E_CUDA. */
 int ofg_residual_rms_noalloc(const double *res, int64_t n_cells, int n_eq, double *rms_out, void *stream);

@@ -164,9 +164,6 @@ void compute_metrics(ofg_ctx *c, int dim, const std::vector<double> &xN, const s
     }
 }
 
-// Level schedule of a sequential sweep: a cell's level is one more than the
-// deepest level among the neighbours it reads (lower: smaller id; upper:
-// larger id).  Cells inside a level keep ascending / descending id order.
 // Greedy colouring of the cell graph (interior faces) in natural order and
 // the colour-major order: colours ascending, ids ascending inside a colour.
 // Returns the number of colours, fills perm[position] = cell.
@@ -1401,7 +1398,7 @@ int ofg_cell_centres(int dim, int nNodes, const double *xN, const double *yN, co
 }
 
 int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm) {
-    if (nCells <= 0 || nFaces < nBFaces || !lCells || !rCells || !perm) return OFG_E_ARG;
+    if (nCells <= 0 || nBFaces < 0 || nFaces < nBFaces || !lCells || !rCells || !perm) return OFG_E_ARG;
     return colour_major_order(nCells, nFaces, nBFaces, lCells, rCells, perm);
 }
 

@@ -2,13 +2,17 @@
 // without allocating anything (the contract is in include/oneflow_b200.h).
 //
 // Scratch lives in this file's static __device__ object: one slot of partial
-// sums per block and a ticket counter, 18,952 bytes per device.  The ticket is
-// zero when the module is loaded and every completed call leaves it at zero
-// again (the last block to finish re-arms it), so the scratch needs no clearing
-// between calls.  Two calls that overlap in time on the same device share the
-// scratch and race: callers serialise them (one stream, or an event between).
+// sums per block and a ticket counter, 18,952 bytes per device.  Every call
+// clears the ticket on its stream before its kernel (a 4-byte memset, no
+// allocation), so a call that never finished cannot leave a stale count for
+// the next one; the partial sums need no clearing, since every block writes
+// its own slot before the ticket counts it.  Two calls that overlap in time on
+// the same device share the scratch and race: callers serialise them (one
+// stream, or an event between).
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <cstddef>
 #include <cstdint>
 
 #include "../../include/oneflow_b200.h"
@@ -21,7 +25,7 @@ constexpr int kMaxEq = OFG_NOALLOC_MAX_EQ;
 
 struct Scratch {
     double partial[kBlocks * kMaxEq];   // per-block sums of squares
-    unsigned int ticket;                // must be 0 when a call starts; the last block re-arms it
+    unsigned int ticket;                // blocks finished; cleared by every call before its kernel
 };
 static_assert(sizeof(Scratch) <= 19 * 1024, "scratch stays small");
 
@@ -74,9 +78,10 @@ __global__ void __launch_bounds__(kThreads) k_rms_noalloc(const double *res, lon
     sc->ticket = 0u;
 }
 
-// address of the scratch on each device, looked up once with that device current
+// address of the scratch on each device, looked up once with that device
+// current (host threads that race on the first call store the same value)
 constexpr int kMaxDevices = 64;
-Scratch *g_scratch_addr[kMaxDevices];
+std::atomic<Scratch *> g_scratch_addr[kMaxDevices];
 
 }  // namespace
 
@@ -87,16 +92,21 @@ extern "C" int ofg_residual_rms_noalloc(const double *res, int64_t n_cells, int 
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return OFG_E_CUDA;
     if (dev >= kMaxDevices) return OFG_E_SIZE;
-    if (!g_scratch_addr[dev]) {
+    Scratch *sc = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!sc) {
         // first call on this device (with it current): resolve the scratch
         // address, which also loads this module on the device
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) return OFG_E_CUDA;
-        g_scratch_addr[dev] = static_cast<Scratch *>(p);
+        sc = static_cast<Scratch *>(p);
+        g_scratch_addr[dev].store(sc, std::memory_order_release);
     }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(reinterpret_cast<char *>(sc) + offsetof(Scratch, ticket), 0, sizeof(unsigned int), st) !=
+        cudaSuccess)
+        return OFG_E_CUDA;
     long long nb = (n_cells + kThreads - 1) / kThreads;
     int blocks = nb < kBlocks ? int(nb) : kBlocks;
-    k_rms_noalloc<<<blocks, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(res, (long long)n_cells, n_eq,
-                                                                              rms_out, g_scratch_addr[dev]);
+    k_rms_noalloc<<<blocks, kThreads, 0, st>>>(res, (long long)n_cells, n_eq, rms_out, sc);
     return cudaGetLastError() == cudaSuccess ? OFG_OK : OFG_E_CUDA;
 }

@@ -1,5 +1,7 @@
 """Seeded cases of the golden fixtures (tests/golden/*.npz): the mesh and the
 parameters of each, regenerated from their seeds."""
+import numpy as np
+
 from oneflow_b200 import colour_order, meshgen, params as P
 from oneflow_b200.walldist import plate_wall_distance, wall_distance
 
@@ -19,6 +21,11 @@ CASES = {
     "plate2d_laminar_roe_visnew1": dict(steps=30),
     "plate2d_laminar_roe_visnew2": dict(steps=30),
     "mixed3d_laminar_vistest": dict(steps=10),
+    # boundary conditions no other case uses: INFLOW (5) and EXTRAPOLATION (1)
+    # on a laminar and an SA plate, and the isothermal no-slip wall (isowallbc 1)
+    "plate2d_laminar_roe_inflow_extrap": dict(steps=30),
+    "plate2d_sa_roe_inflow_extrap": dict(steps=30),
+    "plate2d_laminar_roe_isowall": dict(steps=30),
 }
 # meshes whose wall distance the reference computed itself (ireadwdst = 0):
 # tests/golden/walldist_<name>.npz
@@ -40,8 +47,33 @@ def build_walldist(name):
 RESTART_CASES = {"bump_euler_roe_venkat": 20, "plate2d_sa_roe": 20}
 
 
+def inflow_extrap(mesh):
+    """The plate with its upstream far-field faces (x at the inlet) made
+    INFLOW and its OUTFLOW exit made EXTRAPOLATION."""
+    fnc = mesh.face_node_count[:mesh.n_bfaces]
+    off = np.concatenate([[0], np.cumsum(mesh.face_node_count)])
+    xf = np.array([mesh.x[mesh.face_nodes[off[f]:off[f] + fnc[f]]].mean() for f in range(mesh.n_bfaces)])
+    bct = mesh.bc_type.copy()
+    bct[(bct == 4) & (xf <= mesh.x.min() + 1e-12)] = 5
+    bct[bct == 6] = 1
+    assert (bct == 5).any() and (bct == 1).any()
+    mesh.bc_type = bct.astype(np.int32)
+    return mesh
+
+
 def build(name):
     steps = CASES[name]["steps"]
+    if name == "plate2d_laminar_roe_inflow_extrap":
+        return inflow_extrap(meshgen.plate_2d(24, 16)), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5,
+                                                                    vismodel=1), steps
+    if name == "plate2d_sa_roe_inflow_extrap":
+        mesh = inflow_extrap(meshgen.plate_2d(32, 24, y1=1e-5, ratio=1.25))
+        mesh.wall_dist = wall_distance(mesh)
+        return mesh, P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=5e6, vismodel=3), steps
+    if name == "plate2d_laminar_roe_isowall":
+        # a wall 20 % hotter than the free stream
+        return meshgen.plate_2d(24, 16), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5, vismodel=1,
+                                                     isowallbc=1, twall_dim=360.0), steps
     if name == "bump_euler_rk3":
         # the multi-stage scheme (TimeIntegral::RungeKutta), 3 stages, CFL 0.8
         return meshgen.bump_channel(32, 16), P.euler_bump(time_integral=1, rk_stage=3, cflst=0.8, cfled=0.8), steps

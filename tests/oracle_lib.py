@@ -16,6 +16,9 @@ from oneflow_b200.meshio import Mesh, read_ref_dump, read_res_dat, write_case
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboforacle.so")
 REF_EXE = os.path.join(ROOT, "oracle", "_ref", "oneflow_ref")
+# the reference's source tree (its regression cases are read from there): the
+# ONEFLOW_REF environment variable, as in oracle/Makefile
+REF_ROOT = os.environ.get("ONEFLOW_REF", "/root/reference")
 
 _dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")

@@ -38,10 +38,13 @@ def test_gpu_matches_the_reference_fixture(name):
         assert np.linalg.norm(t - tg) / np.linalg.norm(tg) < 1e-5
 
 
-def test_mixed_mesh_task_by_task_against_the_oracle():
-    # hexahedra + prisms, SLAU2, Green-Gauss, Barth, SA: each task of the
-    # first iterations against the oracle to round-off
-    mesh, prm, _ = build("mixed3d_slau2_gg_barth_sa")
+@pytest.mark.parametrize("name", ["mixed3d_slau2_gg_barth_sa", "plate2d_laminar_roe_inflow_extrap",
+                                  "plate2d_sa_roe_inflow_extrap", "plate2d_laminar_roe_isowall"])
+def test_iteration_by_iteration_against_the_oracle(name):
+    # hexahedra + prisms, SLAU2, Green-Gauss, Barth, SA; and the inflow,
+    # extrapolation and isothermal-wall boundary conditions: the state, time
+    # step and residual of each of the first iterations against the oracle
+    mesh, prm, _ = build(name)
     g = Solver(mesh, prm)
     g.init_flowfield()
     o = Oracle(mesh, prm)

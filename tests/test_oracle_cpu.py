@@ -19,9 +19,9 @@ from oneflow_b200 import colour_order, meshgen, params as P
 from oneflow_b200.meshio import read_ofl, read_res_dat
 from oneflow_b200.walldist import plate_wall_distance, wall_distance
 from golden_cases import CASES, build
-from oracle_lib import Oracle
+from oracle_lib import REF_ROOT, Oracle
 
-REF = "/root/reference/test"
+REF = os.path.join(REF_ROOT, "test")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

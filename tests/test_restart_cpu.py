@@ -10,7 +10,7 @@ import pytest
 
 from oneflow_b200 import meshio
 from golden_cases import RESTART_CASES, build
-from oracle_lib import ref_available, run_ref
+from oracle_lib import REF_ROOT, ref_available, run_ref
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -44,7 +44,7 @@ def test_writer_reproduces_the_record_layout(name, tmp_path):
 
 def test_reader_on_the_reference_s_own_restart_file():
     # the restart file shipped with the reference's plateuns2dslau2_continue case
-    base = "/root/reference/test/plateuns2dslau2_continue"
+    base = os.path.join(REF_ROOT, "test", "plateuns2dslau2_continue")
     if not os.path.isdir(base):
         pytest.skip("reference tree not present")
     mesh = meshio.read_ofl(os.path.join(base, "grid", "plate20182d.ofl"))

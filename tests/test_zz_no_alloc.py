@@ -58,3 +58,24 @@ def test_noalloc_rms_refuses_requests_beyond_its_scratch():
     assert f(x.data_ptr(), 16, 8, o.data_ptr(), None) == 0
     torch.cuda.synchronize()
     assert np.array_equal(o.cpu().numpy()[:8], np.zeros(8))
+
+
+@pytest.mark.parametrize("n,neq", [(1_000_003, 5), (300_001, 8), (77, 3)])
+def test_noalloc_rms_matches_numpy_on_random_data(n, neq):
+    # Large enough that the grid is capped (296 blocks) and every block strides
+    # over more than its 256 threads; odd sizes leave a ragged last range; the
+    # 8-equation case fills every partial-sum slot with nonzero values.
+    import torch
+    f = _bind()
+    rng = np.random.default_rng(n + neq)
+    x = rng.standard_normal((n, neq)) * rng.uniform(0.1, 10.0, size=neq)
+    want = np.sqrt(np.mean(x * x, axis=0))
+    d = torch.tensor(x, dtype=torch.float64, device="cuda")
+    outs = [torch.full((neq,), -1.0, dtype=torch.float64, device="cuda") for _ in range(2)]
+    stream = torch.cuda.current_stream().cuda_stream
+    for o in outs:   # two full-size calls in a row on the shared scratch
+        assert f(d.data_ptr(), n, neq, o.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    a, b = outs[0].cpu().numpy(), outs[1].cpu().numpy()
+    assert np.array_equal(a, b)
+    assert np.allclose(a, want, rtol=1e-12, atol=0.0)
