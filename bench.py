@@ -66,29 +66,22 @@ def make_workload(name: str):
 _SAMPLE = {"plate3d": "plate3d_sample"}
 
 
-def make_workload_desc(name: str):
-    """Description of a workload without building its mesh."""
-    if name == "plate3d":
-        return None, None, dict(workload="3-D RANS-SA flat plate: 200x100x50 hexes split into 6 tets (6,000,000 cells), "
-                                          "Roe 2nd order, least-squares gradients, Venkatakrishnan K=5, SA, LU-SGS",
-                                lattice=[200, 100, 50])
-    return make_workload(name)
-
-
 def _ref_procs(mesh) -> int:
     """Concurrent reference processes: all host cores, bounded by memory
-    (about 1 kB of reference state per cell) and by 64."""
+    (the reference holds about 1.7 kB per cell of a tetrahedral RANS-SA mesh,
+    measured: 80 MB peak for 48,000 cells; 2 kB is budgeted) and by 64."""
     n = os.cpu_count() or 1
     try:
         import psutil
         avail = psutil.virtual_memory().available
-        n = min(n, max(1, int(avail * 0.5 // (mesh.n_cells * 1200 + 1))))
+        n = min(n, max(1, int(avail * 0.6 // (mesh.n_cells * 2000 + 1))))
     except Exception:
         pass
     return max(1, min(n, 64))
 
 
-KERNEL_OF_GROUP = {"gradlim": "k_gradlim", "residual": "k_residual<float,0> (flux + time-step gather)",
+KERNEL_OF_GROUP = {"gradlim": "k_gradlim", "residual": "k_face_pass<0> (face fluxes + spectral radii, mixed path)",
+                   "residual_sum": "k_face_sum<0> (per-cell sum of the face results, time step)",
                    "clip": "k_timestep_clip", "lusgs_lower": "k_lusgs_lower", "lusgs_upper": "k_lusgs_upper",
                    "update": "k_update", "sa_residual": "k_turb_rhs", "sa_grad": "k_turb_grad"}
 
@@ -102,6 +95,13 @@ NCU_TRAFFIC_PER_CELL = {
     ("plate3d", "lusgs_lower"): 445.4, ("plate3d", "lusgs_upper"): 356.9, ("plate3d", "update"): 109.7,
     ("plate3d", "sa_grad"): 63.5, ("plate3d", "sa_residual"): 398.9,
 }
+
+
+def bench_config(desc: dict, st: dict, ordering: str, world: int, flush: bool) -> dict:
+    """The `config` object of the JSON line (the same for both arms)."""
+    return dict(desc, cells=st["N"], faces=st["F"], ordering=ordering,
+                l2="flushed between timed steps" if flush else "working set larger than L2",
+                parallelism=f"replicas x{world}")
 
 
 def mesh_stats(mesh: Mesh):
@@ -141,16 +141,28 @@ def alg_bytes(st, prm) -> dict:
     gradlim = 0
     if need_grad:
         # k_gradlim: states + centres of the cell and its neighbours, list,
-        # face records (Green-Gauss weights or the limiter's face centres)
-        gradlim += qm + cg + nbl + fg + gl
+        # face records (Green-Gauss weights or the limiter's face centres);
+        # the mixed path reads the face-local offsets instead of the centres
+        gradlim += qm + cg + nbl + fg + gl + (F * 32 if mixed else 0)
         if prm.ilim == 2 and not prm.venkat_kh3:
             gradlim += N * 10 * g + (gl + N * 10 * g + cg + nbl + fg + N * 5 * g)   # min/max, global eps pass
     out["gradlim"] = gradlim
-    # k_residual: states, centres, face records, list, gradient records of the
-    # cell and its neighbours, wall states; writes res, dt and the two radii,
-    # and the per-block norm sums
-    out["residual"] = qm + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24 \
-        + ((N + 127) // 128) * 40
+    blocks = (N + 127) // 128
+    if mixed:
+        # k_face_pass: per face its two cells, FP64 normal and area, face-local
+        # offsets, the FP64 state records and gradient records of both cells
+        # (each read once: perfect reuse), wall states of the boundary faces;
+        # writes the 48-B face record.  k_face_sum: the neighbour lists, the
+        # face records, the volumes; writes res, dt and the two radii, and the
+        # per-block norm sums
+        out["residual"] = F * 8 + F * 32 + F * 32 + qm + (gl if need_grad else 0) + B * 44 + F * 48
+        out["residual_sum"] = nbl + F * 48 + N * 4 + N * 40 + N * 24 + blocks * 40
+    else:
+        # k_residual: states, centres, face records, list, gradient records of the
+        # cell and its neighbours, wall states; writes res, dt and the two radii,
+        # and the per-block norm sums
+        out["residual"] = qm + cg + fg + nbl + (gl if need_grad else 0) + B * 44 + N * 40 + N * 24 + blocks * 40
+        out["residual_sum"] = 0
     out["clip"] = N * 24 + N * g + N * 16                        # dt, radii, vol -> dt, diagonal
     dq = N * 8 * g                                               # increment records
     sweep = qs + cg + F * 4 * g + half_lists + dq + dq + N * 8 + N * 4   # neighbour dq, own dq write, diagonal, order
@@ -250,37 +262,109 @@ class ClockSampler:
 # CPU baselines (the reference built from its sources, or the oracle port)
 # ---------------------------------------------------------------------------
 REF_EXE = os.path.join(ROOT, "oracle", "_ref", "oneflow_ref")
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboforacle.so")
 
 
-def _ref_run(mesh, prm, steps, workdir):
-    case = os.path.join(workdir, "case")
-    write_case(case, mesh, P.to_dict(prm), steps)
+def reference_colour_order(mesh: Mesh):
+    """The colour-major renumbering (perm[new] = old) from the oracle
+    library, so that a reference run loads none of the product's code."""
+    import ctypes as C
+    L = C.CDLL(ORACLE_SO)
+    ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+    L.oro_colour_order.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip, ip]
+    perm = np.zeros(mesh.n_cells, np.int32)
+    n = L.oro_colour_order(mesh.n_cells, mesh.n_faces, mesh.n_bfaces, np.ascontiguousarray(mesh.lc, np.int32),
+                           np.ascontiguousarray(mesh.rc, np.int32), perm)
+    if n < 1:
+        raise RuntimeError("oro_colour_order failed")
+    return perm
+
+
+def _run_dirs(mesh, prm, steps, n, dump=False):
+    """One reference project written once (grid, scripts), and n run
+    directories whose case shares its grid and scripts; returns (base, dirs)."""
+    import shutil
+    base = tempfile.mkdtemp(prefix="ofgref_")
+    write_case(os.path.join(base, "case"), mesh, P.to_dict(prm), steps)
+    dirs = []
+    for i in range(n):
+        case = os.path.join(base, f"run{i}", "case")
+        os.makedirs(case)
+        shutil.copytree(os.path.join(base, "case", "script"), os.path.join(case, "script"))
+        os.symlink(os.path.join(base, "case", "grid"), os.path.join(case, "grid"))
+        for sub in ("results", "restart", "visual", "log"):
+            os.makedirs(os.path.join(case, sub))
+        dirs.append(os.path.dirname(case))
+    return base, dirs
+
+
+def reference_timed(mesh, prm, warm: int, timed: int, nproc: int, dump: bool = False):
+    """The reference CPU solver (built from its own sources) on `mesh`:
+    nproc concurrent single-rank solves of warm + timed outer iterations.
+    Each iteration's wall time is read from when its last residual line
+    appears on the process's line-buffered stdout (the reference prints one
+    line per solver per iteration), so set-up is excluded without a second
+    run.  Returns (aggregate cell-iter/s, seconds per iteration (median over
+    the processes), wall seconds of the whole run, the full-precision dump of
+    process 0 or None)."""
+    import shutil
+    base, dirs = _run_dirs(mesh, prm, warm + timed, nproc)
+    cmd = ([shutil.which("stdbuf"), "-oL"] if shutil.which("stdbuf") else []) + [REF_EXE, "0", "case"]
+    stamps = [dict() for _ in dirs]
     t0 = time.perf_counter()
-    r = subprocess.run([REF_EXE, "0", "case"], cwd=workdir, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-    t1 = time.perf_counter()
-    if r.returncode != 0:
-        raise RuntimeError(f"reference run failed ({r.returncode})")
-    return t1 - t0
+    procs = []
+    for i, d in enumerate(dirs):
+        env = dict(os.environ)
+        if dump and i == 0:
+            env["OFG_REF_DUMP"] = os.path.join(d, "dump.bin")
+        procs.append(subprocess.Popen(cmd, cwd=d, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT))
+
+    def reader(p, st):
+        for line in p.stdout:
+            f = line.split()
+            if len(f) >= 3 and f[0].isdigit() and f[1].isdigit():
+                st[int(f[0])] = time.perf_counter()
+
+    ths = [threading.Thread(target=reader, args=(p, st), daemon=True) for p, st in zip(procs, stamps)]
+    for t in ths:
+        t.start()
+    rcs = [p.wait() for p in procs]
+    for t in ths:
+        t.join(timeout=10)
+    wall = time.perf_counter() - t0
+    if any(rcs):
+        shutil.rmtree(base, ignore_errors=True)
+        raise RuntimeError(f"reference run failed: {rcs}")
+    per = []
+    for st in stamps:
+        if warm in st and warm + timed in st:
+            per.append((st[warm + timed] - st[warm]) / timed)
+    if len(per) != len(dirs):
+        shutil.rmtree(base, ignore_errors=True)
+        raise RuntimeError("reference iterations not seen on stdout")
+    out = None
+    if dump:
+        from oneflow_b200.meshio import read_ref_dump
+        out = read_ref_dump(os.path.join(dirs[0], "dump.bin"))
+    shutil.rmtree(base, ignore_errors=True)
+    return sum(mesh.n_cells / t for t in per), statistics.median(per), wall, out
 
 
-def reference_throughput(mesh, prm, n1, n2, nproc):
-    """Cell-iterations/s of the reference CPU solver: nproc concurrent
-    single-rank processes, per-iteration time from the difference of an
-    n1- and an n2-iteration run (setup cancels)."""
-    times = {}
-    for n in (n1, n2):
-        dirs = [tempfile.mkdtemp(prefix="ofgref_") for _ in range(nproc)]
-        for d in dirs:
-            write_case(os.path.join(d, "case"), mesh, P.to_dict(prm), n)
-        t0 = time.perf_counter()
-        procs = [subprocess.Popen([REF_EXE, "0", "case"], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-                 for d in dirs]
-        rcs = [p.wait() for p in procs]
-        times[n] = time.perf_counter() - t0
-        if any(rcs):
-            raise RuntimeError(f"reference run failed: {rcs}")
-    per_iter = (times[n2] - times[n1]) / (n2 - n1)
-    return mesh.n_cells * nproc / per_iter, per_iter
+def reference_options(prm):
+    """The reference's closest options to a configuration: it has only the
+    Green-Gauss gradient and its own Venkatakrishnan eps (vencat_coef *
+    max(qmax - qmin, 1)), so least squares and eps^2 = (K h)^3 fall back to
+    those; precision is its FP64.  Returns (params, note or None)."""
+    q = P.defaults(**P.to_dict(prm))
+    q.precision = 0
+    notes = []
+    if q.igrad == 2:
+        q.igrad = 0
+        notes.append("Green-Gauss gradients in place of least squares")
+    if q.ilim == 2 and q.venkat_kh3:
+        q.venkat_kh3 = 0
+        notes.append("the reference's Venkatakrishnan eps in place of eps^2=(K h)^3")
+    return q, ("; ".join(notes) + " (the reference has no such option)") if notes else None
 
 
 def oracle_port_throughput(mesh, prm, n1, n2):
@@ -305,6 +389,8 @@ def main():
     ap.add_argument("--no-converge", action="store_true", help="skip the time-to-1e-8-drop runs")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched airfoil runs")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start experiment")
+    ap.add_argument("--no-pinned", action="store_true", help="skip the reference-options variant of the workload")
+    ap.add_argument("--no-c1", action="store_true", help="skip the benchmark-size 2-D bump")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -327,28 +413,30 @@ def main():
         if not os.path.exists(REF_EXE):
             print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver not built (oracle/_ref)"}))
             return
-        # the reference runs on a bounded sample of the workload: the same
-        # configuration on a mesh small enough that nproc concurrent
-        # single-rank solves fit the host and the run ends in minutes
-        sample = _SAMPLE.get(args.config, args.config)
-        mesh, prm, desc = make_workload(sample)
-        _, _, full_desc = make_workload_desc(args.config)
-        prm.precision = 0
-        nproc = _ref_procs(mesh)
+        # the reference solver on the workload itself (its own mesh, renumbered
+        # as the GPU sweeps it): nproc concurrent single-rank solves, as many as
+        # host memory holds; one untimed iteration, then a few timed ones (each
+        # takes tens of seconds on one core at 6M cells)
+        mesh, prm, desc = make_workload(args.config)
+        st = mesh_stats(mesh)
+        prm_ref, note = reference_options(prm)
         if args.ordering == "colour":
-            from oneflow_b200 import colour_order
-            perm, _ = colour_order(mesh)
-            mesh = mesh.renumber_cells(perm)
-        steps = min(args.steps, 5) if mesh.n_cells > 200000 else args.steps
-        thr, per_iter = reference_throughput(mesh, prm, 2, 2 + steps, nproc)
+            mesh = mesh.renumber_cells(reference_colour_order(mesh))
+        nproc = _ref_procs(mesh)
+        warm, timed = 1, max(1, min(args.steps, 3))
+        thr, per_iter, wall, _ = reference_timed(mesh, prm_ref, warm, timed, nproc)
+        sample = (f"{nproc} concurrent single-rank solves of the reference CPU solver (built from its sources) on "
+                  f"the workload's {mesh.n_cells:,}-cell mesh, {warm} untimed + {timed} timed outer iterations each; "
+                  f"wall time per iteration from the processes' line-buffered residual output (median over the "
+                  f"processes); precomputed wall distance" + (f"; {note}" if note else ""))
         line = {"metric": "cell-iters/s", "value": thr, "unit": "cell-iter/s", "impl": "reference",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "n_gpus": args.gpus, "steps": timed, "warmup": warm,
                 "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (seeded mesh generator)",
-                "config": dict(full_desc, ordering=args.ordering, sample=desc["workload"], sample_cells=mesh.n_cells),
+                "config": bench_config(desc, st, args.ordering, world,
+                                       sum(alg_bytes(st, prm).values()) < 2 * L2_BYTES),
                 "cpu_baseline": {"value": thr, "unit": "cell-iter/s", "cores": nproc, "kind": "reference",
-                                 "sample": f"{nproc} concurrent single-rank reference solves of a {mesh.n_cells:,}-cell "
-                                           f"sample of the workload; per-iteration time = (t({2 + steps}) - t(2)) / {steps}"},
+                                 "sample": sample, "run_wall_s": wall},
                 "e2e": {"value": thr, "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -454,9 +542,15 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = st["N"] * e2e_steps * world / float(t.item())
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = _cpu_baseline(mesh, prm, args.config)
+        cpu, parity = parity_and_cpu_baseline(args.config, args.ordering, stream)
+    pinned = None
+    if rank == 0 and world == 1 and not args.no_pinned and args.config in _SAMPLE:
+        pinned = pinned_variant(mesh, prm, stream, min(args.steps, 50), args.warmup)
+    c1 = None
+    if rank == 0 and world == 1 and not args.no_c1:
+        c1 = config1_throughput(stream)
     conv = None
     if rank == 0 and world == 1 and not args.no_converge:
         conv = time_to_drop("bump2d_small", 1e-8, stream)
@@ -474,11 +568,10 @@ def main():
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prm.precision == 0 else "f32/f64",
                 "data": "synthetic (seeded mesh generator)",
-                "config": dict(desc, cells=st["N"], faces=st["F"], ordering=args.ordering,
-                               sweep_levels=list(s.sweep_levels()),
-                               l2="flushed between timed steps" if flush else "working set larger than L2",
-                               parallelism=f"replicas x{world}"),
-                "roofline": roofline, "cpu_baseline": cpu,
+                "config": bench_config(desc, st, args.ordering, world, flush),
+                "sweep_levels": list(s.sweep_levels()),
+                "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "pinned_variant": pinned,
+                "config1_bump2d": c1,
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": int(l1 - l0), "clocks": clocks, "time_to_1e-8": conv,
                 "setup": {"calc_wall_dist_s": wall_s, "wall_dist_vs_closed_form": wall_err},
@@ -584,33 +677,165 @@ def time_to_drop(config: str, target: float, stream, chunk: int = 200, max_iters
     return out
 
 
+def _rel_l2(a, b) -> float:
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+FORCE_KEYS = [0, 1, 2, 9, 10]   # Fx Fy Fz CL CD of Solver.forces / the reference's dump
+
+
+def _force_err(f, fr) -> float:
+    f, fr = np.asarray(f)[FORCE_KEYS], np.asarray(fr)[FORCE_KEYS]
+    return float(np.abs(f - fr).max() / max(np.abs(fr).max(), 1e-300))
+
+
+def parity_and_cpu_baseline(config: str, ordering: str, stream, steps: int = 12):
+    """Parity of the benchmarked path against the reference, and the CPU
+    baseline, from one run of the reference solver (built from its sources,
+    one process on one core) on the 600,000-cell sample of the workload with
+    the reference's own gradient and limiter options (Green-Gauss, its
+    Venkatakrishnan eps: the options whose parity the reference pins).  The
+    GPU runs the same mesh and options for the same number of iterations on
+    both paths; the reference sweeps the mesh renumbered in the colour-major
+    order, which is what the GPU's colour-major sweep computes, and its fields
+    are mapped back to the storage order.  Returns (cpu_baseline, parity)."""
+    from oneflow_b200 import Solver
+    from oneflow_b200.solver import TURB_SOLVER
+    sample = _SAMPLE.get(config, config)
+    mesh, prm, desc = make_workload(sample)
+    prm_ref, note = reference_options(prm)
+    N = mesh.n_cells
+    if not os.path.exists(REF_EXE):
+        thr, per_iter = oracle_port_throughput(mesh, prm_ref, 2, 4)
+        return ({"value": thr, "unit": "cell-iter/s", "cores": 1, "kind": "port",
+                 "sample": f"CPU restatement, 1 thread, {N:,}-cell sample, 2 iterations (reference build absent)"},
+                None)
+    perm = reference_colour_order(mesh) if ordering == "colour" else np.arange(N)
+    rmesh = mesh.renumber_cells(perm) if ordering == "colour" else mesh
+    thr, per_iter, wall, dump = reference_timed(rmesh, prm_ref, 1, steps - 1, 1, dump=True)
+    cpu = {"value": thr, "unit": "cell-iter/s", "cores": 1, "kind": "reference",
+           "sample": f"reference CPU solver (built from its sources), 1 process on 1 core, the {N:,}-cell sample of "
+                     f"the workload ({desc['workload'].split(':')[0]}), iterations 2-{steps} timed from its "
+                     f"line-buffered residual output" + (f"; {note}" if note else "")}
+
+    def ref_field(name, e=0):
+        out = np.empty(N)
+        out[perm] = dump[name][e, :N]
+        return out
+
+    ref = {"rho": ref_field("q", 0), "p": ref_field("q", 4), "forces": dump["forces"].ravel()[:13]}
+    sa = prm.vismodel >= 3
+    if sa:
+        ref["nut"] = ref_field("turbq")
+        ref["vist"] = ref_field("vist")
+    out = {"workload": f"{N:,}-cell sample of the workload, the reference's options: "
+                       + (note or "as configured"), "steps": steps,
+           "tolerance": {"forces_rel": 1e-6, "field_rel_l2": 1e-5},
+           "reference_forces": {"CL": float(ref["forces"][9]), "CD": float(ref["forces"][10])}}
+    got = {}
+    for key, prec in (("fp64", 0), ("mixed", 1)):
+        q = P.defaults(**P.to_dict(prm_ref))
+        q.precision = prec
+        q.sweep_order = 1 if ordering == "colour" else 0
+        s = Solver(mesh, q)
+        s.set_stream(stream.cuda_stream)
+        s.init_flowfield()
+        s.step(steps)
+        st = s.state()
+        g = {"rho": st[0, :N], "p": st[4, :N], "forces": s.forces(1.0)}
+        if sa:
+            g["nut"] = s.state(TURB_SOLVER)[:N]
+            g["vist"] = s.field("vist")[:N]
+        got[key] = g
+        r = {"rho_l2": _rel_l2(g["rho"], ref["rho"]), "p_l2": _rel_l2(g["p"], ref["p"]),
+             "forces_rel": _force_err(g["forces"], ref["forces"]),
+             "CL": float(g["forces"][9]), "CD": float(g["forces"][10])}
+        if sa:
+            r["nut_l2"] = _rel_l2(g["nut"], ref["nut"])
+            r["mu_t_l2"] = _rel_l2(g["vist"], ref["vist"])
+        out[f"{key}_vs_reference"] = r
+        s.close()
+    a, b = got["mixed"], got["fp64"]
+    out["mixed_vs_fp64"] = {"rho_l2": _rel_l2(a["rho"], b["rho"]), "p_l2": _rel_l2(a["p"], b["p"]),
+                            "forces_rel": _force_err(a["forces"], b["forces"])}
+    if sa:
+        out["mixed_vs_fp64"]["nut_l2"] = _rel_l2(a["nut"], b["nut"])
+        out["mixed_vs_fp64"]["mu_t_l2"] = _rel_l2(a["vist"], b["vist"])
+    return cpu, out
+
+
+def _timed_steps(s, stream, steps: int, flush_buf=None) -> float:
+    """Device ms of `steps` outer iterations on the solver's stream (CUDA
+    events); with flush_buf, a write larger than L2 before every step, each
+    step timed alone."""
+    import torch
+    if flush_buf is None:
+        a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+        a.record(stream); s.step(steps); b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+    ev = []
+    for _ in range(steps):
+        flush_buf.fill_(1.0)
+        a = torch.cuda.Event(enable_timing=True); b = torch.cuda.Event(enable_timing=True)
+        a.record(stream); s.step(1); b.record(stream)
+        ev.append((a, b))
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev)
+
+
+def pinned_variant(mesh, prm, stream, steps: int, warmup: int):
+    """The workload's mesh on the benchmarked (mixed) path with the reference's
+    own gradient and limiter options -- the variant `parity` pins against the
+    reference -- timed like the main line."""
+    from oneflow_b200 import Solver
+    q, note = reference_options(prm)
+    q.precision = prm.precision
+    q.sweep_order = prm.sweep_order
+    s = Solver(mesh, q)
+    s.set_stream(stream.cuda_stream)
+    s.init_flowfield()
+    s.step(warmup)
+    ms = _timed_steps(s, stream, steps)
+    s.close()
+    return {"options": note, "value": mesh.n_cells * steps / (ms * 1e-3), "unit": "cell-iter/s",
+            "ms_per_step": ms / steps, "steps": steps, "warmup": warmup}
+
+
+def config1_throughput(stream, steps: int = 200, warmup: int = 5):
+    """The 2-D Euler bump at its benchmark size (65,536 triangles, first-order
+    Roe, LU-SGS, CFL 5): cell-iter/s on the FP64 path sweeping in the
+    reference's cell order, and on the mixed path with colour-major sweeps.
+    Its working set (about 40 MB) fits L2, so L2 is flushed before every
+    timed step."""
+    import torch
+    from oneflow_b200 import Solver
+    mesh, prm0, desc = make_workload("bump2d")
+    flush = torch.empty(int(2 * L2_BYTES // 4), dtype=torch.float32, device="cuda")
+    out = {"workload": desc["workload"], "cells": mesh.n_cells, "steps": steps,
+           "l2": "flushed before every timed step"}
+    for key, prec, order in (("fp64_reference_order", 0, 0), ("mixed_colour_order", 1, 1)):
+        q = P.defaults(**P.to_dict(prm0))
+        q.precision = prec
+        q.sweep_order = order
+        s = Solver(mesh, q)
+        s.set_stream(stream.cuda_stream)
+        s.init_flowfield()
+        s.step(warmup)
+        ms = _timed_steps(s, stream, steps, flush)
+        out[key] = {"value": mesh.n_cells * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                    "sweep_levels": list(s.sweep_levels())}
+        s.close()
+    return out
+
+
 def _peak_hbm():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
             return {"value": float(json.load(fh)["hbm_gbs"]), "source": "measured"}
     except Exception:
         return {"value": 6650.0, "source": "fallback"}
-
-
-def _cpu_baseline(mesh, prm, config):
-    if config in _SAMPLE:
-        mesh, prm, _ = make_workload(_SAMPLE[config])
-    prm.precision = 0
-    if os.path.exists(REF_EXE):
-        n1, n2 = (5, 25) if mesh.n_cells < 200000 else (2, 4)
-        try:
-            thr, per_iter = reference_throughput(mesh, prm, n1, n2, 1)
-            return {"value": thr, "unit": "cell-iter/s", "cores": 1, "kind": "reference",
-                    "sample": f"reference CPU solver (built from its sources), 1 process, {mesh.n_cells:,}-cell "
-                              f"{'sample' if config in _SAMPLE else 'full mesh'}, "
-                              f"(t({n2}) - t({n1})) / {n2 - n1} iterations"}
-        except Exception as e:  # fall back to the port
-            note = f"reference run failed: {e}"
-    else:
-        note = "reference build absent"
-    thr, per_iter = oracle_port_throughput(mesh, prm, 2, 6)
-    return {"value": thr, "unit": "cell-iter/s", "cores": 1, "kind": "port",
-            "sample": f"CPU restatement, 1 thread, full mesh, 4 iterations ({note})"}
 
 
 if __name__ == "__main__":

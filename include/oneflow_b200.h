@@ -277,13 +277,15 @@ int ofg_set_stream(ofg_ctx *ctx, void *stream);
 
 /* One outer iteration launched task by task (no graph) with CUDA events
    between the groups; ms[] receives the device time of: CFL advance;
-   CALC_TIME_STEP + UPDATE_RESIDUALS as its three kernels (gradients +
-   limiter, flux/time-step gather, time-step clip); LUSGS_LOWER_SWEEP,
+   CALC_TIME_STEP + UPDATE_RESIDUALS as its parts (gradients + limiter;
+   the flux/time-step pass -- the FP64 path's per-cell gather, the mixed
+   path's face pass; the mixed path's per-cell sum of the face results, an
+   empty group on the FP64 path; time-step clip); LUSGS_LOWER_SWEEP,
    LUSGS_UPPER_SWEEP, UPDATE_FLOWFIELD, CALC_BOUNDARY, residual norm; and
    with the SA model seven more (nu~ boundary + gradient, its rhs gather,
    lower, upper, update, boundary, norm);
    launches[] the number of kernel launches of each group.  Both arrays
-   must hold 16 entries. */
+   must hold 17 entries. */
 int ofg_profile_step(ofg_ctx *ctx, double *ms, int *launches);
 
 /* Number of dependency levels of the lower and upper LU-SGS sweeps in the

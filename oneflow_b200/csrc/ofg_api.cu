@@ -433,6 +433,7 @@ void ofg_destroy(ofg_ctx *c) {
     destroy_graphs(c);
     void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
                     c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist, c->d_wall, c->d_wallG,
+                    c->d_fgeoD, c->d_fofs, c->d_lr, c->d_fout,
                     c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_rad,
                     c->d_bcq, c->d_partial, c->d_npart, c->d_tpart, c->d_red, c->d_redCount, c->d_stage, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
@@ -558,11 +559,34 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         pack_geometry(c, fg, cg);
         if ((rc = upload_bytes(c, &c->d_fgeo, fg.data(), fg.size() * sizeof(float)))) return rc;
         if ((rc = upload_bytes(c, &c->d_cgeo, cg.data(), cg.size() * sizeof(float)))) return rc;
+        // the face pass's inputs: FP64 face records, face-local offsets
+        // (x_f - x_L, x_f - x_R formed in FP64 and rounded once, and their
+        // lengths) and the two cells of each face; and its output records
+        std::vector<double> fgd, cgd;
+        pack_geometry(c, fgd, cgd);
+        if ((rc = upload(c, &c->d_fgeoD, fgd.data(), fgd.size()))) return rc;
+        std::vector<float> fo((size_t)nFaces * FOFS);
+        std::vector<int> lr((size_t)nFaces * 2);
+        for (int f = 0; f < nFaces; ++f) {
+            int l = c->lc[f], r = c->rc[f];
+            double a[3] = {c->xfc[f] - c->xcc[l], c->yfc[f] - c->ycc[l], c->zfc[f] - c->zcc[l]};
+            double b[3] = {c->xfc[f] - c->xcc[r], c->yfc[f] - c->ycc[r], c->zfc[f] - c->zcc[r]};
+            float *o = &fo[(size_t)f * FOFS];
+            for (int k = 0; k < 3; ++k) { o[k] = float(a[k]); o[3 + k] = float(b[k]); }
+            o[6] = float(std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+            o[7] = float(std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]));
+            lr[2 * (size_t)f] = l; lr[2 * (size_t)f + 1] = r;
+        }
+        if ((rc = upload(c, &c->d_fofs, fo.data(), fo.size()))) return rc;
+        if ((rc = upload(c, &c->d_lr, lr.data(), lr.size()))) return rc;
+        if ((rc = upload<double>(c, &c->d_fout, nullptr, (size_t)nFaces * FOR))) return rc;
     } else {
         std::vector<double> fg, cg;
         pack_geometry(c, fg, cg);
         if ((rc = upload_bytes(c, &c->d_fgeo, fg.data(), fg.size() * sizeof(double)))) return rc;
         if ((rc = upload_bytes(c, &c->d_cgeo, cg.data(), cg.size() * sizeof(double)))) return rc;
+        for (void **v : {(void **)&c->d_fgeoD, (void **)&c->d_fofs, (void **)&c->d_lr, (void **)&c->d_fout})
+            if (*v) { cudaFree(*v); *v = nullptr; }
     }
     size_t nT = c->nT, N = nCells;
     if ((rc = upload<double>(c, &c->d_q[0], nullptr, nT * REC))) return rc;
@@ -1317,16 +1341,16 @@ int ofg_profile_step(ofg_ctx *c, double *ms, int *launches) {
     double sc[2] = {double(c->outerSteps), double(c->outerSteps)};
     CK(cudaMemcpyAsync(c->d_scal + S_STEP, sc, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_scal + S_THISTN, sc, sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    // groups: the 9 NS groups (cfl; gradients+limiter, flux/time-step gather,
-    // time-step clip; lower, upper, update, boundary, norm), then the 7 SA
-    // groups (nu~ boundary+gradient, rhs gather, lower, upper, update,
-    // boundary, norm): the kernels of one ofg_step in the same order
-    static const int kNsProf[] = {T_ADVANCE, T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_LOWER, T_UPPER, T_UPDATE,
+    // groups: the 10 NS groups (cfl; gradients+limiter, flux/time-step pass,
+    // face-result sum, time-step clip; lower, upper, update, boundary, norm),
+    // then the 7 SA groups (nu~ boundary+gradient, rhs gather, lower, upper,
+    // update, boundary, norm): the kernels of one ofg_step in the same order
+    static const int kNsProf[] = {T_ADVANCE, T_P_GRADLIM, T_P_FLUX, T_P_FSUM, T_P_CLIP, T_LOWER, T_UPPER, T_UPDATE,
                                   T_BOUNDARY_NEXT, T_NORM};
     static const int kTurbProf[] = {T_P_TURB_GRAD, T_P_TURB_FLUX, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE,
                                     T_TURB_BOUNDARY, T_TURB_NORM};
-    const int nns = 9, nt = has_turb(c) ? 7 : 0, n = nns + nt;
-    cudaEvent_t ev[17];
+    const int nns = 10, nt = has_turb(c) ? 7 : 0, n = nns + nt;
+    cudaEvent_t ev[18];
     for (int i = 0; i <= n; ++i) CK(cudaEventCreate(&ev[i]));
     CK(cudaEventRecord(ev[0], c->stream));
     for (int i = 0; i < n; ++i) {

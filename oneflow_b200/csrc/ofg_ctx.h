@@ -32,6 +32,10 @@ struct ofg_ctx {
     int *d_lo_off = nullptr, *d_lol = nullptr, *d_up_off = nullptr, *d_upl = nullptr;
     int *d_lowOrder = nullptr, *d_upOrder = nullptr, *d_key = nullptr;
     void *d_fgeo = nullptr, *d_cgeo = nullptr;              // face / cell records at the face precision
+    double *d_fgeoD = nullptr;                              // mixed path: FP64 face records
+    float *d_fofs = nullptr;                                // mixed path: face-local offsets [F][FOFS]
+    int *d_lr = nullptr;                                    // mixed path: {left, right} cell of each face
+    double *d_fout = nullptr;                               // mixed path: face-pass results [F][FOR]
     double *d_wdist = nullptr;
     int nWall = 0;
     int *d_wall = nullptr;                                  // solid-wall faces {face, interior cell} (int2)
@@ -84,7 +88,7 @@ enum Task {
     T_TURB_RHS, T_TURB_LOWER, T_TURB_UPPER, T_TURB_UPDATE, T_TURB_BOUNDARY, T_TURB_BOUNDARY_CUR, T_TURB_NORM,
     T_TURB_NORM_ONLY,
     // parts of T_TS_RES / T_TURB_RHS, timed separately by ofg_profile_step
-    T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_P_TURB_GRAD, T_P_TURB_FLUX,
+    T_P_GRADLIM, T_P_FLUX, T_P_CLIP, T_P_TURB_GRAD, T_P_TURB_FLUX, T_P_FSUM,
     T_FORCES, T_GRAD_ONLY, T_CALC_LHS
 };
 int launch_task_f64(ofg_ctx *c, int task, cudaStream_t s);

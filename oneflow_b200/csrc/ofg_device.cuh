@@ -33,9 +33,12 @@ enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4, ITT = 5, IML = 6, IMT = 7 };
 #ifndef OFG_MINB_TR
 #define OFG_MINB_TR 8
 #endif
-template <typename R> struct MinBlocks { enum { res = 1, gl = 1, sw = 1, tr = 1 }; };
+#ifndef OFG_MINB_FP
+#define OFG_MINB_FP 3
+#endif
+template <typename R> struct MinBlocks { enum { res = 1, gl = 1, sw = 1, tr = 1, fp = 1 }; };
 template <> struct MinBlocks<float> {
-    enum { res = OFG_MINB_RES, gl = OFG_MINB_GL, sw = OFG_MINB_SW, tr = OFG_MINB_TR };
+    enum { res = OFG_MINB_RES, gl = OFG_MINB_GL, sw = OFG_MINB_SW, tr = OFG_MINB_TR, fp = OFG_MINB_FP };
 };
 
 constexpr int kRedBlocks = 148;   // blocks of the grid reductions (one per SM)
@@ -45,6 +48,9 @@ constexpr int FGR = 8;    // face record: nx ny nz area xfc yfc zfc dist (|n . (
 constexpr int CGR = 4;    // cell record: xcc ycc zcc vol
 constexpr int DQR = 8;    // increment record: dq[5] + 3 zero slots (64 B FP64, 32 B FP32: whole sectors)
 constexpr int MMR = 10;   // neighbour min/max differences per cell (Venkatakrishnan with the zone-wide eps)
+constexpr int FOR = 6;    // face-pass record (mixed path): flux[5] FP64, then the inviscid and viscous
+                          // spectral radii as two FP32 values in the sixth slot (48 B, three 16-B words)
+constexpr int FOFS = 8;   // face-local offsets record (mixed path), FP32
 
 // slots of the small device scalar array (cfl, min dt, limiter eps, norms,
 // outer-step counter, residual-history length)
@@ -161,10 +167,13 @@ __device__ __forceinline__ void roeFlux(const R *p1, const R *p2, R xn, R yn, R 
 // eigenvalues and the dissipation d = |A| (qR - qL), a small correction near
 // convergence, are FP32, from the FP32 copies f1/f2 of the same states.  The
 // face flux is (fc - d) / 2.  og1 = 1/(gamma-1); the FP64 part has no division.
+// The central part takes the FP64 unit normal (xn, yn, zn), so that the
+// pressure terms of a cell's faces cancel to FP64 round-off in a uniform
+// state; the dissipation takes its FP32 rounding (xnf, ynf, znf).
 __device__ __forceinline__ void roeFluxMixed(const double *p1, const double *p2, const float *f1, const float *f2,
-                                             float xnf, float ynf, float znf, float gam, double og1, int ieigenfix,
-                                             float ce1, float ce2, double *fc, float *d) {
-    const double xn = xnf, yn = ynf, zn = znf;
+                                             double xn, double yn, double zn, float xnf, float ynf, float znf,
+                                             float gam, double og1, int ieigenfix, float ce1, float ce2, double *fc,
+                                             float *d) {
     double rl = p1[IR], ul = p1[IU], vl = p1[IV], wl = p1[IW], pl = p1[IP];
     double rr = p2[IR], ur = p2[IU], vr = p2[IV], wr = p2[IW], pr = p2[IP];
     double el = pl * og1 + 0.5 * rl * SQR3(ul, vl, wl);   // total energy per volume
@@ -269,6 +278,67 @@ __device__ __forceinline__ void slau2Flux(const R *p1, const R *p2, R xn, R yn, 
     flux[2] = (mp * vl + mn * vr) + yn * ps;
     flux[3] = (mp * wl + mn * wr) + zn * ps;
     flux[4] = (mp * hl + mn * hr) + vfn * ps;
+}
+
+// The same SLAU2 flux for the FP32-face path, split by magnitude like the
+// mixed Roe flux.  With mp psi_L + mn psi_R = ms/2 (psi_L + psi_R) -
+// |ms|/2 (psi_R - psi_L), psi = (1, u, v, w, h), the face flux is fc - d with
+//   fc = ms/2 (psi_L + psi_R) + n p_c,   p_c = (p_L + p_R)/2          (FP64)
+//   d  = |ms|/2 (psi_R - psi_L) - n p_d                                (FP32)
+// where p_d = ps - p_c holds the pressure-split and low-Mach terms of ps.
+// The enthalpies, the pressure average and the jumps psi_R - psi_L, p_R - p_L
+// are formed in FP64 from the FP64 face states p1/p2 (at low Mach numbers p
+// and h carry the large 1/(gamma M^2) terms), and so are the O(1) parts of
+// the mass flux ms (rho vn and the averaged normal speed); the Mach splits,
+// the switch g, the low-Mach factor ka, the pressure-diffusion term of ms and
+// p_d are FP32 from the FP32 copies f1/f2 and the FP32 jumps.  The central
+// pressure term takes the FP64 normal (xn, yn, zn); d takes its FP32 rounding
+// (xnf, ynf, znf).
+__device__ __forceinline__ void slau2FluxMixed(const double *p1, const double *p2, const float *f1, const float *f2,
+                                               double xn, double yn, double zn, float xnf, float ynf, float znf,
+                                               float gam, double *fc, float *d) {
+    const float half = 0.5f, one = 1.0f;
+    const double gg = double(gam) / (double(gam) - 1.0);
+    double hlD = gg * (p1[IP] / p1[IR]) + 0.5 * SQR3(p1[IU], p1[IV], p1[IW]);
+    double hrD = gg * (p2[IP] / p2[IR]) + 0.5 * SQR3(p2[IU], p2[IV], p2[IW]);
+    float rl = f1[IR], ul = f1[IU], vl = f1[IV], wl = f1[IW], pl = f1[IP];
+    float rr = f2[IR], ur = f2[IU], vr = f2[IV], wr = f2[IW], pr = f2[IP];
+    float dp = float(p2[IP] - p1[IP]);   // p_R - p_L
+    float v2l = SQR3(ul, vl, wl), v2r = SQR3(ur, vr, wr);
+    const double vnlD = xn * p1[IU] + yn * p1[IV] + zn * p1[IW];
+    const double vnrD = xn * p2[IU] + yn * p2[IV] + zn * p2[IW];
+    float vnl = float(vnlD), vnr = float(vnrD);
+    float orl = one / (rl + small_v<float>()), orr = one / (rr + small_v<float>());
+    float c2l = gam * pl * orl, c2r = gam * pr * orr;
+    float cl = sqrtf(c2l), cr = sqrtf(c2r);
+    float cm = half * (cl + cr);
+    const double tD = p2[IR] / p1[IR];
+    const double vnaD = (fabs(vnlD) + tD * fabs(vnrD)) / (1.0 + tD);
+    float ml = vnl / cm, mr = vnr / cm;
+    float g = -fmaxf(fminf(ml, 0.0f), -1.0f) * fminf(fmaxf(mr, 0.0f), 1.0f);
+    const double gD = g;
+    const double vnpD = (1.0 - gD) * vnaD + gD * fabs(vnlD);
+    const double vnnD = (1.0 - gD) * vnaD + gD * fabs(vnrD);
+    float va = sqrtf(half * (v2l + v2r));
+    float m12 = fminf(one, va / cm);
+    float ka = (one - m12) * (one - m12);
+    const double msD = 0.5 * (p1[IR] * (vnlD + vnpD) + p2[IR] * (vnrD - vnnD)) - double(half * ka * dp / cm);
+    const float ms = float(msD);
+    float fp5ml = fpSplit5(ml, 0.0f, one);
+    float fp5mr = fpSplit5(mr, 0.0f, -one);
+    float pd = half * (fp5ml - fp5mr) * (-dp) + va * (fp5ml + fp5mr - one) * sqrtf(rl * rr) * cm;
+    const double pc = 0.5 * (p1[IP] + p2[IP]);
+    fc[0] = msD;
+    fc[1] = 0.5 * msD * (p1[IU] + p2[IU]) + xn * pc;
+    fc[2] = 0.5 * msD * (p1[IV] + p2[IV]) + yn * pc;
+    fc[3] = 0.5 * msD * (p1[IW] + p2[IW]) + zn * pc;
+    fc[4] = 0.5 * msD * (hlD + hrD);
+    const float am = half * fabsf(ms);
+    d[0] = 0.0f;
+    d[1] = am * float(p2[IU] - p1[IU]) - xnf * pd;
+    d[2] = am * float(p2[IV] - p1[IV]) - ynf * pd;
+    d[3] = am * float(p2[IW] - p1[IW]) - znf * pd;
+    d[4] = am * float(hrD - hlD);
 }
 
 }  // namespace ofg

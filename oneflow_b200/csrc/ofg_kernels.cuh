@@ -27,6 +27,11 @@ struct KArgs {
     const double *walldist;                // [nCells]
     const R *fgeo;                         // [nFaces][FGR]
     const R *cgeo;                         // [nT][CGR]
+    const double *fgeoD;                   // [nFaces][FGR] the face records in FP64 (== fgeo on the FP64 path)
+    // mixed path only: face-local geometry and the face pass of the residual
+    const float *fofs;                     // [nFaces][8] x_f - x_L, x_f - x_R (formed in FP64), |x_f - x_L|, |x_f - x_R|
+    const int2 *lr;                        // [nFaces] left cell, right cell (ghost nCells + f on boundary faces)
+    double *fout;                          // [nFaces][FOR] face results of the face pass
     const double *q;  double *qn;          // master state records [nT][REC], current / next
     const R *qs;      R *qsn;              // state records read by face kernels (== master in FP64)
     double *res, *dt, *invsr, *vissr, *rad, *bcq;   // rad: LU-SGS diagonal
@@ -264,8 +269,19 @@ __device__ __forceinline__ void cell_limiter(const KArgs<R> &A, int c, const R *
         int2 en = __ldg(&A.nbl[k]);
         int f = nb_face(en);
         R fg[FGR];
-        ld8(A.fgeo + (size_t)f * FGR, fg);
-        R dx = fg[4] - cgc[0], dy = fg[5] - cgc[1], dz = fg[6] - cgc[2];
+        R dx, dy, dz;
+        if constexpr (sizeof(R) == 4) {
+            // x_f - x_c from the face's offsets (formed in FP64); the normal
+            // only for Barth
+            float fo[FOFS];
+            ld8(A.fofs + (size_t)f * FOFS, fo);
+            const bool rt = nb_right(en);
+            dx = rt ? fo[3] : fo[0]; dy = rt ? fo[4] : fo[1]; dz = rt ? fo[5] : fo[2];
+            if (A.P.ilim == 1) ld4(A.fgeo + (size_t)f * FGR, fg);
+        } else {
+            ld8(A.fgeo + (size_t)f * FGR, fg);
+            dx = fg[4] - cgc[0]; dy = fg[5] - cgc[1]; dz = fg[6] - cgc[2];
+        }
         R dot = R(0);
         if (A.P.ilim == 1) {
             R ds = Rsqrt(SQR3(dx, dy, dz));
@@ -289,7 +305,9 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
     R mn[NEQ], mx[NEQ];
     // The FP32 path forms every neighbour difference in FP64 from the FP64
     // records (a difference of two FP32-rounded pressures would carry the
-    // rounding of p itself) and sums differences, not values, over the faces.
+    // rounding of p itself) and sums differences, not values, over the faces;
+    // its geometric differences come from the face offsets x_f - x_L,
+    // x_f - x_R (formed in FP64, rounded once), never from FP32 coordinates.
     constexpr bool mixed = sizeof(R) == 4;
     if (active) {
         R qc[REC], cgc[CGR];
@@ -310,19 +328,25 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
                 int2 e2 = __ldg(&A.nbl[k]);
                 int nb = e2.y;
                 R qn[REC], cgn[CGR], dn[6];
+                R dx, dy, dz;
                 if constexpr (mixed) {
                     double t[REC];
                     ld8(A.q + (size_t)nb * REC, t);
 #pragma unroll
                     for (int v = 0; v < 6; ++v)   // the cell's own values re-read (L1 hits), not held
                         dn[v] = R(t[v < 5 ? v : ITT] - __ldg(A.q + (size_t)c * REC + (v < 5 ? v : ITT)));
+                    // x_nb - x_c = (x_f - x_c) - (x_f - x_nb), from the face's offsets
+                    float fo[FOFS];
+                    ld8(A.fofs + (size_t)nb_face(e2) * FOFS, fo);
+                    const float sg = nb_right(e2) ? -1.0f : 1.0f;
+                    dx = sg * (fo[0] - fo[3]); dy = sg * (fo[1] - fo[4]); dz = sg * (fo[2] - fo[5]);
                 } else {
                     ld8(A.qs + (size_t)nb * REC, qn);
 #pragma unroll
                     for (int v = 0; v < 6; ++v) dn[v] = qn[v < 5 ? v : ITT] - qc[v < 5 ? v : ITT];
+                    ld4(A.cgeo + (size_t)nb * CGR, cgn);
+                    dx = cgn[0] - cgc[0]; dy = cgn[1] - cgc[1]; dz = cgn[2] - cgc[2];
                 }
-                ld4(A.cgeo + (size_t)nb * CGR, cgn);
-                R dx = cgn[0] - cgc[0], dy = cgn[1] - cgc[1], dz = cgn[2] - cgc[2];
                 R w = R(1) / (dx * dx + dy * dy + dz * dz);
                 a11 += w * dx * dx; a12 += w * dx * dy; a13 += w * dx * dz;
                 a22 += w * dy * dy; a23 += w * dy * dz; a33 += w * dz * dz;
@@ -365,29 +389,37 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, i
                 int f = nb_face(e2), nb = e2.y;
                 bool right = nb_right(e2);
                 R qn[REC], cgn[CGR], fg[FGR], dn[6];
+                R cl, cr;
                 if constexpr (mixed) {
                     double t[REC];
                     ld8(A.q + (size_t)nb * REC, t);
 #pragma unroll
                     for (int v = 0; v < 6; ++v)   // the cell's own values re-read (L1 hits), not held
                         dn[v] = R(t[v < 5 ? v : ITT] - __ldg(A.q + (size_t)c * REC + (v < 5 ? v : ITT)));
+                    ld4(A.fgeo + (size_t)f * FGR, fg);   // normal and area
+                    if (A.P.igrad == 1) {
+                        cl = R(0.5); cr = R(0.5);
+                    } else {   // |x_f - x_L|, |x_f - x_R| formed in FP64
+                        float2 dd = __ldg(reinterpret_cast<const float2 *>(A.fofs + (size_t)f * FOFS + 6));
+                        R delta = R(1) / (dd.x + dd.y + small_v<R>());
+                        cl = dd.y * delta; cr = dd.x * delta;
+                    }
                 } else {
                     ld8(A.qs + (size_t)nb * REC, qn);
+                    ld4(A.cgeo + (size_t)nb * CGR, cgn);
+                    ld8(A.fgeo + (size_t)f * FGR, fg);
+                    const R *cl_ = right ? cgn : cgc, *cr_ = right ? cgc : cgn;
+                    if (A.P.igrad == 1) {
+                        cl = R(0.5); cr = R(0.5);
+                    } else {
+                        R dxl = fg[4] - cl_[0], dyl = fg[5] - cl_[1], dzl = fg[6] - cl_[2];
+                        R dxr = fg[4] - cr_[0], dyr = fg[5] - cr_[1], dzr = fg[6] - cr_[2];
+                        R delt1 = Rsqrt(SQR3(dxl, dyl, dzl)), delt2 = Rsqrt(SQR3(dxr, dyr, dzr));
+                        R delta = R(1) / (delt1 + delt2 + small_v<R>());
+                        cl = delt2 * delta; cr = delt1 * delta;
+                    }
                 }
-                ld4(A.cgeo + (size_t)nb * CGR, cgn);
-                ld8(A.fgeo + (size_t)f * FGR, fg);
                 const R *ql = right ? qn : qc, *qr = right ? qc : qn;
-                const R *cl_ = right ? cgn : cgc, *cr_ = right ? cgc : cgn;
-                R cl, cr;
-                if (A.P.igrad == 1) {
-                    cl = R(0.5); cr = R(0.5);
-                } else {
-                    R dxl = fg[4] - cl_[0], dyl = fg[5] - cl_[1], dzl = fg[6] - cl_[2];
-                    R dxr = fg[4] - cr_[0], dyr = fg[5] - cr_[1], dzr = fg[6] - cr_[2];
-                    R delt1 = Rsqrt(SQR3(dxl, dyl, dzl)), delt2 = Rsqrt(SQR3(dxr, dyr, dzr));
-                    R delta = R(1) / (delt1 + delt2 + small_v<R>());
-                    cl = delt2 * delta; cr = delt1 * delta;
-                }
                 R ar = fg[3];
                 R fnxa = fg[0] * ar, fnya = fg[1] * ar, fnza = fg[2] * ar;
                 // FP32 path: face value minus the cell value (the cell's own
@@ -799,69 +831,90 @@ __device__ __forceinline__ void face_vis_flux(const DevParams &P, const R *ql, c
     face_vis_flux<R, VV>(P, ql, qr, dlr, fg, cgl, cgr, gl, gr, bface, fv);
 }
 
-// One gather pass per cell: face radii + time step, inviscid residual and
-// viscous residual.  The FP64 path adds the viscous face terms after all the
-// inviscid ones, as the reference's two scatter passes do; the FP32 path adds
-// each face's inviscid and viscous terms together (one pass over the faces
-// instead of two).
+// The end of the residual pass of one cell: its residual and block sums of
+// squares (for the norms), and the local time step from the summed face
+// radii (UTimeStep::CalcInvTimeStep / CalcVisTimeStep) with the zone-wide
+// minimum.  The block epilogue sums the squares in a fixed order
+// (deterministic) and lowers the minimum time step by an atomic minimum on
+// the bit pattern (non-negative doubles order like their bits).  Every thread
+// of the block calls it; `active` is false past the last cell.
+template <bool doRes, bool doDt>
+__device__ __forceinline__ void residual_epilogue(const DevParams &P, double *res, double *dt, double *invsr,
+                                                  double *vissr, double *npart, double *scal, int c, bool active,
+                                                  const double *acc, double inv, double vis, double vol) {
+    double mydt = 1.0e40;
+    double sq[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (active) {
+        if (doRes) {
+            double *o = res + (size_t)c * NEQ;
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) { o[e] = acc[e]; sq[e] = acc[e] * acc[e]; }
+        }
+        if (doDt) {
+            double cfl = scal[S_CFL];
+            double ts;
+            if (P.timestepModel == 1) {
+                ts = P.global_dt;
+            } else {
+                ts = cfl * vol / inv;
+                if (P.vismodel > 0 && P.visTimeStepModel > 0) {
+                    double vts = cfl * vol / vis;
+                    ts *= vts / (ts + vts);
+                }
+            }
+            invsr[c] = inv;
+            vissr[c] = vis;
+            dt[c] = ts;
+            mydt = ts;
+        }
+    }
+    if (doRes) block_sum_to<NEQ>(sq, npart + (size_t)blockIdx.x * NEQ);
+    if (doDt) {
+        double m = block_min(mydt);
+        if (threadIdx.x == 0)
+            atomicMin(reinterpret_cast<unsigned long long *>(scal + S_MINDT), (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// The FP64 path's residual: one gather pass per cell -- face radii + time
+// step, inviscid residual, then the viscous residual in a second loop over the
+// same faces, as the reference's two scatter passes add them (every sum in
+// the reference's order, so the path rounds like the reference).
 // MODE 0: residual and time step (one outer iteration), 1: time step only
 // (the CALC_TIME_STEP task), 2: residual only (the UPDATE_RESIDUALS task).
 template <typename R, int MODE, bool VV = false>
 __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A) {
-    constexpr bool exactOrder = sizeof(R) == 8;
+    static_assert(sizeof(R) == 8, "the mixed path runs k_face_pass + k_face_sum");
     constexpr bool doRes = MODE != 1, doDt = MODE != 2;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double mydt = 1.0e40;
-    double sq[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (c < A.nCells) {
+    bool active = c < A.nCells;
+    double acc[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) acc[e] = -0.0;   // LoadResiduals: res = -rhs, rhs = 0
+    double inv = 0.0, vis = 0.0, vol = 0.0;
+    if (active) {
         const DevParams &P = A.P;
         R qc[REC], cgc[CGR], glc[GLR];
-        if constexpr (exactOrder) {
-            ld8(A.qs + (size_t)c * REC, qc);
-        } else {
-            double t[REC];
-            ld8(A.q + (size_t)c * REC, t);
-#pragma unroll
-            for (int i = 0; i < REC; ++i) qc[i] = R(t[i]);
-        }
+        ld8(A.qs + (size_t)c * REC, qc);
         ld4(A.cgeo + (size_t)c * CGR, cgc);
-        const double og1 = 1.0 / (P.gama - 1.0);
+        vol = double(cgc[3]);
         bool needGl = doRes && (P.ilim != -1 || P.vismodel > 0);
         if (needGl) {
 #pragma unroll
             for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)c * GLR + i, glc + i);
         }
         R gam = R(P.gama), ce1 = R(P.centropy1), ce2 = R(P.centropy2), orey = R(P.oreynolds);
-        double inv = 0.0, vis = 0.0;
-        double acc[NEQ];
-#pragma unroll
-        for (int e = 0; e < NEQ; ++e) acc[e] = -0.0;   // LoadResiduals: res = -rhs, rhs = 0
         int b = A.nb_off[c], en = A.nb_off[c + 1];
         // the next neighbour-list entry is loaded one face ahead, so that the
         // loads of a face's records do not wait on its list entry
         int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);
-        double qcD[NEQ];   // FP32 path: the FP64 cell values the face states start from
-        if constexpr (!exactOrder) {
-            ld4(A.q + (size_t)c * REC, qcD);
-            qcD[IP] = __ldg(A.q + (size_t)c * REC + IP);
-        }
         for (int k = b; k < en; ++k) {
             int2 e2 = e2n;
             if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
             int f = nb_face(e2), nb = e2.y;
             bool right = nb_right(e2);
             R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
-            double qnD[NEQ];
-            if constexpr (exactOrder) {
-                ld8(A.qs + (size_t)nb * REC, qn);
-            } else {
-                double t[REC];
-                ld8(A.q + (size_t)nb * REC, t);
-#pragma unroll
-                for (int i = 0; i < REC; ++i) qn[i] = R(t[i]);
-#pragma unroll
-                for (int e = 0; e < NEQ; ++e) qnD[e] = t[e];
-            }
+            ld8(A.qs + (size_t)nb * REC, qn);
             ld8(A.fgeo + (size_t)f * FGR, fg);
             ld4(A.cgeo + (size_t)nb * CGR, cgn);
             bool ghost = nb >= A.nCells;
@@ -878,46 +931,6 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
                 if (P.vismodel > 0) vis += face_vis_spec(P, ql, qr, fg, cgl, cgr);
             }
             if (!doRes) continue;
-            if constexpr (!exactOrder) {
-                // FP32 path: FP64 face states and central flux; the FP32
-                // dissipation and viscous term join before the FP64 accumulation
-                const double *qlD = right ? qnD : qcD, *qrD = right ? qcD : qnD;
-                R fvs[NEQ];   // viscous term, formed first while fewer values are live
-                if (P.vismodel > 0) {
-                    R fv[NEQ];
-                    face_vis_flux<R, VV>(P, ql, qr, fg, cgl, cgr, gll, glr, ghost, fv);
-                    R coeff = -orey * fg[3];
-#pragma unroll
-                    for (int e = 0; e < NEQ; ++e) fvs[e] = coeff * fv[e];
-                } else {
-#pragma unroll
-                    for (int e = 0; e < NEQ; ++e) fvs[e] = R(0);
-                }
-                double t1[NEQ], t2[NEQ];
-                R s1[NEQ], s2[NEQ];
-                face_states_mixed(A, f, qlD, qrD, ql, qr, fg, cgl, cgr, gll, glr, t1, t2, s1, s2);
-                if (P.ischeme == 12) {
-                    R fs[NEQ];
-                    slau2Flux(s1, s2, fg[0], fg[1], fg[2], gam, fs);
-#pragma unroll
-                    for (int e = 0; e < NEQ; ++e) {
-                        double v = double(fg[3] * fs[e] + fvs[e]);
-                        if (!right) acc[e] -= v; else acc[e] += v;
-                    }
-                } else {
-                    double fc[NEQ];
-                    R d[NEQ];
-                    roeFluxMixed(t1, t2, s1, s2, fg[0], fg[1], fg[2], gam, og1, P.ieigenfix, ce1, ce2, fc, d);
-                    R har = R(0.5) * fg[3];
-                    double hard = double(har);
-#pragma unroll
-                    for (int e = 0; e < NEQ; ++e) {
-                        double v = hard * fc[e] - double(har * d[e] - fvs[e]);
-                        if (!right) acc[e] -= v; else acc[e] += v;
-                    }
-                }
-                continue;
-            }
             R t1[NEQ], t2[NEQ], fl[NEQ];
             face_states(A, f, ql, qr, fg, cgl, cgr, gll, glr, t1, t2);
             if (P.ischeme == 12) slau2Flux(t1, t2, fg[0], fg[1], fg[2], gam, fl);
@@ -929,71 +942,181 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::res) k_residual(KArgs<R> A)
                 if (!right) acc[e] -= v; else acc[e] += v;
             }
         }
-        if (exactOrder && doRes && P.vismodel > 0) {
-            {
-                int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
-                for (int k = b; k < en; ++k) {
-                    int2 e2 = e2n;
-                    if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
-                    int f = nb_face(e2), nb = e2.y;
-                    bool right = nb_right(e2);
-                    R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
-                    ld8(A.qs + (size_t)nb * REC, qn);
-                    ld8(A.fgeo + (size_t)f * FGR, fg);
-                    ld4(A.cgeo + (size_t)nb * CGR, cgn);
-                    bool ghost = nb >= A.nCells;
-                    if (!ghost) {
+        if (doRes && P.vismodel > 0) {
+            int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
+            for (int k = b; k < en; ++k) {
+                int2 e2 = e2n;
+                if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
+                int f = nb_face(e2), nb = e2.y;
+                bool right = nb_right(e2);
+                R qn[REC], cgn[CGR], fg[FGR], gln[GLR];
+                ld8(A.qs + (size_t)nb * REC, qn);
+                ld8(A.fgeo + (size_t)f * FGR, fg);
+                ld4(A.cgeo + (size_t)nb * CGR, cgn);
+                bool ghost = nb >= A.nCells;
+                if (!ghost) {
 #pragma unroll
-                        for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)nb * GLR + i, gln + i);
-                    }
-                    const R *ql = right ? qn : qc, *qr = right ? qc : qn;
-                    const R *cgl = right ? cgn : cgc, *cgr = right ? cgc : cgn;
-                    const R *gll = right ? gln : glc, *glr = (right || ghost) ? glc : gln;
-                    R fv[NEQ];
-                    face_vis_flux<R, VV>(P, ql, qr, fg, cgl, cgr, gll, glr, ghost, fv);
-                    R coeff = -orey * fg[3];
+                    for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)nb * GLR + i, gln + i);
+                }
+                const R *ql = right ? qn : qc, *qr = right ? qc : qn;
+                const R *cgl = right ? cgn : cgc, *cgr = right ? cgc : cgn;
+                const R *gll = right ? gln : glc, *glr = (right || ghost) ? glc : gln;
+                R fv[NEQ];
+                face_vis_flux<R, VV>(P, ql, qr, fg, cgl, cgr, gll, glr, ghost, fv);
+                R coeff = -orey * fg[3];
 #pragma unroll
-                    for (int e = 0; e < NEQ; ++e) {
-                        double v = double(coeff * fv[e]);
-                        if (!right) acc[e] -= v; else acc[e] += v;
-                    }
+                for (int e = 0; e < NEQ; ++e) {
+                    double v = double(coeff * fv[e]);
+                    if (!right) acc[e] -= v; else acc[e] += v;
                 }
             }
-        }
-        if (doRes) {
-            double *o = A.res + (size_t)c * NEQ;
-#pragma unroll
-            for (int e = 0; e < NEQ; ++e) { o[e] = acc[e]; sq[e] = acc[e] * acc[e]; }
-        }
-        if (doDt) {
-            // local time step (UTimeStep::CalcInvTimeStep / CalcVisTimeStep)
-            double cfl = A.scal[S_CFL];
-            double vol = double(cgc[3]);
-            double ts;
-            if (P.timestepModel == 1) {
-                ts = P.global_dt;
-            } else {
-                ts = cfl * vol / inv;
-                if (P.vismodel > 0 && P.visTimeStepModel > 0) {
-                    double vts = cfl * vol / vis;
-                    ts *= vts / (ts + vts);
-                }
-            }
-            A.invsr[c] = inv;
-            A.vissr[c] = vis;
-            A.dt[c] = ts;
-            mydt = ts;
         }
     }
-    // block epilogue: sums of squares for the residual norm (fixed order:
-    // deterministic), and the zone-wide minimum time step by an atomic minimum
-    // on the bit pattern (non-negative doubles order like their bits)
-    if (doRes) block_sum_to<NEQ>(sq, A.npart + (size_t)blockIdx.x * NEQ);
+    residual_epilogue<doRes, doDt>(A.P, A.res, A.dt, A.invsr, A.vissr, A.npart, A.scal, c, active, acc, inv, vis,
+                                   vol);
+}
+
+// ---------------------------------------------------------------------------
+// The mixed path's UPDATE_RESIDUALS + CALC_TIME_STEP in two passes.
+//
+// k_face_pass: one thread per face, in face order (the face arrays are read
+// coalesced, each face's flux is evaluated once): the face's spectral radii,
+// its MUSCL face states, Roe or SLAU2 flux and viscous flux, written to the
+// face record fout[f] = {flux[5] (left to right, FP64), {inviscid, viscous
+// radius} (FP32)}.  Its geometry is local to the face: the offsets from the
+// face centre to the two cell centres, formed in FP64 from the reference's
+// metrics and rounded once to FP32 (so no FP32 rounding of an absolute
+// coordinate enters a difference), and the FP64 unit normal and area for the
+// FP64 central part of the Roe flux (so that in a uniform state the pressure
+// terms of a cell's faces cancel to FP64 round-off, as the reference's do).
+//
+// k_face_sum: one thread per cell adds its faces' records in ascending face
+// id -- the order of the reference's serial scatter (AddF2CField,
+// codes/usolver/src/UCom.cpp:144-171) -- into its residual and radii.  Both
+// cells of a face add the same FP64 value, so the sum over the mesh telescopes
+// exactly.  MODE as in k_residual.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_face_out(double *o, const double *v, float si, float sv) {
+    double packed = __hiloint2double(__float_as_int(sv), __float_as_int(si));
+    reinterpret_cast<double2 *>(o)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(o)[1] = make_double2(v[2], v[3]);
+    reinterpret_cast<double2 *>(o)[2] = make_double2(v[4], packed);
+}
+
+template <int MODE, bool VV = false>
+__global__ void __launch_bounds__(128, MinBlocks<float>::fp) k_face_pass(KArgs<float> A) {
+    constexpr bool doRes = MODE != 1, doDt = MODE != 2;
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= A.nFaces) return;
+    const DevParams &P = A.P;
+    const int2 lr = __ldg(A.lr + f);
+    const bool bface = f < A.nBFaces;
+    double nD[4];   // unit normal and area, FP64
+    ld4(A.fgeoD + (size_t)f * FGR, nD);
+    float fo[FOFS];
+    ld8(A.fofs + (size_t)f * FOFS, fo);
+    // the face's own frame: face centre at the origin, cell centres at
+    // -(x_f - x_L) and -(x_f - x_R); every kernel function below only forms
+    // differences of these positions
+    const float fg[FGR] = {float(nD[0]), float(nD[1]), float(nD[2]), float(nD[3]), 0.0f, 0.0f, 0.0f, 0.0f};
+    const float cgl[CGR] = {-fo[0], -fo[1], -fo[2], 0.0f}, cgr[CGR] = {-fo[3], -fo[4], -fo[5], 0.0f};
+    double tl[REC], tr[REC];
+    ld8(A.q + (size_t)lr.x * REC, tl);
+    ld8(A.q + (size_t)lr.y * REC, tr);
+    float ql[REC], qr[REC];
+#pragma unroll
+    for (int i = 0; i < REC; ++i) { ql[i] = float(tl[i]); qr[i] = float(tr[i]); }
+    float si = 0.0f, sv = 0.0f;
     if (doDt) {
-        double m = block_min(mydt);
-        if (threadIdx.x == 0)
-            atomicMin(reinterpret_cast<unsigned long long *>(A.scal + S_MINDT), (unsigned long long)__double_as_longlong(m));
+        si = float(face_inv_spec(P, ql, qr, fg));
+        if (P.vismodel > 0) sv = float(face_vis_spec(P, ql, qr, fg, cgl, cgr));
     }
+    double v[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (doRes) {
+        float gll[GLR], glr[GLR];
+        if (P.ilim != -1 || P.vismodel > 0) {
+#pragma unroll
+            for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)lr.x * GLR + i, gll + i);
+            // a ghost cell carries its interior cell's gradient (UGrad.cpp:140-148)
+            if (bface) {
+#pragma unroll
+                for (int i = 0; i < GLR; ++i) glr[i] = gll[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < GLR; i += 4) ld4(A.gl + (size_t)lr.y * GLR + i, glr + i);
+            }
+        }
+        const float gam = float(P.gama), ce1 = float(P.centropy1), ce2 = float(P.centropy2);
+        float fvs[NEQ];   // viscous term, formed first while fewer values are live
+        if (P.vismodel > 0) {
+            float fv[NEQ];
+            face_vis_flux<float, VV>(P, ql, qr, fg, cgl, cgr, gll, glr, bface, fv);
+            float coeff = -float(P.oreynolds) * fg[3];
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) fvs[e] = coeff * fv[e];
+        } else {
+#pragma unroll
+            for (int e = 0; e < NEQ; ++e) fvs[e] = 0.0f;
+        }
+        double t1[NEQ], t2[NEQ];
+        float s1[NEQ], s2[NEQ];
+        face_states_mixed(A, f, tl, tr, ql, qr, fg, cgl, cgr, gll, glr, t1, t2, s1, s2);
+        double fc[NEQ];
+        float d[NEQ];
+        double ard;   // the flux is ard * fc - (arf * d - fvs)
+        float arf;
+        if (P.ischeme == 12) {
+            slau2FluxMixed(t1, t2, s1, s2, nD[0], nD[1], nD[2], fg[0], fg[1], fg[2], gam, fc, d);
+            ard = nD[3]; arf = fg[3];
+        } else {
+            const double og1 = 1.0 / (P.gama - 1.0);
+            roeFluxMixed(t1, t2, s1, s2, nD[0], nD[1], nD[2], fg[0], fg[1], fg[2], gam, og1, P.ieigenfix, ce1, ce2,
+                         fc, d);
+            ard = 0.5 * nD[3]; arf = 0.5f * fg[3];
+        }
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) v[e] = ard * fc[e] - double(arf * d[e] - fvs[e]);
+    }
+    store_face_out(A.fout + (size_t)f * FOR, v, si, sv);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_face_sum(KArgs<float> A) {
+    constexpr bool doRes = MODE != 1, doDt = MODE != 2;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = c < A.nCells;
+    double acc[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) acc[e] = -0.0;   // LoadResiduals: res = -rhs, rhs = 0
+    double inv = 0.0, vis = 0.0, vol = 0.0;
+    if (active) {
+        vol = double(__ldg(A.cgeo + (size_t)c * CGR + 3));
+        int b = A.nb_off[c], en = A.nb_off[c + 1];
+        int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
+        for (int k = b; k < en; ++k) {
+            int2 e2 = e2n;
+            if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
+            const double2 *o = reinterpret_cast<const double2 *>(A.fout + (size_t)nb_face(e2) * FOR);
+            double2 a = __ldg(o), bb = __ldg(o + 1), cc = __ldg(o + 2);
+            if (doDt) {
+                int2 sp = make_int2(__double2loint(cc.y), __double2hiint(cc.y));
+                inv += double(__int_as_float(sp.x));
+                vis += double(__int_as_float(sp.y));
+            }
+            if (doRes) {
+                double v[NEQ] = {a.x, a.y, bb.x, bb.y, cc.x};
+                if (!nb_right(e2)) {
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) acc[e] -= v[e];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < NEQ; ++e) acc[e] += v[e];
+                }
+            }
+        }
+    }
+    residual_epilogue<doRes, doDt>(A.P, A.res, A.dt, A.invsr, A.vissr, A.npart, A.scal, c, active, acc, inv, vis,
+                                   vol);
 }
 
 // ---------------------------------------------------------------------------
@@ -1345,8 +1468,8 @@ __global__ void __launch_bounds__(256) k_boundary(KArgs<R> A, const int *lcb) {
     int g = A.nCells + f;
     double t[NEQ], pr[NEQ];
     bool havePrim = false;
-    const R *fg = A.fgeo + (size_t)f * FGR;
-    double xn = double(fg[0]), yn = double(fg[1]), zn = double(fg[2]), vfn = 0.0;
+    const double *fg = A.fgeoD + (size_t)f * FGR;   // FP64 normal on both paths
+    double xn = fg[0], yn = fg[1], zn = fg[2], vfn = 0.0;
     double gama = A.P.gama;
     if (bt == BC_SYM || (bt == BC_SOLID && A.P.vismodel == 0)) {
         double vn = xn * s[IU] + yn * s[IV] + zn * s[IW] - vfn;

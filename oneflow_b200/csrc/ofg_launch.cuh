@@ -42,6 +42,8 @@ KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
     A.up_off = c->d_up_off; A.upl = reinterpret_cast<const int2 *>(c->d_upl);
     A.bcType = c->d_bct; A.key = c->d_key; A.walldist = c->d_wdist;
     A.fgeo = static_cast<const R *>(c->d_fgeo); A.cgeo = static_cast<const R *>(c->d_cgeo);
+    A.fgeoD = sizeof(R) == 8 ? static_cast<const double *>(c->d_fgeo) : c->d_fgeoD;
+    A.fofs = c->d_fofs; A.lr = reinterpret_cast<const int2 *>(c->d_lr); A.fout = c->d_fout;
     int nx = onCurrent ? c->cur : c->cur ^ 1;
     A.q = c->d_q[c->cur];
     A.qn = c->d_q[nx];
@@ -87,6 +89,26 @@ void launch_gradlim(ofg_ctx *c, const KArgs<R> &A, cudaStream_t s) {
     }
 }
 
+// The flux / time-step pass of MODE (as k_residual): the FP64 path's
+// per-cell gather, or the mixed path's face pass followed by the per-cell sum
+// of the face results (part: 1 the first kernel only, 2 the second only, 3 both).
+template <typename R, int MODE>
+void launch_flux(ofg_ctx *c, const KArgs<R> &A, cudaStream_t s, int part = 3) {
+    const int N = c->nCells;
+    const bool vv = c->p.ivischeme >= 2;   // the TEST / NEW1 / NEW2 viscous face gradients
+    if constexpr (sizeof(R) == 8) {
+        if (!(part & 1)) return;
+        if (vv) OFG_LAUNCH((k_residual<R, MODE, true>), nblk(N, 128), 128, s, A);
+        else OFG_LAUNCH((k_residual<R, MODE>), nblk(N, 128), 128, s, A);
+    } else {
+        if (part & 1) {
+            if (vv) OFG_LAUNCH((k_face_pass<MODE, true>), nblk(c->nFaces, 128), 128, s, A);
+            else OFG_LAUNCH((k_face_pass<MODE>), nblk(c->nFaces, 128), 128, s, A);
+        }
+        if (part & 2) OFG_LAUNCH((k_face_sum<MODE>), nblk(N, 128), 128, s, A);
+    }
+}
+
 template <typename R>
 int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     const int N = c->nCells;
@@ -101,27 +123,26 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     }
     case T_TIMESTEP: {   // CALC_TIME_STEP alone (after T_CFL, which resets the minimum)
         KArgs<R> A = make_args<R>(c, false);
-        OFG_LAUNCH((k_residual<R, 1>), nblk(N, 128), 128, s, A);
+        launch_flux<R, 1>(c, A, s);
         OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }
     case T_RESIDUAL: {   // UPDATE_RESIDUALS alone
         KArgs<R> A = make_args<R>(c, false);
         launch_gradlim<R>(c, A, s);
-        if (c->p.ivischeme >= 2) OFG_LAUNCH((k_residual<R, 2, true>), nblk(N, 128), 128, s, A);
-        else OFG_LAUNCH((k_residual<R, 2>), nblk(N, 128), 128, s, A);
+        launch_flux<R, 2>(c, A, s);
         break;
     }
     case T_TS_RES:       // CALC_TIME_STEP + LOAD_RESIDUALS + UPDATE_RESIDUALS in one gather
     case T_P_GRADLIM:    // (its three parts, launched separately by the profiler)
     case T_P_FLUX:
+    case T_P_FSUM:
     case T_P_CLIP: {
         KArgs<R> A = make_args<R>(c, false);
         if (task == T_TS_RES || task == T_P_GRADLIM) launch_gradlim<R>(c, A, s);
-        if (task == T_TS_RES || task == T_P_FLUX) {   // VV: the TEST / NEW1 / NEW2 viscous face gradients
-            if (c->p.ivischeme >= 2) OFG_LAUNCH((k_residual<R, 0, true>), nblk(N, 128), 128, s, A);
-            else OFG_LAUNCH((k_residual<R, 0>), nblk(N, 128), 128, s, A);
-        }
+        if (task == T_TS_RES) launch_flux<R, 0>(c, A, s);
+        if (task == T_P_FLUX) launch_flux<R, 0>(c, A, s, 1);
+        if (task == T_P_FSUM) launch_flux<R, 0>(c, A, s, 2);
         if (task == T_TS_RES || task == T_P_CLIP) OFG_LAUNCH(k_timestep_clip<R>, nblk(N, 256), 256, s, A);
         break;
     }

@@ -182,17 +182,21 @@ class Solver:
         """Launch on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self.L.ofg_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
-    PROFILE_GROUPS = ("cfl", "gradlim", "residual", "clip", "lusgs_lower", "lusgs_upper", "update", "boundary",
-                      "norm", "sa_grad", "sa_residual", "sa_lower", "sa_upper", "sa_update", "sa_boundary", "sa_norm")
+    PROFILE_GROUPS = ("cfl", "gradlim", "residual", "residual_sum", "clip", "lusgs_lower", "lusgs_upper", "update",
+                      "boundary", "norm", "sa_grad", "sa_residual", "sa_lower", "sa_upper", "sa_update", "sa_boundary",
+                      "sa_norm")
 
     def profile_step(self):
         """One iteration task by task with CUDA events: ({group: ms}, {group: launches}).
-        "residual" is the flux + time-step gather kernel alone; "gradlim" the
-        gradient+limiter kernel(s) before it, "clip" the time-step clip after it."""
-        ms = np.zeros(16, np.float64)
-        nl = np.zeros(16, np.int32)
+        "residual" is the flux + time-step pass alone (the FP64 path's per-cell
+        gather, the mixed path's face pass), "residual_sum" the mixed path's
+        per-cell sum of the face results (empty on the FP64 path); "gradlim"
+        the gradient+limiter kernel(s) before them, "clip" the time-step clip
+        after them."""
+        ms = np.zeros(17, np.float64)
+        nl = np.zeros(17, np.int32)
         self._check(self.L.ofg_profile_step(self.h, ms, nl))
-        n = 16 if self.params.vismodel >= 3 else 9
+        n = 17 if self.params.vismodel >= 3 else 10
         names = self.PROFILE_GROUPS[:n]
         return dict(zip(names, ms[:n].tolist())), dict(zip(names, nl[:n].tolist()))
 

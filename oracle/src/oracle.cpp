@@ -36,6 +36,33 @@ const int NEQ = 5;
 
 }  // namespace
 
+// Greedy colouring of the cell graph (interior faces), cells visited in
+// natural order, each taking the smallest colour no earlier neighbour holds;
+// order[k] = the k-th cell of the colour-major order (colours ascending, ids
+// ascending inside a colour).  Returns the number of colours.
+static int colourMajor(int nCells, int nBFaces, const std::vector<std::vector<int>> &c2f,
+                       const std::vector<int> &lc, const std::vector<int> &rc, int *order) {
+    std::vector<int> col(nCells, -1);
+    int ncol = 0;
+    for (int i = 0; i < nCells; ++i) {
+        std::vector<char> used(ncol + 1, 0);
+        for (int f : c2f[i]) {
+            if (f < nBFaces) continue;
+            int nb = lc[f] == i ? rc[f] : lc[f];
+            if (col[nb] >= 0) used[col[nb]] = 1;
+        }
+        int cc = 0;
+        while (cc < (int)used.size() && used[cc]) ++cc;
+        col[i] = cc;
+        ncol = std::max(ncol, cc + 1);
+    }
+    std::vector<int> start(ncol + 1, 0);
+    for (int i = 0; i < nCells; ++i) start[col[i] + 1]++;
+    for (int k = 0; k < ncol; ++k) start[k + 1] += start[k];
+    for (int i = 0; i < nCells; ++i) order[start[col[i]]++] = i;
+    return ncol;
+}
+
 struct Oracle {
     ofg_params p;
     // ---------------- mesh ----------------
@@ -98,24 +125,7 @@ struct Oracle {
     void buildKey() {
         keyOrder.resize(nCells);
         if (p.sweep_order == 1) {
-            std::vector<int> col(nCells, -1);
-            int ncol = 0;
-            for (int i = 0; i < nCells; ++i) {
-                std::vector<char> used(ncol + 1, 0);
-                for (int f : c2f[i]) {
-                    if (f < nBFaces) continue;
-                    int nb = lc[f] == i ? rc[f] : lc[f];
-                    if (col[nb] >= 0) used[col[nb]] = 1;
-                }
-                int cc = 0;
-                while (cc < (int)used.size() && used[cc]) ++cc;
-                col[i] = cc;
-                ncol = std::max(ncol, cc + 1);
-            }
-            int k = 0;
-            for (int cc = 0; cc < ncol; ++cc)
-                for (int i = 0; i < nCells; ++i)
-                    if (col[i] == cc) keyOrder[k++] = i;
+            colourMajor(nCells, nBFaces, c2f, lc, rc, keyOrder.data());
         } else {
             for (int i = 0; i < nCells; ++i) keyOrder[i] = i;
         }
@@ -1590,6 +1600,19 @@ struct Oracle {
 
 // ============================ C interface ============================
 extern "C" {
+
+// The colour-major renumbering of a mesh (perm[new] = old), for running the
+// reference itself in the order the GPU path sweeps; returns the colour count.
+int oro_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm) {
+    if (nCells <= 0 || nBFaces < 0 || nFaces < nBFaces || !lCells || !rCells || !perm) return -1;
+    std::vector<int> lc(lCells, lCells + nFaces), rc(rCells, rCells + nFaces);
+    std::vector<std::vector<int>> c2f(nCells);
+    for (int f = nBFaces; f < nFaces; ++f) {
+        if (lc[f] < 0 || rc[f] < 0 || lc[f] >= nCells || rc[f] >= nCells) return -1;
+        c2f[lc[f]].push_back(f); c2f[rc[f]].push_back(f);
+    }
+    return colourMajor(nCells, nBFaces, c2f, lc, rc, perm);
+}
 
 void *oro_create(const ofg_params *p) {
     Oracle *o = new Oracle();

@@ -20,8 +20,15 @@ files reaches the same state as its uninterrupted run (<case>.npz) bitwise.
 walldist_<name>.npz holds the wall distance the reference computed itself
 (CALC_WALL_DIST, ireadwdst = 0) on the meshes of WALLDIST_CASES.
 
+bump2d_c1.npz is the 2-D Euler bump at its benchmark size (65,536 triangles,
+first-order Roe, LU-SGS, CFL 5, 2,000 outer iterations) as the reference ran
+it: every 16th interior cell of the final state, the per-equation sum and sum
+of squares of the whole interior state, the forces and the residual history
+(the whole state would be 2.6 MB).
+
     python tests/golden/make_golden.py --restart-only   # only the restart fixtures
     python tests/golden/make_golden.py --walldist-only  # only the wall-distance fixtures
+    python tests/golden/make_golden.py --c1-only        # only the benchmark-size bump (about 2 CPU minutes)
     python tests/golden/make_golden.py --case=<name>    # one case fixture"""
 import json
 import os
@@ -35,7 +42,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 from oneflow_b200 import meshio, params as P  # noqa: E402
-from golden_cases import CASES, RESTART_CASES, WALLDIST_CASES, build, build_walldist  # noqa: E402
+from golden_cases import C1_STEPS, C1_STRIDE, CASES, RESTART_CASES, WALLDIST_CASES, build, build_c1, \
+    build_walldist  # noqa: E402
 from oracle_lib import run_ref  # noqa: E402
 
 
@@ -71,7 +79,20 @@ def walldist_fixtures():
         print("walldist", name, mesh.n_cells, "cells", float(wd.min()), float(wd.max()))
 
 
+def c1_fixture():
+    mesh, prm = build_c1()
+    dump, rows = run_ref(mesh, prm, C1_STEPS)
+    q = dump["q"][:, :mesh.n_cells]
+    np.savez_compressed(os.path.join(HERE, "bump2d_c1.npz"), q_sub=q[:, ::C1_STRIDE], q_sum=q.sum(axis=1),
+                        q_sumsq=(q * q).sum(axis=1), forces=dump["forces"].ravel()[:13], reshist=rows[:, 2:7],
+                        steps=C1_STEPS, params=json.dumps(P.to_dict(prm)))
+    print("bump2d_c1", mesh.n_cells, "cells", C1_STEPS, "steps")
+
+
 def main():
+    if "--c1-only" in sys.argv:
+        c1_fixture()
+        return
     if "--walldist-only" in sys.argv:
         walldist_fixtures()
         return

@@ -27,6 +27,16 @@ CASES = {
     "plate2d_sa_roe_inflow_extrap": dict(steps=30),
     "plate2d_laminar_roe_isowall": dict(steps=30),
 }
+# the 2-D Euler bump at its benchmark size: 256x128 quads split into 65,536
+# jittered triangles, first-order Roe, LU-SGS, CFL 5, run for 2,000 outer
+# iterations (tests/golden/bump2d_c1.npz keeps every C1_STRIDE-th cell)
+C1_STEPS, C1_STRIDE = 2000, 16
+
+
+def build_c1():
+    return meshgen.bump_channel(256, 128), P.euler_bump()
+
+
 # meshes whose wall distance the reference computed itself (ireadwdst = 0):
 # tests/golden/walldist_<name>.npz
 WALLDIST_CASES = ("plate2d_sa_roe", "plate3d_sa_roe", "hexbox_sa")

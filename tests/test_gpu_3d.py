@@ -51,13 +51,23 @@ def test_3d_fp64_matches_oracle(name, order):
     assert rel(a, b) < 1e-3
 
 
-def test_3d_mixed_tracks_fp64():
+@pytest.mark.parametrize("name", list(CASES))
+def test_3d_mixed_tracks_fp64(name):
+    # the mixed path after 20 iterations: density and pressure within the
+    # 1e-5 field-L2 tolerance of the FP64 path.  nu~ within 1e-4: mid-transient
+    # it passes two switches that round-off can flip -- the reference's SA
+    # far-field rule (interior or free-stream nu~ on the sign of a sound-speed
+    # difference taken with a zero normal) and, with Barth, the limiter's
+    # branch -- (measured 2e-5 with SLAU2 + Barth, 1e-7 without them)
     m = mesh3d("colour")
-    d = CASES["lsq_venkat_kh3_roe"]
+    d = CASES[name]
     a = Solver(m, P.defaults(**d)); a.init_flowfield(); a.step(20)
     b = Solver(m, P.defaults(**d, precision=1)); b.init_flowfield(); b.step(20)
-    assert rel(b.state(), a.state()) < 1e-4
-    assert rel(b.state(TURB_SOLVER), a.state(TURB_SOLVER)) < 1e-2
+    qa, qb = a.state(), b.state()
+    for e in (0, 4):
+        assert np.linalg.norm(qb[e] - qa[e]) / np.linalg.norm(qa[e]) < 1e-5, e
+    ta, tb = a.state(TURB_SOLVER), b.state(TURB_SOLVER)
+    assert np.linalg.norm(tb - ta) / np.linalg.norm(ta) < 1e-4
 
 
 @pytest.mark.parametrize("name", ["gg_nolim_roe", "lsq_venkat_kh3_roe"])

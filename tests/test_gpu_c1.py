@@ -1,0 +1,72 @@
+"""The 2-D Euler bump at its benchmark size (65,536 jittered triangles,
+first-order Roe, LU-SGS, CFL 5, 2,000 outer iterations) on the GPU against
+the reference's own run of the same case (tests/golden/bump2d_c1.npz): the
+FP64 path to round-off, the mixed path on forces and fields."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oneflow_b200 import params as P
+from oneflow_b200.solver import Solver
+from golden_cases import C1_STEPS, C1_STRIDE, build_c1
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(HERE, "golden", "bump2d_c1.npz"))
+
+
+def _run(precision):
+    mesh, prm = build_c1()
+    prm.precision = precision
+    g = Solver(mesh, prm)
+    g.init_flowfield()
+    g.step(C1_STEPS)
+    return mesh, g
+
+
+def test_c1_parameters_are_the_fixture_parameters(gold):
+    _, prm = build_c1()
+    assert json.loads(str(gold["params"])) == P.to_dict(prm)
+
+
+def test_c1_fp64_path_matches_the_reference(gold):
+    mesh, g = _run(0)
+    N = mesh.n_cells
+    q = g.state()[:, :N]
+    sub = gold["q_sub"]
+    assert np.abs(q[:, ::C1_STRIDE] - sub).max() / np.abs(sub).max() < 1e-12
+    # every cell, through the per-equation sums of the state and of its squares
+    assert np.allclose(q.sum(axis=1), gold["q_sum"], rtol=1e-12, atol=1e-12 * np.abs(gold["q_sum"]).max())
+    assert np.allclose((q * q).sum(axis=1), gold["q_sumsq"], rtol=1e-12, atol=0)
+    # residual history as the reference printed it (6 significant digits)
+    h, hg = g.res_history(), gold["reshist"]
+    assert h.shape == hg.shape
+    assert np.all(np.abs(h - hg) <= 5.01e-6 * np.abs(hg) + 1e-12)
+    f, fr = g.forces(1.0), gold["forces"]
+    k = [0, 1, 9, 10]   # Fx, Fy, CL, CD
+    assert np.abs(f[k] - fr[k]).max() / np.abs(fr[k]).max() < 1e-10
+
+
+def test_c1_mixed_path_tracks_the_reference_transient(gold):
+    # the mixed path (FP32 face terms and LU-SGS increments, FP64
+    # accumulation, update and norms), sweeping in the reference's cell order,
+    # after the same 2,000 iterations -- mid-transient: the residual has
+    # fallen only fivefold, and the FP32 increments move the trajectory (the
+    # converged states agree to 1e-7, tests/test_gpu_forces.py): the density
+    # and pressure fields within 1e-5 relative L2 of the reference's FP64 run,
+    # the forces within 5e-6 (measured 1.6e-6)
+    mesh, g = _run(1)
+    N = mesh.n_cells
+    q = g.state()[:, :N][:, ::C1_STRIDE]
+    sub = gold["q_sub"]
+    for e in (0, 4):
+        assert np.linalg.norm(q[e] - sub[e]) / np.linalg.norm(sub[e]) < 1e-5, e
+    f, fr = g.forces(1.0), gold["forces"]
+    k = [0, 1, 9, 10]
+    assert np.abs(f[k] - fr[k]).max() / np.abs(fr[k]).max() < 5e-6, (f[k], fr[k])
