@@ -38,7 +38,8 @@ extern "C" {
 #define OFG_E_SIZE       -7   /* request larger than a fixed scratch allows  */
 #define OFG_E_IO         -8   /* file could not be opened, read or written   */
 
-/* solver ids (reference SolverState::tid, codes/solver/src/SolverState.cpp) */
+/* solver ids: the reference's SolverState::tid less one (its NS_SOLVER = 1,
+   TURB_SOLVER = 2, codes/global/include/SolverDef.h:31-32) */
 #define OFG_NS_SOLVER     0
 #define OFG_TURB_SOLVER   1
 
