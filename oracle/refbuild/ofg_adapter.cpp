@@ -156,7 +156,8 @@ void CreateContext()
     ReadParams( p );
     Check( ofg_create( & p, & g_ctx ), "ofg_create" );
     FaceTopo * ft = grid->faceTopo;
-    int nFaces = ft->faces.size(), nCells = grid->nCells, nBFaces = ft->nBFaces;
+    // the boundary-face count lives in the BC record (FaceTopo::GetNBFaces)
+    int nFaces = ft->faces.size(), nCells = grid->nCells, nBFaces = (int)ft->GetNBFaces();
     std::vector< int > fnc( nFaces ), fn, lc( nFaces ), rc( nFaces );
     for ( int f = 0; f < nFaces; ++ f )
     {
@@ -255,7 +256,7 @@ void OfgUpdateResiduals( StringField & data )
         Download( grid, tid, g[ d ], g[ d ] );
         MRField & cell = * GetFieldPointer< MRField >( grid, g[ d ] );
         MRField & bc = * GetFieldPointer< MRField >( grid, bg[ d ] );
-        for ( int f = 0; f < (int)ft->nBFaces; ++ f )
+        for ( int f = 0; f < (int)ft->GetNBFaces(); ++ f )
         {
             int lc = ft->lCells[ f ];
             for ( int e = 0; e < (int)cell.GetNEqu(); ++ e ) cell[ e ][ grid->nCells + f ] = cell[ e ][ lc ];
