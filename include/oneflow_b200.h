@@ -317,6 +317,17 @@ int ofg_cell_centres(int dimension, int nNodes, const double *xN, const double *
 int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells,
                      int *perm);
 
+/* Cell renumbering for locality: reverse Cuthill-McKee of the cell graph
+   (cells joined by interior faces; per connected component from a
+   pseudo-peripheral cell, neighbours visited in ascending degree).  Writes
+   perm[newId] = oldId for interior cells.  No counterpart in the reference,
+   which keeps the file's cell order (codes/geometry/src/UnsGrid.cpp:123-129);
+   pure host function, applied to the mesh arrays before ofg_upload_mesh (the
+   reference itself gives the same results on the renumbered mesh).  Returns
+   OFG_OK, or OFG_E_ARG for the arguments ofg_colour_order rejects; perm is
+   undefined after an error. */
+int ofg_rcm_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm);
+
 /* ---- allocation-free entry point (no counterpart in the reference: OneFLOW
    computes its residual norms on the host, ResidualTask::CalcRes) ---- */
 

@@ -54,6 +54,23 @@ class Mesh:
                     lc=c(self.lc, np.int32), rc=c(self.rc, np.int32), bct=c(self.bc_type, np.int32),
                     wd=None if self.wall_dist is None else c(self.wall_dist, np.float64))
 
+    def sort_faces(self) -> "Mesh":
+        """Return the mesh with its faces reordered by their cells: boundary
+        faces (still first) by their left cell, interior faces by (smaller,
+        larger) cell id -- after a cell renumbering, the face order that
+        walks the cells in order.  Each face keeps its nodes and cells."""
+        nb = self.n_bfaces
+        lo, hi = np.minimum(self.lc, np.where(self.rc >= 0, self.rc, self.lc)), np.maximum(self.lc, self.rc)
+        fb = np.argsort(self.lc[:nb], kind="stable")
+        fi = nb + np.lexsort((hi[nb:], lo[nb:]))
+        order = np.concatenate([fb, fi])
+        off = np.concatenate([[0], np.cumsum(self.face_node_count)])
+        fn = np.concatenate([self.face_nodes[off[f]:off[f + 1]] for f in order]) if len(order) else self.face_nodes
+        bcn = None if self.bc_name_id is None else self.bc_name_id[fb]
+        return Mesh(self.dim, self.x, self.y, self.z, self.face_node_count[order], fn.astype(np.int32),
+                    self.lc[order], self.rc[order], self.n_cells, nb, self.bc_type[fb], bcn, self.wall_dist,
+                    dict(self.meta))
+
     def renumber_cells(self, perm: np.ndarray) -> "Mesh":
         """Return the mesh with interior cell ``perm[new] = old`` renumbered.
 

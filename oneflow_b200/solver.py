@@ -69,6 +69,7 @@ def load_library() -> C.CDLL:
     L.ofg_sweep_levels.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.ofg_profile_step.argtypes = [C.c_void_p, _dp, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")]
     L.ofg_colour_order.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip]
+    L.ofg_rcm_order.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip]
     L.ofg_version.restype = C.c_int
     _LIB = L
     return L
@@ -289,3 +290,14 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def rcm_order(mesh: Mesh) -> np.ndarray:
+    """perm[new] = old: the reverse Cuthill-McKee cell order of ofg_rcm_order."""
+    L = load_library()
+    a = mesh.as_arrays()
+    perm = np.zeros(mesh.n_cells, np.int32)
+    rc = L.ofg_rcm_order(mesh.n_cells, mesh.n_faces, mesh.n_bfaces, a["lc"], a["rc"], perm)
+    if rc != 0:
+        raise OfgError(f"ofg_rcm_order failed ({rc})")
+    return perm

@@ -130,3 +130,16 @@ def test_residual_norms_match_the_residual_field_and_leave_the_history():
     got = g.residual_norms()
     assert np.allclose(got, want, rtol=1e-12, atol=0)
     assert np.array_equal(g.res_history(), h0)
+
+
+def test_rcm_renumbered_mesh_matches_the_oracle():
+    # a shuffled mesh renumbered by reverse Cuthill-McKee, faces sorted by
+    # their cells: the GPU and the oracle solve the same renumbered mesh
+    from oneflow_b200 import rcm_order
+    mesh = meshgen.bump_channel(32, 16)
+    m = mesh.renumber_cells(np.random.default_rng(3).permutation(mesh.n_cells))
+    m = m.renumber_cells(rcm_order(m)).sort_faces()
+    for prm in (P.euler_bump(ilim=2, vencat_coef=0.05), P.euler_bump(ilim=2, vencat_coef=0.05, sweep_order=1)):
+        o = Oracle(m, prm); o.init(); o.step(25)
+        g = Solver(m, prm); g.init_flowfield(); g.step(25)
+        assert rel(g.state(), o.q()) < 1e-10

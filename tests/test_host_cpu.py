@@ -147,3 +147,37 @@ def test_replica_aggregation_two_gloo_ranks():
     for r in (0, 1):
         assert out[r][0] == 150.0
         assert out[r][1] == pytest.approx(2 * 1000 * 10 / 0.150)
+
+
+def test_rcm_order_is_a_permutation_and_restores_locality():
+    # a randomly shuffled bump mesh: reverse Cuthill-McKee brings the largest
+    # cell-id gap across an interior face back below the generator's own
+    import numpy as np
+    from oneflow_b200 import meshgen, rcm_order
+    m = meshgen.bump_channel(64, 32)
+    shuffled = m.renumber_cells(np.random.default_rng(7).permutation(m.n_cells))
+
+    def bandwidth(mm):
+        nb = mm.n_bfaces
+        return int(np.abs(mm.lc[nb:] - mm.rc[nb:]).max())
+
+    p = rcm_order(shuffled)
+    assert sorted(p.tolist()) == list(range(m.n_cells))
+    assert np.array_equal(p, rcm_order(shuffled))          # deterministic
+    r = shuffled.renumber_cells(p).sort_faces()
+    assert bandwidth(shuffled) > 50 * bandwidth(r)
+    assert bandwidth(r) <= bandwidth(m)
+    # sort_faces keeps every face with its nodes and cells, boundary faces first
+    assert r.n_bfaces == m.n_bfaces and sorted(r.bc_type.tolist()) == sorted(m.bc_type.tolist())
+    assert np.all(r.rc[:r.n_bfaces] < 0) and np.all(r.rc[r.n_bfaces:] >= 0)
+
+
+def test_rcm_order_rejects_bad_arguments():
+    import ctypes as C
+    import numpy as np
+    from oneflow_b200.solver import load_library
+    L = load_library()
+    lc = np.array([0, 0, 1], np.int32); rc = np.array([-1, 1, 5], np.int32); perm = np.zeros(2, np.int32)
+    assert L.ofg_rcm_order(2, 3, -1, lc, rc, perm) == -1      # negative boundary-face count
+    assert L.ofg_rcm_order(2, 3, 1, lc, rc, perm) == -1       # interior face to a cell out of range
+    assert L.ofg_colour_order(2, 3, -1, lc, rc, perm) == -1
