@@ -400,6 +400,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start experiment")
     ap.add_argument("--no-pinned", action="store_true", help="skip the reference-options variant of the workload")
     ap.add_argument("--no-c1", action="store_true", help="skip the benchmark-size 2-D bump")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -477,6 +478,9 @@ def main():
         wall_err = float(np.abs(wd - mesh.wall_dist).max() / np.abs(mesh.wall_dist).max())
     for _ in range(args.warmup):
         s.step(1)
+    # launch shapes of the gather kernels picked by the autotuner on this mesh
+    tuning = s.autotune() if not args.no_tune else s.tuning()
+    s.step(1)
     torch.cuda.synchronize()
     abytes = alg_bytes(st, prm)
     working = sum(abytes.values())
@@ -582,7 +586,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prm.precision == 0 else "f32/f64",
                 "data": "synthetic (seeded mesh generator)",
                 "config": bench_config(desc, st, args.ordering, world, flush),
-                "sweep_levels": list(s.sweep_levels()),
+                "sweep_levels": list(s.sweep_levels()), "tuning": tuning,
                 "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "pinned_variant": pinned,
                 "config1_bump2d": c1,
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
@@ -625,8 +629,10 @@ def batched_throughput(n_cases: int = 64, steps: int = 10, warmup: int = 3):
         s.init_flowfield()
         ss.append(s)
     cells = sum(m.n_cells for m, _ in cases)
+    tunes = []
     for s in ss:
         s.step(warmup)
+        tunes.append(s.autotune())   # per mesh: launch shapes timed on its own cells
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for s in ss:
@@ -649,6 +655,11 @@ def batched_throughput(n_cases: int = 64, steps: int = 10, warmup: int = 3):
                         "SA, LU-SGS, FP32 faces",
             "cells": cells, "steps": steps, "unit": "cell-iter/s",
             "sequential": cells * steps / seq, "batched": cells * steps / bat,
+            "autotuner": {"tuned_ms_sum": sum(t["ms_tuned"] for t in tunes),
+                          "default_ms_sum": sum(t["ms_default"] for t in tunes),
+                          "choices": {k: {str(v): sum(1 for t in tunes if t[k] == v) for v in sorted({t[k] for t in tunes})}
+                                      for k in ("face_min_blocks", "face_block", "grad_min_blocks", "sweep_min_blocks",
+                                                "sweep_block")}},
             "timing": "host wall clock around synchronous calls, after warm-up"}
 
 

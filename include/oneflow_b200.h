@@ -328,6 +328,40 @@ int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, con
    undefined after an error. */
 int ofg_rcm_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm);
 
+/* ---- launch shapes and the autotuner (no counterpart in the reference) ----
+   The mixed path's heaviest gathers each exist in several compiled shapes:
+   min_blocks = resident 128-thread blocks per SM asked of the compiler, i.e.
+   a register cap of 65536 / (128 min_blocks) per thread (more blocks: more
+   warps in flight, fewer registers, possibly spills); block = threads per
+   block.  The defaults were chosen by timing the 6M-cell plate; the best
+   shape depends on the mesh (cell types, size, ordering). */
+typedef struct ofg_tuning {
+    int    face_min_blocks;   /* face pass: 2, 3 (default), 4 or 5                 */
+    int    face_block;        /* face pass threads per block: 64 or 128 (default)  */
+    int    grad_min_blocks;   /* gradients + limiter: 4, 6 (default) or 8          */
+    int    sweep_min_blocks;  /* LU-SGS level kernels: 6, 8 (default) or 10        */
+    int    sweep_block;       /* LU-SGS level kernels: 64 or 128 (default)         */
+    int    reserved[3];
+    double ms_default;        /* device ms per iteration of these kernels, default shapes */
+    double ms_tuned;          /* the same with the shapes chosen                   */
+} ofg_tuning;
+
+/* Times every candidate shape of the tunable kernels on this context's own
+   mesh and state (each kernel group `reps` times per candidate, CUDA events,
+   the median kept; one group after another, the others at their current
+   choice), keeps the fastest and reports them in *out.  The groups timed are
+   repeatable on a fixed state (gradients, face fluxes and residual, both
+   sweeps), so the solve itself is not advanced; the captured graphs are
+   rebuilt at the next ofg_step.  The result is cached per mesh (cell, face and
+   boundary-face counts and a hash of the face->cell lists) and parameter set:
+   a later context with the same mesh takes the cached shapes without timing.
+   Mixed precision only (the FP64 path keeps its fixed shapes, returned with
+   ms_* = 0).  Needs a state (after ofg_init_flowfield / upload / a step). */
+int ofg_autotune(ofg_ctx *ctx, int reps, ofg_tuning *out);
+int ofg_get_tuning(ofg_ctx *ctx, ofg_tuning *out);
+/* Sets the shapes (values outside the lists above return OFG_E_ARG). */
+int ofg_set_tuning(ofg_ctx *ctx, const ofg_tuning *t);
+
 /* ---- allocation-free entry point (no counterpart in the reference: OneFLOW
    computes its residual norms on the host, ResidualTask::CalcRes) ---- */
 

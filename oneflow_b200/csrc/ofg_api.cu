@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -498,6 +500,13 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     for (int f = 0; f < nFaces; ++f) {
         c->c2f[pos[c->lc[f]]++] = f;
         if (f >= nBFaces) c->c2f[pos[c->rc[f]]++] = f;
+    }
+    {   // FNV-1a of the face->cell lists: the autotuner's cache key for this mesh
+        unsigned long long h = 1469598103934665603ull;
+        auto mix = [&](unsigned v) { for (int b = 0; b < 4; ++b) { h ^= (v >> (8 * b)) & 0xffu; h *= 1099511628211ull; } };
+        mix(unsigned(nCells)); mix(unsigned(nFaces)); mix(unsigned(nBFaces));
+        for (int f = 0; f < nFaces; ++f) { mix(unsigned(c->lc[f])); mix(unsigned(c->rc[f])); }
+        c->meshHash = h;
     }
     build_sweep_key(c);
     build_levels(c, true, c->lowOrder, c->lowOff);
@@ -1502,6 +1511,134 @@ int ofg_rcm_order(int nCells, int nFaces, int nBFaces, const int *lCells, const 
     }
     for (int k = 0; k < nCells; ++k) perm[k] = order[nCells - 1 - k];
     return OFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launch shapes and the autotuner
+// ---------------------------------------------------------------------------
+static bool valid_tuning(const ofg_tuning &t) {
+    auto in = [](int v, std::initializer_list<int> l) { for (int x : l) if (x == v) return true; return false; };
+    return in(t.face_min_blocks, {2, 3, 4, 5}) && in(t.face_block, {64, 128}) && in(t.grad_min_blocks, {4, 6, 8}) &&
+           in(t.sweep_min_blocks, {6, 8, 10}) && in(t.sweep_block, {64, 128});
+}
+
+int ofg_get_tuning(ofg_ctx *c, ofg_tuning *out) {
+    if (!c || !out) return OFG_E_ARG;
+    *out = c->tune;
+    return OFG_OK;
+}
+
+int ofg_set_tuning(ofg_ctx *c, const ofg_tuning *t) {
+    if (!c || !t) return OFG_E_ARG;
+    if (!valid_tuning(*t)) return c->fail(OFG_E_ARG, "launch shape outside the compiled set");
+    int rc = sync(c);
+    if (rc) return rc;
+    ofg_tuning n = *t;
+    n.ms_default = c->tune.ms_default; n.ms_tuned = c->tune.ms_tuned;
+    c->tune = n;
+    destroy_graphs(c);   // recaptured with the new kernels at the next ofg_step
+    return OFG_OK;
+}
+
+namespace {
+std::mutex g_tuneMutex;
+std::map<std::string, ofg_tuning> g_tuneCache;   // mesh + options -> chosen shapes
+
+std::string tune_key(const ofg_ctx *c) {
+    char k[256];
+    std::snprintf(k, sizeof k, "%llx:%d:%d:%d:%d:%d:%d:%d:%d:%d", c->meshHash, c->nCells, c->nFaces, c->p.precision,
+                  c->p.vismodel, c->p.ilim, c->p.igrad, c->p.ischeme, c->p.ivischeme, c->p.sweep_order);
+    return k;
+}
+}  // namespace
+
+int ofg_autotune(ofg_ctx *c, int reps, ofg_tuning *out) {
+    int rc = check_tid(c, OFG_NS_SOLVER);
+    if (rc) return rc;
+    if (c->pendingNext || c->pendingTurb) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
+    if (c->p.precision != OFG_PREC_MIXED || multi_stage(c)) {   // fixed shapes
+        c->tune.ms_default = c->tune.ms_tuned = 0.0;
+        if (out) *out = c->tune;
+        return OFG_OK;
+    }
+    if (reps < 1) reps = 5;
+    const std::string key = tune_key(c);
+    {
+        std::lock_guard<std::mutex> g(g_tuneMutex);
+        auto it = g_tuneCache.find(key);
+        if (it != g_tuneCache.end()) {
+            if ((rc = ofg_set_tuning(c, &it->second))) return rc;
+            c->tune.ms_default = it->second.ms_default; c->tune.ms_tuned = it->second.ms_tuned;
+            if (out) *out = c->tune;
+            return OFG_OK;
+        }
+    }
+    if ((rc = sync(c))) return rc;
+    destroy_graphs(c);
+    // fill every input of the timed groups once: CFL, gradients, fluxes, residual, diagonal
+    if ((rc = launch(c, T_CFL))) return rc;
+    if ((rc = launch(c, T_TS_RES))) return rc;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    // median device time of one group (a list of tasks) over reps runs
+    auto time_group = [&](std::initializer_list<int> tasks, double &ms) -> int {
+        std::vector<float> t(reps);
+        for (int r = 0; r < reps; ++r) {
+            CK(cudaEventRecord(e0, c->stream));
+            for (int task : tasks) { int q = launch(c, task); if (q) return q; }
+            CK(cudaEventRecord(e1, c->stream));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&t[r], e0, e1));
+        }
+        std::sort(t.begin(), t.end());
+        ms = t[reps / 2];
+        return OFG_OK;
+    };
+    const ofg_tuning start = c->tune;
+    double msDefault = 0.0, msTuned = 0.0;
+    // groups in turn, each over its own candidates, the others at their current choice
+    struct Cand { int *a; int *b; std::vector<std::pair<int, int>> values; std::vector<int> tasks; };
+    ofg_tuning &T = c->tune;
+    std::vector<Cand> groups = {
+        {&T.face_min_blocks, &T.face_block, {{2, 128}, {3, 128}, {4, 128}, {5, 128}, {2, 64}, {3, 64}, {4, 64}, {5, 64}},
+         {T_P_FLUX}},
+        {&T.grad_min_blocks, nullptr, {{4, 0}, {6, 0}, {8, 0}}, {T_P_GRADLIM}},
+        {&T.sweep_min_blocks, &T.sweep_block, {{6, 128}, {8, 128}, {10, 128}, {6, 64}, {8, 64}, {10, 64}},
+         {T_LOWER, T_UPPER}},
+    };
+    for (Cand &g : groups) {
+        const int a0 = *g.a, b0 = g.b ? *g.b : 0;
+        double best = 1e30, first = 0.0;
+        int ba = a0, bb = b0;
+        for (size_t k = 0; k < g.values.size(); ++k) {
+            *g.a = g.values[k].first;
+            if (g.b) *g.b = g.values[k].second;
+            double ms = 0.0;
+            std::vector<int> tl(g.tasks);
+            int q;
+            if (tl.size() == 1) q = time_group({tl[0]}, ms);
+            else q = time_group({tl[0], tl[1]}, ms);
+            if (q) { cudaEventDestroy(e0); cudaEventDestroy(e1); c->tune = start; return q; }
+            if (*g.a == a0 && (!g.b || *g.b == b0)) first = ms;   // the shape the context came with
+            if (ms < best) { best = ms; ba = *g.a; bb = g.b ? *g.b : 0; }
+        }
+        *g.a = ba;
+        if (g.b) *g.b = bb;
+        msDefault += first;
+        msTuned += best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    T.ms_default = msDefault;
+    T.ms_tuned = msTuned;
+    destroy_graphs(c);
+    {
+        std::lock_guard<std::mutex> g(g_tuneMutex);
+        g_tuneCache[key] = T;
+    }
+    if (out) *out = T;
+    return sync(c);
 }
 
 int ofg_colour_order(int nCells, int nFaces, int nBFaces, const int *lCells, const int *rCells, int *perm) {

@@ -13,6 +13,8 @@ struct ofg_ctx {
     ofg_params p{};
     ofg::DevParams dp{};
     std::string err;
+    ofg_tuning tune{3, 128, 6, 8, 128, {0, 0, 0}, 0.0, 0.0};   // launch shapes of the mixed path's gathers
+    unsigned long long meshHash = 0;                         // of the face->cell lists (autotuner cache key)
 
     // ---- mesh (host copies, reference numbering) ----
     int nCells = 0, nBFaces = 0, nFaces = 0, nT = 0;

@@ -297,8 +297,11 @@ __device__ __forceinline__ void cell_limiter(const KArgs<R> &A, int c, const R *
     }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(128, MinBlocks<R>::gl) k_gradlim(KArgs<R> A, int nvar, int limMode) {
+// MINB: resident 128-thread blocks per SM asked of the compiler (its register
+// cap is 65536 / (128 MINB)); the default is the measured choice for the 6M
+// plate, other values are instantiated for the autotuner (ofg_autotune).
+template <typename R, int MINB = MinBlocks<R>::gl>
+__global__ void __launch_bounds__(128, MINB) k_gradlim(KArgs<R> A, int nvar, int limMode) {
     __shared__ double sred[2 * NEQ][128];
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     bool active = c < A.nCells;
@@ -1003,8 +1006,8 @@ __device__ __forceinline__ void store_face_out(double *o, const double *v, float
     reinterpret_cast<double2 *>(o)[2] = make_double2(v[4], packed);
 }
 
-template <int MODE, bool VV = false>
-__global__ void __launch_bounds__(128, MinBlocks<float>::fp) k_face_pass(KArgs<float> A) {
+template <int MODE, bool VV = false, int MINB = MinBlocks<float>::fp>
+__global__ void __launch_bounds__(128, MINB) k_face_pass(KArgs<float> A) {
     constexpr bool doRes = MODE != 1, doDt = MODE != 2;
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= A.nFaces) return;
@@ -1225,8 +1228,8 @@ __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *
     }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(128, MinBlocks<R>::sw) k_lusgs_lower(KArgs<R> A, const int *order, int start, int count) {
+template <typename R, int MINB = MinBlocks<R>::sw>
+__global__ void __launch_bounds__(128, MINB) k_lusgs_lower(KArgs<R> A, const int *order, int start, int count) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     int c = order[start + t];
@@ -1242,8 +1245,8 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::sw) k_lusgs_lower(KArgs<R> 
     st4(A.dq + (size_t)c * DQR + 4, o + 4);
 }
 
-template <typename R>
-__global__ void __launch_bounds__(128, MinBlocks<R>::sw) k_lusgs_upper(KArgs<R> A, const int *order, int start, int count) {
+template <typename R, int MINB = MinBlocks<R>::sw>
+__global__ void __launch_bounds__(128, MINB) k_lusgs_upper(KArgs<R> A, const int *order, int start, int count) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     int c = order[start + t];

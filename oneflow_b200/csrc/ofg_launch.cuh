@@ -82,7 +82,15 @@ void launch_gradlim(ofg_ctx *c, const KArgs<R> &A, cudaStream_t s) {
     bool venkatGlobal = c->p.ilim == 2 && !c->p.venkat_kh3;
     int limMode = (c->p.ilim == 1 || c->p.ilim == 2) ? (venkatGlobal ? 2 : 1) : 0;
     int nb = nblk(N, 128);
-    OFG_LAUNCH(k_gradlim<R>, nb, 128, s, A, nvar, limMode);
+    if constexpr (sizeof(R) == 4) {
+        switch (c->tune.grad_min_blocks) {
+        case 4: OFG_LAUNCH((k_gradlim<R, 4>), nb, 128, s, A, nvar, limMode); break;
+        case 8: OFG_LAUNCH((k_gradlim<R, 8>), nb, 128, s, A, nvar, limMode); break;
+        default: OFG_LAUNCH((k_gradlim<R, 6>), nb, 128, s, A, nvar, limMode); break;
+        }
+    } else {
+        OFG_LAUNCH(k_gradlim<R>, nb, 128, s, A, nvar, limMode);
+    }
     if (limMode == 2) {
         OFG_LAUNCH(k_limiter_eps<R>, 1, 256, s, A, nb);
         OFG_LAUNCH(k_limiter_global<R>, nb, 128, s, A);
@@ -102,8 +110,19 @@ void launch_flux(ofg_ctx *c, const KArgs<R> &A, cudaStream_t s, int part = 3) {
         else OFG_LAUNCH((k_residual<R, MODE>), nblk(N, 128), 128, s, A);
     } else {
         if (part & 1) {
-            if (vv) OFG_LAUNCH((k_face_pass<MODE, true>), nblk(c->nFaces, 128), 128, s, A);
-            else OFG_LAUNCH((k_face_pass<MODE>), nblk(c->nFaces, 128), 128, s, A);
+            const int F = c->nFaces, bs = c->tune.face_block;
+            if (vv) {
+                OFG_LAUNCH((k_face_pass<MODE, true>), nblk(F, 128), 128, s, A);
+            } else if constexpr (MODE == 0) {   // the iteration's pass: the tuned shape
+                switch (c->tune.face_min_blocks) {
+                case 2: OFG_LAUNCH((k_face_pass<0, false, 2>), nblk(F, bs), bs, s, A); break;
+                case 4: OFG_LAUNCH((k_face_pass<0, false, 4>), nblk(F, bs), bs, s, A); break;
+                case 5: OFG_LAUNCH((k_face_pass<0, false, 5>), nblk(F, bs), bs, s, A); break;
+                default: OFG_LAUNCH((k_face_pass<0, false, 3>), nblk(F, bs), bs, s, A); break;
+                }
+            } else {
+                OFG_LAUNCH((k_face_pass<MODE>), nblk(F, 128), 128, s, A);
+            }
         }
         if (part & 2) OFG_LAUNCH((k_face_sum<MODE>), nblk(N, 128), 128, s, A);
     }
@@ -156,7 +175,17 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         int nl = int(c->lowOff.size()) - 1;
         for (int l = 0; l < nl; ++l) {
             int st = c->lowOff[l], cnt = c->lowOff[l + 1] - st;
-            OFG_LAUNCH(k_lusgs_lower<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_lowOrder, st, cnt);
+            const int *ord = (const int *)c->d_lowOrder;
+            if constexpr (sizeof(R) == 4) {
+                const int bs = c->tune.sweep_block;
+                switch (c->tune.sweep_min_blocks) {
+                case 6: OFG_LAUNCH((k_lusgs_lower<R, 6>), nblk(cnt, bs), bs, s, A, ord, st, cnt); break;
+                case 10: OFG_LAUNCH((k_lusgs_lower<R, 10>), nblk(cnt, bs), bs, s, A, ord, st, cnt); break;
+                default: OFG_LAUNCH((k_lusgs_lower<R, 8>), nblk(cnt, bs), bs, s, A, ord, st, cnt); break;
+                }
+            } else {
+                OFG_LAUNCH(k_lusgs_lower<R>, nblk(cnt, 128), 128, s, A, ord, st, cnt);
+            }
         }
         break;
     }
@@ -165,7 +194,17 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         int nl = int(c->upOff.size()) - 1;
         for (int l = 0; l < nl; ++l) {
             int st = c->upOff[l], cnt = c->upOff[l + 1] - st;
-            OFG_LAUNCH(k_lusgs_upper<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_upOrder, st, cnt);
+            const int *ord = (const int *)c->d_upOrder;
+            if constexpr (sizeof(R) == 4) {
+                const int bs = c->tune.sweep_block;
+                switch (c->tune.sweep_min_blocks) {
+                case 6: OFG_LAUNCH((k_lusgs_upper<R, 6>), nblk(cnt, bs), bs, s, A, ord, st, cnt); break;
+                case 10: OFG_LAUNCH((k_lusgs_upper<R, 10>), nblk(cnt, bs), bs, s, A, ord, st, cnt); break;
+                default: OFG_LAUNCH((k_lusgs_upper<R, 8>), nblk(cnt, bs), bs, s, A, ord, st, cnt); break;
+                }
+            } else {
+                OFG_LAUNCH(k_lusgs_upper<R>, nblk(cnt, 128), 128, s, A, ord, st, cnt);
+            }
         }
         break;
     }

@@ -23,6 +23,16 @@ class OfgError(RuntimeError):
     pass
 
 
+class OfgTuning(C.Structure):
+    """ctypes mirror of ofg_tuning (include/oneflow_b200.h)."""
+    _fields_ = [("face_min_blocks", C.c_int), ("face_block", C.c_int), ("grad_min_blocks", C.c_int),
+                ("sweep_min_blocks", C.c_int), ("sweep_block", C.c_int), ("reserved", C.c_int * 3),
+                ("ms_default", C.c_double), ("ms_tuned", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
 _LIB = None
 
 
@@ -70,6 +80,9 @@ def load_library() -> C.CDLL:
     L.ofg_profile_step.argtypes = [C.c_void_p, _dp, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")]
     L.ofg_colour_order.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip]
     L.ofg_rcm_order.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip]
+    L.ofg_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(OfgTuning)]
+    L.ofg_get_tuning.argtypes = [C.c_void_p, C.POINTER(OfgTuning)]
+    L.ofg_set_tuning.argtypes = [C.c_void_p, C.POINTER(OfgTuning)]
     L.ofg_version.restype = C.c_int
     _LIB = L
     return L
@@ -200,6 +213,25 @@ class Solver:
         n = 17 if self.params.vismodel >= 3 else 10
         names = self.PROFILE_GROUPS[:n]
         return dict(zip(names, ms[:n].tolist())), dict(zip(names, nl[:n].tolist()))
+
+    def autotune(self, reps: int = 5) -> dict:
+        """ofg_autotune: time the candidate launch shapes on this mesh and keep
+        the fastest (cached per mesh); returns the choice and its timings."""
+        t = OfgTuning()
+        self._check(self.L.ofg_autotune(self.h, reps, C.byref(t)))
+        return t.as_dict()
+
+    def tuning(self) -> dict:
+        t = OfgTuning()
+        self._check(self.L.ofg_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = OfgTuning()
+        self._check(self.L.ofg_get_tuning(self.h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        self._check(self.L.ofg_set_tuning(self.h, C.byref(t)))
 
     FORCE_NAMES = ("Fx", "Fy", "Fz", "Fpx", "Fpy", "Fpz", "Fvx", "Fvy", "Fvz", "CL", "CD", "CD_pres", "CD_vis")
 

@@ -1,0 +1,64 @@
+"""The autotuner (ofg_autotune): candidate launch shapes of the mixed path's
+face pass, gradient/limiter kernel and LU-SGS level kernels timed on the
+context's own mesh; the choice is a valid compiled shape, no slower than the
+context's starting shape, cached per mesh, and does not change the results
+beyond FP32 rounding."""
+import numpy as np
+import pytest
+
+from oneflow_b200 import meshgen, params as P
+from oneflow_b200.solver import OfgError, Solver, TURB_SOLVER
+from oneflow_b200.walldist import plate_wall_distance
+
+pytestmark = pytest.mark.gpu
+
+VALID = {"face_min_blocks": {2, 3, 4, 5}, "face_block": {64, 128}, "grad_min_blocks": {4, 6, 8},
+         "sweep_min_blocks": {6, 8, 10}, "sweep_block": {64, 128}}
+
+
+def plate():
+    m = meshgen.flat_plate_tets(24, 12, 8)
+    m.wall_dist = plate_wall_distance(m)
+    return m
+
+
+def test_autotune_picks_a_valid_shape_and_caches_it():
+    m = plate()
+    prm = P.rans_plate(sweep_order=1)
+    a = Solver(m, prm); a.init_flowfield(); a.step(3)
+    t = a.autotune(reps=3)
+    for k, allowed in VALID.items():
+        assert t[k] in allowed, (k, t[k])
+    assert 0.0 < t["ms_tuned"] <= t["ms_default"]
+    b = Solver(m, prm); b.init_flowfield()
+    tb = b.autotune()            # same mesh and options: the cached choice, no timing
+    assert {k: tb[k] for k in VALID} == {k: t[k] for k in VALID}
+
+
+def test_tuned_shapes_give_the_same_solution():
+    m = plate()
+    prm = P.rans_plate(sweep_order=1)
+    a = Solver(m, prm); a.init_flowfield(); a.step(2)
+    b = Solver(m, prm); b.init_flowfield(); b.step(2)
+    # every non-default shape at once
+    b.set_tuning(face_min_blocks=5, face_block=64, grad_min_blocks=8, sweep_min_blocks=10, sweep_block=64)
+    a.step(10); b.step(10)
+    qa, qb = a.state(), b.state()
+    assert np.abs(qb - qa).max() / np.abs(qa).max() < 1e-6
+    ta, tb = a.state(TURB_SOLVER), b.state(TURB_SOLVER)
+    assert np.linalg.norm(tb - ta) / np.linalg.norm(ta) < 1e-5
+
+
+def test_set_tuning_rejects_shapes_that_are_not_compiled():
+    s = Solver(meshgen.bump_channel(16, 8), P.euler_bump(precision=1))
+    with pytest.raises(OfgError):
+        s.set_tuning(face_min_blocks=7)
+    with pytest.raises(OfgError):
+        s.set_tuning(sweep_block=256)
+
+
+def test_fp64_path_keeps_its_fixed_shapes():
+    s = Solver(meshgen.bump_channel(16, 8), P.euler_bump())
+    s.init_flowfield()
+    t = s.autotune()
+    assert t["ms_default"] == 0.0 and t["ms_tuned"] == 0.0
