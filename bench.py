@@ -49,6 +49,16 @@ def make_workload(name: str):
                              "SA, LU-SGS; FP32 face terms, FP64 accumulation/update/norms",
                     lattice=list(dims))
         return mesh, prm, desc
+    if name in ("wing3d", "wing3d_sample"):
+        kw = {} if name == "wing3d" else dict(n_around=128, n_tet=20, nz_wing=30, nz_tip=10)
+        mesh = meshgen.swept_wing_hybrid(**kw)
+        prm = P.transonic_wing()
+        m = mesh.meta
+        desc = dict(workload=f"3-D transonic swept wing: NACA0012 section, aspect ratio 4, sweep 30 deg, half model; "
+                             f"{m['n_hex']} hexahedral layers (ratio 1.2, y+~1) + tetrahedral far field "
+                             f"({mesh.n_cells:,} cells); Mach 0.84, AoA 3.06, Re 1.2e7, SLAU2, Green-Gauss + Barth, "
+                             "SA, LU-SGS; FP32 face terms, FP64 accumulation/update/norms")
+        return mesh, prm, desc
     if name == "bump2d":
         mesh = meshgen.bump_channel(256, 128)
         prm = P.euler_bump()
@@ -401,6 +411,7 @@ def main():
     ap.add_argument("--no-pinned", action="store_true", help="skip the reference-options variant of the workload")
     ap.add_argument("--no-c1", action="store_true", help="skip the benchmark-size 2-D bump")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
+    ap.add_argument("--no-wing", action="store_true", help="skip the 8M-cell transonic swept wing")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -568,6 +579,9 @@ def main():
     c1 = None
     if rank == 0 and world == 1 and not args.no_c1:
         c1 = config1_throughput(stream)
+    wing = None
+    if rank == 0 and world == 1 and not args.no_wing:
+        wing = config3_wing(stream, args.ordering)
     conv = None
     if rank == 0 and world == 1 and not args.no_converge:
         conv = time_to_drop("bump2d_small", 1e-8, stream)
@@ -588,7 +602,7 @@ def main():
                 "config": bench_config(desc, st, args.ordering, world, flush),
                 "sweep_levels": list(s.sweep_levels()), "tuning": tuning,
                 "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "pinned_variant": pinned,
-                "config1_bump2d": c1,
+                "config1_bump2d": c1, "config3_wing": wing,
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": int(l1 - l0), "clocks": clocks, "time_to_1e-8": conv,
                 "setup": {"calc_wall_dist_s": wall_s, "wall_dist_vs_closed_form": wall_err},
@@ -825,6 +839,71 @@ def pinned_variant(mesh, prm, stream, steps: int, warmup: int):
     s.close()
     return {"options": note, "value": mesh.n_cells * steps / (ms * 1e-3), "unit": "cell-iter/s",
             "ms_per_step": ms / steps, "steps": steps, "warmup": warmup}
+
+
+def config3_wing(stream, ordering: str, steps: int = 20, warmup: int = 5, parity_steps: int = 3):
+    """The transonic swept-wing configuration: the 8.0M-cell hybrid mesh
+    (hexahedral boundary layer, tetrahedral far field) on the mixed path --
+    cell-iter/s, the per-kernel profile and the dominant kernel's roofline --
+    and parity on its 0.8M-cell sample (the same generator, coarser) against
+    the reference solver run for parity_steps iterations on the same mesh, with
+    the wall distance computed on the GPU and passed to it."""
+    import torch
+    from oneflow_b200 import Solver
+    from oneflow_b200.solver import TURB_SOLVER
+    mesh, prm, desc = make_workload("wing3d")
+    prm.sweep_order = 1 if ordering == "colour" else 0
+    st = mesh_stats(mesh)
+    s = Solver(mesh, prm)
+    s.set_stream(stream.cuda_stream)
+    s.init_flowfield()
+    s.step(warmup)
+    tuning = s.autotune()
+    ms = _timed_steps(s, stream, steps)
+    prof = s.profile_step()
+    grp_ms, grp_n = prof
+    ab = alg_bytes(st, prm)
+    top = max((k for k in grp_ms if k != "cfl"), key=lambda k: grp_ms[k])
+    hbm = _peak_hbm()
+    achieved = ab[top] / (grp_ms[top] * 1e-3) / 1e9
+    out = {"workload": desc["workload"], "cells": st["N"], "faces": st["F"], "steps": steps, "warmup": warmup,
+           "value": st["N"] * steps / (ms * 1e-3), "unit": "cell-iter/s", "ms_per_step": ms / steps,
+           "sweep_levels": list(s.sweep_levels()), "tuning": tuning,
+           "roofline": {"bound": "hbm", "kernel": KERNEL_OF_GROUP.get(top, top), "achieved": achieved,
+                        "peak": hbm["value"], "unit": "GB/s", "frac": achieved / hbm["value"],
+                        "whole_step_frac": sum(ab.values()) / (ms / steps * 1e-3) / 1e9 / hbm["value"],
+                        "group_ms": grp_ms}}
+    s.close()
+    # parity on the sample: FP64 and mixed paths against the reference
+    smesh, sprm, sdesc = make_workload("wing3d_sample")
+    g = Solver(smesh, P.defaults(**{**P.to_dict(sprm), "precision": 0, "sweep_order": 0}))
+    g.init_flowfield()
+    smesh.wall_dist = g.field("walldist")[:smesh.n_cells].copy()    # CALC_WALL_DIST on the GPU
+    g.close()
+    N = smesh.n_cells
+    par = {"sample_cells": N, "steps": parity_steps, "tolerance": {"forces_rel": 1e-6, "field_rel_l2": 1e-5}}
+    if os.path.exists(REF_EXE):
+        rprm = P.defaults(**{**P.to_dict(sprm), "precision": 0, "sweep_order": 0})
+        thr, per_iter, wall, dump = reference_timed(smesh, rprm, 1, parity_steps - 1, 1, dump=True)
+        ref = {"rho": dump["q"][0, :N], "p": dump["q"][4, :N], "nut": dump["turbq"][0, :N],
+               "forces": dump["forces"].ravel()[:13]}
+        par["reference_cell_iter_s_1core"] = thr
+        for key, prec in (("fp64", 0), ("mixed", 1)):
+            q = P.defaults(**{**P.to_dict(sprm), "precision": prec, "sweep_order": 0})
+            gs = Solver(smesh, q)
+            gs.set_stream(stream.cuda_stream)
+            gs.init_flowfield()
+            gs.step(parity_steps)
+            stt = gs.state()
+            f = gs.forces(1.0)
+            par[f"{key}_vs_reference"] = {"rho_l2": _rel_l2(stt[0, :N], ref["rho"]), "p_l2": _rel_l2(stt[4, :N], ref["p"]),
+                                          "nut_l2": _rel_l2(gs.state(TURB_SOLVER)[:N], ref["nut"]),
+                                          "forces_rel": _force_err(f, ref["forces"]),
+                                          "CL": float(f[9]), "CD": float(f[10])}
+            gs.close()
+        par["reference_forces"] = {"CL": float(ref["forces"][9]), "CD": float(ref["forces"][10])}
+    out["parity"] = par
+    return out
 
 
 def config1_throughput(stream, steps: int = 200, warmup: int = 5):

@@ -563,3 +563,208 @@ def bump_box_mixed(nx: int = 12, ny: int = 8, nz: int = 10, height: float = 0.15
     flat = fn[np.arange(4)[None, :] < fc[:, None]]          # row by row: each face's nodes in order
     return Mesh(3, x, y, z, fc.astype(np.int32), flat.astype(np.int32), lc.astype(np.int32), rc.astype(np.int32),
                 nc, nb, bct, meta=dict(kind="bump_box_mixed", nx=nx, ny=ny, nz=nz, prism_from=prism_from, seed=seed))
+
+
+# ------------------------------------------------------------------------
+# 3-D swept wing: hexahedral boundary layer + tetrahedral far field
+# ------------------------------------------------------------------------
+def _dedupe_faces(F: np.ndarray, owner: np.ndarray):
+    """Shared faces of one face kind (all rows k nodes, listed outward from
+    their owner): returns (nodes, lc, rc) with rc = -1 on boundary faces and
+    each face in the orientation of its lower-numbered cell (lc < rc).  Rows
+    are matched on their sorted node tuples (no combined integer key, so any
+    node count works)."""
+    s = np.sort(F, axis=1)
+    order = np.lexsort(tuple(s[:, c] for c in range(s.shape[1] - 1, -1, -1)) + ())
+    ss = s[order]
+    new = np.ones(len(order), bool)
+    new[1:] = np.any(ss[1:] != ss[:-1], axis=1)
+    del s, ss
+    grp = np.cumsum(new) - 1
+    nf = int(grp[-1]) + 1
+    cnt = np.bincount(grp, minlength=nf)
+    if cnt.max() > 2:
+        raise ValueError("a face is shared by more than two cells")
+    first = order[new]
+    pos2 = np.minimum(np.flatnonzero(new) + 1, len(order) - 1)
+    second = order[pos2]
+    has2 = cnt == 2
+    lc = owner[first].copy()
+    rc = np.where(has2, owner[second], -1)
+    nodes = F[first].copy()
+    swap = has2 & (rc < lc)
+    lc[swap], rc[swap] = rc[swap], owner[first][swap]
+    nodes[swap] = F[second[swap]]
+    return nodes, lc, rc
+
+
+def swept_wing_hybrid(n_around: int = 256, n_hex: int = 30, hex_ratio: float = 1.2, n_tet: int = 44,
+                      nz_wing: int = 76, nz_tip: int = 30, t: float = 0.12, aspect_ratio: float = 4.0,
+                      sweep_deg: float = 30.0, radius: float = 20.0, reynolds: float = 1.2e7,
+                      yplus: float = 1.0) -> Mesh:
+    """Hybrid mesh around a swept NACA 00xx wing (half model, chord 1, root on
+    the symmetry plane z = 0, semi-span aspect_ratio / 2, leading edge swept
+    back by sweep_deg; the whole grid is sheared with it).  Cross-section: an
+    O-grid of n_around points around the section; its first n_hex layers grow
+    from a first cell at the requested y+ (flat-plate skin-friction estimate
+    at the wing's Reynolds number) by hex_ratio and are hexahedra, the next
+    n_tet layers grow geometrically to a cylinder of the given radius and each
+    hexahedral cell there is split into six tetrahedra (the Kuhn split along
+    the cell's (i, k, z) diagonal, so neighbouring splits conform; the last
+    hexahedral layer carries the two triangles of its outer neighbour's split
+    in place of that quadrilateral face).  Spanwise: nz_wing slabs over the
+    wing (clustered at the tip) and nz_tip slabs beyond it to the far-field
+    plane, where the section's interior is filled by a ladder of cells between
+    matching lower- and upper-surface points (quadrilaterals, triangles at the
+    leading and trailing edges), closed at the tip by a wall.
+    BCs: wing and tip SOLID_SURFACE, root plane SYMMETRY, cylinder and the
+    outer plane FARFIELD.  About 8.0 M cells at the defaults."""
+    nh = n_around // 2
+    S = naca4_surface(0.0, 0.4, t, nh)                   # [n] TE -> lower -> LE -> upper
+    n = S.shape[0]
+    K = n_hex + n_tet
+    cf = 0.0592 * reynolds ** -0.2
+    y1 = yplus / (np.sqrt(0.5 * cf) * reynolds)
+    dh = y1 * hex_ratio ** np.arange(n_hex)              # hexahedral layer thicknesses
+    reach = dh.sum()
+    # tet layers: geometric growth from the last hex layer's thickness to the cylinder
+    lo, hi = 1.0 + 1e-9, 3.0
+    d_last = dh[-1]
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if d_last * r * (r ** n_tet - 1.0) / (r - 1.0) > radius - reach:
+            hi = r
+        else:
+            lo = r
+    dt = d_last * r ** np.arange(1, n_tet + 1)
+    dt *= (radius - reach) / dt.sum()
+    dist = np.concatenate([[0.0], np.cumsum(np.concatenate([dh, dt]))])    # [K+1]
+    seg = np.linalg.norm(np.roll(S, -1, 0) - S, axis=1)
+    sarc = np.concatenate([[0.0], np.cumsum(seg)[:-1]]) / seg.sum()
+    ang = -2.0 * np.pi * sarc
+    Cc = np.stack([0.5 + radius * np.cos(ang), radius * np.sin(ang)], 1)
+    tng = np.roll(S, -1, 0) - np.roll(S, 1, 0)
+    nrm = np.stack([-tng[:, 1], tng[:, 0]], 1)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    d = dist[:, None, None]
+    E = S + reach * nrm
+    near = S[None] + np.minimum(d, reach) * nrm[None]
+    far = E[None] + np.clip((d - reach) / (radius - reach), 0.0, 1.0) * (Cc - E)[None]
+    P2 = np.where(d <= reach, near, far)                 # [K+1, n, 2]
+    semi = 0.5 * aspect_ratio
+    zt = semi * (1.0 - np.cos(np.linspace(0.0, 0.5 * np.pi, nz_wing + 1)))     # clustered at the tip
+    ze = semi + (radius - semi) * np.linspace(0.0, 1.0, nz_tip + 1)[1:] ** 1.5
+    zs = np.concatenate([zt, ze])
+    nz = len(zs) - 1
+    tan = np.tan(np.radians(sweep_deg))
+    # nodes (s, k, i): index (s * (K + 1) + k) * n + i
+    X = P2[None, :, :, 0] + tan * zs[:, None, None]
+    Y = np.broadcast_to(P2[None, :, :, 1], X.shape)
+    Z = np.broadcast_to(zs[:, None, None], X.shape)
+    x, y, z = X.ravel().copy(), Y.ravel().copy(), Z.ravel().copy()
+    nid = lambda s, k, i: (s * (K + 1) + k) * n + (i % n)
+    # ring cells (s, k, i) in natural order (i fastest, then k, then s)
+    ss, kk, ii = np.meshgrid(np.arange(nz), np.arange(K), np.arange(n), indexing="ij")
+    ss, kk, ii = ss.ravel(), kk.ravel(), ii.ravel()
+    # corners in _CORNER order over local axes (i, k, s)
+    corner = np.stack([nid(ss + c[2], kk + c[1], ii + c[0]) for c in _CORNER], axis=1)
+    hexm = kk < n_hex
+    Hc, Tc = corner[hexm], corner[~hexm]
+    H_k = kk[hexm]
+    n_h, n_t = Hc.shape[0], Tc.shape[0] * 6
+    tets = Tc[:, _KUHN].reshape(-1, 4)
+    # ladder cells beyond the tip: lower point j with upper point n - j
+    js = np.arange(nh)
+    lad_q = js[(js >= 1) & (js <= nh - 2)]
+    s_ext = np.arange(nz_wing, nz)
+    lad_cells = []
+    for s in s_ext:
+        a0, a1 = nid(s, 0, 0), nid(s + 1, 0, 0)
+        # prism at the trailing edge (0, 1, n-1), hexahedra (j, j+1, n-j-1, n-j), prism at the leading edge
+        lad_cells.append(("prism", np.array([[a0 + 0, a0 + 1, a0 + n - 1, a1 + 0, a1 + 1, a1 + n - 1]])))
+        q = np.stack([lad_q, lad_q + 1, n - lad_q - 1, n - lad_q], 1)
+        lad_cells.append(("hex", np.concatenate([a0 + q, a1 + q], 1)))
+        lad_cells.append(("prism", np.array([[a0 + nh - 1, a0 + nh, a0 + nh + 1, a1 + nh - 1, a1 + nh, a1 + nh + 1]])))
+    LH = np.concatenate([c for kind, c in lad_cells if kind == "hex"])       # [m, 8]: 4 bottom + 4 top
+    LP = np.concatenate([c for kind, c in lad_cells if kind == "prism"])     # [m, 6]: 3 bottom + 3 top
+    # cell numbering: ring cells in (s, k, i) order with each outer hexahedron's
+    # six tetrahedra in place, then the ladder cells
+    ring_id = np.empty(len(kk), np.int64)
+    per = np.where(hexm, 1, 6)
+    start = np.concatenate([[0], np.cumsum(per)[:-1]])
+    ring_id[:] = start
+    n_ring = int(per.sum())
+    hex_id = ring_id[hexm]
+    tet_id = (ring_id[~hexm][:, None] + np.arange(6)[None, :]).ravel()
+    lh_id = n_ring + np.arange(LH.shape[0])
+    lp_id = n_ring + LH.shape[0] + np.arange(LP.shape[0])
+    nc = n_ring + LH.shape[0] + LP.shape[0]
+    Pn = np.stack([x, y, z], 1)
+
+    def outward(F, own_centre):
+        Fc = Pn[F].mean(1)
+        if F.shape[1] == 3:
+            nv = np.cross(Pn[F[:, 1]] - Pn[F[:, 0]], Pn[F[:, 2]] - Pn[F[:, 0]])
+        else:
+            nv = np.cross(Pn[F[:, 2]] - Pn[F[:, 0]], Pn[F[:, 3]] - Pn[F[:, 1]])
+        inward = np.einsum("ij,ij->i", nv, Fc - own_centre) < 0
+        F = F.copy()
+        F[inward] = F[inward][:, ::-1]
+        return F
+
+    tri_l, tri_o, quad_l, quad_o = [], [], [], []
+    # tetrahedra
+    lf = np.array([[1, 2, 3], [0, 3, 2], [0, 1, 3], [0, 2, 1]], np.int64)
+    tt = tets[:, lf].reshape(-1, 3)
+    to = np.repeat(tet_id, 4)
+    tri_l.append(outward(tt, Pn[tets].mean(1)[np.repeat(np.arange(len(tets)), 4)])); tri_o.append(to)
+    # ring hexahedra: 6 quads, the outer one (k + 1 side) of the last hex layer split in two
+    hcc = Pn[Hc].mean(1)
+    hq = Hc[:, _HEX_FACES]                                   # [n_h, 6, 4]
+    outer = H_k == n_hex - 1
+    # _HEX_FACES[3] = [3, 7, 6, 2] is the k + 1 face (corners with local k = 1)
+    keep = np.ones((n_h, 6), bool)
+    keep[outer, 3] = False
+    quad_l.append(outward(hq[keep], hcc[np.nonzero(keep)[0]])); quad_o.append(hex_id[np.nonzero(keep)[0]])
+    # the split k + 1 face: triangles of the Kuhn split of the tetrahedral cell
+    # above, whose k-face is (c0 c1 c5 c4) with diagonal c0 -> c5; in this
+    # hexahedron's corners those are (3, 2, 6, 7) with diagonal 3 -> 6
+    Ho = Hc[outer]
+    t1 = Ho[:, [3, 2, 6]]; t2 = Ho[:, [3, 6, 7]]
+    own = hex_id[outer]
+    tri_l.append(outward(np.concatenate([t1, t2]), np.concatenate([hcc[outer], hcc[outer]]))); tri_o.append(np.concatenate([own, own]))
+    # ladder hexahedra: corners (bottom j, j+1, n-j-1, n-j, then top) -> hex faces
+    lcc = Pn[LH].mean(1)
+    lhf = np.array([[0, 1, 2, 3], [4, 5, 6, 7], [0, 1, 5, 4], [1, 2, 6, 5], [2, 3, 7, 6], [3, 0, 4, 7]], np.int64)
+    lq = LH[:, lhf].reshape(-1, 4)
+    quad_l.append(outward(lq, lcc[np.repeat(np.arange(len(LH)), 6)])); quad_o.append(np.repeat(lh_id, 6))
+    pcc = Pn[LP].mean(1)
+    pt = LP[:, [[0, 1, 2], [3, 4, 5]]].reshape(-1, 3)
+    pq = LP[:, [[0, 1, 4, 3], [1, 2, 5, 4], [2, 0, 3, 5]]].reshape(-1, 4)
+    tri_l.append(outward(pt, pcc[np.repeat(np.arange(len(LP)), 2)])); tri_o.append(np.repeat(lp_id, 2))
+    quad_l.append(outward(pq, pcc[np.repeat(np.arange(len(LP)), 3)])); quad_o.append(np.repeat(lp_id, 3))
+    Tn, tl, tr = _dedupe_faces(np.concatenate(tri_l), np.concatenate(tri_o))
+    Qn, ql_, qr_ = _dedupe_faces(np.concatenate(quad_l), np.concatenate(quad_o))
+    nodes = np.full((len(Tn) + len(Qn), 4), -1, np.int64)
+    nodes[:len(Tn), :3] = Tn
+    nodes[len(Tn):] = Qn
+    cnt = np.concatenate([np.full(len(Tn), 3), np.full(len(Qn), 4)])
+    lc = np.concatenate([tl, ql_]); rc = np.concatenate([tr, qr_])
+    isb = rc < 0
+    forder = np.lexsort((rc, lc, ~isb))
+    nodes, cnt, lc, rc = nodes[forder], cnt[forder], lc[forder], rc[forder]
+    nb = int(isb.sum())
+    # boundary codes from the node indices: root plane, outer plane, cylinder, wall
+    fb = nodes[:nb]
+    valid = fb >= 0
+    fbs = np.where(valid, fb, fb[:, :1])
+    s_of = fbs // ((K + 1) * n); k_of = (fbs // n) % (K + 1)
+    bct = np.full(nb, FAR, np.int32)
+    bct[np.all(s_of == 0, axis=1)] = SYM
+    wall = np.all(k_of == 0, axis=1) & np.all(s_of <= nz_wing, axis=1)
+    bct[wall] = SOLID
+    flat = nodes[np.arange(4)[None, :] < cnt[:, None]]
+    return Mesh(3, x, y, z, cnt.astype(np.int32), flat.astype(np.int32), lc.astype(np.int32), rc.astype(np.int32),
+                nc, nb, bct, meta=dict(kind="swept_wing_hybrid", n_around=n, n_hex=n_hex, n_tet=n_tet,
+                                       nz_wing=nz_wing, nz_tip=nz_tip, sweep_deg=sweep_deg, y1=y1,
+                                       semi_span=semi))

@@ -104,3 +104,14 @@ def rans_airfoil(mach: float, aoa: float, reynolds: float, **kw) -> OfgParams:
                 aoa_degree=aoa, reynolds=reynolds, cflst=1.0, cfled=20.0, ncfl=200, precision=1, sweep_order=1)
     base.update(kw)
     return defaults(**base)
+
+
+def transonic_wing(**kw) -> OfgParams:
+    """3-D transonic swept wing, RANS-SA: SLAU2, Green-Gauss gradients with the
+    Barth limiter, LU-SGS with the reference regression cases' CFL ramp
+    (0.1 -> 10 over 100 steps), Mach 0.84, AoA 3.06 degrees, Re 1.2e7, mixed
+    precision."""
+    base = dict(dimension=3, ischeme=12, ilim=1, igrad=0, vismodel=3, mach_ref=0.84, aoa_degree=3.06,
+                reynolds=1.2e7, cflst=0.1, cfled=10.0, ncfl=100, precision=1)
+    base.update(kw)
+    return defaults(**base)

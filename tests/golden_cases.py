@@ -26,6 +26,10 @@ CASES = {
     "plate2d_laminar_roe_inflow_extrap": dict(steps=30),
     "plate2d_sa_roe_inflow_extrap": dict(steps=30),
     "plate2d_laminar_roe_isowall": dict(steps=30),
+    # a small swept-wing hybrid mesh: hexahedral layers whose outer face is
+    # split into two triangles, tetrahedra, the tip's prisms and hexahedra;
+    # SLAU2 + Green-Gauss + Barth + SA at the transonic wing condition
+    "wing3d_small_slau2_barth_sa": dict(steps=10),
 }
 # the 2-D Euler bump at its benchmark size: 256x128 quads split into 65,536
 # jittered triangles, first-order Roe, LU-SGS, CFL 5, run for 2,000 outer
@@ -71,8 +75,16 @@ def inflow_extrap(mesh):
     return mesh
 
 
+def small_wing():
+    m = meshgen.swept_wing_hybrid(n_around=32, n_hex=4, n_tet=4, nz_wing=6, nz_tip=3)
+    m.wall_dist = wall_distance(m)
+    return m
+
+
 def build(name):
     steps = CASES[name]["steps"]
+    if name == "wing3d_small_slau2_barth_sa":
+        return small_wing(), P.transonic_wing(precision=0), steps
     if name == "plate2d_laminar_roe_inflow_extrap":
         return inflow_extrap(meshgen.plate_2d(24, 16)), P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=1e5,
                                                                     vismodel=1), steps

@@ -181,3 +181,35 @@ def test_rcm_order_rejects_bad_arguments():
     assert L.ofg_rcm_order(2, 3, -1, lc, rc, perm) == -1      # negative boundary-face count
     assert L.ofg_rcm_order(2, 3, 1, lc, rc, perm) == -1       # interior face to a cell out of range
     assert L.ofg_colour_order(2, 3, -1, lc, rc, perm) == -1
+
+
+def test_swept_wing_mesh_is_closed_and_classified():
+    # every cell's outward face-area vectors sum to zero, every volume is
+    # positive, and the boundary faces are wall (wing and tip), symmetry (root)
+    # and far field, in the counts the construction gives
+    import numpy as np
+    from oneflow_b200 import meshgen
+    m = meshgen.swept_wing_hybrid(n_around=32, n_hex=4, n_tet=4, nz_wing=6, nz_tip=3)
+    P3 = np.stack([m.x, m.y, m.z], 1)
+    off = np.concatenate([[0], np.cumsum(m.face_node_count)])
+    A = np.zeros((m.n_faces, 3)); C = np.zeros((m.n_faces, 3))
+    for k in (3, 4):
+        sel = np.nonzero(m.face_node_count == k)[0]
+        pts = P3[m.face_nodes[off[sel][:, None] + np.arange(k)[None, :]]]
+        c = pts.mean(1)
+        A[sel] = sum(0.5 * np.cross(pts[:, j] - c, pts[:, (j + 1) % k] - c) for j in range(k))
+        C[sel] = c
+    inn = m.rc >= 0
+    acc = np.zeros((m.n_cells, 3)); vol = np.zeros(m.n_cells)
+    np.add.at(acc, m.lc, A); np.add.at(acc, m.rc[inn], -A[inn])
+    fv = np.einsum("ij,ij->i", C, A) / 3.0
+    np.add.at(vol, m.lc, fv); np.add.at(vol, m.rc[inn], -fv[inn])
+    assert np.abs(acc).max() < 1e-12 and vol.min() > 0.0
+    assert np.all(m.rc[:m.n_bfaces] < 0) and np.all(m.rc[m.n_bfaces:] >= 0)
+    counts = np.bincount(m.bc_type, minlength=7)
+    n = 32
+    # the root plane: the hexahedra's quadrilaterals and two triangles per split hexahedron
+    assert counts[3] == n * 4 + n * 4 * 2
+    # wall faces: the wing's quadrilaterals (n per slab) and the tip cap (n / 2 cells)
+    assert counts[2] == n * 6 + (n // 2)
+    assert counts[4] > 0 and counts[1] == counts[5] == counts[6] == 0
