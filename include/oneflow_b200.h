@@ -341,7 +341,11 @@ typedef struct ofg_tuning {
     int    grad_min_blocks;   /* gradients + limiter: 4, 6 (default) or 8          */
     int    sweep_min_blocks;  /* LU-SGS level kernels: 6, 8 (default) or 10        */
     int    sweep_block;       /* LU-SGS level kernels: 64 or 128 (default)         */
-    int    reserved[3];
+    int    sweep_persistent;  /* 0: one launch per level (default); 1: one launch
+                                 per sweep, a single block running every level
+                                 with a block barrier between levels (the same
+                                 bits; for many small levels).  Both paths.   */
+    int    reserved[2];
     double ms_default;        /* device ms per iteration of these kernels, default shapes */
     double ms_tuned;          /* the same with the shapes chosen                   */
 } ofg_tuning;
@@ -355,8 +359,8 @@ typedef struct ofg_tuning {
    rebuilt at the next ofg_step.  The result is cached per mesh (cell, face and
    boundary-face counts and a hash of the face->cell lists) and parameter set:
    a later context with the same mesh takes the cached shapes without timing.
-   Mixed precision only (the FP64 path keeps its fixed shapes, returned with
-   ms_* = 0).  Needs a state (after ofg_init_flowfield / upload / a step). */
+   On the FP64 path only sweep_persistent is timed (its kernels keep their
+   fixed shapes).  Needs a state (after ofg_init_flowfield / upload / a step). */
 int ofg_autotune(ofg_ctx *ctx, int reps, ofg_tuning *out);
 int ofg_get_tuning(ofg_ctx *ctx, ofg_tuning *out);
 /* Sets the shapes (values outside the lists above return OFG_E_ARG). */

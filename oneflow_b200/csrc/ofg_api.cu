@@ -435,7 +435,7 @@ void ofg_destroy(ofg_ctx *c) {
     destroy_graphs(c);
     void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
                     c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist, c->d_wall, c->d_wallG,
-                    c->d_fgeoD, c->d_fofs, c->d_lr, c->d_fout,
+                    c->d_fgeoD, c->d_fofs, c->d_lr, c->d_fout, c->d_lowOff, c->d_upOff,
                     c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_rad,
                     c->d_bcq, c->d_partial, c->d_npart, c->d_tpart, c->d_red, c->d_redCount, c->d_stage, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
@@ -540,6 +540,8 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     if ((rc = upload(c, &c->d_bct, c->bct.data(), nBFaces))) return rc;
     if ((rc = upload(c, &c->d_lowOrder, c->lowOrder.data(), nCells))) return rc;
     if ((rc = upload(c, &c->d_upOrder, c->upOrder.data(), nCells))) return rc;
+    if ((rc = upload(c, &c->d_lowOff, c->lowOff.data(), c->lowOff.size()))) return rc;
+    if ((rc = upload(c, &c->d_upOff, c->upOff.data(), c->upOff.size()))) return rc;
     if ((rc = upload(c, &c->d_key, c->key.data(), c->nT))) return rc;
     if ((rc = upload(c, &c->d_wdist, c->wdist.data(), nCells))) return rc;
     {
@@ -1519,7 +1521,7 @@ int ofg_rcm_order(int nCells, int nFaces, int nBFaces, const int *lCells, const 
 static bool valid_tuning(const ofg_tuning &t) {
     auto in = [](int v, std::initializer_list<int> l) { for (int x : l) if (x == v) return true; return false; };
     return in(t.face_min_blocks, {2, 3, 4, 5}) && in(t.face_block, {64, 128}) && in(t.grad_min_blocks, {4, 6, 8}) &&
-           in(t.sweep_min_blocks, {6, 8, 10}) && in(t.sweep_block, {64, 128});
+           in(t.sweep_min_blocks, {6, 8, 10}) && in(t.sweep_block, {64, 128}) && in(t.sweep_persistent, {0, 1});
 }
 
 int ofg_get_tuning(ofg_ctx *c, ofg_tuning *out) {
@@ -1556,11 +1558,12 @@ int ofg_autotune(ofg_ctx *c, int reps, ofg_tuning *out) {
     int rc = check_tid(c, OFG_NS_SOLVER);
     if (rc) return rc;
     if (c->pendingNext || c->pendingTurb) return c->fail(OFG_E_STATE, "UPDATE_FLOWFIELD without CALC_BOUNDARY");
-    if (c->p.precision != OFG_PREC_MIXED || multi_stage(c)) {   // fixed shapes
+    if (multi_stage(c)) {   // no sweeps, fixed shapes
         c->tune.ms_default = c->tune.ms_tuned = 0.0;
         if (out) *out = c->tune;
         return OFG_OK;
     }
+    const bool mixed = c->p.precision == OFG_PREC_MIXED;
     if (reps < 1) reps = 5;
     const std::string key = tune_key(c);
     {
@@ -1600,13 +1603,20 @@ int ofg_autotune(ofg_ctx *c, int reps, ofg_tuning *out) {
     // groups in turn, each over its own candidates, the others at their current choice
     struct Cand { int *a; int *b; std::vector<std::pair<int, int>> values; std::vector<int> tasks; };
     ofg_tuning &T = c->tune;
-    std::vector<Cand> groups = {
-        {&T.face_min_blocks, &T.face_block, {{2, 128}, {3, 128}, {4, 128}, {5, 128}, {2, 64}, {3, 64}, {4, 64}, {5, 64}},
-         {T_P_FLUX}},
-        {&T.grad_min_blocks, nullptr, {{4, 0}, {6, 0}, {8, 0}}, {T_P_GRADLIM}},
-        {&T.sweep_min_blocks, &T.sweep_block, {{6, 128}, {8, 128}, {10, 128}, {6, 64}, {8, 64}, {10, 64}},
-         {T_LOWER, T_UPPER}},
-    };
+    std::vector<Cand> groups;
+    if (mixed) {
+        groups.push_back({&T.face_min_blocks, &T.face_block,
+                          {{2, 128}, {3, 128}, {4, 128}, {5, 128}, {2, 64}, {3, 64}, {4, 64}, {5, 64}}, {T_P_FLUX}});
+        groups.push_back({&T.grad_min_blocks, nullptr, {{4, 0}, {6, 0}, {8, 0}}, {T_P_GRADLIM}});
+        groups.push_back({&T.sweep_min_blocks, &T.sweep_block,
+                          {{6, 128}, {8, 128}, {10, 128}, {6, 64}, {8, 64}, {10, 64}}, {T_LOWER, T_UPPER}});
+    }
+    // the sweep schedule: level launches or the persistent single-block form
+    // (not tried when the levels average more than 16 passes of the block:
+    // one block cannot keep up with a full-width level launch there)
+    const int nlev = std::max<int>(1, int(c->lowOff.size()) - 1);
+    if (c->nCells / nlev <= 16 * kSeqThreads)
+        groups.push_back({&T.sweep_persistent, nullptr, {{0, 0}, {1, 0}}, {T_LOWER, T_UPPER}});
     for (Cand &g : groups) {
         const int a0 = *g.a, b0 = g.b ? *g.b : 0;
         double best = 1e30, first = 0.0;

@@ -13,7 +13,7 @@ struct ofg_ctx {
     ofg_params p{};
     ofg::DevParams dp{};
     std::string err;
-    ofg_tuning tune{3, 128, 6, 8, 128, {0, 0, 0}, 0.0, 0.0};   // launch shapes of the mixed path's gathers
+    ofg_tuning tune{3, 128, 6, 8, 128, 0, {0, 0}, 0.0, 0.0};   // launch shapes of the gathers and sweeps
     unsigned long long meshHash = 0;                         // of the face->cell lists (autotuner cache key)
 
     // ---- mesh (host copies, reference numbering) ----
@@ -33,6 +33,7 @@ struct ofg_ctx {
     int *d_nb_off = nullptr, *d_nbl = nullptr;              // per-cell neighbour lists (int2 pairs)
     int *d_lo_off = nullptr, *d_lol = nullptr, *d_up_off = nullptr, *d_upl = nullptr;
     int *d_lowOrder = nullptr, *d_upOrder = nullptr, *d_key = nullptr;
+    int *d_lowOff = nullptr, *d_upOff = nullptr;           // level offsets of the sweeps (persistent form)
     void *d_fgeo = nullptr, *d_cgeo = nullptr;              // face / cell records at the face precision
     double *d_fgeoD = nullptr;                              // mixed path: FP64 face records
     float *d_fofs = nullptr;                                // mixed path: face-local offsets [F][FOFS]

@@ -42,6 +42,7 @@ template <> struct MinBlocks<float> {
 };
 
 constexpr int kRedBlocks = 148;   // blocks of the grid reductions (one per SM)
+constexpr int kSeqThreads = 512;  // threads of the one block of a persistent (single-block) sweep
 
 constexpr int GLR = 24;   // gradient+limiter record: [var*3+dir] for 6 vars (q, T), limiter at 18..22
 constexpr int FGR = 8;    // face record: nx ny nz area xfc yfc zfc dist (|n . (x_r - x_l)|)

@@ -1205,7 +1205,10 @@ __device__ __forceinline__ void face_increment(const DevParams &P, const R *qa, 
     for (int e = 0; e < NEQ; ++e) rhs0[e] += double(df[e]);
 }
 
-template <typename R>
+// COH: the neighbours' increments are read with coherent loads, for a kernel
+// that itself wrote them earlier (the persistent sweep); otherwise through the
+// read-only path
+template <typename R, bool COH = false>
 __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *off, const int2 *list, double *rhs0) {
     R qc[REC];
     ld8(A.qs + (size_t)c * REC, qc);
@@ -1218,9 +1221,10 @@ __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *
         R qn[REC], fg[FGR], dqj[DQR];
         ld8(A.qs + (size_t)nb * REC, qn);
         ld8(A.fgeo + (size_t)f * FGR, fg);
-        // the neighbour's increment was written by an earlier level's launch
-        // and is not written by this one: read-only here
-        ld8(A.dq + (size_t)nb * DQR, dqj);
+        // the neighbour's increment was written by an earlier level (an earlier
+        // launch, or an earlier pass of the persistent sweep)
+        if constexpr (COH) ldp8(A.dq + (size_t)nb * DQR, dqj);
+        else ld8(A.dq + (size_t)nb * DQR, dqj);
         R volb = A.P.visSRModel == 1 ? A.cgeo[(size_t)nb * CGR + 3] : R(1);
         R xn = fg[0], yn = fg[1], zn = fg[2];
         if (nb_right(e2)) { xn = -xn; yn = -yn; zn = -zn; }   // GCom::SetGeometry
@@ -1228,13 +1232,10 @@ __device__ __forceinline__ void sweep_rhs0(const KArgs<R> &A, int c, const int *
     }
 }
 
-template <typename R, int MINB = MinBlocks<R>::sw>
-__global__ void __launch_bounds__(128, MINB) k_lusgs_lower(KArgs<R> A, const int *order, int start, int count) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    int c = order[start + t];
+template <typename R, bool COH>
+__device__ __forceinline__ void lusgs_lower_cell(const KArgs<R> &A, int c) {
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    sweep_rhs0(A, c, A.lo_off, A.lol, rhs0);
+    sweep_rhs0<R, COH>(A, c, A.lo_off, A.lol, rhs0);
     double rad = A.rad[c];
     const double *rs = A.res + (size_t)c * NEQ;
     R o[DQR];
@@ -1245,13 +1246,10 @@ __global__ void __launch_bounds__(128, MINB) k_lusgs_lower(KArgs<R> A, const int
     st4(A.dq + (size_t)c * DQR + 4, o + 4);
 }
 
-template <typename R, int MINB = MinBlocks<R>::sw>
-__global__ void __launch_bounds__(128, MINB) k_lusgs_upper(KArgs<R> A, const int *order, int start, int count) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    int c = order[start + t];
+template <typename R, bool COH>
+__device__ __forceinline__ void lusgs_upper_cell(const KArgs<R> &A, int c) {
     double rhs0[NEQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    sweep_rhs0(A, c, A.up_off, A.upl, rhs0);   // ghost increments are zero: boundary faces not listed
+    sweep_rhs0<R, COH>(A, c, A.up_off, A.upl, rhs0);   // ghost increments are zero: boundary faces not listed
     double rad = A.rad[c];
     R o[DQR];
     ldp8(A.dq + (size_t)c * DQR, o);   // its own lower-sweep increment, rewritten below
@@ -1259,6 +1257,46 @@ __global__ void __launch_bounds__(128, MINB) k_lusgs_upper(KArgs<R> A, const int
     for (int e = 0; e < NEQ; ++e) o[e] = R(add_neg_quot(double(o[e]), rhs0[e], rad));
     st4(A.dq + (size_t)c * DQR, o);
     st4(A.dq + (size_t)c * DQR + 4, o + 4);
+}
+
+// one level of a sweep per launch (cells order[start .. start+count))
+template <typename R, int MINB = MinBlocks<R>::sw>
+__global__ void __launch_bounds__(128, MINB) k_lusgs_lower(KArgs<R> A, const int *order, int start, int count) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) lusgs_lower_cell<R, false>(A, order[start + t]);
+}
+
+template <typename R, int MINB = MinBlocks<R>::sw>
+__global__ void __launch_bounds__(128, MINB) k_lusgs_upper(KArgs<R> A, const int *order, int start, int count) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) lusgs_upper_cell<R, false>(A, order[start + t]);
+}
+
+// The persistent form: one block of kSeqThreads runs every level of the sweep
+// in order, with a block barrier between levels (a barrier also orders the
+// block's global writes before its later reads, so each level sees the
+// increments of the levels before it).  The same per-cell arithmetic as the
+// level launches, so the same bits; it replaces nlev launches by one, which
+// pays off when the levels are many and small (natural-order sweeps of
+// structured-like meshes: hundreds of levels of tens to hundreds of cells).
+template <typename R>
+__global__ void __launch_bounds__(kSeqThreads, 1) k_lusgs_lower_seq(KArgs<R> A, const int *order, const int *loff,
+                                                                 int nlev) {
+    for (int l = 0; l < nlev; ++l) {
+        const int st = loff[l], en = loff[l + 1];
+        for (int k = st + threadIdx.x; k < en; k += blockDim.x) lusgs_lower_cell<R, true>(A, order[k]);
+        __syncthreads();
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kSeqThreads, 1) k_lusgs_upper_seq(KArgs<R> A, const int *order, const int *loff,
+                                                                 int nlev) {
+    for (int l = 0; l < nlev; ++l) {
+        const int st = loff[l], en = loff[l + 1];
+        for (int k = st + threadIdx.x; k < en; k += blockDim.x) lusgs_upper_cell<R, true>(A, order[k]);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------

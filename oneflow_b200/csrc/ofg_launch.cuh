@@ -173,6 +173,10 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     case T_LOWER: {
         KArgs<R> A = make_args<R>(c, false);
         int nl = int(c->lowOff.size()) - 1;
+        if (c->tune.sweep_persistent) {
+            OFG_LAUNCH(k_lusgs_lower_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_lowOrder, (const int *)c->d_lowOff, nl);
+            break;
+        }
         for (int l = 0; l < nl; ++l) {
             int st = c->lowOff[l], cnt = c->lowOff[l + 1] - st;
             const int *ord = (const int *)c->d_lowOrder;
@@ -192,6 +196,10 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     case T_UPPER: {
         KArgs<R> A = make_args<R>(c, false);
         int nl = int(c->upOff.size()) - 1;
+        if (c->tune.sweep_persistent) {
+            OFG_LAUNCH(k_lusgs_upper_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_upOrder, (const int *)c->d_upOff, nl);
+            break;
+        }
         for (int l = 0; l < nl; ++l) {
             int st = c->upOff[l], cnt = c->upOff[l + 1] - st;
             const int *ord = (const int *)c->d_upOrder;
@@ -270,6 +278,10 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     case T_TURB_LOWER: {
         KArgs<R> A = make_args<R>(c, true);
         int nl = int(c->lowOff.size()) - 1;
+        if (c->tune.sweep_persistent) {
+            OFG_LAUNCH(k_turb_lower_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_lowOrder, (const int *)c->d_lowOff, nl);
+            break;
+        }
         for (int l = 0; l < nl; ++l) {
             int st = c->lowOff[l], cnt = c->lowOff[l + 1] - st;
             OFG_LAUNCH(k_turb_lower<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_lowOrder, st, cnt);
@@ -279,6 +291,10 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
     case T_TURB_UPPER: {
         KArgs<R> A = make_args<R>(c, true);
         int nl = int(c->upOff.size()) - 1;
+        if (c->tune.sweep_persistent) {
+            OFG_LAUNCH(k_turb_upper_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_upOrder, (const int *)c->d_upOff, nl);
+            break;
+        }
         for (int l = 0; l < nl; ++l) {
             int st = c->upOff[l], cnt = c->upOff[l + 1] - st;
             OFG_LAUNCH(k_turb_upper<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_upOrder, st, cnt);

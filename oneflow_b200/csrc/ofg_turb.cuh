@@ -381,10 +381,7 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_rhs(KArgs<R> A) 
 // LU-SGS sweeps of the SA equation (codes/uturb/src/UTurbLusgs.cpp:90-300,
 // codes/turb/src/TurbLusgs.cpp:123-260): dfj = matrix * dq_j
 template <typename R>
-__global__ void __launch_bounds__(128) k_turb_lower(KArgs<R> A, const int *order, int start, int count) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    int c = order[start + t];
+__device__ __forceinline__ void turb_lower_cell(const KArgs<R> &A, int c) {
     double rhs0 = 0.0;
     for (int k = A.lo_off[c]; k < A.lo_off[c + 1]; ++k) {
         int2 e2 = __ldg(&A.lol[k]);
@@ -392,6 +389,45 @@ __global__ void __launch_bounds__(128) k_turb_lower(KArgs<R> A, const int *order
         rhs0 += (nb_right(e2) ? A.matL[f] : A.matR[f]) * A.dnut[e2.y];
     }
     A.dnut[c] = (A.resT[c] - rhs0) / A.impsrT[c];
+}
+
+template <typename R>
+__device__ __forceinline__ void turb_upper_cell(const KArgs<R> &A, int c) {
+    double rhs0 = 0.0;
+    for (int k = A.up_off[c]; k < A.up_off[c + 1]; ++k) {   // ghost increments are zero: not listed
+        int2 e2 = __ldg(&A.upl[k]);
+        int f = nb_face(e2);
+        rhs0 += (nb_right(e2) ? A.matL[f] : A.matR[f]) * A.dnut[e2.y];
+    }
+    A.dnut[c] = add_neg_quot(A.dnut[c], rhs0, A.impsrT[c]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_turb_lower(KArgs<R> A, const int *order, int start, int count) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) turb_lower_cell(A, order[start + t]);
+}
+
+// the persistent forms (one block, every level, a barrier between levels; the
+// increments are read with plain, coherent loads)
+template <typename R>
+__global__ void __launch_bounds__(kSeqThreads, 1) k_turb_lower_seq(KArgs<R> A, const int *order, const int *loff,
+                                                                int nlev) {
+    for (int l = 0; l < nlev; ++l) {
+        const int st = loff[l], en = loff[l + 1];
+        for (int k = st + threadIdx.x; k < en; k += blockDim.x) turb_lower_cell(A, order[k]);
+        __syncthreads();
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kSeqThreads, 1) k_turb_upper_seq(KArgs<R> A, const int *order, const int *loff,
+                                                                int nlev) {
+    for (int l = 0; l < nlev; ++l) {
+        const int st = loff[l], en = loff[l + 1];
+        for (int k = st + threadIdx.x; k < en; k += blockDim.x) turb_upper_cell(A, order[k]);
+        __syncthreads();
+    }
 }
 
 // UPDATE_FLOWFIELD (TurbUpdate::CalcFlowField1Equ, crelax = 1) fused with the
@@ -410,15 +446,7 @@ __device__ __forceinline__ void turb_update_cell(const KArgs<R> &A, int c, doubl
 template <typename R>
 __global__ void __launch_bounds__(128) k_turb_upper(KArgs<R> A, const int *order, int start, int count) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    int c = order[start + t];
-    double rhs0 = 0.0;
-    for (int k = A.up_off[c]; k < A.up_off[c + 1]; ++k) {   // ghost increments are zero: not listed
-        int2 e2 = __ldg(&A.upl[k]);
-        int f = nb_face(e2);
-        rhs0 += (nb_right(e2) ? A.matL[f] : A.matR[f]) * A.dnut[e2.y];
-    }
-    A.dnut[c] = add_neg_quot(A.dnut[c], rhs0, A.impsrT[c]);
+    if (t < count) turb_upper_cell(A, order[start + t]);
 }
 
 template <typename R>

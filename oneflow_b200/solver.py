@@ -26,7 +26,8 @@ class OfgError(RuntimeError):
 class OfgTuning(C.Structure):
     """ctypes mirror of ofg_tuning (include/oneflow_b200.h)."""
     _fields_ = [("face_min_blocks", C.c_int), ("face_block", C.c_int), ("grad_min_blocks", C.c_int),
-                ("sweep_min_blocks", C.c_int), ("sweep_block", C.c_int), ("reserved", C.c_int * 3),
+                ("sweep_min_blocks", C.c_int), ("sweep_block", C.c_int), ("sweep_persistent", C.c_int),
+                ("reserved", C.c_int * 2),
                 ("ms_default", C.c_double), ("ms_tuned", C.c_double)]
 
     def as_dict(self) -> dict:

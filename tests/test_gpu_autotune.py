@@ -62,3 +62,26 @@ def test_fp64_path_keeps_its_fixed_shapes():
     s.init_flowfield()
     t = s.autotune()
     assert t["ms_default"] == 0.0 and t["ms_tuned"] == 0.0
+
+
+@pytest.mark.parametrize("case", ["bump_fp64_natural", "sa_plate_mixed_natural", "sa_plate_mixed_colour"])
+def test_persistent_sweep_gives_the_same_bits(case):
+    # one launch per sweep (a single block running every level with a block
+    # barrier between levels) against one launch per level: the same
+    # per-cell arithmetic in the same dependency order, so the same bits
+    if case == "bump_fp64_natural":
+        m, prm = meshgen.bump_channel(32, 16), P.euler_bump(ilim=2, vencat_coef=0.05)
+    else:
+        m = meshgen.plate_2d(32, 24, y1=1e-5, ratio=1.25)
+        from oneflow_b200.walldist import wall_distance
+        m.wall_dist = wall_distance(m)
+        prm = P.defaults(ischeme=1, ilim=0, mach_ref=0.2, reynolds=5e6, vismodel=3, precision=1,
+                         sweep_order=1 if case.endswith("colour") else 0)
+    a = Solver(m, prm); a.init_flowfield()
+    b = Solver(m, prm); b.init_flowfield()
+    b.set_tuning(sweep_persistent=1)
+    a.step(15); b.step(15)
+    assert np.array_equal(a.state(), b.state())
+    assert np.array_equal(a.res_history(), b.res_history())
+    if prm.vismodel >= 3:
+        assert np.array_equal(a.state(TURB_SOLVER), b.state(TURB_SOLVER))
