@@ -194,13 +194,17 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         break;
     }
     case T_UPPER: {
+        // level 0 of the upper sweep holds the cells without later
+        // neighbours: their increment gains -(+0)/rad, which leaves it
+        // unchanged bit for bit (add_neg_quot), so that level is not launched
         KArgs<R> A = make_args<R>(c, false);
         int nl = int(c->upOff.size()) - 1;
         if (c->tune.sweep_persistent) {
-            OFG_LAUNCH(k_lusgs_upper_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_upOrder, (const int *)c->d_upOff, nl);
+            OFG_LAUNCH(k_lusgs_upper_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_upOrder, (const int *)c->d_upOff + 1,
+                       nl - 1);
             break;
         }
-        for (int l = 0; l < nl; ++l) {
+        for (int l = 1; l < nl; ++l) {
             int st = c->upOff[l], cnt = c->upOff[l + 1] - st;
             const int *ord = (const int *)c->d_upOrder;
             if constexpr (sizeof(R) == 4) {
@@ -288,14 +292,15 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
         }
         break;
     }
-    case T_TURB_UPPER: {
+    case T_TURB_UPPER: {   // level 0 skipped, as in T_UPPER
         KArgs<R> A = make_args<R>(c, true);
         int nl = int(c->upOff.size()) - 1;
         if (c->tune.sweep_persistent) {
-            OFG_LAUNCH(k_turb_upper_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_upOrder, (const int *)c->d_upOff, nl);
+            OFG_LAUNCH(k_turb_upper_seq<R>, 1, kSeqThreads, s, A, (const int *)c->d_upOrder, (const int *)c->d_upOff + 1,
+                       nl - 1);
             break;
         }
-        for (int l = 0; l < nl; ++l) {
+        for (int l = 1; l < nl; ++l) {
             int st = c->upOff[l], cnt = c->upOff[l + 1] - st;
             OFG_LAUNCH(k_turb_upper<R>, nblk(cnt, 128), 128, s, A, (const int *)c->d_upOrder, st, cnt);
         }

@@ -24,11 +24,15 @@ bump2d_c1.npz is the 2-D Euler bump at its benchmark size (65,536 triangles,
 first-order Roe, LU-SGS, CFL 5, 2,000 outer iterations) as the reference ran
 it: every 16th interior cell of the final state, the per-equation sum and sum
 of squares of the whole interior state, the forces and the residual history
-(the whole state would be 2.6 MB).
+(the whole state would be 2.6 MB).  bump2d_c1_converged.npz: the same case run for
+60,000 iterations, to the round-off floor of its residual (every 16th cell, forces,
+every 100th residual row, the final drop).
 
     python tests/golden/make_golden.py --restart-only   # only the restart fixtures
     python tests/golden/make_golden.py --walldist-only  # only the wall-distance fixtures
     python tests/golden/make_golden.py --c1-only        # only the benchmark-size bump (about 2 CPU minutes)
+    python tests/golden/make_golden.py --c1-converged-only  # the same bump run to its round-off floor
+                                                        # (60,000 iterations, about 55 CPU minutes)
     python tests/golden/make_golden.py --case=<name>    # one case fixture"""
 import json
 import os
@@ -89,9 +93,23 @@ def c1_fixture():
     print("bump2d_c1", mesh.n_cells, "cells", C1_STEPS, "steps")
 
 
+def c1_converged_fixture(steps: int = 60000):
+    mesh, prm = build_c1()
+    dump, rows = run_ref(mesh, prm, steps)
+    q = dump["q"][:, :mesh.n_cells]
+    h = rows[:, 2]
+    np.savez_compressed(os.path.join(HERE, "bump2d_c1_converged.npz"), q_sub=q[:, ::C1_STRIDE],
+                        forces=dump["forces"].ravel()[:13], reshist_every_100=rows[::100, 2:7],
+                        final_drop=float(h[-1] / h[0]), steps=steps, params=json.dumps(P.to_dict(prm)))
+    print("bump2d_c1_converged", mesh.n_cells, "cells", steps, "steps, drop", h[-1] / h[0])
+
+
 def main():
     if "--c1-only" in sys.argv:
         c1_fixture()
+        return
+    if "--c1-converged-only" in sys.argv:
+        c1_converged_fixture()
         return
     if "--walldist-only" in sys.argv:
         walldist_fixtures()

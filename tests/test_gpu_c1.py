@@ -70,3 +70,41 @@ def test_c1_mixed_path_tracks_the_reference_transient(gold):
     f, fr = g.forces(1.0), gold["forces"]
     k = [0, 1, 9, 10]
     assert np.abs(f[k] - fr[k]).max() / np.abs(fr[k]).max() < 5e-6, (f[k], fr[k])
+
+
+@pytest.fixture(scope="module")
+def converged():
+    fn = os.path.join(HERE, "golden", "bump2d_c1_converged.npz")
+    if not os.path.exists(fn):
+        pytest.skip("converged fixture absent")
+    return np.load(fn)
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 1e-6)], ids=["fp64", "mixed"])
+def test_c1_converged_forces_match_the_reference(converged, precision, tol):
+    # The steady solution itself: the reference's run to its round-off floor
+    # (tests/golden/bump2d_c1_converged.npz) against the GPU's, converged with
+    # colour-major sweeps (a different iteration to the same steady state):
+    # forces within 1e-6 relative on the mixed path (the target), within
+    # round-off on the FP64 path; density and pressure within 1e-5 relative L2
+    mesh, prm = build_c1()
+    prm.precision = precision
+    prm.sweep_order = 1
+    g = Solver(mesh, prm)
+    g.init_flowfield()
+    want = float(converged["final_drop"])
+    done = 0
+    while done < int(converged["steps"]):
+        g.step(5000)
+        done += 5000
+        h = g.res_history()[:, 0]
+        if h[-1] / h[0] <= max(want, 1e-12 if precision == 0 else 2e-9):
+            break
+    N = mesh.n_cells
+    q = g.state()[:, :N][:, ::C1_STRIDE]
+    sub = converged["q_sub"]
+    for e in (0, 4):
+        assert np.linalg.norm(q[e] - sub[e]) / np.linalg.norm(sub[e]) < 1e-5, e
+    f, fr = g.forces(1.0), converged["forces"]
+    k = [0, 1, 9, 10]
+    assert np.abs(f[k] - fr[k]).max() / np.abs(fr[k]).max() < tol, (f[k], fr[k], done)
