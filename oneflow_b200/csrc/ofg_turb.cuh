@@ -161,11 +161,96 @@ __device__ __forceinline__ R calc_angle(R dx, R dy, R dz, R dist) {
 // The FP64 path keeps the reference's three face passes (spectrum, convection,
 // diffusion) in order; the FP32 path fuses them into one pass with separate
 // FP64 accumulators that are added in the reference's order at the end.
+// The SA source of cell c (TurbCom::CalcSrcSa, codes/turb/src/TurbCom.cpp:771-881)
+// and its implicit part: adds the source x volume to acc and its linearised
+// part x volume to imp (gnc: the cell's gradient of nu~).
+template <typename R>
+__device__ __forceinline__ void sa_source(const KArgs<R> &A, int c, double nutc, double vol, const R *gnc,
+                                          double &imp, double &acc) {
+    const DevParams &P = A.P;
+    const double half = 0.5;
+    double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
+    {
+        R gq[GLR];
+#pragma unroll
+        for (int i = 0; i < 12; i += 4) ld4(A.gl + (size_t)c * GLR + i, gq + i);
+        dudx = gq[IU * 3]; dudy = gq[IU * 3 + 1]; dudz = gq[IU * 3 + 2];
+        dvdx = gq[IV * 3]; dvdy = gq[IV * 3 + 1]; dvdz = gq[IV * 3 + 2];
+        dwdx = gq[IW * 3]; dwdy = gq[IW * 3 + 1]; dwdz = gq[IW * 3 + 2];
+    }
+    double rho = A.q[(size_t)c * REC + IR], nuet = nutc, vlc = A.q[(size_t)c * REC + IML];
+    double olam = rho / (vlc + SMALLD);
+    double ls = A.walldist[c];
+    double od2 = 1.0 / (ls * ls);
+    double work1 = dudx + dvdy + dwdz;
+    double work2 = SQR3(dudx, dudy, dudz);
+    double work3 = SQR3(dudy + dvdx, dvdz + dwdy, dwdx + dudz);
+    double work4 = sqrt(SQR3(dwdy - dvdz, dudz - dwdx, dvdx - dudy));
+    if (P.iprod_sa == 1) {
+        double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
+        work4 = sqrt(fabs(stp));
+    } else if (P.iprod_sa == 4) {
+        double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
+        double str = work4;
+        work4 = str - 2.0 * fmax(0.0, str - sqrt(fabs(stp)));
+    } else if (P.iprod_sa == 5) {
+        double stp = fabs(2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1);
+        double str = work4;
+        work4 = str * (1.0 - fmax(0.0, (str * str - stp) / (str * str + stp + SMALLD)));
+    }
+    double str = work4;
+    double xsi = nuet * olam + SMALLD;
+    double xsi3 = xsi * xsi * xsi;
+    double fv1 = xsi3 / (xsi3 + P.sa_cv13);
+    double fv2 = 1.0 - xsi / (1.0 + xsi * fv1);
+    double rs = nuet * P.sa_okarm2 * od2 * P.oreynolds;
+    double nuetRs = nuet * rs;
+    double sBar = rs * fv2;
+    double omega = str;
+    double stdv;
+    if (sBar >= -P.sa_sac2 * omega) stdv = omega + sBar;
+    else {
+        double term1 = (P.sa_sac2 * P.sa_sac2 * omega + P.sa_sac3 * sBar);
+        double term2 = (P.sa_sac3 - 2 * P.sa_sac2) * omega - sBar;
+        stdv = omega + omega * term1 / term2;
+    }
+    double ostd = 1.0 / (stdv + SMALLD);
+    double rr = fmin(rs * ostd, 10.0);
+    double r5 = pow(rr, 5.0);
+    double g = rr + P.sa_cw2 * (r5 * rr - rr);
+    double g6 = pow(g, 6.0);
+    double fw = g * pow((1.0 + P.sa_cw36) / (g6 + P.sa_cw36), 1.0 / 6.0);
+    double xsi2 = xsi * xsi;
+    double ft2 = P.ft2_flag ? P.sa_ct3 * exp(-P.sa_ct4 * xsi2) * 1.0 : 0.0;
+    double grd2 = SQR3(double(gnc[0]), double(gnc[1]), double(gnc[2]));
+    double prod = P.sa_cb1 * (1.0 - ft2) * stdv * nuet;
+    double diff = P.sa_cb2s * grd2 * P.oreynolds;
+    double dest = (P.sa_cw1k * fw - P.sa_cb1 * ft2) * nuetRs;
+    diff = fmin(P.rprod * prod, diff);
+    double srcTerm = prod - dest;
+    srcTerm += diff;
+    double q1x = fv1 / (xsi + SMALLD), q1y = 1.0 + xsi * fv1;
+    double dfv2dk = (3.0 * P.sa_cv13 * (q1x * q1x) - 1.0) / (q1y * q1y);
+    double dsdnu = P.oreynolds * P.sa_okarm2 * od2 * (fv2 + xsi * dfv2dk);
+    double dfwdg = fw / (g + SMALLD) * (1.0 - g6 / (g6 + P.sa_cw36));
+    double dgdr = 1.0 + P.sa_cw2 * (6.0 * r5 - 1.0);
+    double drdnu = P.oreynolds * P.sa_okarm2 * od2 * ostd * (1.0 - nuet * ostd * dsdnu);
+    double dfwdnu = dfwdg * dgdr * drdnu;
+    double prod0 = P.sa_cb1 * (1.0 - ft2) * stdv;
+    double dest0 = (P.sa_cw1 * fw - P.sa_cb1 * ft2 * P.sa_okarm2) * nuet * od2 * P.oreynolds;
+    double prodp = P.sa_cb1 * ((1.0 - ft2) * dsdnu);
+    double destp = (P.sa_cw1 * (fw + dfwdnu * nuet) - P.sa_cb1 * ft2 * P.sa_okarm2) * od2 * P.oreynolds;
+    double prde0 = prod0 - dest0, prdep = prodp - destp;
+    double part1 = -half * (prde0 - fabs(prde0));
+    double part2 = -half * (prdep - fabs(prdep)) * nuet;
+    imp += (part1 + part2) * vol;
+    acc += srcTerm * vol;
+}
+
 template <typename R>
 __device__ __forceinline__ double turb_rhs_cell(const KArgs<R> &A, int c) {
     constexpr bool exactOrder = sizeof(R) == 8;
     const DevParams &P = A.P;
-    const double half = 0.5;
     int b = A.nb_off[c], en = A.nb_off[c + 1];
     R qc[REC], cgc[CGR], gnc[4];
     ld8(A.qs + (size_t)c * REC, qc);
@@ -279,85 +364,7 @@ __device__ __forceinline__ double turb_rhs_cell(const KArgs<R> &A, int c) {
                 else { if (!right) diffu -= flux; else diffu += flux; }
             }
         }
-        if (pass == 0 || !exactOrder) {
-            // ---- source term (per cell, after the spectrum) ----
-            double dudx, dudy, dudz, dvdx, dvdy, dvdz, dwdx, dwdy, dwdz;
-            {
-                R gq[GLR];
-#pragma unroll
-                for (int i = 0; i < 12; i += 4) ld4(A.gl + (size_t)c * GLR + i, gq + i);
-                dudx = gq[IU * 3]; dudy = gq[IU * 3 + 1]; dudz = gq[IU * 3 + 2];
-                dvdx = gq[IV * 3]; dvdy = gq[IV * 3 + 1]; dvdz = gq[IV * 3 + 2];
-                dwdx = gq[IW * 3]; dwdy = gq[IW * 3 + 1]; dwdz = gq[IW * 3 + 2];
-            }
-            double rho = A.q[(size_t)c * REC + IR], nuet = nutc, vlc = A.q[(size_t)c * REC + IML];
-            double olam = rho / (vlc + SMALLD);
-            double ls = A.walldist[c];
-            double od2 = 1.0 / (ls * ls);
-            double work1 = dudx + dvdy + dwdz;
-            double work2 = SQR3(dudx, dudy, dudz);
-            double work3 = SQR3(dudy + dvdx, dvdz + dwdy, dwdx + dudz);
-            double work4 = sqrt(SQR3(dwdy - dvdz, dudz - dwdx, dvdx - dudy));
-            if (P.iprod_sa == 1) {
-                double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
-                work4 = sqrt(fabs(stp));
-            } else if (P.iprod_sa == 4) {
-                double stp = 2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1;
-                double str = work4;
-                work4 = str - 2.0 * fmax(0.0, str - sqrt(fabs(stp)));
-            } else if (P.iprod_sa == 5) {
-                double stp = fabs(2.0 * work2 + work3 - (2.0 / 3.0) * work1 * work1);
-                double str = work4;
-                work4 = str * (1.0 - fmax(0.0, (str * str - stp) / (str * str + stp + SMALLD)));
-            }
-            double str = work4;
-            double xsi = nuet * olam + SMALLD;
-            double xsi3 = xsi * xsi * xsi;
-            double fv1 = xsi3 / (xsi3 + P.sa_cv13);
-            double fv2 = 1.0 - xsi / (1.0 + xsi * fv1);
-            double rs = nuet * P.sa_okarm2 * od2 * P.oreynolds;
-            double nuetRs = nuet * rs;
-            double sBar = rs * fv2;
-            double omega = str;
-            double stdv;
-            if (sBar >= -P.sa_sac2 * omega) stdv = omega + sBar;
-            else {
-                double term1 = (P.sa_sac2 * P.sa_sac2 * omega + P.sa_sac3 * sBar);
-                double term2 = (P.sa_sac3 - 2 * P.sa_sac2) * omega - sBar;
-                stdv = omega + omega * term1 / term2;
-            }
-            double ostd = 1.0 / (stdv + SMALLD);
-            double rr = fmin(rs * ostd, 10.0);
-            double r5 = pow(rr, 5.0);
-            double g = rr + P.sa_cw2 * (r5 * rr - rr);
-            double g6 = pow(g, 6.0);
-            double fw = g * pow((1.0 + P.sa_cw36) / (g6 + P.sa_cw36), 1.0 / 6.0);
-            double xsi2 = xsi * xsi;
-            double ft2 = P.ft2_flag ? P.sa_ct3 * exp(-P.sa_ct4 * xsi2) * 1.0 : 0.0;
-            double grd2 = SQR3(double(gnc[0]), double(gnc[1]), double(gnc[2]));
-            double prod = P.sa_cb1 * (1.0 - ft2) * stdv * nuet;
-            double diff = P.sa_cb2s * grd2 * P.oreynolds;
-            double dest = (P.sa_cw1k * fw - P.sa_cb1 * ft2) * nuetRs;
-            diff = fmin(P.rprod * prod, diff);
-            double srcTerm = prod - dest;
-            srcTerm += diff;
-            double q1x = fv1 / (xsi + SMALLD), q1y = 1.0 + xsi * fv1;
-            double dfv2dk = (3.0 * P.sa_cv13 * (q1x * q1x) - 1.0) / (q1y * q1y);
-            double dsdnu = P.oreynolds * P.sa_okarm2 * od2 * (fv2 + xsi * dfv2dk);
-            double dfwdg = fw / (g + SMALLD) * (1.0 - g6 / (g6 + P.sa_cw36));
-            double dgdr = 1.0 + P.sa_cw2 * (6.0 * r5 - 1.0);
-            double drdnu = P.oreynolds * P.sa_okarm2 * od2 * ostd * (1.0 - nuet * ostd * dsdnu);
-            double dfwdnu = dfwdg * dgdr * drdnu;
-            double prod0 = P.sa_cb1 * (1.0 - ft2) * stdv;
-            double dest0 = (P.sa_cw1 * fw - P.sa_cb1 * ft2 * P.sa_okarm2) * nuet * od2 * P.oreynolds;
-            double prodp = P.sa_cb1 * ((1.0 - ft2) * dsdnu);
-            double destp = (P.sa_cw1 * (fw + dfwdnu * nuet) - P.sa_cb1 * ft2 * P.sa_okarm2) * od2 * P.oreynolds;
-            double prde0 = prod0 - dest0, prdep = prodp - destp;
-            double part1 = -half * (prde0 - fabs(prde0));
-            double part2 = -half * (prdep - fabs(prdep)) * nuet;
-            imp += (part1 + part2) * vol;
-            acc += srcTerm * vol;
-        }
+        if (pass == 0 || !exactOrder) sa_source(A, c, nutc, vol, gnc, imp, acc);   // per cell, after the spectrum
     }
     if (!exactOrder) { acc += conv; acc += diffu; }
     A.impsrT[c] = imp;
@@ -374,6 +381,156 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_rhs(KArgs<R> A) 
     if (c < A.nCells) {
         double r = turb_rhs_cell(A, c);
         sq = r * r;
+    }
+    block_sum_to<1>(&sq, A.tpart + blockIdx.x);
+}
+
+// The mixed path's SA right-hand side in two passes, like its NS residual:
+// k_turb_face evaluates every face once (face order) -- the spectral radius
+// and the two LU-SGS coefficients (written to matL/matR), the first-order
+// convection and the VIS_TEST diffusion flux of nu~ -- in the face's own frame
+// (offsets from the face centre formed in FP64, the normal rounded from FP64),
+// leaving {radius, convection, diffusion} in the face record; k_turb_cell adds
+// each cell's face records in ascending face id, then its source, exactly as
+// the fused per-cell form adds them (radius into the diagonal face by face;
+// convection and diffusion in their own sums added after the source).
+// (templates on R = float only, so that they are compiled in the mixed path's
+// translation unit alone)
+template <typename R>
+__global__ void __launch_bounds__(128) k_turb_face(KArgs<R> A) {
+    static_assert(sizeof(R) == 4, "mixed path only");
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= A.nFaces) return;
+    const DevParams &P = A.P;
+    const int2 lr = __ldg(A.lr + f);
+    const bool bface = f < A.nBFaces;
+    double nD[4];
+    ld4(A.fgeoD + (size_t)f * FGR, nD);
+    float fo[FOFS];
+    ld8(A.fofs + (size_t)f * FOFS, fo);
+    const float xn = float(nD[0]), yn = float(nD[1]), zn = float(nD[2]), ar = float(nD[3]);
+    float ql[REC], qr[REC];
+    ld8(A.qs + (size_t)lr.x * REC, ql);
+    ld8(A.qs + (size_t)lr.y * REC, qr);
+    const float nl = float(A.nut[lr.x]), nr = float(A.nut[lr.y]);
+    const float voll = __ldg(A.cgeo + (size_t)lr.x * CGR + 3), volr = __ldg(A.cgeo + (size_t)lr.y * CGR + 3);
+    const float hf = 0.5f;
+    // ---- spectral radius and sweep coefficients ----
+    float r1 = 0.0f, m1 = 0.0f, m2 = 0.0f;
+    {
+        float vnl = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - 0.0f;
+        float vnr = xn * qr[IU] + yn * qr[IV] + zn * qr[IW] - 0.0f;
+        float absVn = fabsf(hf * (vnl + vnr));
+        r1 += ar * hf * absVn;
+        m1 += ar * hf * (-vnl - absVn);
+        m2 += ar * hf * (vnr - absVn);
+        float orl = 1.0f / (ql[IR] + small_v<float>()), orr = 1.0f / (qr[IR] + small_v<float>());
+        float nuet1 = ql[IML] * orl + nl, nuet2 = qr[IML] * orr + nr;
+        float nueff = fabsf(hf * (nuet1 + nuet2));
+        float ovol = 1.0f / (hf * (voll + volr));
+        float d = float(P.oreynolds) * ovol * (float(P.sa_osigma) * nueff * (ar * ar));
+        r1 += d;
+        m1 += -d;
+        m2 += -d;
+        A.matL[f] = double(m1);
+        A.matR[f] = double(m2);
+    }
+    // ---- first-order convection with the NS face states ----
+    double conv;
+    {
+        float t1 = nl, t2 = nr;
+        float u1 = ql[IU], v1 = ql[IV], w1 = ql[IW], u2 = qr[IU], v2 = qr[IV], w2 = qr[IW];
+        if (bface) {
+            float tm = hf * (nl + nr);
+            t1 = t2 = tm;
+            if (A.bcType[f] == BC_SOLID) {
+                const double *bq = A.bcq + (size_t)f * NEQ;
+                u1 = u2 = float(bq[IU]); v1 = v2 = float(bq[IV]); w1 = w2 = float(bq[IW]);
+            } else {
+                u1 = u2 = hf * (ql[IU] + qr[IU]);
+                v1 = v2 = hf * (ql[IV] + qr[IV]);
+                w1 = w2 = hf * (ql[IW] + qr[IW]);
+            }
+        }
+        float vnl = xn * u1 + yn * v1 + zn * w1 - 0.0f;
+        float vnr = xn * u2 + yn * v2 + zn * w2 - 0.0f;
+        float coef_l = hf * (vnl + fabsf(vnl)) * 1.0f;
+        float coef_r = hf * (vnr - fabsf(vnr)) * 1.0f;
+        conv = double(ar * (coef_l * t1 + coef_r * t2));
+    }
+    // ---- diffusion (VIS_TEST face gradient) ----
+    double diffu;
+    {
+        float q1 = nl, q2 = nr;
+        float q11 = q1, q22 = q2, qf = 0.5f * (q1 + q2);
+        // cell centres minus the face centre: -(x_f - x_L), -(x_f - x_R)
+        float dxl = -fo[0], dyl = -fo[1], dzl = -fo[2];
+        float dxr = -fo[3], dyr = -fo[4], dzr = -fo[5];
+        float d1 = xn * dxl + yn * dyl + zn * dzl;
+        float d2 = xn * dxr + yn * dyr + zn * dzr;
+        float angle1 = calc_angle(dxl, dyl, dzl, -d1);
+        float angle2 = calc_angle(dxr, dyr, dzr, d2);
+        float dqdn = 0.0f;
+        if (angle1 > 20.0f && angle2 > 20.0f) {
+            float g1[4], g2[4];
+            ld4(A.gnut + (size_t)lr.x * 4, g1);
+            if (bface) {   // a ghost cell carries its interior cell's gradient
+#pragma unroll
+                for (int i = 0; i < 4; ++i) g2[i] = g1[i];
+            } else {
+                ld4(A.gnut + (size_t)lr.y * 4, g2);
+            }
+            q11 += g1[0] * (xn * d1 - dxl) + g1[1] * (yn * d1 - dyl) + g1[2] * (zn * d1 - dzl);
+            q22 += g2[0] * (xn * d2 - dxr) + g2[1] * (yn * d2 - dyr) + g2[2] * (zn * d2 - dzr);
+            qf = 0.5f * (q1 + q2);
+        }
+        if (angle1 > 0.0f && angle2 > 0.0f && fabsf(d1) > small_v<float>() && fabsf(d2) > small_v<float>()) {
+            float dtmp = d1 * d1 + d2 * d2;
+            float c1 = d1 * d1 / dtmp, c2 = 1.0f - c1;
+            if (bface) { c1 = 1.0f; c2 = 0.0f; }
+            dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
+        }
+        float orl = 1.0f / (ql[IR] + small_v<float>()), orr = 1.0f / (qr[IR] + small_v<float>());
+        float visl_nv = hf * (ql[IML] * orl + qr[IML] * orr);
+        float vist_nv = hf * (nl + nr);
+        float comVis = (visl_nv + vist_nv) * float(P.sa_osigma);
+        diffu = double(-float(P.oreynolds) * comVis * dqdn * ar);
+    }
+    double *o = A.fout + (size_t)f * FOR;
+    reinterpret_cast<double2 *>(o)[0] = make_double2(double(r1), conv);
+    o[2] = diffu;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_cell(KArgs<R> A) {
+    static_assert(sizeof(R) == 4, "mixed path only");
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double sq = 0.0;
+    if (c < A.nCells) {
+        float cgc[CGR], gnc[4];
+        ld4(A.cgeo + (size_t)c * CGR, cgc);
+        ld4(A.gnut + (size_t)c * 4, gnc);
+        const double nutc = A.nut[c], vol = double(cgc[3]);
+        double imp = 0.0;
+        imp += (1.0 / (A.dt[c] * A.P.turb_cfl_ratio)) * vol;
+        double conv = 0.0, diffu = 0.0, acc = -0.0;
+        const int b = A.nb_off[c], en = A.nb_off[c + 1];
+        int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
+        for (int k = b; k < en; ++k) {
+            int2 e2 = e2n;
+            if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
+            const double *o = A.fout + (size_t)nb_face(e2) * FOR;
+            const double2 a = __ldg(reinterpret_cast<const double2 *>(o));
+            const double df = __ldg(o + 2);
+            imp += a.x;
+            if (!nb_right(e2)) { conv -= a.y; diffu -= df; } else { conv += a.y; diffu += df; }
+        }
+        sa_source(A, c, nutc, vol, gnc, imp, acc);
+        acc += conv;
+        acc += diffu;
+        A.impsrT[c] = imp;
+        A.resT[c] = acc;
+        sq = acc * acc;
     }
     block_sum_to<1>(&sq, A.tpart + blockIdx.x);
 }
