@@ -936,9 +936,10 @@ def config1_throughput(stream, steps: int = 200, warmup: int = 5):
         s.set_stream(stream.cuda_stream)
         s.init_flowfield()
         s.step(warmup)
+        tuning = s.autotune()     # the sweep schedule (persistent or level launches), and the mixed shapes
         ms = _timed_steps(s, stream, steps, flush)
         out[key] = {"value": mesh.n_cells * steps / (ms * 1e-3), "ms_per_step": ms / steps,
-                    "sweep_levels": list(s.sweep_levels())}
+                    "sweep_levels": list(s.sweep_levels()), "tuning": tuning}
         s.close()
     return out
 
