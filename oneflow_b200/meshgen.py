@@ -768,3 +768,62 @@ def swept_wing_hybrid(n_around: int = 256, n_hex: int = 30, hex_ratio: float = 1
                 nc, nb, bct, meta=dict(kind="swept_wing_hybrid", n_around=n, n_hex=n_hex, n_tet=n_tet,
                                        nz_wing=nz_wing, nz_tip=nz_tip, sweep_deg=sweep_deg, y1=y1,
                                        semi_span=semi))
+
+
+# ------------------------------------------------------------------------
+# lid-driven cavities for the incompressible solver
+# ------------------------------------------------------------------------
+def lid_cavity_2d(n: int = 64, jitter: float = 0.0, triangles: bool = False, seed: int = 20261206) -> Mesh:
+    """Unit square cavity of n x n quadrilaterals (or 2 n^2 triangles with an
+    alternating diagonal), interior nodes jittered by U(-jitter*h, jitter*h).
+    Every boundary face is SOLID_SURFACE; the lid (y = 1) faces carry
+    bc_name_id 1, the other walls 0 -- the region the wall-velocity data of
+    the incompressible solver refers to (lid_velocity)."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(0.0, 1.0, n + 1)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    interior = np.zeros(X.shape, bool)
+    interior[1:-1, 1:-1] = True
+    h = 1.0 / n
+    X = X + np.where(interior, rng.uniform(-jitter, jitter, X.shape) * h, 0.0)
+    Y = Y + np.where(interior, rng.uniform(-jitter, jitter, X.shape) * h, 0.0)
+    nid = lambda i, j: i * (n + 1) + j
+    cells = []
+    for i in range(n):
+        for j in range(n):
+            a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            if not triangles:
+                cells.append((a, b, c, d))
+            elif (i + j) % 2 == 0:
+                cells.append((a, b, c)); cells.append((a, c, d))
+            else:
+                cells.append((a, b, d)); cells.append((b, c, d))
+    x, y = X.ravel(), Y.ravel()
+    nodes, lc, rc, nb, bct = _faces_from_cells_2d(cells, lambda a, b: SOLID)
+    lid = ((y[nodes[:nb, 0]] > 1.0 - 1e-12) & (y[nodes[:nb, 1]] > 1.0 - 1e-12)).astype(np.int32)
+    nf = nodes.shape[0]
+    return Mesh(2, x, y, np.zeros_like(x), np.full(nf, 2, np.int32), nodes.ravel().astype(np.int32),
+                lc.astype(np.int32), rc.astype(np.int32), len(cells), nb, bct, bc_name_id=lid,
+                meta=dict(kind="lid_cavity_2d", n=n, jitter=jitter, triangles=triangles, seed=seed))
+
+
+def lid_cavity_3d(n: int = 24, jitter: float = 0.1, seed: int = 20261206) -> Mesh:
+    """Unit cube cavity of n^3 hexahedra (interior nodes jittered, so faces
+    are warped), every boundary face SOLID_SURFACE; the lid (y = 1) faces
+    carry bc_name_id 1, the other walls 0."""
+    m = bump_box_hexes(n, n, n, height=0.0, jitter=jitter, seed=seed)
+    nb = m.n_bfaces
+    fn = m.face_nodes.reshape(-1, 4)[:nb]
+    lid = np.all(m.y[fn] > 1.0 - 1e-12, axis=1).astype(np.int32)
+    m.bc_type = np.full(nb, SOLID, np.int32)
+    m.bc_name_id = lid
+    m.meta = dict(kind="lid_cavity_3d", n=n, jitter=jitter, seed=seed)
+    return m
+
+
+def lid_velocity(mesh: Mesh, u_lid: float = 1.0) -> np.ndarray:
+    """Per boundary face wall velocity [nBFaces, 3]: (u_lid, 0, 0) on the lid
+    (bc_name_id 1), zero elsewhere."""
+    w = np.zeros((mesh.n_bfaces, 3), np.float64)
+    w[np.asarray(mesh.bc_name_id) == 1, 0] = u_lid
+    return w

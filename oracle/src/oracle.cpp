@@ -285,7 +285,7 @@ struct Oracle {
     // ======================= reference state =======================
     // codes/chemical/src/Chemical.cpp:280-325, codes/ns/src/NsCom.cpp:45-94
     void initReference() {
-        statecoef = 1.0 / (p.gama_ref * p.mach_ref * p.mach_ref);
+        statecoef = 1.0 / (p.gama_ref * (p.mach_ref * p.mach_ref));   // gama_ref * SQR(mach_ref)
         pref = statecoef * 1.0 * 1.0 / 1.0;
         double aoa = p.aoa_degree * PI / 180.0, aos = p.sideslip_degree * PI / 180.0;
         inflow[IR] = 1.0;
@@ -1598,6 +1598,8 @@ struct Oracle {
     }
 };
 
+#include "oracle_ins.h"
+
 // ============================ C interface ============================
 extern "C" {
 
@@ -1707,6 +1709,46 @@ int oro_set_q(void *h, const double *qin) {
     return 0;
 }
 long oro_outer_steps(void *h) { return ((Oracle *)h)->outerSteps; }
+
+// ---- the incompressible solver on an oracle's mesh (oracle_ins.h) ----
+void *oro_ins_create(void *h) {
+    Oracle *o = (Oracle *)h;
+    InsOracle *s = new InsOracle(*o);
+    std::string why;
+    if (!s->supported(why)) { o->err = why; delete s; return nullptr; }
+    return s;
+}
+void oro_ins_destroy(void *s) { delete (InsOracle *)s; }
+// per boundary face u v w of the wall (the reference's ins_bc data)
+int oro_ins_set_wall(void *s, const double *uvw) {
+    InsOracle *n = (InsOracle *)s;
+    for (int f = 0; f < n->nB; ++f) { n->wu[f] = uvw[3 * f]; n->wv[f] = uvw[3 * f + 1]; n->ww[f] = uvw[3 * f + 2]; }
+    return 0;
+}
+int oro_ins_init(void *s) { ((InsOracle *)s)->init(); return 0; }
+// maxIter > 0: MG::Run's loop up to inner step maxIter; returns the steps run
+int oro_ins_run(void *s, int maxIter) { return ((InsOracle *)s)->run(maxIter); }
+// remax_up vp wp pp, then per solve (u v w p) GMRES iterations and residual
+int oro_ins_stats(void *s, double *out) {
+    InsOracle *n = (InsOracle *)s;
+    for (int k = 0; k < 4; ++k) { out[k] = n->remax[k]; out[4 + k] = n->linIts[k]; out[8 + k] = n->linRes[k]; }
+    out[12] = (double)n->innerSteps;
+    return 0;
+}
+int64_t oro_ins_field(void *s, const char *name, double *out) {
+    InsOracle *n = (InsOracle *)s;
+    std::string k(name);
+    const std::vector<double> *v = nullptr;
+    if (k == "uc") v = &n->uc; else if (k == "vc") v = &n->vc; else if (k == "wc") v = &n->wc;
+    else if (k == "pp") v = &n->pp; else if (k == "spc") v = &n->spc; else if (k == "spp") v = &n->spp;
+    else if (k == "bp") v = &n->bp; else if (k == "buc") v = &n->buc; else if (k == "bvc") v = &n->bvc;
+    else if (k == "fq") v = &n->fq; else if (k == "ajp") v = &n->ajp; else if (k == "ai0") v = &n->ai0;
+    else if (k == "ai1") v = &n->ai1; else if (k == "Fn") v = &n->Fn; else if (k == "dqqdx") v = &n->dqqdx;
+    else if (k == "uf") v = &n->uf; else if (k == "vf") v = &n->vf;
+    else return oro_field(&n->m, name, out);
+    if (out) std::copy(v->begin(), v->end(), out);
+    return (int64_t)v->size();
+}
 int oro_forces(void *h, double aref, double *out) {
     if (!h || !out || !(aref > 0.0)) return OFG_E_ARG;
     ((Oracle *)h)->forces(aref, out);

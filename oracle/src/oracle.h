@@ -16,6 +16,13 @@ int64_t oro_field(void *h, const char *name, double *out);
 int oro_set_q(void *h, const double *qin);
 long oro_outer_steps(void *h);
 int oro_forces(void *h, double aref, double *out);   /* out[13], see Oracle::forces */
+void *oro_ins_create(void *h);
+void oro_ins_destroy(void *s);
+int oro_ins_set_wall(void *s, const double *uvw);
+int oro_ins_init(void *s);
+int oro_ins_run(void *s, int maxIter);
+int oro_ins_stats(void *s, double *out);             /* out[13] */
+int64_t oro_ins_field(void *s, const char *name, double *out);
 #ifdef __cplusplus
 }
 #endif

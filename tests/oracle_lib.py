@@ -43,6 +43,15 @@ def _load():
     lib.oro_outer_steps.argtypes = [C.c_void_p]
     lib.oro_outer_steps.restype = C.c_long
     lib.oro_forces.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+    lib.oro_ins_create.restype = C.c_void_p
+    lib.oro_ins_create.argtypes = [C.c_void_p]
+    lib.oro_ins_destroy.argtypes = [C.c_void_p]
+    lib.oro_ins_set_wall.argtypes = [C.c_void_p, _dp]
+    lib.oro_ins_init.argtypes = [C.c_void_p]
+    lib.oro_ins_run.argtypes = [C.c_void_p, C.c_int]
+    lib.oro_ins_stats.argtypes = [C.c_void_p, _dp]
+    lib.oro_ins_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+    lib.oro_ins_field.restype = C.c_int64
     return lib
 
 
@@ -144,3 +153,79 @@ def run_ref(mesh: Mesh, params: P.OfgParams, steps: int, workdir: str = None, ke
     if not keep and workdir is None:
         shutil.rmtree(tmp, ignore_errors=True)
     return out
+
+
+class InsOracle:
+    """The incompressible SIMPLE solve of the reference (oracle_ins.h) on one
+    mesh whose boundary is all solid wall; ``wall`` [nBFaces, 3] is the wall
+    velocity of each boundary face."""
+
+    def __init__(self, mesh: Mesh, params: P.OfgParams, wall: np.ndarray):
+        self.base = Oracle(mesh, params)
+        self.L = self.base.L
+        self.nT = self.base.nT
+        self.h = self.L.oro_ins_create(self.base.h)
+        assert self.h, "mesh not supported by the incompressible oracle"
+        self.L.oro_ins_set_wall(self.h, np.ascontiguousarray(wall, np.float64).ravel())
+        self.L.oro_ins_init(self.h)
+
+    def __del__(self):
+        try:
+            self.L.oro_ins_destroy(self.h)
+        except Exception:
+            pass
+
+    def run(self, max_inner: int) -> int:
+        return self.L.oro_ins_run(self.h, max_inner)
+
+    def stats(self) -> dict:
+        o = np.zeros(13, np.float64)
+        self.L.oro_ins_stats(self.h, o)
+        return dict(remax=o[:4].copy(), gmres_iters=o[4:8].astype(int), gmres_res=o[8:12].copy(), inner=int(o[12]))
+
+    def field(self, name):
+        n = self.L.oro_ins_field(self.h, name.encode(), None)
+        assert n >= 0, name
+        out = np.empty(n, np.float64)
+        self.L.oro_ins_field(self.h, name.encode(), out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def q(self):
+        return self.field("q").reshape(5, self.nT)
+
+
+def run_ref_ins(mesh: Mesh, params: P.OfgParams, u_lid: float, steps: int, workdir: str = None):
+    """Run the reference's incompressible solver (INsSolver, startStrategy 2,
+    time_integral 3) for ``steps`` inner iterations on a cavity whose
+    bc_name_id 1 faces move at (u_lid, 0, 0) (grid/ins_bc.txt).  Returns the
+    dump dict and the printed remax lines (one [up, vp, wp, pp] per step)."""
+    tmp = workdir or tempfile.mkdtemp(prefix="ofgins_")
+    case = os.path.join(tmp, "case")
+    d = P.to_dict(params)
+    d["time_integral"] = 3
+    write_case(case, mesh, d, steps, start_strategy=2)
+    with open(os.path.join(case, "script", "solver.txt"), "w") as fh:
+        fh.write("INsSolver\n")
+    with open(os.path.join(case, "script", "cfd.txt"), "a") as fh:
+        fh.write(f"int maxIterSteps = {steps};\n")
+    with open(os.path.join(case, "grid", "ins_bc.txt"), "w") as fh:
+        fh.write(f"1 5 1.0 {u_lid!r} 0.0 0.0 0.0\n")
+    dump = os.path.join(tmp, "dump.bin")
+    env = dict(os.environ, OFG_REF_DUMP=dump)
+    r = subprocess.run([REF_EXE, "0", "case"], cwd=tmp, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                       timeout=3600)
+    out = r.stdout.decode(errors="replace")
+    if r.returncode != 0:
+        raise RuntimeError(out[-3000:])
+    rem, cur = [], {}
+    for line in out.splitlines():
+        if line.startswith("iinv.remax_"):
+            k, v = line[len("iinv.remax_"):].split(":")
+            cur[k] = float(v)
+            if k == "pp":
+                rem.append([cur.get("up"), cur.get("vp"), cur.get("wp"), cur.get("pp")])
+                cur = {}
+    res = read_ref_dump(dump), np.array(rem)
+    if workdir is None:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return res
