@@ -401,6 +401,71 @@ int ofg_set_tuning(ofg_ctx *ctx, const ofg_tuning *t);
    or OFG_E_CUDA. */
 int ofg_residual_rms_noalloc(const double *res, int64_t n_cells, int n_eq, double *rms_out, void *stream);
 
+/* ------------------------------------------------------------------------
+   Incompressible solver: the reference's INsSolver run with startStrategy 2
+   and time_integral 3 (TimeIntegral::Simple, codes/solver/src/TimeIntegral.cpp:132-138),
+   whose one task UPDATE_RESIDUALS (CINsUpdateResiduals -> INsCalcRHS,
+   codes/ins/src/INsRhs.cpp:105-132) is one SIMPLE inner iteration: upwind
+   mass-flux and viscous face coefficients, three momentum solves and one
+   pressure-correction solve by GMRES (codes/bgmres: Krylov dimension 500,
+   no restart, relative tolerance 1e-8, identity preconditioner), Rhie-Chow
+   face fluxes, pressure and velocity corrections (relaxation 0.8), and the
+   residual maxima remax_up/vp/wp/pp.  All arithmetic is FP64.
+
+   Scope (the reference's own): every boundary face SOLID_SURFACE -- its
+   MomPre and UpdateSpeed boundary loops index the last boundary-condition
+   region by boundary face id, in bounds only with a single boundary type
+   (codes/uins/src/UINsInvterm.cpp:617-626, 1622-1631) -- and a viscous model
+   (vismodel >= 1).  Wall velocities come per boundary face (the values its
+   region carries in the reference's grid/ins_bc.txt; zero without data).
+   The reference initialises its arrays on the inner step where
+   currTime == 0.001, i.e. with global_dt = 0.001 only; here the first inner
+   step after ofg_ins_init_flowfield does it for any global_dt.
+   ------------------------------------------------------------------------ */
+typedef struct ofg_ins ofg_ins;
+
+/* Creates the solver on a context that holds a mesh (ofg_upload_mesh; its
+   parameters give reynolds, mach_ref, aoa/sideslip and global_dt).
+   wall_uvw: [nBFaces][3] wall velocity of each boundary face, or NULL for
+   still walls.  Allocates (Krylov dimension + 2) x nTCell doubles of Krylov
+   basis besides the fields.  Returns OFG_E_ARG (and *out = NULL) when the
+   mesh or model is outside the scope above, OFG_E_STATE without a mesh,
+   OFG_E_NOMEM. */
+int ofg_ins_create(ofg_ctx *ctx, const double *wall_uvw, ofg_ins **out);
+void ofg_ins_destroy(ofg_ins *s);
+
+/* INIT_INSRESTART + INIT_FINAL (UINsRestart::InitinsRestart,
+   codes/uins/src/UINsRestart.cpp:50-62; INsInitFinal,
+   codes/ins/src/INsSolverImp.cpp:58-77): q = inflow in every cell, ghost
+   states of the adiabatic walls; resets the inner-step count. */
+int ofg_ins_init_flowfield(ofg_ins *s);
+
+/* UPDATE_RESIDUALS of the incompressible solver: one inner iteration. */
+int ofg_ins_update_residuals(ofg_ins *s);
+
+/* MG::Run with startStrategy 2 (codes/multigrid/src/Multigrid.cpp:111-147):
+   inner iterations while remax_up, remax_vp or remax_wp exceeds 1e-8 and
+   fewer than max_inner have run since ofg_ins_init_flowfield; *ran (may be
+   NULL) receives the number run by this call. */
+int ofg_ins_run(ofg_ins *s, int max_inner, int *ran);
+
+/* out[13]: remax_up, remax_vp, remax_wp, remax_pp of the last inner step;
+   GMRES iterations of its u, v, w and pressure solves; their final residual
+   norms (Rank.residual); the inner-step count. */
+int ofg_ins_stats(ofg_ins *s, double *out);
+
+/* Copies a field to host memory, reference layout: "q" [5][nTCell]
+   (rho u v w p), "dqdx" "dqdy" "dqdz" [5][nTCell] (Green-Gauss gradients
+   of u v w p; rho row zero), "pp" "uc" "vc" "wc" "spc" "bp" [nTCell],
+   "fq" "ajp" [nFaces].  n is the capacity of out in doubles; returns
+   OFG_E_SIZE when too small, OFG_E_ARG for an unknown name. */
+int ofg_ins_get_field(ofg_ins *s, const char *name, double *out, int64_t n);
+
+/* Device time (ms, CUDA events on the context's stream) of the inner
+   iterations run since ofg_ins_init_flowfield, and the GMRES iterations
+   they took in total (out[0], out[1]). */
+int ofg_ins_timing(ofg_ins *s, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,15 @@ def load_library() -> C.CDLL:
     L.ofg_get_tuning.argtypes = [C.c_void_p, C.POINTER(OfgTuning)]
     L.ofg_set_tuning.argtypes = [C.c_void_p, C.POINTER(OfgTuning)]
     L.ofg_version.restype = C.c_int
+    L.ofg_ins_create.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]
+    L.ofg_ins_destroy.argtypes = [C.c_void_p]
+    L.ofg_ins_destroy.restype = None
+    for name in ("ofg_ins_init_flowfield", "ofg_ins_update_residuals"):
+        getattr(L, name).argtypes = [C.c_void_p]
+    L.ofg_ins_run.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.ofg_ins_stats.argtypes = [C.c_void_p, _dp]
+    L.ofg_ins_timing.argtypes = [C.c_void_p, _dp]
+    L.ofg_ins_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]
     _LIB = L
     return L
 
@@ -334,3 +343,70 @@ def rcm_order(mesh: Mesh) -> np.ndarray:
     if rc != 0:
         raise OfgError(f"ofg_rcm_order failed ({rc})")
     return perm
+
+
+class Incompressible:
+    """The reference's incompressible solver (INsSolver with startStrategy 2
+    and the SIMPLE time integral) on one GPU: one inner iteration per
+    ``update_residuals`` (its UPDATE_RESIDUALS task), ``run`` for MG::Run's
+    inner loop.  ``params`` gives reynolds, mach_ref, the flow angles,
+    global_dt and the dimension; every boundary face must be a solid wall,
+    ``wall`` [nBFaces, 3] is the velocity of each (None: still walls)."""
+
+    def __init__(self, mesh: Mesh, params: P.OfgParams, wall: np.ndarray = None):
+        self.base = Solver(mesh, params)
+        self.L = self.base.L
+        self.mesh = mesh
+        self.nT = mesh.n_cells + mesh.n_bfaces
+        self._wall = None if wall is None else np.ascontiguousarray(wall, np.float64).reshape(mesh.n_bfaces, 3)
+        h = C.c_void_p()
+        wp = None if self._wall is None else self._wall.ctypes.data_as(C.c_void_p)
+        self.base._check(self.L.ofg_ins_create(self.base.h, wp, C.byref(h)))
+        self.h = h
+        self.init_flowfield()
+
+    def _check(self, rc):
+        self.base._check(rc)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ofg_ins_destroy(self.h)
+            self.h = None
+        self.base.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_flowfield(self):
+        self._check(self.L.ofg_ins_init_flowfield(self.h))
+
+    def update_residuals(self):
+        self._check(self.L.ofg_ins_update_residuals(self.h))
+
+    def run(self, max_inner: int) -> int:
+        n = C.c_int()
+        self._check(self.L.ofg_ins_run(self.h, max_inner, C.byref(n)))
+        return n.value
+
+    def stats(self) -> dict:
+        o = np.zeros(13, np.float64)
+        self._check(self.L.ofg_ins_stats(self.h, o))
+        return dict(remax=o[:4].copy(), gmres_iters=o[4:8].astype(int), gmres_res=o[8:12].copy(), inner=int(o[12]))
+
+    def timing(self) -> dict:
+        o = np.zeros(2, np.float64)
+        self._check(self.L.ofg_ins_timing(self.h, o))
+        return dict(ms=float(o[0]), gmres_iters=int(o[1]))
+
+    def field(self, name: str) -> np.ndarray:
+        n = 5 * self.nT if name in ("q", "dqdx", "dqdy", "dqdz") else (
+            self.mesh.n_faces if name in ("fq", "ajp") else self.nT)
+        out = np.empty(n, np.float64)
+        self._check(self.L.ofg_ins_get_field(self.h, name.encode(), out.ctypes.data_as(C.c_void_p), n))
+        return out
+
+    def q(self) -> np.ndarray:
+        return self.field("q").reshape(5, self.nT)

@@ -25,15 +25,20 @@ first-order Roe, LU-SGS, CFL 5, 2,000 outer iterations) as the reference ran
 it: every 16th interior cell of the final state, the per-equation sum and sum
 of squares of the whole interior state, the forces and the residual history
 (the whole state would be 2.6 MB).  bump2d_c1_converged.npz: the same case run for
-60,000 iterations, to the round-off floor of its residual (every 16th cell, forces,
+40,000 iterations, to a 4.6e-10 drop of its density residual (every 16th cell, forces,
 every 100th residual row, the final drop).
 
     python tests/golden/make_golden.py --restart-only   # only the restart fixtures
     python tests/golden/make_golden.py --walldist-only  # only the wall-distance fixtures
     python tests/golden/make_golden.py --c1-only        # only the benchmark-size bump (about 2 CPU minutes)
-    python tests/golden/make_golden.py --c1-converged-only  # the same bump run to its round-off floor
-                                                        # (60,000 iterations, about 55 CPU minutes)
-    python tests/golden/make_golden.py --case=<name>    # one case fixture"""
+    python tests/golden/make_golden.py --c1-converged-only  # the same bump run for 40,000 iterations
+                                                        # (about 45 CPU minutes)
+    python tests/golden/make_golden.py --case=<name>    # one case fixture
+    python tests/golden/make_golden.py --ins-only       # only the incompressible cavity fixtures
+
+ins_<case>.npz (INS_CASES): the incompressible solver on a lid-driven cavity,
+the reference's state q [5][nCells+nBFaces] and gradients after the case's
+inner iterations, and the remax_up/vp/wp/pp it printed per step (6 digits)."""
 import json
 import os
 import sys
@@ -46,9 +51,9 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 from oneflow_b200 import meshio, params as P  # noqa: E402
-from golden_cases import C1_STEPS, C1_STRIDE, CASES, RESTART_CASES, WALLDIST_CASES, build, build_c1, \
-    build_walldist  # noqa: E402
-from oracle_lib import run_ref  # noqa: E402
+from golden_cases import C1_STEPS, C1_STRIDE, CASES, INS_CASES, RESTART_CASES, WALLDIST_CASES, build, build_c1, \
+    build_ins, build_walldist  # noqa: E402
+from oracle_lib import run_ref, run_ref_ins  # noqa: E402
 
 
 def restart_fixtures():
@@ -93,7 +98,7 @@ def c1_fixture():
     print("bump2d_c1", mesh.n_cells, "cells", C1_STEPS, "steps")
 
 
-def c1_converged_fixture(steps: int = 60000):
+def c1_converged_fixture(steps: int = 40000):
     mesh, prm = build_c1()
     dump, rows = run_ref(mesh, prm, steps)
     q = dump["q"][:, :mesh.n_cells]
@@ -104,7 +109,19 @@ def c1_converged_fixture(steps: int = 60000):
     print("bump2d_c1_converged", mesh.n_cells, "cells", steps, "steps, drop", h[-1] / h[0])
 
 
+def ins_fixtures():
+    for name in INS_CASES:
+        mesh, prm, wall, steps = build_ins(name)
+        dump, rem = run_ref_ins(mesh, prm, 1.0, steps)
+        np.savez_compressed(os.path.join(HERE, f"ins_{name}.npz"), q=dump["q"], dqdx=dump["dqdx"], dqdy=dump["dqdy"],
+                            remax_printed=rem, steps=steps, params=json.dumps(P.to_dict(prm)))
+        print("ins", name, mesh.n_cells, "cells", steps, "inner steps")
+
+
 def main():
+    if "--ins-only" in sys.argv:
+        ins_fixtures()
+        return
     if "--c1-only" in sys.argv:
         c1_fixture()
         return

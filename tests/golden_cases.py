@@ -41,6 +41,33 @@ def build_c1():
     return meshgen.bump_channel(256, 128), P.euler_bump()
 
 
+# the incompressible solver (INsSolver, startStrategy 2, SIMPLE) on lid-driven
+# cavities (every boundary face a solid wall, the lid moving at u = 1):
+# tests/golden/ins_<name>.npz holds the reference's state after the given
+# number of inner iterations and the remax values it printed
+INS_CASES = {
+    "cavity2d_quad": dict(steps=10),
+    "cavity2d_tri_jitter": dict(steps=8),
+    "cavity3d_hex": dict(steps=4),
+}
+
+
+def build_ins(name):
+    """(mesh, params, wall velocity [nBFaces, 3], inner steps) of an incompressible case"""
+    if name == "cavity2d_quad":
+        mesh = meshgen.lid_cavity_2d(16)
+        prm = P.defaults(vismodel=1, reynolds=100.0, mach_ref=0.1)
+    elif name == "cavity2d_tri_jitter":
+        mesh = meshgen.lid_cavity_2d(12, jitter=0.2, triangles=True)
+        prm = P.defaults(vismodel=1, reynolds=400.0, mach_ref=0.1)
+    elif name == "cavity3d_hex":
+        mesh = meshgen.lid_cavity_3d(6, jitter=0.1)
+        prm = P.defaults(dimension=3, vismodel=1, reynolds=100.0, mach_ref=0.1)
+    else:
+        raise KeyError(name)
+    return mesh, prm, meshgen.lid_velocity(mesh, 1.0), INS_CASES[name]["steps"]
+
+
 # meshes whose wall distance the reference computed itself (ireadwdst = 0):
 # tests/golden/walldist_<name>.npz
 WALLDIST_CASES = ("plate2d_sa_roe", "plate3d_sa_roe", "hexbox_sa")
