@@ -422,6 +422,7 @@ def main():
     ap.add_argument("--no-c1", action="store_true", help="skip the benchmark-size 2-D bump")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuner)")
     ap.add_argument("--no-wing", action="store_true", help="skip the 8M-cell transonic swept wing")
+    ap.add_argument("--no-uins", action="store_true", help="skip the incompressible cavity")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -592,6 +593,9 @@ def main():
     wing = None
     if rank == 0 and world == 1 and not args.no_wing:
         wing = config3_wing(stream, args.ordering)
+    uins = None
+    if rank == 0 and world == 1 and not args.no_uins:
+        uins = uins_cavity()
     conv = None
     if rank == 0 and world == 1 and not args.no_converge:
         conv = time_to_drop("bump2d_small", 1e-8, stream)
@@ -612,7 +616,7 @@ def main():
                 "config": bench_config(desc, st, args.ordering, world, flush),
                 "sweep_levels": list(s.sweep_levels()), "tuning": tuning,
                 "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "pinned_variant": pinned,
-                "config1_bump2d": c1, "config3_wing": wing,
+                "config1_bump2d": c1, "config3_wing": wing, "uins_cavity": uins,
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": int(l1 - l0), "clocks": clocks, "time_to_1e-8": conv,
                 "setup": {"calc_wall_dist_s": wall_s, "wall_dist_vs_closed_form": wall_err},
@@ -941,6 +945,79 @@ def config1_throughput(stream, steps: int = 200, warmup: int = 5):
         out[key] = {"value": mesh.n_cells * steps / (ms * 1e-3), "ms_per_step": ms / steps,
                     "sweep_levels": list(s.sweep_levels()), "tuning": tuning}
         s.close()
+    return out
+
+
+def uins_cavity(n: int = 512, inner: int = 4, sample_n: int = 128, parity_n: int = 64, parity_inner: int = 3):
+    """The incompressible solver (the reference's INsSolver with the SIMPLE
+    time integral: momentum and pressure-correction GMRES solves, Krylov
+    dimension 500) on a lid-driven cavity (unit square, jittered quads, lid
+    at u = 1, Re 1000, dt 0.001).  GPU: inner iterations of an n x n cavity
+    from the initial state (device time by CUDA events, GMRES steps and their
+    roofline).  Same-mesh comparison on a sample_n x sample_n cavity: the GPU
+    against the reference CPU solver (oracle/_ref, one core; per inner
+    iteration = the difference of a 1- and a 2-iteration run).  Parity: the
+    GPU against the CPU restatement (bitwise the reference) after
+    parity_inner iterations of a parity_n x parity_n cavity."""
+    from oneflow_b200 import Incompressible
+    prm = P.defaults(vismodel=1, reynolds=1000.0, mach_ref=0.1)
+    out = {"workload": f"lid-driven cavity {n}x{n} quads (jitter 0.1), Re 1000, dt 0.001, FP64"}
+
+    def gpu_run(m, k):
+        g = Incompressible(m, prm, meshgen.lid_velocity(m))
+        g.run(2)                      # warm (first-step initialisation, allocations)
+        g.init_flowfield()
+        its = []
+        for _ in range(k):
+            g.update_residuals()
+            its.append([int(v) for v in g.stats()["gmres_iters"]])
+        t = g.timing()
+        return g, t, its
+
+    mesh = meshgen.lid_cavity_2d(n, jitter=0.1)
+    g, t, its = gpu_run(mesh, inner)
+    hbm = _peak_hbm()
+    gbs = t["gmres_bytes"] / (t["gmres_ms"] * 1e-3) / 1e9
+    out.update({"cells": mesh.n_cells, "inner_iterations": inner, "ms_per_inner": t["ms"] / inner,
+                "value": mesh.n_cells * inner / (t["ms"] * 1e-3), "unit": "cell-iter/s",
+                "gmres_iters_per_inner": its, "gmres_share_of_time": t["gmres_ms"] / t["ms"],
+                "krylov_steps_per_s": t["gmres_iters"] / (t["gmres_ms"] * 1e-3),
+                "roofline": {"bound": "hbm", "kernel": "k_gm_spmv_dots + k_gm_orth (GMRES)", "achieved": gbs,
+                             "peak": hbm["value"], "unit": "GB/s", "frac": gbs / hbm["value"],
+                             "peak_source": hbm["source"], "alg_bytes": t["gmres_bytes"]}})
+    g.close()
+    # same mesh, GPU and the reference CPU solver
+    sm = meshgen.lid_cavity_2d(sample_n, jitter=0.1)
+    gs, ts, _ = gpu_run(sm, 2)
+    gs.close()
+    cmp = {"mesh": f"{sample_n}x{sample_n} quads", "cells": sm.n_cells, "gpu_ms_per_inner": ts["ms"] / 2}
+    if os.path.exists(REF_EXE):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_lib import run_ref_ins
+        wall = []
+        for k in (1, 2):
+            t0 = time.perf_counter()
+            run_ref_ins(sm, prm, 1.0, k)
+            wall.append(time.perf_counter() - t0)
+        cpu_s = wall[1] - wall[0]
+        cmp.update({"reference_cpu_s_per_inner": cpu_s, "cores": 1, "kind": "reference",
+                    "gpu_speedup": cpu_s / (ts["ms"] / 2 * 1e-3)})
+    out["same_mesh_vs_reference"] = cmp
+    # parity against the restatement
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_lib import InsOracle
+    pm = meshgen.lid_cavity_2d(parity_n, jitter=0.1)
+    w = meshgen.lid_velocity(pm)
+    gp = Incompressible(pm, prm, w)
+    gp.run(parity_inner)
+    o = InsOracle(pm, prm, w)
+    o.run(parity_inner)
+    qg, qo = gp.q(), o.q()
+    out["parity"] = {"mesh": f"{parity_n}x{parity_n}", "inner": parity_inner,
+                     "q_max_rel_err": max(float(np.abs(qg[e] - qo[e]).max() / max(np.abs(qo[e]).max(), 1e-300))
+                                          for e in range(5)),
+                     "gmres_iters_equal": list(gp.stats()["gmres_iters"]) == list(o.stats()["gmres_iters"])}
+    gp.close()
     return out
 
 

@@ -440,6 +440,12 @@ void ofg_ins_destroy(ofg_ins *s);
    states of the adiabatic walls; resets the inner-step count. */
 int ofg_ins_init_flowfield(ofg_ins *s);
 
+/* Sets the state from host memory, q [5][nTCell] in the reference's layout
+   (ghost cells included, as its INIT_FINAL leaves them), and resets the
+   inner-step count as ofg_ins_init_flowfield does: the next inner step
+   takes its previous-time velocity and initial face fluxes from this q. */
+int ofg_ins_upload_state(ofg_ins *s, const double *q);
+
 /* UPDATE_RESIDUALS of the incompressible solver: one inner iteration. */
 int ofg_ins_update_residuals(ofg_ins *s);
 
@@ -461,9 +467,12 @@ int ofg_ins_stats(ofg_ins *s, double *out);
    OFG_E_SIZE when too small, OFG_E_ARG for an unknown name. */
 int ofg_ins_get_field(ofg_ins *s, const char *name, double *out, int64_t n);
 
-/* Device time (ms, CUDA events on the context's stream) of the inner
-   iterations run since ofg_ins_init_flowfield, and the GMRES iterations
-   they took in total (out[0], out[1]). */
+/* out[4]: device time (ms, CUDA events on the context's stream) of the
+   inner iterations run since ofg_ins_init_flowfield, the GMRES iterations
+   they took in total, the device time of those GMRES solves (ms), and the
+   solves' algorithmic bytes (per Krylov step j: matrix values, columns and
+   row offsets, the previous vector, the j earlier basis vectors read twice,
+   three vector writes; per update: the basis vectors read, x written). */
 int ofg_ins_timing(ofg_ins *s, double *out);
 
 #ifdef __cplusplus

@@ -678,13 +678,15 @@ struct ofg_ins {
     GmState *hst = nullptr;           // pinned host copy of the GMRES scalars
     double *hred = nullptr;           // pinned host copy of remax
     int nPart = 0, nChunkBlk = 0, nGrid = 0;
+    long long nnz = 0;
     long innerSteps = 0;
     double remax[4] = {1, 1, 1, 1};
     int linIts[4] = {0, 0, 0, 0};
     double linRes[4] = {0, 0, 0, 0};
-    double ms = 0.0;
+    double ms = 0.0, gmresMs = 0.0;
     long gmresTotal = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double gmresBytes = 0.0;   // algorithmic bytes of the Krylov steps run (see gmres())
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, eg0 = nullptr, eg1 = nullptr;
 
     int fail(int code, const std::string &m) { c->err = "ins: " + m; return code; }
     template <typename T> int alloc(T **p, size_t n) {
@@ -712,6 +714,7 @@ int gmres(ofg_ins *s, const double *A, const double *b, double *x, int *its, dou
     G.nT = s->D.nT; G.rOff = s->D.rOff; G.JA = s->D.JA; G.A = A; G.b = b; G.x = x;
     G.V = s->V; G.W = s->W; G.Y = s->Y; G.H = s->H; G.gc = s->gc; G.gs = s->gs; G.s = s->s; G.part = s->gpart;
     G.st = s->st;
+    INS_CK(cudaEventRecord(s->eg0, st));
     INS_CK(cudaMemsetAsync(s->H, 0, sizeof(double) * (size_t)(kKrylov + 1) * kKrylov, st));
     INS_CK(cudaMemsetAsync(s->s, 0, sizeof(double) * (kKrylov + 1), st));
     INS_CK(cudaMemsetAsync(&s->st->ticket, 0, sizeof(unsigned int), st));
@@ -735,9 +738,22 @@ int gmres(ofg_ins *s, const double *A, const double *b, double *x, int *its, dou
         INS_CK(cudaMemcpyAsync(s->hst, s->st, sizeof(GmState), cudaMemcpyDeviceToHost, st));
         INS_CK(cudaStreamSynchronize(st));
     }
+    INS_CK(cudaEventRecord(s->eg1, st));
+    INS_CK(cudaEventSynchronize(s->eg1));
+    float ms = 0.f;
+    INS_CK(cudaEventElapsedTime(&ms, s->eg0, s->eg1));
+    s->gmresMs += ms;
     *its = s->hst->dim >= 0 ? s->hst->iters : 0;
     *res = s->hst->res;
     s->gmresTotal += *its;
+    // algorithmic bytes: Krylov step j reads the matrix (values, columns,
+    // row offsets), the previous vector, the j earlier basis vectors twice
+    // (products, subtraction) and writes v_j, A v_j and the next vector; the
+    // update reads dim + 1 basis vectors and writes x
+    const double T = (double)s->D.nT, nnz = (double)s->nnz;
+    const int steps = s->hst->dim >= 0 ? s->hst->dim + 1 : 0;
+    for (int j = 0; j < steps; ++j) s->gmresBytes += nnz * 12.0 + T * 4.0 + T * 8.0 * (2.0 * j + 6.0);
+    if (steps) s->gmresBytes += T * 8.0 * (steps + 1);
     return OFG_OK;
 }
 
@@ -781,8 +797,8 @@ void release(ofg_ins *s) {
     s->allocs.clear();
     if (s->hst) cudaFreeHost(s->hst);
     if (s->hred) cudaFreeHost(s->hred);
-    if (s->ev0) cudaEventDestroy(s->ev0);
-    if (s->ev1) cudaEventDestroy(s->ev1);
+    for (cudaEvent_t e : {s->ev0, s->ev1, s->eg0, s->eg1})
+        if (e) cudaEventDestroy(e);
 }
 
 }  // namespace
@@ -893,7 +909,10 @@ int ofg_ins_create(ofg_ctx *c, const double *wall_uvw, ofg_ins **out) {
     if (!rc) rc = s->alloc(&s->st, 1);
     if (!rc && cudaMallocHost((void **)&s->hst, sizeof(GmState)) != cudaSuccess) rc = OFG_E_NOMEM;
     if (!rc && cudaMallocHost((void **)&s->hred, 4 * sizeof(double)) != cudaSuccess) rc = OFG_E_NOMEM;
-    if (!rc && (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess)) rc = OFG_E_CUDA;
+    if (!rc && (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess ||
+                cudaEventCreate(&s->eg0) != cudaSuccess || cudaEventCreate(&s->eg1) != cudaSuccess))
+        rc = OFG_E_CUDA;
+    s->nnz = rOff[nT];
     if (!rc && (cudaMemset(D.ticket, 0, sizeof(unsigned)) != cudaSuccess ||
                 cudaMemset(s->st, 0, sizeof(GmState)) != cudaSuccess ||
                 cudaMemset(D.mu, 0, 3 * (size_t)nC * sizeof(double)) != cudaSuccess))
@@ -934,14 +953,22 @@ int ofg_ins_init_flowfield(ofg_ins *s) {
         for (int k = 0; k < 3; ++k)
             q[(size_t)(IU + k) * nT + r] = -q[(size_t)(IU + k) * nT + r] + 2.0 * wall[3 * f + k];
     }
-    INS_CK(cudaStreamSynchronize(c->stream));
-    INS_CK(cudaMemcpy(s->D.q, q.data(), q.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return ofg_ins_upload_state(s, q.data());
+}
+
+int ofg_ins_upload_state(ofg_ins *s, const double *q) {
+    if (!s || !q) return OFG_E_ARG;
+    const int nT = s->D.nT;
+    INS_CK(cudaStreamSynchronize(s->c->stream));
+    INS_CK(cudaMemcpy(s->D.q, q, (size_t)5 * nT * sizeof(double), cudaMemcpyHostToDevice));
     INS_CK(cudaMemset(s->D.mu, 0, 3 * (size_t)s->D.nC * sizeof(double)));
     INS_CK(cudaMemset(s->D.gx, 0, 5 * (size_t)nT * sizeof(double)));
     INS_CK(cudaMemset(s->D.gy, 0, 5 * (size_t)nT * sizeof(double)));
     INS_CK(cudaMemset(s->D.gz, 0, 5 * (size_t)nT * sizeof(double)));
     s->innerSteps = 0;
     s->ms = 0.0;
+    s->gmresMs = 0.0;
+    s->gmresBytes = 0.0;
     s->gmresTotal = 0;
     for (int k = 0; k < 4; ++k) { s->remax[k] = 1; s->linIts[k] = 0; s->linRes[k] = 0; }
     return OFG_OK;
@@ -983,6 +1010,8 @@ int ofg_ins_timing(ofg_ins *s, double *out) {
     if (!s || !out) return OFG_E_ARG;
     out[0] = s->ms;
     out[1] = (double)s->gmresTotal;
+    out[2] = s->gmresMs;
+    out[3] = s->gmresBytes;
     return OFG_OK;
 }
 

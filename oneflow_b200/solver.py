@@ -91,6 +91,7 @@ def load_library() -> C.CDLL:
     for name in ("ofg_ins_init_flowfield", "ofg_ins_update_residuals"):
         getattr(L, name).argtypes = [C.c_void_p]
     L.ofg_ins_run.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.ofg_ins_upload_state.argtypes = [C.c_void_p, _dp]
     L.ofg_ins_stats.argtypes = [C.c_void_p, _dp]
     L.ofg_ins_timing.argtypes = [C.c_void_p, _dp]
     L.ofg_ins_get_field.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_int64]
@@ -383,6 +384,9 @@ class Incompressible:
     def init_flowfield(self):
         self._check(self.L.ofg_ins_init_flowfield(self.h))
 
+    def upload_state(self, q: np.ndarray):
+        self._check(self.L.ofg_ins_upload_state(self.h, np.ascontiguousarray(q, np.float64).reshape(-1)))
+
     def update_residuals(self):
         self._check(self.L.ofg_ins_update_residuals(self.h))
 
@@ -397,9 +401,9 @@ class Incompressible:
         return dict(remax=o[:4].copy(), gmres_iters=o[4:8].astype(int), gmres_res=o[8:12].copy(), inner=int(o[12]))
 
     def timing(self) -> dict:
-        o = np.zeros(2, np.float64)
+        o = np.zeros(4, np.float64)
         self._check(self.L.ofg_ins_timing(self.h, o))
-        return dict(ms=float(o[0]), gmres_iters=int(o[1]))
+        return dict(ms=float(o[0]), gmres_iters=int(o[1]), gmres_ms=float(o[2]), gmres_bytes=float(o[3]))
 
     def field(self, name: str) -> np.ndarray:
         n = 5 * self.nT if name in ("q", "dqdx", "dqdy", "dqdz") else (

@@ -1,4 +1,6 @@
 // Drop-in adapter: the reference solver with its hot-path tasks on the GPU.
+// (The incompressible solver's UPDATE_RESIDUALS likewise, in its own task
+// table system/ins/function/funcMap.txt: OfgInsUpdateResiduals below.)
 //
 // Linked into a second build of the reference (oneflow_ref_ofg, see the
 // Makefile beside this file) whose task tables system/{ns,turb}/function/
@@ -36,8 +38,14 @@
 #include "SolverState.h"
 #include "UnsGrid.h"
 #include "Zone.h"
+#include "BcData.h"
+#include "INsBcSolver.h"
+#include "INsInvterm.h"
+#include "INsIdx.h"
+#include "HXMath.h"
 
 #include <cstdio>
+#include <iostream>
 #include <cstdlib>
 #include <string>
 #include <vector>
@@ -49,6 +57,7 @@ BeginNameSpace( ONEFLOW )
 namespace {
 
 ofg_ctx *g_ctx = nullptr;
+ofg_ins *g_ins = nullptr;
 bool g_turb = false;
 
 void Check( int rc, const char *what )
@@ -149,7 +158,9 @@ void Download( UnsGrid * grid, int tid, const char * name, const char * hostName
     Unflatten( buf, * f );
 }
 
-void CreateContext()
+// the context and the zone's mesh (nodes, face->node lists, lCells/rCells,
+// boundary codes, SA wall distance)
+void CreateMeshContext()
 {
     UnsGrid * grid = Zone::GetUnsGrid();
     ofg_params p;
@@ -174,6 +185,13 @@ void CreateContext()
     const double * wd = ( g_turb && (int)dist.size() >= nCells ) ? dist.data() : nullptr;
     Check( ofg_upload_mesh( g_ctx, nm->xN.size(), nm->xN.data(), nm->yN.data(), nm->zN.data(), nFaces, fnc.data(),
                             fn.data(), lc.data(), rc.data(), nCells, nBFaces, bc.data(), wd ), "ofg_upload_mesh" );
+}
+
+void CreateContext()
+{
+    CreateMeshContext();
+    UnsGrid * grid = Zone::GetUnsGrid();
+    int nCells = grid->nCells, nFaces = grid->faceTopo->faces.size();
     std::vector< double > buf;
     Flatten( * GetFieldPointer< MRField >( grid, "q" ), buf );
     Check( ofg_upload_state( g_ctx, OFG_NS_SOLVER, buf.data() ), "ofg_upload_state (NS)" );
@@ -288,6 +306,64 @@ void OfgCalcBoundary( StringField & data )
     Download( grid, tid, "visl", "visl" );
 }
 
+// UPDATE_RESIDUALS of the incompressible solver (system/ins/function/
+// funcMap.txt; CINsUpdateResiduals -> INsCalcRHS, codes/ins/src/INsRhs.cpp:105-132):
+// one inner SIMPLE iteration on the GPU.  The first call builds the solver
+// from the zone, the wall velocities of the ins_bc data (per boundary face,
+// through its bcNameId region, as UINsBcSolver::SetId reads them,
+// codes/uins/src/UINsBcSolver.cpp:64-81) and the state INIT_FINAL left in q.
+// Afterwards q and the gradients go back to the host fields, and the residual
+// maxima to iinv, whose remax_up/vp/wp MG::Run's inner loop tests
+// (codes/multigrid/src/Multigrid.cpp:132-141); they are printed as
+// UINsInvterm::UpdateINsRes prints them.
+void OfgInsUpdateResiduals( StringField & data )
+{
+    UnsGrid * grid = Zone::GetUnsGrid();
+    MRField * q = GetFieldPointer< MRField >( grid, "q" );
+    std::vector< double > buf;
+    if ( ! g_ins )
+    {
+        CreateMeshContext();
+        FaceTopo * ft = grid->faceTopo;
+        int nBFaces = (int)ft->GetNBFaces();
+        IntField & bcn = ft->bcManager->bcRecord->bcNameId;
+        std::vector< double > wall( 3 * (size_t)nBFaces, 0.0 );
+        for ( int f = 0; f < nBFaces; ++ f )
+        {
+            int id = bcn[ f ];
+            if ( id < 0 || id >= (int)ins_bc_data.r2d.size() ) continue;
+            int dd = ins_bc_data.r2d[ id ];
+            if ( dd == -1 ) continue;
+            for ( int k = 0; k < 3; ++ k ) wall[ 3 * f + k ] = ins_bc_data.dataList[ dd ][ IIDX::IIU + k ];
+        }
+        Check( ofg_ins_create( g_ctx, wall.data(), & g_ins ), "ofg_ins_create" );
+        Flatten( * q, buf );
+        Check( ofg_ins_upload_state( g_ins, buf.data() ), "ofg_ins_upload_state" );
+        std::fprintf( stderr, "oneflow_b200: incompressible inner iterations on the GPU (%d cells)\n", grid->nCells );
+    }
+    Check( ofg_ins_update_residuals( g_ins ), "ofg_ins_update_residuals" );
+    buf.resize( (size_t)q->GetNEqu() * ( * q )[ 0 ].size() );
+    Check( ofg_ins_get_field( g_ins, "q", buf.data(), (int64_t)buf.size() ), "ofg_ins_get_field q" );
+    Unflatten( buf, * q );
+    const char * g[ 3 ] = { "dqdx", "dqdy", "dqdz" };
+    for ( int d = 0; d < 3; ++ d )
+    {
+        MRField * f = GetFieldPointer< MRField >( grid, g[ d ] );
+        Check( ofg_ins_get_field( g_ins, g[ d ], buf.data(), (int64_t)buf.size() ), g[ d ] );
+        Unflatten( buf, * f );
+    }
+    double st[ 13 ];
+    Check( ofg_ins_stats( g_ins, st ), "ofg_ins_stats" );
+    iinv.remax_up = st[ 0 ];
+    iinv.remax_vp = st[ 1 ];
+    iinv.remax_wp = st[ 2 ];
+    iinv.remax_pp = st[ 3 ];
+    std::cout << "iinv.remax_up:" << iinv.remax_up << std::endl;
+    std::cout << "iinv.remax_vp:" << iinv.remax_vp << std::endl;
+    std::cout << "iinv.remax_wp:" << iinv.remax_wp << std::endl;
+    std::cout << "iinv.remax_pp:" << iinv.remax_pp << std::endl;
+}
+
 DEFINE_DATA_CLASS( OfgZeroDq );
 DEFINE_DATA_CLASS( OfgCalcTimeStep );
 DEFINE_DATA_CLASS( OfgLoadResiduals );
@@ -297,6 +373,7 @@ DEFINE_DATA_CLASS( OfgLowerSweep );
 DEFINE_DATA_CLASS( OfgUpperSweep );
 DEFINE_DATA_CLASS( OfgUpdateFlowField );
 DEFINE_DATA_CLASS( OfgCalcBoundary );
+DEFINE_DATA_CLASS( OfgInsUpdateResiduals );
 
 namespace {
 // registered at load time (HXClone::Register keeps a lazily created map)
@@ -313,6 +390,7 @@ struct OfgRegistrar
         REGISTER_DATA_CLASS( OfgUpperSweep );
         REGISTER_DATA_CLASS( OfgUpdateFlowField );
         REGISTER_DATA_CLASS( OfgCalcBoundary );
+        REGISTER_DATA_CLASS( OfgInsUpdateResiduals );
     }
 } g_registrar;
 }  // namespace

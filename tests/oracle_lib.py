@@ -194,11 +194,14 @@ class InsOracle:
         return self.field("q").reshape(5, self.nT)
 
 
-def run_ref_ins(mesh: Mesh, params: P.OfgParams, u_lid: float, steps: int, workdir: str = None):
+def run_ref_ins(mesh: Mesh, params: P.OfgParams, u_lid: float, steps: int, workdir: str = None, exe: str = None,
+                output: list = None):
     """Run the reference's incompressible solver (INsSolver, startStrategy 2,
     time_integral 3) for ``steps`` inner iterations on a cavity whose
     bc_name_id 1 faces move at (u_lid, 0, 0) (grid/ins_bc.txt).  Returns the
-    dump dict and the printed remax lines (one [up, vp, wp, pp] per step)."""
+    dump dict and the printed remax lines (one [up, vp, wp, pp] per step).
+    ``exe``: another build of the reference (the drop-in); ``output``: a list
+    that receives the run's printed output."""
     tmp = workdir or tempfile.mkdtemp(prefix="ofgins_")
     case = os.path.join(tmp, "case")
     d = P.to_dict(params)
@@ -212,9 +215,11 @@ def run_ref_ins(mesh: Mesh, params: P.OfgParams, u_lid: float, steps: int, workd
         fh.write(f"1 5 1.0 {u_lid!r} 0.0 0.0 0.0\n")
     dump = os.path.join(tmp, "dump.bin")
     env = dict(os.environ, OFG_REF_DUMP=dump)
-    r = subprocess.run([REF_EXE, "0", "case"], cwd=tmp, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
-                       timeout=3600)
+    r = subprocess.run([exe or REF_EXE, "0", "case"], cwd=tmp, env=env, stdout=subprocess.PIPE,
+                       stderr=subprocess.STDOUT, timeout=3600)
     out = r.stdout.decode(errors="replace")
+    if output is not None:
+        output.append(out)
     if r.returncode != 0:
         raise RuntimeError(out[-3000:])
     rem, cur = [], {}

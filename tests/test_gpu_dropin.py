@@ -67,3 +67,29 @@ def test_reference_regression_case_through_the_gpu_drop_in(case):
             assert bad is None, (case, fn, bad)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+@pytest.mark.parametrize("name", ["cavity2d_quad", "cavity3d_hex"])
+def test_incompressible_inner_iterations_through_the_gpu_drop_in(name):
+    # The reference's incompressible solver (INsSolver, SIMPLE) with its
+    # UPDATE_RESIDUALS task on the GPU (system/ins/function/funcMap.txt of the
+    # drop-in build -> OfgInsUpdateResiduals -> ofg_ins_update_residuals):
+    # the reference's own loop control, initialisation and output around it.
+    # Its final state matches the reference's stock run (the fixture) within
+    # 1e-9 of each field's magnitude, and every remax line matches the stock
+    # run's to its six printed digits (a last-digit flip allowed).
+    import numpy as np
+    from golden_cases import build_ins
+    from oracle_lib import run_ref_ins
+    if not os.path.exists(EXE):
+        pytest.skip("drop-in build absent (oracle/_ref/dropin: needs the reference sources at build time)")
+    mesh, prm, wall, steps = build_ins(name)
+    out = []
+    dump, rem = run_ref_ins(mesh, prm, 1.0, steps, exe=EXE, output=out)
+    assert "oneflow_b200: incompressible inner iterations on the GPU" in out[0]
+    gold = np.load(os.path.join(ROOT, "tests", "golden", f"ins_{name}.npz"))
+    for e in range(5):
+        scale = max(np.abs(gold["q"][e]).max(), 1e-300)
+        assert np.abs(dump["q"][e] - gold["q"][e]).max() / scale < 1e-9, e
+    assert rem.shape == gold["remax_printed"].shape
+    np.testing.assert_allclose(rem, gold["remax_printed"], rtol=6e-6, atol=0)
