@@ -48,7 +48,7 @@ constexpr double kSmall = 1.0e-40;   // SMALL of codes/basic/include/HXTypeBasic
 constexpr int kKrylov = 500;         // krylovDimension of SolveMRhs::BGMRES
 constexpr double kTol = 1.0e-8;      // its tolerance
 constexpr int kThreads = 256;
-constexpr int kChunk = 1024;         // rows per block of k_gm_spmv_dots
+constexpr int kChunk = kThreads;     // rows per block of k_gm_spmv_dots (one per thread)
 constexpr int kStepsPerSync = 8;     // Krylov steps launched between flag reads
 
 // face record [nFaces][kFR]
@@ -114,29 +114,34 @@ __global__ void k_ins_preflux(Dev D) {
 
 // Green-Gauss gradient with distance-weighted face values (UINsVisterm::
 // CalcPreandVisGrad, UINsVisterm.cpp:98-228; UINsInvterm::CalcPreGrad,
-// UINsInvterm.cpp:1984-2059): nv fields v[k] (stride nT) -> g*[k]; a ghost
+// UINsInvterm.cpp:1984-2059): NV fields v[k] (stride nT) -> g*[k]; a ghost
 // takes its interior cell's gradient (computed again here).  wsel 0: the
 // weights of the viscous gradient, 1: those with SMALL.
-__global__ void k_ins_grad(Dev D, const double *v, int nv, double *gx, double *gy, double *gz, int wsel) {
+template <int NV>
+__global__ void k_ins_grad(Dev D, const double *v, double *gx, double *gy, double *gz, int wsel) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= D.nT) return;
     const int nT = D.nT;
     const int cell = c < D.nC ? c : D.lc[c - D.nC];
-    double ax[4] = {0, 0, 0, 0}, ay[4] = {0, 0, 0, 0}, az[4] = {0, 0, 0, 0};
+    double ax[NV], ay[NV], az[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ax[i] = ay[i] = az[i] = 0.0;
     for (int k = D.cOff[cell]; k < D.cOff[cell + 1]; ++k) {
         const int e = D.cFace[k], f = e >> 1;
         const double *g = D.fr + (size_t)f * kFR;
         const int l = D.lc[f], r = D.rc[f];
         const double cl = g[wsel ? F_G1 : F_W1], cr = g[wsel ? F_G2 : F_W2];
         const double nxa = g[F_NXA], nya = g[F_NYA], nza = g[F_NZA];
-        for (int i = 0; i < nv; ++i) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
             double val = cl * v[i * nT + l] + cr * v[i * nT + r];
             if (!(e & 1)) { ax[i] += nxa * val; ay[i] += nya * val; az[i] += nza * val; }
             else { ax[i] += -nxa * val; ay[i] += -nya * val; az[i] += -nza * val; }
         }
     }
     const double ovol = 1.0 / D.vol[cell];
-    for (int i = 0; i < nv; ++i) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
         gx[i * nT + c] = ax[i] * ovol; gy[i * nT + c] = ay[i] * ovol; gz[i * nT + c] = az[i] * ovol;
     }
 }
@@ -421,10 +426,11 @@ __global__ void k_ins_residuals(Dev D) {
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (threadIdx.x < 4) {
+    if (wid < 4) {   // warp i adds quantity i over the blocks (lanes strided, then the warp tree)
         double v = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) v += ((volatile double *)D.part)[(size_t)b * 4 + threadIdx.x];
-        D.red[threadIdx.x] = sqrt(v);
+        for (unsigned b = lane; b < gridDim.x; b += 32) v += ((volatile double *)D.part)[(size_t)b * 4 + wid];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) D.red[wid] = sqrt(v);
     }
     if (threadIdx.x == 0) *D.ticket = 0;
 }
@@ -457,6 +463,16 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
     return t;   // valid in thread 0
 }
 
+// sum of n partial sums (stride `stride`) by the whole block, in a fixed
+// order (thread t adds t, t + blockDim, ...; then the block tree): the
+// result is valid in thread 0.  Only for the last block of a ticket
+// reduction: the partials are read through volatile loads.
+__device__ __forceinline__ double last_block_sum(const double *part, int n, int stride, double *sh) {
+    double v = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) v += ((volatile const double *)part)[(size_t)b * stride];
+    return block_sum(v, sh);
+}
+
 // |b|^2 per block (the initial residual is b: x starts at zero)
 __global__ void k_gm_init(Gm G) {
     __shared__ double sh[32];
@@ -475,10 +491,10 @@ __global__ void k_gm_init(Gm G) {
         last = atomicAdd(&G.st->ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
-    double sum = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) sum += ((volatile double *)G.part)[b];
+    const double sum = last_block_sum(G.part, gridDim.x, 1, sh);
+    if (threadIdx.x != 0) return;
     GmState *S = G.st;
     const double normr1 = sqrt(sum);
     double normRHS = normr1;
@@ -508,8 +524,8 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
     const int r0 = blockIdx.x * kChunk;
     const int nT = G.nT;
     double *Vj = G.V + (size_t)j * nT;
-    for (int t = threadIdx.x; t < kChunk; t += blockDim.x) {
-        const int i = r0 + t;
+    {
+        const int t = threadIdx.x, i = r0 + t;
         double y = 0.0;
         if (i < nT) {
             Vj[i] = G.W[i] * inv;
@@ -525,6 +541,7 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
         const double *Vr = G.V + (size_t)r * nT + r0;
         double d = 0.0;
         if (r < j) {
+#pragma unroll 4
             for (int t = lane; t < rows; t += 32) d += ys[t] * Vr[t];
         } else {
             for (int t = lane; t < rows; t += 32) d += ys[t] * (G.W[r0 + t] * inv);
@@ -538,10 +555,13 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
     __syncthreads();
     if (!last) return;
     __threadfence();
-    for (int r = threadIdx.x; r <= j; r += blockDim.x) {
+    // column j of H: one warp per r, lanes over the blocks' shares (fixed order)
+    const int nb = gridDim.x;
+    for (int r = wid; r <= j; r += nw) {
         double h = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) h += ((volatile double *)G.part)[(size_t)b * (kKrylov + 1) + r];
-        G.H[(size_t)r * kKrylov + j] = h;
+        for (int b = lane; b < nb; b += 32) h += ((volatile double *)G.part)[(size_t)b * (kKrylov + 1) + r];
+        for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+        if (lane == 0) G.H[(size_t)r * kKrylov + j] = h;
     }
     if (threadIdx.x == 0) S->ticket = 0;
 }
@@ -570,10 +590,10 @@ __global__ void __launch_bounds__(kThreads) k_gm_orth(Gm G) {
         last = atomicAdd(&S->ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
-    double sum = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) sum += ((volatile double *)G.part)[b];
+    const double sum = last_block_sum(G.part, gridDim.x, 1, sh);
+    if (threadIdx.x != 0) return;
     const double normr2 = sqrt(sum);
     double *H = G.H;
     auto h = [&](int a, int b) -> double & { return H[(size_t)a * kKrylov + b]; };
@@ -656,10 +676,10 @@ __global__ void k_gm_residual(Gm G) {
         last = atomicAdd(&G.st->ticket, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
-    double sum = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) sum += ((volatile double *)G.part)[b];
+    const double sum = last_block_sum(G.part, gridDim.x, 1, sh);
+    if (threadIdx.x != 0) return;
     G.st->res = sqrt(sum);
     G.st->ticket = 0;
 }
@@ -764,7 +784,7 @@ int inner(ofg_ins *s) {
     const bool first = s->innerSteps == 0;
     const int bF = blocks(D.nF), bT = blocks(D.nT), bB = blocks(D.nB > 0 ? D.nB : 1);
     if (first) k_ins_preflux<<<bF, kThreads, 0, st>>>(D);
-    k_ins_grad<<<bT, kThreads, 0, st>>>(D, D.q + IU * D.nT, 4, D.gx + IU * D.nT, D.gy + IU * D.nT, D.gz + IU * D.nT, 0);
+    k_ins_grad<4><<<bT, kThreads, 0, st>>>(D, D.q + IU * D.nT, D.gx + IU * D.nT, D.gy + IU * D.nT, D.gz + IU * D.nT, 0);
     k_ins_face_coef<<<bF, kThreads, 0, st>>>(D);
     k_ins_momentum_rows<<<bT, kThreads, 0, st>>>(D, first ? 1 : 0);
     INS_CK(cudaGetLastError());
@@ -780,7 +800,7 @@ int inner(ofg_ins *s) {
     INS_CK(cudaGetLastError());
     if ((rc = gmres(s, D.Ap, D.bp, D.pp, &s->linIts[3], &s->linRes[3]))) return rc;
     k_ins_p_update<<<bT, kThreads, 0, st>>>(D);
-    k_ins_grad<<<bT, kThreads, 0, st>>>(D, D.pp, 1, D.gq, D.gq + D.nT, D.gq + 2 * D.nT, 1);
+    k_ins_grad<1><<<bT, kThreads, 0, st>>>(D, D.pp, D.gq, D.gq + D.nT, D.gq + 2 * D.nT, 1);
     k_ins_speed<<<bT, kThreads, 0, st>>>(D);
     if (D.nF > D.nB) k_ins_face_update<<<blocks(D.nF - D.nB), kThreads, 0, st>>>(D);
     k_ins_residuals<<<bT, kThreads, 0, st>>>(D);
