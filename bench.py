@@ -115,13 +115,13 @@ def bench_config(desc: dict, st: dict, ordering: str, world: int, flush: bool) -
                 parallelism=f"replicas x{world}")
 
 
-# Algorithmic bytes per cell-iteration of the survey's measurement contract
+# Algorithmic bytes per cell-iteration of the agreed measurement contract
 # (every array of a phase counted once at its stored size, perfect neighbour
 # reuse; FP32 shadow state, gradients, limiter and geometry, FP64 residual,
 # increments and master state): tetrahedral RANS-SA plate with least-squares
 # gradients and Venkatakrishnan, F/N = 2.  The count in alg_bytes below is this
 # implementation's own (its FP64 state reads and face records included).
-SURVEY_CONTRACT = {"plate3d": 1296, "plate3d_small": 1296, "plate3d_sample": 1296}
+CONTRACT_BYTES = {"plate3d": 1296, "plate3d_small": 1296, "plate3d_sample": 1296}
 
 
 def mesh_stats(mesh: Mesh):
@@ -558,10 +558,10 @@ def main():
                 "avg_launch_ms": per_launch_ms,
                 "whole_step_achieved_gbs": working / (total_ms / args.steps * 1e-3) / 1e9,
                 "whole_step_frac": working / (total_ms / args.steps * 1e-3) / 1e9 / hbm["value"],
-                "survey_contract_bytes_per_cell": SURVEY_CONTRACT.get(args.config),
-                "whole_step_frac_survey_contract": (SURVEY_CONTRACT[args.config] * st["N"] /
+                "contract_bytes_per_cell": CONTRACT_BYTES.get(args.config),
+                "whole_step_frac_contract": (CONTRACT_BYTES[args.config] * st["N"] /
                                                     (total_ms / args.steps * 1e-3) / 1e9 / hbm["value"])
-                if args.config in SURVEY_CONTRACT else None,
+                if args.config in CONTRACT_BYTES else None,
                 "group_ms": grp_ms, "group_alg_bytes": abytes}
 
     # end to end through the C ABI with host buffers: every step uploads the
