@@ -101,6 +101,9 @@ void ReadParams( ofg_params & p )
     p.ft2_flag = Key< int >( "ft2_flag", p.ft2_flag );
     p.turb_ilim = Key< int >( "turb_ilim", p.turb_ilim );
     p.time_integral = Key< int >( "time_integral", p.time_integral );
+    // 3 (SIMPLE) is the incompressible solver's integrator, which has its own
+    // entry points; the context underneath it keeps the LU-SGS default
+    if ( p.time_integral == 3 ) p.time_integral = 2;
     p.vencat_coef = Key< Real >( "vencat_coef", p.vencat_coef );
     p.centropy1 = Key< Real >( "centropy1", p.centropy1 );
     p.centropy2 = Key< Real >( "centropy2", p.centropy2 );
