@@ -435,7 +435,7 @@ void ofg_destroy(ofg_ctx *c) {
     destroy_graphs(c);
     void *ptrs[] = {c->d_lcb, c->d_bct, c->d_nb_off, c->d_nbl, c->d_lo_off, c->d_lol, c->d_up_off, c->d_upl,
                     c->d_lowOrder, c->d_upOrder, c->d_key, c->d_fgeo, c->d_cgeo, c->d_wdist, c->d_wall, c->d_wallG,
-                    c->d_fgeoD, c->d_fofs, c->d_lr, c->d_fout, c->d_lowOff, c->d_upOff, c->d_lsqw, c->d_lsqm,
+                    c->d_fgeoD, c->d_fofs, c->d_lr, c->d_fout, c->d_lowOff, c->d_upOff,
                     c->d_q[0], c->d_q[1], c->d_qs[0], c->d_qs[1], c->d_res, c->d_dq, c->d_dt, c->d_invsr, c->d_vissr, c->d_rad,
                     c->d_bcq, c->d_partial, c->d_npart, c->d_tpart, c->d_red, c->d_redCount, c->d_stage, c->d_scal, c->d_hist, c->d_gl, c->d_mm, c->d_fix,
                     c->d_nut, c->d_dnut, c->d_resT, c->d_impsrT, c->d_matL, c->d_matR, c->d_thist, c->d_gnut};
@@ -589,41 +589,6 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
             lr[2 * (size_t)f] = l; lr[2 * (size_t)f + 1] = r;
         }
         if ((rc = upload(c, &c->d_fofs, fo.data(), fo.size()))) return rc;
-        // least squares (igrad 2): per face w (x_R - x_L), w = 1/|x_R - x_L|^2, and
-        // per cell the inverse of sum_faces w d d^T (ghosts included), all in FP64
-        // and rounded once
-        if (c->p.igrad == 2) {
-            std::vector<float> lw((size_t)nFaces * 4, 0.0f), lm((size_t)nCells * 8, 0.0f);
-            std::vector<double> a((size_t)nCells * 6, 0.0);
-            for (int f = 0; f < nFaces; ++f) {
-                int l = c->lc[f], r = c->rc[f];
-                double d[3] = {c->xcc[r] - c->xcc[l], c->ycc[r] - c->ycc[l], c->zcc[r] - c->zcc[l]};
-                double w = 1.0 / (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-                for (int k = 0; k < 3; ++k) lw[(size_t)f * 4 + k] = float(w * d[k]);
-                double t[6] = {w * d[0] * d[0], w * d[0] * d[1], w * d[0] * d[2], w * d[1] * d[1], w * d[1] * d[2],
-                               w * d[2] * d[2]};
-                for (int k = 0; k < 6; ++k) {
-                    a[(size_t)l * 6 + k] += t[k];
-                    if (f >= nBFaces) a[(size_t)r * 6 + k] += t[k];
-                }
-            }
-            for (int i = 0; i < nCells; ++i) {
-                const double *s = &a[(size_t)i * 6];
-                double a11 = s[0], a12 = s[1], a13 = s[2], a22 = s[3], a23 = s[4], a33 = s[5], m[6];
-                if (c->p.dimension == 2) {
-                    double id = 1.0 / (a11 * a22 - a12 * a12);
-                    m[0] = a22 * id; m[1] = -a12 * id; m[2] = 0.0; m[3] = a11 * id; m[4] = 0.0; m[5] = 0.0;
-                } else {
-                    double c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
-                    double c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
-                    double id = 1.0 / (a11 * c11 + a12 * c12 + a13 * c13);
-                    m[0] = c11 * id; m[1] = c12 * id; m[2] = c13 * id; m[3] = c22 * id; m[4] = c23 * id; m[5] = c33 * id;
-                }
-                for (int k = 0; k < 6; ++k) lm[(size_t)i * 8 + k] = float(m[k]);
-            }
-            if ((rc = upload(c, &c->d_lsqw, lw.data(), lw.size()))) return rc;
-            if ((rc = upload(c, &c->d_lsqm, lm.data(), lm.size()))) return rc;
-        }
         if ((rc = upload(c, &c->d_lr, lr.data(), lr.size()))) return rc;
         if ((rc = upload<double>(c, &c->d_fout, nullptr, (size_t)nFaces * FOR))) return rc;
     } else {
@@ -631,8 +596,7 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
         pack_geometry(c, fg, cg);
         if ((rc = upload_bytes(c, &c->d_fgeo, fg.data(), fg.size() * sizeof(double)))) return rc;
         if ((rc = upload_bytes(c, &c->d_cgeo, cg.data(), cg.size() * sizeof(double)))) return rc;
-        for (void **v : {(void **)&c->d_fgeoD, (void **)&c->d_fofs, (void **)&c->d_lr, (void **)&c->d_fout,
-                         (void **)&c->d_lsqw, (void **)&c->d_lsqm})
+        for (void **v : {(void **)&c->d_fgeoD, (void **)&c->d_fofs, (void **)&c->d_lr, (void **)&c->d_fout})
             if (*v) { cudaFree(*v); *v = nullptr; }
     }
     size_t nT = c->nT, N = nCells;

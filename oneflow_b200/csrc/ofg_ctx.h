@@ -39,7 +39,6 @@ struct ofg_ctx {
     float *d_fofs = nullptr;                                // mixed path: face-local offsets [F][FOFS]
     int *d_lr = nullptr;                                    // mixed path: {left, right} cell of each face
     double *d_fout = nullptr;                               // mixed path: face-pass results [F][FOR]
-    float *d_lsqw = nullptr, *d_lsqm = nullptr;             // mixed least squares: face weights, cell inverses
     double *d_wdist = nullptr;
     int nWall = 0;
     int *d_wall = nullptr;                                  // solid-wall faces {face, interior cell} (int2)

@@ -32,8 +32,6 @@ struct KArgs {
     const float *fofs;                     // [nFaces][8] x_f - x_L, x_f - x_R (formed in FP64), |x_f - x_L|, |x_f - x_R|
     const int2 *lr;                        // [nFaces] left cell, right cell (ghost nCells + f on boundary faces)
     double *fout;                          // [nFaces][FOR] face results of the face pass
-    const float *lsqw;                     // [nFaces][4] w (x_R - x_L), w = 1/|x_R - x_L|^2 (least squares, mixed)
-    const float *lsqm;                     // [nCells][8] the inverse least-squares matrix (6 entries, symmetric)
     const double *q;  double *qn;          // master state records [nT][REC], current / next
     const R *qs;      R *qsn;              // state records read by face kernels (== master in FP64)
     double *res, *dt, *invsr, *vissr, *rad, *bcq;   // rad: LU-SGS diagonal
@@ -324,47 +322,7 @@ __global__ void __launch_bounds__(128, MINB) k_gradlim(KArgs<R> A, int nvar, int
 #pragma unroll
         for (int e = 0; e < NEQ; ++e) mn[e] = mx[e] = mixed ? R(0) : qc[e];
         int b = A.nb_off[c], en = A.nb_off[c + 1];
-        if (mixed && A.P.igrad == 2) {
-            // weighted least squares with the geometry precomputed at upload
-            // (in FP64, rounded once): per face w (x_R - x_L), per cell the
-            // inverse of sum w d d^T; the loop only forms w d (q_nb - q_c)
-            R bb[6][3];
-#pragma unroll
-            for (int v = 0; v < 6; ++v) bb[v][0] = bb[v][1] = bb[v][2] = R(0);
-            int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
-            for (int k = b; k < en; ++k) {
-                int2 e2 = e2n;
-                if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
-                const int nb = e2.y;
-                double t[REC];
-                ld8(A.q + (size_t)nb * REC, t);
-                R dn[6];
-#pragma unroll
-                for (int v = 0; v < 6; ++v)   // the cell's own values re-read (L1 hits), not held
-                    dn[v] = R(t[v < 5 ? v : ITT] - __ldg(A.q + (size_t)c * REC + (v < 5 ? v : ITT)));
-                const float4 wd = __ldg(reinterpret_cast<const float4 *>(A.lsqw) + nb_face(e2));
-                const R sg = nb_right(e2) ? R(-1) : R(1);   // x_nb - x_c = -(x_R - x_L) seen from the right cell
-                const R wx = sg * wd.x, wy = sg * wd.y, wz = sg * wd.z;
-#pragma unroll
-                for (int v = 0; v < 6; ++v) {
-                    if (v >= nvar) break;
-                    bb[v][0] += wx * dn[v]; bb[v][1] += wy * dn[v]; bb[v][2] += wz * dn[v];
-                }
-                if (nb < A.nCells) {
-#pragma unroll
-                    for (int e = 0; e < NEQ; ++e) { mn[e] = Rmin(mn[e], dn[e]); mx[e] = Rmax(mx[e], dn[e]); }
-                }
-            }
-            float mf[8];
-            ld8(A.lsqm + (size_t)c * 8, mf);
-            const R m0 = mf[0], m1 = mf[1], m2 = mf[2], m3 = mf[3], m4 = mf[4], m5 = mf[5];
-#pragma unroll
-            for (int v = 0; v < 6; ++v) {
-                gx[v] = m0 * bb[v][0] + m1 * bb[v][1] + m2 * bb[v][2];
-                gy[v] = m1 * bb[v][0] + m3 * bb[v][1] + m4 * bb[v][2];
-                gz[v] = m2 * bb[v][0] + m4 * bb[v][1] + m5 * bb[v][2];
-            }
-        } else if (A.P.igrad == 2) {
+        if (A.P.igrad == 2) {
             // weighted least squares over face neighbours (ghosts included), w = 1/|d|^2
             R a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, bb[6][3];
 #pragma unroll

@@ -44,7 +44,6 @@ KArgs<R> make_args(ofg_ctx *c, bool onCurrent) {
     A.fgeo = static_cast<const R *>(c->d_fgeo); A.cgeo = static_cast<const R *>(c->d_cgeo);
     A.fgeoD = sizeof(R) == 8 ? static_cast<const double *>(c->d_fgeo) : c->d_fgeoD;
     A.fofs = c->d_fofs; A.lr = reinterpret_cast<const int2 *>(c->d_lr); A.fout = c->d_fout;
-    A.lsqw = c->d_lsqw; A.lsqm = c->d_lsqm;
     int nx = onCurrent ? c->cur : c->cur ^ 1;
     A.q = c->d_q[c->cur];
     A.qn = c->d_q[nx];
