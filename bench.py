@@ -164,10 +164,6 @@ def alg_bytes(st, prm) -> dict:
         # face records (Green-Gauss weights or the limiter's face centres);
         # the mixed path reads the face-local offsets instead of the centres
         gradlim += qm + cg + nbl + fg + gl + (F * 32 if mixed else 0)
-        if mixed and lsq:
-            # the least-squares geometry precomputed at upload: w (x_R - x_L)
-            # per face (16 B) and the inverse matrix per cell (32 B)
-            gradlim += F * 16 + N * 32
         if prm.ilim == 2 and not prm.venkat_kh3:
             gradlim += N * 10 * g + (gl + N * 10 * g + cg + nbl + fg + N * 5 * g)   # min/max, global eps pass
     out["gradlim"] = gradlim
