@@ -93,8 +93,7 @@ def _ref_procs(mesh) -> int:
 KERNEL_OF_GROUP = {"gradlim": "k_gradlim", "residual": "k_face_pass<0> (face fluxes + spectral radii, mixed path)",
                    "residual_sum": "k_face_sum<0> (per-cell sum of the face results, time step)",
                    "clip": "k_timestep_clip", "lusgs_lower": "k_lusgs_lower", "lusgs_upper": "k_lusgs_upper",
-                   "update": "k_update", "sa_residual": "k_turb_face + k_turb_cell (SA right-hand side)",
-                   "sa_grad": "k_turb_grad"}
+                   "update": "k_update", "sa_residual": "k_turb_rhs", "sa_grad": "k_turb_grad"}
 
 # DRAM bytes (read + write) per cell of one step's launches of a profile
 # group, from `ncu --section MemoryWorkloadAnalysis` of the 600,000-cell plate
@@ -192,18 +191,15 @@ def alg_bytes(st, prm) -> dict:
     out["boundary"] = B * (4 + 4 + 8 * g + 64 + 8 + 64 + 40) + (B * 8 * g if mixed else 0)
     out["norm"] = ((N + 127) // 128) * 40                        # per-block sums left by the residual kernel
     if sa:
-        grad_nut = NT * 8 + nbl + cg + (0 if lsq else fg) + N * 4 * g
-        if mixed:
-            # k_turb_face: cells, FP64 normal + area, face offsets, FP32 state
-            # records, nu~, volumes, grad nu~, wall states; writes the two
-            # sweep coefficients and the 24-B face record.  k_turb_cell: lists,
-            # face records, volume, grad nu~, nu~, dt, velocity gradients, the
-            # FP64 record (rho, mu_l), wall distance; writes diagonal, residual
-            rhs = (F * 8 + F * 32 + F * 32 + qs + NT * 8 + cg + N * 16 + B * 44 + F * 16 + F * 24) \
-                + (nbl + F * 24 + cg + N * 16 + N * 8 + N * 8 + N * 12 * g + N * 64 + N * 8 + N * 16 + N * 8 // 128)
-        else:
-            rhs = qs + cg + fg + nbl + NT * 8 + N * 4 * g + N * 12 * g + N * 16 + N * 8 + N * 8 + B * 44 \
-                + F * 16 + N * 16
+        # the mixed path reads the face-local offsets in place of cell centres
+        # (least squares, Green-Gauss weights)
+        grad_nut = NT * 8 + nbl + cg + (0 if lsq else fg) + N * 4 * g + (F * 32 if mixed else 0)
+        # k_turb_rhs: state records, centres, face records, lists, nu~, grad
+        # nu~, velocity gradients, dt, wall distance, wall states; writes the
+        # sweep coefficients, diagonal and residual (the mixed path also reads
+        # the face-local offsets of the diffusion term)
+        rhs = qs + cg + fg + nbl + NT * 8 + N * 4 * g + N * 12 * g + N * 16 + N * 8 + N * 8 + B * 44 \
+            + F * 16 + N * 16 + (F * 32 if mixed else 0)
         out["sa_grad"] = B * 24 + grad_nut
         out["sa_residual"] = rhs
         sa_sweep = half_lists + FI * 16 + N * 8 + N * 8 + N * 8 + N * 8 + N * 4

@@ -276,14 +276,7 @@ int launch_task(ofg_ctx *c, int task, cudaStream_t s) {
             if (c->nBFaces > 0) OFG_LAUNCH(k_turb_bc<R>, nblk(c->nBFaces, 256), 256, s, A, (const int *)c->d_lcb, 0);
             OFG_LAUNCH(k_turb_grad<R>, nblk(N, 128), 128, s, A);
         }
-        if (task != T_P_TURB_GRAD) {
-            if constexpr (sizeof(R) == 4) {   // face pass + per-cell sum (the face records reuse fout)
-                OFG_LAUNCH(k_turb_face<R>, nblk(c->nFaces, 128), 128, s, A);
-                OFG_LAUNCH(k_turb_cell<R>, nblk(N, 128), 128, s, A);
-            } else {
-                OFG_LAUNCH(k_turb_rhs<R>, nblk(N, 128), 128, s, A);
-            }
-        }
+        if (task != T_P_TURB_GRAD) OFG_LAUNCH(k_turb_rhs<R>, nblk(N, 128), 128, s, A);
         break;
     }
     case T_TURB_LOWER: {

@@ -85,7 +85,65 @@ __global__ void __launch_bounds__(128) k_turb_grad(KArgs<R> A) {
     R gx = 0, gy = 0, gz = 0;
     int b = A.nb_off[c], e = A.nb_off[c + 1];
     R vc = R(A.nut[c]);
-    if (A.P.igrad == 2) {
+    if constexpr (sizeof(R) == 4) {
+        // mixed path: the differences nu~_nb - nu~_c formed in FP64 and the
+        // face-local geometry (distances and least-squares terms formed in
+        // FP64 at upload), as the NS gradient of this path; absolute FP32
+        // coordinates lose the thin near-wall cells' offsets
+        const double nc = A.nut[c];
+        if (A.P.igrad == 2) {
+            R a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, b1 = 0, b2 = 0, b3 = 0;
+            for (int k = b; k < e; ++k) {
+                const int2 e2 = __ldg(&A.nbl[k]);
+                const R dv = R(A.nut[e2.y] - nc);
+                // x_nb - x_c = (x_f - x_c) - (x_f - x_nb), from the face's offsets
+                float fo[FOFS];
+                ld8(A.fofs + (size_t)nb_face(e2) * FOFS, fo);
+                const R sg = nb_right(e2) ? R(-1) : R(1);
+                const R dx = sg * (fo[0] - fo[3]), dy = sg * (fo[1] - fo[4]), dz = sg * (fo[2] - fo[5]);
+                const R w = R(1) / (dx * dx + dy * dy + dz * dz);
+                a11 += w * dx * dx; a12 += w * dx * dy; a13 += w * dx * dz;
+                a22 += w * dy * dy; a23 += w * dy * dz; a33 += w * dz * dz;
+                b1 += w * dx * dv; b2 += w * dy * dv; b3 += w * dz * dv;
+            }
+            if (A.P.dim == 2) {
+                R id = R(1) / (a11 * a22 - a12 * a12);
+                gx = (a22 * b1 - a12 * b2) * id; gy = (a11 * b2 - a12 * b1) * id; gz = R(0);
+            } else {
+                R c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
+                R c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
+                R id = R(1) / (a11 * c11 + a12 * c12 + a13 * c13);
+                gx = (c11 * b1 + c12 * b2 + c13 * b3) * id;
+                gy = (c12 * b1 + c22 * b2 + c23 * b3) * id;
+                gz = (c13 * b1 + c23 * b2 + c33 * b3) * id;
+            }
+        } else {
+            for (int k = b; k < e; ++k) {
+                const int2 e2 = __ldg(&A.nbl[k]);
+                const int f = nb_face(e2);
+                const bool right = nb_right(e2);
+                R fg[4];
+                ld4(A.fgeo + (size_t)f * FGR, fg);   // normal and area
+                R wn;
+                if (A.P.igrad == 1) {
+                    wn = R(0.5);
+                } else {   // |x_f - x_L|, |x_f - x_R| formed in FP64
+                    const float2 dd = __ldg(reinterpret_cast<const float2 *>(A.fofs + (size_t)f * FOFS + 6));
+                    const R delta = R(1) / (dd.x + dd.y + small_v<R>());
+                    wn = right ? dd.y * delta : dd.x * delta;
+                }
+                // the face value less the cell's own (which sums to zero over
+                // the closed cell surface)
+                const R value = wn * R(A.nut[e2.y] - nc);
+                const R ar = fg[3];
+                const R fx = fg[0] * ar, fy = fg[1] * ar, fz = fg[2] * ar;
+                if (!right) { gx += fx * value; gy += fy * value; gz += fz * value; }
+                else        { gx -= fx * value; gy -= fy * value; gz -= fz * value; }
+            }
+            const R ovol = R(1) / cgc[3];
+            gx *= ovol; gy *= ovol; gz *= ovol;
+        }
+    } else if (A.P.igrad == 2) {
         R a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, b1 = 0, b2 = 0, b3 = 0;
         for (int k = b; k < e; ++k) {
             int nb = __ldg(&A.nbl[k]).y;
@@ -332,8 +390,24 @@ __device__ __forceinline__ double turb_rhs_cell(const KArgs<R> &A, int c) {
                 R fxn = fg[0], fyn = fg[1], fzn = fg[2];
                 R q1 = nl, q2 = nr;
                 R q11 = q1, q22 = q2, qf = R(0.5) * (q1 + q2);
-                R dxl = cgl[0] - fg[4], dyl = cgl[1] - fg[5], dzl = cgl[2] - fg[6];
-                R dxr = cgr[0] - fg[4], dyr = cgr[1] - fg[5], dzr = cgr[2] - fg[6];
+                R dxl, dyl, dzl, dxr, dyr, dzr;
+                R e1, e2;   // FP32 path: q11 - qf and q22 - qf
+                if constexpr (exactOrder) {
+                    dxl = cgl[0] - fg[4]; dyl = cgl[1] - fg[5]; dzl = cgl[2] - fg[6];
+                    dxr = cgr[0] - fg[4]; dyr = cgr[1] - fg[5]; dzr = cgr[2] - fg[6];
+                } else {
+                    // the cell centres seen from the face centre, formed in FP64
+                    // (absolute FP32 coordinates lose thin cells' offsets), and
+                    // q - qf from the FP64 difference of nu~ (its FP32 values
+                    // would cancel where nu~ varies little)
+                    float fo[FOFS];
+                    ld8(A.fofs + (size_t)f * FOFS, fo);
+                    dxl = -fo[0]; dyl = -fo[1]; dzl = -fo[2];
+                    dxr = -fo[3]; dyr = -fo[4]; dzr = -fo[5];
+                    const double nlD = right ? A.nut[nb] : nutc, nrD = right ? nutc : A.nut[nb];
+                    e1 = R(0.5 * (nlD - nrD));
+                    e2 = -e1;
+                }
                 R d1 = fxn * dxl + fyn * dyl + fzn * dzl;
                 R d2 = fxn * dxr + fyn * dyr + fzn * dzr;
                 R angle1 = calc_angle(dxl, dyl, dzl, -d1);
@@ -345,15 +419,23 @@ __device__ __forceinline__ double turb_rhs_cell(const KArgs<R> &A, int c) {
                     if (!ghost) ld4(A.gnut + (size_t)nb * 4, gn);
                     const R *g1 = right ? gn : gnc;
                     const R *g2 = (right || ghost) ? gnc : gn;
-                    q11 += g1[0] * (fxn * d1 - dxl) + g1[1] * (fyn * d1 - dyl) + g1[2] * (fzn * d1 - dzl);
-                    q22 += g2[0] * (fxn * d2 - dxr) + g2[1] * (fyn * d2 - dyr) + g2[2] * (fzn * d2 - dzr);
-                    qf = R(0.5) * (q1 + q2);
+                    const R c1x = g1[0] * (fxn * d1 - dxl) + g1[1] * (fyn * d1 - dyl) + g1[2] * (fzn * d1 - dzl);
+                    const R c2x = g2[0] * (fxn * d2 - dxr) + g2[1] * (fyn * d2 - dyr) + g2[2] * (fzn * d2 - dzr);
+                    if constexpr (exactOrder) {
+                        q11 += c1x;
+                        q22 += c2x;
+                        qf = R(0.5) * (q1 + q2);
+                    } else {
+                        e1 += c1x;
+                        e2 += c2x;
+                    }
                 }
                 if (angle1 > R(0) && angle2 > R(0) && Rabs(d1) > small_v<R>() && Rabs(d2) > small_v<R>()) {
                     R dtmp = d1 * d1 + d2 * d2;
                     R c1 = d1 * d1 / dtmp, c2 = R(1) - c1;
                     if (f < A.nBFaces) { c1 = R(1); c2 = R(0); }
-                    dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
+                    if constexpr (exactOrder) dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
+                    else dqdn = c1 * (e1 / d1) + c2 * (e2 / d2);
                 }
                 R orl = R(1) / (ql[IR] + small_v<R>()), orr = R(1) / (qr[IR] + small_v<R>());
                 R visl_nv = hf * (ql[IML] * orl + qr[IML] * orr);
@@ -385,155 +467,6 @@ __global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_rhs(KArgs<R> A) 
     block_sum_to<1>(&sq, A.tpart + blockIdx.x);
 }
 
-// The mixed path's SA right-hand side in two passes, like its NS residual:
-// k_turb_face evaluates every face once (face order) -- the spectral radius
-// and the two LU-SGS coefficients (written to matL/matR), the first-order
-// convection and the VIS_TEST diffusion flux of nu~ -- in the face's own frame
-// (offsets from the face centre formed in FP64, the normal rounded from FP64),
-// leaving {radius, convection, diffusion} in the face record; k_turb_cell adds
-// each cell's face records in ascending face id, then its source, exactly as
-// the fused per-cell form adds them (radius into the diagonal face by face;
-// convection and diffusion in their own sums added after the source).
-// (templates on R = float only, so that they are compiled in the mixed path's
-// translation unit alone)
-template <typename R>
-__global__ void __launch_bounds__(128) k_turb_face(KArgs<R> A) {
-    static_assert(sizeof(R) == 4, "mixed path only");
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= A.nFaces) return;
-    const DevParams &P = A.P;
-    const int2 lr = __ldg(A.lr + f);
-    const bool bface = f < A.nBFaces;
-    double nD[4];
-    ld4(A.fgeoD + (size_t)f * FGR, nD);
-    float fo[FOFS];
-    ld8(A.fofs + (size_t)f * FOFS, fo);
-    const float xn = float(nD[0]), yn = float(nD[1]), zn = float(nD[2]), ar = float(nD[3]);
-    float ql[REC], qr[REC];
-    ld8(A.qs + (size_t)lr.x * REC, ql);
-    ld8(A.qs + (size_t)lr.y * REC, qr);
-    const float nl = float(A.nut[lr.x]), nr = float(A.nut[lr.y]);
-    const float voll = __ldg(A.cgeo + (size_t)lr.x * CGR + 3), volr = __ldg(A.cgeo + (size_t)lr.y * CGR + 3);
-    const float hf = 0.5f;
-    // ---- spectral radius and sweep coefficients ----
-    float r1 = 0.0f, m1 = 0.0f, m2 = 0.0f;
-    {
-        float vnl = xn * ql[IU] + yn * ql[IV] + zn * ql[IW] - 0.0f;
-        float vnr = xn * qr[IU] + yn * qr[IV] + zn * qr[IW] - 0.0f;
-        float absVn = fabsf(hf * (vnl + vnr));
-        r1 += ar * hf * absVn;
-        m1 += ar * hf * (-vnl - absVn);
-        m2 += ar * hf * (vnr - absVn);
-        float orl = 1.0f / (ql[IR] + small_v<float>()), orr = 1.0f / (qr[IR] + small_v<float>());
-        float nuet1 = ql[IML] * orl + nl, nuet2 = qr[IML] * orr + nr;
-        float nueff = fabsf(hf * (nuet1 + nuet2));
-        float ovol = 1.0f / (hf * (voll + volr));
-        float d = float(P.oreynolds) * ovol * (float(P.sa_osigma) * nueff * (ar * ar));
-        r1 += d;
-        m1 += -d;
-        m2 += -d;
-        A.matL[f] = double(m1);
-        A.matR[f] = double(m2);
-    }
-    // ---- first-order convection with the NS face states ----
-    double conv;
-    {
-        float t1 = nl, t2 = nr;
-        float u1 = ql[IU], v1 = ql[IV], w1 = ql[IW], u2 = qr[IU], v2 = qr[IV], w2 = qr[IW];
-        if (bface) {
-            float tm = hf * (nl + nr);
-            t1 = t2 = tm;
-            if (A.bcType[f] == BC_SOLID) {
-                const double *bq = A.bcq + (size_t)f * NEQ;
-                u1 = u2 = float(bq[IU]); v1 = v2 = float(bq[IV]); w1 = w2 = float(bq[IW]);
-            } else {
-                u1 = u2 = hf * (ql[IU] + qr[IU]);
-                v1 = v2 = hf * (ql[IV] + qr[IV]);
-                w1 = w2 = hf * (ql[IW] + qr[IW]);
-            }
-        }
-        float vnl = xn * u1 + yn * v1 + zn * w1 - 0.0f;
-        float vnr = xn * u2 + yn * v2 + zn * w2 - 0.0f;
-        float coef_l = hf * (vnl + fabsf(vnl)) * 1.0f;
-        float coef_r = hf * (vnr - fabsf(vnr)) * 1.0f;
-        conv = double(ar * (coef_l * t1 + coef_r * t2));
-    }
-    // ---- diffusion (VIS_TEST face gradient) ----
-    double diffu;
-    {
-        float q1 = nl, q2 = nr;
-        float q11 = q1, q22 = q2, qf = 0.5f * (q1 + q2);
-        // cell centres minus the face centre: -(x_f - x_L), -(x_f - x_R)
-        float dxl = -fo[0], dyl = -fo[1], dzl = -fo[2];
-        float dxr = -fo[3], dyr = -fo[4], dzr = -fo[5];
-        float d1 = xn * dxl + yn * dyl + zn * dzl;
-        float d2 = xn * dxr + yn * dyr + zn * dzr;
-        float angle1 = calc_angle(dxl, dyl, dzl, -d1);
-        float angle2 = calc_angle(dxr, dyr, dzr, d2);
-        float dqdn = 0.0f;
-        if (angle1 > 20.0f && angle2 > 20.0f) {
-            float g1[4], g2[4];
-            ld4(A.gnut + (size_t)lr.x * 4, g1);
-            if (bface) {   // a ghost cell carries its interior cell's gradient
-#pragma unroll
-                for (int i = 0; i < 4; ++i) g2[i] = g1[i];
-            } else {
-                ld4(A.gnut + (size_t)lr.y * 4, g2);
-            }
-            q11 += g1[0] * (xn * d1 - dxl) + g1[1] * (yn * d1 - dyl) + g1[2] * (zn * d1 - dzl);
-            q22 += g2[0] * (xn * d2 - dxr) + g2[1] * (yn * d2 - dyr) + g2[2] * (zn * d2 - dzr);
-            qf = 0.5f * (q1 + q2);
-        }
-        if (angle1 > 0.0f && angle2 > 0.0f && fabsf(d1) > small_v<float>() && fabsf(d2) > small_v<float>()) {
-            float dtmp = d1 * d1 + d2 * d2;
-            float c1 = d1 * d1 / dtmp, c2 = 1.0f - c1;
-            if (bface) { c1 = 1.0f; c2 = 0.0f; }
-            dqdn = c1 * ((q11 - qf) / d1) + c2 * ((q22 - qf) / d2);
-        }
-        float orl = 1.0f / (ql[IR] + small_v<float>()), orr = 1.0f / (qr[IR] + small_v<float>());
-        float visl_nv = hf * (ql[IML] * orl + qr[IML] * orr);
-        float vist_nv = hf * (nl + nr);
-        float comVis = (visl_nv + vist_nv) * float(P.sa_osigma);
-        diffu = double(-float(P.oreynolds) * comVis * dqdn * ar);
-    }
-    double *o = A.fout + (size_t)f * FOR;
-    reinterpret_cast<double2 *>(o)[0] = make_double2(double(r1), conv);
-    o[2] = diffu;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(128, MinBlocks<R>::tr) k_turb_cell(KArgs<R> A) {
-    static_assert(sizeof(R) == 4, "mixed path only");
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double sq = 0.0;
-    if (c < A.nCells) {
-        float cgc[CGR], gnc[4];
-        ld4(A.cgeo + (size_t)c * CGR, cgc);
-        ld4(A.gnut + (size_t)c * 4, gnc);
-        const double nutc = A.nut[c], vol = double(cgc[3]);
-        double imp = 0.0;
-        imp += (1.0 / (A.dt[c] * A.P.turb_cfl_ratio)) * vol;
-        double conv = 0.0, diffu = 0.0, acc = -0.0;
-        const int b = A.nb_off[c], en = A.nb_off[c + 1];
-        int2 e2n = b < en ? __ldg(&A.nbl[b]) : make_int2(0, 0);   // list entry one face ahead
-        for (int k = b; k < en; ++k) {
-            int2 e2 = e2n;
-            if (k + 1 < en) e2n = __ldg(&A.nbl[k + 1]);
-            const double *o = A.fout + (size_t)nb_face(e2) * FOR;
-            const double2 a = __ldg(reinterpret_cast<const double2 *>(o));
-            const double df = __ldg(o + 2);
-            imp += a.x;
-            if (!nb_right(e2)) { conv -= a.y; diffu -= df; } else { conv += a.y; diffu += df; }
-        }
-        sa_source(A, c, nutc, vol, gnc, imp, acc);
-        acc += conv;
-        acc += diffu;
-        A.impsrT[c] = imp;
-        A.resT[c] = acc;
-        sq = acc * acc;
-    }
-    block_sum_to<1>(&sq, A.tpart + blockIdx.x);
-}
 
 // LU-SGS sweeps of the SA equation (codes/uturb/src/UTurbLusgs.cpp:90-300,
 // codes/turb/src/TurbLusgs.cpp:123-260): dfj = matrix * dq_j
