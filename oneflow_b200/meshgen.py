@@ -807,17 +807,21 @@ def lid_cavity_2d(n: int = 64, jitter: float = 0.0, triangles: bool = False, see
                 meta=dict(kind="lid_cavity_2d", n=n, jitter=jitter, triangles=triangles, seed=seed))
 
 
-def lid_cavity_3d(n: int = 24, jitter: float = 0.1, seed: int = 20261206) -> Mesh:
+def lid_cavity_3d(n: int = 24, jitter: float = 0.1, prisms: bool = False, seed: int = 20261206) -> Mesh:
     """Unit cube cavity of n^3 hexahedra (interior nodes jittered, so faces
     are warped), every boundary face SOLID_SURFACE; the lid (y = 1) faces
-    carry bc_name_id 1, the other walls 0."""
-    m = bump_box_hexes(n, n, n, height=0.0, jitter=jitter, seed=seed)
+    carry bc_name_id 1, the other walls 0.  prisms: the columns of the upper
+    half in x split into two triangular prisms each (bump_box_mixed)."""
+    if prisms:
+        m = bump_box_mixed(n, n, n, height=0.0, jitter=jitter, seed=seed)
+    else:
+        m = bump_box_hexes(n, n, n, height=0.0, jitter=jitter, seed=seed)
     nb = m.n_bfaces
-    fn = m.face_nodes.reshape(-1, 4)[:nb]
-    lid = np.all(m.y[fn] > 1.0 - 1e-12, axis=1).astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(m.face_node_count)])
+    lid = np.array([np.all(m.y[m.face_nodes[off[f]:off[f + 1]]] > 1.0 - 1e-12) for f in range(nb)], np.int32)
     m.bc_type = np.full(nb, SOLID, np.int32)
     m.bc_name_id = lid
-    m.meta = dict(kind="lid_cavity_3d", n=n, jitter=jitter, seed=seed)
+    m.meta = dict(kind="lid_cavity_3d", n=n, jitter=jitter, prisms=prisms, seed=seed)
     return m
 
 

@@ -49,6 +49,7 @@ INS_CASES = {
     "cavity2d_quad": dict(steps=10),
     "cavity2d_tri_jitter": dict(steps=8),
     "cavity3d_hex": dict(steps=4),
+    "cavity3d_hex_prism": dict(steps=3),
 }
 
 
@@ -63,6 +64,9 @@ def build_ins(name):
     elif name == "cavity3d_hex":
         mesh = meshgen.lid_cavity_3d(6, jitter=0.1)
         prm = P.defaults(dimension=3, vismodel=1, reynolds=100.0, mach_ref=0.1)
+    elif name == "cavity3d_hex_prism":
+        mesh = meshgen.lid_cavity_3d(6, jitter=0.1, prisms=True)
+        prm = P.defaults(dimension=3, vismodel=1, reynolds=200.0, mach_ref=0.1)
     else:
         raise KeyError(name)
     return mesh, prm, meshgen.lid_velocity(mesh, 1.0), INS_CASES[name]["steps"]
