@@ -941,6 +941,26 @@ def config1_throughput(stream, steps: int = 200, warmup: int = 5):
         out[key] = {"value": mesh.n_cells * steps / (ms * 1e-3), "ms_per_step": ms / steps,
                     "sweep_levels": list(s.sweep_levels()), "tuning": tuning}
         s.close()
+    # parity at the config's own length: 2,000 iterations in the reference's
+    # cell order against the reference's run of the same case (the committed
+    # fixture tests/golden/bump2d_c1.npz: every 16th cell, forces)
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "bump2d_c1.npz"))
+    stride, n_it = 16, int(gold["steps"])
+    par = {"iterations": n_it, "against": "the reference CPU solver's run of the same mesh (every 16th cell, forces)"}
+    for key, prec in (("fp64", 0), ("mixed", 1)):
+        q = P.defaults(**P.to_dict(prm0))
+        q.precision = prec
+        q.sweep_order = 0
+        s = Solver(mesh, q)
+        s.set_stream(stream.cuda_stream)
+        s.init_flowfield()
+        s.step(n_it)
+        st = s.state()[:, :mesh.n_cells][:, ::stride]
+        f = s.forces(1.0)
+        par[key] = {"rho_l2": _rel_l2(st[0], gold["q_sub"][0]), "p_l2": _rel_l2(st[4], gold["q_sub"][4]),
+                    "forces_rel": _force_err(f, gold["forces"])}
+        s.close()
+    out["parity"] = par
     return out
 
 
