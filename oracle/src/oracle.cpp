@@ -1699,6 +1699,7 @@ int64_t oro_field(void *h, const char *name, double *out) {
     if (s == "turbdq") return put(&o->dnut, 1, nT);
     if (s == "turbimpsr") return put(&o->impsrT, 1, nT);
     if (s == "walldist") return put(&o->walldist, 1, nT);
+    if (s == "nfixes") { if (out) out[0] = double(o->nFixes); return 1; }
     return -1;
 }
 int oro_set_q(void *h, const double *qin) {

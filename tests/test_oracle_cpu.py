@@ -107,3 +107,21 @@ def test_oracle_first_order_bump_is_bitwise_reference():
     g = np.load(os.path.join(HERE, "golden", "bump_euler_roe1.npz"))
     o = Oracle(mesh, prm); o.init(); o.step(steps)
     assert np.array_equal(o.q(), g["q"])
+
+
+def test_oracle_positivity_fix_runs_on_a_violent_state():
+    # the state tests/test_gpu_solution_fix.py gives the GPU: the oracle's
+    # update repairs tens of cells per iteration and stays finite
+    mesh = meshgen.bump_channel(32, 16)
+    prm = P.euler_bump(cflst=5.0, cfled=5.0, ilim=-1)
+    o = Oracle(mesh, prm)
+    o.init()
+    q = o.q().copy()
+    rng = np.random.default_rng(7)
+    n = mesh.n_cells
+    q[1:4, :n] += rng.normal(0.0, 1.0, (3, n))
+    q[4, :n] *= rng.uniform(0.001, 1.0, n)
+    o.set_q(q)
+    o.step(3)
+    assert o.field("nfixes")[0] > 10
+    assert np.isfinite(o.q()).all()
