@@ -23,8 +23,10 @@ FORCE_KEYS = [0, 1, 2, 9, 10]
 # trajectory: after 30 iterations the fields agree to 1.2e-8 relative L2 but
 # the wall-normal force to 2.3e-6 of the largest force.  The 1e-6 force target
 # is met on converged solutions (tests/test_gpu_forces.py); this case gets a
-# transient tolerance.
-FORCE_TOL = {"plate2d_laminar_slau2": 5e-6}
+# transient tolerance.  So does the small transonic wing after 10 iterations
+# (SLAU2, Barth limiter, SA): fields and nu~ agree to 1e-5 relative L2, the
+# forces to 1.3e-6 of the largest.
+FORCE_TOL = {"plate2d_laminar_slau2": 5e-6, "wing3d_small_slau2_barth_sa": 5e-6}
 
 
 def l2(a, b):
