@@ -24,10 +24,10 @@
 //
 // GMRES on the device: per Krylov step two kernels.  k_gm_spmv_dots scales
 // the previous unnormalised vector on read, stores the new basis vector,
-// forms w = A v and, per 1024-row chunk, the chunk's share of every inner
-// product V[r] . w (one warp per r); the last block to finish (ticket
-// counter, no waiting) sums the shares into column j of the Hessenberg
-// matrix.  k_gm_orth subtracts the projections row by row in the reference's
+// forms w = A v and, per 256-row chunk, the chunk's share of every inner
+// product V[r] . w (one warp per r), summed per block in shared memory; the
+// last block to finish (ticket counter, no waiting) sums the blocks' shares
+// into column j of the Hessenberg matrix.  k_gm_orth subtracts the projections row by row in the reference's
 // order and sums |w|^2; its last block applies the earlier rotations and the
 // new one to column j, updates the rotated residual and decides convergence.
 // The host launches the steps in chunks and reads one flag per chunk; a step
@@ -513,53 +513,66 @@ __global__ void k_gm_init(Gm G) {
 }
 
 // one Krylov step, first half: v_j = W / |W| (stored), Y = A v_j, and the
-// inner products V[r] . Y, r <= j, into column j of H
+// inner products V[r] . Y, r <= j, into column j of H.  Each block walks its
+// 256-row chunks (grid stride), forms the chunk's rows of A v_j in shared
+// memory and adds the chunk's share of each product to its own sum in shared
+// memory (warp r % 8 owns r); its sums go out r-major, and the last block
+// (ticket counter, no waiting) adds the blocks' sums for each r with a warp
+// over the blocks -- a fixed order throughout.
 __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
     __shared__ double ys[kChunk];
+    __shared__ double acc[kKrylov + 1];
     __shared__ bool last;
     GmState *S = G.st;
     if (((volatile int *)&S->done)[0]) return;
     const int j = S->j;
     const double inv = S->inv;
-    const int r0 = blockIdx.x * kChunk;
     const int nT = G.nT;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     double *Vj = G.V + (size_t)j * nT;
-    {
-        const int t = threadIdx.x, i = r0 + t;
-        double y = 0.0;
-        if (i < nT) {
-            Vj[i] = G.W[i] * inv;
-            for (int k = G.rOff[i]; k < G.rOff[i + 1]; ++k) y += G.A[k] * (G.W[G.JA[k]] * inv);
-            G.Y[i] = y;
+    for (int r = threadIdx.x; r <= j; r += blockDim.x) acc[r] = 0.0;
+    const int nChunks = (nT + kChunk - 1) / kChunk;
+    for (int ch = blockIdx.x; ch < nChunks; ch += gridDim.x) {
+        const int r0 = ch * kChunk;
+        __syncthreads();   // ys of the previous chunk consumed
+        {
+            const int t = threadIdx.x, i = r0 + t;
+            double y = 0.0;
+            if (i < nT) {
+                Vj[i] = G.W[i] * inv;
+                for (int k = G.rOff[i]; k < G.rOff[i + 1]; ++k) y += G.A[k] * (G.W[G.JA[k]] * inv);
+                G.Y[i] = y;
+            }
+            ys[t] = y;
         }
-        ys[t] = y;
+        __syncthreads();
+        const int rows = min(kChunk, nT - r0);
+        for (int r = wid; r <= j; r += nw) {
+            const double *Vr = G.V + (size_t)r * nT + r0;
+            double d = 0.0;
+            if (r < j) {
+#pragma unroll 4
+                for (int t = lane; t < rows; t += 32) d += ys[t] * Vr[t];
+            } else {
+                for (int t = lane; t < rows; t += 32) d += ys[t] * (G.W[r0 + t] * inv);
+            }
+            for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+            if (lane == 0) acc[r] += d;
+        }
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int rows = min(kChunk, nT - r0);
-    for (int r = wid; r <= j; r += nw) {
-        const double *Vr = G.V + (size_t)r * nT + r0;
-        double d = 0.0;
-        if (r < j) {
-#pragma unroll 4
-            for (int t = lane; t < rows; t += 32) d += ys[t] * Vr[t];
-        } else {
-            for (int t = lane; t < rows; t += 32) d += ys[t] * (G.W[r0 + t] * inv);
-        }
-        for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
-        if (lane == 0) G.part[(size_t)blockIdx.x * (kKrylov + 1) + r] = d;
-    }
+    const int nb = gridDim.x;
+    for (int r = threadIdx.x; r <= j; r += blockDim.x) G.part[(size_t)r * nb + blockIdx.x] = acc[r];
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = atomicAdd(&S->ticket, 1u) == gridDim.x - 1;
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // column j of H: one warp per r, lanes over the blocks' shares (fixed order)
-    const int nb = gridDim.x;
+    // column j of H: one warp per r, lanes over the blocks' sums (fixed order)
     for (int r = wid; r <= j; r += nw) {
         double h = 0.0;
-        for (int b = lane; b < nb; b += 32) h += ((volatile double *)G.part)[(size_t)b * (kKrylov + 1) + r];
+        for (int b = lane; b < nb; b += 32) h += ((volatile double *)G.part)[(size_t)r * nb + b];
         for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
         if (lane == 0) G.H[(size_t)r * kKrylov + j] = h;
     }
@@ -579,6 +592,7 @@ __global__ void __launch_bounds__(kThreads) k_gm_orth(Gm G) {
     double v = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nT; i += gridDim.x * blockDim.x) {
         double w = G.Y[i];
+#pragma unroll 8
         for (int r = 0; r <= j; ++r) w = w - G.V[(size_t)r * nT + i] * G.H[(size_t)r * kKrylov + j];
         G.W[i] = w;
         v += w * w;
@@ -920,7 +934,7 @@ int ofg_ins_create(ofg_ctx *c, const double *wall_uvw, ofg_ins **out) {
     z(&D.Am, rOff[nT]); z(&D.Ap, rOff[nT]);
     z(&D.part, 4 * (size_t)blocks(nT)); z(&D.red, 4);
     if (!rc) rc = s->alloc(&D.ticket, 1);
-    s->nChunkBlk = (nT + kChunk - 1) / kChunk;
+    s->nChunkBlk = std::min((nT + kChunk - 1) / kChunk, 148 * 4);   // blocks of k_gm_spmv_dots (grid stride)
     s->nGrid = std::min(blocks(nT), 148 * 8);
     s->nPart = std::max(s->nChunkBlk * (kKrylov + 1), s->nGrid);
     z(&s->V, (size_t)(kKrylov + 1) * T); z(&s->W, T); z(&s->Y, T);
