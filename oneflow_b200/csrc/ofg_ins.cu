@@ -584,16 +584,19 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
 // the Givens rotations of column j, the rotated residual and the decision
 __global__ void __launch_bounds__(kThreads) k_gm_orth(Gm G) {
     __shared__ double sh[32];
+    __shared__ double hcol[kKrylov + 1];
     __shared__ bool last;
     GmState *S = G.st;
     if (((volatile int *)&S->done)[0]) return;
     const int j = S->j;
     const int nT = G.nT;
+    for (int r = threadIdx.x; r <= j; r += blockDim.x) hcol[r] = G.H[(size_t)r * kKrylov + j];
+    __syncthreads();
     double v = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nT; i += gridDim.x * blockDim.x) {
         double w = G.Y[i];
 #pragma unroll 8
-        for (int r = 0; r <= j; ++r) w = w - G.V[(size_t)r * nT + i] * G.H[(size_t)r * kKrylov + j];
+        for (int r = 0; r <= j; ++r) w = w - G.V[(size_t)r * nT + i] * hcol[r];
         G.W[i] = w;
         v += w * w;
     }
