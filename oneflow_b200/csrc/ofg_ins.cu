@@ -547,17 +547,43 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
         }
         __syncthreads();
         const int rows = min(kChunk, nT - r0);
-        for (int r = wid; r <= j; r += nw) {
-            const double *Vr = G.V + (size_t)r * nT + r0;
-            double d = 0.0;
-            if (r < j) {
-#pragma unroll 4
-                for (int t = lane; t < rows; t += 32) d += ys[t] * Vr[t];
-            } else {
-                for (int t = lane; t < rows; t += 32) d += ys[t] * (G.W[r0 + t] * inv);
+        // this lane's rows of the chunk: lane, lane + 32, ... (kChunk / 32 of them)
+        constexpr int KR = kChunk / 32;
+        double yv[KR];
+#pragma unroll
+        for (int k = 0; k < KR; ++k) yv[k] = ys[lane + 32 * k];
+        // four products per pass of the warp (32 loads in flight per lane),
+        // each summed over the lane's rows in ascending order, then over the
+        // warp; warp w owns r = 4w..4w+3, 4w+32.. (the sums of one r stay in
+        // one warp)
+        for (int rb = 4 * wid; rb <= j; rb += 4 * nw) {
+            double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
+            const double *V0 = G.V + (size_t)rb * nT + r0;
+#pragma unroll
+            for (int k = 0; k < KR; ++k) {
+                const int t = lane + 32 * k;
+                if (t < rows) {
+                    const double y = yv[k];
+                    // basis vectors r < j are stored; v_j is W * inv (this step's)
+                    const double wj = G.W[r0 + t] * inv;
+                    d0 += y * (rb < j ? __ldg(V0 + t) : wj);
+                    if (rb + 1 <= j) d1 += y * (rb + 1 < j ? __ldg(V0 + nT + t) : wj);
+                    if (rb + 2 <= j) d2 += y * (rb + 2 < j ? __ldg(V0 + 2 * (size_t)nT + t) : wj);
+                    if (rb + 3 <= j) d3 += y * (rb + 3 < j ? __ldg(V0 + 3 * (size_t)nT + t) : wj);
+                }
             }
-            for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
-            if (lane == 0) acc[r] += d;
+            for (int o = 16; o > 0; o >>= 1) {
+                d0 += __shfl_down_sync(0xffffffffu, d0, o);
+                d1 += __shfl_down_sync(0xffffffffu, d1, o);
+                d2 += __shfl_down_sync(0xffffffffu, d2, o);
+                d3 += __shfl_down_sync(0xffffffffu, d3, o);
+            }
+            if (lane == 0) {
+                acc[rb] += d0;
+                if (rb + 1 <= j) acc[rb + 1] += d1;
+                if (rb + 2 <= j) acc[rb + 2] += d2;
+                if (rb + 3 <= j) acc[rb + 3] += d3;
+            }
         }
     }
     __syncthreads();
@@ -595,8 +621,17 @@ __global__ void __launch_bounds__(kThreads) k_gm_orth(Gm G) {
     double v = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nT; i += gridDim.x * blockDim.x) {
         double w = G.Y[i];
-#pragma unroll 8
-        for (int r = 0; r <= j; ++r) w = w - G.V[(size_t)r * nT + i] * hcol[r];
+        // in the reference's order r = 0..j; the basis entries of 16 steps
+        // are loaded together ahead of their subtractions
+        int r = 0;
+        for (; r + 16 <= j + 1; r += 16) {
+            double vv[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) vv[q] = __ldg(G.V + (size_t)(r + q) * nT + i);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) w = w - vv[q] * hcol[r + q];
+        }
+        for (; r <= j; ++r) w = w - __ldg(G.V + (size_t)r * nT + i) * hcol[r];
         G.W[i] = w;
         v += w * w;
     }
