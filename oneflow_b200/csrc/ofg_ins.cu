@@ -552,24 +552,40 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
         double yv[KR];
 #pragma unroll
         for (int k = 0; k < KR; ++k) yv[k] = ys[lane + 32 * k];
-        // four products per pass of the warp (32 loads in flight per lane),
-        // each summed over the lane's rows in ascending order, then over the
-        // warp; warp w owns r = 4w..4w+3, 4w+32.. (the sums of one r stay in
-        // one warp)
-        for (int rb = 4 * wid; rb <= j; rb += 4 * nw) {
-            double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
-            const double *V0 = G.V + (size_t)rb * nT + r0;
+        // v_j = W * inv for the lane's rows (this step's vector, not stored yet)
+        double wv[KR];
 #pragma unroll
-            for (int k = 0; k < KR; ++k) {
-                const int t = lane + 32 * k;
-                if (t < rows) {
-                    const double y = yv[k];
-                    // basis vectors r < j are stored; v_j is W * inv (this step's)
-                    const double wj = G.W[r0 + t] * inv;
-                    d0 += y * (rb < j ? __ldg(V0 + t) : wj);
-                    if (rb + 1 <= j) d1 += y * (rb + 1 < j ? __ldg(V0 + nT + t) : wj);
-                    if (rb + 2 <= j) d2 += y * (rb + 2 < j ? __ldg(V0 + 2 * (size_t)nT + t) : wj);
-                    if (rb + 3 <= j) d3 += y * (rb + 3 < j ? __ldg(V0 + 3 * (size_t)nT + t) : wj);
+        for (int k = 0; k < KR; ++k) wv[k] = lane + 32 * k < rows ? G.W[r0 + lane + 32 * k] * inv : 0.0;
+        // the stored basis vectors r < j, four per pass of the warp (32 loads
+        // in flight per lane), each summed over the lane's rows in ascending
+        // order, then over the warp; warp w owns r with (r / 4) % 8 == w
+        for (int rb = 4 * wid; rb < j; rb += 4 * nw) {
+            const double *V0 = G.V + (size_t)rb * nT + r0;
+            double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
+            if (rows == kChunk && rb + 4 <= j) {   // the common case: no guards
+                double a[KR], b[KR], c[KR], e[KR];
+#pragma unroll
+                for (int k = 0; k < KR; ++k) {
+                    const int t = lane + 32 * k;
+                    a[k] = __ldg(V0 + t);
+                    b[k] = __ldg(V0 + nT + t);
+                    c[k] = __ldg(V0 + 2 * (size_t)nT + t);
+                    e[k] = __ldg(V0 + 3 * (size_t)nT + t);
+                }
+#pragma unroll
+                for (int k = 0; k < KR; ++k) {
+                    d0 += yv[k] * a[k]; d1 += yv[k] * b[k]; d2 += yv[k] * c[k]; d3 += yv[k] * e[k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < KR; ++k) {
+                    const int t = lane + 32 * k;
+                    if (t < rows) {
+                        d0 += yv[k] * __ldg(V0 + t);
+                        if (rb + 1 < j) d1 += yv[k] * __ldg(V0 + nT + t);
+                        if (rb + 2 < j) d2 += yv[k] * __ldg(V0 + 2 * (size_t)nT + t);
+                        if (rb + 3 < j) d3 += yv[k] * __ldg(V0 + 3 * (size_t)nT + t);
+                    }
                 }
             }
             for (int o = 16; o > 0; o >>= 1) {
@@ -580,10 +596,19 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
             }
             if (lane == 0) {
                 acc[rb] += d0;
-                if (rb + 1 <= j) acc[rb + 1] += d1;
-                if (rb + 2 <= j) acc[rb + 2] += d2;
-                if (rb + 3 <= j) acc[rb + 3] += d3;
+                if (rb + 1 < j) acc[rb + 1] += d1;
+                if (rb + 2 < j) acc[rb + 2] += d2;
+                if (rb + 3 < j) acc[rb + 3] += d3;
             }
+        }
+        // r = j, by the warp that owns it
+        if (((j / 4) % nw) == wid) {
+            double d = 0.0;
+#pragma unroll
+            for (int k = 0; k < KR; ++k)
+                if (lane + 32 * k < rows) d += yv[k] * wv[k];
+            for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+            if (lane == 0) acc[j] += d;
         }
     }
     __syncthreads();
@@ -972,7 +997,7 @@ int ofg_ins_create(ofg_ctx *c, const double *wall_uvw, ofg_ins **out) {
     z(&D.Am, rOff[nT]); z(&D.Ap, rOff[nT]);
     z(&D.part, 4 * (size_t)blocks(nT)); z(&D.red, 4);
     if (!rc) rc = s->alloc(&D.ticket, 1);
-    s->nChunkBlk = std::min((nT + kChunk - 1) / kChunk, 148 * 4);   // blocks of k_gm_spmv_dots (grid stride)
+    s->nChunkBlk = std::min((nT + kChunk - 1) / kChunk, 148 * 3);   // blocks of k_gm_spmv_dots: one resident wave (grid stride)
     s->nGrid = std::min(blocks(nT), 148 * 8);
     s->nPart = std::max(s->nChunkBlk * (kKrylov + 1), s->nGrid);
     z(&s->V, (size_t)(kKrylov + 1) * T); z(&s->W, T); z(&s->Y, T);
