@@ -345,7 +345,9 @@ typedef struct ofg_tuning {
                                  per sweep, a single block running every level
                                  with a block barrier between levels (the same
                                  bits; for many small levels).  Both paths.   */
-    int    reserved[2];
+    int    grad_block;        /* gradients + limiter threads per block: 64 or 128
+                                 (default; 0 also means 128)                  */
+    int    reserved[1];
     double ms_default;        /* device ms per iteration of these kernels, default shapes */
     double ms_tuned;          /* the same with the shapes chosen                   */
 } ofg_tuning;

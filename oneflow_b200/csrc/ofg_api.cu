@@ -615,7 +615,8 @@ int ofg_upload_mesh(ofg_ctx *c, int nNodes, const double *xN, const double *yN, 
     if ((rc = upload<double>(c, &c->d_vissr, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_rad, nullptr, N))) return rc;
     if ((rc = upload<double>(c, &c->d_bcq, nullptr, (size_t)std::max(nBFaces, 1) * NEQ))) return rc;
-    c->nPartialMax = std::max<size_t>((N + 127) / 128 * 10, 2 * 148 * NEQ) + 16;
+    // (the gradient kernel's limiter extremes: 10 per block, blocks of 64 threads at the smallest)
+    c->nPartialMax = std::max<size_t>((N + 63) / 64 * 10, 2 * 148 * NEQ) + 16;
     if ((rc = upload<double>(c, &c->d_partial, nullptr, c->nPartialMax))) return rc;
     size_t nb128 = (N + 127) / 128;
     if ((rc = upload<double>(c, &c->d_npart, nullptr, nb128 * NEQ))) return rc;
@@ -1521,7 +1522,8 @@ int ofg_rcm_order(int nCells, int nFaces, int nBFaces, const int *lCells, const 
 static bool valid_tuning(const ofg_tuning &t) {
     auto in = [](int v, std::initializer_list<int> l) { for (int x : l) if (x == v) return true; return false; };
     return in(t.face_min_blocks, {2, 3, 4, 5}) && in(t.face_block, {64, 128}) && in(t.grad_min_blocks, {4, 6, 8}) &&
-           in(t.sweep_min_blocks, {6, 8, 10}) && in(t.sweep_block, {64, 128}) && in(t.sweep_persistent, {0, 1});
+           in(t.sweep_min_blocks, {6, 8, 10}) && in(t.sweep_block, {64, 128}) && in(t.sweep_persistent, {0, 1}) &&
+           in(t.grad_block, {0, 64, 128});
 }
 
 int ofg_get_tuning(ofg_ctx *c, ofg_tuning *out) {
@@ -1607,7 +1609,8 @@ int ofg_autotune(ofg_ctx *c, int reps, ofg_tuning *out) {
     if (mixed) {
         groups.push_back({&T.face_min_blocks, &T.face_block,
                           {{2, 128}, {3, 128}, {4, 128}, {5, 128}, {2, 64}, {3, 64}, {4, 64}, {5, 64}}, {T_P_FLUX}});
-        groups.push_back({&T.grad_min_blocks, nullptr, {{4, 0}, {6, 0}, {8, 0}}, {T_P_GRADLIM}});
+        groups.push_back({&T.grad_min_blocks, &T.grad_block,
+                          {{4, 128}, {6, 128}, {8, 128}, {4, 64}, {6, 64}, {8, 64}}, {T_P_GRADLIM}});
         groups.push_back({&T.sweep_min_blocks, &T.sweep_block,
                           {{6, 128}, {8, 128}, {10, 128}, {6, 64}, {8, 64}, {10, 64}}, {T_LOWER, T_UPPER}});
     }

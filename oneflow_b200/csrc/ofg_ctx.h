@@ -13,7 +13,7 @@ struct ofg_ctx {
     ofg_params p{};
     ofg::DevParams dp{};
     std::string err;
-    ofg_tuning tune{3, 128, 6, 8, 128, 0, {0, 0}, 0.0, 0.0};   // launch shapes of the gathers and sweeps
+    ofg_tuning tune{3, 128, 6, 8, 128, 0, 128, {0}, 0.0, 0.0};   // launch shapes of the gathers and sweeps
     unsigned long long meshHash = 0;                         // of the face->cell lists (autotuner cache key)
 
     // ---- mesh (host copies, reference numbering) ----

@@ -83,10 +83,12 @@ void launch_gradlim(ofg_ctx *c, const KArgs<R> &A, cudaStream_t s) {
     int limMode = (c->p.ilim == 1 || c->p.ilim == 2) ? (venkatGlobal ? 2 : 1) : 0;
     int nb = nblk(N, 128);
     if constexpr (sizeof(R) == 4) {
+        const int gb = c->tune.grad_block == 64 ? 64 : 128;   // the limiter's block extremes are exact either way
+        nb = nblk(N, gb);
         switch (c->tune.grad_min_blocks) {
-        case 4: OFG_LAUNCH((k_gradlim<R, 4>), nb, 128, s, A, nvar, limMode); break;
-        case 8: OFG_LAUNCH((k_gradlim<R, 8>), nb, 128, s, A, nvar, limMode); break;
-        default: OFG_LAUNCH((k_gradlim<R, 6>), nb, 128, s, A, nvar, limMode); break;
+        case 4: OFG_LAUNCH((k_gradlim<R, 4>), nb, gb, s, A, nvar, limMode); break;
+        case 8: OFG_LAUNCH((k_gradlim<R, 8>), nb, gb, s, A, nvar, limMode); break;
+        default: OFG_LAUNCH((k_gradlim<R, 6>), nb, gb, s, A, nvar, limMode); break;
         }
     } else {
         OFG_LAUNCH(k_gradlim<R>, nb, 128, s, A, nvar, limMode);

@@ -27,7 +27,7 @@ class OfgTuning(C.Structure):
     """ctypes mirror of ofg_tuning (include/oneflow_b200.h)."""
     _fields_ = [("face_min_blocks", C.c_int), ("face_block", C.c_int), ("grad_min_blocks", C.c_int),
                 ("sweep_min_blocks", C.c_int), ("sweep_block", C.c_int), ("sweep_persistent", C.c_int),
-                ("reserved", C.c_int * 2),
+                ("grad_block", C.c_int), ("reserved", C.c_int * 1),
                 ("ms_default", C.c_double), ("ms_tuned", C.c_double)]
 
     def as_dict(self) -> dict:

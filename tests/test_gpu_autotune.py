@@ -12,7 +12,7 @@ from oneflow_b200.walldist import plate_wall_distance
 
 pytestmark = pytest.mark.gpu
 
-VALID = {"face_min_blocks": {2, 3, 4, 5}, "face_block": {64, 128}, "grad_min_blocks": {4, 6, 8},
+VALID = {"face_min_blocks": {2, 3, 4, 5}, "face_block": {64, 128}, "grad_min_blocks": {4, 6, 8}, "grad_block": {64, 128},
          "sweep_min_blocks": {6, 8, 10}, "sweep_block": {64, 128}}
 
 
@@ -41,12 +41,25 @@ def test_tuned_shapes_give_the_same_solution():
     a = Solver(m, prm); a.init_flowfield(); a.step(2)
     b = Solver(m, prm); b.init_flowfield(); b.step(2)
     # every non-default shape at once
-    b.set_tuning(face_min_blocks=5, face_block=64, grad_min_blocks=8, sweep_min_blocks=10, sweep_block=64)
+    b.set_tuning(face_min_blocks=5, face_block=64, grad_min_blocks=8, grad_block=64, sweep_min_blocks=10,
+                 sweep_block=64)
     a.step(10); b.step(10)
     qa, qb = a.state(), b.state()
     assert np.abs(qb - qa).max() / np.abs(qa).max() < 1e-6
     ta, tb = a.state(TURB_SOLVER), b.state(TURB_SOLVER)
     assert np.linalg.norm(tb - ta) / np.linalg.norm(ta) < 1e-5
+
+
+def test_gradient_block_size_gives_the_same_bits():
+    # the gradient kernel's cells do not depend on the block size, and the
+    # zone-wide Venkatakrishnan eps reduces exact minima and maxima per block
+    m = meshgen.bump_channel(32, 16)
+    prm = P.euler_bump(ilim=2, vencat_coef=0.05, precision=1)
+    a = Solver(m, prm); a.init_flowfield()
+    b = Solver(m, prm); b.init_flowfield()
+    b.set_tuning(grad_block=64)
+    a.step(20); b.step(20)
+    assert np.array_equal(a.state(), b.state())
 
 
 def test_set_tuning_rejects_shapes_that_are_not_compiled():
@@ -55,6 +68,8 @@ def test_set_tuning_rejects_shapes_that_are_not_compiled():
         s.set_tuning(face_min_blocks=7)
     with pytest.raises(OfgError):
         s.set_tuning(sweep_block=256)
+    with pytest.raises(OfgError):
+        s.set_tuning(grad_block=32)
 
 
 def test_fp64_path_keeps_its_fixed_shapes_and_tunes_its_sweep_schedule():
