@@ -682,8 +682,8 @@ def batched_throughput(n_cases: int = 64, steps: int = 10, warmup: int = 3):
             "autotuner": {"tuned_ms_sum": sum(t["ms_tuned"] for t in tunes),
                           "default_ms_sum": sum(t["ms_default"] for t in tunes),
                           "choices": {k: {str(v): sum(1 for t in tunes if t[k] == v) for v in sorted({t[k] for t in tunes})}
-                                      for k in ("face_min_blocks", "face_block", "grad_min_blocks", "sweep_min_blocks",
-                                                "sweep_block")}},
+                                      for k in ("face_min_blocks", "face_block", "grad_min_blocks", "grad_block",
+                                                "sweep_min_blocks", "sweep_block")}},
             "timing": "host wall clock around synchronous calls, after warm-up"}
 
 
