@@ -434,6 +434,7 @@ typedef struct ofg_ins ofg_ins;
    mesh or model is outside the scope above, OFG_E_STATE without a mesh,
    OFG_E_NOMEM. */
 int ofg_ins_create(ofg_ctx *ctx, const double *wall_uvw, ofg_ins **out);
+/* Destroy the solver before its context (it runs on the context's stream). */
 void ofg_ins_destroy(ofg_ins *s);
 
 /* INIT_INSRESTART + INIT_FINAL (UINsRestart::InitinsRestart,
