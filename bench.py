@@ -638,18 +638,23 @@ def replica_aggregate(total_ms, cells, steps, world, dist):
     return total_ms, cells * steps * world / (total_ms * 1e-3)
 
 
-def batched_throughput(n_cases: int = 64, steps: int = 10, warmup: int = 3):
+def batched_throughput(n_cases: int = 64, steps: int = 100, warmup: int = 3):
     """The batched configuration: 64 seeded 2-D RANS-SA airfoil solves of
     uneven sizes (20k-400k cells, 7.9M in all), advanced (a) one after
     another, each by its own graph launches, and (b) together by one batch
-    graph launch per iteration.  Host wall clock around the synchronous calls
-    (both include their launch overheads), after warm-up (graphs captured)."""
+    graph launch per iteration.  Device time with CUDA events: (a) the sum over
+    the solves of the events around each one's `steps` iterations on one
+    stream, (b) the batch's own events around its graph launches.  Each leg
+    starts from the free stream (the second-order airfoil cases do not
+    converge, and a few blow up after 150 iterations or more)."""
     import torch
     from oneflow_b200 import Batch, Solver
     cases = meshgen.airfoil_cases(n_cases)
+    stream = torch.cuda.Stream()
     ss = []
     for mesh, fs in cases:
         s = Solver(mesh, P.rans_airfoil(**fs))
+        s.set_stream(stream.cuda_stream)
         s.init_flowfield()
         ss.append(s)
     cells = sum(m.n_cells for m, _ in cases)
@@ -658,18 +663,18 @@ def batched_throughput(n_cases: int = 64, steps: int = 10, warmup: int = 3):
         s.step(warmup)
         tunes.append(s.autotune())   # per mesh: launch shapes timed on its own cells
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    seq_ms = 0.0
     for s in ss:
-        s.step(steps)
-    torch.cuda.synchronize()
-    seq = time.perf_counter() - t0
+        a = torch.cuda.Event(enable_timing=True); e = torch.cuda.Event(enable_timing=True)
+        a.record(stream); s.step(steps); e.record(stream)
+        e.synchronize()
+        seq_ms += a.elapsed_time(e)
+    for s in ss:
+        s.init_flowfield()
     b = Batch(ss)
     b.step(warmup)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
     b.step(steps)
-    torch.cuda.synchronize()
-    bat = time.perf_counter() - t0
+    bat_ms = b.device_ms()
     b.close()
     for s in ss:
         s.close()
@@ -677,14 +682,16 @@ def batched_throughput(n_cases: int = 64, steps: int = 10, warmup: int = 3):
                         f"{min(m.n_cells for m, _ in cases):,}-{max(m.n_cells for m, _ in cases):,} cells, "
                         "Mach 0.3-0.8, AoA -2..8 deg, Re 1e6-1e7 (seeded); Roe 2nd order Green-Gauss + Venkatakrishnan, "
                         "SA, LU-SGS, FP32 faces",
-            "cells": cells, "steps": steps, "unit": "cell-iter/s",
-            "sequential": cells * steps / seq, "batched": cells * steps / bat,
+            "cells": cells, "steps": steps, "warmup": warmup, "unit": "cell-iter/s",
+            "sequential": cells * steps / (seq_ms * 1e-3), "batched": cells * steps / (bat_ms * 1e-3),
+            "sequential_ms_per_step": seq_ms / steps, "batched_ms_per_step": bat_ms / steps,
             "autotuner": {"tuned_ms_sum": sum(t["ms_tuned"] for t in tunes),
                           "default_ms_sum": sum(t["ms_default"] for t in tunes),
                           "choices": {k: {str(v): sum(1 for t in tunes if t[k] == v) for v in sorted({t[k] for t in tunes})}
                                       for k in ("face_min_blocks", "face_block", "grad_min_blocks", "grad_block",
-                                                "sweep_min_blocks", "sweep_block")}},
-            "timing": "host wall clock around synchronous calls, after warm-up"}
+                                                "sweep_min_blocks", "sweep_block", "sweep_persistent")}},
+            "timing": "CUDA events on the launching stream: sequential = sum over the solves, batched = around the "
+                      "batch's graph launches; each leg from the free stream after warm-up"}
 
 
 def time_to_drop(config: str, target: float, stream, chunk: int = 200, max_iters: int = 40000):

@@ -213,6 +213,10 @@ int         ofg_batch_create(ofg_ctx *const *ctxs, int n, ofg_batch **out);
 int         ofg_batch_step(ofg_batch *batch, int nsteps);
 void        ofg_batch_destroy(ofg_batch *batch);
 const char *ofg_batch_last_error(const ofg_batch *batch);
+/* Device time of the last successful ofg_batch_step, in milliseconds: CUDA
+   events on the batch's stream before its first and after its last graph
+   launch.  OFG_E_ARG before the first step. */
+int         ofg_batch_device_ms(const ofg_batch *batch, float *ms);
 
 /* Coordinate MLP for warm starts (no counterpart in the reference): n_in
    inputs -> depth hidden layers of `width` (a multiple of 16) with GELU ->

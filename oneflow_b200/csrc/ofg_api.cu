@@ -1045,6 +1045,8 @@ int ofg_step(ofg_ctx *c, int nsteps) {
 struct ofg_batch {
     std::vector<ofg_ctx *> ctx;
     cudaStream_t stream = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};         // around the graph launches of one ofg_batch_step
+    float lastMs = -1.f;                            // their device time, after a successful step
     cudaGraphExec_t exec[2] = {nullptr, nullptr};   // [k]: each context at parity built[i] ^ k
     std::vector<int> built;                          // the contexts' parities when the execs were built
     std::vector<unsigned> gen;                       // and their graph generations
@@ -1067,6 +1069,13 @@ int ofg_batch_create(ofg_ctx *const *ctxs, int n, ofg_batch **out) {
         b->ctx.push_back(ctxs[i]);
     }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { delete b; return OFG_E_CUDA; }
+    if (cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess) {
+        for (auto &e : b->ev)
+            if (e) cudaEventDestroy(e);
+        cudaStreamDestroy(b->stream);
+        delete b;
+        return OFG_E_CUDA;
+    }
     *out = b;
     return OFG_OK;
 }
@@ -1075,11 +1084,18 @@ void ofg_batch_destroy(ofg_batch *b) {
     if (!b) return;
     cudaStreamSynchronize(b->stream);
     batch_release(b);
+    for (auto &e : b->ev) cudaEventDestroy(e);
     cudaStreamDestroy(b->stream);
     delete b;
 }
 
 const char *ofg_batch_last_error(const ofg_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int ofg_batch_device_ms(const ofg_batch *b, float *ms) {
+    if (!b || !ms || b->lastMs < 0.f) return OFG_E_ARG;
+    *ms = b->lastMs;
+    return OFG_OK;
+}
 
 int ofg_batch_step(ofg_batch *b, int nsteps) {
     if (!b) return OFG_E_ARG;
@@ -1116,17 +1132,23 @@ int ofg_batch_step(ofg_batch *b, int nsteps) {
         }
         flip = 0;
     }
+    b->lastMs = -1.f;
+    if (cudaEventRecord(b->ev[0], b->stream) != cudaSuccess) return b->fail(OFG_E_CUDA, "cudaEventRecord");
     for (int it = 0; it < nsteps; ++it) {
         if (cudaGraphLaunch(b->exec[flip], b->stream) != cudaSuccess) return b->fail(OFG_E_CUDA, "cudaGraphLaunch");
         for (ofg_ctx *c : b->ctx) account_step(c);
         flip ^= 1;
     }
+    if (cudaEventRecord(b->ev[1], b->stream) != cudaSuccess) return b->fail(OFG_E_CUDA, "cudaEventRecord");
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return b->fail(OFG_E_CUDA, cudaGetErrorString(e));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]) != cudaSuccess) return b->fail(OFG_E_CUDA, "cudaEventElapsedTime");
     for (int i = 0; i < n; ++i) {
         int rc = sync_history(b->ctx[i]);
         if (rc) return b->fail(rc, "context " + std::to_string(i) + ": " + b->ctx[i]->err);
     }
+    b->lastMs = ms;
     return OFG_OK;
 }
 

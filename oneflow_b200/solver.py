@@ -64,6 +64,7 @@ def load_library() -> C.CDLL:
     L.ofg_batch_destroy.argtypes = [C.c_void_p]
     L.ofg_batch_last_error.argtypes = [C.c_void_p]
     L.ofg_batch_last_error.restype = C.c_char_p
+    L.ofg_batch_device_ms.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
     L.ofg_write_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_double]
     L.ofg_read_restart.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.POINTER(C.c_int64), C.POINTER(C.c_double)]
     for name in ("ofg_zero_dq", "ofg_calc_time_step", "ofg_load_residuals", "ofg_update_residuals", "ofg_init_lusgs",
@@ -322,6 +323,14 @@ class Batch:
         if rc != 0:
             msg = self.L.ofg_batch_last_error(self.h)
             raise OfgError(f"error {rc}: {msg.decode() if msg else ''}")
+
+    def device_ms(self) -> float:
+        """Device time of the last ``step`` call (CUDA events around its graph launches)."""
+        ms = C.c_float()
+        rc = self.L.ofg_batch_device_ms(self.h, C.byref(ms))
+        if rc != 0:
+            raise OfgError(f"ofg_batch_device_ms failed ({rc})")
+        return ms.value
 
     def close(self):
         if getattr(self, "h", None):

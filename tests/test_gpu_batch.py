@@ -46,8 +46,12 @@ def test_batch_equals_separate_solves():
     for s in solo:
         s.step(10)
     b = Batch(batched)
+    with pytest.raises(OfgError):
+        b.device_ms()                    # no step timed yet
     b.step(6)
+    ms6 = b.device_ms()
     b.step(4)
+    assert 0.0 < b.device_ms() and 0.0 < ms6
     for x, y in zip(solo, batched):
         same(x, y)
     b.close()
