@@ -638,15 +638,17 @@ def replica_aggregate(total_ms, cells, steps, world, dist):
     return total_ms, cells * steps * world / (total_ms * 1e-3)
 
 
-def batched_throughput(n_cases: int = 64, steps: int = 100, warmup: int = 3):
+def batched_throughput(n_cases: int = 64, steps: int = 100, warmup: int = 3, reps: int = 5):
     """The batched configuration: 64 seeded 2-D RANS-SA airfoil solves of
     uneven sizes (20k-400k cells, 7.9M in all), advanced (a) one after
     another, each by its own graph launches, and (b) together by one batch
     graph launch per iteration.  Device time with CUDA events: (a) the sum over
-    the solves of the events around each one's `steps` iterations on one
-    stream, (b) the batch's own events around its graph launches.  Each leg
-    starts from the free stream (the second-order airfoil cases do not
-    converge, and a few blow up after 150 iterations or more)."""
+    the solves of the events around each one's iterations on one stream, (b)
+    the batch's own events around its graph launches.  The `steps` timed
+    iterations are taken as `reps` runs of steps / reps, each from the free
+    stream after `warmup` untimed iterations: the second-order airfoil cases do
+    not converge, and a few of the 64 blow up within about a hundred
+    iterations."""
     import torch
     from oneflow_b200 import Batch, Solver
     cases = meshgen.airfoil_cases(n_cases)
@@ -663,35 +665,44 @@ def batched_throughput(n_cases: int = 64, steps: int = 100, warmup: int = 3):
         s.step(warmup)
         tunes.append(s.autotune())   # per mesh: launch shapes timed on its own cells
     torch.cuda.synchronize()
+    per = steps // reps
     seq_ms = 0.0
-    for s in ss:
-        a = torch.cuda.Event(enable_timing=True); e = torch.cuda.Event(enable_timing=True)
-        a.record(stream); s.step(steps); e.record(stream)
-        e.synchronize()
-        seq_ms += a.elapsed_time(e)
-    for s in ss:
-        s.init_flowfield()
+    for _ in range(reps):
+        for s in ss:
+            s.init_flowfield()
+            s.step(warmup)
+        for s in ss:
+            a = torch.cuda.Event(enable_timing=True); e = torch.cuda.Event(enable_timing=True)
+            a.record(stream); s.step(per); e.record(stream)
+            e.synchronize()
+            seq_ms += a.elapsed_time(e)
     b = Batch(ss)
-    b.step(warmup)
-    b.step(steps)
-    bat_ms = b.device_ms()
+    bat_ms = 0.0
+    for _ in range(reps):
+        for s in ss:
+            s.init_flowfield()
+        b.step(warmup)
+        b.step(per)
+        bat_ms += b.device_ms()
     b.close()
     for s in ss:
         s.close()
+    timed = per * reps
     return {"workload": f"{n_cases} 2-D RANS-SA NACA 4-digit airfoils, hybrid O-grids of "
                         f"{min(m.n_cells for m, _ in cases):,}-{max(m.n_cells for m, _ in cases):,} cells, "
                         "Mach 0.3-0.8, AoA -2..8 deg, Re 1e6-1e7 (seeded); Roe 2nd order Green-Gauss + Venkatakrishnan, "
                         "SA, LU-SGS, FP32 faces",
-            "cells": cells, "steps": steps, "warmup": warmup, "unit": "cell-iter/s",
-            "sequential": cells * steps / (seq_ms * 1e-3), "batched": cells * steps / (bat_ms * 1e-3),
-            "sequential_ms_per_step": seq_ms / steps, "batched_ms_per_step": bat_ms / steps,
+            "cells": cells, "steps": timed, "runs": reps, "warmup_per_run": warmup, "unit": "cell-iter/s",
+            "sequential": cells * timed / (seq_ms * 1e-3), "batched": cells * timed / (bat_ms * 1e-3),
+            "sequential_ms_per_step": seq_ms / timed, "batched_ms_per_step": bat_ms / timed,
             "autotuner": {"tuned_ms_sum": sum(t["ms_tuned"] for t in tunes),
                           "default_ms_sum": sum(t["ms_default"] for t in tunes),
                           "choices": {k: {str(v): sum(1 for t in tunes if t[k] == v) for v in sorted({t[k] for t in tunes})}
                                       for k in ("face_min_blocks", "face_block", "grad_min_blocks", "grad_block",
                                                 "sweep_min_blocks", "sweep_block", "sweep_persistent")}},
             "timing": "CUDA events on the launching stream: sequential = sum over the solves, batched = around the "
-                      "batch's graph launches; each leg from the free stream after warm-up"}
+                      f"batch's graph launches; {reps} runs of {per} iterations, each from the free stream after "
+                      f"{warmup} untimed iterations"}
 
 
 def time_to_drop(config: str, target: float, stream, chunk: int = 200, max_iters: int = 40000):

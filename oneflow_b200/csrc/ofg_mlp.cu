@@ -1,6 +1,6 @@
 // Coordinate MLP for warm-starting steady solves: BF16 weights and
-// activations on the tensor cores (warp-level WMMA 16x16x16 BF16 tiles with
-// FP32 accumulation), FP32 master weights, Adam.  Not part of the reference:
+// activations on the tensor cores (tcgen05.mma with FP32 accumulation in
+// tensor memory), FP32 master weights, Adam.  Not part of the reference:
 // it learns flow fields from solutions this solver produced, and the
 // cold-started solve remains the fallback and the judge of convergence.
 //
@@ -9,7 +9,6 @@
 // padded outputs carry no loss, so the padding never changes the result.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
-#include <mma.h>
 
 #include <algorithm>
 #include <cmath>
@@ -24,51 +23,230 @@
 namespace {
 
 using bf16 = __nv_bfloat16;
-constexpr int GT = 128;        // threads of a GEMM block: 4 warps
-constexpr int TM = 64, TN = 64;  // block tile
+constexpr int ROWS = 64;       // row granularity of the batches the API takes
 constexpr int SPLITK = 32;     // batch chunks of the weight-gradient GEMMs
 
 inline int pad16(int v) { return (v + 15) / 16 * 16; }
 
-// C[M x N] (fp32, row-major, ldc) = op(A)[M x K] * op(B)[K x N] over the
-// K range [k0, k1) of blockIdx.z's chunk.  op(A): A row-major (lda), or, with
-// AT, the transpose of a row-major [K x M] array.  op(B): B row-major [K x N],
-// or, with BT, the transpose of a row-major [N x K] array.  Warp w of the
-// block computes rows [16 w, 16 w + 16) of the block tile, four 16x16 tiles.
-template <bool AT, bool BT>
-__global__ void __launch_bounds__(GT) k_gemm(int M, int N, int K, int kchunk, const bf16 *__restrict__ A, int lda,
-                                             const bf16 *__restrict__ B, int ldb, float *C, int ldc,
-                                             size_t zstride) {
-    using namespace nvcuda;
-    int warp = threadIdx.x >> 5;
-    int row0 = blockIdx.y * TM + warp * 16, col0 = blockIdx.x * TN;
-    if (row0 >= M) return;
-    int k0 = blockIdx.z * kchunk, k1 = min(K, k0 + kchunk);
-    C += blockIdx.z * zstride;
-    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[4];
+// ---------------------------------------------------------------------------
+// GEMM on the fifth-generation tensor cores.  A CTA of four warps computes a
+// BM x BN tile of C = op(A) op(B): the BF16 operand tiles of one K block
+// (BM x BK of A, up to BN x BK of B) are staged in shared memory in core
+// matrices without swizzle (128 bytes each, 128 B apart along K, 1,024 B apart
+// along M / N; K-major or MN-major as the operand lies in memory), one
+// thread issues tcgen05.mma (M 128, N the tile's width, K 16, FP32
+// accumulation in tensor memory) and tcgen05.commit arrives on the stage's
+// mbarrier, so the loads of the next K block overlap the MMAs of the last
+// (two stages).  The epilogue
+// reads the accumulator with tcgen05.ld: warp w holds rows 32w..32w+31 (its
+// tensor-memory lanes), 16 columns per load.  Every wait is bounded; a wait
+// that runs out sets g_gemm_status and the CTA frees its tensor memory and
+// returns.
+// ---------------------------------------------------------------------------
+constexpr int GT = 128;                       // threads of a GEMM block
+constexpr int BM = 128, BN = 128, BK = 64;    // block tile
+constexpr int SBO = (BK / 8) * 128;           // bytes between 8-row core-matrix groups
+constexpr int TILE_A = BM * BK * 2, TILE_B = BN * BK * 2, STAGE = TILE_A + TILE_B;
+constexpr int SMEM_GEMM = 2 * STAGE + 1024 + 64;   // two stages, 1,024-B alignment slack, barriers
+constexpr unsigned WAIT_LIMIT = 1u << 20;     // try_wait rounds before a wait gives up
+
+__device__ unsigned g_gemm_status;            // nonzero: a GEMM wait ran out
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: start address, leading (K) byte offset
+// 128, stride (M/N) byte offset SBO, descriptor version 1, no swizzle (the
+// same fields describe the K-major and the MN-major staging)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    return uint64_t((addr >> 4) & 0x3FFF) | (uint64_t(128 >> 4) << 16) | (uint64_t(SBO >> 4) << 32) |
+           (uint64_t(1) << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, each
+// K-major (0) or MN-major (1), N = n, M = BM
+__device__ __forceinline__ uint32_t instr_desc(int n, uint32_t a_mn, uint32_t b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (a_mn << 15) | (b_mn << 16) | (uint32_t(n >> 3) << 17) |
+           (uint32_t(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (unsigned i = 0; i < WAIT_LIMIT; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(addr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Stage the rows [r0, r0 + nr) x K block [kb, kb + BK) of an operand whose
+// element (r, k) is g[r * ld + k] (T false: K contiguous, staged K-major: a
+// core matrix holds 8 rows x 8 K) or g[k * ld + r] (T true: rows contiguous,
+// staged MN-major: a core matrix holds 8 K x 8 rows); either way core
+// matrices lie 128 B apart along K and SBO apart along the rows, and every
+// 16-byte chunk of the source is one 16-byte store.  A warp's 32 stores cover
+// 512 contiguous bytes.  Rows at or beyond `rows` and K at or beyond k1 are
+// zero.  rows, nr, ld, kb and k1 are multiples of 8; nr <= 128.
+template <bool T>
+__device__ __forceinline__ void stage_tile(unsigned char *s, const bf16 *__restrict__ g, int ld, int rows, int r0,
+                                           int nr, int kb, int k1) {
+    static_assert(BK == 64, "eight 8-element K chunks per block");
+    const int items = nr * (BK / 8), nc = nr >> 3;
+    uint4 v[8];
+    uint32_t off[8];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) wmma::fill_fragment(acc[j], 0.0f);
-    using LA = typename std::conditional<AT, wmma::col_major, wmma::row_major>::type;
-    using LB = typename std::conditional<BT, wmma::col_major, wmma::row_major>::type;
-    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, LA> fa;
-    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, LB> fb;
-    for (int k = k0; k < k1; k += 16) {
-        const bf16 *pa = AT ? A + (size_t)k * lda + row0 : A + (size_t)row0 * lda + k;
-        wmma::load_matrix_sync(fa, pa, lda);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            int c = col0 + 16 * j;
-            if (c >= N) break;
-            const bf16 *pb = BT ? B + (size_t)c * ldb + k : B + (size_t)k * ldb + c;
-            wmma::load_matrix_sync(fb, pb, ldb);
-            wmma::mma_sync(acc[j], fa, fb, acc[j]);
+    for (int u = 0; u < 8; ++u) {
+        const int i = threadIdx.x + u * GT;
+        v[u] = make_uint4(0u, 0u, 0u, 0u);
+        off[u] = 0xFFFFFFFFu;
+        if (i < items) {
+            int r, k;   // first row and K of the chunk
+            if (!T) {   // i: row % 8, then K chunk, then row / 8
+                r = (i & 7) + ((i >> 6) << 3);
+                k = ((i >> 3) & 7) * 8;
+                off[u] = (r >> 3) * SBO + (k >> 3) * 128 + (r & 7) * 16;
+            } else {    // i: K % 8, then row chunk, then K / 8
+                k = (i & 7) + ((i >> 3) / nc) * 8;
+                r = ((i >> 3) % nc) * 8;
+                off[u] = (r >> 3) * SBO + (k >> 3) * 128 + (k & 7) * 16;
+            }
+            if (r0 + r < rows && kb + k < k1)
+                v[u] = *reinterpret_cast<const uint4 *>(T ? g + (size_t)(kb + k) * ld + r0 + r
+                                                          : g + (size_t)(r0 + r) * ld + kb + k);
         }
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        int c = col0 + 16 * j;
-        if (c >= N) break;
-        wmma::store_matrix_sync(C + (size_t)row0 * ldc + c, acc[j], ldc, wmma::mem_row_major);
+    for (int u = 0; u < 8; ++u)
+        if (off[u] != 0xFFFFFFFFu) *reinterpret_cast<uint4 *>(s + off[u]) = v[u];
+}
+
+// C[M x N] (FP32, row-major, ldc) = op(A)[M x K] op(B)[K x N] over the K range
+// [k0, k1) of blockIdx.z's chunk, into C + blockIdx.z * zstride.  op(A): A
+// row-major (lda), or, with AT, the transpose of a row-major [K x M] array.
+// op(B): B row-major [K x N], or, with BT, the transpose of a row-major
+// [N x K] array.  M, N, K, kchunk and the leading dimensions are multiples of
+// 16; the arrays are 16-byte aligned.
+template <bool AT, bool BT>
+__global__ void __launch_bounds__(GT, 1) k_gemm(int M, int N, int K, int kchunk, const bf16 *__restrict__ A, int lda,
+                                                const bf16 *__restrict__ B, int ldb, float *C, int ldc,
+                                                size_t zstride) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                          ~uintptr_t(1023));
+    const uint32_t bar0 = smem_u32(sm + 2 * STAGE), slot = smem_u32(sm + 2 * STAGE + 16);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN, nt = min(BN, N - n0);
+    const int k0 = blockIdx.z * kchunk, k1 = min(K, k0 + kchunk);
+    const int nkb = k1 > k0 ? (k1 - k0 + BK - 1) / BK : 0;
+    C += blockIdx.z * zstride;
+    if (threadIdx.x == 0) {
+        mbar_init(bar0);
+        mbar_init(bar0 + 8);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(sm + 2 * STAGE + 16);
+    const uint32_t idesc = instr_desc(nt, AT ? 1u : 0u, BT ? 0u : 1u);
+    int ok = 1, issued = 0;   // K blocks whose MMAs have been committed (the same in every thread)
+    for (int kb = 0; kb < nkb; ++kb) {
+        const int st = kb & 1;
+        // the MMAs of K block kb - 2 read this stage: wait for their commit
+        if (kb >= 2) ok = mbar_wait(bar0 + 8 * st, ((kb - 2) >> 1) & 1);
+        if (!__syncthreads_and(ok)) break;
+        issued = kb + 1;
+        unsigned char *sa = sm + st * STAGE, *sb = sa + TILE_A;
+        const int kbase = k0 + kb * BK;
+        stage_tile<AT>(sa, A, lda, M, m0, BM, kbase, k1);
+        stage_tile<!BT>(sb, B, ldb, N, n0, nt, kbase, k1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic-proxy stores -> tensor core
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const int nk16 = min(BK, k1 - kbase) / 16;
+            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+            for (int j = 0; j < nk16; ++j)
+                mma_bf16(tmem, smem_desc(a0 + j * 256), smem_desc(b0 + j * 256), idesc, (kb | j) != 0);
+            mma_commit(bar0 + 8 * st);
+        }
+    }
+    // the last commit covers every MMA issued before it
+    if (ok && issued > 0) ok = mbar_wait(bar0 + 8 * ((issued - 1) & 1), ((issued - 1) >> 1) & 1);
+    ok = __syncthreads_and(ok);
+    tc_fence_after();
+    if (ok) {
+        const int r = m0 + warp * 32 + lane;
+        for (int c = 0; c < nt; c += 16) {
+            uint32_t v[16];
+            if (nkb > 0) {
+                tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c), v);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = 0u;
+            }
+            if (r < M) {
+                float4 *o = reinterpret_cast<float4 *>(C + (size_t)r * ldc + n0 + c);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    o[j] = make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]),
+                                       __uint_as_float(v[4 * j + 2]), __uint_as_float(v[4 * j + 3]));
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        atomicOr(&g_gemm_status, 1u);
+        // give MMAs still in flight a bounded time to retire before the memory is freed
+        if (issued > 0) mbar_wait(bar0 + 8 * ((issued - 1) & 1), ((issued - 1) >> 1) & 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
     }
 }
 
@@ -203,6 +381,7 @@ struct ofg_mlp {
     bf16 *dZ = nullptr, *dHb = nullptr;              // [rows x maxdim]
     float *dH = nullptr, *part = nullptr, *Tb = nullptr, *rowErr = nullptr;
     long long adamStep = 0;
+    bool gemmReady[4] = {false, false, false, false};   // k_gemm forms whose shared memory limit is raised
     std::string err;
     int fail(int code, const std::string &m) { err = m; return code; }
 };
@@ -246,13 +425,39 @@ int ensure_work(ofg_mlp *m, int rows) {
 
 inline unsigned blocks(int64_t n, int t) { return unsigned((n + t - 1) / t); }
 
+// one launch of k_gemm<AT, BT> over a grid of (N / BN) x (M / BM) x parts
+// tiles (the first launch of each form raises its dynamic shared memory limit)
+template <bool AT, bool BT>
+int gemm(ofg_mlp *m, int M, int N, int K, int kchunk, int parts, const bf16 *A, int lda, const bf16 *B, int ldb,
+         float *C, int ldc, size_t zstride) {
+    const int form = int(AT) * 2 + int(BT);
+    if (!m->gemmReady[form]) {
+        MCK(cudaFuncSetAttribute(k_gemm<AT, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_GEMM));
+        m->gemmReady[form] = true;
+    }
+    dim3 g(blocks(N, BN), blocks(M, BM), parts);
+    k_gemm<AT, BT><<<g, GT, SMEM_GEMM>>>(M, N, K, kchunk, A, lda, B, ldb, C, ldc, zstride);
+    return OFG_OK;
+}
+
+// after a synchronisation: an error if a GEMM wait ran out (the flag is cleared)
+int gemm_status(ofg_mlp *m) {
+    unsigned st = 0, zero = 0;
+    MCK(cudaMemcpyFromSymbol(&st, g_gemm_status, sizeof st));
+    if (st) {
+        MCK(cudaMemcpyToSymbol(g_gemm_status, &zero, sizeof zero));
+        return m->fail(OFG_E_TIMEOUT, "a tensor-core GEMM wait ran out");
+    }
+    return OFG_OK;
+}
+
 // forward through every layer for `rows` rows already packed in H[0]; with a
 // target Tb, the output gradient and per-row errors as well
 int forward(ofg_mlp *m, int rows, bool withTarget) {
     for (int l = 0; l < m->L; ++l) {
-        dim3 g(blocks(m->N[l], TN), blocks(rows, TM), 1);
-        k_gemm<false, false><<<g, GT>>>(rows, m->N[l], m->K[l], m->K[l], m->H[l], m->K[l], m->wb + m->woff[l],
-                                        m->N[l], m->Z[l], m->N[l], 0);
+        int rc = gemm<false, false>(m, rows, m->N[l], m->K[l], m->K[l], 1, m->H[l], m->K[l], m->wb + m->woff[l],
+                                    m->N[l], m->Z[l], m->N[l], 0);
+        if (rc) return rc;
         if (l + 1 < m->L) {
             int64_t tot = (int64_t)rows * m->N[l];
             k_bias_gelu<<<blocks(tot, 256), 256>>>(tot, m->N[l], m->Z[l], m->b + m->boff[l], m->H[l + 1]);
@@ -272,14 +477,14 @@ int backward(ofg_mlp *m, int rows) {
         // dW = H^T dZ, split over the rows, partials summed in order
         int chunk = pad16((rows + SPLITK - 1) / SPLITK);
         int parts = (rows + chunk - 1) / chunk;
-        dim3 g(blocks(N, TN), blocks(K, TM), parts);
-        k_gemm<true, false><<<g, GT>>>(K, N, rows, chunk, m->H[l], K, m->dZ, N, m->part, N, (size_t)K * N);
+        int rc = gemm<true, false>(m, K, N, rows, chunk, parts, m->H[l], K, m->dZ, N, m->part, N, (size_t)K * N);
+        if (rc) return rc;
         k_reduce_parts<<<blocks((int64_t)K * N, 256), 256>>>((int64_t)K * N, parts, m->part, m->gw + m->woff[l]);
         k_colsum<<<N, 256>>>(rows, N, m->dZ, m->gb + m->boff[l]);
         if (l > 0) {
             // dH = dZ W^T, then through the GELU of the layer below
-            dim3 g2(blocks(K, TN), blocks(rows, TM), 1);
-            k_gemm<false, true><<<g2, GT>>>(rows, K, N, N, m->dZ, N, m->wb + m->woff[l], N, m->dH, K, 0);
+            if ((rc = gemm<false, true>(m, rows, K, N, N, 1, m->dZ, N, m->wb + m->woff[l], N, m->dH, K, 0)))
+                return rc;
             int64_t tot = (int64_t)rows * K;
             k_gelu_back<<<blocks(tot, 256), 256>>>(tot, m->dH, m->Z[l - 1], m->dZ);
         }
@@ -404,20 +609,20 @@ int ofg_mlp_predict(ofg_mlp *m, const float *x, int64_t n, float *y) {
     if (rc) return rc;
     for (int64_t r0 = 0; r0 < n; r0 += rows) {
         int rr = int(std::min<int64_t>(rows, n - r0));
-        int rp = (rr + TM - 1) / TM * TM;
+        int rp = (rr + ROWS - 1) / ROWS * ROWS;
         k_pack_rows<<<blocks(rp, 128), 128>>>(rp, n, r0, m->nin, m->K[0], x, m->H[0]);
         if ((rc = forward(m, rp, false))) return rc;
         k_unpack_rows<<<blocks(rp, 128), 128>>>(rp, n, r0, m->N[m->L - 1], m->nout, m->Z[m->L - 1], y);
     }
     MCK(cudaGetLastError());
     MCK(cudaDeviceSynchronize());
-    return OFG_OK;
+    return gemm_status(m);
 }
 
 // Mean squared error of the batch X[n], Y[n] (n a multiple of 64, at most
 // 65,536) and its gradient (host arrays in the parameter layout); no update
 int ofg_mlp_loss_grad(ofg_mlp *m, const float *x, const float *y, int64_t n, float *loss, float *grad) {
-    if (!m || !x || !y || n <= 0 || n % TM || n > 65536) return OFG_E_ARG;
+    if (!m || !x || !y || n <= 0 || n % ROWS || n > 65536) return OFG_E_ARG;
     int rows = int(n);
     int rc = ensure_work(m, rows);
     if (rc) return rc;
@@ -428,6 +633,7 @@ int ofg_mlp_loss_grad(ofg_mlp *m, const float *x, const float *y, int64_t n, flo
     MCK(cudaMemcpy(e.data(), m->rowErr, rows * sizeof(float), cudaMemcpyDeviceToHost));
     MCK(cudaMemcpy(gw.data(), m->gw, m->nw * sizeof(float), cudaMemcpyDeviceToHost));
     MCK(cudaMemcpy(gb.data(), m->gb, m->nb * sizeof(float), cudaMemcpyDeviceToHost));
+    if ((rc = gemm_status(m))) return rc;
     double s = 0.0;
     for (float v : e) s += v;
     if (loss) *loss = float(s / (double(rows) * m->nout));
@@ -447,7 +653,7 @@ int ofg_mlp_loss_grad(ofg_mlp *m, const float *x, const float *y, int64_t n, flo
 // step's minibatch loss
 int ofg_mlp_train(ofg_mlp *m, const float *x, const float *y, int64_t n, int batch, int steps, float lr,
                   uint64_t seed, float *loss_out) {
-    if (!m || !x || !y || n <= 0 || batch <= 0 || batch % TM || batch > 65536 || steps < 0) return OFG_E_ARG;
+    if (!m || !x || !y || n <= 0 || batch <= 0 || batch % ROWS || batch > 65536 || steps < 0) return OFG_E_ARG;
     int rc = ensure_work(m, batch);
     if (rc) return rc;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
@@ -470,7 +676,7 @@ int ofg_mlp_train(ofg_mlp *m, const float *x, const float *y, int64_t n, int bat
     }
     MCK(cudaGetLastError());
     MCK(cudaDeviceSynchronize());
-    return OFG_OK;
+    return gemm_status(m);
 }
 
 }  // extern "C"

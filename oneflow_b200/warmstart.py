@@ -187,7 +187,7 @@ def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth
 
     out = {"family": "2-D Euler bump channels, 64x32 quads -> 4,096 jittered triangles each, bump thickness "
                      "4-10 %, Mach 0.3-0.6, first-order Roe, LU-SGS, CFL 5, colour-major sweeps, FP64",
-           "features": list(FEATURES), "network": f"{X.shape[1]}->{depth}x{width} GELU->{Y.shape[1]}, BF16 WMMA",
+           "features": list(FEATURES), "network": f"{X.shape[1]}->{depth}x{width} GELU->{Y.shape[1]}, BF16 tcgen05.mma GEMMs",
            "train_cases": n_train, "test_cases": n_test, "train_samples": int(X.shape[0]),
            "train_steps": train_steps, "batch": batch, "lr": lr,
            "loss_first": float(losses[0]), "loss_last": float(np.mean(losses[-50:])),

@@ -1,7 +1,8 @@
-"""The warm-start MLP's tensor-core kernels (ofg_mlp_*) against a plain
-PyTorch FP32 restatement of the same network: forward within the BF16
-rounding of weights and activations (tolerance 2e-2 relative), gradients to
-the same level, and Adam training that fits a smooth field."""
+"""The warm-start MLP's tensor-core kernels (ofg_mlp_*: tcgen05.mma GEMMs)
+against a plain FP32 restatement of the same network on the CPU: forward
+within the BF16 rounding of weights and activations (tolerance 2e-2
+relative), gradients to the same level, and Adam training that fits a smooth
+field."""
 import numpy as np
 import pytest
 import torch
@@ -41,23 +42,25 @@ def data(n, n_in, n_out, seed=0):
 
 
 @pytest.mark.parametrize("shape", [(8, 64, 3, 4), (22, 256, 6, 5)])
-def test_forward_matches_torch(shape):
+def test_forward_matches_a_cpu_fp32_restatement(shape):
     net = MLP(*shape, seed=3)
     x, _ = data(1000, shape[0], shape[3])
-    y = net.predict(x)
-    ref = torch_forward(net, net.params(), x)
+    y = net.predict(x).cpu()
+    ref = torch_forward(net, net.params(), x.cpu())
     err = (y - ref).abs().max().item() / ref.abs().max().item()
     assert err < 2e-2, err
 
 
-def test_gradient_matches_torch_autograd():
-    shape = (8, 64, 3, 4)
+@pytest.mark.parametrize("shape,rows", [((8, 64, 3, 4), 4096), ((22, 256, 6, 5), 4160)])
+def test_gradient_matches_a_cpu_fp32_restatement(shape, rows):
+    # rows 4,160 = 32.5 row tiles of 128: a partial tile; width 256 = two column tiles
     net = MLP(*shape, seed=5)
-    x, y = data(4096, shape[0], shape[3], seed=1)
+    x, y = data(rows, shape[0], shape[3], seed=1)
     loss, g = net.loss_grad(x, y)
-    flat = torch.tensor(net.params(), device="cuda", requires_grad=True)
-    # the same network with torch's autograd, BF16 rounding emulated in the
-    # forward (straight-through in the backward)
+    flat = torch.tensor(net.params(), device="cpu", requires_grad=True)
+    x, y = x.cpu(), y.cpu()
+    # the same network in FP32 on the CPU with torch's autograd, BF16 rounding
+    # emulated in the forward (straight-through in the backward)
     layers, o = [], 0
     for fi, fo in net.layer_shapes():
         layers.append((flat[o:o + fi * fo].view(fi, fo), flat[o + fi * fo:o + fi * fo + fo]))
@@ -73,7 +76,7 @@ def test_gradient_matches_torch_autograd():
             h = z
     ref_loss = ((h - y) ** 2).mean()
     ref_loss.backward()
-    gr = flat.grad.cpu().numpy()
+    gr = flat.grad.numpy()
     assert abs(loss - ref_loss.item()) <= 1e-2 * ref_loss.item()
     cos = float(np.dot(g, gr) / (np.linalg.norm(g) * np.linalg.norm(gr)))
     assert cos > 0.999, cos
