@@ -620,12 +620,21 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // column j of H: one warp per r, lanes over the blocks' sums (fixed order)
-    for (int r = wid; r <= j; r += nw) {
-        double h = 0.0;
-        for (int b = lane; b < nb; b += 32) h += ((volatile double *)G.part)[(size_t)r * nb + b];
-        for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
-        if (lane == 0) G.H[(size_t)r * kKrylov + j] = h;
+    // column j of H: per r, the lanes over the blocks' sums (fixed order) and
+    // a warp reduction; a warp takes four r per pass (four loads in flight)
+    for (int rq = 4 * wid; rq <= j; rq += 4 * nw) {
+        double h[4] = {0.0, 0.0, 0.0, 0.0};
+        const double *P = G.part + (size_t)rq * nb;
+        for (int b = lane; b < nb; b += 32) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (rq + q <= j) h[q] += __ldcg(P + (size_t)q * nb + b);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            for (int o = 16; o > 0; o >>= 1) h[q] += __shfl_down_sync(0xffffffffu, h[q], o);
+            if (lane == 0 && rq + q <= j) G.H[(size_t)(rq + q) * kKrylov + j] = h[q];
+        }
     }
     if (threadIdx.x == 0) S->ticket = 0;
 }
@@ -636,6 +645,7 @@ __global__ void __launch_bounds__(kThreads) k_gm_spmv_dots(Gm G) {
 __global__ void __launch_bounds__(kThreads) k_gm_orth(Gm G) {
     __shared__ double sh[32];
     __shared__ double hcol[kKrylov + 1];
+    __shared__ double rc[kKrylov], rs[kKrylov];   // the last block's copy of the earlier rotations
     __shared__ bool last;
     GmState *S = G.st;
     if (((volatile int *)&S->done)[0]) return;
@@ -670,35 +680,47 @@ __global__ void __launch_bounds__(kThreads) k_gm_orth(Gm G) {
     if (!last) return;
     __threadfence();
     const double sum = last_block_sum(G.part, gridDim.x, 1, sh);
+    for (int r = threadIdx.x; r < j; r += blockDim.x) { rc[r] = G.gc[r]; rs[r] = G.gs[r]; }
+    __syncthreads();
     if (threadIdx.x != 0) return;
     const double normr2 = sqrt(sum);
     double *H = G.H;
     auto h = [&](int a, int b) -> double & { return H[(size_t)a * kKrylov + b]; };
-    h(j + 1, j) = normr2;
     const int col = j;
+    // the earlier rotations down column j (hcol holds it as the products left
+    // it): the running entry h(row, col) stays in a register, the rotated
+    // entries go out as they are final
+    double hr = hcol[0];
     for (int row = 0; row < col; ++row) {
-        double tmp = G.gc[row] * h(row, col) + G.gs[row] * h(row + 1, col);
-        h(row + 1, col) = -G.gs[row] * h(row, col) + G.gc[row] * h(row + 1, col);
+        const double hn = hcol[row + 1], c = rc[row], sn = rs[row];
+        double tmp = c * hr + sn * hn;
+        hr = -sn * hr + c * hn;
         h(row, col) = tmp;
     }
-    if (h(col + 1, col) == 0.0) {
+    double hcc = hr, hc1 = normr2;   // h(col, col), h(col + 1, col)
+    if (hc1 == 0.0) {
         G.gc[col] = 1.0; G.gs[col] = 0.0;
-    } else if (fabs(h(col + 1, col)) > fabs(h(col, col))) {
-        double tmp = h(col, col) / h(col + 1, col);
+    } else if (fabs(hc1) > fabs(hcc)) {
+        double tmp = hcc / hc1;
         G.gs[col] = 1.0 / sqrt(1.0 + tmp * tmp);
         G.gc[col] = tmp * G.gs[col];
     } else {
-        double tmp = h(col + 1, col) / h(col, col);
+        double tmp = hc1 / hcc;
         G.gc[col] = 1.0 / sqrt(1.0 + tmp * tmp);
         G.gs[col] = tmp * G.gc[col];
     }
-    double tmp = G.gc[col] * h(col, col) + G.gs[col] * h(col + 1, col);
-    h(col + 1, col) = -G.gs[col] * h(col, col) + G.gc[col] * h(col + 1, col);
-    h(col, col) = tmp;
-    if (h(col + 1, col) < 1e-10) h(col + 1, col) = 0;
-    tmp = G.gc[col] * G.s[col] + G.gs[col] * G.s[col + 1];
+    {
+        const double c = G.gc[col], sn = G.gs[col];
+        double tmp = c * hcc + sn * hc1;
+        hc1 = -sn * hcc + c * hc1;
+        hcc = tmp;
+    }
+    if (hc1 < 1e-10) hc1 = 0;
+    h(col, col) = hcc;
+    h(col + 1, col) = hc1;
+    const double st = G.gc[col] * G.s[col] + G.gs[col] * G.s[col + 1];
     G.s[col + 1] = -G.gs[col] * G.s[col] + G.gc[col] * G.s[col + 1];
-    G.s[col] = tmp;
+    G.s[col] = st;
     const double Sv = G.s[j + 1];
     S->rho = sqrt(Sv * Sv);
     S->inv = 1.0 / normr2;
