@@ -1019,7 +1019,14 @@ int ofg_ins_create(ofg_ctx *c, const double *wall_uvw, ofg_ins **out) {
     z(&D.Am, rOff[nT]); z(&D.Ap, rOff[nT]);
     z(&D.part, 4 * (size_t)blocks(nT)); z(&D.red, 4);
     if (!rc) rc = s->alloc(&D.ticket, 1);
-    s->nChunkBlk = std::min((nT + kChunk - 1) / kChunk, 148 * 3);   // blocks of k_gm_spmv_dots: one resident wave (grid stride)
+    // blocks of k_gm_spmv_dots: at most one resident wave (three per SM) taking
+    // the 256-row chunks in grid stride, as few as give every block the same
+    // number of chunks (a last round of a few blocks leaves most SMs idle)
+    {
+        const int nChunks = (nT + kChunk - 1) / kChunk, slots = 148 * 3;
+        const int rounds = (nChunks + slots - 1) / slots;
+        s->nChunkBlk = (nChunks + rounds - 1) / rounds;
+    }
     s->nGrid = std::min(blocks(nT), 148 * 8);
     s->nPart = std::max(s->nChunkBlk * (kKrylov + 1), s->nGrid);
     z(&s->V, (size_t)(kKrylov + 1) * T); z(&s->W, T); z(&s->Y, T);
