@@ -598,10 +598,11 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_throughput()
-    learned = None
+    learned = learned_af = None
     if rank == 0 and world == 1 and not args.no_learned:
         from oneflow_b200 import warmstart
         learned = warmstart.run_experiment()
+        learned_af = warmstart.run_experiment(family="airfoil")
 
     clocks = clk.summary()
     if rank == 0:
@@ -616,7 +617,8 @@ def main():
                 "e2e": {"value": e2e_val, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
                 "gpu_launches": int(l1 - l0), "clocks": clocks, "time_to_1e-8": conv,
                 "setup": {"calc_wall_dist_s": wall_s, "wall_dist_vs_closed_form": wall_err},
-                "batched": batched, "learned_warm_start": learned}
+                "batched": batched, "learned_warm_start": learned,
+                "learned_warm_start_airfoils": learned_af}
         print(json.dumps(line))
     if dist:
         dist.barrier()

@@ -338,13 +338,10 @@ def _faces_from_polygons_2d(poly: np.ndarray, counts: np.ndarray, n_nodes: int):
     return nodes[forder], lc[forder], rc[forder], int(isb.sum())
 
 
-def naca4_surface(m: float, p: float, t: float, n_half: int) -> np.ndarray:
-    """Closed NACA 4-digit section (max camber m, its position p, thickness t,
-    chord 1; thickness polynomial with the closed-trailing-edge coefficient
-    -0.1036), cosine-spaced: 2 n_half points from the trailing edge along the
-    lower surface to the leading edge and back along the upper surface."""
-    beta = np.linspace(0.0, np.pi, n_half + 1)
-    x = 0.5 * (1.0 - np.cos(beta))
+def naca4_parts(m: float, p: float, t: float, x: np.ndarray):
+    """NACA 4-digit section at chord stations x (chord 1): half thickness yt
+    (closed-trailing-edge coefficient -0.1036), camber line yc and its angle"""
+    x = np.asarray(x, np.float64)
     yt = 5.0 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
     if m > 0.0:
         fore = x < p
@@ -352,7 +349,16 @@ def naca4_surface(m: float, p: float, t: float, n_half: int) -> np.ndarray:
         dyc = np.where(fore, 2 * m / p ** 2 * (p - x), 2 * m / (1 - p) ** 2 * (p - x))
     else:
         yc = np.zeros_like(x); dyc = np.zeros_like(x)
-    th = np.arctan(dyc)
+    return yt, yc, np.arctan(dyc)
+
+
+def naca4_surface(m: float, p: float, t: float, n_half: int) -> np.ndarray:
+    """Closed NACA 4-digit section (max camber m, its position p, thickness t,
+    chord 1), cosine-spaced: 2 n_half points from the trailing edge along the
+    lower surface to the leading edge and back along the upper surface."""
+    beta = np.linspace(0.0, np.pi, n_half + 1)
+    x = 0.5 * (1.0 - np.cos(beta))
+    yt, yc, th = naca4_parts(m, p, t, x)
     xu, yu = x - yt * np.sin(th), yc + yt * np.cos(th)
     xl, yl = x + yt * np.sin(th), yc - yt * np.cos(th)
     lower = np.stack([xl[::-1], yl[::-1]], 1)          # TE -> LE
@@ -368,16 +374,13 @@ def naca_ogrid(m: float = 0.02, p: float = 0.4, t: float = 0.12, n_surface: int 
     wall.  The inner n_quad_layers layers are quadrilaterals (the boundary
     layer), the rest split into triangles (alternating diagonals).  Layers
     leave the wall along its normals (the bisector at the trailing edge) and
-    then run straight to the circle point at the same arc-length fraction.
+    then run straight to the circle point at the same arc-length fraction of
+    the offset curve where they turn.
     BCs: section SOLID_SURFACE, circle FARFIELD."""
     if n_quad_layers is None:
         n_quad_layers = n_layers // 2
     S = naca4_surface(m, p, t, n_surface // 2)
     n = S.shape[0]
-    seg = np.linalg.norm(np.roll(S, -1, 0) - S, axis=1)
-    s = np.concatenate([[0.0], np.cumsum(seg)[:-1]]) / seg.sum()
-    ang = -2.0 * np.pi * s                              # same turning sense as the section loop
-    Cc = np.stack([0.5 + radius * np.cos(ang), radius * np.sin(ang)], 1)
     # layer fractions: first step y1/radius, geometric growth to 1
     d0 = y1 / radius
     lo, hi = 1.0 + 1e-12, 2.0
@@ -398,6 +401,14 @@ def naca_ogrid(m: float = 0.02, p: float = 0.4, t: float = 0.12, n_surface: int 
     reach = 0.05
     d = (f * radius)[:, None, None]
     E = S + reach * nrm
+    # the outer lines run straight from the offset curve E to the circle point
+    # at the same arc-length fraction of E (matched by the section's own arc
+    # length instead, the clustered trailing-edge points went to nearly one
+    # circle point and the grid folded where the lines turned)
+    seg = np.linalg.norm(np.roll(E, -1, 0) - E, axis=1)
+    s = np.concatenate([[0.0], np.cumsum(seg)[:-1]]) / seg.sum()
+    ang = -2.0 * np.pi * s                              # same turning sense as the section loop
+    Cc = np.stack([0.5 + radius * np.cos(ang), radius * np.sin(ang)], 1)
     near = S[None] + np.minimum(d, reach) * nrm[None]
     far = E[None] + np.clip((d - reach) / (radius - reach), 0.0, 1.0) * (Cc - E)[None]
     P = np.where(d <= reach, near, far)                                 # [K+1, n, 2]

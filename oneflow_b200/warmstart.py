@@ -5,10 +5,15 @@ solve stays the fallback and the judge: a warm-started case counts as
 converged only when its RMS density residual falls below the same absolute
 threshold as the cold start's (the cold start's first residual x 1e-8).
 
-The case family here is the 2-D Euler bump channel (circular-arc bumps of
-thickness 4-10 % in a 3 x 1 channel, jittered triangles, Mach 0.3-0.6,
-first-order Roe, LU-SGS, colour-major sweeps, FP64): every case has its own
-mesh, so the network sees the geometry through its inputs."""
+Two case families, each case with its own mesh, so the network sees the
+geometry through its inputs:
+* BumpFamily: 2-D Euler bump channels (circular-arc bumps of thickness
+  4-10 % in a 3 x 1 channel, jittered triangles, Mach 0.3-0.6);
+* AirfoilFamily: 2-D Euler flow past NACA 4-digit sections drawn from the
+  batched configuration's shape distribution (camber 0-6 % at 40 % chord,
+  thickness 8-18 %) on triangle O-grids, Mach 0.3-0.6, AoA -2..6 degrees; 22
+  inputs, 16 of them shape features of the section.
+Both solve first-order Roe, LU-SGS, colour-major sweeps, FP64."""
 from __future__ import annotations
 
 import time
@@ -68,6 +73,96 @@ def state_from_prediction(pred: np.ndarray, mach: float, n_t: int) -> np.ndarray
     return q
 
 
+class BumpFamily:
+    """The bump channels: a case is (mesh, mach, thickness)."""
+    name = "bump"
+    description = ("2-D Euler bump channels, 64x32 quads -> 4,096 jittered triangles each, bump thickness 4-10 %, "
+                   "Mach 0.3-0.6, first-order Roe, LU-SGS, CFL 5, colour-major sweeps, FP64")
+    feature_names = FEATURES
+
+    def cases(self, n: int, seed: int):
+        return bump_cases(n, seed)
+
+    def params(self, case):
+        return case_params(case[1])
+
+    def features(self, solver: Solver, case) -> np.ndarray:
+        return features(solver, case[1], case[2])
+
+    def targets(self, q: np.ndarray, case) -> np.ndarray:
+        return targets(q, case[1], case[0].n_cells)
+
+    def state(self, pred: np.ndarray, case, n_t: int) -> np.ndarray:
+        return state_from_prediction(pred, case[1], n_t)
+
+
+AIRFOIL_STATIONS = (0.05, 0.1, 0.2, 0.3, 0.4, 0.6, 0.8, 0.95)
+
+
+def naca4_ordinates(m: float, p: float, t: float, xs) -> np.ndarray:
+    """upper and lower surface heights of a NACA 4-digit section at the chord
+    stations xs (taken on the camber line): [2 len(xs)] = upper..., lower..."""
+    yt, yc, th = meshgen.naca4_parts(m, p, t, xs)
+    return np.concatenate([yc + yt * np.cos(th), yc - yt * np.cos(th)])
+
+
+class AirfoilFamily:
+    """Inviscid flow past NACA 4-digit sections on triangle O-grids (96 points
+    on the section, 48 layers to a circle of 20 chords, 9,216 cells): a case is
+    a dict(mesh, m, t, mach, aoa).  Inputs (22): x, y, the wall distance, Mach,
+    sin and cos of the angle of attack and 16 shape features -- the upper and
+    lower surface heights at eight chord stations; outputs rho, u, v and p
+    scaled by the free-stream pressure."""
+    name = "airfoil"
+    description = ("2-D Euler NACA 4-digit sections (camber 0-6 % at 40 % chord, thickness 8-18 %), triangle O-grids "
+                   "of 9,216 cells (far field at 20 chords), Mach 0.3-0.6, AoA -2..6 deg, first-order Roe, LU-SGS, "
+                   "CFL 20, colour-major sweeps, FP64")
+    feature_names = (("x", "y", "wall_distance", "mach", "sin_aoa", "cos_aoa")
+                     + tuple(f"y_upper_{x:g}" for x in AIRFOIL_STATIONS)
+                     + tuple(f"y_lower_{x:g}" for x in AIRFOIL_STATIONS))
+
+    def __init__(self, n_surface: int = 96, n_layers: int = 48):
+        self.n_surface, self.n_layers = n_surface, n_layers
+
+    def cases(self, n: int, seed: int):
+        rng = np.random.default_rng(seed)
+        out = []
+        for _ in range(n):
+            m, t = rng.uniform(0.0, 0.06), rng.uniform(0.08, 0.18)
+            mach, aoa = rng.uniform(0.3, 0.6), rng.uniform(-2.0, 6.0)
+            mesh = meshgen.naca_ogrid(m, 0.4, t, self.n_surface, self.n_layers, n_quad_layers=0, y1=2e-3,
+                                      radius=20.0)
+            out.append(dict(mesh=mesh, m=m, t=t, mach=mach, aoa=aoa))
+        return out
+
+    def params(self, case):
+        return P.euler_bump(mach_ref=case["mach"], aoa_degree=case["aoa"], cflst=20.0, cfled=20.0, sweep_order=1)
+
+    def features(self, solver: Solver, case) -> np.ndarray:
+        N = solver.mesh.n_cells
+        x, y = solver.field("xcc")[:N], solver.field("ycc")[:N]
+        solver.calc_wall_dist()
+        d = solver.field("walldist")[:N]
+        a = np.radians(case["aoa"])
+        shape = naca4_ordinates(case["m"], 0.4, case["t"], AIRFOIL_STATIONS)
+        cols = [x, y, d, np.full(N, case["mach"]), np.full(N, np.sin(a)), np.full(N, np.cos(a))]
+        cols += [np.full(N, v) for v in shape]
+        return np.stack(cols, 1)
+
+    def targets(self, q: np.ndarray, case) -> np.ndarray:
+        return targets(q, case["mach"], case["mesh"].n_cells)
+
+    def state(self, pred: np.ndarray, case, n_t: int) -> np.ndarray:
+        return state_from_prediction(pred, case["mach"], n_t)
+
+
+FAMILIES = {"bump": BumpFamily, "airfoil": AirfoilFamily}
+
+
+def case_mesh(case):
+    return case["mesh"] if isinstance(case, dict) else case[0]
+
+
 def solve_to(solvers, threshold, batch: bool, chunk: int = 200, max_iters: int = 40000):
     """Iterate the solvers until each one's RMS density residual is below its
     threshold.  batch: one Batch for all (every case advances until the last
@@ -103,12 +198,13 @@ def solve_to(solvers, threshold, batch: bool, chunk: int = 200, max_iters: int =
     return iters, time.perf_counter() - t0
 
 
-def build_dataset(cases, drop: float = 1e-8):
+def build_dataset(family, cases, drop: float = 1e-8):
     """Converge every case (batched, cold start) and return the network's
-    inputs and outputs over all interior cells, and the iteration counts"""
+    inputs and outputs over all interior cells of the cases that reached the
+    threshold, and the iteration counts (None: not converged, left out)"""
     solvers = []
-    for mesh, mach, t in cases:
-        s = Solver(mesh, case_params(mach))
+    for case in cases:
+        s = Solver(case_mesh(case), family.params(case))
         s.init_flowfield()
         solvers.append(s)
     first = []
@@ -117,9 +213,10 @@ def build_dataset(cases, drop: float = 1e-8):
         first.append(s.res_history()[0, 0])
     iters, _ = solve_to(solvers, [f * drop for f in first], batch=True)
     X, Y = [], []
-    for (mesh, mach, t), s in zip(cases, solvers):
-        X.append(features(s, mach, t))
-        Y.append(targets(s.state(), mach, mesh.n_cells))
+    for case, s, it in zip(cases, solvers, iters):
+        if it is not None:
+            X.append(family.features(s, case))
+            Y.append(family.targets(s.state(), case))
         s.close()
     return np.concatenate(X), np.concatenate(Y), iters
 
@@ -137,15 +234,21 @@ class Normaliser:
 
 
 def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth: int = 6, train_steps: int = 3000,
-                   batch: int = 8192, lr: float = 1e-3, seed: int = 20261206, drop: float = 1e-8):
-    """Train on n_train converged cases, then solve n_test held-out cases to
-    the same absolute threshold four ways: cold one after another (the plain
-    solve), cold batched, warm one after another, warm batched.  Returns a
-    dict of iterations, wall seconds and the training summary."""
+                   batch: int = 8192, lr: float = 1e-3, seed: int = 20261206, drop: float = 1e-8,
+                   family: str = "bump", max_iters: int = 40000, polish_drop: float = 1e-11):
+    """Train on n_train converged cases of the family, then solve n_test
+    held-out cases to the same absolute threshold four ways: cold one after
+    another (the plain solve), cold batched, warm one after another, warm
+    batched.  Returns a dict of iterations, wall seconds, the training summary
+    and the largest difference of the lift and drag, warm against cold
+    (relative to the cold value, or to 1e-3 where that is smaller): at the
+    threshold, and after both solves went on (untimed) to the first residual x
+    polish_drop, where each has converged to its own steady state."""
     import torch
     from .mlp import MLP
+    fam = FAMILIES[family]()
     t0 = time.perf_counter()
-    X, Y, _ = build_dataset(bump_cases(n_train, seed), drop)
+    X, Y, train_iters = build_dataset(fam, fam.cases(n_train, seed), drop)
     t_data = time.perf_counter() - t0
     nx, ny = Normaliser(X), Normaliser(Y)
     xd = torch.tensor(nx.fwd(X), dtype=torch.float32, device="cuda").contiguous()
@@ -156,12 +259,12 @@ def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
 
-    test = bump_cases(n_test, seed + 1)
+    test = fam.cases(n_test, seed + 1)
 
     def cold():
         ss = []
-        for mesh, mach, t in test:
-            s = Solver(mesh, case_params(mach))
+        for case in test:
+            s = Solver(case_mesh(case), fam.params(case))
             s.init_flowfield()
             ss.append(s)
         return ss
@@ -176,34 +279,54 @@ def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth
     def warm():
         t0 = time.perf_counter()
         ss = []
-        for mesh, mach, t in test:
-            s = Solver(mesh, case_params(mach))
+        for case in test:
+            s = Solver(case_mesh(case), fam.params(case))
             s.init_flowfield()
-            f = torch.tensor(nx.fwd(features(s, mach, t)), dtype=torch.float32, device="cuda").contiguous()
+            f = torch.tensor(nx.fwd(fam.features(s, case)), dtype=torch.float32, device="cuda").contiguous()
             pred = ny.inv(net.predict(f).cpu().numpy().astype(np.float64))
-            s.upload_state(state_from_prediction(pred, mach, s.nT))
+            s.upload_state(fam.state(pred, case, s.nT))
             ss.append(s)
         return ss, time.perf_counter() - t0
 
-    out = {"family": "2-D Euler bump channels, 64x32 quads -> 4,096 jittered triangles each, bump thickness "
-                     "4-10 %, Mach 0.3-0.6, first-order Roe, LU-SGS, CFL 5, colour-major sweeps, FP64",
-           "features": list(FEATURES), "network": f"{X.shape[1]}->{depth}x{width} GELU->{Y.shape[1]}, BF16 tcgen05.mma GEMMs",
-           "train_cases": n_train, "test_cases": n_test, "train_samples": int(X.shape[0]),
+    out = {"family": fam.description,
+           "features": list(fam.feature_names),
+           "network": f"{X.shape[1]}->{depth}x{width} GELU->{Y.shape[1]}, BF16 tcgen05.mma GEMMs",
+           "train_cases": n_train, "train_cases_converged": int(sum(i is not None for i in train_iters)),
+           "test_cases": n_test, "train_samples": int(X.shape[0]),
            "train_steps": train_steps, "batch": batch, "lr": lr,
            "loss_first": float(losses[0]), "loss_last": float(np.mean(losses[-50:])),
            "data_s": t_data, "train_s": t_train, "threshold": f"cold first residual x {drop:g}"}
+    forces = {}
     for name, is_warm, batched in (("plain", False, False), ("cold_batched", False, True),
                                    ("warm", True, False), ("warm_batched", True, True)):
         if is_warm:
             ss, t_pred = warm()
         else:
             ss, t_pred = cold(), 0.0
-        it, t = solve_to(ss, thr, batch=batched)
+        it, t = solve_to(ss, thr, batch=batched, max_iters=max_iters)
         out[name] = {"iterations_mean": float(np.mean([i if i is not None else np.nan for i in it])),
                      "converged": int(sum(i is not None for i in it)), "seconds": t + t_pred,
                      "predict_s": t_pred}
+        if name in ("plain", "warm"):
+            ok = [i is not None for i in it]
+            forces[name] = [(s.forces()[9:11] if k else None) for s, k in zip(ss, ok)]
+            # untimed: on to the tighter threshold, every case in one batch
+            sub = [s for s, k in zip(ss, ok) if k]
+            tight = [tr / drop * polish_drop for tr, k in zip(thr, ok) if k]
+            it2, _ = solve_to(sub, tight, batch=True, max_iters=max_iters)
+            fp = iter([(s.forces()[9:11] if i is not None else None) for s, i in zip(sub, it2)])
+            forces[name + "_polished"] = [next(fp) if k else None for k in ok]
         for s in ss:
             s.close()
+
+    def compare(a, b):
+        errs = [np.abs(w - c) / np.maximum(np.abs(c), 1e-3) for c, w in zip(forces[a], forces[b])
+                if c is not None and w is not None]
+        return {"cases": len(errs), "cl_rel_max": float(max(e[0] for e in errs)) if errs else None,
+                "cd_rel_max": float(max(e[1] for e in errs)) if errs else None}
+
+    out["forces_warm_vs_cold"] = {"at_threshold": compare("plain", "warm"),
+                                  f"at_{polish_drop:g}": compare("plain_polished", "warm_polished")}
     out["speedup_warm_batched_vs_plain"] = out["plain"]["seconds"] / out["warm_batched"]["seconds"]
     net.close()
     return out

@@ -1,8 +1,8 @@
-"""Learned warm start end to end on a small budget: converged bump solutions
-from this solver train the BF16 tensor-core MLP, whose predictions start
-held-out cases; the cold-started solve is the judge -- every warm-started
-case must reach the cold start's absolute threshold (first residual x 1e-8),
-and it must get there in fewer iterations."""
+"""Learned warm start end to end on a small budget: converged solutions from
+this solver (bump channels; NACA airfoils) train the BF16 tensor-core MLP,
+whose predictions start held-out cases; the cold-started solve is the judge --
+every warm-started case must reach the cold start's absolute threshold (first
+residual x 1e-8), and it must get there in fewer iterations."""
 import numpy as np
 import pytest
 
@@ -21,6 +21,25 @@ def test_warm_start_converges_to_the_cold_threshold_in_fewer_iterations():
     assert r["warm"]["iterations_mean"] == r["warm_batched"]["iterations_mean"]
     # measured 5,563 against 7,559 with this budget
     assert r["warm"]["iterations_mean"] < 0.9 * r["plain"]["iterations_mean"]
+
+
+def test_airfoil_warm_start_converges_and_keeps_the_forces():
+    # NACA sections of the batched configuration's shape distribution (22
+    # inputs, 16 of them shape features), inviscid: the warm-started solves
+    # reach the cold threshold in fewer iterations and converge to the same
+    # lift and drag
+    r = warmstart.run_experiment(n_train=24, n_test=4, train_steps=1500, family="airfoil")
+    assert len(r["features"]) == 22
+    assert r["train_cases_converged"] == r["train_cases"]
+    assert r["loss_last"] < 0.2 * r["loss_first"]
+    for k in ("plain", "cold_batched", "warm", "warm_batched"):
+        assert r[k]["converged"] == r["test_cases"], k
+    assert r["warm"]["iterations_mean"] == r["warm_batched"]["iterations_mean"]
+    assert r["warm"]["iterations_mean"] < r["plain"]["iterations_mean"]
+    # both converge to the same steady state: lift and drag within 1e-6 once
+    # the solves have gone on to a 1e-11 drop
+    f = r["forces_warm_vs_cold"]["at_1e-11"]
+    assert f["cases"] == r["test_cases"] and f["cl_rel_max"] < 1e-6 and f["cd_rel_max"] < 1e-6, f
 
 
 def test_prediction_state_is_physical():

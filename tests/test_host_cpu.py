@@ -213,3 +213,21 @@ def test_swept_wing_mesh_is_closed_and_classified():
     # wall faces: the wing's quadrilaterals (n per slab) and the tip cap (n / 2 cells)
     assert counts[2] == n * 6 + (n // 2)
     assert counts[4] > 0 and counts[1] == counts[5] == counts[6] == 0
+
+
+@pytest.mark.parametrize("m,t,y1,quads", [(0.06, 0.08, 2e-3, 0), (0.0, 0.18, 2e-3, 0), (0.06, 0.08, 8.6e-6, 24),
+                                          (0.03, 0.12, 1e-5, 24)])
+def test_naca_ogrid_has_no_folded_cells(m, t, y1, quads):
+    # node k * n + i is point i of layer k: every grid quadrilateral between
+    # two layers keeps the orientation of the section loop (a fold behind the
+    # trailing edge of thin cambered sections inverted some, and the cells
+    # there overlapped), and the cells tile the ring between section and circle
+    n, K = 96, 48
+    msh = meshgen.naca_ogrid(m, 0.4, t, n, K, n_quad_layers=quads, y1=y1, radius=20.0)
+    x, y = msh.x.reshape(K + 1, n), msh.y.reshape(K + 1, n)
+    xa, ya, xd, yd = x[:-1], y[:-1], x[1:], y[1:]
+    xb, yb, xc, yc = np.roll(xa, -1, 1), np.roll(ya, -1, 1), np.roll(xd, -1, 1), np.roll(yd, -1, 1)
+    area = 0.5 * ((xa * yb - xb * ya) + (xb * yc - xc * yb) + (xc * yd - xd * yc) + (xd * ya - xa * yd))
+    assert np.all(area < 0) or np.all(area > 0)
+    ring = lambda k: 0.5 * abs(np.sum(x[k] * np.roll(y[k], -1) - np.roll(x[k], -1) * y[k]))
+    assert abs(np.abs(area).sum() - (ring(K) - ring(0))) < 1e-9 * ring(K)
