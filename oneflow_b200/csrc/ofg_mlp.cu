@@ -319,6 +319,21 @@ __global__ void k_reduce_parts(int64_t n, int parts, const float *part, float *o
     out[i] = a;
 }
 
+// loss of one minibatch: the rows' squared errors summed in FP64 in a fixed
+// order (thread-strided, then a shared-memory tree), one block
+__global__ void k_batch_loss(int rows, double scale, const float *rowErr, float *loss) {
+    __shared__ double s[256];
+    double a = 0.0;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) a += rowErr[r];
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *loss = float(s[0] * scale);
+}
+
 // Adam on the FP32 master copy, BF16 working copy refreshed; padded entries
 // (mask 0) stay zero
 __global__ void k_adam(int64_t n, float *w, float *m, float *v, const float *g, const unsigned char *mask,
@@ -657,25 +672,29 @@ int ofg_mlp_train(ofg_mlp *m, const float *x, const float *y, int64_t n, int bat
     int rc = ensure_work(m, batch);
     if (rc) return rc;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    std::vector<float> e(batch);
+    // the minibatch losses stay on the device until the end: no host
+    // synchronisation between steps
+    float *dLoss = nullptr;
+    if (loss_out && steps > 0) MCK(cudaMalloc(&dLoss, (size_t)steps * sizeof(float)));
     for (int s = 0; s < steps; ++s) {
         k_gather<<<blocks(batch, 128), 128>>>(batch, n, m->nin, m->K[0], m->nout, x, y, seed, uint64_t(s), m->H[0],
                                               m->Tb);
-        if ((rc = forward(m, batch, true)) || (rc = backward(m, batch))) return rc;
+        if ((rc = forward(m, batch, true)) || (rc = backward(m, batch))) {
+            cudaFree(dLoss);
+            return rc;
+        }
         ++m->adamStep;
         float c1 = 1.0f - std::pow(b1, float(m->adamStep)), c2 = 1.0f - std::pow(b2, float(m->adamStep));
         k_adam<<<blocks(m->nw, 256), 256>>>(m->nw, m->w, m->mw, m->vw, m->gw, m->wmask, m->wb, lr, b1, b2, eps, c1, c2);
         k_adam<<<blocks(m->nb, 256), 256>>>(m->nb, m->b, m->mb, m->vb, m->gb, m->bmask, nullptr, lr, b1, b2, eps, c1,
                                             c2);
-        if (loss_out) {
-            MCK(cudaMemcpy(e.data(), m->rowErr, batch * sizeof(float), cudaMemcpyDeviceToHost));
-            double t = 0.0;
-            for (float v : e) t += v;
-            loss_out[s] = float(t / (double(batch) * m->nout));
-        }
+        if (dLoss) k_batch_loss<<<1, 256>>>(batch, 1.0 / (double(batch) * m->nout), m->rowErr, dLoss + s);
     }
-    MCK(cudaGetLastError());
-    MCK(cudaDeviceSynchronize());
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && dLoss) e = cudaMemcpy(loss_out, dLoss, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(dLoss);
+    if (e != cudaSuccess) return m->fail(OFG_E_CUDA, std::string("ofg_mlp_train: ") + cudaGetErrorString(e));
     return gemm_status(m);
 }
 
