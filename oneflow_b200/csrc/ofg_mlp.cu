@@ -2,7 +2,7 @@
 // activations on the tensor cores (tcgen05.mma with FP32 accumulation in
 // tensor memory), FP32 master weights, Adam.  Not part of the reference:
 // it learns flow fields from solutions this solver produced, and the
-// cold-started solve remains the fallback and the judge of convergence.
+// cold-started solve remains the fallback and the arbiter of convergence.
 //
 // Network: n_in -> width (GELU) -> ... (depth hidden layers) -> n_out.  Every
 // matrix dimension is padded to a multiple of 16; padded inputs are zero and

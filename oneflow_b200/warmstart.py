@@ -1,7 +1,7 @@
 """Learned warm start of steady solves: a coordinate MLP (BF16 tensor-core
 kernels, oneflow_b200.mlp) trained on converged solutions this solver
 produced, predicting the initial flow field of a new case.  The cold-started
-solve stays the fallback and the judge: a warm-started case counts as
+solve stays the fallback and the arbiter: a warm-started case counts as
 converged only when its RMS density residual falls below the same absolute
 threshold as the cold start's (the cold start's first residual x 1e-8).
 

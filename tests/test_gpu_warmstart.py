@@ -1,6 +1,6 @@
 """Learned warm start end to end on a small budget: converged solutions from
 this solver (bump channels; NACA airfoils) train the BF16 tensor-core MLP,
-whose predictions start held-out cases; the cold-started solve is the judge --
+whose predictions start held-out cases; the cold-started solve is the arbiter --
 every warm-started case must reach the cold start's absolute threshold (first
 residual x 1e-8), and it must get there in fewer iterations."""
 import numpy as np
