@@ -12,7 +12,8 @@ geometry through its inputs:
 * AirfoilFamily: 2-D Euler flow past NACA 4-digit sections drawn from the
   batched configuration's shape distribution (camber 0-6 % at 40 % chord,
   thickness 8-18 %) on triangle O-grids, Mach 0.3-0.6, AoA -2..6 degrees; 22
-  inputs, 16 of them shape features of the section.
+  inputs, 16 of them shape features of the section, the others polar
+  coordinates about mid-chord, the wall distance and the flow parameters.
 Both solve first-order Roe, LU-SGS, colour-major sweeps, FP64."""
 from __future__ import annotations
 
@@ -76,6 +77,7 @@ def state_from_prediction(pred: np.ndarray, mach: float, n_t: int) -> np.ndarray
 class BumpFamily:
     """The bump channels: a case is (mesh, mach, thickness)."""
     name = "bump"
+    train_steps = 3000
     description = ("2-D Euler bump channels, 64x32 quads -> 4,096 jittered triangles each, bump thickness 4-10 %, "
                    "Mach 0.3-0.6, first-order Roe, LU-SGS, CFL 5, colour-major sweeps, FP64")
     feature_names = FEATURES
@@ -109,17 +111,20 @@ def naca4_ordinates(m: float, p: float, t: float, xs) -> np.ndarray:
 class AirfoilFamily:
     """Inviscid flow past NACA 4-digit sections on triangle O-grids (96 points
     on the section, 48 layers to a circle of 20 chords, 9,216 cells): a case is
-    a dict(mesh, m, t, mach, aoa).  Inputs (22): x, y, the wall distance, Mach,
-    sin and cos of the angle of attack and 16 shape features -- the upper and
-    lower surface heights at eight chord stations; outputs rho, u, v and p
-    scaled by the free-stream pressure."""
+    a dict(mesh, m, t, mach, aoa).  Inputs (22): the log of the distance r from
+    mid-chord, the cosine and sine of the polar angle about mid-chord, the log
+    of the wall distance, Mach, the angle of attack and 16 shape features --
+    the upper and lower surface heights at eight chord stations (polar inputs
+    resolve the near field of a domain 40 chords wide better than x and y);
+    outputs rho, u, v and p scaled by the free-stream pressure."""
     name = "airfoil"
     description = ("2-D Euler NACA 4-digit sections (camber 0-6 % at 40 % chord, thickness 8-18 %), triangle O-grids "
                    "of 9,216 cells (far field at 20 chords), Mach 0.3-0.6, AoA -2..6 deg, first-order Roe, LU-SGS, "
                    "CFL 20, colour-major sweeps, FP64")
-    feature_names = (("x", "y", "wall_distance", "mach", "sin_aoa", "cos_aoa")
+    feature_names = (("log_r", "cos_theta", "sin_theta", "log_wall_distance", "mach", "aoa_deg")
                      + tuple(f"y_upper_{x:g}" for x in AIRFOIL_STATIONS)
                      + tuple(f"y_lower_{x:g}" for x in AIRFOIL_STATIONS))
+    train_steps = 10000
 
     def __init__(self, n_surface: int = 96, n_layers: int = 48):
         self.n_surface, self.n_layers = n_surface, n_layers
@@ -140,12 +145,12 @@ class AirfoilFamily:
 
     def features(self, solver: Solver, case) -> np.ndarray:
         N = solver.mesh.n_cells
-        x, y = solver.field("xcc")[:N], solver.field("ycc")[:N]
+        dx, dy = solver.field("xcc")[:N] - 0.5, solver.field("ycc")[:N]
         solver.calc_wall_dist()
         d = solver.field("walldist")[:N]
-        a = np.radians(case["aoa"])
+        r = np.sqrt(dx * dx + dy * dy)
         shape = naca4_ordinates(case["m"], 0.4, case["t"], AIRFOIL_STATIONS)
-        cols = [x, y, d, np.full(N, case["mach"]), np.full(N, np.sin(a)), np.full(N, np.cos(a))]
+        cols = [np.log(r), dx / r, dy / r, np.log(d + 1e-3), np.full(N, case["mach"]), np.full(N, case["aoa"])]
         cols += [np.full(N, v) for v in shape]
         return np.stack(cols, 1)
 
@@ -233,7 +238,7 @@ class Normaliser:
         return a * self.std + self.mean
 
 
-def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth: int = 6, train_steps: int = 3000,
+def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth: int = 6, train_steps: int = None,
                    batch: int = 8192, lr: float = 1e-3, seed: int = 20261206, drop: float = 1e-8,
                    family: str = "bump", max_iters: int = 40000, polish_drop: float = 1e-11):
     """Train on n_train converged cases of the family, then solve n_test
@@ -247,6 +252,8 @@ def run_experiment(n_train: int = 192, n_test: int = 32, width: int = 256, depth
     import torch
     from .mlp import MLP
     fam = FAMILIES[family]()
+    if train_steps is None:
+        train_steps = fam.train_steps
     t0 = time.perf_counter()
     X, Y, train_iters = build_dataset(fam, fam.cases(n_train, seed), drop)
     t_data = time.perf_counter() - t0
