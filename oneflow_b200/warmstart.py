@@ -77,7 +77,7 @@ def state_from_prediction(pred: np.ndarray, mach: float, n_t: int) -> np.ndarray
 class BumpFamily:
     """The bump channels: a case is (mesh, mach, thickness)."""
     name = "bump"
-    train_steps = 3000
+    train_steps = 20000
     description = ("2-D Euler bump channels, 64x32 quads -> 4,096 jittered triangles each, bump thickness 4-10 %, "
                    "Mach 0.3-0.6, first-order Roe, LU-SGS, CFL 5, colour-major sweeps, FP64")
     feature_names = FEATURES
@@ -124,7 +124,7 @@ class AirfoilFamily:
     feature_names = (("log_r", "cos_theta", "sin_theta", "log_wall_distance", "mach", "aoa_deg")
                      + tuple(f"y_upper_{x:g}" for x in AIRFOIL_STATIONS)
                      + tuple(f"y_lower_{x:g}" for x in AIRFOIL_STATIONS))
-    train_steps = 10000
+    train_steps = 20000
 
     def __init__(self, n_surface: int = 96, n_layers: int = 48):
         self.n_surface, self.n_layers = n_surface, n_layers
