@@ -231,3 +231,22 @@ def test_naca_ogrid_has_no_folded_cells(m, t, y1, quads):
     assert np.all(area < 0) or np.all(area > 0)
     ring = lambda k: 0.5 * abs(np.sum(x[k] * np.roll(y[k], -1) - np.roll(x[k], -1) * y[k]))
     assert abs(np.abs(area).sum() - (ring(K) - ring(0))) < 1e-9 * ring(K)
+
+
+def test_airfoil_shape_features():
+    # the 16 shape inputs of the airfoil warm-start family: upper and lower
+    # surface heights at eight chord stations; symmetric sections give
+    # mirror-image ordinates equal to the thickness polynomial, camber shifts
+    # both by the camber line, and they lie on the mesh generator's section
+    from oneflow_b200 import warmstart
+    xs = np.array(warmstart.AIRFOIL_STATIONS)
+    o = warmstart.naca4_ordinates(0.0, 0.4, 0.12, xs)
+    yt = 5 * 0.12 * (0.2969 * np.sqrt(xs) - 0.1260 * xs - 0.3516 * xs ** 2 + 0.2843 * xs ** 3 - 0.1036 * xs ** 4)
+    assert o.shape == (16,) and np.allclose(o[:8], yt, rtol=0, atol=1e-15) and np.allclose(o[8:], -yt, atol=1e-15)
+    c = warmstart.naca4_ordinates(0.04, 0.4, 0.12, xs)
+    assert np.all(c[:8] > c[8:]) and abs(c[4] + c[12] - 2 * 0.04) < 1e-12   # camber line at p = 0.4 is m
+    S = meshgen.naca4_surface(0.0, 0.4, 0.12, 200)
+    up = S[S[:, 1] > 0]
+    i = np.argsort(up[:, 0])
+    assert np.allclose(np.interp(xs, up[i, 0], up[i, 1]), o[:8], atol=2e-4)
+    assert len(warmstart.AirfoilFamily.feature_names) == 22
