@@ -36,8 +36,9 @@ inline int pad16(int v) { return (v + 15) / 16 * 16; }
 // along M / N; K-major or MN-major as the operand lies in memory), one
 // thread issues tcgen05.mma (M 128, N the tile's width, K 16, FP32
 // accumulation in tensor memory) and tcgen05.commit arrives on the stage's
-// mbarrier, so the loads of the next K block overlap the MMAs of the last
-// (two stages).  The epilogue
+// mbarrier.  The operand tiles arrive by cp.async 16-byte copies into a ring
+// of four stages: the copies of the next three K blocks are in flight while
+// the MMAs of the current one run.  The epilogue
 // reads the accumulator with tcgen05.ld: warp w holds rows 32w..32w+31 (its
 // tensor-memory lanes), 16 columns per load.  Every wait is bounded; a wait
 // that runs out sets g_gemm_status and the CTA frees its tensor memory and
@@ -46,8 +47,9 @@ inline int pad16(int v) { return (v + 15) / 16 * 16; }
 constexpr int GT = 128;                       // threads of a GEMM block
 constexpr int BM = 128, BN = 128, BK = 64;    // block tile
 constexpr int SBO = (BK / 8) * 128;           // bytes between 8-row core-matrix groups
+constexpr int NSTAGE = 4;                     // K blocks in flight
 constexpr int TILE_A = BM * BK * 2, TILE_B = BN * BK * 2, STAGE = TILE_A + TILE_B;
-constexpr int SMEM_GEMM = 2 * STAGE + 1024 + 64;   // two stages, 1,024-B alignment slack, barriers
+constexpr int SMEM_GEMM = NSTAGE * STAGE + 1024 + 8 * NSTAGE + 16;   // stages, alignment slack, barriers, slot
 constexpr unsigned WAIT_LIMIT = 1u << 20;     // try_wait rounds before a wait gives up
 
 __device__ unsigned g_gemm_status;            // nonzero: a GEMM wait ran out
@@ -118,46 +120,47 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Stage the rows [r0, r0 + nr) x K block [kb, kb + BK) of an operand whose
-// element (r, k) is g[r * ld + k] (T false: K contiguous, staged K-major: a
-// core matrix holds 8 rows x 8 K) or g[k * ld + r] (T true: rows contiguous,
-// staged MN-major: a core matrix holds 8 K x 8 rows); either way core
-// matrices lie 128 B apart along K and SBO apart along the rows, and every
-// 16-byte chunk of the source is one 16-byte store.  A warp's 32 stores cover
-// 512 contiguous bytes.  Rows at or beyond `rows` and K at or beyond k1 are
-// zero.  rows, nr, ld, kb and k1 are multiples of 8; nr <= 128.
+// Start the copies of rows [r0, r0 + nr) x K block [kb, kb + BK) of an
+// operand whose element (r, k) is g[r * ld + k] (T false: K contiguous,
+// staged K-major: a core matrix holds 8 rows x 8 K) or g[k * ld + r] (T true:
+// rows contiguous, staged MN-major: a core matrix holds 8 K x 8 rows); either
+// way core matrices lie 128 B apart along K and SBO apart along the rows, and
+// every 16-byte chunk of the source is one 16-byte cp.async.  A warp's 32
+// copies cover 512 contiguous bytes of shared memory.  Chunks of rows at or
+// beyond `rows` or of K at or beyond k1 are filled with zeros (source size
+// 0).  rows, nr, ld, kb and k1 are multiples of 8; nr <= 128.
 template <bool T>
 __device__ __forceinline__ void stage_tile(unsigned char *s, const bf16 *__restrict__ g, int ld, int rows, int r0,
                                            int nr, int kb, int k1) {
     static_assert(BK == 64, "eight 8-element K chunks per block");
     const int items = nr * (BK / 8), nc = nr >> 3;
-    uint4 v[8];
-    uint32_t off[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
         const int i = threadIdx.x + u * GT;
-        v[u] = make_uint4(0u, 0u, 0u, 0u);
-        off[u] = 0xFFFFFFFFu;
         if (i < items) {
             int r, k;   // first row and K of the chunk
+            uint32_t off;
             if (!T) {   // i: row % 8, then K chunk, then row / 8
                 r = (i & 7) + ((i >> 6) << 3);
                 k = ((i >> 3) & 7) * 8;
-                off[u] = (r >> 3) * SBO + (k >> 3) * 128 + (r & 7) * 16;
+                off = (r >> 3) * SBO + (k >> 3) * 128 + (r & 7) * 16;
             } else {    // i: K % 8, then row chunk, then K / 8
                 k = (i & 7) + ((i >> 3) / nc) * 8;
                 r = ((i >> 3) % nc) * 8;
-                off[u] = (r >> 3) * SBO + (k >> 3) * 128 + (k & 7) * 16;
+                off = (r >> 3) * SBO + (k >> 3) * 128 + (k & 7) * 16;
             }
-            if (r0 + r < rows && kb + k < k1)
-                v[u] = *reinterpret_cast<const uint4 *>(T ? g + (size_t)(kb + k) * ld + r0 + r
-                                                          : g + (size_t)(r0 + r) * ld + kb + k);
+            const bool in = r0 + r < rows && kb + k < k1;
+            const bf16 *src = in ? (T ? g + (size_t)(kb + k) * ld + r0 + r : g + (size_t)(r0 + r) * ld + kb + k) : g;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(s + off)), "l"(src),
+                         "r"(in ? 16 : 0)
+                         : "memory");
         }
     }
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-        if (off[u] != 0xFFFFFFFFu) *reinterpret_cast<uint4 *>(s + off[u]) = v[u];
 }
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // C[M x N] (FP32, row-major, ldc) = op(A)[M x K] op(B)[K x N] over the K range
 // [k0, k1) of blockIdx.z's chunk, into C + blockIdx.z * zstride.  op(A): A
@@ -172,15 +175,14 @@ __global__ void __launch_bounds__(GT, 1) k_gemm(int M, int N, int K, int kchunk,
     extern __shared__ unsigned char smem_raw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                           ~uintptr_t(1023));
-    const uint32_t bar0 = smem_u32(sm + 2 * STAGE), slot = smem_u32(sm + 2 * STAGE + 16);
+    const uint32_t bar0 = smem_u32(sm + NSTAGE * STAGE), slot = smem_u32(sm + NSTAGE * STAGE + 8 * NSTAGE);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN, nt = min(BN, N - n0);
     const int k0 = blockIdx.z * kchunk, k1 = min(K, k0 + kchunk);
     const int nkb = k1 > k0 ? (k1 - k0 + BK - 1) / BK : 0;
     C += blockIdx.z * zstride;
     if (threadIdx.x == 0) {
-        mbar_init(bar0);
-        mbar_init(bar0 + 8);
+        for (int q = 0; q < NSTAGE; ++q) mbar_init(bar0 + 8 * q);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -191,32 +193,43 @@ __global__ void __launch_bounds__(GT, 1) k_gemm(int M, int N, int K, int kchunk,
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(sm + 2 * STAGE + 16);
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(sm + NSTAGE * STAGE + 8 * NSTAGE);
     const uint32_t idesc = instr_desc(nt, AT ? 1u : 0u, BT ? 0u : 1u);
+    // start the copies of K block kb into its stage; one commit group per call
+    // (empty past the last block), so that the group count stays uniform
+    auto issue = [&](int kb) {
+        if (kb < nkb) {
+            unsigned char *sa = sm + (kb % NSTAGE) * STAGE;
+            const int kbase = k0 + kb * BK;
+            stage_tile<AT>(sa, A, lda, M, m0, BM, kbase, k1);
+            stage_tile<!BT>(sa + TILE_A, B, ldb, N, n0, nt, kbase, k1);
+        }
+        cp_async_commit();
+    };
+    for (int q = 0; q < NSTAGE - 1; ++q) issue(q);
     int ok = 1, issued = 0;   // K blocks whose MMAs have been committed (the same in every thread)
     for (int kb = 0; kb < nkb; ++kb) {
-        const int st = kb & 1;
-        // the MMAs of K block kb - 2 read this stage: wait for their commit
-        if (kb >= 2) ok = mbar_wait(bar0 + 8 * st, ((kb - 2) >> 1) & 1);
-        if (!__syncthreads_and(ok)) break;
-        issued = kb + 1;
-        unsigned char *sa = sm + st * STAGE, *sb = sa + TILE_A;
-        const int kbase = k0 + kb * BK;
-        stage_tile<AT>(sa, A, lda, M, m0, BM, kbase, k1);
-        stage_tile<!BT>(sb, B, ldb, N, n0, nt, kbase, k1);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic-proxy stores -> tensor core
-        __syncthreads();
+        const int st = kb % NSTAGE;
+        cp_async_wait<NSTAGE - 2>();                                    // this thread's copies of block kb
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // visible to the tensor core
+        __syncthreads();                                                // everyone's
         if (threadIdx.x == 0) {
             tc_fence_after();
-            const int nk16 = min(BK, k1 - kbase) / 16;
-            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+            const int nk16 = min(BK, k1 - (k0 + kb * BK)) / 16;
+            const uint32_t a0 = smem_u32(sm + st * STAGE), b0 = a0 + TILE_A;
             for (int j = 0; j < nk16; ++j)
                 mma_bf16(tmem, smem_desc(a0 + j * 256), smem_desc(b0 + j * 256), idesc, (kb | j) != 0);
             mma_commit(bar0 + 8 * st);
         }
+        issued = kb + 1;
+        // the next copies go to the stage of block kb - 1: its MMAs must be done
+        if (kb >= 1) ok = mbar_wait(bar0 + 8 * ((kb - 1) % NSTAGE), ((kb - 1) / NSTAGE) & 1);
+        if (!__syncthreads_and(ok)) break;
+        issue(kb + NSTAGE - 1);
     }
+    cp_async_wait<0>();
     // the last commit covers every MMA issued before it
-    if (ok && issued > 0) ok = mbar_wait(bar0 + 8 * ((issued - 1) & 1), ((issued - 1) >> 1) & 1);
+    if (ok && issued > 0) ok = mbar_wait(bar0 + 8 * ((issued - 1) % NSTAGE), ((issued - 1) / NSTAGE) & 1);
     ok = __syncthreads_and(ok);
     tc_fence_after();
     if (ok) {
@@ -240,7 +253,7 @@ __global__ void __launch_bounds__(GT, 1) k_gemm(int M, int N, int K, int kchunk,
     } else if (threadIdx.x == 0) {
         atomicOr(&g_gemm_status, 1u);
         // give MMAs still in flight a bounded time to retire before the memory is freed
-        if (issued > 0) mbar_wait(bar0 + 8 * ((issued - 1) & 1), ((issued - 1) >> 1) & 1);
+        if (issued > 0) mbar_wait(bar0 + 8 * ((issued - 1) % NSTAGE), ((issued - 1) / NSTAGE) & 1);
     }
     tc_fence_before();
     __syncthreads();
