@@ -125,3 +125,90 @@ def test_oracle_positivity_fix_runs_on_a_violent_state():
     o.step(3)
     assert o.field("nfixes")[0] > 10
     assert np.isfinite(o.q()).all()
+
+
+def _lsq_case(name):
+    if name == "tri2d":
+        return meshgen.bump_channel(32, 16), 2
+    return meshgen.bump_box_mixed(8, 6, 4), 3
+
+
+def _interior(m):
+    near = np.zeros(m.n_cells, bool)
+    near[m.lc[:m.n_bfaces]] = True
+    return ~near
+
+
+@pytest.mark.parametrize("name", ["tri2d", "mixed3d"])
+def test_least_squares_gradient_is_exact_for_linear_fields(name):
+    # the weighted least-squares gradient (igrad = 2) has no reference
+    # implementation; pinned analytically: it reproduces a linear field's
+    # gradient exactly in every cell whose faces are all interior (boundary
+    # cells see their ghosts, which UPDATE_RESIDUALS sets by the boundary rules)
+    m, dim = _lsq_case(name)
+    o = Oracle(m, P.defaults(dimension=dim, ischeme=1, igrad=2, ilim=0, vismodel=0, mach_ref=0.5))
+    o.init()
+    nT, N = o.nT, m.n_cells
+    x, y, z = o.field("xcc"), o.field("ycc"), o.field("zcc")
+    g = np.array([[0.01, -0.02, 0.03], [0.1, 0.05, -0.02], [-0.04, 0.02, 0.01], [0.02, -0.01, 0.03], [0.3, -0.1, 0.2]])
+    if dim == 2:
+        g[:, 2] = 0.0
+        g[3] = 0.0
+    base = np.array([1.0, 0.5, 0.1, 0.0, 1.0 / (1.4 * 0.25)])
+    o.set_q(base[:, None] + g @ np.stack([x, y, z]))
+    o.task("UPDATE_RESIDUALS")
+    G = np.stack([o.field(f).reshape(5, nT)[:, :N] for f in ("dqdx", "dqdy", "dqdz")], 2)
+    inner = _interior(m)
+    assert inner.sum() > N // 4
+    assert np.abs(G[:, inner] - g[:, None, :]).max() < 1e-12
+
+
+@pytest.mark.parametrize("name", ["tri2d", "mixed3d"])
+def test_venkatakrishnan_kh3_limiter_matches_an_independent_restatement(name):
+    # the eps^2 = (K h)^3 form (venkat_kh3 = 1, no reference implementation):
+    # per cell the minimum over its faces of Venkatakrishnan's function of the
+    # neighbour extreme and the face extrapolation grad q . (x_f - x_c), with
+    # h = vol^(1/dim), restated here from the published formula
+    m, dim = _lsq_case(name)
+    K = 0.3
+    o = Oracle(m, P.defaults(dimension=dim, ischeme=1, igrad=2, ilim=2, vencat_coef=K, venkat_kh3=1, vismodel=0,
+                             mach_ref=0.5))
+    o.init()
+    nT, N = o.nT, m.n_cells
+    x, y, z = o.field("xcc"), o.field("ycc"), o.field("zcc")
+    base = np.array([1.0, 0.5, 0.1, 0.0, 1.0 / (1.4 * 0.25)])
+    amp = np.array([0.05, 0.1, 0.05, 0.0 if dim == 2 else 0.05, 0.2])
+    o.set_q(base[:, None] + amp[:, None] * np.sin(3 * x + 2 * y + (z if dim == 3 else 0.0))[None])
+    o.task("UPDATE_RESIDUALS")
+    q = o.q()
+    G = np.stack([o.field(f).reshape(5, nT) for f in ("dqdx", "dqdy", "dqdz")], 2)
+    lim = o.field("limiter").reshape(5, nT)
+    vol = o.field("vol")
+    xf = np.stack([o.field("xfc"), o.field("yfc"), o.field("zfc")], 1)
+    xc = np.stack([x, y, z], 1)
+    faces = [[] for _ in range(N)]
+    for f in range(m.n_faces):
+        faces[m.lc[f]].append(f)
+        if f >= m.n_bfaces:
+            faces[m.rc[f]].append(f)
+    inner = _interior(m)
+    limited = 0
+    for c in np.nonzero(inner)[0]:
+        nbrs = [m.rc[f] if m.lc[f] == c else m.lc[f] for f in faces[c]]
+        h = np.sqrt(vol[c]) if dim == 2 else np.cbrt(vol[c])
+        eps = (K * h) ** 3 + 1e-40
+        for e in range(5):
+            if dim == 2 and e == 3:
+                continue
+            mx = max(q[e, nbrs].max() - q[e, c], 0.0)
+            mn = min(q[e, nbrs].min() - q[e, c], 0.0)
+            phi = 1.0
+            for f in faces[c]:
+                d2 = G[e, c] @ (xf[f] - xc[c])
+                if abs(d2) <= 1e-40:
+                    continue
+                d1 = mx if d2 > 0 else mn
+                phi = min(phi, (d1 * d1 + eps + 2 * d1 * d2) / (d1 * d1 + 2 * d2 * d2 + d1 * d2 + eps))
+            assert abs(phi - lim[e, c]) < 1e-14, (c, e, phi, lim[e, c])
+            limited += phi < 1.0
+    assert limited > 100
